@@ -1,0 +1,76 @@
+"""ctypes binding of libandfn_b200.so (include/andfn_b200.h).
+
+The library must exist in-tree; there is no fallback implementation, so a
+missing or unloadable library raises immediately.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+from .records import AndfnConstants, AndfnLayout, AndfnSolveStats
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libandfn_b200.so")
+
+EXPORTS = ("andfn_b200_solve", "andfn_b200_create", "andfn_b200_upload_state", "andfn_b200_reset_state",
+           "andfn_b200_run", "andfn_b200_download", "andfn_b200_eval_heads", "andfn_b200_eval_omega",
+           "andfn_b200_destroy", "andfn_b200_stream", "andfn_b200_last_error", "andfn_b200_version",
+           "andfn_b200_set_profiling", "andfn_b200_kernel_times", "andfn_b200_fp64_peak")
+
+STATUS = {0: "ok", 1: "max_iterations", 2: "nonfinite", 3: "singular", 10: "bad_layout", 11: "bad_input",
+          12: "cuda_error", 13: "no_device", 14: "out_of_memory"}
+
+_lib = None
+
+
+class AndfnError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"andfn_b200 error {code} ({STATUS.get(code, '?')}): {msg}")
+        self.code = code
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m andfn_b200.build` "
+                          "(there is no CPU fallback)")
+    L = ctypes.CDLL(LIB_PATH)
+    P, I64, I32 = ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32
+    LP = ctypes.POINTER(AndfnLayout)
+    CP = ctypes.POINTER(AndfnConstants)
+    SP = ctypes.POINTER(AndfnSolveStats)
+    for name, res, args in (
+        ("andfn_b200_solve", ctypes.c_int, [P, I64, P, I64, LP, I64, CP, SP]),
+        ("andfn_b200_create", ctypes.c_int, [ctypes.POINTER(P), P, I64, P, I64, LP, I64, I32]),
+        ("andfn_b200_upload_state", ctypes.c_int, [P, P, P]),
+        ("andfn_b200_reset_state", ctypes.c_int, [P]),
+        ("andfn_b200_run", ctypes.c_int, [P, CP, SP]),
+        ("andfn_b200_download", ctypes.c_int, [P, P, P]),
+        ("andfn_b200_eval_heads", ctypes.c_int, [P, P, P, I64, P]),
+        ("andfn_b200_eval_omega", ctypes.c_int, [P, P, P, I64, P]),
+        ("andfn_b200_destroy", None, [P]),
+        ("andfn_b200_stream", P, [P]),
+        ("andfn_b200_last_error", ctypes.c_char_p, []),
+        ("andfn_b200_version", ctypes.c_char_p, []),
+        ("andfn_b200_set_profiling", ctypes.c_int, [P, ctypes.c_int]),
+        ("andfn_b200_kernel_times", ctypes.c_int, [P, P, P, ctypes.c_int]),
+        ("andfn_b200_fp64_peak", ctypes.c_int, [I32, P]),
+    ):
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def last_error() -> str:
+    return lib().andfn_b200_last_error().decode(errors="replace")
+
+
+def check(code: int, ok=(0,)):
+    if code not in ok:
+        raise AndfnError(code, last_error())
+    return code

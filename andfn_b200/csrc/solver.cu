@@ -1,0 +1,2188 @@
+// B200-native analytic-element DFN solve: kernels, host orchestration, C ABI.
+//
+// Replaces andfn.hpc.hpc_solve.solve (andfn/hpc/hpc_solve.py:55-257).  One
+// outer iteration of the reference is
+//   (1) head vector from the series part of every fracture potential at the
+//       discharge elements' D points (build_head_matrix, hpc_solve.py:779-829),
+//   (2) x = A^-1 b with the factorised discharge system (hpc_solve.py:651),
+//       scatter q and fracture constants (post_matrix_solve, :721-761),
+//   (3) a damped Jacobi sweep: every element re-fits its coefficients from the
+//       potential of all *other* elements of its fracture(s) at its nint
+//       collocation points (element_solver, :311-390, element_solver2
+//       :394-591),
+//   (4) max-reductions of the element errors and the convergence rule
+//       (:196-239).
+// Here (1) and (3) are one evaluation kernel (eval_kernel) in two modes,
+// (2) is a single-CTA dependency-driven triangular solve (trisolve_kernel),
+// the per-element fit is update_kernel and (4) is reduce_kernel.  Every kernel
+// reads a device status word first and returns once the loop is finished, so
+// iterations are launched in batches (CUDA graphs) without a host round trip
+// per iteration.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/andfn_b200.h"
+#include "dmath.cuh"
+#include "sparse_lu.h"
+
+namespace andfn {
+
+static constexpr double PI = 3.141592653589793115997963468544185161590576171875;
+static constexpr int EVAL_THREADS = 128;
+static constexpr int UPDATE_WARPS = 4;
+static constexpr int SOLVE_THREADS = 1024;
+static constexpr int ITER_BATCH = 4;  // iterations per graph launch
+
+enum GroupKind { KIND_PHI = 0, KIND_PSI = 1 };
+// kernel classes of one outer iteration, in launch order
+enum KClass { K_RHS = 0, K_TRISOLVE = 1, K_SWEEP = 2, K_UPDATE = 3, K_REDUCE = 4, KCLASSES = 5 };
+
+// Target points of one element side (sweep) or one discharge element side (RHS).
+struct Group {
+  int elem, frac, side, npts;
+  int out;   // offset into the value buffer
+  int kind;  // KIND_PHI: real part (+ fracture constant); KIND_PSI: imaginary part
+  int pad0, pad1;
+};
+struct Item {
+  int frac, p0, p1, pad;
+};
+// A source element as seen from one fracture, staged in shared memory.
+struct Src {
+  int id, type, m, pad;
+  cd p0, p1;  // line: Z = p0 * z + p1;  circle: p0 = center, p1.re = 1/r
+  double qk;  // sign * q / (2 pi)
+  double pad2;
+};
+
+struct SolveState {
+  int nit, cnt_error, done, status;
+  int worst, abort_flag, nonfinite, solve_q;
+  double error_q, error, error_coef, pad;
+  double max_error, damping;
+  int max_it, fused_blend2;
+};
+
+// Device view of one network.
+struct Net {
+  int ne, nf, n_de, N, MC, D;
+  // elements
+  const int *type, *frac0, *frac1;
+  int *ncoef, *nint;
+  const cd *ep0, *ep1;  // [ne][2]
+  const double *radius, *phi;
+  const cd *center;
+  double *q;
+  cd *coef, *wcoef;  // [ne][MC]
+  double *err, *err_old, *err_old2, *err_coef;
+  double *dpsi_corr;  // [ne][2*MC]
+  // fractures
+  const double *t;
+  double *constant;
+  const int *fptr, *felem;
+  // discharge system
+  const int *de_ids;
+  cd *zint0, *zint1;  // [n_de][D]
+  // branch cuts of psi elements: [ne][cut_cap]
+  int cut_cap;
+  int *cut_n, *cut_pos, *cut_elem, *cut_sign;
+  // factors
+  const int *pinv, *qcol, *l_ptr, *l_col, *u_ptr, *u_col;
+  const double *l_val, *u_val, *u_inv;
+  double *disc;  // current discharges [N]
+  double *work;  // [N] scratch (solve in global memory when N is large)
+  int *ready;    // [N]
+  SolveState *st;
+};
+
+// ------------------------------------------------------------------------
+// small device helpers
+// ------------------------------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ cd warp_sum(cd v) { return mk(warp_sum(v.re), warp_sum(v.im)); }
+
+__device__ __forceinline__ void theta_of(int type, int n, int k, double &theta) {
+  // hpc_math_functions.py:674-699 calc_thetas
+  double del = PI / n;
+  double start = del / 2;
+  if (type == 1) {
+    del = 2 * PI / n;
+    start = 0.0;
+  }
+  theta = start + k * del;
+}
+
+// Collocation point k of element e on side s (hpc_math_functions.py:279-284,
+// 491-495, 581-585: z = map_chi_to_z(exp(i theta_k))).
+__device__ __forceinline__ cd sweep_point(const Net &net, int e, int side, int k) {
+  int type = net.type[e];
+  int n = net.nint[e];
+  double th;
+  theta_of(type, n, k, th);
+  double s, c;
+  sincos(th, &s, &c);
+  cd chi = mk(c, s);
+  if (type == 1 || type == 4) {
+    double r = net.radius[e];
+    cd ctr = net.center[e];
+    return mk(chi.re * r - chi.im * 0.0 + ctr.re, chi.re * 0.0 + chi.im * r + ctr.im);
+  }
+  const cd *ep = side ? net.ep1 + 2 * e : net.ep0 + 2 * e;
+  cd a = ep[0], b = ep[1];
+  cd inv = cdiv_ref(mk(1.0, 0.0), chi);
+  cd bz = 0.5 * (chi + inv);
+  cd d = b - a;
+  cd p = mk(bz.re * d.re - bz.im * d.im, bz.re * d.im + bz.im * d.re);
+  return 0.5 * (p + a + b);
+}
+
+// ------------------------------------------------------------------------
+// Evaluation kernel: Omega_f(z) over the elements of one fracture.
+// RHS mode: series part only (q = C = 0 as after pre_matrix_solve), every
+// element included (build_head_matrix).  Sweep mode: full potential without
+// the target element itself (calc_omega(..., exclude=e)).
+// ------------------------------------------------------------------------
+template <bool RHS>
+__global__ void __launch_bounds__(EVAL_THREADS) eval_kernel(Net net, const Item *__restrict__ items,
+                                                              const int2 *__restrict__ pts,
+                                                              const Group *__restrict__ groups,
+                                                              double *__restrict__ out, int chunk) {
+  const SolveState *st = net.st;
+  if (st->done) return;
+  if (RHS && !st->solve_q) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Src *src = reinterpret_cast<Src *>(smem_raw);
+  cd *scoef = reinterpret_cast<cd *>(smem_raw + sizeof(Src) * chunk);
+  const int MC = net.MC;
+
+  const Item it = items[blockIdx.x];
+  const int p = it.p0 + threadIdx.x;
+  const bool active = p < it.p1;
+  cd z = mk(0.0, 0.0);
+  int exclude = -1, kind = KIND_PHI;
+  int gout = 0;
+  if (active) {
+    int2 gk = pts[p];
+    const Group g = groups[gk.x];
+    gout = g.out + gk.y;
+    if (RHS) {
+      z = (g.side ? net.zint1 : net.zint0)[(size_t)g.elem * net.D + gk.y];
+    } else {
+      exclude = g.elem;
+      kind = g.kind;
+      z = sweep_point(net, g.elem, g.side, gk.y);
+    }
+  }
+  const int f = it.frac;
+  const int e0 = net.fptr[f], e1 = net.fptr[f + 1];
+  double acc_re = 0.0, acc_im = 0.0;
+  for (int base = e0; base < e1; base += chunk) {
+    const int cnt = min(chunk, e1 - base);
+    __syncthreads();
+    for (int s = threadIdx.x; s < cnt; s += blockDim.x) {
+      const int el = net.felem[base + s];
+      Src h;
+      h.id = el;
+      h.type = net.type[el];
+      h.m = net.ncoef[el];
+      h.pad = 0;
+      const int side = (h.type == 0 && net.frac0[el] != f) ? 1 : 0;
+      const double sg = side ? -1.0 : 1.0;
+      h.qk = RHS ? 0.0 : sg * net.q[el] / (2 * PI);
+      h.pad2 = 0.0;
+      if (h.type == 0 || h.type == 3 || h.type == 5) {
+        const cd *ep = side ? net.ep1 + 2 * el : net.ep0 + 2 * el;
+        cd a = ep[0], b = ep[1];
+        cd inv = recip(b - a);
+        h.p0 = 2.0 * inv;
+        cd ab = a + b;
+        h.p1 = mk(-(ab.re * inv.re - ab.im * inv.im), -(ab.re * inv.im + ab.im * inv.re));
+      } else {
+        h.p0 = (h.type == 1) ? mk(0.0, 0.0) : net.center[el];
+        h.p1 = mk(1.0 / net.radius[el], 0.0);
+      }
+      src[s] = h;
+    }
+    for (int idx = threadIdx.x; idx < cnt * MC; idx += blockDim.x) {
+      const int s = idx / MC, k = idx - s * MC;
+      const int el = net.felem[base + s];
+      const int m = net.ncoef[el];
+      const int type = net.type[el];
+      const bool neg = (type == 0 && net.frac0[el] != f);
+      cd c = (k < m) ? net.coef[(size_t)el * MC + k] : mk(0.0, 0.0);
+      if (neg) c = mk(-c.re, -c.im);
+      scoef[idx] = c;
+    }
+    __syncthreads();
+    if (active) {
+      for (int s = 0; s < cnt; s++) {
+        const Src &h = src[s];
+        if (h.id == exclude) continue;
+        const cd *c = scoef + s * MC;
+        const int m = h.m;
+        if (h.type == 0 || h.type == 3 || h.type == 5) {
+          cd Z = fma_c(h.p0, z, h.p1);
+          cd chi = exterior_chi(Z);
+          if (m > 0) {
+            cd w = recip(chi);
+            cd r = c[m - 1];
+            for (int k = m - 2; k >= 0; k--) r = fma_c(r, w, c[k]);
+            acc_re += r.re;
+            acc_im += r.im;
+          }
+          if (!RHS && h.type != 5) {
+            if (kind == KIND_PSI)
+              acc_im += h.qk * atan2(chi.im, chi.re);
+            else
+              acc_re += h.qk * (0.5 * log(norm2(chi)));
+          }
+        } else if (h.type == 1) {
+          cd chi = h.p1.re * z;
+          if (m > 0) {
+            cd r = c[m - 1];
+            for (int k = m - 2; k >= 0; k--) r = fma_c(r, chi, c[k]);
+            acc_re += r.re;
+            acc_im += r.im;
+          }
+        } else if (h.type == 2) {
+          cd chi = h.p1.re * (z - h.p0);
+          const double thr = (1.0 - 1e-12) * (1.0 - 1e-12);
+          if (norm2(chi) < thr) {
+            acc_re = NAN;
+            acc_im = NAN;
+          } else if (!RHS) {
+            if (kind == KIND_PSI)
+              acc_im += h.qk * atan2(chi.im, chi.re);
+            else
+              acc_re += h.qk * (0.5 * log(norm2(chi)));
+          }
+        } else if (h.type == 4) {
+          cd chi = h.p1.re * (z - h.p0);
+          const double thr = (1.0 - 1e-10) * (1.0 - 1e-10);
+          if (norm2(chi) < thr) {
+            acc_re = NAN;
+            acc_im = NAN;
+          } else if (m > 0) {
+            cd w = recip(chi);
+            cd r = c[m - 1];
+            for (int k = m - 2; k >= 0; k--) r = fma_c(r, w, c[k]);
+            acc_re += r.re;
+            acc_im += r.im;
+          }
+        }
+      }
+    }
+  }
+  if (active) {
+    if (RHS)
+      out[gout] = acc_re;
+    else
+      out[gout] = (kind == KIND_PSI) ? acc_im : (acc_re + net.constant[f]);
+  }
+}
+
+// ------------------------------------------------------------------------
+// Per-element fit: Cauchy-integral DFT, per-type transform, errors, blends.
+// One warp per element.  vals holds phi (or psi) at the collocation points.
+// ------------------------------------------------------------------------
+__device__ __forceinline__ void dft_lane(const double *v, int n, int type, int j, bool imag_unit, cd &out) {
+  // integral_j = sum_k v_k exp(-i j theta_k), theta_k = start + k del: the
+  // phase advances by a fixed rotation; it is re-anchored every 32 points.
+  double del = PI / n, start = del / 2;
+  if (type == 1) {
+    del = 2 * PI / n;
+    start = 0.0;
+  }
+  double rs, rc;
+  sincos((double)j * del, &rs, &rc);
+  double sr = 0.0, si = 0.0;
+  double c = 1.0, s = 0.0;
+  for (int k = 0; k < n; k++) {
+    if ((k & 31) == 0) sincos((double)j * (start + k * del), &s, &c);
+    sr = fma(v[k], c, sr);
+    si = fma(-v[k], s, si);
+    const double c2 = fma(c, rc, -s * rs);
+    s = fma(s, rc, c * rs);
+    c = c2;
+  }
+  // coef_j = 2 * integral_j / n   (real Cauchy integral)
+  // coef_j = 2i * integral_j / n  (stream-function Cauchy integral)
+  if (imag_unit)
+    out = mk(-2.0 * si / n, 2.0 * sr / n);
+  else
+    out = mk(2.0 * sr / n, 2.0 * si / n);
+  if (j == 0) out = mk(out.re / 2, out.im / 2);
+}
+
+__global__ void __launch_bounds__(UPDATE_WARPS * 32) update_kernel(Net net, const int *__restrict__ elist, int nlist,
+                                                                    const int *__restrict__ group_of,
+                                                                    const Group *__restrict__ groups,
+                                                                    const double *__restrict__ vals, int nvmax,
+                                                                    int single_blend) {
+  SolveState *st = net.st;
+  if (st->done) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double *v0 = reinterpret_cast<double *>(smem_raw) + (size_t)warp * 2 * nvmax;
+  double *v1 = v0 + nvmax;
+  const int idx = blockIdx.x * UPDATE_WARPS + warp;
+  if (idx >= nlist) return;
+  const int e = elist[idx];
+  const int type = net.type[e];
+  const int MC = net.MC;
+  if (type == 2) {  // hpc_solve.py:366-368
+    if (lane == 0) net.err[e] = 0.0;
+    return;
+  }
+  const int n = net.nint[e], m = net.ncoef[e];
+  const Group g0 = groups[group_of[2 * e]];
+  for (int k = lane; k < n; k += 32) v0[k] = vals[g0.out + k];
+  if (type == 0) {
+    const Group g1 = groups[group_of[2 * e + 1]];
+    for (int k = lane; k < n; k += 32) v1[k] = vals[g1.out + k];
+  }
+  const bool psi = (type == 1 || type == 4 || type == 5);
+  if (psi) {
+    // get_dpsi_corr (hpc_math_functions.py:407-447) and the unwrapping of
+    // psi in cauchy_integral_domega(_line) (:496-505, :586-595):
+    // psi'_k = psi_k - sum_{i<k} dpsi_corr_i.
+    const int nc = net.cut_n[e];
+    const int *cp = net.cut_pos + (size_t)e * net.cut_cap;
+    const int *ce = net.cut_elem + (size_t)e * net.cut_cap;
+    const int *cs = net.cut_sign + (size_t)e * net.cut_cap;
+    double *dc = net.dpsi_corr + (size_t)e * 2 * MC;
+    __syncwarp();
+    for (int k = lane; k < n; k += 32) {
+      double cum = 0.0, here = 0.0;
+      for (int c = 0; c < nc; c++) {
+        const double qv = net.q[ce[c]] * (double)cs[c];
+        if (cp[c] < k) cum += qv;
+        if (cp[c] == k) here += qv;
+      }
+      if (k < n - 1) dc[k] = here;
+      v0[k] -= cum;
+    }
+  }
+  __syncwarp();
+  const double t0 = net.t[net.frac0[e]];
+  const double t1 = (type == 0) ? net.t[net.frac1[e]] : 0.0;
+  const cd *oldc = net.coef + (size_t)e * MC;
+  cd *neww = net.wcoef + (size_t)e * MC;
+  const int i90 = (int)(m * 0.9);
+  double s5 = 0.0, ecoef = 0.0;
+  cd c1 = mk(0.0, 0.0), c10 = mk(0.0, 0.0);
+  for (int j = lane; j < m; j += 32) {
+    cd nj;
+    if (type == 0) {
+      cd a0, a1;
+      dft_lane(v0, n, type, j, false, a0);
+      dft_lane(v1, n, type, j, false, a1);
+      // Re((t0 c1 - t1 c0) / (t0 + t1)), coef_0 = 0 (hpc_intersection.py:95-102)
+      nj = mk((t0 * a1.re - t1 * a0.re) / (t0 + t1), 0.0);
+      if (j == 0) nj = mk(0.0, 0.0);
+    } else if (type == 3) {
+      cd a;
+      dft_lane(v0, n, type, j, false, a);
+      nj = mk(-a.re, 0.0);  // hpc_const_head_line.py:72-76
+      if (j == 0) nj = mk(0.0, 0.0);
+    } else {
+      cd a;
+      dft_lane(v0, n, type, j, true, a);
+      if (type == 1) {
+        nj = mk(-a.re, -a.im);  // hpc_bounding_circle.py:154
+      } else if (type == 4) {
+        nj = mk(a.re, -a.im);  // hpc_imp_object.py:54-56
+        if (j == 0) nj = mk(0.0, 0.0);
+      } else {
+        nj = mk(-a.im * 0.0 - 0.0, -a.im);  // hpc_imp_object.py:173-175
+        if (j == 0) nj = mk(0.0, 0.0);
+      }
+    }
+    neww[j] = nj;
+    const cd oj = oldc[j];
+    if (j < 5) s5 += hypot(oj.re, oj.im);
+    c1 = c1 + nj;
+    if (j >= i90) c10 = c10 + nj;
+    ecoef += hypot(nj.re - oj.re, nj.im - oj.im);
+  }
+  s5 = warp_sum(s5);
+  ecoef = warp_sum(ecoef);
+  c1 = warp_sum(c1);
+  c10 = warp_sum(c10);
+  if (lane == 0) {
+    // calc_error / calc_coef_error (hpc_math_functions.py:612-670)
+    double er = 0.0, erc = 0.0;
+    if (!(s5 < 1e-15)) {
+      er = fabs(hypot(c1.re - c10.re, c1.im - c10.im) / hypot(c1.re + 1e-16, c1.im) - 1);
+      erc = ecoef / m;
+    }
+    net.err_old2[e] = net.err_old[e];
+    net.err_old[e] = net.err[e];
+    net.err[e] = er;
+    net.err_coef[e] = erc;
+  }
+  // damped blends (hpc_solve.py:383-388 and, for nit >= 2, 561-575)
+  const double d = st->damping;
+  const int nb = single_blend ? 1 : ((st->fused_blend2 && st->nit >= 2) ? 2 : 1);
+  cd *cc = net.coef + (size_t)e * MC;
+  for (int j = lane; j < m; j += 32) {
+    cd w = neww[j], c = cc[j];
+    for (int b = 0; b < nb; b++) c = mk(d * w.re + (1 - d) * c.re, d * w.im + (1 - d) * c.im);
+    cc[j] = c;
+  }
+}
+
+// ------------------------------------------------------------------------
+// Max-reductions of the element errors and the convergence rule.
+// ------------------------------------------------------------------------
+__global__ void __launch_bounds__(1024) reduce_kernel(Net net) {
+  SolveState *st = net.st;
+  if (st->done) return;
+  __shared__ double s_err[32], s_ec[32];
+  __shared__ int s_idx[32], s_nf[32];
+  double best = -INFINITY, bec = -INFINITY;
+  int bidx = 0x7fffffff, nonfin = 0;
+  for (int i = threadIdx.x; i < net.ne; i += blockDim.x) {
+    double e = net.err[i], ec = net.err_coef[i];
+    if (!(e == e)) {  // NaN wins (np.max / np.argmax semantics)
+      if (best == best || i < bidx) {
+        best = NAN;
+        bidx = (best == best) ? i : min(bidx, i);
+      }
+      best = NAN;
+      nonfin = 1;
+    } else if (best == best && (e > best || (e == best && i < bidx))) {
+      best = e;
+      bidx = i;
+    }
+    if (!(ec == ec)) {
+      bec = NAN;
+      nonfin = 1;
+    } else if (bec == bec && ec > bec) {
+      bec = ec;
+    }
+    if (!isfinite(net.coef[(size_t)i * net.MC].re)) nonfin = 1;
+  }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int o = 16; o > 0; o >>= 1) {
+    double ob = __shfl_xor_sync(0xffffffffu, best, o);
+    int oi = __shfl_xor_sync(0xffffffffu, bidx, o);
+    double oec = __shfl_xor_sync(0xffffffffu, bec, o);
+    int onf = __shfl_xor_sync(0xffffffffu, nonfin, o);
+    bool onan = !(ob == ob), mnan = !(best == best);
+    if (onan && (!mnan || oi < bidx)) {
+      best = ob;
+      bidx = oi;
+    } else if (!onan && !mnan && (ob > best || (ob == best && oi < bidx))) {
+      best = ob;
+      bidx = oi;
+    }
+    if (!(oec == oec) || (bec == bec && oec > bec)) bec = oec;
+    nonfin |= onf;
+  }
+  if (lane == 0) {
+    s_err[w] = best;
+    s_idx[w] = bidx;
+    s_ec[w] = bec;
+    s_nf[w] = nonfin;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double b = s_err[0], ec = s_ec[0];
+    int bi = s_idx[0], nf = s_nf[0];
+    for (int k = 1; k < (int)(blockDim.x + 31) / 32; k++) {
+      bool onan = !(s_err[k] == s_err[k]), mnan = !(b == b);
+      if (onan && (!mnan || s_idx[k] < bi)) {
+        b = s_err[k];
+        bi = s_idx[k];
+      } else if (!onan && !mnan && (s_err[k] > b || (s_err[k] == b && s_idx[k] < bi))) {
+        b = s_err[k];
+        bi = s_idx[k];
+      }
+      if (!(s_ec[k] == s_ec[k]) || (ec == ec && s_ec[k] > ec)) ec = s_ec[k];
+      nf |= s_nf[k];
+    }
+    st->error = b;
+    st->worst = bi;
+    st->error_coef = ec;
+    if (!(st->error_q == st->error_q)) nf = 1;
+    if (nf) st->nonfinite = 1;
+    // hpc_solve.py:237-239
+    if (ec < st->max_error && st->error_q < st->max_error) {
+      st->cnt_error += 1;
+      st->error_q = 1e30;
+    }
+    if (st->cnt_error >= 2 || st->nit >= st->max_it || st->nonfinite) st->done = 1;
+    st->solve_q = (st->error_q > st->max_error / 1e30) ? 1 : 0;
+  }
+}
+
+// ------------------------------------------------------------------------
+// Discharge solve: b from the RHS point values, x = Q U^-1 L^-1 P b, scatter.
+// One CTA; rows are solved by warps in dependency order, each waiting on
+// per-row ready flags (all warps are resident, and a row only waits on rows
+// of smaller (L) / larger (U) index, so the waits always end).  Every wait is
+// bounded; on timeout the CTA sets abort_flag and finishes without waiting.
+// ------------------------------------------------------------------------
+// Factor rows are stored in level order (rows of one level contiguous, each
+// row's entries contiguous): a level's rows depend only on earlier levels.
+struct LevelSolve {
+  const int *lev_ptr;   // [nlev + 1] slot ranges of the levels
+  const int *rows;      // [N] row solved in each slot
+  const int *eptr;      // [N + 1] entry range of each slot
+  const int *col;       // entries: column (pivot-step index)
+  const double *val;    // entries: value
+  const double *scale;  // [N] per-slot multiplier (1/U(i,i)) or null
+  int nlev;
+};
+
+static constexpr int PF = 4;  // factor entries per lane kept in registers
+
+struct RowRegs {
+  int row, beg, end;
+  int c[PF];
+  double v[PF];
+};
+
+__device__ __forceinline__ void load_row(RowRegs &r, const LevelSolve &F, int slot, int lane) {
+  r.row = F.rows[slot];
+  r.beg = F.eptr[slot];
+  r.end = F.eptr[slot + 1];
+#pragma unroll
+  for (int k = 0; k < PF; k++) {
+    const int p = r.beg + lane + 32 * k;
+    r.c[k] = (p < r.end) ? F.col[p] : 0;
+    r.v[k] = (p < r.end) ? F.val[p] : 0.0;
+  }
+}
+
+__device__ __forceinline__ void solve_row(const RowRegs &r, const LevelSolve &F, int slot, int lane, double *y) {
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < PF; k++) s = fma(r.v[k], y[r.c[k]], s);
+  for (int p = r.beg + 32 * PF + lane; p < r.end; p += 32) s = fma(F.val[p], y[F.col[p]], s);
+  s = warp_sum(s);
+  if (lane == 0) {
+    double v = y[r.row] - s;
+    if (F.scale) v *= F.scale[slot];
+    y[r.row] = v;
+  }
+}
+
+// One triangular solve, level by level with a block barrier between levels.
+// The first row of the next level is loaded into registers before the
+// barrier, so its global-memory latency overlaps the wait.
+__device__ void level_solve(const LevelSolve &F, double *y, int *s_levptr, int cap_levptr) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const bool lev_in_smem = F.nlev + 1 <= cap_levptr;
+  if (lev_in_smem)
+    for (int i = threadIdx.x; i <= F.nlev; i += blockDim.x) s_levptr[i] = F.lev_ptr[i];
+  __syncthreads();
+  const int *lp = lev_in_smem ? s_levptr : F.lev_ptr;
+  RowRegs cur;
+  bool have = false;
+  if (F.nlev > 0 && lp[0] + warp < lp[1]) {
+    load_row(cur, F, lp[0] + warp, lane);
+    have = true;
+  }
+  for (int l = 0; l < F.nlev; l++) {
+    const int r0 = lp[l], r1 = lp[l + 1];
+    if (have) solve_row(cur, F, r0 + warp, lane, y);
+    for (int slot = r0 + warp + nw; slot < r1; slot += nw) {
+      RowRegs t;
+      load_row(t, F, slot, lane);
+      solve_row(t, F, slot, lane, y);
+    }
+    have = false;
+    if (l + 1 < F.nlev) {
+      const int n0 = r1, n1 = lp[l + 2];
+      if (n0 + warp < n1) {
+        load_row(cur, F, n0 + warp, lane);
+        have = true;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(SOLVE_THREADS) trisolve_kernel(Net net, const double *__restrict__ rhs_vals,
+                                                                  const int *__restrict__ rhs_group,
+                                                                  const Group *__restrict__ groups, int use_smem,
+                                                                  LevelSolve Lf, LevelSolve Ub, int cap_levptr) {
+  SolveState *st = net.st;
+  if (st->done) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int N = net.N, n_de = net.n_de, D = net.D;
+  double *y = use_smem ? reinterpret_cast<double *>(smem_raw) : net.work;
+  int *s_levptr = reinterpret_cast<int *>(smem_raw + (use_smem ? sizeof(double) * (size_t)N : 0));
+  if (threadIdx.x == 0) st->nit += 1;
+  if (!st->solve_q) return;  // uniform: solve_q is written only by reduce_kernel
+  // b = head vector (hpc_solve.py:811-829); y = P b
+  for (int r = threadIdx.x; r < N; r += blockDim.x) {
+    double b = 0.0;
+    if (r < n_de) {
+      const int e = net.de_ids[r];
+      const int type = net.type[e];
+      const Group g0 = groups[rhs_group[2 * r]];
+      double s0 = 0.0;
+      for (int k = 0; k < D; k++) s0 += rhs_vals[g0.out + k];
+      if (type == 0) {
+        const Group g1 = groups[rhs_group[2 * r + 1]];
+        double s1 = 0.0;
+        for (int k = 0; k < D; k++) s1 += rhs_vals[g1.out + k];
+        b = (s1 / D) / net.t[net.frac1[e]] - (s0 / D) / net.t[net.frac0[e]];
+      } else {
+        b = net.phi[e] - s0 / D;
+      }
+    }
+    y[net.pinv[r]] = b;
+  }
+  __syncthreads();
+  level_solve(Lf, y, s_levptr, cap_levptr);  // L unit lower
+  level_solve(Ub, y, s_levptr, cap_levptr);  // U upper, scale = 1/U(i,i)
+  // x = Q y; error_q = max|x - x_old| / (max|x_old| + 1e-16) (hpc_solve.py:169-174)
+  __shared__ double s_d[32], s_o[32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  double md = 0.0, mo = 0.0;
+  for (int k = threadIdx.x; k < N; k += blockDim.x) {
+    const int c = net.qcol[k];
+    const double xv = y[k];
+    const double xo = net.disc[c];
+    double dd = fabs(xv - xo);
+    if (!(dd == dd)) dd = INFINITY;
+    md = fmax(md, dd);
+    mo = fmax(mo, fabs(xo));
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < N; k += blockDim.x) {
+    const int c = net.qcol[k];
+    const double xv = y[k];
+    net.disc[c] = xv;
+    if (c < n_de)
+      net.q[net.de_ids[c]] = xv;
+    else
+      net.constant[c - n_de] = xv;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    md = fmax(md, __shfl_xor_sync(0xffffffffu, md, o));
+    mo = fmax(mo, __shfl_xor_sync(0xffffffffu, mo, o));
+  }
+  if (lane == 0) {
+    s_d[warp] = md;
+    s_o[warp] = mo;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0, bb = 0.0;
+    for (int k = 0; k < nw; k++) {
+      a = fmax(a, s_d[k]);
+      bb = fmax(bb, s_o[k]);
+    }
+    st->error_q = a / (bb + 1e-16);
+  }
+}
+
+// ------------------------------------------------------------------------
+// Setup kernels
+// ------------------------------------------------------------------------
+// numba np.linspace(a, b, D + 2)[1:D+1] (np.divide of a complex by an int is
+// NumPy's Smith division with a reciprocal, numba npyfuncs.np_complex_div_impl)
+__device__ __forceinline__ cd linspace_interior(cd a, cd b, int D, int i /*1..D*/) {
+  const int num = D + 2;
+  cd delta = b - a;
+  const double br = (double)(num - 1);
+  const double scl = 1.0 / (br + 0.0 * 0.0);
+  cd step = mk((delta.re + delta.im * 0.0) * scl, (delta.im - delta.re * 0.0) * scl);
+  if (i == num - 1) return b;
+  return mk(a.re + (i * step.re - 0.0 * step.im), a.im + (i * step.im + 0.0 * step.re));
+}
+
+__global__ void zint_kernel(Net net) {
+  const int D = net.D;
+  const long long tot = (long long)net.n_de * D;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < tot;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const int j = (int)(idx / D), i = (int)(idx - (long long)j * D);
+    const int e = net.de_ids[j];
+    const int type = net.type[e];
+    if (type == 0 || type == 3) {
+      net.zint0[idx] = linspace_interior(net.ep0[2 * e], net.ep0[2 * e + 1], D, i + 1);
+      if (type == 0) net.zint1[idx] = linspace_interior(net.ep1[2 * e], net.ep1[2 * e + 1], D, i + 1);
+    } else if (type == 2) {
+      // hpc_well.py:128-130
+      const double stop = 2.0 * PI - 2 * PI / D;
+      double th = (D > 1) ? (0.0 + i * ((stop - 0.0) / (double)(D - 1))) : 0.0;
+      if (D > 1 && i == D - 1) th = stop;
+      double s, c;
+      sincos(th, &s, &c);
+      const double r = net.radius[e];
+      const cd ctr = net.center[e];
+      net.zint0[idx] = mk(r * c - 0.0 * s + ctr.re, r * s + 0.0 * c + ctr.im);
+    }
+  }
+}
+
+// Branch-cut crossings of the discharge elements' log cuts through the
+// collocation polygon of every psi element (find_branch_cuts / get_sign,
+// hpc_math_functions.py:301-403), in the reference's (segment, element)
+// order.  One warp per element; lanes take consecutive segments.
+__device__ __forceinline__ cd psi_polygon_point(const Net &net, int e, int type, int n, int k) {
+  double th;
+  theta_of(type, n, k, th);
+  double s, c;
+  sincos(th, &s, &c);
+  cd chi = mk(c, s);
+  if (type == 1 || type == 4) {
+    const double r = net.radius[e];
+    const cd ctr = net.center[e];
+    return mk(chi.re * r - chi.im * 0.0 + ctr.re, chi.re * 0.0 + chi.im * r + ctr.im);
+  }
+  cd a = net.ep0[2 * e], b = net.ep0[2 * e + 1];
+  cd inv = cdiv_ref(mk(1.0, 0.0), chi);
+  cd bz = 0.5 * (chi + inv);
+  cd d = b - a;
+  cd pp = mk(bz.re * d.re - bz.im * d.im, bz.re * d.im + bz.im * d.re);
+  return 0.5 * (pp + a + b);
+}
+
+__global__ void cuts_kernel(Net net, const int *__restrict__ elist, int nlist) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (warp >= nlist) return;
+  const int e = elist[warp];
+  const int type = net.type[e];
+  const int n = net.nint[e];
+  const int f = net.frac0[e];
+  const int k0 = net.fptr[f], k1 = net.fptr[f + 1];
+  int total = 0;
+  for (int base = 0; base < n - 1; base += 32) {
+    const int ii = base + lane;
+    cd zp0 = mk(0, 0), zp1 = mk(0, 0);
+    if (ii < n - 1) {
+      zp0 = psi_polygon_point(net, e, type, n, ii);
+      zp1 = psi_polygon_point(net, e, type, n, ii + 1);
+    }
+    int mine = 0, off = 0;
+    // pass 0 counts this lane's crossings, pass 1 writes them after an
+    // exclusive scan, so entries come out in (segment, element) order
+    for (int pass = 0; pass < 2; pass++) {
+      int wrote = 0;
+      if (ii < n - 1) {
+        for (int k = k0; k < k1; k++) {
+          const int el = net.felem[k];
+          const int t = net.type[el];
+          bool hit = false;
+          cd chi0 = mk(0, 0), chi1 = mk(0, 0);
+          int sdef = -1;
+          if (t == 0) {
+            const bool s0 = (net.frac0[el] == f);
+            const cd *ep = s0 ? net.ep0 + 2 * el : net.ep1 + 2 * el;
+            sdef = s0 ? -1 : 1;
+            chi0 = map_z_line_to_chi_ref(zp0, ep[0], ep[1]);
+            chi1 = map_z_line_to_chi_ref(zp1, ep[0], ep[1]);
+            const double ln0 = atan2(chi0.im, chi0.re), ln1 = atan2(chi1.im, chi1.re);
+            const int sg0 = (ln0 > 0) - (ln0 < 0), sg1 = (ln1 > 0) - (ln1 < 0);
+            hit = (sg0 != sg1) && (fabs(ln0) + fabs(ln1) > PI);
+          } else if (t == 2 || t == 3) {
+            if (t == 2) {
+              const double r = net.radius[el];
+              const cd c = net.center[el];
+              chi0 = cdiv_ref(zp0 - c, mk(r, 0.0));
+              chi1 = cdiv_ref(zp1 - c, mk(r, 0.0));
+            } else {
+              chi0 = map_z_line_to_chi_ref(zp0, net.ep0[2 * el], net.ep0[2 * el + 1]);
+              chi1 = map_z_line_to_chi_ref(zp1, net.ep0[2 * el], net.ep0[2 * el + 1]);
+            }
+            const int sg0 = (chi0.im > 0) - (chi0.im < 0), sg1 = (chi1.im > 0) - (chi1.im < 0);
+            hit = (sg0 != sg1) && (chi0.re < 0);
+          }
+          if (!hit) continue;
+          if (pass == 0) {
+            mine++;
+          } else {
+            const int slot = total + off + wrote;
+            wrote++;
+            if (slot < net.cut_cap) {
+              const size_t o = (size_t)e * net.cut_cap + slot;
+              net.cut_pos[o] = ii;
+              net.cut_elem[o] = el;
+              int sg = sdef;
+              if (type != 1) sg = (chi0.im < chi1.im) ? -1 * sdef : sdef;  // get_sign
+              net.cut_sign[o] = sg;
+            } else {
+              atomicExch(&net.st->status, (int)ANDFN_BAD_INPUT);
+            }
+          }
+        }
+      }
+      if (pass == 0) {
+        int v = mine;
+        for (int o = 1; o < 32; o <<= 1) {
+          int u = __shfl_up_sync(0xffffffffu, v, o);
+          if (lane >= o) v += u;
+        }
+        off = v - mine;
+      }
+    }
+    total += __shfl_sync(0xffffffffu, off + mine, 31);
+  }
+  if (lane == 0) net.cut_n[e] = min(total, net.cut_cap);
+}
+
+// Omega_f(z) at arbitrary points (hpc_fracture.py:52-94, exclude = -1), one
+// thread per point; used for heads (hpc_fracture.py:205-252).
+__global__ void points_kernel(Net net, const int *__restrict__ frac, const cd *__restrict__ z, int npts,
+                              cd *__restrict__ out_omega, double *__restrict__ out_head) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= npts) return;
+  const int f = frac[i];
+  const cd zz = z[i];
+  double ar = net.constant[f], ai = 0.0;
+  for (int k = net.fptr[f]; k < net.fptr[f + 1]; k++) {
+    const int el = net.felem[k];
+    const int ty = net.type[el];
+    const int m = net.ncoef[el];
+    const cd *c = net.coef + (size_t)el * net.MC;
+    const bool neg = (ty == 0 && net.frac0[el] != f);
+    const double sg = neg ? -1.0 : 1.0;
+    const double qk = sg * net.q[el] / (2 * PI);
+    if (ty == 0 || ty == 3 || ty == 5) {
+      const cd *ep = neg ? net.ep1 + 2 * el : net.ep0 + 2 * el;
+      cd inv = recip(ep[1] - ep[0]);
+      cd ab = ep[0] + ep[1];
+      cd Z = fma_c(2.0 * inv, zz, mk(-(ab.re * inv.re - ab.im * inv.im), -(ab.re * inv.im + ab.im * inv.re)));
+      cd chi = exterior_chi(Z);
+      if (m > 0) {
+        cd w = recip(chi);
+        cd r = sg * c[m - 1];
+        for (int j = m - 2; j >= 0; j--) r = fma_c(r, w, sg * c[j]);
+        ar += r.re;
+        ai += r.im;
+      }
+      if (ty != 5) {
+        ar += qk * 0.5 * log(norm2(chi));
+        ai += qk * atan2(chi.im, chi.re);
+      }
+    } else if (ty == 1) {
+      cd chi = (1.0 / net.radius[el]) * zz;
+      if (m > 0) {
+        cd r = c[m - 1];
+        for (int j = m - 2; j >= 0; j--) r = fma_c(r, chi, c[j]);
+        ar += r.re;
+        ai += r.im;
+      }
+    } else if (ty == 2) {
+      cd chi = (1.0 / net.radius[el]) * (zz - net.center[el]);
+      if (norm2(chi) < (1.0 - 1e-12) * (1.0 - 1e-12)) {
+        ar = NAN;
+        ai = NAN;
+      } else {
+        ar += qk * 0.5 * log(norm2(chi));
+        ai += qk * atan2(chi.im, chi.re);
+      }
+    } else if (ty == 4) {
+      cd chi = (1.0 / net.radius[el]) * (zz - net.center[el]);
+      if (norm2(chi) < (1.0 - 1e-10) * (1.0 - 1e-10)) {
+        ar = NAN;
+        ai = NAN;
+      } else if (m > 0) {
+        cd w = recip(chi);
+        cd r = c[m - 1];
+        for (int j = m - 2; j >= 0; j--) r = fma_c(r, w, c[j]);
+        ar += r.re;
+        ai += r.im;
+      }
+    }
+  }
+  if (out_omega) out_omega[i] = mk(ar, ai);
+  if (out_head) out_head[i] = ar / net.t[f];
+}
+
+// Average discharge term of source element ee over the D points of row j
+// (get_discharge_term, hpc_solve.py:1451-1459 and the per-type
+// discharge_term functions).  One warp per matrix entry.
+__global__ void matrix_values_kernel(Net net, const int *__restrict__ ent_row, const int *__restrict__ ent_src,
+                                     const int *__restrict__ ent_side, const int *__restrict__ ent_kind,
+                                     double *__restrict__ vals, long long nent) {
+  const long long w = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (w >= nent) return;
+  const int kind = ent_kind[w];
+  const int j = ent_row[w];
+  if (kind == 1) {  // fracture-constant column: 1/t0, -1/t1 (intersections) or 1
+    if (lane == 0) {
+      const int e = net.de_ids[j];
+      const int side = ent_side[w];
+      if (net.type[e] == 0)
+        vals[w] = side ? -1.0 / net.t[net.frac1[e]] : 1.0 / net.t[net.frac0[e]];
+      else
+        vals[w] = 1.0;
+    }
+    return;
+  }
+  if (kind == 2) {  // continuity row: +1 / -1
+    if (lane == 0) {
+      const int el = ent_src[w];
+      const int f = j - net.n_de;
+      vals[w] = (net.type[el] != 0 || net.frac0[el] == f) ? 1.0 : -1.0;
+    }
+    return;
+  }
+  const int e = net.de_ids[j];
+  const int side = ent_side[w];
+  const int ee = ent_src[w];
+  const int f = side ? net.frac1[e] : net.frac0[e];
+  const cd *z = (side ? net.zint1 : net.zint0) + (size_t)j * net.D;
+  const int t = net.type[ee];
+  double s = 0.0;
+  for (int i = lane; i < net.D; i += 32) {
+    cd chi;
+    double sg = 1.0;
+    if (t == 2) {
+      chi = (1.0 / net.radius[ee]) * (z[i] - net.center[ee]);
+    } else {
+      const bool s0 = (t != 0) || (net.frac0[ee] == f);
+      if (t == 0 && !s0) sg = -1.0;
+      const cd *ep = s0 ? net.ep0 + 2 * ee : net.ep1 + 2 * ee;
+      cd inv = recip(ep[1] - ep[0]);
+      cd Z = fma_c(2.0 * inv, z[i], mk(-((ep[0] + ep[1]).re * inv.re - (ep[0] + ep[1]).im * inv.im),
+                                        -((ep[0] + ep[1]).re * inv.im + (ep[0] + ep[1]).im * inv.re)));
+      chi = exterior_chi(Z);
+    }
+    s += sg / (2 * PI) * (0.5 * log(norm2(chi)));
+  }
+  s = warp_sum(s);
+  if (lane == 0) {
+    double v = s / net.D;
+    if (net.type[e] == 0) v = (side ? -v : v) / net.t[f];
+    vals[w] = v;
+  }
+}
+
+// hpc_solve.py:124-128: error and error_old start at 1e30.
+__global__ void init_state_kernel(Net net) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < net.ne; i += gridDim.x * blockDim.x) {
+    net.err_old[i] = 1e30;
+    net.err[i] = 1e30;
+  }
+}
+
+// FP64 FMA throughput probe: 8 independent dependent chains per thread.
+__global__ void fp64_peak_kernel(double *out, int iters, double a, double b) {
+  double x[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) x[k] = threadIdx.x * 1e-9 + k;
+  for (int i = 0; i < iters; i++) {
+#pragma unroll
+    for (int k = 0; k < 8; k++) x[k] = fma(x[k], a, b);
+  }
+  double s = 0;
+#pragma unroll
+  for (int k = 0; k < 8; k++) s += x[k];
+  if (s == 12345.678) out[0] = s;
+}
+
+// ------------------------------------------------------------------------
+// Host side
+// ------------------------------------------------------------------------
+static thread_local std::string g_last_error;
+static void set_error(const std::string &s) { g_last_error = s; }
+
+#define CK(call)                                                                                    \
+  do {                                                                                              \
+    cudaError_t _e = (call);                                                                        \
+    if (_e != cudaSuccess) {                                                                        \
+      set_error(std::string(#call) + ": " + cudaGetErrorString(_e));                                \
+      return ANDFN_CUDA_ERROR;                                                                      \
+    }                                                                                               \
+  } while (0)
+
+template <class T>
+struct DBuf {
+  T *p = nullptr;
+  size_t n = 0;
+  cudaError_t alloc(size_t count) {
+    free();
+    n = count;
+    if (count == 0) return cudaSuccess;
+    return cudaMalloc(&p, sizeof(T) * count);
+  }
+  void free() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  ~DBuf() { free(); }
+};
+
+struct HostNet {
+  // element SoA (host copies of the geometry and of the initial state)
+  std::vector<int> type, frac0, frac1, ncoef, nint;
+  std::vector<cd> ep0, ep1, center;
+  std::vector<double> radius, phi, q, err, err_old, err_old2, err_coef;
+  std::vector<cd> coef;  // [ne][MC]
+  std::vector<double> t, constant;
+  std::vector<int> fptr, felem;
+  std::vector<int> de_ids, elem_de;
+};
+
+}  // namespace andfn
+
+using namespace andfn;
+
+struct AndfnHandle {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  AndfnLayout L;
+  int64_t ne = 0, nf = 0, D = 0;
+  int MC = 0;  // coefficient capacity (per element, device)
+  int max_nint = 0;
+  HostNet h;
+  // device arrays
+  DBuf<int> type, frac0, frac1, ncoef, nint, ncoef0, nint0;
+  DBuf<cd> ep0, ep1, center, coef, coef0, wcoef;
+  DBuf<double> radius, phi, q, q0, err, err_old, err_old2, err_coef, err_in, err_old_in, err_old2_in, err_coef_in;
+  DBuf<double> dpsi_corr, t, constant, constant0;
+  DBuf<int> fptr, felem, de_ids;
+  DBuf<cd> zint0, zint1;
+  DBuf<int> cut_n, cut_pos, cut_elem, cut_sign;
+  int cut_cap = 0;
+  // discharge system
+  int N = 0;
+  std::vector<int> mrow_ptr, mcol;  // CSR pattern (row = equation, col = unknown)
+  std::vector<int> ent_row, ent_src, ent_side, ent_kind;
+  DBuf<int> d_ent_row, d_ent_src, d_ent_side, d_ent_kind;
+  DBuf<double> d_mvals;
+  std::vector<int> colorder;  // cached symbolic analysis (depends on the pattern only)
+  DBuf<int> pinv, qcol, l_ptr, l_col, u_ptr, u_col;
+  DBuf<double> l_val, u_val, u_inv, disc, work;
+  DBuf<int> ready;
+  // level-ordered factors for trisolve_kernel
+  DBuf<int> lf_lev, lf_rows, lf_eptr, lf_col, ub_lev, ub_rows, ub_eptr, ub_col;
+  DBuf<double> lf_val, ub_val, ub_scale;
+  int lf_nlev = 0, ub_nlev = 0;
+  int64_t nnz_factors = 0;
+  // evaluation tables
+  std::vector<Group> groups;
+  DBuf<Group> d_groups;
+  DBuf<Item> sweep_items, rhs_items;
+  DBuf<int2> sweep_pts, rhs_pts;
+  int n_sweep_items = 0, n_rhs_items = 0;
+  DBuf<int> group_of;   // [ne][2] -> sweep group
+  DBuf<int> rhs_group;  // [n_de][2] -> rhs group
+  DBuf<double> sweep_vals, rhs_vals;
+  DBuf<int> upd_list, psi_list;
+  int n_upd = 0, n_psi = 0;
+  int nvmax = 0;
+  int chunk = 0;
+  size_t eval_smem = 0;
+  DBuf<SolveState> st;
+  SolveState *h_st = nullptr;  // pinned host mirror
+  cudaGraphExec_t graph_exec = nullptr;
+  int graph_fused = -1;
+  int solve_threads = SOLVE_THREADS;
+  // per-kernel timing: event pairs recorded as graph nodes around every
+  // kernel of every captured iteration
+  int profiling = 0;
+  cudaEvent_t ev[ITER_BATCH][KCLASSES][2] = {};
+  double k_ms[KCLASSES] = {};
+  int64_t k_n[KCLASSES] = {};
+  int64_t launches = 0;
+
+  Net net() const {
+    Net n;
+    n.ne = (int)ne;
+    n.nf = (int)nf;
+    n.n_de = (int)h.de_ids.size();
+    n.N = N;
+    n.MC = MC;
+    n.D = (int)D;
+    n.type = type.p;
+    n.frac0 = frac0.p;
+    n.frac1 = frac1.p;
+    n.ncoef = ncoef.p;
+    n.nint = nint.p;
+    n.ep0 = ep0.p;
+    n.ep1 = ep1.p;
+    n.radius = radius.p;
+    n.phi = phi.p;
+    n.center = center.p;
+    n.q = q.p;
+    n.coef = coef.p;
+    n.wcoef = wcoef.p;
+    n.err = err.p;
+    n.err_old = err_old.p;
+    n.err_old2 = err_old2.p;
+    n.err_coef = err_coef.p;
+    n.dpsi_corr = dpsi_corr.p;
+    n.t = t.p;
+    n.constant = constant.p;
+    n.fptr = fptr.p;
+    n.felem = felem.p;
+    n.de_ids = de_ids.p;
+    n.zint0 = zint0.p;
+    n.zint1 = zint1.p;
+    n.cut_cap = cut_cap;
+    n.cut_n = cut_n.p;
+    n.cut_pos = cut_pos.p;
+    n.cut_elem = cut_elem.p;
+    n.cut_sign = cut_sign.p;
+    n.pinv = pinv.p;
+    n.qcol = qcol.p;
+    n.l_ptr = l_ptr.p;
+    n.l_col = l_col.p;
+    n.u_ptr = u_ptr.p;
+    n.u_col = u_col.p;
+    n.l_val = l_val.p;
+    n.u_val = u_val.p;
+    n.u_inv = u_inv.p;
+    n.disc = disc.p;
+    n.work = work.p;
+    n.ready = ready.p;
+    n.st = st.p;
+    return n;
+  }
+  ~AndfnHandle() {
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    for (auto &b : ev)
+      for (auto &c : b)
+        for (auto &e : c)
+          if (e) cudaEventDestroy(e);
+    if (h_st) cudaFreeHost(h_st);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace andfn {
+
+static inline int64_t rd_i64(const char *rec, int64_t off) {
+  int64_t v;
+  std::memcpy(&v, rec + off, 8);
+  return v;
+}
+static inline double rd_f64(const char *rec, int64_t off) {
+  double v;
+  std::memcpy(&v, rec + off, 8);
+  return v;
+}
+static inline cd rd_cd(const char *rec, int64_t off, int k) {
+  cd v;
+  std::memcpy(&v, rec + off + 16 * k, 16);
+  return v;
+}
+
+static int check_layout(const AndfnLayout *L) {
+  if (!L || L->elem_size <= 0 || L->frac_size <= 0 || L->max_ncoef <= 0 || L->max_elements <= 0) return 1;
+  const int64_t eo[] = {L->e_id, L->e_type, L->e_frac0, L->e_frac1, L->e_radius, L->e_head, L->e_phi, L->e_ncoef,
+                        L->e_nint, L->e_q, L->e_error, L->e_error_old, L->e_error_old2, L->e_error_coef};
+  for (int64_t o : eo)
+    if (o < 0 || o + 8 > L->elem_size) return 1;
+  if (L->e_endpoints0 < 0 || L->e_endpoints0 + 32 > L->elem_size) return 1;
+  if (L->e_endpoints1 < 0 || L->e_endpoints1 + 32 > L->elem_size) return 1;
+  if (L->e_center < 0 || L->e_center + 16 > L->elem_size) return 1;
+  if (L->e_coef < 0 || L->e_coef + 16 * L->max_ncoef > L->elem_size) return 1;
+  if (L->e_thetas < 0 || L->e_thetas + 16 * L->max_ncoef > L->elem_size) return 1;
+  if (L->e_dpsi_corr < 0 || L->e_dpsi_corr + 16 * L->max_ncoef > L->elem_size) return 1;
+  const int64_t fo[] = {L->f_id, L->f_t, L->f_radius, L->f_nelements, L->f_constant};
+  for (int64_t o : fo)
+    if (o < 0 || o + 8 > L->frac_size) return 1;
+  if (L->f_elements < 0 || L->f_elements + 8 * L->max_elements > L->frac_size) return 1;
+  return 0;
+}
+
+// Parses records into host SoA and validates ids.
+static int parse_records(AndfnHandle *H, const char *F, const char *E) {
+  const AndfnLayout &L = H->L;
+  HostNet &h = H->h;
+  const int64_t ne = H->ne, nf = H->nf;
+  h.type.resize(ne);
+  h.frac0.resize(ne);
+  h.frac1.resize(ne);
+  h.ncoef.resize(ne);
+  h.nint.resize(ne);
+  h.ep0.resize(2 * ne);
+  h.ep1.resize(2 * ne);
+  h.center.resize(ne);
+  h.radius.resize(ne);
+  h.phi.resize(ne);
+  h.q.resize(ne);
+  h.err.resize(ne);
+  h.err_old.resize(ne);
+  h.err_old2.resize(ne);
+  h.err_coef.resize(ne);
+  int maxm = 0;
+  for (int64_t i = 0; i < ne; i++) {
+    const char *r = E + i * L.elem_size;
+    if (rd_i64(r, L.e_id) != i) {
+      set_error("element _id must equal its index (andfn/dfn.py:1062-1063)");
+      return ANDFN_BAD_INPUT;
+    }
+    int64_t ty = rd_i64(r, L.e_type);
+    if (ty < 0 || ty > 5) {
+      set_error("element type out of range");
+      return ANDFN_BAD_INPUT;
+    }
+    h.type[i] = (int)ty;
+    int64_t f0 = rd_i64(r, L.e_frac0), f1 = rd_i64(r, L.e_frac1);
+    if (f0 < 0 || f0 >= nf || (ty == 0 && (f1 < 0 || f1 >= nf))) {
+      set_error("element fracture id out of range");
+      return ANDFN_BAD_INPUT;
+    }
+    h.frac0[i] = (int)f0;
+    h.frac1[i] = (ty == 0) ? (int)f1 : -1;
+    int64_t m = rd_i64(r, L.e_ncoef), n = rd_i64(r, L.e_nint);
+    if (m < 0 || m > L.max_ncoef || n < 0 || n > 2 * L.max_ncoef || (ty != 2 && (m < 1 || n < 2))) {
+      set_error("ncoef/nint out of range for the record capacity");
+      return ANDFN_BAD_INPUT;
+    }
+    h.ncoef[i] = (int)m;
+    h.nint[i] = (int)n;
+    maxm = std::max(maxm, (int)m);
+    h.ep0[2 * i] = rd_cd(r, L.e_endpoints0, 0);
+    h.ep0[2 * i + 1] = rd_cd(r, L.e_endpoints0, 1);
+    h.ep1[2 * i] = rd_cd(r, L.e_endpoints1, 0);
+    h.ep1[2 * i + 1] = rd_cd(r, L.e_endpoints1, 1);
+    h.center[i] = rd_cd(r, L.e_center, 0);
+    h.radius[i] = rd_f64(r, L.e_radius);
+    h.phi[i] = rd_f64(r, L.e_phi);
+    h.q[i] = rd_f64(r, L.e_q);
+    h.err[i] = rd_f64(r, L.e_error);
+    h.err_old[i] = rd_f64(r, L.e_error_old);
+    h.err_old2[i] = rd_f64(r, L.e_error_old2);
+    h.err_coef[i] = rd_f64(r, L.e_error_coef);
+  }
+  H->MC = std::max(1, maxm);
+  h.t.resize(nf);
+  h.constant.resize(nf);
+  h.fptr.assign(nf + 1, 0);
+  h.felem.clear();
+  for (int64_t f = 0; f < nf; f++) {
+    const char *r = F + f * L.frac_size;
+    if (rd_i64(r, L.f_id) != f) {
+      set_error("fracture _id must equal its index (andfn/dfn.py:1119-1120)");
+      return ANDFN_BAD_INPUT;
+    }
+    h.t[f] = rd_f64(r, L.f_t);
+    h.constant[f] = rd_f64(r, L.f_constant);
+    int64_t nel = rd_i64(r, L.f_nelements);
+    if (nel < 0 || nel > L.max_elements) {
+      set_error("fracture nelements out of range");
+      return ANDFN_BAD_INPUT;
+    }
+    for (int64_t k = 0; k < nel; k++) {
+      int64_t el = rd_i64(r, L.f_elements + 8 * k);
+      if (el < 0 || el >= ne) {
+        set_error("fracture element id out of range");
+        return ANDFN_BAD_INPUT;
+      }
+      h.felem.push_back((int)el);
+    }
+    h.fptr[f + 1] = (int)h.felem.size();
+  }
+  h.de_ids.clear();
+  h.elem_de.assign(ne, -1);
+  for (int64_t i = 0; i < ne; i++)
+    if (h.type[i] == 0 || h.type[i] == 2 || h.type[i] == 3) {
+      h.elem_de[i] = (int)h.de_ids.size();
+      h.de_ids.push_back((int)i);
+    }
+  return 0;
+}
+
+static void read_coefs(AndfnHandle *H, const char *E) {
+  const AndfnLayout &L = H->L;
+  H->h.coef.assign((size_t)H->ne * H->MC, mk(0.0, 0.0));
+  for (int64_t i = 0; i < H->ne; i++) {
+    const char *r = E + i * L.elem_size;
+    const int m = H->h.ncoef[i];
+    for (int k = 0; k < m && k < H->MC; k++) H->h.coef[(size_t)i * H->MC + k] = rd_cd(r, L.e_coef, k);
+  }
+}
+
+static thread_local int64_t g_h2d_bytes = 0, g_d2h_bytes = 0;
+
+template <class T>
+static cudaError_t upload(DBuf<T> &d, const std::vector<T> &v, cudaStream_t s) {
+  cudaError_t e = d.alloc(v.size());
+  if (e != cudaSuccess || v.empty()) return e;
+  g_h2d_bytes += (int64_t)(sizeof(T) * v.size());
+  return cudaMemcpyAsync(d.p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, s);
+}
+
+// Evaluation tables: groups, flattened points and tiles per fracture.
+static void build_tables(AndfnHandle *H, bool rhs, std::vector<Group> &groups, std::vector<int> &index_of,
+                         std::vector<Item> &items, std::vector<int2> &pts, int &nvals) {
+  const HostNet &h = H->h;
+  const int ne = (int)H->ne, nf = (int)H->nf;
+  const int D = (int)H->D;
+  const int n_de = (int)h.de_ids.size();
+  // per fracture, the groups whose points lie in it
+  std::vector<std::vector<int>> per_frac(nf);
+  nvals = 0;
+  if (!rhs) {
+    index_of.assign(2 * (size_t)ne, -1);
+    for (int e = 0; e < ne; e++) {
+      const int ty = h.type[e];
+      if (ty == 2) continue;
+      const int sides = (ty == 0) ? 2 : 1;
+      for (int s = 0; s < sides; s++) {
+        Group g;
+        g.elem = e;
+        g.side = s;
+        g.frac = s ? h.frac1[e] : h.frac0[e];
+        g.npts = h.nint[e];
+        g.kind = (ty == 1 || ty == 4 || ty == 5) ? KIND_PSI : KIND_PHI;
+        g.out = nvals;
+        g.pad0 = g.pad1 = 0;
+        nvals += g.npts;
+        index_of[2 * (size_t)e + s] = (int)groups.size();
+        per_frac[g.frac].push_back((int)groups.size());
+        groups.push_back(g);
+      }
+    }
+  } else {
+    index_of.assign(2 * (size_t)n_de, -1);
+    for (int j = 0; j < n_de; j++) {
+      const int e = h.de_ids[j];
+      const int sides = (h.type[e] == 0) ? 2 : 1;
+      for (int s = 0; s < sides; s++) {
+        Group g;
+        g.elem = j;  // row index (z_int is per discharge element)
+        g.side = s;
+        g.frac = s ? h.frac1[e] : h.frac0[e];
+        g.npts = D;
+        g.kind = KIND_PHI;
+        g.out = nvals;
+        g.pad0 = g.pad1 = 0;
+        nvals += D;
+        index_of[2 * (size_t)j + s] = (int)groups.size();
+        per_frac[g.frac].push_back((int)groups.size());
+        groups.push_back(g);
+      }
+    }
+  }
+  // flatten: within a fracture, PSI groups first (bounding circles lead the
+  // element order) so mixed warps are rare
+  struct Cost {
+    double c;
+    Item it;
+  };
+  std::vector<Cost> costs;
+  for (int f = 0; f < nf; f++) {
+    auto &gl = per_frac[f];
+    std::stable_sort(gl.begin(), gl.end(), [&](int a, int b) { return groups[a].kind > groups[b].kind; });
+    const int start = (int)pts.size();
+    for (int gi : gl)
+      for (int k = 0; k < groups[gi].npts; k++) pts.push_back(make_int2(gi, k));
+    const int end = (int)pts.size();
+    double work_per_pt = 0.0;
+    for (int k = h.fptr[f]; k < h.fptr[f + 1]; k++) work_per_pt += 30.0 + 4.0 * h.ncoef[h.felem[k]];
+    for (int p = start; p < end; p += EVAL_THREADS) {
+      Item it;
+      it.frac = f;
+      it.p0 = p;
+      it.p1 = std::min(end, p + EVAL_THREADS);
+      it.pad = 0;
+      costs.push_back({work_per_pt * (it.p1 - it.p0), it});
+    }
+  }
+  std::stable_sort(costs.begin(), costs.end(), [](const Cost &a, const Cost &b) { return a.c > b.c; });
+  for (auto &c : costs) items.push_back(c.it);
+}
+
+// Discharge-system pattern, row by row exactly as fill_discharge_matrix
+// (hpc_solve.py:1117-1201) orders it.
+static void build_pattern(AndfnHandle *H) {
+  const HostNet &h = H->h;
+  const int n_de = (int)h.de_ids.size();
+  const int nf = (int)H->nf;
+  H->N = n_de + nf;
+  H->mrow_ptr.assign(1, 0);
+  H->mcol.clear();
+  H->ent_row.clear();
+  H->ent_src.clear();
+  H->ent_side.clear();
+  H->ent_kind.clear();
+  auto disch = [&](int ty) { return ty == 0 || ty == 2 || ty == 3; };
+  for (int j = 0; j < n_de; j++) {
+    const int e = h.de_ids[j];
+    const int sides = (h.type[e] == 0) ? 2 : 1;
+    for (int s = 0; s < sides; s++) {
+      const int f = s ? h.frac1[e] : h.frac0[e];
+      for (int k = h.fptr[f]; k < h.fptr[f + 1]; k++) {
+        const int ee = h.felem[k];
+        if (ee == e || !disch(h.type[ee])) continue;
+        H->mcol.push_back(h.elem_de[ee]);
+        H->ent_row.push_back(j);
+        H->ent_src.push_back(ee);
+        H->ent_side.push_back(s);
+        H->ent_kind.push_back(0);
+      }
+    }
+    for (int s = 0; s < sides; s++) {
+      const int f = s ? h.frac1[e] : h.frac0[e];
+      H->mcol.push_back(n_de + f);
+      H->ent_row.push_back(j);
+      H->ent_src.push_back(-1);
+      H->ent_side.push_back(s);
+      H->ent_kind.push_back(1);
+    }
+    H->mrow_ptr.push_back((int)H->mcol.size());
+  }
+  for (int f = 0; f < nf; f++) {
+    for (int k = h.fptr[f]; k < h.fptr[f + 1]; k++) {
+      const int el = h.felem[k];
+      if (!disch(h.type[el])) continue;
+      H->mcol.push_back(h.elem_de[el]);
+      H->ent_row.push_back(n_de + f);
+      H->ent_src.push_back(el);
+      H->ent_side.push_back(0);
+      H->ent_kind.push_back(2);
+    }
+    H->mrow_ptr.push_back((int)H->mcol.size());
+  }
+}
+
+static int reset_impl(AndfnHandle *H);
+
+static int create_impl(AndfnHandle *H, const char *F, const char *E) {
+  int rc = parse_records(H, F, E);
+  if (rc) return rc;
+  read_coefs(H, E);
+  HostNet &h = H->h;
+  cudaStream_t s = H->stream;
+  const int ne = (int)H->ne;
+  CK(upload(H->type, h.type, s));
+  CK(upload(H->frac0, h.frac0, s));
+  CK(upload(H->frac1, h.frac1, s));
+  CK(upload(H->ncoef0, h.ncoef, s));
+  CK(upload(H->nint0, h.nint, s));
+  CK(H->ncoef.alloc(ne));
+  CK(H->nint.alloc(ne));
+  CK(upload(H->ep0, h.ep0, s));
+  CK(upload(H->ep1, h.ep1, s));
+  CK(upload(H->center, h.center, s));
+  CK(upload(H->radius, h.radius, s));
+  CK(upload(H->phi, h.phi, s));
+  CK(upload(H->q0, h.q, s));
+  CK(H->q.alloc(ne));
+  CK(upload(H->coef0, h.coef, s));
+  CK(H->coef.alloc((size_t)ne * H->MC));
+  CK(H->wcoef.alloc((size_t)ne * H->MC));
+  CK(upload(H->err_in, h.err, s));
+  CK(upload(H->err_old_in, h.err_old, s));
+  CK(upload(H->err_old2_in, h.err_old2, s));
+  CK(upload(H->err_coef_in, h.err_coef, s));
+  CK(H->err.alloc(ne));
+  CK(H->err_old.alloc(ne));
+  CK(H->err_old2.alloc(ne));
+  CK(H->err_coef.alloc(ne));
+  CK(H->dpsi_corr.alloc((size_t)ne * 2 * H->MC));
+  CK(upload(H->t, h.t, s));
+  CK(upload(H->constant0, h.constant, s));
+  CK(H->constant.alloc(h.constant.size()));
+  CK(upload(H->fptr, h.fptr, s));
+  CK(upload(H->felem, h.felem, s));
+  CK(upload(H->de_ids, h.de_ids, s));
+  const int n_de = (int)h.de_ids.size();
+  CK(H->zint0.alloc((size_t)std::max(1, n_de) * H->D));
+  CK(H->zint1.alloc((size_t)std::max(1, n_de) * H->D));
+  // branch-cut capacity: crossings per psi element are bounded by twice the
+  // discharge elements of its fracture
+  int maxd = 0;
+  for (int f = 0; f < (int)H->nf; f++) {
+    int c = 0;
+    for (int k = h.fptr[f]; k < h.fptr[f + 1]; k++) {
+      int ty = h.type[h.felem[k]];
+      c += (ty == 0 || ty == 2 || ty == 3);
+    }
+    maxd = std::max(maxd, c);
+  }
+  H->cut_cap = 2 * maxd + 4;
+  CK(H->cut_n.alloc(ne));
+  CK(H->cut_pos.alloc((size_t)ne * H->cut_cap));
+  CK(H->cut_elem.alloc((size_t)ne * H->cut_cap));
+  CK(H->cut_sign.alloc((size_t)ne * H->cut_cap));
+  // tables
+  std::vector<Group> groups;
+  std::vector<int> group_of, rhs_group;
+  std::vector<Item> sitems, ritems;
+  std::vector<int2> spts, rpts;
+  int nsv = 0, nrv = 0;
+  build_tables(H, false, groups, group_of, sitems, spts, nsv);
+  build_tables(H, true, groups, rhs_group, ritems, rpts, nrv);
+  H->groups = groups;
+  CK(upload(H->d_groups, groups, s));
+  CK(upload(H->group_of, group_of, s));
+  CK(upload(H->rhs_group, rhs_group, s));
+  CK(upload(H->sweep_items, sitems, s));
+  CK(upload(H->rhs_items, ritems, s));
+  CK(upload(H->sweep_pts, spts, s));
+  CK(upload(H->rhs_pts, rpts, s));
+  H->n_sweep_items = (int)sitems.size();
+  H->n_rhs_items = (int)ritems.size();
+  CK(H->sweep_vals.alloc(std::max(1, nsv)));
+  CK(H->rhs_vals.alloc(std::max(1, nrv)));
+  std::vector<int> upd, psi;
+  int nvmax = 2;
+  for (int e = 0; e < ne; e++) {
+    upd.push_back(e);
+    if (h.type[e] == 1 || h.type[e] == 4 || h.type[e] == 5) psi.push_back(e);
+    nvmax = std::max(nvmax, h.nint[e]);
+  }
+  H->n_upd = (int)upd.size();
+  H->n_psi = (int)psi.size();
+  H->nvmax = nvmax;
+  CK(upload(H->upd_list, upd, s));
+  CK(upload(H->psi_list, psi, s));
+  // eval staging: sources per chunk within the shared-memory budget
+  int maxnf = 1;
+  for (int f = 0; f < (int)H->nf; f++) maxnf = std::max(maxnf, h.fptr[f + 1] - h.fptr[f]);
+  const size_t budget = 96 * 1024;
+  int chunk = (int)(budget / (sizeof(Src) + sizeof(cd) * H->MC));
+  chunk = std::max(1, std::min(chunk, maxnf));
+  H->chunk = chunk;
+  H->eval_smem = (sizeof(Src) + sizeof(cd) * H->MC) * chunk;
+  // discharge system
+  build_pattern(H);
+  CK(upload(H->d_ent_row, H->ent_row, s));
+  CK(upload(H->d_ent_src, H->ent_src, s));
+  CK(upload(H->d_ent_side, H->ent_side, s));
+  CK(upload(H->d_ent_kind, H->ent_kind, s));
+  CK(H->d_mvals.alloc(std::max<size_t>(1, H->ent_row.size())));
+  {
+    // fill-reducing column order from the pattern alone (values do not
+    // matter for it), computed once per network
+    CscMatrix P;
+    P.n = H->N;
+    P.colptr.assign(H->N + 1, 0);
+    for (int c : H->mcol) P.colptr[c + 1]++;
+    for (int i = 0; i < H->N; i++) P.colptr[i + 1] += P.colptr[i];
+    P.rowind.resize(H->mcol.size());
+    P.val.assign(H->mcol.size(), 1.0);
+    std::vector<int> fill(P.colptr.begin(), P.colptr.end() - 1);
+    for (int r = 0; r < H->N; r++)
+      for (int p = H->mrow_ptr[r]; p < H->mrow_ptr[r + 1]; p++) P.rowind[fill[H->mcol[p]]++] = r;
+    H->colorder = column_min_degree_order(P);
+  }
+  CK(H->disc.alloc(H->N));
+  CK(H->work.alloc(H->N));
+  CK(H->ready.alloc(H->N));
+  CK(H->st.alloc(1));
+  if (!H->h_st) CK(cudaMallocHost(&H->h_st, sizeof(SolveState)));
+  CK(cudaFuncSetAttribute(eval_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+  CK(cudaFuncSetAttribute(eval_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+  CK(cudaFuncSetAttribute(trisolve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+  CK(cudaFuncSetAttribute(update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+  rc = reset_impl(H);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(s));
+  return 0;
+}
+
+// Copies the initial state into the working arrays.
+static int reset_impl(AndfnHandle *H) {
+  cudaStream_t s = H->stream;
+  const size_t ne = H->ne;
+  CK(cudaMemcpyAsync(H->ncoef.p, H->ncoef0.p, sizeof(int) * ne, cudaMemcpyDeviceToDevice, s));
+  CK(cudaMemcpyAsync(H->nint.p, H->nint0.p, sizeof(int) * ne, cudaMemcpyDeviceToDevice, s));
+  CK(cudaMemcpyAsync(H->q.p, H->q0.p, sizeof(double) * ne, cudaMemcpyDeviceToDevice, s));
+  CK(cudaMemcpyAsync(H->coef.p, H->coef0.p, sizeof(cd) * ne * H->MC, cudaMemcpyDeviceToDevice, s));
+  CK(cudaMemcpyAsync(H->err.p, H->err_in.p, sizeof(double) * ne, cudaMemcpyDeviceToDevice, s));
+  CK(cudaMemcpyAsync(H->err_old.p, H->err_old_in.p, sizeof(double) * ne, cudaMemcpyDeviceToDevice, s));
+  CK(cudaMemcpyAsync(H->err_old2.p, H->err_old2_in.p, sizeof(double) * ne, cudaMemcpyDeviceToDevice, s));
+  CK(cudaMemcpyAsync(H->err_coef.p, H->err_coef_in.p, sizeof(double) * ne, cudaMemcpyDeviceToDevice, s));
+  CK(cudaMemcpyAsync(H->constant.p, H->constant0.p, sizeof(double) * H->nf, cudaMemcpyDeviceToDevice, s));
+  CK(cudaMemsetAsync(H->dpsi_corr.p, 0, sizeof(double) * ne * 2 * H->MC, s));
+  return 0;
+}
+
+static double ms_since(std::chrono::steady_clock::time_point t0) {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// Groups the rows of a triangular factor by dependency level and stores their
+// entries in that order (level_solve reads one contiguous range per level).
+static void build_levels(int n, const std::vector<int> &ptr, const std::vector<int> &col,
+                         const std::vector<double> &val, const std::vector<double> *scale, bool lower,
+                         std::vector<int> &lev_ptr, std::vector<int> &rows, std::vector<int> &eptr,
+                         std::vector<int> &ecol, std::vector<double> &evals, std::vector<double> &escale) {
+  std::vector<int> lev(n, 0);
+  int nlev = 0;
+  for (int t = 0; t < n; t++) {
+    const int i = lower ? t : n - 1 - t;
+    int l = 0;
+    for (int p = ptr[i]; p < ptr[i + 1]; p++) l = std::max(l, lev[col[p]] + 1);
+    lev[i] = l;
+    nlev = std::max(nlev, l + 1);
+  }
+  lev_ptr.assign(nlev + 1, 0);
+  for (int i = 0; i < n; i++) lev_ptr[lev[i] + 1]++;
+  for (int l = 0; l < nlev; l++) lev_ptr[l + 1] += lev_ptr[l];
+  rows.assign(n, 0);
+  std::vector<int> fill(lev_ptr.begin(), lev_ptr.end() - 1);
+  for (int t = 0; t < n; t++) {
+    const int i = lower ? t : n - 1 - t;
+    rows[fill[lev[i]]++] = i;
+  }
+  eptr.assign(n + 1, 0);
+  ecol.clear();
+  evals.clear();
+  escale.assign(n, 1.0);
+  for (int sl = 0; sl < n; sl++) {
+    const int i = rows[sl];
+    for (int p = ptr[i]; p < ptr[i + 1]; p++) {
+      ecol.push_back(col[p]);
+      evals.push_back(val[p]);
+    }
+    eptr[sl + 1] = (int)ecol.size();
+    if (scale) escale[sl] = (*scale)[i];
+  }
+}
+
+static inline void mark(AndfnHandle *H, cudaStream_t s, int b, int c, int w) {
+  if (H->profiling && b >= 0) cudaEventRecordWithFlags(H->ev[b][c][w], s, cudaEventRecordExternal);
+}
+
+static int enqueue_iteration(AndfnHandle *H, cudaStream_t s, int single_blend_sweep, int b = -1) {
+  Net net = H->net();
+  mark(H, s, b, K_RHS, 0);
+  if (H->n_rhs_items > 0) {
+    eval_kernel<true><<<H->n_rhs_items, EVAL_THREADS, H->eval_smem, s>>>(net, H->rhs_items.p, H->rhs_pts.p,
+                                                                          H->d_groups.p, H->rhs_vals.p, H->chunk);
+  }
+  mark(H, s, b, K_RHS, 1);
+  LevelSolve Lf{H->lf_lev.p, H->lf_rows.p, H->lf_eptr.p, H->lf_col.p, H->lf_val.p, nullptr, H->lf_nlev};
+  LevelSolve Ub{H->ub_lev.p, H->ub_rows.p, H->ub_eptr.p, H->ub_col.p, H->ub_val.p, H->ub_scale.p, H->ub_nlev};
+  const size_t ybytes = sizeof(double) * (size_t)H->N;
+  const int use_smem = ybytes <= 150 * 1024;
+  const size_t lev_bytes = sizeof(int) * (size_t)(std::max(H->lf_nlev, H->ub_nlev) + 1);
+  const int cap_levptr = (int)std::min<size_t>(lev_bytes, 40 * 1024) / (int)sizeof(int);
+  const size_t solve_smem = (use_smem ? ybytes : 0) + sizeof(int) * (size_t)cap_levptr;
+  mark(H, s, b, K_TRISOLVE, 0);
+  trisolve_kernel<<<1, H->solve_threads, solve_smem, s>>>(net, H->rhs_vals.p, H->rhs_group.p, H->d_groups.p,
+                                                          use_smem, Lf, Ub, cap_levptr);
+  mark(H, s, b, K_TRISOLVE, 1);
+  mark(H, s, b, K_SWEEP, 0);
+  if (H->n_sweep_items > 0)
+    eval_kernel<false><<<H->n_sweep_items, EVAL_THREADS, H->eval_smem, s>>>(
+        net, H->sweep_items.p, H->sweep_pts.p, H->d_groups.p, H->sweep_vals.p, H->chunk);
+  mark(H, s, b, K_SWEEP, 1);
+  const int ub = (H->n_upd + UPDATE_WARPS - 1) / UPDATE_WARPS;
+  const size_t usmem = sizeof(double) * 2 * H->nvmax * UPDATE_WARPS;
+  mark(H, s, b, K_UPDATE, 0);
+  if (ub > 0)
+    update_kernel<<<ub, UPDATE_WARPS * 32, usmem, s>>>(net, H->upd_list.p, H->n_upd, H->group_of.p, H->d_groups.p,
+                                                        H->sweep_vals.p, H->nvmax, single_blend_sweep);
+  mark(H, s, b, K_UPDATE, 1);
+  mark(H, s, b, K_REDUCE, 0);
+  reduce_kernel<<<1, 1024, 0, s>>>(net);
+  mark(H, s, b, K_REDUCE, 1);
+  H->launches += 5;
+  return 0;
+}
+
+static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S) {
+  auto t_all = std::chrono::steady_clock::now();
+  cudaStream_t s = H->stream;
+  AndfnSolveStats stats;
+  std::memset(&stats, 0, sizeof(stats));
+  stats.device = H->device;
+  H->launches = 0;
+  if (C->max_ncoef > H->L.max_ncoef || C->max_iterations < 0) {
+    set_error("constants out of range");
+    return ANDFN_BAD_INPUT;
+  }
+  // Adaptive coefficient growth (hpc_solve.py:465-559) needs MAX_NCOEF above
+  // the current ncoef somewhere; this build implements the pinned case.
+  bool growth_possible = false;
+  for (int64_t i = 0; i < H->ne; i++)
+    if (H->h.type[i] != 2 && H->h.ncoef[i] < C->max_ncoef) growth_possible = true;
+  if (growth_possible) {
+    set_error("adaptive ncoef growth (MAX_NCOEF > ncoef) is not supported by this entry point yet");
+    return ANDFN_BAD_INPUT;
+  }
+  int rc = reset_impl(H);
+  if (rc) return rc;
+  Net net = H->net();
+  SolveState st0;
+  std::memset(&st0, 0, sizeof(st0));
+  st0.error_q = 1.0;
+  st0.max_error = C->max_error;
+  st0.damping = C->damping;
+  st0.max_it = (int)C->max_iterations;
+  st0.fused_blend2 = 1;
+  st0.solve_q = 1;
+  st0.done = (C->max_iterations <= 0) ? 1 : 0;
+  CK(cudaMemcpyAsync(H->st.p, &st0, sizeof(st0), cudaMemcpyHostToDevice, s));
+  auto t_setup = std::chrono::steady_clock::now();
+  init_state_kernel<<<std::max<int64_t>(1, (H->ne + 255) / 256), 256, 0, s>>>(net);
+  const int n_de = (int)H->h.de_ids.size();
+  if (n_de > 0) zint_kernel<<<std::max(1, std::min(1184, (int)((n_de * H->D + 255) / 256))), 256, 0, s>>>(net);
+  if (H->n_psi > 0) cuts_kernel<<<(H->n_psi * 32 + 127) / 128, 128, 0, s>>>(net, H->psi_list.p, H->n_psi);
+  const long long nent = (long long)H->ent_row.size();
+  if (nent > 0)
+    matrix_values_kernel<<<(unsigned)((nent * 32 + 255) / 256), 256, 0, s>>>(
+        net, H->d_ent_row.p, H->d_ent_src.p, H->d_ent_side.p, H->d_ent_kind.p, H->d_mvals.p, nent);
+  H->launches += 4;
+  std::vector<double> mv(nent);
+  if (nent > 0) CK(cudaMemcpyAsync(mv.data(), H->d_mvals.p, sizeof(double) * nent, cudaMemcpyDeviceToHost, s));
+  g_d2h_bytes += 8 * nent;
+  // initial discharges (get_old_discharges, hpc_solve.py:765-775)
+  std::vector<double> disc0(H->N, 0.0);
+  for (int j = 0; j < n_de; j++) disc0[j] = H->h.q[H->h.de_ids[j]];
+  for (int64_t f = 0; f < H->nf; f++) disc0[n_de + f] = H->h.constant[f];
+  CK(cudaMemcpyAsync(H->disc.p, disc0.data(), sizeof(double) * H->N, cudaMemcpyHostToDevice, s));
+  g_h2d_bytes += 8 * (int64_t)H->N;
+  CK(cudaStreamSynchronize(s));
+  stats.ms_setup = ms_since(t_setup);
+  // factorisation (host): CSC of the pattern, cached column order
+  auto t_fac = std::chrono::steady_clock::now();
+  CscMatrix A;
+  A.n = H->N;
+  A.colptr.assign(H->N + 1, 0);
+  for (int c : H->mcol) A.colptr[c + 1]++;
+  for (int i = 0; i < H->N; i++) A.colptr[i + 1] += A.colptr[i];
+  A.rowind.resize(H->mcol.size());
+  A.val.resize(H->mcol.size());
+  {
+    std::vector<int> fill(A.colptr.begin(), A.colptr.end() - 1);
+    for (int r = 0; r < H->N; r++)
+      for (int p = H->mrow_ptr[r]; p < H->mrow_ptr[r + 1]; p++) {
+        const int c = H->mcol[p];
+        A.rowind[fill[c]] = r;
+        A.val[fill[c]++] = mv[p];
+      }
+  }
+  if ((int)H->colorder.size() != H->N) H->colorder = column_min_degree_order(A);
+  LuFactors LU;
+  rc = sparse_lu_factor(A, H->colorder, 1.0, LU);
+  if (rc) {
+    set_error("discharge system is singular (a fracture without a head boundary?)");
+    return ANDFN_SINGULAR;
+  }
+  H->nnz_factors = LU.nnz();
+  CK(upload(H->pinv, LU.pinv, s));
+  CK(upload(H->qcol, LU.q, s));
+  CK(upload(H->l_ptr, LU.l_ptr, s));
+  CK(upload(H->l_col, LU.l_col, s));
+  CK(upload(H->l_val, LU.l_val, s));
+  CK(upload(H->u_ptr, LU.u_ptr, s));
+  CK(upload(H->u_col, LU.u_col, s));
+  CK(upload(H->u_val, LU.u_val, s));
+  CK(upload(H->u_inv, LU.u_inv_diag, s));
+  {
+    std::vector<int> lev, rows, eptr, ecol;
+    std::vector<double> ev, esc;
+    build_levels(H->N, LU.l_ptr, LU.l_col, LU.l_val, nullptr, true, lev, rows, eptr, ecol, ev, esc);
+    H->lf_nlev = (int)lev.size() - 1;
+    CK(upload(H->lf_lev, lev, s));
+    CK(upload(H->lf_rows, rows, s));
+    CK(upload(H->lf_eptr, eptr, s));
+    CK(upload(H->lf_col, ecol, s));
+    CK(upload(H->lf_val, ev, s));
+    CK(cudaStreamSynchronize(s));
+    build_levels(H->N, LU.u_ptr, LU.u_col, LU.u_val, &LU.u_inv_diag, false, lev, rows, eptr, ecol, ev, esc);
+    H->ub_nlev = (int)lev.size() - 1;
+    CK(upload(H->ub_lev, lev, s));
+    CK(upload(H->ub_rows, rows, s));
+    CK(upload(H->ub_eptr, eptr, s));
+    CK(upload(H->ub_col, ecol, s));
+    CK(upload(H->ub_val, ev, s));
+    CK(upload(H->ub_scale, esc, s));
+    CK(cudaStreamSynchronize(s));
+  }
+  stats.ms_factor = ms_since(t_fac);
+  // iterations, in graph batches
+  auto t_it = std::chrono::steady_clock::now();
+  if (H->graph_exec) {
+    cudaGraphExecDestroy(H->graph_exec);
+    H->graph_exec = nullptr;
+  }
+  {
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    if (H->profiling && !H->ev[0][0][0])
+      for (auto &bb : H->ev)
+        for (auto &c : bb)
+          for (auto &e : c) CK(cudaEventCreate(&e));
+    for (int b = 0; b < ITER_BATCH; b++) enqueue_iteration(H, s, 0, b);
+    CK(cudaStreamEndCapture(s, &g));
+    CK(cudaGraphInstantiate(&H->graph_exec, g, 0));
+    cudaGraphDestroy(g);
+  }
+  H->launches -= ITER_BATCH * 5;  // capture does not launch
+  int guard = 0;
+  int nit_before = 0;
+  while (true) {
+    CK(cudaGraphLaunch(H->graph_exec, s));
+    CK(cudaMemcpyAsync(H->h_st, H->st.p, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    H->launches += ITER_BATCH * 5;
+    if (H->profiling) {
+      // only the iterations that did work (later ones return at entry)
+      const int real = std::min(ITER_BATCH, H->h_st->nit - nit_before);
+      for (int b = 0; b < real; b++)
+        for (int c = 0; c < KCLASSES; c++) {
+          float ms = 0.f;
+          if (cudaEventElapsedTime(&ms, H->ev[b][c][0], H->ev[b][c][1]) == cudaSuccess) {
+            H->k_ms[c] += ms;
+            H->k_n[c] += 1;
+          }
+        }
+      nit_before = H->h_st->nit;
+    }
+    if (H->h_st->done) break;
+    if (++guard > 1 + C->max_iterations / ITER_BATCH + 2) break;
+  }
+  SolveState fin = *H->h_st;
+  // hpc_solve.py:224-234: an extra element_solver sweep at nit == MAX_ITERATIONS
+  if (fin.nit == C->max_iterations && !fin.nonfinite && fin.status == 0) {
+    SolveState tmp = fin;
+    tmp.done = 0;
+    CK(cudaMemcpyAsync(H->st.p, &tmp, sizeof(tmp), cudaMemcpyHostToDevice, s));
+    if (H->n_sweep_items > 0)
+      eval_kernel<false><<<H->n_sweep_items, EVAL_THREADS, H->eval_smem, s>>>(
+          net, H->sweep_items.p, H->sweep_pts.p, H->d_groups.p, H->sweep_vals.p, H->chunk);
+    const int ub = (H->n_upd + UPDATE_WARPS - 1) / UPDATE_WARPS;
+    const size_t usmem = sizeof(double) * 2 * H->nvmax * UPDATE_WARPS;
+    if (ub > 0)
+      update_kernel<<<ub, UPDATE_WARPS * 32, usmem, s>>>(net, H->upd_list.p, H->n_upd, H->group_of.p,
+                                                          H->d_groups.p, H->sweep_vals.p, H->nvmax, 1);
+    H->launches += 2;
+    CK(cudaMemcpyAsync(H->st.p, &fin, sizeof(fin), cudaMemcpyHostToDevice, s));
+  }
+  CK(cudaStreamSynchronize(s));
+  CK(cudaGetLastError());
+  stats.ms_iterate = ms_since(t_it);
+  stats.iterations = fin.nit;
+  stats.cnt_error = fin.cnt_error;
+  stats.error = fin.error;
+  stats.error_coef = fin.error_coef;
+  stats.error_q = fin.error_q;
+  stats.worst_element = fin.worst;
+  stats.n_unknowns = H->N;
+  stats.nnz_matrix = (int64_t)H->mcol.size();
+  stats.nnz_factors = H->nnz_factors;
+  stats.gpu_launches = H->launches;
+  int status = ANDFN_OK;
+  if (fin.status) status = fin.status;
+  else if (fin.nonfinite) status = ANDFN_NONFINITE;
+  else if (fin.cnt_error < 2) status = ANDFN_MAX_ITERATIONS;
+  stats.status = status;
+  stats.ms_total = ms_since(t_all);
+  if (S) *S = stats;
+  return status;
+}
+
+static int download_impl(AndfnHandle *H, char *F, char *E) {
+  cudaStream_t s = H->stream;
+  const int64_t ne = H->ne, nf = H->nf;
+  const int MC = H->MC;
+  std::vector<cd> coef((size_t)ne * MC);
+  std::vector<int> ncoef(ne), nint(ne);
+  std::vector<double> q(ne), err(ne), eo(ne), eo2(ne), ec(ne), dc((size_t)ne * 2 * MC), cst(nf);
+  CK(cudaMemcpyAsync(coef.data(), H->coef.p, sizeof(cd) * coef.size(), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(ncoef.data(), H->ncoef.p, sizeof(int) * ne, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(nint.data(), H->nint.p, sizeof(int) * ne, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(q.data(), H->q.p, sizeof(double) * ne, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(err.data(), H->err.p, sizeof(double) * ne, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(eo.data(), H->err_old.p, sizeof(double) * ne, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(eo2.data(), H->err_old2.p, sizeof(double) * ne, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(ec.data(), H->err_coef.p, sizeof(double) * ne, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(dc.data(), H->dpsi_corr.p, sizeof(double) * dc.size(), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(cst.data(), H->constant.p, sizeof(double) * nf, cudaMemcpyDeviceToHost, s));
+  g_d2h_bytes += (int64_t)(sizeof(cd) * coef.size() + 4 * 2 * ne + 8 * 5 * ne + 8 * dc.size() + 8 * nf);
+  CK(cudaStreamSynchronize(s));
+  const AndfnLayout &L = H->L;
+  for (int64_t i = 0; i < ne; i++) {
+    char *r = E + i * L.elem_size;
+    const int m = ncoef[i], n = nint[i], ty = H->h.type[i];
+    int64_t v;
+    v = m;
+    std::memcpy(r + L.e_ncoef, &v, 8);
+    v = n;
+    std::memcpy(r + L.e_nint, &v, 8);
+    std::memcpy(r + L.e_coef, &coef[(size_t)i * MC], sizeof(cd) * std::min(m, MC));
+    // thetas as calc_thetas writes them (hpc_math_functions.py:693-699)
+    double del = PI / n, start = del / 2;
+    if (ty == 1) {
+      del = 2 * PI / n;
+      start = 0.0;
+    }
+    for (int k = 0; k < n; k++) {
+      double th = start + k * del;
+      std::memcpy(r + L.e_thetas + 8 * k, &th, 8);
+    }
+    std::memcpy(r + L.e_q, &q[i], 8);
+    std::memcpy(r + L.e_error, &err[i], 8);
+    std::memcpy(r + L.e_error_old, &eo[i], 8);
+    if (ty != 2) {
+      std::memcpy(r + L.e_error_old2, &eo2[i], 8);
+      std::memcpy(r + L.e_error_coef, &ec[i], 8);
+    }
+    if (ty == 1 || ty == 4 || ty == 5)
+      std::memcpy(r + L.e_dpsi_corr, &dc[(size_t)i * 2 * MC], 8 * std::max(0, n - 1));
+  }
+  for (int64_t f = 0; f < nf; f++) std::memcpy(F + f * L.frac_size + L.f_constant, &cst[f], 8);
+  return 0;
+}
+
+}  // namespace andfn
+
+// ==========================================================================
+// C ABI
+// ==========================================================================
+extern "C" {
+
+const char *andfn_b200_last_error(void) { return g_last_error.c_str(); }
+const char *andfn_b200_version(void) { return "andfn_b200 0.1.0 (sm_100a, fp64)"; }
+
+int andfn_b200_create(AndfnHandle **out, const void *frac_recs, int64_t nf, const void *elem_recs, int64_t ne,
+                      const AndfnLayout *layout, int64_t discharge_int, int32_t device) {
+  if (!out) return ANDFN_BAD_INPUT;
+  *out = nullptr;
+  if (check_layout(layout)) {
+    set_error("inconsistent record layout");
+    return ANDFN_BAD_LAYOUT;
+  }
+  if (nf <= 0 || ne <= 0 || !frac_recs || !elem_recs || discharge_int < 1 || discharge_int > 100000) {
+    set_error("empty network or discharge_int out of range");
+    return ANDFN_BAD_INPUT;
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    set_error("no CUDA device visible");
+    return ANDFN_NO_DEVICE;
+  }
+  AndfnHandle *H = new AndfnHandle();
+  if (device >= 0) {
+    if (cudaSetDevice(device) != cudaSuccess) {
+      delete H;
+      set_error("cudaSetDevice failed");
+      return ANDFN_NO_DEVICE;
+    }
+  }
+  cudaGetDevice(&H->device);
+  cudaDeviceProp prop;
+  cudaGetDeviceProperties(&prop, H->device);
+  if (prop.major < 10) {
+    delete H;
+    set_error("an sm_100 (Blackwell) device is required");
+    return ANDFN_NO_DEVICE;
+  }
+  if (cudaStreamCreateWithFlags(&H->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete H;
+    set_error("cudaStreamCreate failed");
+    return ANDFN_CUDA_ERROR;
+  }
+  H->L = *layout;
+  if (const char *v = getenv("ANDFN_B200_SOLVE_THREADS")) {
+    int t = atoi(v);
+    if (t >= 32 && t <= 1024 && t % 32 == 0) H->solve_threads = t;
+  }
+  H->ne = ne;
+  H->nf = nf;
+  H->D = discharge_int;
+  int rc = create_impl(H, (const char *)frac_recs, (const char *)elem_recs);
+  if (rc) {
+    delete H;
+    return rc;
+  }
+  *out = H;
+  return 0;
+}
+
+int andfn_b200_upload_state(AndfnHandle *H, const void *frac_recs, const void *elem_recs) {
+  if (!H) return ANDFN_BAD_INPUT;
+  cudaSetDevice(H->device);
+  const char *E = (const char *)elem_recs;
+  const char *F = (const char *)frac_recs;
+  const AndfnLayout &L = H->L;
+  for (int64_t i = 0; i < H->ne; i++) {
+    const char *r = E + i * L.elem_size;
+    H->h.q[i] = rd_f64(r, L.e_q);
+    H->h.err[i] = rd_f64(r, L.e_error);
+    H->h.err_old[i] = rd_f64(r, L.e_error_old);
+    H->h.err_old2[i] = rd_f64(r, L.e_error_old2);
+    H->h.err_coef[i] = rd_f64(r, L.e_error_coef);
+    int64_t m = rd_i64(r, L.e_ncoef);
+    if (m != H->h.ncoef[i]) {
+      set_error("upload_state: ncoef changed; create a new handle");
+      return ANDFN_BAD_INPUT;
+    }
+  }
+  for (int64_t f = 0; f < H->nf; f++) H->h.constant[f] = rd_f64(F + f * L.frac_size, L.f_constant);
+  read_coefs(H, E);
+  cudaStream_t s = H->stream;
+  CK(cudaMemcpyAsync(H->q0.p, H->h.q.data(), 8 * H->ne, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(H->err_in.p, H->h.err.data(), 8 * H->ne, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(H->err_old_in.p, H->h.err_old.data(), 8 * H->ne, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(H->err_old2_in.p, H->h.err_old2.data(), 8 * H->ne, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(H->err_coef_in.p, H->h.err_coef.data(), 8 * H->ne, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(H->constant0.p, H->h.constant.data(), 8 * H->nf, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(H->coef0.p, H->h.coef.data(), sizeof(cd) * H->h.coef.size(), cudaMemcpyHostToDevice, s));
+  int rc = reset_impl(H);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(s));
+  return 0;
+}
+
+int andfn_b200_reset_state(AndfnHandle *H) {
+  if (!H) return ANDFN_BAD_INPUT;
+  cudaSetDevice(H->device);
+  int rc = reset_impl(H);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(H->stream));
+  return 0;
+}
+
+int andfn_b200_run(AndfnHandle *H, const AndfnConstants *constants, AndfnSolveStats *stats) {
+  if (!H || !constants) return ANDFN_BAD_INPUT;
+  cudaSetDevice(H->device);
+  return run_impl(H, constants, stats);
+}
+
+int andfn_b200_download(AndfnHandle *H, void *frac_recs, void *elem_recs) {
+  if (!H || !frac_recs || !elem_recs) return ANDFN_BAD_INPUT;
+  cudaSetDevice(H->device);
+  return download_impl(H, (char *)frac_recs, (char *)elem_recs);
+}
+
+static int eval_points_impl(AndfnHandle *H, const int64_t *frac, const double *z, int64_t npts, double *omega,
+                            double *head) {
+  if (npts <= 0) return 0;
+  if (npts > (1LL << 31) - 1) return ANDFN_BAD_INPUT;
+  std::vector<int> fr(npts);
+  for (int64_t i = 0; i < npts; i++) {
+    if (frac[i] < 0 || frac[i] >= H->nf) {
+      set_error("point fracture index out of range");
+      return ANDFN_BAD_INPUT;
+    }
+    fr[i] = (int)frac[i];
+  }
+  cudaStream_t s = H->stream;
+  DBuf<int> dfr;
+  DBuf<cd> dz, dom;
+  DBuf<double> dh;
+  CK(dfr.alloc(npts));
+  CK(dz.alloc(npts));
+  CK(cudaMemcpyAsync(dfr.p, fr.data(), sizeof(int) * npts, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(dz.p, z, sizeof(cd) * npts, cudaMemcpyHostToDevice, s));
+  if (omega) CK(dom.alloc(npts));
+  if (head) CK(dh.alloc(npts));
+  points_kernel<<<(unsigned)((npts + 127) / 128), 128, 0, s>>>(H->net(), dfr.p, dz.p, (int)npts, dom.p, dh.p);
+  CK(cudaGetLastError());
+  if (omega) CK(cudaMemcpyAsync(omega, dom.p, sizeof(cd) * npts, cudaMemcpyDeviceToHost, s));
+  if (head) CK(cudaMemcpyAsync(head, dh.p, sizeof(double) * npts, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return 0;
+}
+
+int andfn_b200_eval_heads(AndfnHandle *H, const int64_t *frac, const double *z, int64_t npts, double *out) {
+  if (!H || (npts > 0 && (!frac || !z || !out))) return ANDFN_BAD_INPUT;
+  cudaSetDevice(H->device);
+  return eval_points_impl(H, frac, z, npts, nullptr, out);
+}
+
+int andfn_b200_eval_omega(AndfnHandle *H, const int64_t *frac, const double *z, int64_t npts, double *out) {
+  if (!H || (npts > 0 && (!frac || !z || !out))) return ANDFN_BAD_INPUT;
+  cudaSetDevice(H->device);
+  return eval_points_impl(H, frac, z, npts, out, nullptr);
+}
+
+void andfn_b200_destroy(AndfnHandle *H) {
+  if (!H) return;
+  cudaSetDevice(H->device);
+  cudaStreamSynchronize(H->stream);
+  delete H;
+}
+
+void *andfn_b200_stream(AndfnHandle *H) { return H ? (void *)H->stream : nullptr; }
+
+int andfn_b200_set_profiling(AndfnHandle *H, int on) {
+  if (!H) return ANDFN_BAD_INPUT;
+  H->profiling = on ? 1 : 0;
+  for (int c = 0; c < KCLASSES; c++) {
+    H->k_ms[c] = 0.0;
+    H->k_n[c] = 0;
+  }
+  return 0;
+}
+
+int andfn_b200_kernel_times(AndfnHandle *H, double *ms, int64_t *launches, int n) {
+  if (!H || n < KCLASSES) return ANDFN_BAD_INPUT;
+  for (int c = 0; c < KCLASSES; c++) {
+    ms[c] = H->k_ms[c];
+    launches[c] = H->k_n[c];
+  }
+  return 0;
+}
+
+int andfn_b200_fp64_peak(int32_t device, double *tflops) {
+  if (!tflops) return ANDFN_BAD_INPUT;
+  if (device >= 0 && cudaSetDevice(device) != cudaSuccess) return ANDFN_NO_DEVICE;
+  int dev = 0, nsm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  double *d = nullptr;
+  CK(cudaMalloc(&d, sizeof(double)));
+  const int iters = 1 << 14, threads = 256, blocks = nsm * 8;
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  fp64_peak_kernel<<<blocks, threads>>>(d, 64, 1.0000001, 1e-7);
+  float best = 1e30f;
+  for (int r = 0; r < 5; r++) {
+    cudaEventRecord(a);
+    fp64_peak_kernel<<<blocks, threads>>>(d, iters, 1.0000001, 1e-7);
+    cudaEventRecord(b);
+    cudaEventSynchronize(b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    best = std::min(best, ms);
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(d);
+  CK(cudaGetLastError());
+  *tflops = 2.0 * 8.0 * iters * (double)threads * blocks / (best * 1e-3) / 1e12;
+  return 0;
+}
+
+int andfn_b200_solve(void *frac_recs, int64_t nf, void *elem_recs, int64_t ne, const AndfnLayout *layout,
+                     int64_t discharge_int, const AndfnConstants *constants, AndfnSolveStats *stats) {
+  auto t0 = std::chrono::steady_clock::now();
+  g_h2d_bytes = g_d2h_bytes = 0;
+  AndfnHandle *H = nullptr;
+  int rc = andfn_b200_create(&H, frac_recs, nf, elem_recs, ne, layout, discharge_int, -1);
+  if (rc) return rc;
+  double ms_up = ms_since(t0);
+  AndfnSolveStats st;
+  std::memset(&st, 0, sizeof(st));
+  rc = andfn_b200_run(H, constants, &st);
+  if (rc == ANDFN_OK || rc == ANDFN_MAX_ITERATIONS || rc == ANDFN_NONFINITE) {
+    auto t1 = std::chrono::steady_clock::now();
+    int rc2 = andfn_b200_download(H, frac_recs, elem_recs);
+    st.ms_download = ms_since(t1);
+    if (rc2) rc = rc2;
+  }
+  st.ms_upload = ms_up;
+  st.h2d_bytes = g_h2d_bytes;
+  st.d2h_bytes = g_d2h_bytes;
+  andfn_b200_destroy(H);
+  st.ms_total = ms_since(t0);
+  if (stats) *stats = st;
+  return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,104 @@
+"""Handle API: keep one network resident in HBM across solves.
+
+``Solver`` wraps ``andfn_b200_create/run/download`` (include/andfn_b200.h).
+It is what repeated solves (benchmarks, parameter sweeps, the adjoint) use,
+so uploads and table construction happen once per network.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _ffi
+from .records import AndfnSolveStats, constants_struct, layout_of
+
+
+class Solver:
+    def __init__(self, fractures: np.ndarray, elements: np.ndarray, discharge_int: int = 50, device: int = -1):
+        if not (fractures.flags.c_contiguous and elements.flags.c_contiguous):
+            raise ValueError("records must be C-contiguous")
+        self.fractures, self.elements = fractures, elements
+        self.layout = layout_of(elements.dtype, fractures.dtype)
+        self._h = ctypes.c_void_p()
+        L = _ffi.lib()
+        _ffi.check(L.andfn_b200_create(ctypes.byref(self._h), fractures.ctypes.data_as(ctypes.c_void_p),
+                                       len(fractures), elements.ctypes.data_as(ctypes.c_void_p), len(elements),
+                                       ctypes.byref(self.layout), int(discharge_int), int(device)))
+        self.stats: dict = {}
+
+    def close(self):
+        if self._h:
+            _ffi.lib().andfn_b200_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def upload_state(self, fractures=None, elements=None):
+        f = self.fractures if fractures is None else fractures
+        e = self.elements if elements is None else elements
+        _ffi.check(_ffi.lib().andfn_b200_upload_state(self._h, f.ctypes.data_as(ctypes.c_void_p),
+                                                     e.ctypes.data_as(ctypes.c_void_p)))
+
+    def reset(self):
+        _ffi.check(_ffi.lib().andfn_b200_reset_state(self._h))
+
+    def run(self, constants) -> dict:
+        cst = constants_struct(constants)
+        st = AndfnSolveStats()
+        rc = _ffi.lib().andfn_b200_run(self._h, ctypes.byref(cst), ctypes.byref(st))
+        self.stats = st.as_dict()
+        _ffi.check(rc, ok=(0, 1, 2))
+        return self.stats
+
+    def download(self, fractures=None, elements=None):
+        f = self.fractures if fractures is None else fractures
+        e = self.elements if elements is None else elements
+        _ffi.check(_ffi.lib().andfn_b200_download(self._h, f.ctypes.data_as(ctypes.c_void_p),
+                                                 e.ctypes.data_as(ctypes.c_void_p)))
+        return e
+
+    KERNEL_CLASSES = ("eval_rhs", "trisolve", "eval_sweep", "update", "reduce")
+
+    def set_profiling(self, on: bool = True):
+        _ffi.check(_ffi.lib().andfn_b200_set_profiling(self._h, 1 if on else 0))
+
+    def kernel_times(self) -> dict:
+        ms = np.zeros(5)
+        n = np.zeros(5, np.int64)
+        _ffi.check(_ffi.lib().andfn_b200_kernel_times(self._h, ms.ctypes.data_as(ctypes.c_void_p),
+                                                     n.ctypes.data_as(ctypes.c_void_p), 5))
+        return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(self.KERNEL_CLASSES)}
+
+    def stream(self) -> int:
+        return int(_ffi.lib().andfn_b200_stream(self._h) or 0)
+
+    def eval_heads(self, frac_idx, z) -> np.ndarray:
+        """Heads Re(Omega_f(z))/t_f (andfn/hpc/hpc_fracture.py:205-252)."""
+        frac_idx = np.ascontiguousarray(frac_idx, np.int64)
+        z = np.ascontiguousarray(z, np.complex128)
+        out = np.empty(len(z))
+        _ffi.check(_ffi.lib().andfn_b200_eval_heads(self._h, frac_idx.ctypes.data_as(ctypes.c_void_p),
+                                                   z.ctypes.data_as(ctypes.c_void_p), len(z),
+                                                   out.ctypes.data_as(ctypes.c_void_p)))
+        return out
+
+    def eval_omega(self, frac_idx, z) -> np.ndarray:
+        """Omega_f(z) (andfn/hpc/hpc_fracture.py:52-94)."""
+        frac_idx = np.ascontiguousarray(frac_idx, np.int64)
+        z = np.ascontiguousarray(z, np.complex128)
+        out = np.empty(len(z), np.complex128)
+        _ffi.check(_ffi.lib().andfn_b200_eval_omega(self._h, frac_idx.ctypes.data_as(ctypes.c_void_p),
+                                                   z.ctypes.data_as(ctypes.c_void_p), len(z),
+                                                   out.ctypes.data_as(ctypes.c_void_p)))
+        return out

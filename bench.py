@@ -1,0 +1,348 @@
+"""Benchmark of the B200 analytic-element DFN solve.
+
+One step = one complete plain solve (discharge-system assembly, sparse LU,
+and the damped Jacobi iteration to convergence at MAX_ERROR = 1e-8) of the
+~2,000-fracture network: power-law radii (alpha 2.6, 0.5-20 m), Fisher
+(kappa 5) normals, log10 T ~ N(-5, 1), heads 1 / 0 on the x faces, ncoef 20,
+nint 40, discharge_int 50.  The literal 2,000 discs in a 100 m cube do not
+percolate, so 5,500 discs are drawn in a 50 m cube (seed 0) and the largest
+cluster joining both heads is kept (2,015 fractures, 4,912 elements).
+
+value: solves/s with the network resident in HBM (handle API), timed with
+CUDA events on the library's stream, L2 flushed (256 MiB write) between steps.
+e2e:   solves/s through the one-call C ABI (andfn_b200_solve) from host
+records, host<->device copies included.
+--impl reference: the CPU oracle (a C + OpenMP restatement of the reference's
+Numba solver with SciPy's SuperLU) on all host cores, each step a bounded
+sample (10 outer iterations) scaled to a full solve.
+
+Multi-GPU (torchrun): every rank solves its own copy of the network
+(independent replicas; the solve has no exchange step).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "batched vs plain DFN solves/s at 1e-8 BC residual; adjoint/forward time ratio"
+WORKLOAD = ("plain solve: 2,015-fracture spanning cluster of 5,500 power-law/Fisher discs in a 50 m cube "
+            "(seed 0), ncoef 20, nint 40, discharge_int 50, MAX_ERROR 1e-8")
+MAX_ERROR = 1e-8
+SAMPLE_ITS = 10
+
+
+def build_network(seed=0):
+    from andfn_b200 import network as nw
+    net = nw.power_law_fisher(seed, nf=5500, L=50.0, ncoef=20, nint=40)
+    return nw.to_records(net)
+
+
+def constants():
+    from andfn_b200.records import default_constants
+    return default_constants(MAX_ITERATIONS=200, MAX_ERROR=MAX_ERROR, MAX_NCOEF=20)
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def algorithmic_work(F, E, D):
+    """Per-launch algorithmic FP64 flops of the evaluation kernels and bytes
+    of the triangular solve (pair cost P(e') = 8(m'-1) + 2 + M + R + L + 2 with
+    M = 48 (line) / 4 (circle), R = 11 (Laurent), L = 20 (discharge types))."""
+    ty, m, n = E["_type"], E["ncoef"], E["nint"]
+    P = np.zeros(len(E))
+    line = np.isin(ty, (0, 3, 5))
+    P += np.where(m > 0, 8.0 * (m - 1) + 2, 0.0)
+    P += np.where(line, 48.0, 4.0)
+    P += np.where(np.isin(ty, (0, 3, 4, 5)), 11.0, 0.0)
+    P += np.where(np.isin(ty, (0, 2, 3)), 20.0, 0.0)
+    P += 2.0
+    psum = np.zeros(len(F))
+    for f in range(len(F)):
+        els = F["elements"][f, : F["nelements"][f]]
+        psum[f] = P[els].sum()
+    sweep = rhs = dft = 0.0
+    for e in range(len(E)):
+        if ty[e] == 2:
+            continue
+        sides = [E["frac0"][e]] + ([E["frac1"][e]] if ty[e] == 0 else [])
+        for f in sides:
+            sweep += n[e] * (psum[f] - P[e])
+            dft += 4.0 * n[e] * m[e]
+            if ty[e] in (0, 3):
+                rhs += D * psum[f]
+    for e in np.nonzero(ty == 2)[0]:
+        rhs += D * psum[E["frac0"][e]]
+    return {"eval_sweep_flops": sweep, "eval_rhs_flops": rhs, "update_flops": dft}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def cpu_sample(F, E, D, c, iterations_full, threads=None):
+    """The oracle on a bounded sample: assembly + LU + SAMPLE_ITS iterations,
+    scaled to a full solve of iterations_full iterations."""
+    from oracle import oracle as orc
+    if threads:
+        orc.set_num_threads(threads)
+    cc = c.copy()
+    cc["MAX_ITERATIONS"] = SAMPLE_ITS
+    Fs, Es = F.copy(), E.copy()
+    st = {}
+    t0 = time.perf_counter()
+    orc.solve(Fs, Es, D, cc, stats=st)
+    wall = time.perf_counter() - t0
+    per_it = (st["s_discharge"] + st["s_elements"]) / st["iterations"]
+    est = st["s_matrix"] + st["s_lu"] + per_it * iterations_full
+    return {"seconds_per_solve": est, "sample_seconds": wall, "threads": st["threads"]}
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    F, E = build_network()
+    c = constants()
+    D = 50
+    its_full = int(os.environ.get("ANDFN_BENCH_ITERATIONS", "91"))
+    for _ in range(args.warmup):
+        cpu_sample(F, E, D, c, its_full)
+    secs = []
+    thr = None
+    for _ in range(args.steps):
+        r = cpu_sample(F, E, D, c, its_full)
+        secs.append(r["seconds_per_solve"])
+        thr = r["threads"]
+    v = 1.0 / float(np.mean(secs))
+    sample = (f"oracle (C+OpenMP restatement of the reference's Numba solve, SciPy SuperLU): assembly, LU and "
+              f"{SAMPLE_ITS} outer iterations per step, scaled to {its_full} iterations")
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": WORKLOAD, "parallelism": "cpu threads"},
+            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": thr, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_gpu(args):
+    import torch
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    device = local if ws > 1 else 0
+    torch.cuda.set_device(device)
+    import andfn_b200
+    from andfn_b200 import _ffi
+    F, E = build_network()
+    c = constants()
+    D = 50
+    # FP64 roofline denominator
+    fp64 = ctypes_double()
+    _ffi.check(_ffi.lib().andfn_b200_fp64_peak(device, ctypes_ref(fp64)))
+    fp64_tflops = fp64.value
+    solver = andfn_b200.Solver(F, E, D, device=device)
+    stream = torch.cuda.ExternalStream(solver.stream())
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{device}")
+    for _ in range(args.warmup):
+        solver.reset()
+        solver.run(c)
+    torch.cuda.synchronize()
+    solver.set_profiling(True)
+    clocks = ClockSampler(device)
+    clocks.start()
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    step_ms = []
+    launches = 0
+    stats = {}
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        solver.reset()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        stats = solver.run(c)
+        b.record(stream)
+        b.synchronize()
+        step_ms.append(a.elapsed_time(b))
+        launches += stats["gpu_launches"]
+    torch.cuda.synchronize()
+    if ws > 1:
+        torch.distributed.barrier()
+    kt = solver.kernel_times()
+    clk = clocks.stop()
+    total_ms = float(np.sum(step_ms))
+    if ws > 1:
+        t = torch.tensor([total_ms], device=f"cuda:{device}", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = ws * args.steps / (total_ms / 1e3)
+    # e2e: one-call C ABI from host records
+    e2e_ms = []
+    h2d = d2h = 0
+    for _ in range(max(1, min(args.steps, 3))):
+        Fh, Eh = F.copy(), E.copy()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        andfn_b200.solve(Fh, Eh, D, c)
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+        h2d = andfn_b200.last_stats["h2d_bytes"]
+        d2h = andfn_b200.last_stats["d2h_bytes"]
+    e2e_val = ws * 1e3 / float(np.mean(e2e_ms))
+    # roofline of the dominant kernel
+    work = algorithmic_work(F, E, D)
+    peaks = measured_peaks()
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    dom = max(kt, key=lambda k: kt[k][0])
+    per = {k: (v[0] / v[1] if v[1] else None) for k, v in kt.items()}
+    nnz = stats.get("nnz_factors", 0)
+    N = stats.get("n_unknowns", 0)
+    tri_bytes = 12.0 * nnz + 24.0 * N  # factor entries (int32 col + f64 value) + per-row tables
+    roof = {}
+    if dom in ("eval_sweep", "eval_rhs"):
+        fl = work["eval_sweep_flops"] if dom == "eval_sweep" else work["eval_rhs_flops"]
+        ach = fl / (per[dom] * 1e-3) / 1e12
+        roof = {"kernel": dom, "bound": "fp64", "achieved": ach, "peak": fp64_tflops, "unit": "TFLOP/s",
+                "frac": ach / fp64_tflops, "traffic": None, "peak_source": "measured FP64 FMA probe"}
+    else:
+        bytes_ = tri_bytes if dom == "trisolve" else 0.0
+        ach = bytes_ / (per[dom] * 1e-3) / 1e9
+        roof = {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                "traffic": None, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
+                "note": "latency-bound dependency chain (levels of L and U)"}
+    ev = {}
+    for k in ("eval_sweep", "eval_rhs"):
+        if per.get(k):
+            fl = work["eval_sweep_flops"] if k == "eval_sweep" else work["eval_rhs_flops"]
+            ev[k] = {"achieved_tflops": fl / (per[k] * 1e-3) / 1e12, "frac_of_fp64": fl / (per[k] * 1e-3) / 1e12 / fp64_tflops,
+                     "avg_us": per[k] * 1e3}
+    if rank == 0:
+        cpu = None
+        if not args.no_cpu:
+            r = cpu_sample(F, E, D, c, int(stats["iterations"]))
+            cpu = {"value": 1.0 / r["seconds_per_solve"], "unit": "solves/s", "cores": r["threads"], "kind": "port",
+                   "sample": f"oracle: assembly + LU + {SAMPLE_ITS} iterations ({r['sample_seconds']:.1f} s), "
+                             f"scaled to {stats['iterations']} iterations"}
+        line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+                "config": {"workload": WORKLOAD, "fractures": int(len(F)), "elements": int(len(E)),
+                           "iterations": int(stats["iterations"]), "n_unknowns": int(N), "nnz_lu": int(nnz),
+                           "l2": "flushed (256 MiB write) between steps", "parallelism": f"replicas x{ws}"},
+                "e2e": {"value": e2e_val, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
+                        "d2h_bytes_per_step": int(d2h)},
+                "gpu_launches": int(launches), "roofline": roof, "kernels_us": {k: (v * 1e3 if v else None) for k, v in per.items()},
+                "kernel_share": {k: kt[k][0] / max(1e-12, sum(v[0] for v in kt.values())) for k in kt},
+                "eval_roofline": ev, "phase_ms": {k: stats[k] for k in ("ms_setup", "ms_factor", "ms_iterate")},
+                "fp64_peak_tflops": fp64_tflops, "clocks": clk, "cpu_baseline": cpu}
+        print(json.dumps(line), flush=True)
+    solver.close()
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+
+
+def ctypes_double():
+    import ctypes
+    return ctypes.c_double()
+
+
+def ctypes_ref(x):
+    import ctypes
+    return ctypes.byref(x)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

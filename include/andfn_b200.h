@@ -1,0 +1,153 @@
+/*
+ * andfn_b200.h -- C ABI of the B200-native AnDFN analytic-element solve.
+ *
+ * The library replaces AnDFN's iterative solve
+ *     andfn.hpc.hpc_solve.solve(fracture_struc_array, element_struc_array,
+ *                               discharge_int, constants, ntype_elements)
+ * (andfn/hpc/hpc_solve.py:55-257), which andfn.dfn.DFN.solve calls at
+ * andfn/dfn.py:1840-1846 through the module-level name bound at andfn/dfn.py:21.
+ *
+ * Records are the reference's packed numpy structured arrays:
+ *   element_dtype_hpc   (andfn/element.py:45-69)
+ *   fracture_dtype_hpc  (andfn/element.py:146-159)
+ * Their field offsets depend on the YAML-configurable MAX_NCOEF / MAX_ELEMENTS
+ * (andfn/element.py:13-20), so every entry point takes an AndfnLayout that the
+ * caller derives from dtype.fields.  Records are read and written in place with
+ * the reference's semantics: elements get coef[:ncoef], ncoef, nint, thetas, q,
+ * error, error_old, error_old2, error_coef and dpsi_corr; fractures get
+ * constant.
+ *
+ * All arithmetic is IEEE binary64 / complex128.  No entry point allocates on
+ * the calling thread's CUDA stream other than its own; handles are not
+ * re-entrant (use one handle per host thread).
+ */
+#ifndef ANDFN_B200_H
+#define ANDFN_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Return codes (int).  0 is success; the solve-outcome codes (1..3) still
+ * leave the records updated with the last iterate, like the reference, which
+ * returns silently in those cases (andfn/hpc/hpc_solve.py:152,257). */
+enum {
+  ANDFN_OK = 0,
+  ANDFN_MAX_ITERATIONS = 1, /* loop stopped at MAX_ITERATIONS before 2 converged rounds */
+  ANDFN_NONFINITE = 2,      /* a coefficient, discharge or error became NaN/Inf        */
+  ANDFN_SINGULAR = 3,       /* discharge system has a zero pivot (disconnected fracture) */
+  ANDFN_BAD_LAYOUT = 10,    /* offsets/strides inconsistent or sizes out of range      */
+  ANDFN_BAD_INPUT = 11,     /* ids out of range, ncoef > capacity, nint/ncoef mismatch */
+  ANDFN_CUDA_ERROR = 12,    /* a CUDA runtime call failed (message via andfn_b200_last_error) */
+  ANDFN_NO_DEVICE = 13,     /* no sm_100 device visible                                */
+  ANDFN_OUT_OF_MEMORY = 14
+};
+
+/* Byte offsets of the record fields, as given by numpy dtype.fields[name][1].
+ * Complex fields are (re, im) double pairs; integer fields are int64. */
+typedef struct AndfnLayout {
+  int64_t elem_size; /* element_dtype_hpc.itemsize */
+  int64_t e_id, e_type, e_frac0, e_frac1, e_endpoints0, e_endpoints1, e_radius,
+      e_center, e_head, e_phi, e_ncoef, e_nint, e_q, e_thetas, e_coef,
+      e_old_coef, e_dpsi_corr, e_error, e_error_old, e_error_old2, e_error_coef;
+  int64_t max_ncoef; /* capacity of coef / old_coef; thetas and dpsi_corr hold 2*max_ncoef */
+  int64_t frac_size; /* fracture_dtype_hpc.itemsize */
+  int64_t f_id, f_t, f_radius, f_center, f_normal, f_x_vector, f_y_vector,
+      f_elements, f_nelements, f_constant;
+  int64_t max_elements; /* capacity of fracture.elements */
+} AndfnLayout;
+
+/* Solver fields of the reference's dtype_constants record
+ * (andfn/constants.py:13-29), as read at andfn/hpc/hpc_solve.py:81-86. */
+typedef struct AndfnConstants {
+  double max_error;       /* MAX_ERROR      */
+  int64_t max_iterations; /* MAX_ITERATIONS */
+  int64_t max_ncoef;      /* MAX_NCOEF (runtime cap on adaptive growth) */
+  double damping;         /* DAMPING        */
+  int64_t coef_increase;  /* COEF_INCREASE  */
+  double coef_ratio;      /* COEF_RATIO     */
+} AndfnConstants;
+
+/* What the reference only logs (andfn/hpc/hpc_solve.py:196-255), returned. */
+typedef struct AndfnSolveStats {
+  int64_t iterations;    /* nit at exit                                   */
+  int64_t cnt_error;     /* converged rounds seen (2 = converged)         */
+  double error;          /* max element error (truncation indicator)      */
+  double error_coef;     /* max element mean |delta coef|                 */
+  double error_q;        /* relative max |delta discharge| of last round  */
+  int64_t worst_element; /* argmax of error                               */
+  int64_t n_unknowns;    /* discharge-system size                         */
+  int64_t nnz_matrix;    /* discharge-system nonzeros                     */
+  int64_t nnz_factors;   /* nonzeros of L+U                               */
+  int64_t gpu_launches;  /* kernels this library launched for the solve   */
+  double ms_upload, ms_setup, ms_factor, ms_iterate, ms_download, ms_total;
+  int32_t status;        /* same as the return code                       */
+  int32_t device;        /* CUDA ordinal used                             */
+  int64_t h2d_bytes;     /* host->device bytes of andfn_b200_solve        */
+  int64_t d2h_bytes;     /* device->host bytes of andfn_b200_solve        */
+} AndfnSolveStats;
+
+/* ---- one-call drop-in (replaces andfn/hpc/hpc_solve.py:55 solve) --------
+ * frac_recs/elem_recs: host pointers to the structured arrays (C-contiguous).
+ * ntype_elements is ignored by the reference (andfn/hpc/hpc_solve.py:55-79)
+ * and is therefore not part of this signature.  stats may be NULL. */
+int andfn_b200_solve(void *frac_recs, int64_t nf, void *elem_recs, int64_t ne,
+                     const AndfnLayout *layout, int64_t discharge_int,
+                     const AndfnConstants *constants, AndfnSolveStats *stats);
+
+/* ---- handle API: keep a network resident in HBM across calls ------------ */
+typedef struct AndfnHandle AndfnHandle;
+
+/* Uploads the records, builds device tables.  device < 0 = current device. */
+int andfn_b200_create(AndfnHandle **out, const void *frac_recs, int64_t nf,
+                      const void *elem_recs, int64_t ne,
+                      const AndfnLayout *layout, int64_t discharge_int,
+                      int32_t device);
+/* Re-uploads coefficient/discharge state (warm start) from host records. */
+int andfn_b200_upload_state(AndfnHandle *h, const void *frac_recs,
+                            const void *elem_recs);
+/* Restores the state captured at create()/upload_state() on the device. */
+int andfn_b200_reset_state(AndfnHandle *h);
+/* Full solve on device-resident data (assembly, factorisation, iterations). */
+int andfn_b200_run(AndfnHandle *h, const AndfnConstants *constants,
+                   AndfnSolveStats *stats);
+/* Writes the solved fields back into host records in place. */
+int andfn_b200_download(AndfnHandle *h, void *frac_recs, void *elem_recs);
+/* Heads h = Re(Omega_f(z)) / t_f at npts points of fracture frac[i]
+ * (andfn/hpc/hpc_fracture.py:205-252).  z: complex128 [npts]; out: [npts]. */
+int andfn_b200_eval_heads(AndfnHandle *h, const int64_t *frac, const double *z,
+                          int64_t npts, double *out);
+/* Complex potential Omega_f(z) at npts points (andfn/hpc/hpc_fracture.py:52-94,
+ * exclude = -1).  out: complex128 [npts]. */
+int andfn_b200_eval_omega(AndfnHandle *h, const int64_t *frac, const double *z,
+                          int64_t npts, double *out);
+void andfn_b200_destroy(AndfnHandle *h);
+
+/* CUDA stream the handle launches on (cudaStream_t as void*). */
+void *andfn_b200_stream(AndfnHandle *h);
+
+/* Per-kernel device timing of the outer iterations (no reference
+ * counterpart; the reference only logs wall-clock phases,
+ * andfn/hpc/hpc_solve.py:109-122,149-215).  When on, run() records CUDA
+ * events around every kernel of every iteration; kernel_times() returns the
+ * accumulated milliseconds and launch counts per kernel class, in the order
+ * head-vector evaluation, triangular solve, sweep evaluation, element update,
+ * reduction (n >= 5).  Turning it on resets the accumulators. */
+int andfn_b200_set_profiling(AndfnHandle *h, int on);
+int andfn_b200_kernel_times(AndfnHandle *h, double *ms, int64_t *launches, int n);
+
+/* Measured FP64 FMA throughput of a device in TFLOP/s (the denominator of
+ * the evaluation kernels' roofline). */
+int andfn_b200_fp64_peak(int32_t device, double *tflops);
+
+/* Thread-local text of the last error. */
+const char *andfn_b200_last_error(void);
+/* Library version string. */
+const char *andfn_b200_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ANDFN_B200_H */
