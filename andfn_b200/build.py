@@ -15,7 +15,7 @@ SOURCES = [os.path.join(HERE, "csrc", f) for f in ("solver.cu", "sparse_lu.cpp")
 DEPS = SOURCES + [os.path.join(HERE, "csrc", f) for f in ("dmath.cuh", "sparse_lu.h")] + [
     os.path.join(os.path.dirname(HERE), "include", "andfn_b200.h")]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
-              "-Xcompiler", "-fPIC,-O3", "-shared", "-diag-suppress", "550"]
+              "-Xcompiler", "-fPIC,-O3,-fopenmp", "-shared", "-diag-suppress", "550", "-lgomp"]
 
 
 def nvcc() -> str:

@@ -37,7 +37,7 @@ namespace andfn {
 static constexpr double PI = 3.141592653589793115997963468544185161590576171875;
 static constexpr int EVAL_THREADS = 128;
 static constexpr int UPDATE_WARPS = 4;
-static constexpr int SOLVE_THREADS = 1024;
+static constexpr int SOLVE_THREADS = 512;
 static constexpr int ITER_BATCH = 4;  // iterations per graph launch
 
 enum GroupKind { KIND_PHI = 0, KIND_PSI = 1 };
@@ -328,7 +328,7 @@ __global__ void __launch_bounds__(UPDATE_WARPS * 32) update_kernel(Net net, cons
                                                                     const int *__restrict__ group_of,
                                                                     const Group *__restrict__ groups,
                                                                     const double *__restrict__ vals, int nvmax,
-                                                                    int single_blend) {
+                                                                    int blend_mode) {
   SolveState *st = net.st;
   if (st->done) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -433,12 +433,81 @@ __global__ void __launch_bounds__(UPDATE_WARPS * 32) update_kernel(Net net, cons
   }
   // damped blends (hpc_solve.py:383-388 and, for nit >= 2, 561-575)
   const double d = st->damping;
-  const int nb = single_blend ? 1 : ((st->fused_blend2 && st->nit >= 2) ? 2 : 1);
+  const int nb = (blend_mode == 2) ? 0 : (blend_mode == 1 ? 1 : ((st->fused_blend2 && st->nit >= 2) ? 2 : 1));
   cd *cc = net.coef + (size_t)e * MC;
   for (int j = lane; j < m; j += 32) {
     cd w = neww[j], c = cc[j];
     for (int b = 0; b < nb; b++) c = mk(d * w.re + (1 - d) * c.re, d * w.im + (1 - d) * c.im);
     cc[j] = c;
+  }
+}
+
+// ------------------------------------------------------------------------
+// Adaptive coefficient growth (element_solver2, hpc_solve.py:465-559): after
+// the first blend, an element whose tail coefficients are large relative to
+// the rest, or whose error rose three times in a row, gets COEF_INCREASE more
+// coefficients and nint = 2 ncoef, at most once per iteration.  The decision
+// uses the reference's operation order (sequential complex sums, Smith
+// division, hypot) on the blended coefficients.  One warp per element; the
+// grown elements are appended to grow_list.
+// ------------------------------------------------------------------------
+__global__ void growth_kernel(Net net, const int *__restrict__ elist, int nlist, double max_coef_ratio,
+                              int max_coef, int coef_increase, int *grow_list, int *grow_count) {
+  const SolveState *st = net.st;
+  if (st->done) return;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (warp >= nlist || lane != 0) return;
+  const int e = elist[warp];
+  if (net.type[e] == 2) return;
+  const int nit = st->nit;
+  if (nit < 2) return;
+  const int m = net.ncoef[e];
+  const cd *c = net.coef + (size_t)e * net.MC;
+  const int ncc = 3;
+  double s = 0.0;
+  int cnt = 0;
+  for (int k = 1; k < min(ncc, m); k++) {
+    s += hypot(c[k].re, c[k].im);
+    cnt++;
+  }
+  const double coef0 = (cnt > 0 ? s / cnt : NAN) + 1e-30;
+  double coef1 = -INFINITY;
+  for (int k = max(0, m - ncc); k < m; k++) {
+    const double v = hypot(c[k].re, c[k].im);
+    if (v != v) {
+      coef1 = v;
+      break;
+    }
+    if (v > coef1) coef1 = v;
+  }
+  double ratio = (coef0 == 0.0) ? 0.0 : coef1 / coef0 * 0;
+  if (m > 1 && hypot(c[1].re, c[1].im) < st->max_error / 1e10) ratio = 0.0;
+  const double err = net.err[e], eo = net.err_old[e], eo2 = net.err_old2[e];
+  if (err > eo && err > eo2 && err > st->max_error && nit > 5) ratio = max_coef_ratio + 1.0;
+  cd sl = mk(0.0, 0.0), sr = mk(0.0, 0.0);
+  for (int k = max(0, m - ncc); k < m; k++) sl = mk(sl.re + c[k].re, sl.im + c[k].im);
+  for (int k = 0; k < max(0, m - ncc); k++) sr = mk(sr.re + c[k].re, sr.im + c[k].im);
+  const cd qt = cdiv_ref(sl, mk(sr.re + 1e-30, sr.im + 0.0));
+  if (hypot(qt.re, qt.im) > max_coef_ratio && err > st->max_error) ratio = max_coef_ratio + 1.0;
+  if (ratio > max_coef_ratio && m < max_coef && nit > 1) {
+    net.ncoef[e] = m + coef_increase;
+    net.nint[e] = (m + coef_increase) * 2;
+    const int slot = atomicAdd(grow_count, 1);
+    grow_list[slot] = e;
+  }
+}
+
+// Second damped blend of element_solver2 (hpc_solve.py:561-575), nit >= 2.
+__global__ void blend2_kernel(Net net) {
+  const SolveState *st = net.st;
+  if (st->done || st->nit < 2) return;
+  const double d = st->damping;
+  const long long tot = (long long)net.ne * net.MC;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < tot; i += (long long)gridDim.x * blockDim.x) {
+    const int e = (int)(i / net.MC), j = (int)(i - (long long)e * net.MC);
+    if (j >= net.ncoef[e]) continue;
+    const cd w = net.wcoef[i], c = net.coef[i];
+    net.coef[i] = mk(d * w.re + (1 - d) * c.re, d * w.im + (1 - d) * c.im);
   }
 }
 
@@ -542,8 +611,9 @@ struct LevelSolve {
   const int *eptr;      // [N + 1] entry range of each slot
   const int *col;       // entries: column (pivot-step index)
   const double *val;    // entries: value
-  const double *scale;  // [N] per-slot multiplier (1/U(i,i)) or null
+  const double *scale;  // [nslots] per-slot multiplier (1/U(i,i)) or null
   int nlev;
+  int nslots;           // rows in this solve (rows[] has nslots, eptr[] nslots + 1 entries)
 };
 
 static constexpr int PF = 4;  // factor entries per lane kept in registers
@@ -552,17 +622,25 @@ struct RowRegs {
   int row, beg, end;
   int c[PF];
   double v[PF];
+  double scale;
 };
 
-__device__ __forceinline__ void load_row(RowRegs &r, const LevelSolve &F, int slot, int lane) {
-  r.row = F.rows[slot];
-  r.beg = F.eptr[slot];
-  r.end = F.eptr[slot + 1];
+// Slot metadata (row solved in a slot and its entry range) comes from shared
+// memory when it fits, so a prefetch costs one global round trip.
+struct SlotMeta {
+  const int *rows, *eptr;
+};
+
+__device__ __forceinline__ void load_row(RowRegs &r, const LevelSolve &F, const SlotMeta &M, int slot, int lane) {
+  r.row = M.rows[slot];
+  r.beg = M.eptr[slot];
+  r.end = M.eptr[slot + 1];
+  r.scale = F.scale ? __ldg(F.scale + slot) : 1.0;
 #pragma unroll
   for (int k = 0; k < PF; k++) {
     const int p = r.beg + lane + 32 * k;
-    r.c[k] = (p < r.end) ? F.col[p] : 0;
-    r.v[k] = (p < r.end) ? F.val[p] : 0.0;
+    r.c[k] = (p < r.end) ? __ldg(F.col + p) : 0;
+    r.v[k] = (p < r.end) ? __ldg(F.val + p) : 0.0;
   }
 }
 
@@ -570,61 +648,161 @@ __device__ __forceinline__ void solve_row(const RowRegs &r, const LevelSolve &F,
   double s = 0.0;
 #pragma unroll
   for (int k = 0; k < PF; k++) s = fma(r.v[k], y[r.c[k]], s);
-  for (int p = r.beg + 32 * PF + lane; p < r.end; p += 32) s = fma(F.val[p], y[F.col[p]], s);
-  s = warp_sum(s);
-  if (lane == 0) {
-    double v = y[r.row] - s;
-    if (F.scale) v *= F.scale[slot];
-    y[r.row] = v;
+  int p = r.beg + 32 * PF + lane;
+  for (; p + 96 < r.end; p += 128) {  // long rows: four independent loads in flight
+    const double v0 = __ldg(F.val + p), v1 = __ldg(F.val + p + 32), v2 = __ldg(F.val + p + 64),
+                 v3 = __ldg(F.val + p + 96);
+    const int c0 = __ldg(F.col + p), c1 = __ldg(F.col + p + 32), c2 = __ldg(F.col + p + 64),
+              c3 = __ldg(F.col + p + 96);
+    s = fma(v0, y[c0], s);
+    s = fma(v1, y[c1], s);
+    s = fma(v2, y[c2], s);
+    s = fma(v3, y[c3], s);
   }
+  for (; p < r.end; p += 32) s = fma(__ldg(F.val + p), y[__ldg(F.col + p)], s);
+  s = warp_sum(s);
+  if (lane == 0) y[r.row] = (y[r.row] - s) * r.scale;
 }
 
 // One triangular solve, level by level with a block barrier between levels.
-// The first row of the next level is loaded into registers before the
-// barrier, so its global-memory latency overlaps the wait.
-__device__ void level_solve(const LevelSolve &F, double *y, int *s_levptr, int cap_levptr) {
+// Each warp keeps the factor row of its first slot of the next two levels in
+// registers (loads issued two levels ahead), so the global-memory latency
+// overlaps two barrier waits.  s_meta holds (row, entry start) per slot when
+// there is room (meta_cap >= N + 1 ints each).
+__device__ void level_solve(const LevelSolve &F, double *y, int *s_levptr, int cap_levptr, int *s_meta,
+                            int meta_cap) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   const bool lev_in_smem = F.nlev + 1 <= cap_levptr;
+  const bool meta_in_smem = F.nslots + 1 <= meta_cap;
+  __syncthreads();
   if (lev_in_smem)
     for (int i = threadIdx.x; i <= F.nlev; i += blockDim.x) s_levptr[i] = F.lev_ptr[i];
+  if (meta_in_smem) {
+    for (int i = threadIdx.x; i < F.nslots; i += blockDim.x) s_meta[i] = F.rows[i];
+    for (int i = threadIdx.x; i <= F.nslots; i += blockDim.x) s_meta[meta_cap + i] = F.eptr[i];
+  }
   __syncthreads();
   const int *lp = lev_in_smem ? s_levptr : F.lev_ptr;
-  RowRegs cur;
-  bool have = false;
+  SlotMeta M{meta_in_smem ? s_meta : F.rows, meta_in_smem ? s_meta + meta_cap : F.eptr};
+  RowRegs a, b;
+  bool ha = false, hb = false;
   if (F.nlev > 0 && lp[0] + warp < lp[1]) {
-    load_row(cur, F, lp[0] + warp, lane);
-    have = true;
+    load_row(a, F, M, lp[0] + warp, lane);
+    ha = true;
+  }
+  if (F.nlev > 1 && lp[1] + warp < lp[2]) {
+    load_row(b, F, M, lp[1] + warp, lane);
+    hb = true;
   }
   for (int l = 0; l < F.nlev; l++) {
     const int r0 = lp[l], r1 = lp[l + 1];
-    if (have) solve_row(cur, F, r0 + warp, lane, y);
+    if (ha) solve_row(a, F, r0 + warp, lane, y);
     for (int slot = r0 + warp + nw; slot < r1; slot += nw) {
       RowRegs t;
-      load_row(t, F, slot, lane);
+      load_row(t, F, M, slot, lane);
       solve_row(t, F, slot, lane, y);
     }
-    have = false;
-    if (l + 1 < F.nlev) {
-      const int n0 = r1, n1 = lp[l + 2];
+    a = b;
+    ha = hb;
+    hb = false;
+    if (l + 2 < F.nlev) {
+      const int n0 = lp[l + 2], n1 = lp[l + 3];
       if (n0 + warp < n1) {
-        load_row(cur, F, n0 + warp, lane);
-        have = true;
+        load_row(b, F, M, n0 + warp, lane);
+        hb = true;
       }
     }
     __syncthreads();
   }
 }
 
+// Dense trailing block of the factors (the last K pivot steps, where the LU
+// of a minimum-degree order fills in): column-major K x K, solved in panels of
+// 32 rows.  One warp solves the panel's triangle with its 32 rows in
+// registers (shuffle broadcast of each solved value), then the whole CTA
+// updates the rows below (lower) / above (upper) with coalesced column reads.
+__device__ void dense_lower_solve(const double *__restrict__ Lcm, int K, double *y) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int r0 = 0; r0 < K; r0 += 32) {
+    const int nb = min(32, K - r0);
+    if (warp == 0) {
+      double row[32];
+#pragma unroll
+      for (int j = 0; j < 32; j++)
+        row[j] = (lane < nb && j < lane) ? __ldg(Lcm + (size_t)(r0 + j) * K + r0 + lane) : 0.0;
+      double yi = (lane < nb) ? y[r0 + lane] : 0.0;
+#pragma unroll
+      for (int j = 0; j < 32; j++) {
+        const double yj = __shfl_sync(0xffffffffu, yi, j);
+        if (lane > j) yi = fma(-row[j], yj, yi);
+      }
+      if (lane < nb) y[r0 + lane] = yi;
+    }
+    __syncthreads();
+    for (int i = r0 + nb + threadIdx.x; i < K; i += blockDim.x) {
+      double acc = 0.0;
+      const double *col = Lcm + (size_t)r0 * K + i;
+#pragma unroll 8
+      for (int j = 0; j < nb; j++) acc = fma(__ldg(col + (size_t)j * K), y[r0 + j], acc);
+      y[i] -= acc;
+    }
+    __syncthreads();
+  }
+}
+
+__device__ void dense_upper_solve(const double *__restrict__ Ucm, const double *__restrict__ uinv, int K, double *y) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int npan = (K + 31) / 32;
+  for (int pi = npan - 1; pi >= 0; pi--) {
+    const int r0 = pi * 32;
+    const int nb = min(32, K - r0);
+    if (warp == 0) {
+      double row[32];
+#pragma unroll
+      for (int j = 0; j < 32; j++)
+        row[j] = (lane < nb && j > lane && j < nb) ? __ldg(Ucm + (size_t)(r0 + j) * K + r0 + lane) : 0.0;
+      const double di = (lane < nb) ? __ldg(uinv + r0 + lane) : 0.0;
+      double yi = (lane < nb) ? y[r0 + lane] : 0.0;
+#pragma unroll
+      for (int j = 31; j >= 0; j--) {
+        if (lane == j) yi *= di;
+        const double xj = __shfl_sync(0xffffffffu, yi, j);
+        if (lane < j) yi = fma(-row[j], xj, yi);
+      }
+      if (lane < nb) y[r0 + lane] = yi;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < r0; i += blockDim.x) {
+      double acc = 0.0;
+      const double *col = Ucm + (size_t)r0 * K + i;
+#pragma unroll 8
+      for (int j = 0; j < nb; j++) acc = fma(__ldg(col + (size_t)j * K), y[r0 + j], acc);
+      y[i] -= acc;
+    }
+    __syncthreads();
+  }
+}
+
+struct DenseTail {
+  int K;               // trailing block size (0 = none)
+  const double *L;     // K x K column-major, strictly lower part
+  const double *U;     // K x K column-major, strictly upper part
+  const double *uinv;  // [K] 1 / U(i,i)
+};
+
 __global__ void __launch_bounds__(SOLVE_THREADS) trisolve_kernel(Net net, const double *__restrict__ rhs_vals,
                                                                   const int *__restrict__ rhs_group,
                                                                   const Group *__restrict__ groups, int use_smem,
-                                                                  LevelSolve Lf, LevelSolve Ub, int cap_levptr) {
+                                                                  LevelSolve Lf, LevelSolve Lx, LevelSolve Ux,
+                                                                  LevelSolve Ub, DenseTail T, int cap_levptr,
+                                                                  int meta_cap) {
   SolveState *st = net.st;
   if (st->done) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int N = net.N, n_de = net.n_de, D = net.D;
   double *y = use_smem ? reinterpret_cast<double *>(smem_raw) : net.work;
   int *s_levptr = reinterpret_cast<int *>(smem_raw + (use_smem ? sizeof(double) * (size_t)N : 0));
+  int *s_meta = s_levptr + cap_levptr;
   if (threadIdx.x == 0) st->nit += 1;
   if (!st->solve_q) return;  // uniform: solve_q is written only by reduce_kernel
   // b = head vector (hpc_solve.py:811-829); y = P b
@@ -648,8 +826,16 @@ __global__ void __launch_bounds__(SOLVE_THREADS) trisolve_kernel(Net net, const 
     y[net.pinv[r]] = b;
   }
   __syncthreads();
-  level_solve(Lf, y, s_levptr, cap_levptr);  // L unit lower
-  level_solve(Ub, y, s_levptr, cap_levptr);  // U upper, scale = 1/U(i,i)
+  // L: sparse leading rows, coupling of the trailing rows to them, dense tail
+  level_solve(Lf, y, s_levptr, cap_levptr, s_meta, meta_cap);
+  if (T.K > 0) {
+    level_solve(Lx, y, s_levptr, cap_levptr, s_meta, meta_cap);
+    dense_lower_solve(T.L, T.K, y + (N - T.K));
+    // U: dense tail, coupling of the leading rows to it, sparse leading rows
+    dense_upper_solve(T.U, T.uinv, T.K, y + (N - T.K));
+    level_solve(Ux, y, s_levptr, cap_levptr, s_meta, meta_cap);
+  }
+  level_solve(Ub, y, s_levptr, cap_levptr, s_meta, meta_cap);  // scale = 1/U(i,i)
   // x = Q y; error_q = max|x - x_old| / (max|x_old| + 1e-16) (hpc_solve.py:169-174)
   __shared__ double s_d[32], s_o[32];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
@@ -1006,22 +1192,28 @@ static void set_error(const std::string &s) { g_last_error = s; }
     }                                                                                               \
   } while (0)
 
+// Device buffer that keeps its allocation when it is re-filled with no more
+// elements than it holds (cudaFree synchronises the device, so repeated
+// solves on one handle should not reallocate).
 template <class T>
 struct DBuf {
   T *p = nullptr;
-  size_t n = 0;
+  size_t n = 0, cap = 0;
   cudaError_t alloc(size_t count) {
-    free();
+    n = count;
+    if (count <= cap && p) return cudaSuccess;
+    release();
     n = count;
     if (count == 0) return cudaSuccess;
+    cap = count;
     return cudaMalloc(&p, sizeof(T) * count);
   }
-  void free() {
+  void release() {
     if (p) cudaFree(p);
     p = nullptr;
-    n = 0;
+    n = cap = 0;
   }
-  ~DBuf() { free(); }
+  ~DBuf() { release(); }
 };
 
 struct HostNet {
@@ -1063,6 +1255,7 @@ struct AndfnHandle {
   DBuf<int> d_ent_row, d_ent_src, d_ent_side, d_ent_kind;
   DBuf<double> d_mvals;
   std::vector<int> colorder;  // cached symbolic analysis (depends on the pattern only)
+  int dense_k = 0;            // trailing pivot steps factorised and solved as a dense block
   DBuf<int> pinv, qcol, l_ptr, l_col, u_ptr, u_col;
   DBuf<double> l_val, u_val, u_inv, disc, work;
   DBuf<int> ready;
@@ -1070,6 +1263,11 @@ struct AndfnHandle {
   DBuf<int> lf_lev, lf_rows, lf_eptr, lf_col, ub_lev, ub_rows, ub_eptr, ub_col;
   DBuf<double> lf_val, ub_val, ub_scale;
   int lf_nlev = 0, ub_nlev = 0;
+  DBuf<int> lx_lev, lx_rows, lx_eptr, lx_col, ux_lev, ux_rows, ux_eptr, ux_col;
+  DBuf<double> lx_val, ux_val;
+  int lx_nlev = 0, ux_nlev = 0;
+  int tail_k = 0;
+  DBuf<double> tail_l, tail_u, tail_uinv;
   int64_t nnz_factors = 0;
   // evaluation tables
   std::vector<Group> groups;
@@ -1083,6 +1281,15 @@ struct AndfnHandle {
   DBuf<int> upd_list, psi_list;
   int n_upd = 0, n_psi = 0;
   int nvmax = 0;
+  // current ncoef / nint the tables were built for (they change with adaptive growth)
+  std::vector<int> cur_ncoef, cur_nint;
+  bool tables_dirty = false;
+  // re-solve tables of the elements grown in one iteration
+  DBuf<Group> rs_groups;
+  DBuf<Item> rs_items;
+  DBuf<int2> rs_pts;
+  DBuf<int> rs_group_of, rs_list, grow_list, grow_count;
+  DBuf<double> rs_vals;
   int chunk = 0;
   size_t eval_smem = 0;
   DBuf<SolveState> st;
@@ -1320,8 +1527,11 @@ static cudaError_t upload(DBuf<T> &d, const std::vector<T> &v, cudaStream_t s) {
 
 // Evaluation tables: groups, flattened points and tiles per fracture.
 static void build_tables(AndfnHandle *H, bool rhs, std::vector<Group> &groups, std::vector<int> &index_of,
-                         std::vector<Item> &items, std::vector<int2> &pts, int &nvals) {
+                         std::vector<Item> &items, std::vector<int2> &pts, int &nvals,
+                         const std::vector<char> *only = nullptr) {
   const HostNet &h = H->h;
+  const std::vector<int> &cnint = H->cur_nint;
+  const std::vector<int> &cncoef = H->cur_ncoef;
   const int ne = (int)H->ne, nf = (int)H->nf;
   const int D = (int)H->D;
   const int n_de = (int)h.de_ids.size();
@@ -1333,13 +1543,14 @@ static void build_tables(AndfnHandle *H, bool rhs, std::vector<Group> &groups, s
     for (int e = 0; e < ne; e++) {
       const int ty = h.type[e];
       if (ty == 2) continue;
+      if (only && !(*only)[e]) continue;
       const int sides = (ty == 0) ? 2 : 1;
       for (int s = 0; s < sides; s++) {
         Group g;
         g.elem = e;
         g.side = s;
         g.frac = s ? h.frac1[e] : h.frac0[e];
-        g.npts = h.nint[e];
+        g.npts = cnint[e];
         g.kind = (ty == 1 || ty == 4 || ty == 5) ? KIND_PSI : KIND_PHI;
         g.out = nvals;
         g.pad0 = g.pad1 = 0;
@@ -1385,7 +1596,7 @@ static void build_tables(AndfnHandle *H, bool rhs, std::vector<Group> &groups, s
       for (int k = 0; k < groups[gi].npts; k++) pts.push_back(make_int2(gi, k));
     const int end = (int)pts.size();
     double work_per_pt = 0.0;
-    for (int k = h.fptr[f]; k < h.fptr[f + 1]; k++) work_per_pt += 30.0 + 4.0 * h.ncoef[h.felem[k]];
+    for (int k = h.fptr[f]; k < h.fptr[f + 1]; k++) work_per_pt += 30.0 + 4.0 * cncoef[h.felem[k]];
     for (int p = start; p < end; p += EVAL_THREADS) {
       Item it;
       it.frac = f;
@@ -1454,6 +1665,74 @@ static void build_pattern(AndfnHandle *H) {
 
 static int reset_impl(AndfnHandle *H);
 
+// Sweep / head-vector tables for the current ncoef and nint, uploaded.
+static int build_eval_tables(AndfnHandle *H) {
+  HostNet &h = H->h;
+  cudaStream_t s = H->stream;
+  const int ne = (int)H->ne;
+  std::vector<Group> groups;
+  std::vector<int> group_of, rhs_group;
+  std::vector<Item> sitems, ritems;
+  std::vector<int2> spts, rpts;
+  int nsv = 0, nrv = 0;
+  build_tables(H, false, groups, group_of, sitems, spts, nsv);
+  build_tables(H, true, groups, rhs_group, ritems, rpts, nrv);
+  H->groups = groups;
+  CK(upload(H->d_groups, groups, s));
+  CK(upload(H->group_of, group_of, s));
+  CK(upload(H->rhs_group, rhs_group, s));
+  CK(upload(H->sweep_items, sitems, s));
+  CK(upload(H->rhs_items, ritems, s));
+  CK(upload(H->sweep_pts, spts, s));
+  CK(upload(H->rhs_pts, rpts, s));
+  H->n_sweep_items = (int)sitems.size();
+  H->n_rhs_items = (int)ritems.size();
+  if (H->sweep_vals.cap < (size_t)std::max(1, nsv)) CK(H->sweep_vals.alloc(std::max(1, nsv)));
+  if (H->rhs_vals.cap < (size_t)std::max(1, nrv)) CK(H->rhs_vals.alloc(std::max(1, nrv)));
+  std::vector<int> upd, psi;
+  int nvmax = 2;
+  for (int e = 0; e < ne; e++) {
+    upd.push_back(e);
+    if (h.type[e] == 1 || h.type[e] == 4 || h.type[e] == 5) psi.push_back(e);
+    nvmax = std::max(nvmax, H->cur_nint[e]);
+  }
+  H->n_upd = (int)upd.size();
+  H->n_psi = (int)psi.size();
+  H->nvmax = nvmax;
+  CK(upload(H->upd_list, upd, s));
+  CK(upload(H->psi_list, psi, s));
+  // eval staging: sources per chunk within the shared-memory budget
+  int maxnf = 1;
+  for (int f = 0; f < (int)H->nf; f++) maxnf = std::max(maxnf, h.fptr[f + 1] - h.fptr[f]);
+  const size_t budget = 96 * 1024;
+  int chunk = (int)(budget / (sizeof(Src) + sizeof(cd) * H->MC));
+  chunk = std::max(1, std::min(chunk, maxnf));
+  H->chunk = chunk;
+  H->eval_smem = (sizeof(Src) + sizeof(cd) * H->MC) * chunk;
+  CK(cudaStreamSynchronize(s));
+  H->tables_dirty = false;
+  return 0;
+}
+
+// Coefficient capacity per element on the device (>= the largest ncoef the
+// run can reach); re-strides the stored initial coefficients when it grows.
+static int ensure_capacity(AndfnHandle *H, int mc) {
+  if (mc <= H->MC) return 0;
+  const int old = H->MC;
+  std::vector<cd> nc((size_t)H->ne * mc, mk(0.0, 0.0));
+  for (int64_t i = 0; i < H->ne; i++)
+    for (int k = 0; k < old; k++) nc[(size_t)i * mc + k] = H->h.coef[(size_t)i * old + k];
+  H->h.coef.swap(nc);
+  H->MC = mc;
+  cudaStream_t s = H->stream;
+  CK(upload(H->coef0, H->h.coef, s));
+  CK(H->coef.alloc((size_t)H->ne * mc));
+  CK(H->wcoef.alloc((size_t)H->ne * mc));
+  CK(H->dpsi_corr.alloc((size_t)H->ne * 2 * mc));
+  H->tables_dirty = true;
+  return 0;
+}
+
 static int create_impl(AndfnHandle *H, const char *F, const char *E) {
   int rc = parse_records(H, F, E);
   if (rc) return rc;
@@ -1512,46 +1791,10 @@ static int create_impl(AndfnHandle *H, const char *F, const char *E) {
   CK(H->cut_pos.alloc((size_t)ne * H->cut_cap));
   CK(H->cut_elem.alloc((size_t)ne * H->cut_cap));
   CK(H->cut_sign.alloc((size_t)ne * H->cut_cap));
-  // tables
-  std::vector<Group> groups;
-  std::vector<int> group_of, rhs_group;
-  std::vector<Item> sitems, ritems;
-  std::vector<int2> spts, rpts;
-  int nsv = 0, nrv = 0;
-  build_tables(H, false, groups, group_of, sitems, spts, nsv);
-  build_tables(H, true, groups, rhs_group, ritems, rpts, nrv);
-  H->groups = groups;
-  CK(upload(H->d_groups, groups, s));
-  CK(upload(H->group_of, group_of, s));
-  CK(upload(H->rhs_group, rhs_group, s));
-  CK(upload(H->sweep_items, sitems, s));
-  CK(upload(H->rhs_items, ritems, s));
-  CK(upload(H->sweep_pts, spts, s));
-  CK(upload(H->rhs_pts, rpts, s));
-  H->n_sweep_items = (int)sitems.size();
-  H->n_rhs_items = (int)ritems.size();
-  CK(H->sweep_vals.alloc(std::max(1, nsv)));
-  CK(H->rhs_vals.alloc(std::max(1, nrv)));
-  std::vector<int> upd, psi;
-  int nvmax = 2;
-  for (int e = 0; e < ne; e++) {
-    upd.push_back(e);
-    if (h.type[e] == 1 || h.type[e] == 4 || h.type[e] == 5) psi.push_back(e);
-    nvmax = std::max(nvmax, h.nint[e]);
-  }
-  H->n_upd = (int)upd.size();
-  H->n_psi = (int)psi.size();
-  H->nvmax = nvmax;
-  CK(upload(H->upd_list, upd, s));
-  CK(upload(H->psi_list, psi, s));
-  // eval staging: sources per chunk within the shared-memory budget
-  int maxnf = 1;
-  for (int f = 0; f < (int)H->nf; f++) maxnf = std::max(maxnf, h.fptr[f + 1] - h.fptr[f]);
-  const size_t budget = 96 * 1024;
-  int chunk = (int)(budget / (sizeof(Src) + sizeof(cd) * H->MC));
-  chunk = std::max(1, std::min(chunk, maxnf));
-  H->chunk = chunk;
-  H->eval_smem = (sizeof(Src) + sizeof(cd) * H->MC) * chunk;
+  H->cur_ncoef = h.ncoef;
+  H->cur_nint = h.nint;
+  rc = build_eval_tables(H);
+  if (rc) return rc;
   // discharge system
   build_pattern(H);
   CK(upload(H->d_ent_row, H->ent_row, s));
@@ -1572,7 +1815,7 @@ static int create_impl(AndfnHandle *H, const char *F, const char *E) {
     std::vector<int> fill(P.colptr.begin(), P.colptr.end() - 1);
     for (int r = 0; r < H->N; r++)
       for (int p = H->mrow_ptr[r]; p < H->mrow_ptr[r + 1]; p++) P.rowind[fill[H->mcol[p]]++] = r;
-    H->colorder = column_min_degree_order(P);
+    H->colorder = column_min_degree_order(P, &H->dense_k);
   }
   CK(H->disc.alloc(H->N));
   CK(H->work.alloc(H->N));
@@ -1610,43 +1853,75 @@ static double ms_since(std::chrono::steady_clock::time_point t0) {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
 
-// Groups the rows of a triangular factor by dependency level and stores their
-// entries in that order (level_solve reads one contiguous range per level).
+// Groups rows [row_lo, row_hi) of a triangular factor by dependency level and
+// stores their entries with columns in [col_lo, col_hi) in that order
+// (level_solve reads one contiguous range per level).  single_level puts all
+// rows in one level (the coupling terms between the sparse part and the dense
+// tail, whose rows are independent).
 static void build_levels(int n, const std::vector<int> &ptr, const std::vector<int> &col,
-                         const std::vector<double> &val, const std::vector<double> *scale, bool lower,
-                         std::vector<int> &lev_ptr, std::vector<int> &rows, std::vector<int> &eptr,
-                         std::vector<int> &ecol, std::vector<double> &evals, std::vector<double> &escale) {
-  std::vector<int> lev(n, 0);
-  int nlev = 0;
-  for (int t = 0; t < n; t++) {
-    const int i = lower ? t : n - 1 - t;
-    int l = 0;
-    for (int p = ptr[i]; p < ptr[i + 1]; p++) l = std::max(l, lev[col[p]] + 1);
-    lev[i] = l;
-    nlev = std::max(nlev, l + 1);
+                         const std::vector<double> &val, const std::vector<double> *scale, bool lower, int row_lo,
+                         int row_hi, int col_lo, int col_hi, bool single_level, std::vector<int> &lev_ptr,
+                         std::vector<int> &rows, std::vector<int> &eptr, std::vector<int> &ecol,
+                         std::vector<double> &evals, std::vector<double> &escale) {
+  (void)n;
+  const int nr = std::max(0, row_hi - row_lo);
+  std::vector<int> lev(std::max(1, row_hi), 0);
+  int nlev = nr > 0 ? 1 : 0;
+  if (!single_level) {
+    for (int t = 0; t < nr; t++) {
+      const int i = lower ? row_lo + t : row_hi - 1 - t;
+      int l = 0;
+      for (int p = ptr[i]; p < ptr[i + 1]; p++) {
+        const int c = col[p];
+        if (c >= col_lo && c < col_hi && c >= row_lo && c < row_hi) l = std::max(l, lev[c] + 1);
+      }
+      lev[i] = l;
+      nlev = std::max(nlev, l + 1);
+    }
   }
   lev_ptr.assign(nlev + 1, 0);
-  for (int i = 0; i < n; i++) lev_ptr[lev[i] + 1]++;
+  for (int i = row_lo; i < row_hi; i++) lev_ptr[lev[i] + 1]++;
   for (int l = 0; l < nlev; l++) lev_ptr[l + 1] += lev_ptr[l];
-  rows.assign(n, 0);
+  rows.assign(nr, 0);
   std::vector<int> fill(lev_ptr.begin(), lev_ptr.end() - 1);
-  for (int t = 0; t < n; t++) {
-    const int i = lower ? t : n - 1 - t;
+  for (int t = 0; t < nr; t++) {
+    const int i = lower ? row_lo + t : row_hi - 1 - t;
     rows[fill[lev[i]]++] = i;
   }
-  eptr.assign(n + 1, 0);
+  eptr.assign(nr + 1, 0);
   ecol.clear();
   evals.clear();
-  escale.assign(n, 1.0);
-  for (int sl = 0; sl < n; sl++) {
+  escale.assign(nr, 1.0);
+  for (int sl = 0; sl < nr; sl++) {
     const int i = rows[sl];
     for (int p = ptr[i]; p < ptr[i + 1]; p++) {
+      if (col[p] < col_lo || col[p] >= col_hi) continue;
       ecol.push_back(col[p]);
       evals.push_back(val[p]);
     }
     eptr[sl + 1] = (int)ecol.size();
     if (scale) escale[sl] = (*scale)[i];
   }
+}
+
+static void launch_trisolve(AndfnHandle *H, cudaStream_t s) {
+  Net net = H->net();
+  const int m0 = H->N - H->tail_k;
+  LevelSolve Lf{H->lf_lev.p, H->lf_rows.p, H->lf_eptr.p, H->lf_col.p, H->lf_val.p, nullptr, H->lf_nlev, m0};
+  LevelSolve Ub{H->ub_lev.p, H->ub_rows.p, H->ub_eptr.p, H->ub_col.p, H->ub_val.p, H->ub_scale.p, H->ub_nlev, m0};
+  LevelSolve Lx{H->lx_lev.p, H->lx_rows.p, H->lx_eptr.p, H->lx_col.p, H->lx_val.p, nullptr, H->lx_nlev, H->tail_k};
+  LevelSolve Ux{H->ux_lev.p, H->ux_rows.p, H->ux_eptr.p, H->ux_col.p, H->ux_val.p, nullptr, H->ux_nlev, m0};
+  DenseTail T{H->tail_k, H->tail_l.p, H->tail_u.p, H->tail_uinv.p};
+  const size_t ybytes = sizeof(double) * (size_t)H->N;
+  const int use_smem = ybytes <= 150 * 1024;
+  const size_t lev_bytes = sizeof(int) * (size_t)(std::max(std::max(H->lf_nlev, H->ub_nlev), 1) + 1);
+  const int cap_levptr = (int)std::min<size_t>(lev_bytes, 40 * 1024) / (int)sizeof(int);
+  size_t solve_smem = (use_smem ? ybytes : 0) + sizeof(int) * (size_t)cap_levptr;
+  const size_t meta_bytes = sizeof(int) * 2 * ((size_t)H->N + 1);
+  const int meta_cap = (solve_smem + meta_bytes <= 200 * 1024) ? H->N + 1 : 0;
+  if (meta_cap) solve_smem += meta_bytes;
+  trisolve_kernel<<<1, H->solve_threads, solve_smem, s>>>(net, H->rhs_vals.p, H->rhs_group.p, H->d_groups.p,
+                                                          use_smem, Lf, Lx, Ux, Ub, T, cap_levptr, meta_cap);
 }
 
 static inline void mark(AndfnHandle *H, cudaStream_t s, int b, int c, int w) {
@@ -1661,16 +1936,8 @@ static int enqueue_iteration(AndfnHandle *H, cudaStream_t s, int single_blend_sw
                                                                           H->d_groups.p, H->rhs_vals.p, H->chunk);
   }
   mark(H, s, b, K_RHS, 1);
-  LevelSolve Lf{H->lf_lev.p, H->lf_rows.p, H->lf_eptr.p, H->lf_col.p, H->lf_val.p, nullptr, H->lf_nlev};
-  LevelSolve Ub{H->ub_lev.p, H->ub_rows.p, H->ub_eptr.p, H->ub_col.p, H->ub_val.p, H->ub_scale.p, H->ub_nlev};
-  const size_t ybytes = sizeof(double) * (size_t)H->N;
-  const int use_smem = ybytes <= 150 * 1024;
-  const size_t lev_bytes = sizeof(int) * (size_t)(std::max(H->lf_nlev, H->ub_nlev) + 1);
-  const int cap_levptr = (int)std::min<size_t>(lev_bytes, 40 * 1024) / (int)sizeof(int);
-  const size_t solve_smem = (use_smem ? ybytes : 0) + sizeof(int) * (size_t)cap_levptr;
   mark(H, s, b, K_TRISOLVE, 0);
-  trisolve_kernel<<<1, H->solve_threads, solve_smem, s>>>(net, H->rhs_vals.p, H->rhs_group.p, H->d_groups.p,
-                                                          use_smem, Lf, Ub, cap_levptr);
+  launch_trisolve(H, s);
   mark(H, s, b, K_TRISOLVE, 1);
   mark(H, s, b, K_SWEEP, 0);
   if (H->n_sweep_items > 0)
@@ -1691,6 +1958,93 @@ static int enqueue_iteration(AndfnHandle *H, cudaStream_t s, int single_blend_sw
   return 0;
 }
 
+// One outer iteration at a time with the coefficient growth of
+// element_solver2 between the two blends (hpc_solve.py:394-591).
+static int run_adaptive(AndfnHandle *H, const AndfnConstants *C) {
+  cudaStream_t s = H->stream;
+  const int ne = (int)H->ne;
+  if (H->grow_list.cap < (size_t)ne) CK(H->grow_list.alloc(ne));
+  if (H->grow_count.cap < 1) CK(H->grow_count.alloc(1));
+  int guard = 0;
+  while (true) {
+    Net net = H->net();
+    // head vector, discharge solve, sweep, fit + first blend (no fused second blend)
+    if (H->n_rhs_items > 0)
+      eval_kernel<true><<<H->n_rhs_items, EVAL_THREADS, H->eval_smem, s>>>(net, H->rhs_items.p, H->rhs_pts.p,
+                                                                            H->d_groups.p, H->rhs_vals.p, H->chunk);
+    launch_trisolve(H, s);
+    if (H->n_sweep_items > 0)
+      eval_kernel<false><<<H->n_sweep_items, EVAL_THREADS, H->eval_smem, s>>>(
+          net, H->sweep_items.p, H->sweep_pts.p, H->d_groups.p, H->sweep_vals.p, H->chunk);
+    const int ub = (H->n_upd + UPDATE_WARPS - 1) / UPDATE_WARPS;
+    const size_t usmem = sizeof(double) * 2 * H->nvmax * UPDATE_WARPS;
+    if (ub > 0)
+      update_kernel<<<ub, UPDATE_WARPS * 32, usmem, s>>>(net, H->upd_list.p, H->n_upd, H->group_of.p,
+                                                          H->d_groups.p, H->sweep_vals.p, H->nvmax, 0);
+    CK(cudaMemsetAsync(H->grow_count.p, 0, sizeof(int), s));
+    growth_kernel<<<(H->n_upd * 32 + 127) / 128, 128, 0, s>>>(net, H->upd_list.p, H->n_upd, C->coef_ratio,
+                                                               (int)C->max_ncoef, (int)C->coef_increase,
+                                                               H->grow_list.p, H->grow_count.p);
+    int ngrow = 0;
+    CK(cudaMemcpyAsync(&ngrow, H->grow_count.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    H->launches += 6;
+    if (ngrow > 0) {
+      std::vector<int> grown(ngrow);
+      CK(cudaMemcpy(grown.data(), H->grow_list.p, sizeof(int) * ngrow, cudaMemcpyDeviceToHost));
+      std::sort(grown.begin(), grown.end());
+      std::vector<char> mask(ne, 0);
+      std::vector<int> psi;
+      for (int e : grown) {
+        mask[e] = 1;
+        H->cur_ncoef[e] += (int)C->coef_increase;
+        H->cur_nint[e] = 2 * H->cur_ncoef[e];
+        const int ty = H->h.type[e];
+        if (ty == 1 || ty == 4 || ty == 5) psi.push_back(e);
+      }
+      // tables for the next iterations, and for re-solving the grown elements
+      int rct = build_eval_tables(H);
+      if (rct) return rct;
+      std::vector<Group> rg;
+      std::vector<int> rgo;
+      std::vector<Item> ri;
+      std::vector<int2> rp;
+      int nrv = 0;
+      build_tables(H, false, rg, rgo, ri, rp, nrv, &mask);
+      CK(upload(H->rs_groups, rg, s));
+      CK(upload(H->rs_group_of, rgo, s));
+      CK(upload(H->rs_items, ri, s));
+      CK(upload(H->rs_pts, rp, s));
+      CK(upload(H->rs_list, grown, s));
+      if (H->rs_vals.cap < (size_t)std::max(1, nrv)) CK(H->rs_vals.alloc(std::max(1, nrv)));
+      net = H->net();
+      if (!psi.empty()) {
+        DBuf<int> dpsi;
+        CK(upload(dpsi, psi, s));
+        cuts_kernel<<<((int)psi.size() * 32 + 127) / 128, 128, 0, s>>>(net, dpsi.p, (int)psi.size());
+        CK(cudaStreamSynchronize(s));
+        H->launches += 1;
+      }
+      if (!ri.empty())
+        eval_kernel<false><<<(int)ri.size(), EVAL_THREADS, H->eval_smem, s>>>(net, H->rs_items.p, H->rs_pts.p,
+                                                                              H->rs_groups.p, H->rs_vals.p,
+                                                                              H->chunk);
+      const size_t us2 = sizeof(double) * 2 * H->nvmax * UPDATE_WARPS;
+      update_kernel<<<(ngrow + UPDATE_WARPS - 1) / UPDATE_WARPS, UPDATE_WARPS * 32, us2, s>>>(
+          net, H->rs_list.p, ngrow, H->rs_group_of.p, H->rs_groups.p, H->rs_vals.p, H->nvmax, 2);
+      H->launches += 2;
+    }
+    blend2_kernel<<<std::max(1, std::min(1184, (int)((H->ne * H->MC + 255) / 256))), 256, 0, s>>>(net);
+    reduce_kernel<<<1, 1024, 0, s>>>(net);
+    H->launches += 2;
+    CK(cudaMemcpyAsync(H->h_st, H->st.p, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (H->h_st->done) break;
+    if (++guard > C->max_iterations + 2) break;
+  }
+  return 0;
+}
+
 static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S) {
   auto t_all = std::chrono::steady_clock::now();
   cudaStream_t s = H->stream;
@@ -1702,14 +2056,39 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
     set_error("constants out of range");
     return ANDFN_BAD_INPUT;
   }
-  // Adaptive coefficient growth (hpc_solve.py:465-559) needs MAX_NCOEF above
-  // the current ncoef somewhere; this build implements the pinned case.
+  // Adaptive coefficient growth (hpc_solve.py:465-559) can happen when some
+  // element may still grow (ncoef < MAX_NCOEF); it needs coefficient capacity
+  // MAX_NCOEF and the host-driven loop below.
   bool growth_possible = false;
   for (int64_t i = 0; i < H->ne; i++)
     if (H->h.type[i] != 2 && H->h.ncoef[i] < C->max_ncoef) growth_possible = true;
   if (growth_possible) {
-    set_error("adaptive ncoef growth (MAX_NCOEF > ncoef) is not supported by this entry point yet");
-    return ANDFN_BAD_INPUT;
+    if (C->coef_increase <= 0) {
+      set_error("COEF_INCREASE must be positive");
+      return ANDFN_BAD_INPUT;
+    }
+    // largest ncoef reachable: growth stops at the first step >= MAX_NCOEF
+    int64_t top = 0;
+    for (int64_t i = 0; i < H->ne; i++) {
+      int64_t m = H->h.ncoef[i];
+      if (H->h.type[i] != 2 && m < C->max_ncoef) m += C->coef_increase * ((C->max_ncoef - m + C->coef_increase - 1) / C->coef_increase);
+      top = std::max(top, m);
+    }
+    if (top > H->L.max_ncoef) {
+      set_error("adaptive growth can exceed the record capacity (element MAX_NCOEF)");
+      return ANDFN_BAD_INPUT;
+    }
+    int rce = ensure_capacity(H, (int)top);
+    if (rce) return rce;
+  }
+  if (H->cur_nint != H->h.nint || H->cur_ncoef != H->h.ncoef) {
+    H->cur_nint = H->h.nint;
+    H->cur_ncoef = H->h.ncoef;
+    H->tables_dirty = true;
+  }
+  if (H->tables_dirty) {
+    int rct = build_eval_tables(H);
+    if (rct) return rct;
   }
   int rc = reset_impl(H);
   if (rc) return rc;
@@ -1720,7 +2099,7 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
   st0.max_error = C->max_error;
   st0.damping = C->damping;
   st0.max_it = (int)C->max_iterations;
-  st0.fused_blend2 = 1;
+  st0.fused_blend2 = growth_possible ? 0 : 1;
   st0.solve_q = 1;
   st0.done = (C->max_iterations <= 0) ? 1 : 0;
   CK(cudaMemcpyAsync(H->st.p, &st0, sizeof(st0), cudaMemcpyHostToDevice, s));
@@ -1763,9 +2142,9 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
         A.val[fill[c]++] = mv[p];
       }
   }
-  if ((int)H->colorder.size() != H->N) H->colorder = column_min_degree_order(A);
+  if ((int)H->colorder.size() != H->N) H->colorder = column_min_degree_order(A, &H->dense_k);
   LuFactors LU;
-  rc = sparse_lu_factor(A, H->colorder, 1.0, LU);
+  rc = sparse_lu_factor(A, H->colorder, 1.0, LU, H->dense_k);
   if (rc) {
     set_error("discharge system is singular (a fracture without a head boundary?)");
     return ANDFN_SINGULAR;
@@ -1781,9 +2160,14 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
   CK(upload(H->u_val, LU.u_val, s));
   CK(upload(H->u_inv, LU.u_inv_diag, s));
   {
+    const int n = H->N;
+    const int K = LU.dense;
+    const int m0 = n - K;  // rows [0, m0) sparse, [m0, n) dense tail
+    H->tail_k = K;
     std::vector<int> lev, rows, eptr, ecol;
     std::vector<double> ev, esc;
-    build_levels(H->N, LU.l_ptr, LU.l_col, LU.l_val, nullptr, true, lev, rows, eptr, ecol, ev, esc);
+    build_levels(n, LU.l_ptr, LU.l_col, LU.l_val, nullptr, true, 0, m0, 0, m0, false, lev, rows, eptr, ecol, ev,
+                 esc);
     H->lf_nlev = (int)lev.size() - 1;
     CK(upload(H->lf_lev, lev, s));
     CK(upload(H->lf_rows, rows, s));
@@ -1791,7 +2175,8 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
     CK(upload(H->lf_col, ecol, s));
     CK(upload(H->lf_val, ev, s));
     CK(cudaStreamSynchronize(s));
-    build_levels(H->N, LU.u_ptr, LU.u_col, LU.u_val, &LU.u_inv_diag, false, lev, rows, eptr, ecol, ev, esc);
+    build_levels(n, LU.u_ptr, LU.u_col, LU.u_val, &LU.u_inv_diag, false, 0, m0, 0, m0, false, lev, rows, eptr,
+                 ecol, ev, esc);
     H->ub_nlev = (int)lev.size() - 1;
     CK(upload(H->ub_lev, lev, s));
     CK(upload(H->ub_rows, rows, s));
@@ -1800,53 +2185,85 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
     CK(upload(H->ub_val, ev, s));
     CK(upload(H->ub_scale, esc, s));
     CK(cudaStreamSynchronize(s));
+    if (K > 0) {
+      build_levels(n, LU.l_ptr, LU.l_col, LU.l_val, nullptr, true, m0, n, 0, m0, true, lev, rows, eptr, ecol, ev,
+                   esc);
+      H->lx_nlev = (int)lev.size() - 1;
+      CK(upload(H->lx_lev, lev, s));
+      CK(upload(H->lx_rows, rows, s));
+      CK(upload(H->lx_eptr, eptr, s));
+      CK(upload(H->lx_col, ecol, s));
+      CK(upload(H->lx_val, ev, s));
+      CK(cudaStreamSynchronize(s));
+      build_levels(n, LU.u_ptr, LU.u_col, LU.u_val, nullptr, false, 0, m0, m0, n, true, lev, rows, eptr, ecol, ev,
+                   esc);
+      H->ux_nlev = (int)lev.size() - 1;
+      CK(upload(H->ux_lev, lev, s));
+      CK(upload(H->ux_rows, rows, s));
+      CK(upload(H->ux_eptr, eptr, s));
+      CK(upload(H->ux_col, ecol, s));
+      CK(upload(H->ux_val, ev, s));
+      CK(cudaStreamSynchronize(s));
+      std::vector<double> ui(LU.u_inv_diag.begin() + m0, LU.u_inv_diag.end());
+      CK(upload(H->tail_l, LU.l22, s));
+      CK(upload(H->tail_u, LU.u22, s));
+      CK(upload(H->tail_uinv, ui, s));
+      CK(cudaStreamSynchronize(s));
+    }
   }
   stats.ms_factor = ms_since(t_fac);
   // iterations, in graph batches
   auto t_it = std::chrono::steady_clock::now();
-  if (H->graph_exec) {
-    cudaGraphExecDestroy(H->graph_exec);
-    H->graph_exec = nullptr;
-  }
-  {
-    cudaGraph_t g;
-    CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-    if (H->profiling && !H->ev[0][0][0])
-      for (auto &bb : H->ev)
-        for (auto &c : bb)
-          for (auto &e : c) CK(cudaEventCreate(&e));
-    for (int b = 0; b < ITER_BATCH; b++) enqueue_iteration(H, s, 0, b);
-    CK(cudaStreamEndCapture(s, &g));
-    CK(cudaGraphInstantiate(&H->graph_exec, g, 0));
-    cudaGraphDestroy(g);
-  }
-  H->launches -= ITER_BATCH * 5;  // capture does not launch
-  int guard = 0;
-  int nit_before = 0;
-  while (true) {
-    CK(cudaGraphLaunch(H->graph_exec, s));
-    CK(cudaMemcpyAsync(H->h_st, H->st.p, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
-    H->launches += ITER_BATCH * 5;
-    if (H->profiling) {
-      // only the iterations that did work (later ones return at entry)
-      const int real = std::min(ITER_BATCH, H->h_st->nit - nit_before);
-      for (int b = 0; b < real; b++)
-        for (int c = 0; c < KCLASSES; c++) {
-          float ms = 0.f;
-          if (cudaEventElapsedTime(&ms, H->ev[b][c][0], H->ev[b][c][1]) == cudaSuccess) {
-            H->k_ms[c] += ms;
-            H->k_n[c] += 1;
-          }
-        }
-      nit_before = H->h_st->nit;
+  if (growth_possible) {
+    int rca = run_adaptive(H, C);
+    if (rca) return rca;
+  } else {
+    if (H->graph_exec) {
+      cudaGraphExecDestroy(H->graph_exec);
+      H->graph_exec = nullptr;
     }
-    if (H->h_st->done) break;
-    if (++guard > 1 + C->max_iterations / ITER_BATCH + 2) break;
+    {
+      cudaGraph_t g;
+      CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      if (H->profiling && !H->ev[0][0][0])
+        for (auto &bb : H->ev)
+          for (auto &c : bb)
+            for (auto &e : c) CK(cudaEventCreate(&e));
+      for (int b = 0; b < ITER_BATCH; b++) enqueue_iteration(H, s, 0, b);
+      CK(cudaStreamEndCapture(s, &g));
+      CK(cudaGraphInstantiate(&H->graph_exec, g, 0));
+      cudaGraphDestroy(g);
+    }
+    H->launches -= ITER_BATCH * 5;  // capture does not launch
+    int guard = 0;
+    int nit_before = 0;
+    while (true) {
+      CK(cudaGraphLaunch(H->graph_exec, s));
+      CK(cudaMemcpyAsync(H->h_st, H->st.p, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      H->launches += ITER_BATCH * 5;
+      if (H->profiling) {
+        // only the iterations that did work (later ones return at entry)
+        const int real = std::min(ITER_BATCH, H->h_st->nit - nit_before);
+        for (int b = 0; b < real; b++)
+          for (int c = 0; c < KCLASSES; c++) {
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, H->ev[b][c][0], H->ev[b][c][1]) == cudaSuccess) {
+              H->k_ms[c] += ms;
+              H->k_n[c] += 1;
+            }
+          }
+        nit_before = H->h_st->nit;
+      }
+      if (H->h_st->done) break;
+      if (++guard > 1 + C->max_iterations / ITER_BATCH + 2) break;
+    }
+
   }
   SolveState fin = *H->h_st;
   // hpc_solve.py:224-234: an extra element_solver sweep at nit == MAX_ITERATIONS
   if (fin.nit == C->max_iterations && !fin.nonfinite && fin.status == 0) {
+    net = H->net();
     SolveState tmp = fin;
     tmp.done = 0;
     CK(cudaMemcpyAsync(H->st.p, &tmp, sizeof(tmp), cudaMemcpyHostToDevice, s));
@@ -1873,6 +2290,9 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
   stats.n_unknowns = H->N;
   stats.nnz_matrix = (int64_t)H->mcol.size();
   stats.nnz_factors = H->nnz_factors;
+  stats.dense_tail = H->tail_k;
+  stats.levels_l = H->lf_nlev;
+  stats.levels_u = H->ub_nlev;
   stats.gpu_launches = H->launches;
   int status = ANDFN_OK;
   if (fin.status) status = fin.status;
@@ -1988,7 +2408,7 @@ int andfn_b200_create(AndfnHandle **out, const void *frac_recs, int64_t nf, cons
   H->L = *layout;
   if (const char *v = getenv("ANDFN_B200_SOLVE_THREADS")) {
     int t = atoi(v);
-    if (t >= 32 && t <= 1024 && t % 32 == 0) H->solve_threads = t;
+    if (t >= 32 && t <= SOLVE_THREADS && t % 32 == 0) H->solve_threads = t;
   }
   H->ne = ne;
   H->nf = nf;
@@ -2177,7 +2597,7 @@ int andfn_b200_solve(void *frac_recs, int64_t nf, void *elem_recs, int64_t ne, c
     if (rc2) rc = rc2;
   }
   st.ms_upload = ms_up;
-  st.h2d_bytes = g_h2d_bytes;
+  st.h2d_bytes = g_h2d_bytes;  // create + run + download of this call
   st.d2h_bytes = g_d2h_bytes;
   andfn_b200_destroy(H);
   st.ms_total = ms_since(t0);

@@ -25,8 +25,9 @@
 
 namespace andfn {
 
-std::vector<int> column_min_degree_order(const CscMatrix &A) {
+std::vector<int> column_min_degree_order(const CscMatrix &A, int *dense_tail, double dense_frac, int max_dense) {
   const int n = A.n;
+  if (dense_tail) *dense_tail = 0;
   // Row-wise pattern: row r is the initial element r (a clique of its columns).
   std::vector<std::vector<int>> Le(2 * (size_t)n + 1);
   std::vector<std::vector<int>> Ei(n);
@@ -70,6 +71,11 @@ std::vector<int> column_min_degree_order(const CscMatrix &A) {
   for (int k = 0; k < n; k++) {
     auto it = queue.begin();
     int p = it->second;
+    if (dense_tail && *dense_tail == 0) {
+      const int remaining = n - k;
+      if (remaining >= 64 && remaining <= max_dense && it->first >= dense_frac * (remaining - 1))
+        *dense_tail = remaining;
+    }
     queue.erase(it);
     order.push_back(p);
     alive[p] = 0;
@@ -145,10 +151,68 @@ std::vector<int> column_min_degree_order(const CscMatrix &A) {
   return order;
 }
 
-int sparse_lu_factor(const CscMatrix &A, const std::vector<int> &q, double pivot_threshold, LuFactors &F) {
+// Blocked right-looking LU with partial pivoting of a column-major n x n
+// matrix (unit lower L and U overwrite S); piv[j] = row swapped with row j.
+static int dense_lu(double *S, int n, std::vector<int> &piv, double &min_piv) {
+  const int NB = 48;
+  piv.assign(n, 0);
+  for (int j0 = 0; j0 < n; j0 += NB) {
+    const int jb = std::min(NB, n - j0);
+    // panel factorisation, columns j0 .. j0+jb-1
+    for (int j = j0; j < j0 + jb; j++) {
+      double *cj = S + (size_t)j * n;
+      int p = j;
+      double amax = std::fabs(cj[j]);
+      for (int i = j + 1; i < n; i++)
+        if (std::fabs(cj[i]) > amax) {
+          amax = std::fabs(cj[i]);
+          p = i;
+        }
+      piv[j] = p;
+      if (amax == 0.0 || !std::isfinite(amax)) return 3;
+      min_piv = std::min(min_piv, amax);
+      if (p != j)
+        for (int c = 0; c < n; c++) std::swap(S[(size_t)c * n + j], S[(size_t)c * n + p]);
+      const double inv = 1.0 / cj[j];
+      for (int i = j + 1; i < n; i++) cj[i] *= inv;
+      for (int c = j + 1; c < j0 + jb; c++) {
+        double *cc = S + (size_t)c * n;
+        const double u = cc[j];
+        if (u != 0.0)
+          for (int i = j + 1; i < n; i++) cc[i] -= cj[i] * u;
+      }
+    }
+    const int c0 = j0 + jb;
+    if (c0 >= n) break;
+    // U12 = L11^-1 A12 and trailing update A22 -= L21 U12, by columns
+#pragma omp parallel for schedule(dynamic, 8)
+    for (int c = c0; c < n; c++) {
+      double *cc = S + (size_t)c * n;
+      for (int j = j0; j < c0; j++) {
+        const double u = cc[j];
+        if (u == 0.0) continue;
+        const double *cj = S + (size_t)j * n;
+        for (int i = j + 1; i < c0; i++) cc[i] -= cj[i] * u;
+      }
+      for (int j = j0; j < c0; j++) {
+        const double u = cc[j];
+        if (u == 0.0) continue;
+        const double *cj = S + (size_t)j * n;
+        for (int i = c0; i < n; i++) cc[i] -= cj[i] * u;
+      }
+    }
+  }
+  return 0;
+}
+
+int sparse_lu_factor(const CscMatrix &A, const std::vector<int> &q, double pivot_threshold, LuFactors &F,
+                     int dense) {
   const int n = A.n;
+  if (dense < 0 || dense > n) dense = 0;
+  const int m0 = n - dense;
   F.n = n;
   F.q = q;
+  F.dense = dense;
   F.pinv.assign(n, -1);
   std::vector<int> prow(n, -1);
   // Column-wise L (original row indices) and U (pivot-step indices).
@@ -163,10 +227,24 @@ int sparse_lu_factor(const CscMatrix &A, const std::vector<int> &q, double pivot
   pattern.reserve(n);
   topo.reserve(n);
   double min_piv = INFINITY;
+  std::vector<int> tail_row;           // dense-block row of each original row (or -1)
+  std::vector<double> S;               // Schur complement, column-major dense x dense
+  std::vector<int> tail_rows;          // original rows of the dense block, in block order
   for (int k = 0; k < n; k++) {
     const int col = q[k];
     pattern.clear();
     topo.clear();
+    if (k == m0 && dense > 0) {
+      // rows not pivoted yet form the dense block
+      tail_row.assign(n, -1);
+      for (int r = 0; r < n; r++)
+        if (F.pinv[r] < 0) {
+          tail_row[r] = (int)tail_rows.size();
+          tail_rows.push_back(r);
+        }
+      if ((int)tail_rows.size() != dense) return 3;
+      S.assign((size_t)dense * dense, 0.0);
+    }
     // Scatter A(:, col) and find the reach of its pivoted rows in L's graph.
     for (int p = A.colptr[col]; p < A.colptr[col + 1]; p++) {
       int r = A.rowind[p];
@@ -234,6 +312,14 @@ int sparse_lu_factor(const CscMatrix &A, const std::vector<int> &q, double pivot
       }
     }
     Ucp.push_back((int)Uri.size());
+    if (k >= m0) {
+      // dense block column: the not-yet-pivoted rows
+      double *sc = S.data() + (size_t)(k - m0) * dense;
+      for (int r : pattern)
+        if (F.pinv[r] < 0) sc[tail_row[r]] = x[r];
+      Lcp.push_back((int)Lri.size());
+      continue;
+    }
     // Partial pivoting over the not-yet-pivoted rows.
     int piv = -1;
     double amax = 0.0;
@@ -259,17 +345,43 @@ int sparse_lu_factor(const CscMatrix &A, const std::vector<int> &q, double pivot
       }
     Lcp.push_back((int)Lri.size());
   }
+  if (dense > 0) {
+    std::vector<int> dpiv;
+    if (dense_lu(S.data(), dense, dpiv, min_piv)) return 3;
+    // block row order after the dense pivoting
+    std::vector<int> order(dense);
+    for (int i = 0; i < dense; i++) order[i] = i;
+    for (int j = 0; j < dense; j++) std::swap(order[j], order[dpiv[j]]);
+    for (int i = 0; i < dense; i++) {
+      const int r = tail_rows[order[i]];
+      F.pinv[r] = m0 + i;
+      prow[m0 + i] = r;
+    }
+    F.l22.assign((size_t)dense * dense, 0.0);
+    F.u22.assign((size_t)dense * dense, 0.0);
+    for (int c = 0; c < dense; c++)
+      for (int i = 0; i < dense; i++) {
+        const double v = S[(size_t)c * dense + i];
+        if (i > c)
+          F.l22[(size_t)c * dense + i] = v;
+        else if (i < c)
+          F.u22[(size_t)c * dense + i] = v;
+        else
+          diag[m0 + i] = v;
+      }
+  }
   F.min_abs_pivot = min_piv;
-  // Row-oriented factors in pivot-step indices.
+  // Row-oriented factors in pivot-step indices (entries inside the dense
+  // block are kept only in l22 / u22).
   F.l_ptr.assign(n + 1, 0);
-  for (int k = 0; k < n; k++)
+  for (int k = 0; k < m0; k++)
     for (int p = Lcp[k]; p < Lcp[k + 1]; p++) F.l_ptr[F.pinv[Lri[p]] + 1]++;
   for (int i = 0; i < n; i++) F.l_ptr[i + 1] += F.l_ptr[i];
   F.l_col.assign(F.l_ptr[n], 0);
   F.l_val.assign(F.l_ptr[n], 0.0);
   {
     std::vector<int> fill(F.l_ptr.begin(), F.l_ptr.end() - 1);
-    for (int k = 0; k < n; k++)
+    for (int k = 0; k < m0; k++)
       for (int p = Lcp[k]; p < Lcp[k + 1]; p++) {
         int i = F.pinv[Lri[p]];
         F.l_col[fill[i]] = k;
@@ -297,18 +409,22 @@ int sparse_lu_factor(const CscMatrix &A, const std::vector<int> &q, double pivot
 }
 
 void sparse_lu_solve_host(const LuFactors &F, const double *b, double *xout) {
-  const int n = F.n;
+  const int n = F.n, K = F.dense, m0 = n - K;
   std::vector<double> y(n);
   // y = P b
   for (int r = 0; r < n; r++) y[F.pinv[r]] = b[r];
   for (int i = 0; i < n; i++) {
     double s = y[i];
     for (int p = F.l_ptr[i]; p < F.l_ptr[i + 1]; p++) s -= F.l_val[p] * y[F.l_col[p]];
+    if (i >= m0)
+      for (int c = m0; c < i; c++) s -= F.l22[(size_t)(c - m0) * K + (i - m0)] * y[c];
     y[i] = s;
   }
   for (int i = n - 1; i >= 0; i--) {
     double s = y[i];
     for (int p = F.u_ptr[i]; p < F.u_ptr[i + 1]; p++) s -= F.u_val[p] * y[F.u_col[p]];
+    if (i >= m0)
+      for (int c = i + 1; c < n; c++) s -= F.u22[(size_t)(c - m0) * K + (i - m0)] * y[c];
     y[i] = s * F.u_inv_diag[i];
   }
   for (int k = 0; k < n; k++) xout[F.q[k]] = y[k];

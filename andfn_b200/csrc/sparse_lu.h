@@ -21,6 +21,12 @@ struct CscMatrix {
 
 struct LuFactors {
   int n = 0;
+  // Dense trailing block: the last `dense` pivot steps are factorised as a
+  // dense matrix (column-major dense x dense, strictly lower part of L and
+  // strictly upper part of U; the CSR arrays below then hold only entries
+  // outside that block).
+  int dense = 0;
+  std::vector<double> l22, u22;
   std::vector<int> q;       // column order: pivot step k eliminates column q[k]
   std::vector<int> pinv;    // row -> pivot step (P as inverse permutation)
   // Row-oriented (CSR) factors in pivot-step indices, for the device solve:
@@ -36,11 +42,19 @@ struct LuFactors {
 // Column ordering: minimum degree on the column-intersection graph of A,
 // computed on a quotient graph whose initial elements are the rows of A
 // (each row is a clique of its columns), with approximate external degrees.
-std::vector<int> column_min_degree_order(const CscMatrix &A);
+// *dense_tail (optional) receives the number of trailing columns that remain
+// once the minimum degree reaches dense_frac of the remaining columns (the
+// graph is then nearly complete; 0 if that never happens with >= 64 left).
+std::vector<int> column_min_degree_order(const CscMatrix &A, int *dense_tail = nullptr, double dense_frac = 0.4,
+                                         int max_dense = 3072);
 
-// Left-looking sparse LU with partial pivoting (Gilbert-Peierls).
-// Returns 0 on success, 3 (singular) if a column has no nonzero pivot.
-int sparse_lu_factor(const CscMatrix &A, const std::vector<int> &q, double pivot_threshold, LuFactors &out);
+// LU with partial pivoting: left-looking sparse (Gilbert-Peierls) for the
+// first n - dense pivot steps, then the Schur complement of the last `dense`
+// columns as a dense matrix, factorised by a blocked right-looking dense LU
+// with partial pivoting (OpenMP).  Returns 0 on success, 3 (singular) if a
+// column has no nonzero pivot.
+int sparse_lu_factor(const CscMatrix &A, const std::vector<int> &q, double pivot_threshold, LuFactors &out,
+                     int dense = 0);
 
 // Reference triangular solve on the host (used for checks): x = A^-1 b.
 void sparse_lu_solve_host(const LuFactors &F, const double *b, double *x);

@@ -88,7 +88,8 @@ class AndfnSolveStats(ctypes.Structure):
                 ("ms_setup", ctypes.c_double), ("ms_factor", ctypes.c_double),
                 ("ms_iterate", ctypes.c_double), ("ms_download", ctypes.c_double),
                 ("ms_total", ctypes.c_double), ("status", ctypes.c_int32), ("device", ctypes.c_int32),
-                ("h2d_bytes", ctypes.c_int64), ("d2h_bytes", ctypes.c_int64)]
+                ("h2d_bytes", ctypes.c_int64), ("d2h_bytes", ctypes.c_int64), ("dense_tail", ctypes.c_int64),
+                ("levels_l", ctypes.c_int64), ("levels_u", ctypes.c_int64)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}

@@ -5,8 +5,10 @@ and the damped Jacobi iteration to convergence at MAX_ERROR = 1e-8) of the
 ~2,000-fracture network: power-law radii (alpha 2.6, 0.5-20 m), Fisher
 (kappa 5) normals, log10 T ~ N(-5, 1), heads 1 / 0 on the x faces, ncoef 20,
 nint 40, discharge_int 50.  The literal 2,000 discs in a 100 m cube do not
-percolate, so 5,500 discs are drawn in a 50 m cube (seed 0) and the largest
-cluster joining both heads is kept (2,015 fractures, 4,912 elements).
+percolate, so 5,500 discs are drawn in a 50 m cube (seed 5) and the largest
+cluster joining both heads is kept (2,118 fractures, 5,376 elements; it
+converges in 90 outer iterations -- like the reference, some seeds of this
+recipe do not converge, so the seed is fixed).
 
 value: solves/s with the network resident in HBM (handle API), timed with
 CUDA events on the library's stream, L2 flushed (256 MiB write) between steps.
@@ -35,13 +37,13 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "batched vs plain DFN solves/s at 1e-8 BC residual; adjoint/forward time ratio"
-WORKLOAD = ("plain solve: 2,015-fracture spanning cluster of 5,500 power-law/Fisher discs in a 50 m cube "
-            "(seed 0), ncoef 20, nint 40, discharge_int 50, MAX_ERROR 1e-8")
+WORKLOAD = ("plain solve: 2,118-fracture spanning cluster of 5,500 power-law/Fisher discs in a 50 m cube "
+            "(seed 5), ncoef 20, nint 40, discharge_int 50, MAX_ERROR 1e-8")
 MAX_ERROR = 1e-8
 SAMPLE_ITS = 10
 
 
-def build_network(seed=0):
+def build_network(seed=5):
     from andfn_b200 import network as nw
     net = nw.power_law_fisher(seed, nf=5500, L=50.0, ncoef=20, nint=40)
     return nw.to_records(net)
@@ -176,7 +178,7 @@ def run_reference(args):
     F, E = build_network()
     c = constants()
     D = 50
-    its_full = int(os.environ.get("ANDFN_BENCH_ITERATIONS", "91"))
+    its_full = 90  # outer iterations of this network to MAX_ERROR 1e-8 (GPU and oracle agree)
     for _ in range(args.warmup):
         cpu_sample(F, E, D, c, its_full)
     secs = []

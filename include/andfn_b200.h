@@ -87,6 +87,9 @@ typedef struct AndfnSolveStats {
   int32_t device;        /* CUDA ordinal used                             */
   int64_t h2d_bytes;     /* host->device bytes of andfn_b200_solve        */
   int64_t d2h_bytes;     /* device->host bytes of andfn_b200_solve        */
+  int64_t dense_tail;    /* pivot steps solved as a dense trailing block  */
+  int64_t levels_l;      /* dependency levels of the sparse part of L     */
+  int64_t levels_u;      /* dependency levels of the sparse part of U     */
 } AndfnSolveStats;
 
 /* ---- one-call drop-in (replaces andfn/hpc/hpc_solve.py:55 solve) --------
