@@ -68,6 +68,10 @@ struct SolveState {
   double error_q, error, error_coef, pad;
   double max_error, damping;
   int max_it, fused_blend2;
+  // SM clock cycles spent in the phases of trisolve_kernel, summed over
+  // launches (thread 0's view): gather, L sparse, L coupling, L dense,
+  // U dense, U coupling, U sparse, scatter
+  long long tri_cycles[8];
 };
 
 // Device view of one network.
@@ -98,6 +102,7 @@ struct Net {
   const double *l_val, *u_val, *u_inv;
   double *disc;  // current discharges [N]
   double *work;  // [N] scratch (solve in global memory when N is large)
+  double *bvec;  // [N] head vector of the current iteration
   int *ready;    // [N]
   SolveState *st;
 };
@@ -684,6 +689,9 @@ __device__ void level_solve(const LevelSolve &F, double *y, int *s_levptr, int c
   __syncthreads();
   const int *lp = lev_in_smem ? s_levptr : F.lev_ptr;
   SlotMeta M{meta_in_smem ? s_meta : F.rows, meta_in_smem ? s_meta + meta_cap : F.eptr};
+  // Levels are processed in pairs: registers a hold the first row of even
+  // levels, b of odd levels; each is refilled two levels ahead right after it
+  // is consumed, so no register copy waits on loads in flight.
   RowRegs a, b;
   bool ha = false, hb = false;
   if (F.nlev > 0 && lp[0] + warp < lp[1]) {
@@ -694,25 +702,88 @@ __device__ void level_solve(const LevelSolve &F, double *y, int *s_levptr, int c
     load_row(b, F, M, lp[1] + warp, lane);
     hb = true;
   }
-  for (int l = 0; l < F.nlev; l++) {
-    const int r0 = lp[l], r1 = lp[l + 1];
-    if (ha) solve_row(a, F, r0 + warp, lane, y);
-    for (int slot = r0 + warp + nw; slot < r1; slot += nw) {
-      RowRegs t;
-      load_row(t, F, M, slot, lane);
-      solve_row(t, F, slot, lane, y);
+  for (int l = 0; l < F.nlev; l += 2) {
+    {
+      const int r0 = lp[l], r1 = lp[l + 1];
+      if (ha) solve_row(a, F, r0 + warp, lane, y);
+      // a level with more rows than warps: rows loaded one ahead
+      int slot = r0 + warp + nw;
+      if (slot < r1) {
+        RowRegs t0, t1;
+        load_row(t0, F, M, slot, lane);
+        for (; slot < r1; slot += 2 * nw) {
+          const bool more = slot + nw < r1;
+          if (more) load_row(t1, F, M, slot + nw, lane);
+          solve_row(t0, F, slot, lane, y);
+          if (!more) break;
+          const bool more2 = slot + 2 * nw < r1;
+          if (more2) load_row(t0, F, M, slot + 2 * nw, lane);
+          solve_row(t1, F, slot + nw, lane, y);
+          if (!more2) break;
+        }
+      }
+      ha = false;
+      if (l + 2 < F.nlev && lp[l + 2] + warp < lp[l + 3]) {
+        load_row(a, F, M, lp[l + 2] + warp, lane);
+        ha = true;
+      }
+      __syncthreads();
     }
-    a = b;
-    ha = hb;
-    hb = false;
-    if (l + 2 < F.nlev) {
-      const int n0 = lp[l + 2], n1 = lp[l + 3];
-      if (n0 + warp < n1) {
-        load_row(b, F, M, n0 + warp, lane);
+    if (l + 1 < F.nlev) {
+      const int r0 = lp[l + 1], r1 = lp[l + 2];
+      if (hb) solve_row(b, F, r0 + warp, lane, y);
+      int slot = r0 + warp + nw;
+      if (slot < r1) {
+        RowRegs t0, t1;
+        load_row(t0, F, M, slot, lane);
+        for (; slot < r1; slot += 2 * nw) {
+          const bool more = slot + nw < r1;
+          if (more) load_row(t1, F, M, slot + nw, lane);
+          solve_row(t0, F, slot, lane, y);
+          if (!more) break;
+          const bool more2 = slot + 2 * nw < r1;
+          if (more2) load_row(t0, F, M, slot + 2 * nw, lane);
+          solve_row(t1, F, slot + nw, lane, y);
+          if (!more2) break;
+        }
+      }
+      hb = false;
+      if (l + 3 < F.nlev && lp[l + 3] + warp < lp[l + 4]) {
+        load_row(b, F, M, lp[l + 3] + warp, lane);
         hb = true;
       }
+      __syncthreads();
     }
-    __syncthreads();
+  }
+}
+
+// Head vector b (build_head_matrix, hpc_solve.py:811-829): the mean of the
+// series potential over the D points of each discharge element side; one
+// warp per row, lanes over the points.  Continuity rows are zero.
+__global__ void rhs_reduce_kernel(Net net, const double *__restrict__ rhs_vals, const int *__restrict__ rhs_group,
+                                  const Group *__restrict__ groups) {
+  const SolveState *st = net.st;
+  if (st->done || !st->solve_q) return;
+  const int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (r >= net.N) return;
+  if (r >= net.n_de) {
+    if (lane == 0) net.bvec[r] = 0.0;
+    return;
+  }
+  const int D = net.D;
+  const int e = net.de_ids[r];
+  const Group g0 = groups[rhs_group[2 * r]];
+  double s0 = 0.0;
+  for (int k = lane; k < D; k += 32) s0 += rhs_vals[g0.out + k];
+  s0 = warp_sum(s0);
+  if (net.type[e] == 0) {
+    const Group g1 = groups[rhs_group[2 * r + 1]];
+    double s1 = 0.0;
+    for (int k = lane; k < D; k += 32) s1 += rhs_vals[g1.out + k];
+    s1 = warp_sum(s1);
+    if (lane == 0) net.bvec[r] = (s1 / D) / net.t[net.frac1[e]] - (s0 / D) / net.t[net.frac0[e]];
+  } else if (lane == 0) {
+    net.bvec[r] = net.phi[e] - s0 / D;
   }
 }
 
@@ -799,43 +870,40 @@ __global__ void __launch_bounds__(SOLVE_THREADS) trisolve_kernel(Net net, const 
   SolveState *st = net.st;
   if (st->done) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int N = net.N, n_de = net.n_de, D = net.D;
+  const int N = net.N, n_de = net.n_de;
   double *y = use_smem ? reinterpret_cast<double *>(smem_raw) : net.work;
   int *s_levptr = reinterpret_cast<int *>(smem_raw + (use_smem ? sizeof(double) * (size_t)N : 0));
   int *s_meta = s_levptr + cap_levptr;
   if (threadIdx.x == 0) st->nit += 1;
   if (!st->solve_q) return;  // uniform: solve_q is written only by reduce_kernel
-  // b = head vector (hpc_solve.py:811-829); y = P b
-  for (int r = threadIdx.x; r < N; r += blockDim.x) {
-    double b = 0.0;
-    if (r < n_de) {
-      const int e = net.de_ids[r];
-      const int type = net.type[e];
-      const Group g0 = groups[rhs_group[2 * r]];
-      double s0 = 0.0;
-      for (int k = 0; k < D; k++) s0 += rhs_vals[g0.out + k];
-      if (type == 0) {
-        const Group g1 = groups[rhs_group[2 * r + 1]];
-        double s1 = 0.0;
-        for (int k = 0; k < D; k++) s1 += rhs_vals[g1.out + k];
-        b = (s1 / D) / net.t[net.frac1[e]] - (s0 / D) / net.t[net.frac0[e]];
-      } else {
-        b = net.phi[e] - s0 / D;
-      }
+  long long clk = clock64();
+  auto phase = [&](int i) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const long long now = clock64();
+      st->tri_cycles[i] += now - clk;
+      clk = now;
     }
-    y[net.pinv[r]] = b;
-  }
-  __syncthreads();
+  };
+  // y = P b (b from rhs_reduce_kernel)
+  for (int r = threadIdx.x; r < N; r += blockDim.x) y[net.pinv[r]] = net.bvec[r];
+  phase(0);
   // L: sparse leading rows, coupling of the trailing rows to them, dense tail
   level_solve(Lf, y, s_levptr, cap_levptr, s_meta, meta_cap);
+  phase(1);
   if (T.K > 0) {
     level_solve(Lx, y, s_levptr, cap_levptr, s_meta, meta_cap);
+    phase(2);
     dense_lower_solve(T.L, T.K, y + (N - T.K));
+    phase(3);
     // U: dense tail, coupling of the leading rows to it, sparse leading rows
     dense_upper_solve(T.U, T.uinv, T.K, y + (N - T.K));
+    phase(4);
     level_solve(Ux, y, s_levptr, cap_levptr, s_meta, meta_cap);
+    phase(5);
   }
   level_solve(Ub, y, s_levptr, cap_levptr, s_meta, meta_cap);  // scale = 1/U(i,i)
+  phase(6);
   // x = Q y; error_q = max|x - x_old| / (max|x_old| + 1e-16) (hpc_solve.py:169-174)
   __shared__ double s_d[32], s_o[32];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
@@ -875,6 +943,7 @@ __global__ void __launch_bounds__(SOLVE_THREADS) trisolve_kernel(Net net, const 
       bb = fmax(bb, s_o[k]);
     }
     st->error_q = a / (bb + 1e-16);
+    st->tri_cycles[7] += clock64() - clk;
   }
 }
 
@@ -1256,8 +1325,9 @@ struct AndfnHandle {
   DBuf<double> d_mvals;
   std::vector<int> colorder;  // cached symbolic analysis (depends on the pattern only)
   int dense_k = 0;            // trailing pivot steps factorised and solved as a dense block
+  double ms_create_upload = 0, ms_create_tables = 0, ms_create_order = 0;
   DBuf<int> pinv, qcol, l_ptr, l_col, u_ptr, u_col;
-  DBuf<double> l_val, u_val, u_inv, disc, work;
+  DBuf<double> l_val, u_val, u_inv, disc, work, bvec;
   DBuf<int> ready;
   // level-ordered factors for trisolve_kernel
   DBuf<int> lf_lev, lf_rows, lf_eptr, lf_col, ub_lev, ub_rows, ub_eptr, ub_col;
@@ -1354,6 +1424,7 @@ struct AndfnHandle {
     n.u_inv = u_inv.p;
     n.disc = disc.p;
     n.work = work.p;
+    n.bvec = bvec.p;
     n.ready = ready.p;
     n.st = st.p;
     return n;
@@ -1516,6 +1587,10 @@ static void read_coefs(AndfnHandle *H, const char *E) {
 }
 
 static thread_local int64_t g_h2d_bytes = 0, g_d2h_bytes = 0;
+
+static double ms_since(std::chrono::steady_clock::time_point t0) {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
 
 template <class T>
 static cudaError_t upload(DBuf<T> &d, const std::vector<T> &v, cudaStream_t s) {
@@ -1734,6 +1809,7 @@ static int ensure_capacity(AndfnHandle *H, int mc) {
 }
 
 static int create_impl(AndfnHandle *H, const char *F, const char *E) {
+  auto tc0 = std::chrono::steady_clock::now();
   int rc = parse_records(H, F, E);
   if (rc) return rc;
   read_coefs(H, E);
@@ -1791,10 +1867,13 @@ static int create_impl(AndfnHandle *H, const char *F, const char *E) {
   CK(H->cut_pos.alloc((size_t)ne * H->cut_cap));
   CK(H->cut_elem.alloc((size_t)ne * H->cut_cap));
   CK(H->cut_sign.alloc((size_t)ne * H->cut_cap));
+  H->ms_create_upload = ms_since(tc0);
+  auto tc1 = std::chrono::steady_clock::now();
   H->cur_ncoef = h.ncoef;
   H->cur_nint = h.nint;
   rc = build_eval_tables(H);
   if (rc) return rc;
+  H->ms_create_tables = ms_since(tc1);
   // discharge system
   build_pattern(H);
   CK(upload(H->d_ent_row, H->ent_row, s));
@@ -1802,6 +1881,7 @@ static int create_impl(AndfnHandle *H, const char *F, const char *E) {
   CK(upload(H->d_ent_side, H->ent_side, s));
   CK(upload(H->d_ent_kind, H->ent_kind, s));
   CK(H->d_mvals.alloc(std::max<size_t>(1, H->ent_row.size())));
+  auto tc2 = std::chrono::steady_clock::now();
   {
     // fill-reducing column order from the pattern alone (values do not
     // matter for it), computed once per network
@@ -1817,8 +1897,10 @@ static int create_impl(AndfnHandle *H, const char *F, const char *E) {
       for (int p = H->mrow_ptr[r]; p < H->mrow_ptr[r + 1]; p++) P.rowind[fill[H->mcol[p]]++] = r;
     H->colorder = column_min_degree_order(P, &H->dense_k);
   }
+  H->ms_create_order = ms_since(tc2);
   CK(H->disc.alloc(H->N));
   CK(H->work.alloc(H->N));
+  CK(H->bvec.alloc(H->N));
   CK(H->ready.alloc(H->N));
   CK(H->st.alloc(1));
   if (!H->h_st) CK(cudaMallocHost(&H->h_st, sizeof(SolveState)));
@@ -1849,9 +1931,6 @@ static int reset_impl(AndfnHandle *H) {
   return 0;
 }
 
-static double ms_since(std::chrono::steady_clock::time_point t0) {
-  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-}
 
 // Groups rows [row_lo, row_hi) of a triangular factor by dependency level and
 // stores their entries with columns in [col_lo, col_hi) in that order
@@ -1935,6 +2014,8 @@ static int enqueue_iteration(AndfnHandle *H, cudaStream_t s, int single_blend_sw
     eval_kernel<true><<<H->n_rhs_items, EVAL_THREADS, H->eval_smem, s>>>(net, H->rhs_items.p, H->rhs_pts.p,
                                                                           H->d_groups.p, H->rhs_vals.p, H->chunk);
   }
+  rhs_reduce_kernel<<<(H->N * 32 + 255) / 256, 256, 0, s>>>(net, H->rhs_vals.p, H->rhs_group.p, H->d_groups.p);
+  H->launches += 1;
   mark(H, s, b, K_RHS, 1);
   mark(H, s, b, K_TRISOLVE, 0);
   launch_trisolve(H, s);
@@ -1972,6 +2053,7 @@ static int run_adaptive(AndfnHandle *H, const AndfnConstants *C) {
     if (H->n_rhs_items > 0)
       eval_kernel<true><<<H->n_rhs_items, EVAL_THREADS, H->eval_smem, s>>>(net, H->rhs_items.p, H->rhs_pts.p,
                                                                             H->d_groups.p, H->rhs_vals.p, H->chunk);
+    rhs_reduce_kernel<<<(H->N * 32 + 255) / 256, 256, 0, s>>>(net, H->rhs_vals.p, H->rhs_group.p, H->d_groups.p);
     launch_trisolve(H, s);
     if (H->n_sweep_items > 0)
       eval_kernel<false><<<H->n_sweep_items, EVAL_THREADS, H->eval_smem, s>>>(
@@ -1988,7 +2070,7 @@ static int run_adaptive(AndfnHandle *H, const AndfnConstants *C) {
     int ngrow = 0;
     CK(cudaMemcpyAsync(&ngrow, H->grow_count.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
-    H->launches += 6;
+    H->launches += 7;
     if (ngrow > 0) {
       std::vector<int> grown(ngrow);
       CK(cudaMemcpy(grown.data(), H->grow_list.p, sizeof(int) * ngrow, cudaMemcpyDeviceToHost));
@@ -2234,14 +2316,14 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
       CK(cudaGraphInstantiate(&H->graph_exec, g, 0));
       cudaGraphDestroy(g);
     }
-    H->launches -= ITER_BATCH * 5;  // capture does not launch
+    H->launches -= ITER_BATCH * 6;  // capture does not launch
     int guard = 0;
     int nit_before = 0;
     while (true) {
       CK(cudaGraphLaunch(H->graph_exec, s));
       CK(cudaMemcpyAsync(H->h_st, H->st.p, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
       CK(cudaStreamSynchronize(s));
-      H->launches += ITER_BATCH * 5;
+      H->launches += ITER_BATCH * 6;
       if (H->profiling) {
         // only the iterations that did work (later ones return at entry)
         const int real = std::min(ITER_BATCH, H->h_st->nit - nit_before);
@@ -2291,6 +2373,10 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
   stats.nnz_matrix = (int64_t)H->mcol.size();
   stats.nnz_factors = H->nnz_factors;
   stats.dense_tail = H->tail_k;
+  for (int i = 0; i < 8; i++) stats.tri_cycles[i] = fin.tri_cycles[i];
+  stats.ms_create_upload = H->ms_create_upload;
+  stats.ms_create_tables = H->ms_create_tables;
+  stats.ms_create_order = H->ms_create_order;
   stats.levels_l = H->lf_nlev;
   stats.levels_u = H->ub_nlev;
   stats.gpu_launches = H->launches;

@@ -20,10 +20,41 @@
 
 #include <algorithm>
 #include <cmath>
-#include <set>
 #include <utility>
 
 namespace andfn {
+
+// Degree-bucketed priority queue with O(1) insert / remove / decrease.
+struct DegreeBuckets {
+  std::vector<int> head, next, prev, deg;
+  int mindeg = 0;
+  explicit DegreeBuckets(int n) : head(n + 1, -1), next(n, -1), prev(n, -1), deg(n, 0) {}
+  void insert(int i, int d) {
+    deg[i] = d;
+    prev[i] = -1;
+    next[i] = head[d];
+    if (head[d] >= 0) prev[head[d]] = i;
+    head[d] = i;
+    if (d < mindeg) mindeg = d;
+  }
+  void remove(int i) {
+    const int d = deg[i];
+    if (prev[i] >= 0)
+      next[prev[i]] = next[i];
+    else
+      head[d] = next[i];
+    if (next[i] >= 0) prev[next[i]] = prev[i];
+  }
+  int pop_min() {
+    while (head[mindeg] < 0) mindeg++;
+    int i = head[mindeg];
+    // smallest index among the minimum-degree columns (deterministic order)
+    for (int j = next[i]; j >= 0; j = next[j])
+      if (j < i) i = j;
+    remove(i);
+    return i;
+  }
+};
 
 std::vector<int> column_min_degree_order(const CscMatrix &A, int *dense_tail, double dense_frac, int max_dense) {
   const int n = A.n;
@@ -48,7 +79,7 @@ std::vector<int> column_min_degree_order(const CscMatrix &A, int *dense_tail, do
   std::vector<char> elem_active(2 * (size_t)n + 1, 0), alive(n, 1);
   for (int r = 0; r < n; r++) elem_active[r] = !Le[r].empty();
   std::vector<int> mark(n, -1), wstamp(2 * (size_t)n + 1, -1), w(2 * (size_t)n + 1, 0);
-  std::vector<int> degree(n, 0);
+  DegreeBuckets queue(n);
   // Exact initial degree |union of row cliques containing j| - 1.
   for (int j = 0; j < n; j++) {
     int d = 0;
@@ -58,25 +89,31 @@ std::vector<int> column_min_degree_order(const CscMatrix &A, int *dense_tail, do
           mark[v] = j;
           d++;
         }
-    degree[j] = d;
+    queue.insert(j, std::min(d, n - 1));
   }
+  queue.mindeg = 0;
   std::fill(mark.begin(), mark.end(), -1);
-  std::set<std::pair<int, int>> queue;
-  for (int j = 0; j < n; j++) queue.insert({degree[j], j});
 
   std::vector<int> order;
   order.reserve(n);
   int stamp = 0;
   std::vector<int> Lp;
   for (int k = 0; k < n; k++) {
-    auto it = queue.begin();
-    int p = it->second;
-    if (dense_tail && *dense_tail == 0) {
-      const int remaining = n - k;
-      if (remaining >= 64 && remaining <= max_dense && it->first >= dense_frac * (remaining - 1))
-        *dense_tail = remaining;
+    const int remaining = n - k;
+    while (queue.head[queue.mindeg] < 0) queue.mindeg++;
+    if (dense_tail && remaining >= 64 && remaining <= max_dense && queue.mindeg >= dense_frac * (remaining - 1)) {
+      // The remaining graph is nearly complete: it is factorised as a dense
+      // block, where the column order does not change the fill.  Append the
+      // remaining columns by (degree, index).
+      *dense_tail = remaining;
+      std::vector<std::pair<int, int>> rest;
+      for (int j = 0; j < n; j++)
+        if (alive[j]) rest.push_back({queue.deg[j], j});
+      std::sort(rest.begin(), rest.end());
+      for (auto &pr : rest) order.push_back(pr.second);
+      return order;
     }
-    queue.erase(it);
+    const int p = queue.pop_min();
     order.push_back(p);
     alive[p] = 0;
     // New element: union of the active elements adjacent to p, minus p.
@@ -120,7 +157,7 @@ std::vector<int> column_min_degree_order(const CscMatrix &A, int *dense_tail, do
         w[e] -= 1;
       }
     // Aggressive absorption of elements contained in Lp, then degrees.
-    const int remaining = n - k - 1;
+    const int rem = n - k - 1;
     for (int i : Lp) {
       auto &E = Ei[i];
       size_t o = 0;
@@ -139,13 +176,12 @@ std::vector<int> column_min_degree_order(const CscMatrix &A, int *dense_tail, do
         if (e != ne) d += w[e];
       }
       E.resize(o);
-      long bound = (long)degree[i] + lp - 1;
+      long bound = (long)queue.deg[i] + lp - 1;
       if (d > bound) d = bound;
-      if (d > remaining - 1) d = remaining - 1;
+      if (d > rem - 1) d = rem - 1;
       if (d < 0) d = 0;
-      queue.erase({degree[i], i});
-      degree[i] = (int)d;
-      queue.insert({degree[i], i});
+      queue.remove(i);
+      queue.insert(i, (int)d);
     }
   }
   return order;

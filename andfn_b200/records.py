@@ -89,11 +89,14 @@ class AndfnSolveStats(ctypes.Structure):
                 ("ms_iterate", ctypes.c_double), ("ms_download", ctypes.c_double),
                 ("ms_total", ctypes.c_double), ("status", ctypes.c_int32), ("device", ctypes.c_int32),
                 ("h2d_bytes", ctypes.c_int64), ("d2h_bytes", ctypes.c_int64), ("dense_tail", ctypes.c_int64),
-                ("levels_l", ctypes.c_int64), ("levels_u", ctypes.c_int64)]
+                ("levels_l", ctypes.c_int64), ("levels_u", ctypes.c_int64),
+                ("ms_create_upload", ctypes.c_double), ("ms_create_tables", ctypes.c_double),
+                ("ms_create_order", ctypes.c_double), ("tri_cycles", ctypes.c_int64 * 8)]
 
     def as_dict(self) -> dict:
-        return {name: getattr(self, name) for name, _ in self._fields_}
-
+        d = {name: getattr(self, name) for name, _ in self._fields_}
+        d["tri_cycles"] = list(self.tri_cycles)
+        return d
 
 _INT_FIELDS = ("_id", "_type", "frac0", "frac1", "ncoef", "nint")
 

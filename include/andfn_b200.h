@@ -90,6 +90,10 @@ typedef struct AndfnSolveStats {
   int64_t dense_tail;    /* pivot steps solved as a dense trailing block  */
   int64_t levels_l;      /* dependency levels of the sparse part of L     */
   int64_t levels_u;      /* dependency levels of the sparse part of U     */
+  double ms_create_upload, ms_create_tables, ms_create_order; /* handle creation phases */
+  int64_t tri_cycles[8]; /* SM cycles of the discharge-solve phases, summed over iterations:
+                            head vector, L sparse, L coupling, L dense, U dense,
+                            U coupling, U sparse, scatter */
 } AndfnSolveStats;
 
 /* ---- one-call drop-in (replaces andfn/hpc/hpc_solve.py:55 solve) --------
