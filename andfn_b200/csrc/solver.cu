@@ -619,6 +619,7 @@ struct LevelSolve {
   const double *scale;  // [nslots] per-slot multiplier (1/U(i,i)) or null
   int nlev;
   int nslots;           // rows in this solve (rows[] has nslots, eptr[] nslots + 1 entries)
+  int group;            // lanes per row: 8, 16 or 32
 };
 
 static constexpr int PF = 4;  // factor entries per lane kept in registers
@@ -636,47 +637,79 @@ struct SlotMeta {
   const int *rows, *eptr;
 };
 
-__device__ __forceinline__ void load_row(RowRegs &r, const LevelSolve &F, const SlotMeta &M, int slot, int lane) {
-  r.row = M.rows[slot];
-  r.beg = M.eptr[slot];
-  r.end = M.eptr[slot + 1];
-  r.scale = F.scale ? __ldg(F.scale + slot) : 1.0;
+// A row is handled by a group of G lanes (G = 8, 16 or 32, chosen per factor
+// part from its mean row length), so one warp solves 32/G rows of a level at
+// once and every group keeps its row's first G*PF entries in registers.
+template <int G>
+__device__ __forceinline__ void load_row(RowRegs &r, const LevelSolve &F, const SlotMeta &M, int slot, bool valid,
+                                         int sub) {
+  r.row = valid ? M.rows[slot] : 0;
+  r.beg = valid ? M.eptr[slot] : 0;
+  r.end = valid ? M.eptr[slot + 1] : 0;
+  r.scale = (valid && F.scale) ? __ldg(F.scale + slot) : 1.0;
 #pragma unroll
   for (int k = 0; k < PF; k++) {
-    const int p = r.beg + lane + 32 * k;
+    const int p = r.beg + sub + G * k;
     r.c[k] = (p < r.end) ? __ldg(F.col + p) : 0;
     r.v[k] = (p < r.end) ? __ldg(F.val + p) : 0.0;
   }
 }
 
-__device__ __forceinline__ void solve_row(const RowRegs &r, const LevelSolve &F, int slot, int lane, double *y) {
+template <int G>
+__device__ __forceinline__ void solve_row(const RowRegs &r, const LevelSolve &F, bool valid, int sub, double *y) {
   double s = 0.0;
 #pragma unroll
   for (int k = 0; k < PF; k++) s = fma(r.v[k], y[r.c[k]], s);
-  int p = r.beg + 32 * PF + lane;
-  for (; p + 96 < r.end; p += 128) {  // long rows: four independent loads in flight
-    const double v0 = __ldg(F.val + p), v1 = __ldg(F.val + p + 32), v2 = __ldg(F.val + p + 64),
-                 v3 = __ldg(F.val + p + 96);
-    const int c0 = __ldg(F.col + p), c1 = __ldg(F.col + p + 32), c2 = __ldg(F.col + p + 64),
-              c3 = __ldg(F.col + p + 96);
+  int p = r.beg + G * PF + sub;
+  for (; p + 3 * G < r.end; p += 4 * G) {  // long rows: four independent loads in flight
+    const double v0 = __ldg(F.val + p), v1 = __ldg(F.val + p + G), v2 = __ldg(F.val + p + 2 * G),
+                 v3 = __ldg(F.val + p + 3 * G);
+    const int c0 = __ldg(F.col + p), c1 = __ldg(F.col + p + G), c2 = __ldg(F.col + p + 2 * G),
+              c3 = __ldg(F.col + p + 3 * G);
     s = fma(v0, y[c0], s);
     s = fma(v1, y[c1], s);
     s = fma(v2, y[c2], s);
     s = fma(v3, y[c3], s);
   }
-  for (; p < r.end; p += 32) s = fma(__ldg(F.val + p), y[__ldg(F.col + p)], s);
-  s = warp_sum(s);
-  if (lane == 0) y[r.row] = (y[r.row] - s) * r.scale;
+  for (; p < r.end; p += G) s = fma(__ldg(F.val + p), y[__ldg(F.col + p)], s);
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (valid && sub == 0) y[r.row] = (y[r.row] - s) * r.scale;
+}
+
+// Rows of one level beyond the first ng: every group walks its extra slots
+// with the next row's loads in flight.  The loop count is uniform across a
+// warp (groups past the end are predicated off) so the shuffles stay
+// converged.
+template <int G>
+__device__ __forceinline__ void extra_rows(const LevelSolve &F, const SlotMeta &M, int r0, int r1, int gid, int ng,
+                                           int sub, double *y) {
+  const int first = r0 + gid + ng;
+  const int wfirst = r0 + (gid - gid % (32 / G)) + ng;  // first group of this warp
+  const int cnt = (r1 > wfirst) ? (r1 - wfirst + ng - 1) / ng : 0;
+  if (cnt == 0) return;
+  RowRegs t0, t1;
+  load_row<G>(t0, F, M, first, first < r1, sub);
+  for (int k = 0; k < cnt; k++) {
+    const int slot = first + k * ng;
+    const bool nxt = k + 1 < cnt;
+    if (nxt) load_row<G>(t1, F, M, slot + ng, slot + ng < r1, sub);
+    solve_row<G>(t0, F, slot < r1, sub, y);
+    if (!nxt) break;
+    t0 = t1;
+  }
 }
 
 // One triangular solve, level by level with a block barrier between levels.
-// Each warp keeps the factor row of its first slot of the next two levels in
-// registers (loads issued two levels ahead), so the global-memory latency
-// overlaps two barrier waits.  s_meta holds (row, entry start) per slot when
-// there is room (meta_cap >= N + 1 ints each).
-__device__ void level_solve(const LevelSolve &F, double *y, int *s_levptr, int cap_levptr, int *s_meta,
-                            int meta_cap) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+// Levels are processed in pairs: registers a hold each group's first row of
+// the even levels, b of the odd levels, each refilled two levels ahead right
+// after it is consumed.  s_meta holds (row, entry start) per slot when there
+// is room (meta_cap >= nslots + 1 ints each).
+template <int G>
+__device__ void level_solve_g(const LevelSolve &F, double *y, int *s_levptr, int cap_levptr, int *s_meta,
+                              int meta_cap) {
+  const int lane = threadIdx.x & 31, sub = lane % G;
+  const int gid = threadIdx.x / G, ng = blockDim.x / G;
   const bool lev_in_smem = F.nlev + 1 <= cap_levptr;
   const bool meta_in_smem = F.nslots + 1 <= meta_cap;
   __syncthreads();
@@ -689,72 +722,50 @@ __device__ void level_solve(const LevelSolve &F, double *y, int *s_levptr, int c
   __syncthreads();
   const int *lp = lev_in_smem ? s_levptr : F.lev_ptr;
   SlotMeta M{meta_in_smem ? s_meta : F.rows, meta_in_smem ? s_meta + meta_cap : F.eptr};
-  // Levels are processed in pairs: registers a hold the first row of even
-  // levels, b of odd levels; each is refilled two levels ahead right after it
-  // is consumed, so no register copy waits on loads in flight.
   RowRegs a, b;
   bool ha = false, hb = false;
-  if (F.nlev > 0 && lp[0] + warp < lp[1]) {
-    load_row(a, F, M, lp[0] + warp, lane);
-    ha = true;
+  if (F.nlev > 0) {
+    ha = lp[0] + gid < lp[1];
+    load_row<G>(a, F, M, lp[0] + gid, ha, sub);
   }
-  if (F.nlev > 1 && lp[1] + warp < lp[2]) {
-    load_row(b, F, M, lp[1] + warp, lane);
-    hb = true;
+  if (F.nlev > 1) {
+    hb = lp[1] + gid < lp[2];
+    load_row<G>(b, F, M, lp[1] + gid, hb, sub);
   }
   for (int l = 0; l < F.nlev; l += 2) {
     {
       const int r0 = lp[l], r1 = lp[l + 1];
-      if (ha) solve_row(a, F, r0 + warp, lane, y);
-      // a level with more rows than warps: rows loaded one ahead
-      int slot = r0 + warp + nw;
-      if (slot < r1) {
-        RowRegs t0, t1;
-        load_row(t0, F, M, slot, lane);
-        for (; slot < r1; slot += 2 * nw) {
-          const bool more = slot + nw < r1;
-          if (more) load_row(t1, F, M, slot + nw, lane);
-          solve_row(t0, F, slot, lane, y);
-          if (!more) break;
-          const bool more2 = slot + 2 * nw < r1;
-          if (more2) load_row(t0, F, M, slot + 2 * nw, lane);
-          solve_row(t1, F, slot + nw, lane, y);
-          if (!more2) break;
-        }
-      }
+      solve_row<G>(a, F, ha, sub, y);
+      extra_rows<G>(F, M, r0, r1, gid, ng, sub, y);
       ha = false;
-      if (l + 2 < F.nlev && lp[l + 2] + warp < lp[l + 3]) {
-        load_row(a, F, M, lp[l + 2] + warp, lane);
-        ha = true;
+      if (l + 2 < F.nlev) {
+        ha = lp[l + 2] + gid < lp[l + 3];
+        load_row<G>(a, F, M, lp[l + 2] + gid, ha, sub);
       }
       __syncthreads();
     }
     if (l + 1 < F.nlev) {
       const int r0 = lp[l + 1], r1 = lp[l + 2];
-      if (hb) solve_row(b, F, r0 + warp, lane, y);
-      int slot = r0 + warp + nw;
-      if (slot < r1) {
-        RowRegs t0, t1;
-        load_row(t0, F, M, slot, lane);
-        for (; slot < r1; slot += 2 * nw) {
-          const bool more = slot + nw < r1;
-          if (more) load_row(t1, F, M, slot + nw, lane);
-          solve_row(t0, F, slot, lane, y);
-          if (!more) break;
-          const bool more2 = slot + 2 * nw < r1;
-          if (more2) load_row(t0, F, M, slot + 2 * nw, lane);
-          solve_row(t1, F, slot + nw, lane, y);
-          if (!more2) break;
-        }
-      }
+      solve_row<G>(b, F, hb, sub, y);
+      extra_rows<G>(F, M, r0, r1, gid, ng, sub, y);
       hb = false;
-      if (l + 3 < F.nlev && lp[l + 3] + warp < lp[l + 4]) {
-        load_row(b, F, M, lp[l + 3] + warp, lane);
-        hb = true;
+      if (l + 3 < F.nlev) {
+        hb = lp[l + 3] + gid < lp[l + 4];
+        load_row<G>(b, F, M, lp[l + 3] + gid, hb, sub);
       }
       __syncthreads();
     }
   }
+}
+
+__device__ void level_solve(const LevelSolve &F, double *y, int *s_levptr, int cap_levptr, int *s_meta,
+                            int meta_cap) {
+  if (F.group == 8)
+    level_solve_g<8>(F, y, s_levptr, cap_levptr, s_meta, meta_cap);
+  else if (F.group == 16)
+    level_solve_g<16>(F, y, s_levptr, cap_levptr, s_meta, meta_cap);
+  else
+    level_solve_g<32>(F, y, s_levptr, cap_levptr, s_meta, meta_cap);
 }
 
 // Head vector b (build_head_matrix, hpc_solve.py:811-829): the mean of the
@@ -1336,6 +1347,7 @@ struct AndfnHandle {
   DBuf<int> lx_lev, lx_rows, lx_eptr, lx_col, ux_lev, ux_rows, ux_eptr, ux_col;
   DBuf<double> lx_val, ux_val;
   int lx_nlev = 0, ux_nlev = 0;
+  int g_lf = 32, g_ub = 32, g_lx = 32, g_ux = 32;  // lanes per row of each part
   int tail_k = 0;
   DBuf<double> tail_l, tail_u, tail_uinv;
   int64_t nnz_factors = 0;
@@ -1983,13 +1995,25 @@ static void build_levels(int n, const std::vector<int> &ptr, const std::vector<i
   }
 }
 
+// Lanes per factor row: the smallest group whose registers hold a mean row.
+static int group_for(const std::vector<int> &eptr) {
+  const int n = (int)eptr.size() - 1;
+  const double mean = n > 0 ? (double)eptr[n] / n : 0.0;
+  if (mean <= 8.0 * PF) return 8;
+  if (mean <= 16.0 * PF) return 16;
+  return 32;
+}
+
 static void launch_trisolve(AndfnHandle *H, cudaStream_t s) {
   Net net = H->net();
   const int m0 = H->N - H->tail_k;
-  LevelSolve Lf{H->lf_lev.p, H->lf_rows.p, H->lf_eptr.p, H->lf_col.p, H->lf_val.p, nullptr, H->lf_nlev, m0};
-  LevelSolve Ub{H->ub_lev.p, H->ub_rows.p, H->ub_eptr.p, H->ub_col.p, H->ub_val.p, H->ub_scale.p, H->ub_nlev, m0};
-  LevelSolve Lx{H->lx_lev.p, H->lx_rows.p, H->lx_eptr.p, H->lx_col.p, H->lx_val.p, nullptr, H->lx_nlev, H->tail_k};
-  LevelSolve Ux{H->ux_lev.p, H->ux_rows.p, H->ux_eptr.p, H->ux_col.p, H->ux_val.p, nullptr, H->ux_nlev, m0};
+  LevelSolve Lf{H->lf_lev.p, H->lf_rows.p, H->lf_eptr.p, H->lf_col.p, H->lf_val.p, nullptr, H->lf_nlev, m0, H->g_lf};
+  LevelSolve Ub{H->ub_lev.p, H->ub_rows.p, H->ub_eptr.p, H->ub_col.p, H->ub_val.p, H->ub_scale.p, H->ub_nlev, m0,
+                H->g_ub};
+  LevelSolve Lx{H->lx_lev.p, H->lx_rows.p, H->lx_eptr.p, H->lx_col.p, H->lx_val.p, nullptr, H->lx_nlev, H->tail_k,
+                H->g_lx};
+  LevelSolve Ux{H->ux_lev.p, H->ux_rows.p, H->ux_eptr.p, H->ux_col.p, H->ux_val.p, nullptr, H->ux_nlev, m0,
+                H->g_ux};
   DenseTail T{H->tail_k, H->tail_l.p, H->tail_u.p, H->tail_uinv.p};
   const size_t ybytes = sizeof(double) * (size_t)H->N;
   const int use_smem = ybytes <= 150 * 1024;
@@ -2251,6 +2275,7 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
     build_levels(n, LU.l_ptr, LU.l_col, LU.l_val, nullptr, true, 0, m0, 0, m0, false, lev, rows, eptr, ecol, ev,
                  esc);
     H->lf_nlev = (int)lev.size() - 1;
+    H->g_lf = group_for(eptr);
     CK(upload(H->lf_lev, lev, s));
     CK(upload(H->lf_rows, rows, s));
     CK(upload(H->lf_eptr, eptr, s));
@@ -2260,6 +2285,7 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
     build_levels(n, LU.u_ptr, LU.u_col, LU.u_val, &LU.u_inv_diag, false, 0, m0, 0, m0, false, lev, rows, eptr,
                  ecol, ev, esc);
     H->ub_nlev = (int)lev.size() - 1;
+    H->g_ub = group_for(eptr);
     CK(upload(H->ub_lev, lev, s));
     CK(upload(H->ub_rows, rows, s));
     CK(upload(H->ub_eptr, eptr, s));
@@ -2271,6 +2297,7 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
       build_levels(n, LU.l_ptr, LU.l_col, LU.l_val, nullptr, true, m0, n, 0, m0, true, lev, rows, eptr, ecol, ev,
                    esc);
       H->lx_nlev = (int)lev.size() - 1;
+      H->g_lx = group_for(eptr);
       CK(upload(H->lx_lev, lev, s));
       CK(upload(H->lx_rows, rows, s));
       CK(upload(H->lx_eptr, eptr, s));
@@ -2280,6 +2307,7 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
       build_levels(n, LU.u_ptr, LU.u_col, LU.u_val, nullptr, false, 0, m0, m0, n, true, lev, rows, eptr, ecol, ev,
                    esc);
       H->ux_nlev = (int)lev.size() - 1;
+      H->g_ux = group_for(eptr);
       CK(upload(H->ux_lev, lev, s));
       CK(upload(H->ux_rows, rows, s));
       CK(upload(H->ux_eptr, eptr, s));

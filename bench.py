@@ -253,11 +253,7 @@ def run_gpu(args):
     kt = solver.kernel_times()
     clk = clocks.stop()
     total_ms = float(np.sum(step_ms))
-    if ws > 1:
-        t = torch.tensor([total_ms], device=f"cuda:{device}", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = ws * args.steps / (total_ms / 1e3)
+    total_ms, value = aggregate_ranks(total_ms, args.steps, ws, f"cuda:{device}")
     # e2e: one-call C ABI from host records
     e2e_ms = []
     h2d = d2h = 0
@@ -320,6 +316,19 @@ def run_gpu(args):
     solver.close()
     if ws > 1:
         torch.distributed.destroy_process_group()
+
+
+def aggregate_ranks(total_ms: float, steps: int, world_size: int, device=None) -> tuple[float, float]:
+    """Slowest rank's timed milliseconds (all-reduce MAX) and the whole-job
+    value: every rank solves its own network, so value = world_size * steps
+    / max time."""
+    if world_size > 1:
+        import torch
+        import torch.distributed as dist
+        t = torch.tensor([total_ms], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    return total_ms, world_size * steps / (total_ms / 1e3)
 
 
 def ctypes_double():
