@@ -11,6 +11,7 @@ from .hpc_solve import last_stats, solve
 from .records import (AndfnConstants, AndfnLayout, AndfnSolveStats, constants_dtype, default_constants,
                       element_dtype, fracture_dtype, layout_of)
 from .solver import Solver
+from .batch import BatchSolver, solve_batch
 
 __version__ = "0.1.0"
 
@@ -31,6 +32,6 @@ def uninstall():
         dfn_mod.hpc_solve = _saved.pop("hpc_solve")
 
 
-__all__ = ["solve", "install", "uninstall", "Solver", "last_stats", "element_dtype", "fracture_dtype",
+__all__ = ["solve", "install", "uninstall", "Solver", "BatchSolver", "solve_batch", "last_stats", "element_dtype", "fracture_dtype",
            "constants_dtype", "default_constants", "layout_of", "AndfnLayout", "AndfnConstants",
            "AndfnSolveStats"]

@@ -16,7 +16,9 @@ LIB_PATH = os.path.join(HERE, "libandfn_b200.so")
 EXPORTS = ("andfn_b200_solve", "andfn_b200_create", "andfn_b200_upload_state", "andfn_b200_reset_state",
            "andfn_b200_run", "andfn_b200_download", "andfn_b200_eval_heads", "andfn_b200_eval_omega",
            "andfn_b200_destroy", "andfn_b200_stream", "andfn_b200_last_error", "andfn_b200_version",
-           "andfn_b200_set_profiling", "andfn_b200_kernel_times", "andfn_b200_fp64_peak")
+           "andfn_b200_set_profiling", "andfn_b200_kernel_times", "andfn_b200_fp64_peak",
+           "andfn_b200_batch_solve", "andfn_b200_batch_create", "andfn_b200_batch_run",
+           "andfn_b200_batch_download", "andfn_b200_batch_eval_heads", "andfn_b200_realizations")
 
 STATUS = {0: "ok", 1: "max_iterations", 2: "nonfinite", 3: "singular", 10: "bad_layout", 11: "bad_input",
           12: "cuda_error", 13: "no_device", 14: "out_of_memory"}
@@ -58,6 +60,12 @@ def lib() -> ctypes.CDLL:
         ("andfn_b200_set_profiling", ctypes.c_int, [P, ctypes.c_int]),
         ("andfn_b200_kernel_times", ctypes.c_int, [P, P, P, ctypes.c_int]),
         ("andfn_b200_fp64_peak", ctypes.c_int, [I32, P]),
+        ("andfn_b200_batch_solve", ctypes.c_int, [I64, P, P, P, P, LP, I64, CP, P]),
+        ("andfn_b200_batch_create", ctypes.c_int, [ctypes.POINTER(P), I64, P, P, P, P, LP, I64, I32]),
+        ("andfn_b200_batch_run", ctypes.c_int, [P, CP, P]),
+        ("andfn_b200_batch_download", ctypes.c_int, [P, P, P]),
+        ("andfn_b200_batch_eval_heads", ctypes.c_int, [P, I64, P, P, I64, P]),
+        ("andfn_b200_realizations", I64, [P]),
     ):
         fn = getattr(L, name)
         fn.restype = res

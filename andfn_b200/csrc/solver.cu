@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -74,6 +75,8 @@ struct SolveState {
   long long tri_cycles[8];
 };
 
+struct TriDesc;
+
 // Device view of one network.
 struct Net {
   int ne, nf, n_de, N, MC, D;
@@ -104,7 +107,19 @@ struct Net {
   double *work;  // [N] scratch (solve in global memory when N is large)
   double *bvec;  // [N] head vector of the current iteration
   int *ready;    // [N]
-  SolveState *st;
+  // Several independent networks (realizations) can share one launch: every
+  // element, fracture and discharge-system row knows its realization, each
+  // realization has its own loop state and its own factorised system.
+  int R;
+  SolveState *st;            // [R]
+  const int *real_elem;      // [ne]
+  const int *real_frac;      // [nf]
+  const int *real_row;       // [N]
+  const int *eoff;           // [R + 1] element range of each realization
+  const int *row_de;         // [N] discharge-element index of a row, -1 for continuity rows
+  const int *row_frac;       // [N] fracture of a continuity row, -1 otherwise
+  int *ndone;                // realizations whose loop has finished
+  const struct TriDesc *tri; // [R]
 };
 
 // ------------------------------------------------------------------------
@@ -162,7 +177,8 @@ __global__ void __launch_bounds__(EVAL_THREADS) eval_kernel(Net net, const Item 
                                                               const int2 *__restrict__ pts,
                                                               const Group *__restrict__ groups,
                                                               double *__restrict__ out, int chunk) {
-  const SolveState *st = net.st;
+  const Item it = items[blockIdx.x];
+  const SolveState *st = net.st + net.real_frac[it.frac];
   if (st->done) return;
   if (RHS && !st->solve_q) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -170,7 +186,6 @@ __global__ void __launch_bounds__(EVAL_THREADS) eval_kernel(Net net, const Item 
   cd *scoef = reinterpret_cast<cd *>(smem_raw + sizeof(Src) * chunk);
   const int MC = net.MC;
 
-  const Item it = items[blockIdx.x];
   const int p = it.p0 + threadIdx.x;
   const bool active = p < it.p1;
   cd z = mk(0.0, 0.0);
@@ -334,8 +349,6 @@ __global__ void __launch_bounds__(UPDATE_WARPS * 32) update_kernel(Net net, cons
                                                                     const Group *__restrict__ groups,
                                                                     const double *__restrict__ vals, int nvmax,
                                                                     int blend_mode) {
-  SolveState *st = net.st;
-  if (st->done) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double *v0 = reinterpret_cast<double *>(smem_raw) + (size_t)warp * 2 * nvmax;
@@ -343,6 +356,8 @@ __global__ void __launch_bounds__(UPDATE_WARPS * 32) update_kernel(Net net, cons
   const int idx = blockIdx.x * UPDATE_WARPS + warp;
   if (idx >= nlist) return;
   const int e = elist[idx];
+  SolveState *st = net.st + net.real_elem[e];
+  if (st->done) return;
   const int type = net.type[e];
   const int MC = net.MC;
   if (type == 2) {  // hpc_solve.py:366-368
@@ -458,11 +473,11 @@ __global__ void __launch_bounds__(UPDATE_WARPS * 32) update_kernel(Net net, cons
 // ------------------------------------------------------------------------
 __global__ void growth_kernel(Net net, const int *__restrict__ elist, int nlist, double max_coef_ratio,
                               int max_coef, int coef_increase, int *grow_list, int *grow_count) {
-  const SolveState *st = net.st;
-  if (st->done) return;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (warp >= nlist || lane != 0) return;
   const int e = elist[warp];
+  const SolveState *st = net.st + net.real_elem[e];
+  if (st->done) return;
   if (net.type[e] == 2) return;
   const int nit = st->nit;
   if (nit < 2) return;
@@ -504,13 +519,13 @@ __global__ void growth_kernel(Net net, const int *__restrict__ elist, int nlist,
 
 // Second damped blend of element_solver2 (hpc_solve.py:561-575), nit >= 2.
 __global__ void blend2_kernel(Net net) {
-  const SolveState *st = net.st;
-  if (st->done || st->nit < 2) return;
-  const double d = st->damping;
   const long long tot = (long long)net.ne * net.MC;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < tot; i += (long long)gridDim.x * blockDim.x) {
     const int e = (int)(i / net.MC), j = (int)(i - (long long)e * net.MC);
     if (j >= net.ncoef[e]) continue;
+    const SolveState *st = net.st + net.real_elem[e];
+    if (st->done || st->nit < 2) continue;
+    const double d = st->damping;
     const cd w = net.wcoef[i], c = net.coef[i];
     net.coef[i] = mk(d * w.re + (1 - d) * c.re, d * w.im + (1 - d) * c.im);
   }
@@ -520,13 +535,15 @@ __global__ void blend2_kernel(Net net) {
 // Max-reductions of the element errors and the convergence rule.
 // ------------------------------------------------------------------------
 __global__ void __launch_bounds__(1024) reduce_kernel(Net net) {
-  SolveState *st = net.st;
+  const int r = blockIdx.x;
+  SolveState *st = net.st + r;
   if (st->done) return;
   __shared__ double s_err[32], s_ec[32];
   __shared__ int s_idx[32], s_nf[32];
   double best = -INFINITY, bec = -INFINITY;
   int bidx = 0x7fffffff, nonfin = 0;
-  for (int i = threadIdx.x; i < net.ne; i += blockDim.x) {
+  const int e0 = net.eoff[r], e1 = net.eoff[r + 1];
+  for (int i = e0 + threadIdx.x; i < e1; i += blockDim.x) {
     double e = net.err[i], ec = net.err_coef[i];
     if (!(e == e)) {  // NaN wins (np.max / np.argmax semantics)
       if (best == best || i < bidx) {
@@ -587,7 +604,7 @@ __global__ void __launch_bounds__(1024) reduce_kernel(Net net) {
       nf |= s_nf[k];
     }
     st->error = b;
-    st->worst = bi;
+    st->worst = bi - e0;
     st->error_coef = ec;
     if (!(st->error_q == st->error_q)) nf = 1;
     if (nf) st->nonfinite = 1;
@@ -596,7 +613,10 @@ __global__ void __launch_bounds__(1024) reduce_kernel(Net net) {
       st->cnt_error += 1;
       st->error_q = 1e30;
     }
-    if (st->cnt_error >= 2 || st->nit >= st->max_it || st->nonfinite) st->done = 1;
+    if (st->cnt_error >= 2 || st->nit >= st->max_it || st->nonfinite) {
+      st->done = 1;
+      atomicAdd(net.ndone, 1);
+    }
     st->solve_q = (st->error_q > st->max_error / 1e30) ? 1 : 0;
   }
 }
@@ -773,12 +793,13 @@ __device__ void level_solve(const LevelSolve &F, double *y, int *s_levptr, int c
 // warp per row, lanes over the points.  Continuity rows are zero.
 __global__ void rhs_reduce_kernel(Net net, const double *__restrict__ rhs_vals, const int *__restrict__ rhs_group,
                                   const Group *__restrict__ groups) {
-  const SolveState *st = net.st;
+  const int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (g >= net.N) return;
+  const SolveState *st = net.st + net.real_row[g];
   if (st->done || !st->solve_q) return;
-  const int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  if (r >= net.N) return;
-  if (r >= net.n_de) {
-    if (lane == 0) net.bvec[r] = 0.0;
+  const int r = net.row_de[g];
+  if (r < 0) {
+    if (lane == 0) net.bvec[g] = 0.0;
     return;
   }
   const int D = net.D;
@@ -792,9 +813,9 @@ __global__ void rhs_reduce_kernel(Net net, const double *__restrict__ rhs_vals, 
     double s1 = 0.0;
     for (int k = lane; k < D; k += 32) s1 += rhs_vals[g1.out + k];
     s1 = warp_sum(s1);
-    if (lane == 0) net.bvec[r] = (s1 / D) / net.t[net.frac1[e]] - (s0 / D) / net.t[net.frac0[e]];
+    if (lane == 0) net.bvec[g] = (s1 / D) / net.t[net.frac1[e]] - (s0 / D) / net.t[net.frac0[e]];
   } else if (lane == 0) {
-    net.bvec[r] = net.phi[e] - s0 / D;
+    net.bvec[g] = net.phi[e] - s0 / D;
   }
 }
 
@@ -872,18 +893,28 @@ struct DenseTail {
   const double *uinv;  // [K] 1 / U(i,i)
 };
 
-__global__ void __launch_bounds__(SOLVE_THREADS) trisolve_kernel(Net net, const double *__restrict__ rhs_vals,
-                                                                  const int *__restrict__ rhs_group,
-                                                                  const Group *__restrict__ groups, int use_smem,
-                                                                  LevelSolve Lf, LevelSolve Lx, LevelSolve Ux,
-                                                                  LevelSolve Ub, DenseTail T, int cap_levptr,
+// The factorised discharge system of one realization (its rows are the
+// global rows row0 .. row0 + n - 1; all indices inside are local).
+struct TriDesc {
+  LevelSolve Lf, Lx, Ux, Ub;
+  DenseTail T;
+  const int *pinv;  // [n] row -> pivot step
+  const int *qcol;  // [n] pivot step -> column
+  int row0, n;
+};
+
+__global__ void __launch_bounds__(SOLVE_THREADS) trisolve_kernel(Net net, int use_smem, int cap_levptr,
                                                                   int meta_cap) {
-  SolveState *st = net.st;
+  const int r = blockIdx.x;
+  SolveState *st = net.st + r;
   if (st->done) return;
+  const TriDesc &TD = net.tri[r];
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int N = net.N, n_de = net.n_de;
-  double *y = use_smem ? reinterpret_cast<double *>(smem_raw) : net.work;
-  int *s_levptr = reinterpret_cast<int *>(smem_raw + (use_smem ? sizeof(double) * (size_t)N : 0));
+  const int N = TD.n, row0 = TD.row0;
+  size_t ycap = 0;
+  if (use_smem) ycap = (size_t)use_smem;
+  double *y = use_smem ? reinterpret_cast<double *>(smem_raw) : net.work + row0;
+  int *s_levptr = reinterpret_cast<int *>(smem_raw + sizeof(double) * ycap);
   int *s_meta = s_levptr + cap_levptr;
   if (threadIdx.x == 0) st->nit += 1;
   if (!st->solve_q) return;  // uniform: solve_q is written only by reduce_kernel
@@ -897,30 +928,30 @@ __global__ void __launch_bounds__(SOLVE_THREADS) trisolve_kernel(Net net, const 
     }
   };
   // y = P b (b from rhs_reduce_kernel)
-  for (int r = threadIdx.x; r < N; r += blockDim.x) y[net.pinv[r]] = net.bvec[r];
+  for (int i = threadIdx.x; i < N; i += blockDim.x) y[TD.pinv[i]] = net.bvec[row0 + i];
   phase(0);
   // L: sparse leading rows, coupling of the trailing rows to them, dense tail
-  level_solve(Lf, y, s_levptr, cap_levptr, s_meta, meta_cap);
+  level_solve(TD.Lf, y, s_levptr, cap_levptr, s_meta, meta_cap);
   phase(1);
-  if (T.K > 0) {
-    level_solve(Lx, y, s_levptr, cap_levptr, s_meta, meta_cap);
+  if (TD.T.K > 0) {
+    level_solve(TD.Lx, y, s_levptr, cap_levptr, s_meta, meta_cap);
     phase(2);
-    dense_lower_solve(T.L, T.K, y + (N - T.K));
+    dense_lower_solve(TD.T.L, TD.T.K, y + (N - TD.T.K));
     phase(3);
     // U: dense tail, coupling of the leading rows to it, sparse leading rows
-    dense_upper_solve(T.U, T.uinv, T.K, y + (N - T.K));
+    dense_upper_solve(TD.T.U, TD.T.uinv, TD.T.K, y + (N - TD.T.K));
     phase(4);
-    level_solve(Ux, y, s_levptr, cap_levptr, s_meta, meta_cap);
+    level_solve(TD.Ux, y, s_levptr, cap_levptr, s_meta, meta_cap);
     phase(5);
   }
-  level_solve(Ub, y, s_levptr, cap_levptr, s_meta, meta_cap);  // scale = 1/U(i,i)
+  level_solve(TD.Ub, y, s_levptr, cap_levptr, s_meta, meta_cap);  // scale = 1/U(i,i)
   phase(6);
   // x = Q y; error_q = max|x - x_old| / (max|x_old| + 1e-16) (hpc_solve.py:169-174)
   __shared__ double s_d[32], s_o[32];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   double md = 0.0, mo = 0.0;
   for (int k = threadIdx.x; k < N; k += blockDim.x) {
-    const int c = net.qcol[k];
+    const int c = row0 + TD.qcol[k];
     const double xv = y[k];
     const double xo = net.disc[c];
     double dd = fabs(xv - xo);
@@ -930,13 +961,14 @@ __global__ void __launch_bounds__(SOLVE_THREADS) trisolve_kernel(Net net, const 
   }
   __syncthreads();
   for (int k = threadIdx.x; k < N; k += blockDim.x) {
-    const int c = net.qcol[k];
+    const int c = row0 + TD.qcol[k];
     const double xv = y[k];
     net.disc[c] = xv;
-    if (c < n_de)
-      net.q[net.de_ids[c]] = xv;
+    const int d = net.row_de[c];
+    if (d >= 0)
+      net.q[net.de_ids[d]] = xv;
     else
-      net.constant[c - n_de] = xv;
+      net.constant[net.row_frac[c]] = xv;
   }
   for (int o = 16; o > 0; o >>= 1) {
     md = fmax(md, __shfl_xor_sync(0xffffffffu, md, o));
@@ -1085,7 +1117,7 @@ __global__ void cuts_kernel(Net net, const int *__restrict__ elist, int nlist) {
               if (type != 1) sg = (chi0.im < chi1.im) ? -1 * sdef : sdef;  // get_sign
               net.cut_sign[o] = sg;
             } else {
-              atomicExch(&net.st->status, (int)ANDFN_BAD_INPUT);
+              atomicExch(&net.st[net.real_elem[e]].status, (int)ANDFN_BAD_INPUT);
             }
           }
         }
@@ -1183,7 +1215,8 @@ __global__ void matrix_values_kernel(Net net, const int *__restrict__ ent_row, c
   const int lane = threadIdx.x & 31;
   if (w >= nent) return;
   const int kind = ent_kind[w];
-  const int j = ent_row[w];
+  const int g = ent_row[w];   // global row
+  const int j = net.row_de[g];  // discharge-element index (-1 for continuity rows)
   if (kind == 1) {  // fracture-constant column: 1/t0, -1/t1 (intersections) or 1
     if (lane == 0) {
       const int e = net.de_ids[j];
@@ -1198,7 +1231,7 @@ __global__ void matrix_values_kernel(Net net, const int *__restrict__ ent_row, c
   if (kind == 2) {  // continuity row: +1 / -1
     if (lane == 0) {
       const int el = ent_src[w];
-      const int f = j - net.n_de;
+      const int f = net.row_frac[g];
       vals[w] = (net.type[el] != 0 || net.frac0[el] == f) ? 1.0 : -1.0;
     }
     return;
@@ -1297,7 +1330,7 @@ struct DBuf {
 };
 
 struct HostNet {
-  // element SoA (host copies of the geometry and of the initial state)
+  // element SoA of all realizations (host copies of the geometry and of the initial state)
   std::vector<int> type, frac0, frac1, ncoef, nint;
   std::vector<cd> ep0, ep1, center;
   std::vector<double> radius, phi, q, err, err_old, err_old2, err_coef;
@@ -1305,6 +1338,28 @@ struct HostNet {
   std::vector<double> t, constant;
   std::vector<int> fptr, felem;
   std::vector<int> de_ids, elem_de;
+  // realization r owns elements [eoff[r], eoff[r+1]), fractures [foff[r], foff[r+1]),
+  // discharge elements [doff[r], doff[r+1]) and system rows [roff[r], roff[r+1])
+  std::vector<int> eoff, foff, doff, roff;
+  std::vector<int> real_elem, real_frac, real_row, row_de, row_frac;
+};
+
+// Discharge system of one realization (local row / column indices).
+struct RealSys {
+  int n = 0, n_de = 0;
+  std::vector<int> mrow_ptr, mcol;  // CSR pattern (row = equation, col = unknown)
+  int ent0 = 0;                     // first entry in the global assembly arrays
+  std::vector<int> colorder;        // cached symbolic analysis (pattern only)
+  int dense_k = 0;
+  // factor statistics of the last run
+  int tail_k = 0, nlev_l = 0, nlev_u = 0;
+  int64_t nnz = 0;
+};
+
+// Level-ordered factor part of all realizations, concatenated.
+struct LevelParts {
+  std::vector<int> lev, rows, eptr, col;
+  std::vector<double> val, scale;
 };
 
 }  // namespace andfn
@@ -1315,9 +1370,9 @@ struct AndfnHandle {
   int device = 0;
   cudaStream_t stream = nullptr;
   AndfnLayout L;
+  int R = 1;
   int64_t ne = 0, nf = 0, D = 0;
   int MC = 0;  // coefficient capacity (per element, device)
-  int max_nint = 0;
   HostNet h;
   // device arrays
   DBuf<int> type, frac0, frac1, ncoef, nint, ncoef0, nint0;
@@ -1325,31 +1380,28 @@ struct AndfnHandle {
   DBuf<double> radius, phi, q, q0, err, err_old, err_old2, err_coef, err_in, err_old_in, err_old2_in, err_coef_in;
   DBuf<double> dpsi_corr, t, constant, constant0;
   DBuf<int> fptr, felem, de_ids;
+  DBuf<int> real_elem, real_frac, real_row, eoff, row_de, row_frac, ndone;
   DBuf<cd> zint0, zint1;
   DBuf<int> cut_n, cut_pos, cut_elem, cut_sign;
   int cut_cap = 0;
-  // discharge system
-  int N = 0;
-  std::vector<int> mrow_ptr, mcol;  // CSR pattern (row = equation, col = unknown)
+  // discharge systems
+  int N = 0;  // rows of all realizations
+  std::vector<RealSys> sys;
   std::vector<int> ent_row, ent_src, ent_side, ent_kind;
   DBuf<int> d_ent_row, d_ent_src, d_ent_side, d_ent_kind;
   DBuf<double> d_mvals;
-  std::vector<int> colorder;  // cached symbolic analysis (depends on the pattern only)
-  int dense_k = 0;            // trailing pivot steps factorised and solved as a dense block
   double ms_create_upload = 0, ms_create_tables = 0, ms_create_order = 0;
-  DBuf<int> pinv, qcol, l_ptr, l_col, u_ptr, u_col;
-  DBuf<double> l_val, u_val, u_inv, disc, work, bvec;
+  DBuf<double> disc, work, bvec;
   DBuf<int> ready;
-  // level-ordered factors for trisolve_kernel
+  // factors of all realizations (level-ordered parts, dense tails, permutations)
   DBuf<int> lf_lev, lf_rows, lf_eptr, lf_col, ub_lev, ub_rows, ub_eptr, ub_col;
   DBuf<double> lf_val, ub_val, ub_scale;
-  int lf_nlev = 0, ub_nlev = 0;
   DBuf<int> lx_lev, lx_rows, lx_eptr, lx_col, ux_lev, ux_rows, ux_eptr, ux_col;
   DBuf<double> lx_val, ux_val;
-  int lx_nlev = 0, ux_nlev = 0;
-  int g_lf = 32, g_ub = 32, g_lx = 32, g_ux = 32;  // lanes per row of each part
-  int tail_k = 0;
   DBuf<double> tail_l, tail_u, tail_uinv;
+  DBuf<int> pinv, qcol;
+  DBuf<TriDesc> tri;
+  int max_n = 0, max_nlev = 0;
   int64_t nnz_factors = 0;
   // evaluation tables
   std::vector<Group> groups;
@@ -1375,9 +1427,9 @@ struct AndfnHandle {
   int chunk = 0;
   size_t eval_smem = 0;
   DBuf<SolveState> st;
-  SolveState *h_st = nullptr;  // pinned host mirror
+  std::vector<SolveState> h_st;  // host copy of the R loop states
+  int *h_ndone = nullptr;        // pinned
   cudaGraphExec_t graph_exec = nullptr;
-  int graph_fused = -1;
   int solve_threads = SOLVE_THREADS;
   // per-kernel timing: event pairs recorded as graph nodes around every
   // kernel of every captured iteration
@@ -1386,6 +1438,7 @@ struct AndfnHandle {
   double k_ms[KCLASSES] = {};
   int64_t k_n[KCLASSES] = {};
   int64_t launches = 0;
+  std::vector<AndfnSolveStats> last;  // per realization
 
   Net net() const {
     Net n;
@@ -1427,18 +1480,27 @@ struct AndfnHandle {
     n.cut_sign = cut_sign.p;
     n.pinv = pinv.p;
     n.qcol = qcol.p;
-    n.l_ptr = l_ptr.p;
-    n.l_col = l_col.p;
-    n.u_ptr = u_ptr.p;
-    n.u_col = u_col.p;
-    n.l_val = l_val.p;
-    n.u_val = u_val.p;
-    n.u_inv = u_inv.p;
+    n.l_ptr = nullptr;
+    n.l_col = nullptr;
+    n.u_ptr = nullptr;
+    n.u_col = nullptr;
+    n.l_val = nullptr;
+    n.u_val = nullptr;
+    n.u_inv = nullptr;
     n.disc = disc.p;
     n.work = work.p;
     n.bvec = bvec.p;
     n.ready = ready.p;
+    n.R = R;
     n.st = st.p;
+    n.real_elem = real_elem.p;
+    n.real_frac = real_frac.p;
+    n.real_row = real_row.p;
+    n.eoff = eoff.p;
+    n.row_de = row_de.p;
+    n.row_frac = row_frac.p;
+    n.ndone = ndone.p;
+    n.tri = tri.p;
     return n;
   }
   ~AndfnHandle() {
@@ -1447,7 +1509,7 @@ struct AndfnHandle {
       for (auto &c : b)
         for (auto &e : c)
           if (e) cudaEventDestroy(e);
-    if (h_st) cudaFreeHost(h_st);
+    if (h_ndone) cudaFreeHost(h_ndone);
     if (stream) cudaStreamDestroy(stream);
   }
 };
@@ -1489,112 +1551,114 @@ static int check_layout(const AndfnLayout *L) {
   return 0;
 }
 
-// Parses records into host SoA and validates ids.
-static int parse_records(AndfnHandle *H, const char *F, const char *E) {
+// Appends realization r's records to the host SoA (ids shifted by the
+// realization's offsets) and validates them.
+static int parse_records(AndfnHandle *H, int r, const char *F, int64_t nf, const char *E, int64_t ne) {
   const AndfnLayout &L = H->L;
   HostNet &h = H->h;
-  const int64_t ne = H->ne, nf = H->nf;
-  h.type.resize(ne);
-  h.frac0.resize(ne);
-  h.frac1.resize(ne);
-  h.ncoef.resize(ne);
-  h.nint.resize(ne);
-  h.ep0.resize(2 * ne);
-  h.ep1.resize(2 * ne);
-  h.center.resize(ne);
-  h.radius.resize(ne);
-  h.phi.resize(ne);
-  h.q.resize(ne);
-  h.err.resize(ne);
-  h.err_old.resize(ne);
-  h.err_old2.resize(ne);
-  h.err_coef.resize(ne);
+  const int e0 = h.eoff[r], f0 = h.foff[r];
   int maxm = 0;
   for (int64_t i = 0; i < ne; i++) {
-    const char *r = E + i * L.elem_size;
-    if (rd_i64(r, L.e_id) != i) {
+    const char *rec = E + i * L.elem_size;
+    if (rd_i64(rec, L.e_id) != i) {
       set_error("element _id must equal its index (andfn/dfn.py:1062-1063)");
       return ANDFN_BAD_INPUT;
     }
-    int64_t ty = rd_i64(r, L.e_type);
+    int64_t ty = rd_i64(rec, L.e_type);
     if (ty < 0 || ty > 5) {
       set_error("element type out of range");
       return ANDFN_BAD_INPUT;
     }
-    h.type[i] = (int)ty;
-    int64_t f0 = rd_i64(r, L.e_frac0), f1 = rd_i64(r, L.e_frac1);
-    if (f0 < 0 || f0 >= nf || (ty == 0 && (f1 < 0 || f1 >= nf))) {
+    int64_t fa = rd_i64(rec, L.e_frac0), fb = rd_i64(rec, L.e_frac1);
+    if (fa < 0 || fa >= nf || (ty == 0 && (fb < 0 || fb >= nf))) {
       set_error("element fracture id out of range");
       return ANDFN_BAD_INPUT;
     }
-    h.frac0[i] = (int)f0;
-    h.frac1[i] = (ty == 0) ? (int)f1 : -1;
-    int64_t m = rd_i64(r, L.e_ncoef), n = rd_i64(r, L.e_nint);
+    int64_t m = rd_i64(rec, L.e_ncoef), n = rd_i64(rec, L.e_nint);
     if (m < 0 || m > L.max_ncoef || n < 0 || n > 2 * L.max_ncoef || (ty != 2 && (m < 1 || n < 2))) {
       set_error("ncoef/nint out of range for the record capacity");
       return ANDFN_BAD_INPUT;
     }
-    h.ncoef[i] = (int)m;
-    h.nint[i] = (int)n;
+    h.type.push_back((int)ty);
+    h.frac0.push_back(f0 + (int)fa);
+    h.frac1.push_back(ty == 0 ? f0 + (int)fb : -1);
+    h.ncoef.push_back((int)m);
+    h.nint.push_back((int)n);
     maxm = std::max(maxm, (int)m);
-    h.ep0[2 * i] = rd_cd(r, L.e_endpoints0, 0);
-    h.ep0[2 * i + 1] = rd_cd(r, L.e_endpoints0, 1);
-    h.ep1[2 * i] = rd_cd(r, L.e_endpoints1, 0);
-    h.ep1[2 * i + 1] = rd_cd(r, L.e_endpoints1, 1);
-    h.center[i] = rd_cd(r, L.e_center, 0);
-    h.radius[i] = rd_f64(r, L.e_radius);
-    h.phi[i] = rd_f64(r, L.e_phi);
-    h.q[i] = rd_f64(r, L.e_q);
-    h.err[i] = rd_f64(r, L.e_error);
-    h.err_old[i] = rd_f64(r, L.e_error_old);
-    h.err_old2[i] = rd_f64(r, L.e_error_old2);
-    h.err_coef[i] = rd_f64(r, L.e_error_coef);
+    h.ep0.push_back(rd_cd(rec, L.e_endpoints0, 0));
+    h.ep0.push_back(rd_cd(rec, L.e_endpoints0, 1));
+    h.ep1.push_back(rd_cd(rec, L.e_endpoints1, 0));
+    h.ep1.push_back(rd_cd(rec, L.e_endpoints1, 1));
+    h.center.push_back(rd_cd(rec, L.e_center, 0));
+    h.radius.push_back(rd_f64(rec, L.e_radius));
+    h.phi.push_back(rd_f64(rec, L.e_phi));
+    h.q.push_back(rd_f64(rec, L.e_q));
+    h.err.push_back(rd_f64(rec, L.e_error));
+    h.err_old.push_back(rd_f64(rec, L.e_error_old));
+    h.err_old2.push_back(rd_f64(rec, L.e_error_old2));
+    h.err_coef.push_back(rd_f64(rec, L.e_error_coef));
+    h.real_elem.push_back(r);
   }
-  H->MC = std::max(1, maxm);
-  h.t.resize(nf);
-  h.constant.resize(nf);
-  h.fptr.assign(nf + 1, 0);
-  h.felem.clear();
+  H->MC = std::max(H->MC, std::max(1, maxm));
   for (int64_t f = 0; f < nf; f++) {
-    const char *r = F + f * L.frac_size;
-    if (rd_i64(r, L.f_id) != f) {
+    const char *rec = F + f * L.frac_size;
+    if (rd_i64(rec, L.f_id) != f) {
       set_error("fracture _id must equal its index (andfn/dfn.py:1119-1120)");
       return ANDFN_BAD_INPUT;
     }
-    h.t[f] = rd_f64(r, L.f_t);
-    h.constant[f] = rd_f64(r, L.f_constant);
-    int64_t nel = rd_i64(r, L.f_nelements);
+    h.t.push_back(rd_f64(rec, L.f_t));
+    h.constant.push_back(rd_f64(rec, L.f_constant));
+    int64_t nel = rd_i64(rec, L.f_nelements);
     if (nel < 0 || nel > L.max_elements) {
       set_error("fracture nelements out of range");
       return ANDFN_BAD_INPUT;
     }
     for (int64_t k = 0; k < nel; k++) {
-      int64_t el = rd_i64(r, L.f_elements + 8 * k);
+      int64_t el = rd_i64(rec, L.f_elements + 8 * k);
       if (el < 0 || el >= ne) {
         set_error("fracture element id out of range");
         return ANDFN_BAD_INPUT;
       }
-      h.felem.push_back((int)el);
+      h.felem.push_back(e0 + (int)el);
     }
-    h.fptr[f + 1] = (int)h.felem.size();
+    h.fptr.push_back((int)h.felem.size());
+    h.real_frac.push_back(r);
   }
-  h.de_ids.clear();
-  h.elem_de.assign(ne, -1);
-  for (int64_t i = 0; i < ne; i++)
-    if (h.type[i] == 0 || h.type[i] == 2 || h.type[i] == 3) {
-      h.elem_de[i] = (int)h.de_ids.size();
-      h.de_ids.push_back((int)i);
+  // discharge elements (types 0, 2, 3 in element order) and system rows
+  h.elem_de.resize(h.type.size(), -1);
+  const int d0 = (int)h.de_ids.size();
+  for (int64_t i = 0; i < ne; i++) {
+    const int ty = h.type[e0 + i];
+    if (ty == 0 || ty == 2 || ty == 3) {
+      h.elem_de[e0 + i] = (int)h.de_ids.size();
+      h.de_ids.push_back(e0 + (int)i);
     }
+  }
+  const int nde = (int)h.de_ids.size() - d0;
+  for (int j = 0; j < nde; j++) {
+    h.row_de.push_back(d0 + j);
+    h.row_frac.push_back(-1);
+    h.real_row.push_back(r);
+  }
+  for (int64_t f = 0; f < nf; f++) {
+    h.row_de.push_back(-1);
+    h.row_frac.push_back(f0 + (int)f);
+    h.real_row.push_back(r);
+  }
+  h.eoff[r + 1] = e0 + (int)ne;
+  h.foff[r + 1] = f0 + (int)nf;
+  h.doff[r + 1] = (int)h.de_ids.size();
+  h.roff[r + 1] = h.roff[r] + nde + (int)nf;
   return 0;
 }
 
-static void read_coefs(AndfnHandle *H, const char *E) {
+static void read_coefs(AndfnHandle *H, int r, const char *E) {
   const AndfnLayout &L = H->L;
-  H->h.coef.assign((size_t)H->ne * H->MC, mk(0.0, 0.0));
-  for (int64_t i = 0; i < H->ne; i++) {
-    const char *r = E + i * L.elem_size;
+  const int e0 = H->h.eoff[r], e1 = H->h.eoff[r + 1];
+  for (int i = e0; i < e1; i++) {
+    const char *rec = E + (int64_t)(i - e0) * L.elem_size;
     const int m = H->h.ncoef[i];
-    for (int k = 0; k < m && k < H->MC; k++) H->h.coef[(size_t)i * H->MC + k] = rd_cd(r, L.e_coef, k);
+    for (int k = 0; k < m && k < H->MC; k++) H->h.coef[(size_t)i * H->MC + k] = rd_cd(rec, L.e_coef, k);
   }
 }
 
@@ -1612,7 +1676,80 @@ static cudaError_t upload(DBuf<T> &d, const std::vector<T> &v, cudaStream_t s) {
   return cudaMemcpyAsync(d.p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, s);
 }
 
-// Evaluation tables: groups, flattened points and tiles per fracture.
+// Discharge-system pattern of realization r, row by row exactly as
+// fill_discharge_matrix (hpc_solve.py:1117-1201) orders it; local indices
+// (rows: its discharge elements then its fractures).  The assembly entries are
+// appended to the global arrays (global row, global source element).
+static void build_pattern(AndfnHandle *H, int r) {
+  const HostNet &h = H->h;
+  RealSys &S = H->sys[r];
+  const int d0 = h.doff[r], d1 = h.doff[r + 1], f0 = h.foff[r], f1 = h.foff[r + 1];
+  const int n_de = d1 - d0, nf = f1 - f0, row0 = h.roff[r];
+  S.n_de = n_de;
+  S.n = n_de + nf;
+  S.mrow_ptr.assign(1, 0);
+  S.mcol.clear();
+  S.ent0 = (int)H->ent_row.size();
+  auto disch = [&](int ty) { return ty == 0 || ty == 2 || ty == 3; };
+  for (int j = 0; j < n_de; j++) {
+    const int e = h.de_ids[d0 + j];
+    const int sides = (h.type[e] == 0) ? 2 : 1;
+    for (int s = 0; s < sides; s++) {
+      const int f = s ? h.frac1[e] : h.frac0[e];
+      for (int k = h.fptr[f]; k < h.fptr[f + 1]; k++) {
+        const int ee = h.felem[k];
+        if (ee == e || !disch(h.type[ee])) continue;
+        S.mcol.push_back(h.elem_de[ee] - d0);
+        H->ent_row.push_back(row0 + j);
+        H->ent_src.push_back(ee);
+        H->ent_side.push_back(s);
+        H->ent_kind.push_back(0);
+      }
+    }
+    for (int s = 0; s < sides; s++) {
+      const int f = s ? h.frac1[e] : h.frac0[e];
+      S.mcol.push_back(n_de + (f - f0));
+      H->ent_row.push_back(row0 + j);
+      H->ent_src.push_back(-1);
+      H->ent_side.push_back(s);
+      H->ent_kind.push_back(1);
+    }
+    S.mrow_ptr.push_back((int)S.mcol.size());
+  }
+  for (int f = f0; f < f1; f++) {
+    for (int k = h.fptr[f]; k < h.fptr[f + 1]; k++) {
+      const int el = h.felem[k];
+      if (!disch(h.type[el])) continue;
+      S.mcol.push_back(h.elem_de[el] - d0);
+      H->ent_row.push_back(row0 + n_de + (f - f0));
+      H->ent_src.push_back(el);
+      H->ent_side.push_back(0);
+      H->ent_kind.push_back(2);
+    }
+    S.mrow_ptr.push_back((int)S.mcol.size());
+  }
+}
+
+// CSC of realization r's system with the given entry values (vals indexed by
+// global assembly entry).
+static CscMatrix system_csc(const RealSys &S, const double *vals) {
+  CscMatrix A;
+  A.n = S.n;
+  A.colptr.assign(S.n + 1, 0);
+  for (int c : S.mcol) A.colptr[c + 1]++;
+  for (int i = 0; i < S.n; i++) A.colptr[i + 1] += A.colptr[i];
+  A.rowind.resize(S.mcol.size());
+  A.val.resize(S.mcol.size());
+  std::vector<int> fill(A.colptr.begin(), A.colptr.end() - 1);
+  for (int rr = 0; rr < S.n; rr++)
+    for (int p = S.mrow_ptr[rr]; p < S.mrow_ptr[rr + 1]; p++) {
+      const int c = S.mcol[p];
+      A.rowind[fill[c]] = rr;
+      A.val[fill[c]++] = vals ? vals[S.ent0 + p] : 1.0;
+    }
+  return A;
+}
+
 static void build_tables(AndfnHandle *H, bool rhs, std::vector<Group> &groups, std::vector<int> &index_of,
                          std::vector<Item> &items, std::vector<int2> &pts, int &nvals,
                          const std::vector<char> *only = nullptr) {
@@ -1697,58 +1834,6 @@ static void build_tables(AndfnHandle *H, bool rhs, std::vector<Group> &groups, s
   for (auto &c : costs) items.push_back(c.it);
 }
 
-// Discharge-system pattern, row by row exactly as fill_discharge_matrix
-// (hpc_solve.py:1117-1201) orders it.
-static void build_pattern(AndfnHandle *H) {
-  const HostNet &h = H->h;
-  const int n_de = (int)h.de_ids.size();
-  const int nf = (int)H->nf;
-  H->N = n_de + nf;
-  H->mrow_ptr.assign(1, 0);
-  H->mcol.clear();
-  H->ent_row.clear();
-  H->ent_src.clear();
-  H->ent_side.clear();
-  H->ent_kind.clear();
-  auto disch = [&](int ty) { return ty == 0 || ty == 2 || ty == 3; };
-  for (int j = 0; j < n_de; j++) {
-    const int e = h.de_ids[j];
-    const int sides = (h.type[e] == 0) ? 2 : 1;
-    for (int s = 0; s < sides; s++) {
-      const int f = s ? h.frac1[e] : h.frac0[e];
-      for (int k = h.fptr[f]; k < h.fptr[f + 1]; k++) {
-        const int ee = h.felem[k];
-        if (ee == e || !disch(h.type[ee])) continue;
-        H->mcol.push_back(h.elem_de[ee]);
-        H->ent_row.push_back(j);
-        H->ent_src.push_back(ee);
-        H->ent_side.push_back(s);
-        H->ent_kind.push_back(0);
-      }
-    }
-    for (int s = 0; s < sides; s++) {
-      const int f = s ? h.frac1[e] : h.frac0[e];
-      H->mcol.push_back(n_de + f);
-      H->ent_row.push_back(j);
-      H->ent_src.push_back(-1);
-      H->ent_side.push_back(s);
-      H->ent_kind.push_back(1);
-    }
-    H->mrow_ptr.push_back((int)H->mcol.size());
-  }
-  for (int f = 0; f < nf; f++) {
-    for (int k = h.fptr[f]; k < h.fptr[f + 1]; k++) {
-      const int el = h.felem[k];
-      if (!disch(h.type[el])) continue;
-      H->mcol.push_back(h.elem_de[el]);
-      H->ent_row.push_back(n_de + f);
-      H->ent_src.push_back(el);
-      H->ent_side.push_back(0);
-      H->ent_kind.push_back(2);
-    }
-    H->mrow_ptr.push_back((int)H->mcol.size());
-  }
-}
 
 static int reset_impl(AndfnHandle *H);
 
@@ -1820,46 +1905,67 @@ static int ensure_capacity(AndfnHandle *H, int mc) {
   return 0;
 }
 
-static int create_impl(AndfnHandle *H, const char *F, const char *E) {
+static int create_impl(AndfnHandle *H, int R, const char *const *F, const int64_t *nf, const char *const *E,
+                       const int64_t *ne) {
   auto tc0 = std::chrono::steady_clock::now();
-  int rc = parse_records(H, F, E);
-  if (rc) return rc;
-  read_coefs(H, E);
   HostNet &h = H->h;
+  H->R = R;
+  h.eoff.assign(R + 1, 0);
+  h.foff.assign(R + 1, 0);
+  h.doff.assign(R + 1, 0);
+  h.roff.assign(R + 1, 0);
+  h.fptr.assign(1, 0);
+  H->MC = 1;
+  for (int r = 0; r < R; r++) {
+    int rc = parse_records(H, r, F[r], nf[r], E[r], ne[r]);
+    if (rc) return rc;
+  }
+  H->ne = h.eoff[R];
+  H->nf = h.foff[R];
+  H->N = h.roff[R];
+  h.coef.assign((size_t)H->ne * H->MC, mk(0.0, 0.0));
+  for (int r = 0; r < R; r++) read_coefs(H, r, E[r]);
   cudaStream_t s = H->stream;
-  const int ne = (int)H->ne;
+  const int nel = (int)H->ne;
   CK(upload(H->type, h.type, s));
   CK(upload(H->frac0, h.frac0, s));
   CK(upload(H->frac1, h.frac1, s));
   CK(upload(H->ncoef0, h.ncoef, s));
   CK(upload(H->nint0, h.nint, s));
-  CK(H->ncoef.alloc(ne));
-  CK(H->nint.alloc(ne));
+  CK(H->ncoef.alloc(nel));
+  CK(H->nint.alloc(nel));
   CK(upload(H->ep0, h.ep0, s));
   CK(upload(H->ep1, h.ep1, s));
   CK(upload(H->center, h.center, s));
   CK(upload(H->radius, h.radius, s));
   CK(upload(H->phi, h.phi, s));
   CK(upload(H->q0, h.q, s));
-  CK(H->q.alloc(ne));
+  CK(H->q.alloc(nel));
   CK(upload(H->coef0, h.coef, s));
-  CK(H->coef.alloc((size_t)ne * H->MC));
-  CK(H->wcoef.alloc((size_t)ne * H->MC));
+  CK(H->coef.alloc((size_t)nel * H->MC));
+  CK(H->wcoef.alloc((size_t)nel * H->MC));
   CK(upload(H->err_in, h.err, s));
   CK(upload(H->err_old_in, h.err_old, s));
   CK(upload(H->err_old2_in, h.err_old2, s));
   CK(upload(H->err_coef_in, h.err_coef, s));
-  CK(H->err.alloc(ne));
-  CK(H->err_old.alloc(ne));
-  CK(H->err_old2.alloc(ne));
-  CK(H->err_coef.alloc(ne));
-  CK(H->dpsi_corr.alloc((size_t)ne * 2 * H->MC));
+  CK(H->err.alloc(nel));
+  CK(H->err_old.alloc(nel));
+  CK(H->err_old2.alloc(nel));
+  CK(H->err_coef.alloc(nel));
+  CK(H->dpsi_corr.alloc((size_t)nel * 2 * H->MC));
   CK(upload(H->t, h.t, s));
   CK(upload(H->constant0, h.constant, s));
   CK(H->constant.alloc(h.constant.size()));
   CK(upload(H->fptr, h.fptr, s));
   CK(upload(H->felem, h.felem, s));
   CK(upload(H->de_ids, h.de_ids, s));
+  CK(upload(H->real_elem, h.real_elem, s));
+  CK(upload(H->real_frac, h.real_frac, s));
+  CK(upload(H->real_row, h.real_row, s));
+  CK(upload(H->eoff, h.eoff, s));
+  CK(upload(H->row_de, h.row_de, s));
+  CK(upload(H->row_frac, h.row_frac, s));
+  CK(H->ndone.alloc(1));
   const int n_de = (int)h.de_ids.size();
   CK(H->zint0.alloc((size_t)std::max(1, n_de) * H->D));
   CK(H->zint1.alloc((size_t)std::max(1, n_de) * H->D));
@@ -1875,47 +1981,44 @@ static int create_impl(AndfnHandle *H, const char *F, const char *E) {
     maxd = std::max(maxd, c);
   }
   H->cut_cap = 2 * maxd + 4;
-  CK(H->cut_n.alloc(ne));
-  CK(H->cut_pos.alloc((size_t)ne * H->cut_cap));
-  CK(H->cut_elem.alloc((size_t)ne * H->cut_cap));
-  CK(H->cut_sign.alloc((size_t)ne * H->cut_cap));
+  CK(H->cut_n.alloc(nel));
+  CK(H->cut_pos.alloc((size_t)nel * H->cut_cap));
+  CK(H->cut_elem.alloc((size_t)nel * H->cut_cap));
+  CK(H->cut_sign.alloc((size_t)nel * H->cut_cap));
   H->ms_create_upload = ms_since(tc0);
   auto tc1 = std::chrono::steady_clock::now();
   H->cur_ncoef = h.ncoef;
   H->cur_nint = h.nint;
-  rc = build_eval_tables(H);
+  int rc = build_eval_tables(H);
   if (rc) return rc;
   H->ms_create_tables = ms_since(tc1);
-  // discharge system
-  build_pattern(H);
+  // discharge systems: patterns, then fill-reducing column orders from the
+  // patterns alone, computed once per network (in parallel over realizations)
+  H->sys.assign(R, RealSys());
+  H->ent_row.clear();
+  H->ent_src.clear();
+  H->ent_side.clear();
+  H->ent_kind.clear();
+  for (int r = 0; r < R; r++) build_pattern(H, r);
   CK(upload(H->d_ent_row, H->ent_row, s));
   CK(upload(H->d_ent_src, H->ent_src, s));
   CK(upload(H->d_ent_side, H->ent_side, s));
   CK(upload(H->d_ent_kind, H->ent_kind, s));
   CK(H->d_mvals.alloc(std::max<size_t>(1, H->ent_row.size())));
   auto tc2 = std::chrono::steady_clock::now();
-  {
-    // fill-reducing column order from the pattern alone (values do not
-    // matter for it), computed once per network
-    CscMatrix P;
-    P.n = H->N;
-    P.colptr.assign(H->N + 1, 0);
-    for (int c : H->mcol) P.colptr[c + 1]++;
-    for (int i = 0; i < H->N; i++) P.colptr[i + 1] += P.colptr[i];
-    P.rowind.resize(H->mcol.size());
-    P.val.assign(H->mcol.size(), 1.0);
-    std::vector<int> fill(P.colptr.begin(), P.colptr.end() - 1);
-    for (int r = 0; r < H->N; r++)
-      for (int p = H->mrow_ptr[r]; p < H->mrow_ptr[r + 1]; p++) P.rowind[fill[H->mcol[p]]++] = r;
-    H->colorder = column_min_degree_order(P, &H->dense_k);
+#pragma omp parallel for schedule(dynamic, 1) if (R > 1)
+  for (int r = 0; r < R; r++) {
+    CscMatrix P = system_csc(H->sys[r], nullptr);
+    H->sys[r].colorder = column_min_degree_order(P, &H->sys[r].dense_k);
   }
   H->ms_create_order = ms_since(tc2);
   CK(H->disc.alloc(H->N));
   CK(H->work.alloc(H->N));
   CK(H->bvec.alloc(H->N));
   CK(H->ready.alloc(H->N));
-  CK(H->st.alloc(1));
-  if (!H->h_st) CK(cudaMallocHost(&H->h_st, sizeof(SolveState)));
+  CK(H->st.alloc(R));
+  H->h_st.assign(R, SolveState());
+  if (!H->h_ndone) CK(cudaMallocHost(&H->h_ndone, sizeof(int)));
   CK(cudaFuncSetAttribute(eval_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
   CK(cudaFuncSetAttribute(eval_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
   CK(cudaFuncSetAttribute(trisolve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
@@ -1942,7 +2045,6 @@ static int reset_impl(AndfnHandle *H) {
   CK(cudaMemsetAsync(H->dpsi_corr.p, 0, sizeof(double) * ne * 2 * H->MC, s));
   return 0;
 }
-
 
 // Groups rows [row_lo, row_hi) of a triangular factor by dependency level and
 // stores their entries with columns in [col_lo, col_hi) in that order
@@ -2004,42 +2106,180 @@ static int group_for(const std::vector<int> &eptr) {
   return 32;
 }
 
+// Factorises every realization's system (in parallel over realizations) and
+// uploads the level-ordered factor parts, dense tails, permutations and one
+// TriDesc per realization.
+static int factor_all(AndfnHandle *H, const std::vector<double> &mv) {
+  const int R = H->R;
+  cudaStream_t s = H->stream;
+  std::vector<LuFactors> LU(R);
+  std::vector<int> rcs(R, 0);
+  // one realization: the dense Schur LU inside uses the host threads; several:
+  // one realization per thread
+  auto factor_one = [&](int r) {
+    CscMatrix A = system_csc(H->sys[r], mv.data());
+    rcs[r] = sparse_lu_factor(A, H->sys[r].colorder, 1.0, LU[r], H->sys[r].dense_k);
+  };
+  if (R == 1) {
+    factor_one(0);
+  } else {
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int r = 0; r < R; r++) factor_one(r);
+  }
+  for (int r = 0; r < R; r++)
+    if (rcs[r]) {
+      set_error("discharge system of realization " + std::to_string(r) +
+                " is singular (a fracture without a head boundary?)");
+      return ANDFN_SINGULAR;
+    }
+  struct PartOff {
+    int lev, rows, ent;
+  };
+  LevelParts parts[4];  // lf, lx, ux, ub
+  std::vector<std::array<PartOff, 4>> off(R);
+  std::vector<std::array<int, 4>> nlev(R), nslots(R), grp(R);
+  std::vector<double> tl, tu, tui;
+  std::vector<size_t> toff(R), tuoff(R);
+  std::vector<int> pinv, qcol;
+  H->nnz_factors = 0;
+  H->max_n = 0;
+  H->max_nlev = 1;
+  for (int r = 0; r < R; r++) {
+    const LuFactors &F = LU[r];
+    const int n = F.n, K = F.dense, m0 = n - K;
+    H->max_n = std::max(H->max_n, n);
+    H->nnz_factors += F.nnz() + 2LL * K * K;
+    pinv.insert(pinv.end(), F.pinv.begin(), F.pinv.end());
+    qcol.insert(qcol.end(), F.q.begin(), F.q.end());
+    const struct {
+      bool lower, single;
+      int rlo, rhi, clo, chi;
+      bool scaled;
+    } spec[4] = {{true, false, 0, m0, 0, m0, false},
+                 {true, true, m0, n, 0, m0, false},
+                 {false, true, 0, m0, m0, n, false},
+                 {false, false, 0, m0, 0, m0, true}};
+    for (int k = 0; k < 4; k++) {
+      std::vector<int> lev, rows, eptr, ecol;
+      std::vector<double> ev, esc;
+      const auto &sp = spec[k];
+      // without a dense tail the coupling parts are empty
+      const int rlo = (K == 0 && (k == 1 || k == 2)) ? 0 : sp.rlo;
+      const int rhi = (K == 0 && (k == 1 || k == 2)) ? 0 : sp.rhi;
+      if (sp.lower)
+        build_levels(n, F.l_ptr, F.l_col, F.l_val, nullptr, true, rlo, rhi, sp.clo, sp.chi, sp.single, lev, rows,
+                     eptr, ecol, ev, esc);
+      else
+        build_levels(n, F.u_ptr, F.u_col, F.u_val, sp.scaled ? &F.u_inv_diag : nullptr, false, rlo, rhi, sp.clo,
+                     sp.chi, sp.single, lev, rows, eptr, ecol, ev, esc);
+      LevelParts &P = parts[k];
+      off[r][k] = {(int)P.lev.size(), (int)P.rows.size(), (int)P.col.size()};
+      nlev[r][k] = (int)lev.size() - 1;
+      nslots[r][k] = (int)rows.size();
+      grp[r][k] = group_for(eptr);
+      H->max_nlev = std::max(H->max_nlev, nlev[r][k]);
+      P.lev.insert(P.lev.end(), lev.begin(), lev.end());
+      P.rows.insert(P.rows.end(), rows.begin(), rows.end());
+      P.eptr.insert(P.eptr.end(), eptr.begin(), eptr.end());
+      P.col.insert(P.col.end(), ecol.begin(), ecol.end());
+      P.val.insert(P.val.end(), ev.begin(), ev.end());
+      P.scale.insert(P.scale.end(), esc.begin(), esc.end());
+      // keep eptr and rows indexable by slot: eptr has nslots + 1 entries, so
+      // the next part starts one entry later; rows pad to the same length
+      P.rows.push_back(0);
+      P.scale.push_back(1.0);
+    }
+    toff[r] = tl.size();
+    tuoff[r] = tui.size();
+    tl.insert(tl.end(), F.l22.begin(), F.l22.end());
+    tu.insert(tu.end(), F.u22.begin(), F.u22.end());
+    tui.insert(tui.end(), F.u_inv_diag.begin() + m0, F.u_inv_diag.end());
+    H->sys[r].tail_k = K;
+    H->sys[r].nlev_l = nlev[r][0];
+    H->sys[r].nlev_u = nlev[r][3];
+    H->sys[r].nnz = F.nnz() + 2LL * K * K;
+  }
+  DBuf<int> *dlev[4] = {&H->lf_lev, &H->lx_lev, &H->ux_lev, &H->ub_lev};
+  DBuf<int> *drows[4] = {&H->lf_rows, &H->lx_rows, &H->ux_rows, &H->ub_rows};
+  DBuf<int> *deptr[4] = {&H->lf_eptr, &H->lx_eptr, &H->ux_eptr, &H->ub_eptr};
+  DBuf<int> *dcol[4] = {&H->lf_col, &H->lx_col, &H->ux_col, &H->ub_col};
+  DBuf<double> *dval[4] = {&H->lf_val, &H->lx_val, &H->ux_val, &H->ub_val};
+  for (int k = 0; k < 4; k++) {
+    if (parts[k].col.empty()) {
+      parts[k].col.push_back(0);
+      parts[k].val.push_back(0.0);
+    }
+    CK(upload(*dlev[k], parts[k].lev, s));
+    CK(upload(*drows[k], parts[k].rows, s));
+    CK(upload(*deptr[k], parts[k].eptr, s));
+    CK(upload(*dcol[k], parts[k].col, s));
+    CK(upload(*dval[k], parts[k].val, s));
+  }
+  CK(upload(H->ub_scale, parts[3].scale, s));
+  if (tl.empty()) {
+    tl.push_back(0.0);
+    tu.push_back(0.0);
+    tui.push_back(0.0);
+  }
+  CK(upload(H->tail_l, tl, s));
+  CK(upload(H->tail_u, tu, s));
+  CK(upload(H->tail_uinv, tui, s));
+  CK(upload(H->pinv, pinv, s));
+  CK(upload(H->qcol, qcol, s));
+  std::vector<TriDesc> td(R);
+  for (int r = 0; r < R; r++) {
+    const int n = LU[r].n, K = LU[r].dense;
+    LevelSolve *ls[4] = {&td[r].Lf, &td[r].Lx, &td[r].Ux, &td[r].Ub};
+    for (int k = 0; k < 4; k++) {
+      LevelSolve &L = *ls[k];
+      const PartOff &o = off[r][k];
+      L.lev_ptr = dlev[k]->p + o.lev;
+      L.rows = drows[k]->p + o.rows;
+      L.eptr = deptr[k]->p + o.rows;
+      L.col = dcol[k]->p + o.ent;
+      L.val = dval[k]->p + o.ent;
+      L.scale = (k == 3) ? H->ub_scale.p + o.rows : nullptr;
+      L.nlev = nlev[r][k];
+      L.nslots = nslots[r][k];
+      L.group = grp[r][k];
+    }
+    td[r].T.K = K;
+    td[r].T.L = H->tail_l.p + toff[r];
+    td[r].T.U = H->tail_u.p + toff[r];
+    td[r].T.uinv = H->tail_uinv.p + tuoff[r];
+    td[r].pinv = H->pinv.p + H->h.roff[r];
+    td[r].qcol = H->qcol.p + H->h.roff[r];
+    td[r].row0 = H->h.roff[r];
+    td[r].n = n;
+  }
+  CK(upload(H->tri, td, s));
+  CK(cudaStreamSynchronize(s));
+  return 0;
+}
+
 static void launch_trisolve(AndfnHandle *H, cudaStream_t s) {
   Net net = H->net();
-  const int m0 = H->N - H->tail_k;
-  LevelSolve Lf{H->lf_lev.p, H->lf_rows.p, H->lf_eptr.p, H->lf_col.p, H->lf_val.p, nullptr, H->lf_nlev, m0, H->g_lf};
-  LevelSolve Ub{H->ub_lev.p, H->ub_rows.p, H->ub_eptr.p, H->ub_col.p, H->ub_val.p, H->ub_scale.p, H->ub_nlev, m0,
-                H->g_ub};
-  LevelSolve Lx{H->lx_lev.p, H->lx_rows.p, H->lx_eptr.p, H->lx_col.p, H->lx_val.p, nullptr, H->lx_nlev, H->tail_k,
-                H->g_lx};
-  LevelSolve Ux{H->ux_lev.p, H->ux_rows.p, H->ux_eptr.p, H->ux_col.p, H->ux_val.p, nullptr, H->ux_nlev, m0,
-                H->g_ux};
-  DenseTail T{H->tail_k, H->tail_l.p, H->tail_u.p, H->tail_uinv.p};
-  const size_t ybytes = sizeof(double) * (size_t)H->N;
-  const int use_smem = ybytes <= 150 * 1024;
-  const size_t lev_bytes = sizeof(int) * (size_t)(std::max(std::max(H->lf_nlev, H->ub_nlev), 1) + 1);
-  const int cap_levptr = (int)std::min<size_t>(lev_bytes, 40 * 1024) / (int)sizeof(int);
+  const size_t ybytes = sizeof(double) * (size_t)H->max_n;
+  const int use_smem = ybytes <= 150 * 1024 ? H->max_n : 0;
+  const int cap_levptr = std::min(H->max_nlev + 1, 10240);
   size_t solve_smem = (use_smem ? ybytes : 0) + sizeof(int) * (size_t)cap_levptr;
-  const size_t meta_bytes = sizeof(int) * 2 * ((size_t)H->N + 1);
-  const int meta_cap = (solve_smem + meta_bytes <= 200 * 1024) ? H->N + 1 : 0;
+  const size_t meta_bytes = sizeof(int) * 2 * ((size_t)H->max_n + 1);
+  const int meta_cap = (solve_smem + meta_bytes <= 200 * 1024) ? H->max_n + 1 : 0;
   if (meta_cap) solve_smem += meta_bytes;
-  trisolve_kernel<<<1, H->solve_threads, solve_smem, s>>>(net, H->rhs_vals.p, H->rhs_group.p, H->d_groups.p,
-                                                          use_smem, Lf, Lx, Ux, Ub, T, cap_levptr, meta_cap);
+  trisolve_kernel<<<H->R, H->solve_threads, solve_smem, s>>>(net, use_smem, cap_levptr, meta_cap);
 }
 
 static inline void mark(AndfnHandle *H, cudaStream_t s, int b, int c, int w) {
   if (H->profiling && b >= 0) cudaEventRecordWithFlags(H->ev[b][c][w], s, cudaEventRecordExternal);
 }
 
-static int enqueue_iteration(AndfnHandle *H, cudaStream_t s, int single_blend_sweep, int b = -1) {
+static int enqueue_iteration(AndfnHandle *H, cudaStream_t s, int blend_mode, int b = -1) {
   Net net = H->net();
   mark(H, s, b, K_RHS, 0);
-  if (H->n_rhs_items > 0) {
+  if (H->n_rhs_items > 0)
     eval_kernel<true><<<H->n_rhs_items, EVAL_THREADS, H->eval_smem, s>>>(net, H->rhs_items.p, H->rhs_pts.p,
                                                                           H->d_groups.p, H->rhs_vals.p, H->chunk);
-  }
   rhs_reduce_kernel<<<(H->N * 32 + 255) / 256, 256, 0, s>>>(net, H->rhs_vals.p, H->rhs_group.p, H->d_groups.p);
-  H->launches += 1;
   mark(H, s, b, K_RHS, 1);
   mark(H, s, b, K_TRISOLVE, 0);
   launch_trisolve(H, s);
@@ -2054,12 +2294,12 @@ static int enqueue_iteration(AndfnHandle *H, cudaStream_t s, int single_blend_sw
   mark(H, s, b, K_UPDATE, 0);
   if (ub > 0)
     update_kernel<<<ub, UPDATE_WARPS * 32, usmem, s>>>(net, H->upd_list.p, H->n_upd, H->group_of.p, H->d_groups.p,
-                                                        H->sweep_vals.p, H->nvmax, single_blend_sweep);
+                                                        H->sweep_vals.p, H->nvmax, blend_mode);
   mark(H, s, b, K_UPDATE, 1);
   mark(H, s, b, K_REDUCE, 0);
-  reduce_kernel<<<1, 1024, 0, s>>>(net);
+  reduce_kernel<<<H->R, 1024, 0, s>>>(net);
   mark(H, s, b, K_REDUCE, 1);
-  H->launches += 5;
+  H->launches += 6;
   return 0;
 }
 
@@ -2141,22 +2381,29 @@ static int run_adaptive(AndfnHandle *H, const AndfnConstants *C) {
       H->launches += 2;
     }
     blend2_kernel<<<std::max(1, std::min(1184, (int)((H->ne * H->MC + 255) / 256))), 256, 0, s>>>(net);
-    reduce_kernel<<<1, 1024, 0, s>>>(net);
+    reduce_kernel<<<H->R, 1024, 0, s>>>(net);
     H->launches += 2;
-    CK(cudaMemcpyAsync(H->h_st, H->st.p, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(H->h_ndone, H->ndone.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
-    if (H->h_st->done) break;
+    if (*H->h_ndone >= H->R) break;
     if (++guard > C->max_iterations + 2) break;
   }
+  return 0;
+}
+
+static int read_states(AndfnHandle *H) {
+  CK(cudaMemcpyAsync(H->h_st.data(), H->st.p, sizeof(SolveState) * H->R, cudaMemcpyDeviceToHost, H->stream));
+  CK(cudaStreamSynchronize(H->stream));
   return 0;
 }
 
 static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S) {
   auto t_all = std::chrono::steady_clock::now();
   cudaStream_t s = H->stream;
-  AndfnSolveStats stats;
-  std::memset(&stats, 0, sizeof(stats));
-  stats.device = H->device;
+  const int R = H->R;
+  AndfnSolveStats base;
+  std::memset(&base, 0, sizeof(base));
+  base.device = H->device;
   H->launches = 0;
   if (C->max_ncoef > H->L.max_ncoef || C->max_iterations < 0) {
     set_error("constants out of range");
@@ -2164,7 +2411,7 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
   }
   // Adaptive coefficient growth (hpc_solve.py:465-559) can happen when some
   // element may still grow (ncoef < MAX_NCOEF); it needs coefficient capacity
-  // MAX_NCOEF and the host-driven loop below.
+  // up to the largest reachable ncoef and the host-driven loop.
   bool growth_possible = false;
   for (int64_t i = 0; i < H->ne; i++)
     if (H->h.type[i] != 2 && H->h.ncoef[i] < C->max_ncoef) growth_possible = true;
@@ -2177,7 +2424,8 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
     int64_t top = 0;
     for (int64_t i = 0; i < H->ne; i++) {
       int64_t m = H->h.ncoef[i];
-      if (H->h.type[i] != 2 && m < C->max_ncoef) m += C->coef_increase * ((C->max_ncoef - m + C->coef_increase - 1) / C->coef_increase);
+      if (H->h.type[i] != 2 && m < C->max_ncoef)
+        m += C->coef_increase * ((C->max_ncoef - m + C->coef_increase - 1) / C->coef_increase);
       top = std::max(top, m);
     }
     if (top > H->L.max_ncoef) {
@@ -2208,7 +2456,10 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
   st0.fused_blend2 = growth_possible ? 0 : 1;
   st0.solve_q = 1;
   st0.done = (C->max_iterations <= 0) ? 1 : 0;
-  CK(cudaMemcpyAsync(H->st.p, &st0, sizeof(st0), cudaMemcpyHostToDevice, s));
+  std::vector<SolveState> st_init(R, st0);
+  CK(cudaMemcpyAsync(H->st.p, st_init.data(), sizeof(SolveState) * R, cudaMemcpyHostToDevice, s));
+  const int ndone0 = st0.done ? R : 0;
+  CK(cudaMemcpyAsync(H->ndone.p, &ndone0, sizeof(int), cudaMemcpyHostToDevice, s));
   auto t_setup = std::chrono::steady_clock::now();
   init_state_kernel<<<std::max<int64_t>(1, (H->ne + 255) / 256), 256, 0, s>>>(net);
   const int n_de = (int)H->h.de_ids.size();
@@ -2219,109 +2470,24 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
     matrix_values_kernel<<<(unsigned)((nent * 32 + 255) / 256), 256, 0, s>>>(
         net, H->d_ent_row.p, H->d_ent_src.p, H->d_ent_side.p, H->d_ent_kind.p, H->d_mvals.p, nent);
   H->launches += 4;
-  std::vector<double> mv(nent);
+  std::vector<double> mv(std::max<long long>(1, nent));
   if (nent > 0) CK(cudaMemcpyAsync(mv.data(), H->d_mvals.p, sizeof(double) * nent, cudaMemcpyDeviceToHost, s));
   g_d2h_bytes += 8 * nent;
   // initial discharges (get_old_discharges, hpc_solve.py:765-775)
   std::vector<double> disc0(H->N, 0.0);
-  for (int j = 0; j < n_de; j++) disc0[j] = H->h.q[H->h.de_ids[j]];
-  for (int64_t f = 0; f < H->nf; f++) disc0[n_de + f] = H->h.constant[f];
+  for (int g = 0; g < H->N; g++) {
+    const int d = H->h.row_de[g];
+    disc0[g] = d >= 0 ? H->h.q[H->h.de_ids[d]] : H->h.constant[H->h.row_frac[g]];
+  }
   CK(cudaMemcpyAsync(H->disc.p, disc0.data(), sizeof(double) * H->N, cudaMemcpyHostToDevice, s));
   g_h2d_bytes += 8 * (int64_t)H->N;
   CK(cudaStreamSynchronize(s));
-  stats.ms_setup = ms_since(t_setup);
-  // factorisation (host): CSC of the pattern, cached column order
+  base.ms_setup = ms_since(t_setup);
+  // factorisation (host)
   auto t_fac = std::chrono::steady_clock::now();
-  CscMatrix A;
-  A.n = H->N;
-  A.colptr.assign(H->N + 1, 0);
-  for (int c : H->mcol) A.colptr[c + 1]++;
-  for (int i = 0; i < H->N; i++) A.colptr[i + 1] += A.colptr[i];
-  A.rowind.resize(H->mcol.size());
-  A.val.resize(H->mcol.size());
-  {
-    std::vector<int> fill(A.colptr.begin(), A.colptr.end() - 1);
-    for (int r = 0; r < H->N; r++)
-      for (int p = H->mrow_ptr[r]; p < H->mrow_ptr[r + 1]; p++) {
-        const int c = H->mcol[p];
-        A.rowind[fill[c]] = r;
-        A.val[fill[c]++] = mv[p];
-      }
-  }
-  if ((int)H->colorder.size() != H->N) H->colorder = column_min_degree_order(A, &H->dense_k);
-  LuFactors LU;
-  rc = sparse_lu_factor(A, H->colorder, 1.0, LU, H->dense_k);
-  if (rc) {
-    set_error("discharge system is singular (a fracture without a head boundary?)");
-    return ANDFN_SINGULAR;
-  }
-  H->nnz_factors = LU.nnz();
-  CK(upload(H->pinv, LU.pinv, s));
-  CK(upload(H->qcol, LU.q, s));
-  CK(upload(H->l_ptr, LU.l_ptr, s));
-  CK(upload(H->l_col, LU.l_col, s));
-  CK(upload(H->l_val, LU.l_val, s));
-  CK(upload(H->u_ptr, LU.u_ptr, s));
-  CK(upload(H->u_col, LU.u_col, s));
-  CK(upload(H->u_val, LU.u_val, s));
-  CK(upload(H->u_inv, LU.u_inv_diag, s));
-  {
-    const int n = H->N;
-    const int K = LU.dense;
-    const int m0 = n - K;  // rows [0, m0) sparse, [m0, n) dense tail
-    H->tail_k = K;
-    std::vector<int> lev, rows, eptr, ecol;
-    std::vector<double> ev, esc;
-    build_levels(n, LU.l_ptr, LU.l_col, LU.l_val, nullptr, true, 0, m0, 0, m0, false, lev, rows, eptr, ecol, ev,
-                 esc);
-    H->lf_nlev = (int)lev.size() - 1;
-    H->g_lf = group_for(eptr);
-    CK(upload(H->lf_lev, lev, s));
-    CK(upload(H->lf_rows, rows, s));
-    CK(upload(H->lf_eptr, eptr, s));
-    CK(upload(H->lf_col, ecol, s));
-    CK(upload(H->lf_val, ev, s));
-    CK(cudaStreamSynchronize(s));
-    build_levels(n, LU.u_ptr, LU.u_col, LU.u_val, &LU.u_inv_diag, false, 0, m0, 0, m0, false, lev, rows, eptr,
-                 ecol, ev, esc);
-    H->ub_nlev = (int)lev.size() - 1;
-    H->g_ub = group_for(eptr);
-    CK(upload(H->ub_lev, lev, s));
-    CK(upload(H->ub_rows, rows, s));
-    CK(upload(H->ub_eptr, eptr, s));
-    CK(upload(H->ub_col, ecol, s));
-    CK(upload(H->ub_val, ev, s));
-    CK(upload(H->ub_scale, esc, s));
-    CK(cudaStreamSynchronize(s));
-    if (K > 0) {
-      build_levels(n, LU.l_ptr, LU.l_col, LU.l_val, nullptr, true, m0, n, 0, m0, true, lev, rows, eptr, ecol, ev,
-                   esc);
-      H->lx_nlev = (int)lev.size() - 1;
-      H->g_lx = group_for(eptr);
-      CK(upload(H->lx_lev, lev, s));
-      CK(upload(H->lx_rows, rows, s));
-      CK(upload(H->lx_eptr, eptr, s));
-      CK(upload(H->lx_col, ecol, s));
-      CK(upload(H->lx_val, ev, s));
-      CK(cudaStreamSynchronize(s));
-      build_levels(n, LU.u_ptr, LU.u_col, LU.u_val, nullptr, false, 0, m0, m0, n, true, lev, rows, eptr, ecol, ev,
-                   esc);
-      H->ux_nlev = (int)lev.size() - 1;
-      H->g_ux = group_for(eptr);
-      CK(upload(H->ux_lev, lev, s));
-      CK(upload(H->ux_rows, rows, s));
-      CK(upload(H->ux_eptr, eptr, s));
-      CK(upload(H->ux_col, ecol, s));
-      CK(upload(H->ux_val, ev, s));
-      CK(cudaStreamSynchronize(s));
-      std::vector<double> ui(LU.u_inv_diag.begin() + m0, LU.u_inv_diag.end());
-      CK(upload(H->tail_l, LU.l22, s));
-      CK(upload(H->tail_u, LU.u22, s));
-      CK(upload(H->tail_uinv, ui, s));
-      CK(cudaStreamSynchronize(s));
-    }
-  }
-  stats.ms_factor = ms_since(t_fac);
+  rc = factor_all(H, mv);
+  if (rc) return rc;
+  base.ms_factor = ms_since(t_fac);
   // iterations, in graph batches
   auto t_it = std::chrono::steady_clock::now();
   if (growth_possible) {
@@ -2334,11 +2500,11 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
     }
     {
       cudaGraph_t g;
-      CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
       if (H->profiling && !H->ev[0][0][0])
         for (auto &bb : H->ev)
           for (auto &c : bb)
             for (auto &e : c) CK(cudaEventCreate(&e));
+      CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
       for (int b = 0; b < ITER_BATCH; b++) enqueue_iteration(H, s, 0, b);
       CK(cudaStreamEndCapture(s, &g));
       CK(cudaGraphInstantiate(&H->graph_exec, g, 0));
@@ -2349,12 +2515,16 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
     int nit_before = 0;
     while (true) {
       CK(cudaGraphLaunch(H->graph_exec, s));
-      CK(cudaMemcpyAsync(H->h_st, H->st.p, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(H->h_ndone, H->ndone.p, sizeof(int), cudaMemcpyDeviceToHost, s));
       CK(cudaStreamSynchronize(s));
       H->launches += ITER_BATCH * 6;
       if (H->profiling) {
         // only the iterations that did work (later ones return at entry)
-        const int real = std::min(ITER_BATCH, H->h_st->nit - nit_before);
+        int rcs = read_states(H);
+        if (rcs) return rcs;
+        int nit_max = 0;
+        for (int r = 0; r < R; r++) nit_max = std::max(nit_max, H->h_st[r].nit);
+        const int real = std::min(ITER_BATCH, nit_max - nit_before);
         for (int b = 0; b < real; b++)
           for (int c = 0; c < KCLASSES; c++) {
             float ms = 0.f;
@@ -2363,62 +2533,85 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
               H->k_n[c] += 1;
             }
           }
-        nit_before = H->h_st->nit;
+        nit_before = nit_max;
       }
-      if (H->h_st->done) break;
+      if (*H->h_ndone >= R) break;
       if (++guard > 1 + C->max_iterations / ITER_BATCH + 2) break;
     }
-
   }
-  SolveState fin = *H->h_st;
-  // hpc_solve.py:224-234: an extra element_solver sweep at nit == MAX_ITERATIONS
-  if (fin.nit == C->max_iterations && !fin.nonfinite && fin.status == 0) {
-    net = H->net();
-    SolveState tmp = fin;
-    tmp.done = 0;
-    CK(cudaMemcpyAsync(H->st.p, &tmp, sizeof(tmp), cudaMemcpyHostToDevice, s));
-    if (H->n_sweep_items > 0)
-      eval_kernel<false><<<H->n_sweep_items, EVAL_THREADS, H->eval_smem, s>>>(
-          net, H->sweep_items.p, H->sweep_pts.p, H->d_groups.p, H->sweep_vals.p, H->chunk);
-    const int ub = (H->n_upd + UPDATE_WARPS - 1) / UPDATE_WARPS;
-    const size_t usmem = sizeof(double) * 2 * H->nvmax * UPDATE_WARPS;
-    if (ub > 0)
-      update_kernel<<<ub, UPDATE_WARPS * 32, usmem, s>>>(net, H->upd_list.p, H->n_upd, H->group_of.p,
-                                                          H->d_groups.p, H->sweep_vals.p, H->nvmax, 1);
-    H->launches += 2;
-    CK(cudaMemcpyAsync(H->st.p, &fin, sizeof(fin), cudaMemcpyHostToDevice, s));
+  rc = read_states(H);
+  if (rc) return rc;
+  std::vector<SolveState> fin = H->h_st;
+  // hpc_solve.py:224-234: an extra element_solver sweep at nit == MAX_ITERATIONS,
+  // for the realizations that stopped there
+  {
+    std::vector<SolveState> tmp = fin;
+    bool any = false;
+    for (int r = 0; r < R; r++) {
+      const bool extra = fin[r].nit == C->max_iterations && !fin[r].nonfinite && fin[r].status == 0;
+      tmp[r].done = extra ? 0 : 1;
+      any |= extra;
+    }
+    if (any) {
+      net = H->net();
+      CK(cudaMemcpyAsync(H->st.p, tmp.data(), sizeof(SolveState) * R, cudaMemcpyHostToDevice, s));
+      if (H->n_sweep_items > 0)
+        eval_kernel<false><<<H->n_sweep_items, EVAL_THREADS, H->eval_smem, s>>>(
+            net, H->sweep_items.p, H->sweep_pts.p, H->d_groups.p, H->sweep_vals.p, H->chunk);
+      const int ub = (H->n_upd + UPDATE_WARPS - 1) / UPDATE_WARPS;
+      const size_t usmem = sizeof(double) * 2 * H->nvmax * UPDATE_WARPS;
+      if (ub > 0)
+        update_kernel<<<ub, UPDATE_WARPS * 32, usmem, s>>>(net, H->upd_list.p, H->n_upd, H->group_of.p,
+                                                            H->d_groups.p, H->sweep_vals.p, H->nvmax, 1);
+      H->launches += 2;
+      CK(cudaMemcpyAsync(H->st.p, fin.data(), sizeof(SolveState) * R, cudaMemcpyHostToDevice, s));
+    }
   }
   CK(cudaStreamSynchronize(s));
   CK(cudaGetLastError());
-  stats.ms_iterate = ms_since(t_it);
-  stats.iterations = fin.nit;
-  stats.cnt_error = fin.cnt_error;
-  stats.error = fin.error;
-  stats.error_coef = fin.error_coef;
-  stats.error_q = fin.error_q;
-  stats.worst_element = fin.worst;
-  stats.n_unknowns = H->N;
-  stats.nnz_matrix = (int64_t)H->mcol.size();
-  stats.nnz_factors = H->nnz_factors;
-  stats.dense_tail = H->tail_k;
-  for (int i = 0; i < 8; i++) stats.tri_cycles[i] = fin.tri_cycles[i];
-  stats.ms_create_upload = H->ms_create_upload;
-  stats.ms_create_tables = H->ms_create_tables;
-  stats.ms_create_order = H->ms_create_order;
-  stats.levels_l = H->lf_nlev;
-  stats.levels_u = H->ub_nlev;
-  stats.gpu_launches = H->launches;
+  base.ms_iterate = ms_since(t_it);
+  base.gpu_launches = H->launches;
+  base.ms_create_upload = H->ms_create_upload;
+  base.ms_create_tables = H->ms_create_tables;
+  base.ms_create_order = H->ms_create_order;
   int status = ANDFN_OK;
-  if (fin.status) status = fin.status;
-  else if (fin.nonfinite) status = ANDFN_NONFINITE;
-  else if (fin.cnt_error < 2) status = ANDFN_MAX_ITERATIONS;
-  stats.status = status;
-  stats.ms_total = ms_since(t_all);
-  if (S) *S = stats;
+  H->last.assign(R, base);
+  for (int r = 0; r < R; r++) {
+    AndfnSolveStats &st = H->last[r];
+    const SolveState &f = fin[r];
+    st.iterations = f.nit;
+    st.cnt_error = f.cnt_error;
+    st.error = f.error;
+    st.error_coef = f.error_coef;
+    st.error_q = f.error_q;
+    st.worst_element = f.worst;
+    st.n_unknowns = H->sys[r].n;
+    st.nnz_matrix = (int64_t)H->sys[r].mcol.size();
+    st.nnz_factors = H->sys[r].nnz;
+    st.dense_tail = H->sys[r].tail_k;
+    st.levels_l = H->sys[r].nlev_l;
+    st.levels_u = H->sys[r].nlev_u;
+    for (int i = 0; i < 8; i++) st.tri_cycles[i] = f.tri_cycles[i];
+    int sr = ANDFN_OK;
+    if (f.status)
+      sr = f.status;
+    else if (f.nonfinite)
+      sr = ANDFN_NONFINITE;
+    else if (f.cnt_error < 2)
+      sr = ANDFN_MAX_ITERATIONS;
+    st.status = sr;
+    if (sr >= ANDFN_BAD_LAYOUT)
+      status = std::max(status, sr);
+    else if (status < ANDFN_BAD_LAYOUT)
+      status = std::max(status, sr);
+    st.ms_total = ms_since(t_all);
+  }
+  if (S)
+    for (int r = 0; r < R; r++) S[r] = H->last[r];
   return status;
 }
 
-static int download_impl(AndfnHandle *H, char *F, char *E) {
+static int download_impl(AndfnHandle *H, char *const *F, char *const *E) {
   cudaStream_t s = H->stream;
   const int64_t ne = H->ne, nf = H->nf;
   const int MC = H->MC;
@@ -2438,36 +2631,75 @@ static int download_impl(AndfnHandle *H, char *F, char *E) {
   g_d2h_bytes += (int64_t)(sizeof(cd) * coef.size() + 4 * 2 * ne + 8 * 5 * ne + 8 * dc.size() + 8 * nf);
   CK(cudaStreamSynchronize(s));
   const AndfnLayout &L = H->L;
-  for (int64_t i = 0; i < ne; i++) {
-    char *r = E + i * L.elem_size;
-    const int m = ncoef[i], n = nint[i], ty = H->h.type[i];
-    int64_t v;
-    v = m;
-    std::memcpy(r + L.e_ncoef, &v, 8);
-    v = n;
-    std::memcpy(r + L.e_nint, &v, 8);
-    std::memcpy(r + L.e_coef, &coef[(size_t)i * MC], sizeof(cd) * std::min(m, MC));
-    // thetas as calc_thetas writes them (hpc_math_functions.py:693-699)
-    double del = PI / n, start = del / 2;
-    if (ty == 1) {
-      del = 2 * PI / n;
-      start = 0.0;
+  for (int r = 0; r < H->R; r++) {
+    const int e0 = H->h.eoff[r], e1 = H->h.eoff[r + 1], f0 = H->h.foff[r], f1 = H->h.foff[r + 1];
+    for (int i = e0; i < e1; i++) {
+      char *rec = E[r] + (int64_t)(i - e0) * L.elem_size;
+      const int m = ncoef[i], n = nint[i], ty = H->h.type[i];
+      int64_t v;
+      v = m;
+      std::memcpy(rec + L.e_ncoef, &v, 8);
+      v = n;
+      std::memcpy(rec + L.e_nint, &v, 8);
+      std::memcpy(rec + L.e_coef, &coef[(size_t)i * MC], sizeof(cd) * std::min(m, MC));
+      // thetas as calc_thetas writes them (hpc_math_functions.py:693-699)
+      double del = PI / n, start = del / 2;
+      if (ty == 1) {
+        del = 2 * PI / n;
+        start = 0.0;
+      }
+      for (int k = 0; k < n; k++) {
+        double th = start + k * del;
+        std::memcpy(rec + L.e_thetas + 8 * k, &th, 8);
+      }
+      std::memcpy(rec + L.e_q, &q[i], 8);
+      std::memcpy(rec + L.e_error, &err[i], 8);
+      std::memcpy(rec + L.e_error_old, &eo[i], 8);
+      if (ty != 2) {
+        std::memcpy(rec + L.e_error_old2, &eo2[i], 8);
+        std::memcpy(rec + L.e_error_coef, &ec[i], 8);
+      }
+      if (ty == 1 || ty == 4 || ty == 5)
+        std::memcpy(rec + L.e_dpsi_corr, &dc[(size_t)i * 2 * MC], 8 * std::max(0, n - 1));
     }
-    for (int k = 0; k < n; k++) {
-      double th = start + k * del;
-      std::memcpy(r + L.e_thetas + 8 * k, &th, 8);
-    }
-    std::memcpy(r + L.e_q, &q[i], 8);
-    std::memcpy(r + L.e_error, &err[i], 8);
-    std::memcpy(r + L.e_error_old, &eo[i], 8);
-    if (ty != 2) {
-      std::memcpy(r + L.e_error_old2, &eo2[i], 8);
-      std::memcpy(r + L.e_error_coef, &ec[i], 8);
-    }
-    if (ty == 1 || ty == 4 || ty == 5)
-      std::memcpy(r + L.e_dpsi_corr, &dc[(size_t)i * 2 * MC], 8 * std::max(0, n - 1));
+    for (int f = f0; f < f1; f++) std::memcpy(F[r] + (int64_t)(f - f0) * L.frac_size + L.f_constant, &cst[f], 8);
   }
-  for (int64_t f = 0; f < nf; f++) std::memcpy(F + f * L.frac_size + L.f_constant, &cst[f], 8);
+  return 0;
+}
+
+// Points of realization r (fracture indices local to it).
+static int eval_points_impl(AndfnHandle *H, int64_t r, const int64_t *frac, const double *z, int64_t npts,
+                            double *omega, double *head) {
+  if (r < 0 || r >= H->R) {
+    set_error("realization index out of range");
+    return ANDFN_BAD_INPUT;
+  }
+  if (npts <= 0) return 0;
+  if (npts > (1LL << 31) - 1) return ANDFN_BAD_INPUT;
+  const int f0 = H->h.foff[r], nfr = H->h.foff[r + 1] - f0;
+  std::vector<int> fr(npts);
+  for (int64_t i = 0; i < npts; i++) {
+    if (frac[i] < 0 || frac[i] >= nfr) {
+      set_error("point fracture index out of range");
+      return ANDFN_BAD_INPUT;
+    }
+    fr[i] = f0 + (int)frac[i];
+  }
+  cudaStream_t s = H->stream;
+  DBuf<int> dfr;
+  DBuf<cd> dz, dom;
+  DBuf<double> dh;
+  CK(dfr.alloc(npts));
+  CK(dz.alloc(npts));
+  CK(cudaMemcpyAsync(dfr.p, fr.data(), sizeof(int) * npts, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(dz.p, z, sizeof(cd) * npts, cudaMemcpyHostToDevice, s));
+  if (omega) CK(dom.alloc(npts));
+  if (head) CK(dh.alloc(npts));
+  points_kernel<<<(unsigned)((npts + 127) / 128), 128, 0, s>>>(H->net(), dfr.p, dz.p, (int)npts, dom.p, dh.p);
+  CK(cudaGetLastError());
+  if (omega) CK(cudaMemcpyAsync(omega, dom.p, sizeof(cd) * npts, cudaMemcpyDeviceToHost, s));
+  if (head) CK(cudaMemcpyAsync(head, dh.p, sizeof(double) * npts, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
   return 0;
 }
 
@@ -2479,18 +2711,33 @@ static int download_impl(AndfnHandle *H, char *F, char *E) {
 extern "C" {
 
 const char *andfn_b200_last_error(void) { return g_last_error.c_str(); }
-const char *andfn_b200_version(void) { return "andfn_b200 0.1.0 (sm_100a, fp64)"; }
+const char *andfn_b200_version(void) { return "andfn_b200 0.2.0 (sm_100a, fp64)"; }
 
-int andfn_b200_create(AndfnHandle **out, const void *frac_recs, int64_t nf, const void *elem_recs, int64_t ne,
-                      const AndfnLayout *layout, int64_t discharge_int, int32_t device) {
+int andfn_b200_batch_create(AndfnHandle **out, int64_t R, void *const *frac_recs, const int64_t *nf,
+                            void *const *elem_recs, const int64_t *ne, const AndfnLayout *layout,
+                            int64_t discharge_int, int32_t device) {
   if (!out) return ANDFN_BAD_INPUT;
   *out = nullptr;
   if (check_layout(layout)) {
     set_error("inconsistent record layout");
     return ANDFN_BAD_LAYOUT;
   }
-  if (nf <= 0 || ne <= 0 || !frac_recs || !elem_recs || discharge_int < 1 || discharge_int > 100000) {
-    set_error("empty network or discharge_int out of range");
+  if (R < 1 || R > (1 << 20) || !frac_recs || !elem_recs || !nf || !ne || discharge_int < 1 ||
+      discharge_int > 100000) {
+    set_error("bad realization count, pointers or discharge_int");
+    return ANDFN_BAD_INPUT;
+  }
+  int64_t tot_e = 0, tot_f = 0;
+  for (int64_t r = 0; r < R; r++) {
+    if (nf[r] <= 0 || ne[r] <= 0 || !frac_recs[r] || !elem_recs[r]) {
+      set_error("empty network in the batch");
+      return ANDFN_BAD_INPUT;
+    }
+    tot_e += ne[r];
+    tot_f += nf[r];
+  }
+  if (tot_e > (1LL << 30) || tot_f > (1LL << 30)) {
+    set_error("batch too large");
     return ANDFN_BAD_INPUT;
   }
   int ndev = 0;
@@ -2524,10 +2771,8 @@ int andfn_b200_create(AndfnHandle **out, const void *frac_recs, int64_t nf, cons
     int t = atoi(v);
     if (t >= 32 && t <= SOLVE_THREADS && t % 32 == 0) H->solve_threads = t;
   }
-  H->ne = ne;
-  H->nf = nf;
   H->D = discharge_int;
-  int rc = create_impl(H, (const char *)frac_recs, (const char *)elem_recs);
+  int rc = create_impl(H, (int)R, (const char *const *)frac_recs, nf, (const char *const *)elem_recs, ne);
   if (rc) {
     delete H;
     return rc;
@@ -2536,8 +2781,20 @@ int andfn_b200_create(AndfnHandle **out, const void *frac_recs, int64_t nf, cons
   return 0;
 }
 
+int andfn_b200_create(AndfnHandle **out, const void *frac_recs, int64_t nf, const void *elem_recs, int64_t ne,
+                      const AndfnLayout *layout, int64_t discharge_int, int32_t device) {
+  void *F[1] = {const_cast<void *>(frac_recs)};
+  void *E[1] = {const_cast<void *>(elem_recs)};
+  return andfn_b200_batch_create(out, 1, F, &nf, E, &ne, layout, discharge_int, device);
+}
+
+int64_t andfn_b200_realizations(AndfnHandle *H) { return H ? H->R : 0; }
+
 int andfn_b200_upload_state(AndfnHandle *H, const void *frac_recs, const void *elem_recs) {
-  if (!H) return ANDFN_BAD_INPUT;
+  if (!H || H->R != 1) {
+    set_error("upload_state needs a single-network handle");
+    return ANDFN_BAD_INPUT;
+  }
   cudaSetDevice(H->device);
   const char *E = (const char *)elem_recs;
   const char *F = (const char *)frac_recs;
@@ -2556,7 +2813,8 @@ int andfn_b200_upload_state(AndfnHandle *H, const void *frac_recs, const void *e
     }
   }
   for (int64_t f = 0; f < H->nf; f++) H->h.constant[f] = rd_f64(F + f * L.frac_size, L.f_constant);
-  read_coefs(H, E);
+  std::fill(H->h.coef.begin(), H->h.coef.end(), mk(0.0, 0.0));
+  read_coefs(H, 0, E);
   cudaStream_t s = H->stream;
   CK(cudaMemcpyAsync(H->q0.p, H->h.q.data(), 8 * H->ne, cudaMemcpyHostToDevice, s));
   CK(cudaMemcpyAsync(H->err_in.p, H->h.err.data(), 8 * H->ne, cudaMemcpyHostToDevice, s));
@@ -2580,58 +2838,53 @@ int andfn_b200_reset_state(AndfnHandle *H) {
   return 0;
 }
 
-int andfn_b200_run(AndfnHandle *H, const AndfnConstants *constants, AndfnSolveStats *stats) {
+int andfn_b200_batch_run(AndfnHandle *H, const AndfnConstants *constants, AndfnSolveStats *stats) {
   if (!H || !constants) return ANDFN_BAD_INPUT;
   cudaSetDevice(H->device);
   return run_impl(H, constants, stats);
 }
 
-int andfn_b200_download(AndfnHandle *H, void *frac_recs, void *elem_recs) {
-  if (!H || !frac_recs || !elem_recs) return ANDFN_BAD_INPUT;
+int andfn_b200_run(AndfnHandle *H, const AndfnConstants *constants, AndfnSolveStats *stats) {
+  if (!H || !constants) return ANDFN_BAD_INPUT;
+  if (H->R != 1) {
+    set_error("run() on a batch handle: use andfn_b200_batch_run");
+    return ANDFN_BAD_INPUT;
+  }
   cudaSetDevice(H->device);
-  return download_impl(H, (char *)frac_recs, (char *)elem_recs);
+  return run_impl(H, constants, stats);
 }
 
-static int eval_points_impl(AndfnHandle *H, const int64_t *frac, const double *z, int64_t npts, double *omega,
-                            double *head) {
-  if (npts <= 0) return 0;
-  if (npts > (1LL << 31) - 1) return ANDFN_BAD_INPUT;
-  std::vector<int> fr(npts);
-  for (int64_t i = 0; i < npts; i++) {
-    if (frac[i] < 0 || frac[i] >= H->nf) {
-      set_error("point fracture index out of range");
-      return ANDFN_BAD_INPUT;
-    }
-    fr[i] = (int)frac[i];
-  }
-  cudaStream_t s = H->stream;
-  DBuf<int> dfr;
-  DBuf<cd> dz, dom;
-  DBuf<double> dh;
-  CK(dfr.alloc(npts));
-  CK(dz.alloc(npts));
-  CK(cudaMemcpyAsync(dfr.p, fr.data(), sizeof(int) * npts, cudaMemcpyHostToDevice, s));
-  CK(cudaMemcpyAsync(dz.p, z, sizeof(cd) * npts, cudaMemcpyHostToDevice, s));
-  if (omega) CK(dom.alloc(npts));
-  if (head) CK(dh.alloc(npts));
-  points_kernel<<<(unsigned)((npts + 127) / 128), 128, 0, s>>>(H->net(), dfr.p, dz.p, (int)npts, dom.p, dh.p);
-  CK(cudaGetLastError());
-  if (omega) CK(cudaMemcpyAsync(omega, dom.p, sizeof(cd) * npts, cudaMemcpyDeviceToHost, s));
-  if (head) CK(cudaMemcpyAsync(head, dh.p, sizeof(double) * npts, cudaMemcpyDeviceToHost, s));
-  CK(cudaStreamSynchronize(s));
-  return 0;
+int andfn_b200_batch_download(AndfnHandle *H, void *const *frac_recs, void *const *elem_recs) {
+  if (!H || !frac_recs || !elem_recs) return ANDFN_BAD_INPUT;
+  cudaSetDevice(H->device);
+  return download_impl(H, (char *const *)frac_recs, (char *const *)elem_recs);
+}
+
+int andfn_b200_download(AndfnHandle *H, void *frac_recs, void *elem_recs) {
+  if (!H || !frac_recs || !elem_recs || H->R != 1) return ANDFN_BAD_INPUT;
+  cudaSetDevice(H->device);
+  char *F[1] = {(char *)frac_recs};
+  char *E[1] = {(char *)elem_recs};
+  return download_impl(H, F, E);
 }
 
 int andfn_b200_eval_heads(AndfnHandle *H, const int64_t *frac, const double *z, int64_t npts, double *out) {
   if (!H || (npts > 0 && (!frac || !z || !out))) return ANDFN_BAD_INPUT;
   cudaSetDevice(H->device);
-  return eval_points_impl(H, frac, z, npts, nullptr, out);
+  return eval_points_impl(H, 0, frac, z, npts, nullptr, out);
+}
+
+int andfn_b200_batch_eval_heads(AndfnHandle *H, int64_t r, const int64_t *frac, const double *z, int64_t npts,
+                                double *out) {
+  if (!H || (npts > 0 && (!frac || !z || !out))) return ANDFN_BAD_INPUT;
+  cudaSetDevice(H->device);
+  return eval_points_impl(H, r, frac, z, npts, nullptr, out);
 }
 
 int andfn_b200_eval_omega(AndfnHandle *H, const int64_t *frac, const double *z, int64_t npts, double *out) {
   if (!H || (npts > 0 && (!frac || !z || !out))) return ANDFN_BAD_INPUT;
   cudaSetDevice(H->device);
-  return eval_points_impl(H, frac, z, npts, out, nullptr);
+  return eval_points_impl(H, 0, frac, z, npts, out, nullptr);
 }
 
 void andfn_b200_destroy(AndfnHandle *H) {
@@ -2693,30 +2946,42 @@ int andfn_b200_fp64_peak(int32_t device, double *tflops) {
   return 0;
 }
 
-int andfn_b200_solve(void *frac_recs, int64_t nf, void *elem_recs, int64_t ne, const AndfnLayout *layout,
-                     int64_t discharge_int, const AndfnConstants *constants, AndfnSolveStats *stats) {
+int andfn_b200_batch_solve(int64_t R, void *const *frac_recs, const int64_t *nf, void *const *elem_recs,
+                           const int64_t *ne, const AndfnLayout *layout, int64_t discharge_int,
+                           const AndfnConstants *constants, AndfnSolveStats *stats) {
   auto t0 = std::chrono::steady_clock::now();
   g_h2d_bytes = g_d2h_bytes = 0;
   AndfnHandle *H = nullptr;
-  int rc = andfn_b200_create(&H, frac_recs, nf, elem_recs, ne, layout, discharge_int, -1);
+  int rc = andfn_b200_batch_create(&H, R, frac_recs, nf, elem_recs, ne, layout, discharge_int, -1);
   if (rc) return rc;
-  double ms_up = ms_since(t0);
-  AndfnSolveStats st;
-  std::memset(&st, 0, sizeof(st));
-  rc = andfn_b200_run(H, constants, &st);
+  const double ms_up = ms_since(t0);
+  rc = run_impl(H, constants, nullptr);
+  double ms_down = 0;
   if (rc == ANDFN_OK || rc == ANDFN_MAX_ITERATIONS || rc == ANDFN_NONFINITE) {
     auto t1 = std::chrono::steady_clock::now();
-    int rc2 = andfn_b200_download(H, frac_recs, elem_recs);
-    st.ms_download = ms_since(t1);
+    int rc2 = download_impl(H, (char *const *)frac_recs, (char *const *)elem_recs);
+    ms_down = ms_since(t1);
     if (rc2) rc = rc2;
   }
-  st.ms_upload = ms_up;
-  st.h2d_bytes = g_h2d_bytes;  // create + run + download of this call
-  st.d2h_bytes = g_d2h_bytes;
+  const double ms_tot = ms_since(t0);
+  if (stats)
+    for (int64_t r = 0; r < R && r < (int64_t)H->last.size(); r++) {
+      stats[r] = H->last[r];
+      stats[r].ms_upload = ms_up;
+      stats[r].ms_download = ms_down;
+      stats[r].ms_total = ms_tot;
+      stats[r].h2d_bytes = g_h2d_bytes;
+      stats[r].d2h_bytes = g_d2h_bytes;
+    }
   andfn_b200_destroy(H);
-  st.ms_total = ms_since(t0);
-  if (stats) *stats = st;
   return rc;
+}
+
+int andfn_b200_solve(void *frac_recs, int64_t nf, void *elem_recs, int64_t ne, const AndfnLayout *layout,
+                     int64_t discharge_int, const AndfnConstants *constants, AndfnSolveStats *stats) {
+  void *F[1] = {frac_recs};
+  void *E[1] = {elem_recs};
+  return andfn_b200_batch_solve(1, F, &nf, E, &ne, layout, discharge_int, constants, stats);
 }
 
 }  // extern "C"

@@ -396,3 +396,11 @@ def power_law_fisher(seed, nf, L, rmin=0.5, rmax=20.0, alpha=2.6, kappa=5.0, log
     order = np.argsort(-r, kind="stable")  # large fractures first
     return build(c[order], n[order], r[order], t[order], ncoef, nint, se_factor,
                  heads=((0.0, 1.0), (L, 0.0)), box=L, keep=keep, **kw)
+
+
+def to_records_batch(nets):
+    """Records of several networks with one shared layout (the batch API needs
+    a common MAX_NCOEF / MAX_ELEMENTS)."""
+    mc = max(max(1, max(e.ncoef for e in n.elements)) for n in nets)
+    me = max(max(1, max(len(lst) for lst in n.frac_elems)) for n in nets)
+    return [to_records(n, max_ncoef=mc, max_elements=me) for n in nets]

@@ -135,6 +135,39 @@ void andfn_b200_destroy(AndfnHandle *h);
 /* CUDA stream the handle launches on (cudaStream_t as void*). */
 void *andfn_b200_stream(AndfnHandle *h);
 
+/* ---- batched realizations ------------------------------------------------
+ * R independent networks (e.g. Monte-Carlo realizations of one fracture
+ * statistics) solved by one launch sequence: every kernel of an outer
+ * iteration covers all realizations, each realization keeps its own loop
+ * state, factorisation and convergence test, and stops iterating on its own
+ * (the reference solves them one at a time with hpc_solve.solve,
+ * andfn/hpc/hpc_solve.py:55-257; each realization's result equals that
+ * call's).  Arrays of length R give each realization's records and sizes;
+ * stats, where given, has R entries.  The single-network functions above are
+ * the R = 1 case; run() and download() refuse handles with R > 1. */
+int andfn_b200_batch_solve(int64_t R, void *const *frac_recs, const int64_t *nf,
+                           void *const *elem_recs, const int64_t *ne,
+                           const AndfnLayout *layout, int64_t discharge_int,
+                           const AndfnConstants *constants,
+                           AndfnSolveStats *stats);
+int andfn_b200_batch_create(AndfnHandle **out, int64_t R,
+                            void *const *frac_recs, const int64_t *nf,
+                            void *const *elem_recs, const int64_t *ne,
+                            const AndfnLayout *layout, int64_t discharge_int,
+                            int32_t device);
+/* Returns the worst status over the realizations (per-realization status in
+ * stats[r].status). */
+int andfn_b200_batch_run(AndfnHandle *h, const AndfnConstants *constants,
+                         AndfnSolveStats *stats);
+int andfn_b200_batch_download(AndfnHandle *h, void *const *frac_recs,
+                              void *const *elem_recs);
+/* Heads at points of realization r (frac[] indexes that realization's
+ * fractures). */
+int andfn_b200_batch_eval_heads(AndfnHandle *h, int64_t r, const int64_t *frac,
+                                const double *z, int64_t npts, double *out);
+/* Number of realizations held by a handle. */
+int64_t andfn_b200_realizations(AndfnHandle *h);
+
 /* Per-kernel device timing of the outer iterations (no reference
  * counterpart; the reference only logs wall-clock phases,
  * andfn/hpc/hpc_solve.py:109-122,149-215).  When on, run() records CUDA

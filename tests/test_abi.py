@@ -5,6 +5,7 @@ import os
 import re
 
 import numpy as np
+import pytest
 
 from conftest import ROOT, load_golden
 
@@ -51,3 +52,34 @@ def test_bad_layout_rejected_before_device_use():
                              buf.ctypes.data_as(ctypes.c_void_p), 1, ctypes.byref(lay), 50, -1)
     assert rc == 10
     assert "layout" in _ffi.last_error()
+
+
+def test_batch_inputs_rejected_before_device_use():
+    from andfn_b200 import _ffi
+    from andfn_b200.records import layout_of
+    L = _ffi.lib()
+    g = load_golden("mixed")
+    F, E = g["F_in"].copy(), g["E_in"].copy()
+    lay = layout_of(E.dtype, F.dtype)
+    h = ctypes.c_void_p()
+    fp = (ctypes.c_void_p * 2)(F.ctypes.data, F.ctypes.data)
+    ep = (ctypes.c_void_p * 2)(E.ctypes.data, E.ctypes.data)
+    nf = np.array([len(F), 0], np.int64)  # second realization empty
+    ne = np.array([len(E), len(E)], np.int64)
+    rc = L.andfn_b200_batch_create(ctypes.byref(h), 2, fp, nf.ctypes.data_as(ctypes.c_void_p), ep,
+                                   ne.ctypes.data_as(ctypes.c_void_p), ctypes.byref(lay), 50, -1)
+    assert rc == 11 and "empty" in _ffi.last_error()
+    rc = L.andfn_b200_batch_create(ctypes.byref(h), 0, fp, nf.ctypes.data_as(ctypes.c_void_p), ep,
+                                   ne.ctypes.data_as(ctypes.c_void_p), ctypes.byref(lay), 50, -1)
+    assert rc == 11
+    assert L.andfn_b200_realizations(None) == 0
+
+
+def test_batch_records_must_share_dtypes():
+    import andfn_b200
+    from andfn_b200.records import element_dtype
+    g = load_golden("mixed")
+    F, E = g["F_in"].copy(), g["E_in"].copy()
+    E2 = np.zeros(len(E), element_dtype(12))
+    with pytest.raises(ValueError):
+        andfn_b200.solve_batch([(F, E), (F.copy(), E2)], 50, g["constants_1"])

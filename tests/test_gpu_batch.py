@@ -1,0 +1,129 @@
+"""Batched realizations: every realization of a batch must give what a
+separate solve of it gives.
+
+  * against the reference's golden outputs (several networks, one batch);
+  * bit-for-bit against separate GPU solves of the same networks (the batch
+    runs the same per-element arithmetic in the same order; only the launch
+    is shared), including iteration counts that differ between realizations;
+  * against the oracle on generated networks, with realizations that stop at
+    MAX_ITERATIONS (the extra sweep) beside ones that converge;
+  * adaptive coefficient growth inside a batch;
+  * heads of one realization through the batched handle.
+Tolerances as in test_gpu_parity.
+"""
+import numpy as np
+import pytest
+
+from conftest import load_golden
+from test_gpu_parity import _compare
+
+pytestmark = pytest.mark.gpu
+
+
+def _generated(seeds, nf=40):
+    from andfn_b200 import network as nw
+    return nw.to_records_batch([nw.uniform_discs(s, nf=nf, L=20.0) for s in seeds])
+
+
+def _recast(a, dtype):
+    """Copy of record array a in a wider dtype (same fields, larger arrays)."""
+    out = np.zeros(len(a), dtype)
+    for name in a.dtype.names:
+        src = a[name]
+        if src.ndim == 1:
+            out[name] = src
+        else:
+            out[name][:, : src.shape[1]] = src
+    return out
+
+
+def test_batch_matches_reference_golden():
+    import andfn_b200
+    cases = ["c1_seed3", "c1_seed13", "c1_trivial_seed0", "c1_seed3"]
+    gs = [load_golden(c) for c in cases]
+    nets = [(g["F_in"].copy(), g["E_in"].copy()) for g in gs]
+    c = gs[0]["constants_200"]
+    st = andfn_b200.solve_batch(nets, 50, c)
+    assert len(st) == len(cases)
+    for (F, E), g, s, name in zip(nets, gs, st, cases):
+        assert s["status"] in (0, 1), s
+        _compare(E, F, g["E_out_200"], g["F_out_200"], ("batch", name))
+    # the duplicated realization is identical to its first copy
+    assert np.array_equal(nets[0][1]["coef"], nets[3][1]["coef"])
+
+
+def test_batch_equals_separate_solves_bitwise():
+    import andfn_b200
+    from andfn_b200.records import default_constants
+    recs = _generated(range(1, 9))
+    c = default_constants(MAX_ITERATIONS=60, MAX_ERROR=1e-8, MAX_NCOEF=10)
+    batch = [(F.copy(), E.copy()) for F, E in recs]
+    st = andfn_b200.solve_batch(batch, 50, c)
+    its = set()
+    for (F0, E0), (Fb, Eb), s in zip(recs, batch, st):
+        F, E = F0.copy(), E0.copy()
+        andfn_b200.solve(F, E, 50, c)
+        s1 = dict(andfn_b200.last_stats)
+        assert s["iterations"] == s1["iterations"] and s["status"] == s1["status"], (s, s1)
+        its.add(s["iterations"])
+        for name in ("coef", "q", "error", "error_coef", "dpsi_corr", "ncoef", "nint"):
+            assert np.array_equal(Eb[name], E[name], equal_nan=True), name
+        assert np.array_equal(Fb["constant"], F["constant"])
+    assert len(its) > 1  # realizations stopped at different iterations
+
+
+def test_batch_matches_oracle_with_max_iterations_stop():
+    """MAX_ITERATIONS 12: some realizations converge, the others stop at 12
+    and take the reference's extra sweep (hpc_solve.py:224-234)."""
+    import andfn_b200
+    from andfn_b200.records import default_constants
+    from oracle import oracle as orc
+    g = load_golden("mixed")
+    gen = _generated(range(11, 16))
+    Fd, Ed = gen[0][0].dtype, gen[0][1].dtype
+    assert Ed["coef"].shape[0] >= g["E_in"].dtype["coef"].shape[0]
+    recs = [(_recast(g["F_in"], Fd), _recast(g["E_in"], Ed))] + gen
+    c = default_constants(MAX_ITERATIONS=12, MAX_ERROR=1e-8, MAX_NCOEF=10)
+    batch = [(F.copy(), E.copy()) for F, E in recs]
+    st = andfn_b200.solve_batch(batch, 50, c)
+    for r, ((F0, E0), (Fb, Eb), s) in enumerate(zip(recs, batch, st)):
+        Fo, Eo = F0.copy(), E0.copy()
+        so = {}
+        orc.solve(Fo, Eo, 50, c, stats=so)
+        assert s["iterations"] == so["iterations"], (r, s["iterations"], so["iterations"])
+        _compare(Eb, Fb, Eo, Fo, ("oracle", r))
+
+
+def test_batch_adaptive_growth_matches_reference_golden():
+    import andfn_b200
+    g = load_golden("c1_seed3_adaptive")
+    k = g["its"][-1]
+    nets = [(g["F_in"].copy(), g["E_in"].copy()) for _ in range(3)]
+    st = andfn_b200.solve_batch(nets, int(g["D"]), g[f"constants_{k}"])
+    for (F, E), s in zip(nets, st):
+        assert s["status"] in (0, 1), s
+        assert (E["ncoef"] > g["E_in"]["ncoef"]).any()
+        _compare(E, F, g[f"E_out_{k}"], g[f"F_out_{k}"], ("adaptive batch", int(k)))
+
+
+def test_batch_handle_heads_and_rerun():
+    import andfn_b200
+    from andfn_b200.records import default_constants
+    recs = _generated(range(21, 25))
+    c = default_constants(MAX_ITERATIONS=40, MAX_ERROR=1e-8, MAX_NCOEF=10)
+    batch = [(F.copy(), E.copy()) for F, E in recs]
+    rng = np.random.default_rng(0)
+    with andfn_b200.BatchSolver(batch, 50) as bs:
+        assert bs.R == 4
+        st1 = bs.run(c)
+        st2 = bs.run(c)  # a second run restarts from the uploaded state
+        assert [s["iterations"] for s in st1] == [s["iterations"] for s in st2]
+        bs.download()
+        for r, (F, E) in enumerate(batch):
+            n = 500
+            fr = rng.integers(0, len(F), n)
+            z = F["radius"][fr] * 0.9 * np.sqrt(rng.uniform(size=n)) * np.exp(2j * np.pi * rng.uniform(size=n))
+            hb = bs.eval_heads(r, fr, z)
+            with andfn_b200.Solver(F, E, 50) as s:
+                hs = s.eval_heads(fr, z)
+            assert np.array_equal(hb, hs, equal_nan=True), r
