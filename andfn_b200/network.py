@@ -404,3 +404,47 @@ def to_records_batch(nets):
     mc = max(max(1, max(e.ncoef for e in n.elements)) for n in nets)
     me = max(max(1, max(len(lst) for lst in n.frac_elems)) for n in nets)
     return [to_records(n, max_ncoef=mc, max_elements=me) for n in nets]
+
+
+def _seg_dist(z, a, b):
+    d = b - a
+    t = 0.0 if d == 0 else min(1.0, max(0.0, ((z - a) * d.conjugate()).real / abs(d) ** 2))
+    return abs(z - (a + t * d))
+
+
+def place_wells(net, rng, n, radius=0.05, head=(0.0, 1.0), clearance=10.0, rim=0.8, tries=200):
+    """n head-specified wells at uniform random points (inside rim * R) of
+    random fractures, at least clearance * radius away from every line
+    element of that fracture and from the other wells."""
+    nf = len(net.radii)
+    for _ in range(n):
+        for _t in range(tries):
+            f = int(rng.integers(0, nf))
+            R = float(net.radii[f])
+            z = rim * R * np.sqrt(rng.uniform()) * np.exp(2j * np.pi * rng.uniform())
+            ok = True
+            for el in net.frac_elems[f]:
+                e = net.elements[el]
+                if e.type in (0, 3, 5):
+                    ep = e.ep1 if (e.type == 0 and e.frac1 == f) else e.ep0
+                    ok = _seg_dist(z, complex(ep[0]), complex(ep[1])) > clearance * radius
+                elif e.type in (2, 4):
+                    ok = abs(z - e.center) > clearance * radius + e.radius
+                if not ok:
+                    break
+            if ok:
+                add_well(net, f, z, radius, float(rng.uniform(*head)))
+                break
+
+
+def batch_realization(seed, L=40.0, nf_range=(200, 800), wells=4, ncoef=15, nint=30, **kw):
+    """One realization of the batched workload: N_gen ~ U{200..800} discs drawn
+    as power_law_fisher in an L cube, head planes 1 / 0 at x = 0 / L, then
+    `wells` head-specified wells (radius 0.05 m, head U[0, 1]) on random
+    fractures; the fractures connected to a head boundary (plane or well) are
+    kept, as check_connectivity does."""
+    rng = np.random.default_rng([seed, 7])
+    nf = int(rng.integers(nf_range[0], nf_range[1] + 1))
+    net = power_law_fisher(seed, nf, L, ncoef=ncoef, nint=nint, keep="all", **kw)
+    place_wells(net, rng, wells)
+    return _prune(net, "connected")

@@ -54,6 +54,23 @@ def constants():
     return default_constants(MAX_ITERATIONS=200, MAX_ERROR=MAX_ERROR, MAX_NCOEF=20)
 
 
+BATCH_R = 256
+BATCH_WORKLOAD = ("batched: 256 realizations, each N_gen ~ U{200..800} power-law/Fisher discs in a 40 m cube "
+                  "(seeds 1000..1255), heads 1 / 0 on the x faces, 4 head-specified wells (r 0.05 m, head U[0, 1]) "
+                  "per realization, clusters connected to a head boundary kept, ncoef 15, nint 30, discharge_int 50, "
+                  "MAX_ERROR 1e-8")
+
+
+def build_batch(R=BATCH_R, seed0=1000):
+    from andfn_b200 import network as nw
+    return nw.to_records_batch([nw.batch_realization(seed0 + i) for i in range(R)])
+
+
+def batch_constants():
+    from andfn_b200.records import default_constants
+    return default_constants(MAX_ITERATIONS=200, MAX_ERROR=MAX_ERROR, MAX_NCOEF=15)
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -302,6 +319,7 @@ def run_gpu(args):
             fl = work["eval_sweep_flops"] if k == "eval_sweep" else work["eval_rhs_flops"]
             ev[k] = {"achieved_tflops": fl / (per[k] * 1e-3) / 1e12, "frac_of_fp64": fl / (per[k] * 1e-3) / 1e12 / fp64_tflops,
                      "avg_us": per[k] * 1e3}
+    batched = None if args.no_batch else run_batched(args, device, flush)
     if rank == 0:
         cpu = None
         if not args.no_cpu:
@@ -321,11 +339,85 @@ def run_gpu(args):
                 "gpu_launches": int(launches), "roofline": roof, "kernels_us": {k: (v * 1e3 if v else None) for k, v in per.items()},
                 "kernel_share": {k: kt[k][0] / max(1e-12, sum(v[0] for v in kt.values())) for k in kt},
                 "eval_roofline": ev, "phase_ms": {k: stats[k] for k in ("ms_setup", "ms_factor", "ms_iterate")},
-                "fp64_peak_tflops": fp64_tflops, "clocks": clk, "cpu_baseline": cpu}
+                "fp64_peak_tflops": fp64_tflops, "clocks": clk, "cpu_baseline": cpu, "batched": batched}
         print(json.dumps(line), flush=True)
     solver.close()
     if ws > 1:
         torch.distributed.destroy_process_group()
+
+
+def run_batched(args, device, flush, sample=32):
+    """Batched realizations on one GPU: one BatchSolver run over all of them
+    against the same realizations solved one at a time by the plain handle
+    API (a sample of them, timed the same way)."""
+    import torch
+    import andfn_b200
+    recs = build_batch()
+    c = batch_constants()
+    D = 50
+    bs = andfn_b200.BatchSolver([(F.copy(), E.copy()) for F, E in recs], D, device=device)
+    stream = torch.cuda.ExternalStream(bs.stream())
+    for _ in range(args.warmup):
+        bs.run(c)
+    torch.cuda.synchronize()
+    bs.set_profiling(True)
+    ms = []
+    st = []
+    launches = 0
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        st = bs.run(c)
+        b.record(stream)
+        b.synchronize()
+        ms.append(a.elapsed_time(b))
+        launches += st[0]["gpu_launches"]
+    kt = bs.kernel_times()
+    bs.close()
+    R = len(recs)
+    value = R * args.steps / (float(np.sum(ms)) / 1e3)
+    # the same realizations through the plain single-network path
+    plain_ms = []
+    for F, E in recs[:sample]:
+        with andfn_b200.Solver(F.copy(), E.copy(), D, device=device) as s1:
+            s1.run(c)  # warm-up
+            flush.zero_()
+            torch.cuda.synchronize()
+            st1 = torch.cuda.ExternalStream(s1.stream())
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(st1)
+            s1.run(c)
+            b.record(st1)
+            b.synchronize()
+            plain_ms.append(a.elapsed_time(b))
+    plain_rate = len(plain_ms) / (float(np.sum(plain_ms)) / 1e3)
+    # end to end from host records (one call per batch)
+    e2e = []
+    for i in range(2):
+        nets = [(F.copy(), E.copy()) for F, E in recs]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sts = andfn_b200.solve_batch(nets, D, c)
+        if i:
+            e2e.append(time.perf_counter() - t0)
+    its = np.array([x["iterations"] for x in st])
+    status = np.array([x["status"] for x in st])
+    return {"workload": BATCH_WORKLOAD, "realizations": R, "fractures": int(sum(len(F) for F, _ in recs)),
+            "elements": int(sum(len(E) for _, E in recs)), "value": value, "unit": "realizations/s",
+            "ms_per_step": float(np.mean(ms)), "gpu_launches_per_step": launches / args.steps,
+            "e2e": {"value": R / float(np.mean(e2e)), "unit": "realizations/s",
+                    "h2d_bytes_per_step": int(sts[0]["h2d_bytes"]), "d2h_bytes_per_step": int(sts[0]["d2h_bytes"])},
+            "plain_sequential": {"value": plain_rate, "unit": "realizations/s", "sample": len(plain_ms),
+                                 "ms_per_realization": float(np.mean(plain_ms))},
+            "speedup_vs_plain": value / plain_rate,
+            "iterations": {"max": int(its.max()), "mean": float(its.mean())},
+            "status_counts": {str(k): int(v) for k, v in zip(*np.unique(status, return_counts=True))},
+            "phase_ms": {k: st[0][k] for k in ("ms_setup", "ms_factor", "ms_iterate")},
+            "kernels_ms_per_step": {k: v[0] / args.steps for k, v in kt.items()}}
 
 
 def aggregate_ranks(total_ms: float, steps: int, world_size: int, device=None) -> tuple[float, float]:
@@ -358,6 +450,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-realizations measurement")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

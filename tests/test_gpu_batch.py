@@ -127,3 +127,24 @@ def test_batch_handle_heads_and_rerun():
             with andfn_b200.Solver(F, E, 50) as s:
                 hs = s.eval_heads(fr, z)
             assert np.array_equal(hb, hs, equal_nan=True), r
+
+
+def test_batch_realizations_with_wells_match_oracle():
+    """The batched workload's own recipe (uneven sizes, head-specified wells,
+    clusters connected to any head boundary kept): each realization vs the
+    oracle."""
+    import andfn_b200
+    from andfn_b200 import network as nw
+    from andfn_b200.records import default_constants
+    from oracle import oracle as orc
+    recs = nw.to_records_batch([nw.batch_realization(1000 + i) for i in range(8)])
+    assert all((E["_type"] == 2).sum() == 4 for _, E in recs)
+    c = default_constants(MAX_ITERATIONS=200, MAX_ERROR=1e-8, MAX_NCOEF=15)
+    batch = [(F.copy(), E.copy()) for F, E in recs]
+    st = andfn_b200.solve_batch(batch, 50, c)
+    for r, ((F0, E0), (Fb, Eb), s) in enumerate(zip(recs, batch, st)):
+        Fo, Eo = F0.copy(), E0.copy()
+        so = {}
+        orc.solve(Fo, Eo, 50, c, stats=so)
+        assert s["iterations"] == so["iterations"], (r, s["iterations"], so["iterations"])
+        _compare(Eb, Fb, Eo, Fo, ("wells", r))
