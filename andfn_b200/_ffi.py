@@ -18,7 +18,8 @@ EXPORTS = ("andfn_b200_solve", "andfn_b200_create", "andfn_b200_upload_state", "
            "andfn_b200_destroy", "andfn_b200_stream", "andfn_b200_last_error", "andfn_b200_version",
            "andfn_b200_set_profiling", "andfn_b200_kernel_times", "andfn_b200_fp64_peak",
            "andfn_b200_batch_solve", "andfn_b200_batch_create", "andfn_b200_batch_run",
-           "andfn_b200_batch_download", "andfn_b200_batch_eval_heads", "andfn_b200_realizations")
+           "andfn_b200_batch_download", "andfn_b200_batch_eval_heads", "andfn_b200_realizations",
+           "andfn_b200_eval_heads_noalloc")
 
 STATUS = {0: "ok", 1: "max_iterations", 2: "nonfinite", 3: "singular", 10: "bad_layout", 11: "bad_input",
           12: "cuda_error", 13: "no_device", 14: "out_of_memory"}
@@ -66,6 +67,7 @@ def lib() -> ctypes.CDLL:
         ("andfn_b200_batch_download", ctypes.c_int, [P, P, P]),
         ("andfn_b200_batch_eval_heads", ctypes.c_int, [P, I64, P, P, I64, P]),
         ("andfn_b200_realizations", I64, [P]),
+        ("andfn_b200_eval_heads_noalloc", ctypes.c_int, [P, P, P, I64, P]),
     ):
         fn = getattr(L, name)
         fn.restype = res

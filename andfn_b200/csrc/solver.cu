@@ -2985,3 +2985,149 @@ int andfn_b200_solve(void *frac_recs, int64_t nf, void *elem_recs, int64_t ne, c
 }
 
 }  // extern "C"
+
+// ==========================================================================
+// Head evaluation without device allocation.
+//
+// andfn_b200_eval_heads allocates device buffers for the points on every
+// call (cudaMalloc, and cudaFree, which waits for the whole device).  Some
+// callers cannot do that: a process whose memory pool already holds the
+// device memory it is allowed, or a loop that must not stall other streams
+// on the device.  This variant stages the points in one fixed device array
+// of NOALLOC_MAX_POINTS entries that lives in the library image, so a call
+// allocates nothing on the device or the host.
+//
+// * The first call on a device looks up the array's address
+//   (cudaGetSymbolAddress, with that device current) and caches it; make
+//   that first call before any stream capture on the device.
+// * Nothing in the array has to start at zero: every entry the kernel reads
+//   is copied in by the same call first, and the kernel writes every result
+//   entry that is copied out.
+// * There is one array per device, shared by all handles: calls that
+//   overlap in time on one device (from several host threads) race on it and
+//   must be serialised by the caller.
+// ==========================================================================
+namespace andfn {
+
+static constexpr int NOALLOC_MAX_POINTS = 65536;
+
+struct NoAllocScratch {
+  int64_t frac[NOALLOC_MAX_POINTS];  // fracture of each point (local index)
+  cd z[NOALLOC_MAX_POINTS];          // point in the fracture's plane
+  double head[NOALLOC_MAX_POINTS];   // result
+};
+
+static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
+
+// Omega_f(z) of one point: the series of every element of fracture f, as
+// points_kernel evaluates them (hpc_fracture.py:52-94, exclude = -1).
+__device__ __forceinline__ cd omega_at(const Net &net, int f, cd zz) {
+  double ar = net.constant[f], ai = 0.0;
+  for (int k = net.fptr[f]; k < net.fptr[f + 1]; k++) {
+    const int el = net.felem[k];
+    const int ty = net.type[el];
+    const int m = net.ncoef[el];
+    const cd *c = net.coef + (size_t)el * net.MC;
+    const bool neg = (ty == 0 && net.frac0[el] != f);
+    const double sg = neg ? -1.0 : 1.0;
+    const double qk = sg * net.q[el] / (2 * PI);
+    if (ty == 0 || ty == 3 || ty == 5) {
+      const cd *ep = neg ? net.ep1 + 2 * el : net.ep0 + 2 * el;
+      cd inv = recip(ep[1] - ep[0]);
+      cd ab = ep[0] + ep[1];
+      cd Z = fma_c(2.0 * inv, zz, mk(-(ab.re * inv.re - ab.im * inv.im), -(ab.re * inv.im + ab.im * inv.re)));
+      cd chi = exterior_chi(Z);
+      if (m > 0) {
+        cd w = recip(chi);
+        cd r = sg * c[m - 1];
+        for (int j = m - 2; j >= 0; j--) r = fma_c(r, w, sg * c[j]);
+        ar += r.re;
+        ai += r.im;
+      }
+      if (ty != 5) {
+        ar += qk * 0.5 * log(norm2(chi));
+        ai += qk * atan2(chi.im, chi.re);
+      }
+    } else if (ty == 1) {
+      cd chi = (1.0 / net.radius[el]) * zz;
+      if (m > 0) {
+        cd r = c[m - 1];
+        for (int j = m - 2; j >= 0; j--) r = fma_c(r, chi, c[j]);
+        ar += r.re;
+        ai += r.im;
+      }
+    } else if (ty == 2) {
+      cd chi = (1.0 / net.radius[el]) * (zz - net.center[el]);
+      if (norm2(chi) < (1.0 - 1e-12) * (1.0 - 1e-12)) {
+        ar = NAN;
+        ai = NAN;
+      } else {
+        ar += qk * 0.5 * log(norm2(chi));
+        ai += qk * atan2(chi.im, chi.re);
+      }
+    } else if (ty == 4) {
+      cd chi = (1.0 / net.radius[el]) * (zz - net.center[el]);
+      if (norm2(chi) < (1.0 - 1e-10) * (1.0 - 1e-10)) {
+        ar = NAN;
+        ai = NAN;
+      } else if (m > 0) {
+        cd w = recip(chi);
+        cd r = c[m - 1];
+        for (int j = m - 2; j >= 0; j--) r = fma_c(r, w, c[j]);
+        ar += r.re;
+        ai += r.im;
+      }
+    }
+  }
+  return mk(ar, ai);
+}
+
+// One thread per point; fracture indices are local to the realization whose
+// fractures start at f0.
+__global__ void heads_noalloc_kernel(Net net, NoAllocScratch *s, int npts, int f0) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= npts) return;
+  const int f = f0 + (int)s->frac[i];
+  s->head[i] = omega_at(net, f, s->z[i]).re / net.t[f];
+}
+
+static NoAllocScratch *g_noalloc_ptr[64] = {};
+
+}  // namespace andfn
+
+extern "C" int andfn_b200_eval_heads_noalloc(AndfnHandle *H, const int64_t *frac, const double *z, int64_t npts,
+                                             double *out) {
+  if (!H || (npts > 0 && (!frac || !z || !out)) || npts < 0) return ANDFN_BAD_INPUT;
+  if (npts > NOALLOC_MAX_POINTS) {
+    set_error("eval_heads_noalloc: more points than its fixed device array holds (65536); split the call or "
+              "use andfn_b200_eval_heads");
+    return ANDFN_BAD_INPUT;
+  }
+  const int64_t nfr = H->h.foff[1] - H->h.foff[0];
+  for (int64_t i = 0; i < npts; i++)
+    if (frac[i] < 0 || frac[i] >= nfr) {
+      set_error("point fracture index out of range");
+      return ANDFN_BAD_INPUT;
+    }
+  if (H->device < 0 || H->device >= 64) {
+    set_error("eval_heads_noalloc: device ordinal above 63");
+    return ANDFN_NO_DEVICE;
+  }
+  CK(cudaSetDevice(H->device));
+  NoAllocScratch *s = g_noalloc_ptr[H->device];
+  if (!s) {  // first call on this device: look the array up once
+    void *p = nullptr;
+    CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    s = static_cast<NoAllocScratch *>(p);
+    g_noalloc_ptr[H->device] = s;
+  }
+  if (npts == 0) return 0;
+  cudaStream_t st = H->stream;
+  CK(cudaMemcpyAsync(s->frac, frac, sizeof(int64_t) * npts, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(s->z, z, sizeof(cd) * npts, cudaMemcpyHostToDevice, st));
+  heads_noalloc_kernel<<<(unsigned)((npts + 127) / 128), 128, 0, st>>>(H->net(), s, (int)npts, H->h.foff[0]);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, s->head, sizeof(double) * npts, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return 0;
+}

@@ -93,6 +93,22 @@ class Solver:
                                                    out.ctypes.data_as(ctypes.c_void_p)))
         return out
 
+    NOALLOC_MAX_POINTS = 65536
+
+    def eval_heads_noalloc(self, frac_idx, z, out=None) -> np.ndarray:
+        """Heads through the entry point that allocates no device memory
+        (at most NOALLOC_MAX_POINTS points per call; calls on one device must
+        not overlap in time).  Pass C-contiguous int64 / complex128 arrays and
+        an out array to avoid host-side copies as well."""
+        frac_idx = np.ascontiguousarray(frac_idx, np.int64)
+        z = np.ascontiguousarray(z, np.complex128)
+        if out is None:
+            out = np.empty(len(z))
+        _ffi.check(_ffi.lib().andfn_b200_eval_heads_noalloc(self._h, frac_idx.ctypes.data_as(ctypes.c_void_p),
+                                                           z.ctypes.data_as(ctypes.c_void_p), len(z),
+                                                           out.ctypes.data_as(ctypes.c_void_p)))
+        return out
+
     def eval_omega(self, frac_idx, z) -> np.ndarray:
         """Omega_f(z) (andfn/hpc/hpc_fracture.py:52-94)."""
         frac_idx = np.ascontiguousarray(frac_idx, np.int64)

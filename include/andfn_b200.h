@@ -182,6 +182,23 @@ int andfn_b200_kernel_times(AndfnHandle *h, double *ms, int64_t *launches, int n
  * the evaluation kernels' roofline). */
 int andfn_b200_fp64_peak(int32_t device, double *tflops);
 
+/* Heads like andfn_b200_eval_heads, without allocating any memory (no
+ * reference counterpart: the reference evaluates heads on the host).
+ * For callers that cannot allocate device memory during a call -- a process
+ * whose memory pool already holds all the device memory it may use, or a
+ * loop that must not stall the device's other streams, which cudaFree does.
+ * The points are staged in one fixed device array inside the library, so:
+ *   - npts is at most ANDFN_NOALLOC_MAX_POINTS; larger calls are refused
+ *     with ANDFN_BAD_INPUT (split them, or use andfn_b200_eval_heads);
+ *   - the first call on a device looks the array up and caches its address:
+ *     make it before any stream capture on that device;
+ *   - the array is shared by all handles on a device: calls that overlap in
+ *     time on one device race on it and must be serialised by the caller.
+ * Fracture indices are those of the handle's first (or only) network. */
+#define ANDFN_NOALLOC_MAX_POINTS 65536
+int andfn_b200_eval_heads_noalloc(AndfnHandle *h, const int64_t *frac,
+                                  const double *z, int64_t npts, double *out);
+
 /* Thread-local text of the last error. */
 const char *andfn_b200_last_error(void);
 /* Library version string. */
