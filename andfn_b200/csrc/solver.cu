@@ -887,10 +887,11 @@ __device__ void dense_upper_solve(const double *__restrict__ Ucm, const double *
 }
 
 struct DenseTail {
-  int K;               // trailing block size (0 = none)
-  const double *L;     // K x K column-major, strictly lower part
-  const double *U;     // K x K column-major, strictly upper part
-  const double *uinv;  // [K] 1 / U(i,i)
+  int K;                 // trailing block size (0 = none)
+  const double *L;       // K x K column-major, strictly lower part
+  const double *U;       // K x K column-major, strictly upper part
+  const double *uinv;    // [K] 1 / U(i,i)
+  const double *lscale;  // [K] multiplier after the unit lower solve, or null
 };
 
 // The factorised discharge system of one realization (its rows are the
@@ -903,6 +904,9 @@ struct TriDesc {
   int row0, n;
 };
 
+// ADJ: the transposed solve of the adjoint (the factor parts passed in
+// net.tri are those of A^T): reads net.bvec, writes net.disc only.
+template <bool ADJ>
 __global__ void __launch_bounds__(SOLVE_THREADS) trisolve_kernel(Net net, int use_smem, int cap_levptr,
                                                                   int meta_cap) {
   const int r = blockIdx.x;
@@ -916,8 +920,10 @@ __global__ void __launch_bounds__(SOLVE_THREADS) trisolve_kernel(Net net, int us
   double *y = use_smem ? reinterpret_cast<double *>(smem_raw) : net.work + row0;
   int *s_levptr = reinterpret_cast<int *>(smem_raw + sizeof(double) * ycap);
   int *s_meta = s_levptr + cap_levptr;
-  if (threadIdx.x == 0) st->nit += 1;
-  if (!st->solve_q) return;  // uniform: solve_q is written only by reduce_kernel
+  if (!ADJ) {
+    if (threadIdx.x == 0) st->nit += 1;
+    if (!st->solve_q) return;  // uniform: solve_q is written only by reduce_kernel
+  }
   long long clk = clock64();
   auto phase = [&](int i) {
     __syncthreads();
@@ -937,6 +943,10 @@ __global__ void __launch_bounds__(SOLVE_THREADS) trisolve_kernel(Net net, int us
     level_solve(TD.Lx, y, s_levptr, cap_levptr, s_meta, meta_cap);
     phase(2);
     dense_lower_solve(TD.T.L, TD.T.K, y + (N - TD.T.K));
+    if (TD.T.lscale) {
+      for (int i = threadIdx.x; i < TD.T.K; i += blockDim.x) y[N - TD.T.K + i] *= TD.T.lscale[i];
+      __syncthreads();
+    }
     phase(3);
     // U: dense tail, coupling of the leading rows to it, sparse leading rows
     dense_upper_solve(TD.T.U, TD.T.uinv, TD.T.K, y + (N - TD.T.K));
@@ -960,6 +970,10 @@ __global__ void __launch_bounds__(SOLVE_THREADS) trisolve_kernel(Net net, int us
     mo = fmax(mo, fabs(xo));
   }
   __syncthreads();
+  if (ADJ) {
+    for (int k = threadIdx.x; k < N; k += blockDim.x) net.disc[row0 + TD.qcol[k]] = y[k];
+    return;
+  }
   for (int k = threadIdx.x; k < N; k += blockDim.x) {
     const int c = row0 + TD.qcol[k];
     const double xv = y[k];
@@ -1342,6 +1356,7 @@ struct HostNet {
   // discharge elements [doff[r], doff[r+1]) and system rows [roff[r], roff[r+1])
   std::vector<int> eoff, foff, doff, roff;
   std::vector<int> real_elem, real_frac, real_row, row_de, row_frac;
+  std::vector<double> head;  // prescribed head of constant-head lines and wells
 };
 
 // Discharge system of one realization (local row / column indices).
@@ -1361,6 +1376,9 @@ struct LevelParts {
   std::vector<int> lev, rows, eptr, col;
   std::vector<double> val, scale;
 };
+
+struct AdjBufs;
+static void destroy_adj(AdjBufs *a);
 
 }  // namespace andfn
 
@@ -1439,6 +1457,13 @@ struct AndfnHandle {
   int64_t k_n[KCLASSES] = {};
   int64_t launches = 0;
   std::vector<AndfnSolveStats> last;  // per realization
+  // adjoint (single network): factors of the last run and their transposed
+  // device form, loop state and work arrays
+  LuFactors lu_keep;
+  bool adj_factors_ready = false;
+  bool have_solution = false;
+  double last_damping = 0.5;
+  AdjBufs *adj = nullptr;
 
   Net net() const {
     Net n;
@@ -1504,6 +1529,7 @@ struct AndfnHandle {
     return n;
   }
   ~AndfnHandle() {
+    andfn::destroy_adj(adj);
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
     for (auto &b : ev)
       for (auto &c : b)
@@ -1597,6 +1623,7 @@ static int parse_records(AndfnHandle *H, int r, const char *F, int64_t nf, const
     h.err_old.push_back(rd_f64(rec, L.e_error_old));
     h.err_old2.push_back(rd_f64(rec, L.e_error_old2));
     h.err_coef.push_back(rd_f64(rec, L.e_error_coef));
+    h.head.push_back(rd_f64(rec, L.e_head));
     h.real_elem.push_back(r);
   }
   H->MC = std::max(H->MC, std::max(1, maxm));
@@ -2021,7 +2048,8 @@ static int create_impl(AndfnHandle *H, int R, const char *const *F, const int64_
   if (!H->h_ndone) CK(cudaMallocHost(&H->h_ndone, sizeof(int)));
   CK(cudaFuncSetAttribute(eval_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
   CK(cudaFuncSetAttribute(eval_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-  CK(cudaFuncSetAttribute(trisolve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+  CK(cudaFuncSetAttribute(trisolve_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+  CK(cudaFuncSetAttribute(trisolve_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
   CK(cudaFuncSetAttribute(update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
   rc = reset_impl(H);
   if (rc) return rc;
@@ -2247,6 +2275,7 @@ static int factor_all(AndfnHandle *H, const std::vector<double> &mv) {
     td[r].T.L = H->tail_l.p + toff[r];
     td[r].T.U = H->tail_u.p + toff[r];
     td[r].T.uinv = H->tail_uinv.p + tuoff[r];
+    td[r].T.lscale = nullptr;
     td[r].pinv = H->pinv.p + H->h.roff[r];
     td[r].qcol = H->qcol.p + H->h.roff[r];
     td[r].row0 = H->h.roff[r];
@@ -2254,6 +2283,12 @@ static int factor_all(AndfnHandle *H, const std::vector<double> &mv) {
   }
   CK(upload(H->tri, td, s));
   CK(cudaStreamSynchronize(s));
+  // the adjoint solves with the transposed factors of a single network
+  H->adj_factors_ready = false;
+  if (R == 1)
+    H->lu_keep = std::move(LU[0]);
+  else
+    H->lu_keep = LuFactors();
   return 0;
 }
 
@@ -2266,7 +2301,7 @@ static void launch_trisolve(AndfnHandle *H, cudaStream_t s) {
   const size_t meta_bytes = sizeof(int) * 2 * ((size_t)H->max_n + 1);
   const int meta_cap = (solve_smem + meta_bytes <= 200 * 1024) ? H->max_n + 1 : 0;
   if (meta_cap) solve_smem += meta_bytes;
-  trisolve_kernel<<<H->R, H->solve_threads, solve_smem, s>>>(net, use_smem, cap_levptr, meta_cap);
+  trisolve_kernel<false><<<H->R, H->solve_threads, solve_smem, s>>>(net, use_smem, cap_levptr, meta_cap);
 }
 
 static inline void mark(AndfnHandle *H, cudaStream_t s, int b, int c, int w) {
@@ -2444,6 +2479,8 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
     int rct = build_eval_tables(H);
     if (rct) return rct;
   }
+  H->have_solution = false;
+  H->last_damping = C->damping;
   int rc = reset_impl(H);
   if (rc) return rc;
   Net net = H->net();
@@ -2576,6 +2613,7 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
   base.ms_create_order = H->ms_create_order;
   int status = ANDFN_OK;
   H->last.assign(R, base);
+  H->have_solution = true;
   for (int r = 0; r < R; r++) {
     AndfnSolveStats &st = H->last[r];
     const SolveState &f = fin[r];
@@ -2795,6 +2833,7 @@ int andfn_b200_upload_state(AndfnHandle *H, const void *frac_recs, const void *e
     set_error("upload_state needs a single-network handle");
     return ANDFN_BAD_INPUT;
   }
+  H->have_solution = false;
   cudaSetDevice(H->device);
   const char *E = (const char *)elem_recs;
   const char *F = (const char *)frac_recs;
@@ -2832,6 +2871,7 @@ int andfn_b200_upload_state(AndfnHandle *H, const void *frac_recs, const void *e
 int andfn_b200_reset_state(AndfnHandle *H) {
   if (!H) return ANDFN_BAD_INPUT;
   cudaSetDevice(H->device);
+  H->have_solution = false;
   int rc = reset_impl(H);
   if (rc) return rc;
   CK(cudaStreamSynchronize(H->stream));
@@ -3131,3 +3171,924 @@ extern "C" int andfn_b200_eval_heads_noalloc(AndfnHandle *H, const int64_t *frac
   CK(cudaStreamSynchronize(st));
   return 0;
 }
+
+// ==========================================================================
+// Adjoint: the gradient of an objective J(coef, q, C, log t) with respect to
+// the natural log of every fracture's transmissivity, through the converged
+// solve (no reference counterpart; the reference computes no derivatives).
+//
+// At convergence the solve satisfies, with c the element coefficients, d =
+// (q of the discharge elements, fracture constants C) and theta = log t,
+//     c = Phi(c, d, theta)          element sweep (evaluation, DFT fit,
+//                                   per-type update; hpc_solve.py:311-390)
+//     A(theta) d = b(c, theta)      discharge system (hpc_solve.py:594-887)
+// Both are linear in (c, d).  With the Lagrangian
+//     L = J + lam^T (Phi - c) + mu^T (b - A d)
+// the multipliers solve
+//     mu  = A^-T (dJ/dd + Phi_d^T lam)
+//     lam = dJ/dc + Phi_c^T lam + b_c^T mu
+// and dJ/dtheta = J_theta + lam^T Phi_theta + mu^T (b_theta - A_theta d).
+// lam is found by the transposed fixed-point iteration, damped like the
+// forward loop (omega = 1 - (1 - DAMPING)^2, the weight of the forward
+// loop's two blends), whose iteration operator has the forward one's
+// eigenvalues; no forward iterate is stored.  Each iteration runs the
+// transposes of the forward kernels:
+//   adj_fit_kernel        the DFT fit and per-type update transposed: lam ->
+//                         weights at the collocation points (+ the q terms of
+//                         the stream-function branch-cut unwrapping)
+//   adj_eval_kernel<0>    the sweep evaluation transposed: point weights ->
+//                         dJ/d(coef, q, C) of the source elements
+//   trisolve_kernel<1>    A^-T with the transposed factors of the last run
+//   adj_eval_kernel<1>    the head-vector evaluation transposed (b_c^T mu)
+//   adj_update / reduce   damped update of lam and the relative stop test
+// theta enters Phi only through the intersection update
+// (t0 c1 - t1 c0) / (t0 + t1), b through 1/t of the intersection rows and
+// phi = t * head of constant-head lines and wells, and A through 1/t of the
+// intersection rows.  Complex quantities are (d/dRe, d/dIm) pairs.
+// ==========================================================================
+namespace andfn {
+
+static constexpr int ADJ_PPT = 4;  // points per thread in adj_eval_kernel
+static constexpr int ADJ_ITEM = EVAL_THREADS * ADJ_PPT;
+
+struct AdjState {
+  SolveState s;  // s.done / s.nit belong to the adjoint loop (trisolve_kernel<true> reads s.done)
+  double tol, omega, delta, lam;
+  int max_it, nonfinite;
+};
+
+struct AdjBufs {
+  DBuf<AdjState> st;
+  DBuf<SolveState> st_eval;
+  DBuf<cd> lam, gobj, gc;          // [ne][MC]
+  DBuf<double> gq, gC, gd, b, mu;  // [ne], [nf], [N], [N], [N]
+  DBuf<double> wsw, emax, gtheta, obar;
+  DBuf<Item> items_sw, items_rhs;
+  int n_items_sw = 0, n_items_rhs = 0;
+  int chunk = 1;
+  size_t smem = 0;
+  // transposed factors
+  DBuf<int> lev[4], rows[4], eptr[4], col[4];
+  DBuf<double> val[4], scale0, tl, tu, tones, tlscale;
+  DBuf<int> pinv, qcol;
+  DBuf<TriDesc> tri;
+  int max_nlev = 1;
+  cudaGraphExec_t graph = nullptr;
+  ~AdjBufs() {
+    if (graph) cudaGraphExecDestroy(graph);
+  }
+};
+
+static void destroy_adj(AdjBufs *a) { delete a; }
+
+// The DFT fit and per-type update of one element transposed (one warp): lam
+// (the multiplier of the element's new coefficients) -> weights of the
+// values at its collocation points, written to wsw in the sweep-value
+// layout.  For stream-function elements the branch-cut unwrapping
+// (psi'_k = psi_k - sum over cuts before k of sign * q) adds
+// -sign * (sum of the weights after the cut) to the cut's discharge element.
+__global__ void __launch_bounds__(UPDATE_WARPS * 32) adj_fit_kernel(Net net, const cd *__restrict__ lam,
+                                                                     const int *__restrict__ group_of,
+                                                                     const Group *__restrict__ groups, double *wsw,
+                                                                     double *gq, int nvmax, const AdjState *as) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  if (as->s.done) return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double *wk = reinterpret_cast<double *>(smem_raw) + (size_t)warp * nvmax;
+  const int e = blockIdx.x * UPDATE_WARPS + warp;
+  if (e >= net.ne) return;
+  const int type = net.type[e];
+  if (type == 2) return;
+  const int n = net.nint[e], m = net.ncoef[e];
+  const cd *L = lam + (size_t)e * net.MC;
+  double del = PI / n, start = del / 2;
+  if (type == 1) {
+    del = 2 * PI / n;
+    start = 0.0;
+  }
+  const double t0 = net.t[net.frac0[e]], t1 = (type == 0) ? net.t[net.frac1[e]] : 0.0;
+  const int sides = (type == 0) ? 2 : 1;
+  const double tn = 2.0 / n;
+  for (int s = 0; s < sides; s++) {
+    const Group g = groups[group_of[2 * e + s]];
+    const double side_f = (type == 0) ? (s ? t0 / (t0 + t1) : -t1 / (t0 + t1)) : 0.0;
+    for (int k = lane; k < n; k += 32) {
+      double sn, cs;
+      sincos(start + k * del, &sn, &cs);
+      double cj = 1.0, sj = 0.0, acc = 0.0;
+      for (int j = 0; j < m; j++) {
+        const cd l = L[j];
+        double a = 0.0, b = 0.0;  // weights of cos(j theta_k) and sin(j theta_k)
+        if (type == 0) {
+          if (j >= 1) a = side_f * l.re * tn;
+        } else if (type == 3) {
+          if (j >= 1) a = -l.re * tn;
+        } else if (type == 1) {
+          const double h = (j == 0) ? 0.5 : 1.0;
+          a = -l.im * tn * h;
+          b = -l.re * tn * h;
+        } else if (type == 4) {
+          if (j >= 1) {
+            a = -l.im * tn;
+            b = l.re * tn;
+          }
+        } else {  // type 5
+          if (j >= 1) a = -l.im * tn;
+        }
+        acc = fma(a, cj, fma(b, sj, acc));
+        const double c2 = cj * cs - sj * sn;
+        sj = sj * cs + cj * sn;
+        cj = c2;
+      }
+      wk[k] = acc;
+      wsw[g.out + k] = acc;
+    }
+  }
+  if (type == 1 || type == 4 || type == 5) {
+    __syncwarp();
+    const int nc = net.cut_n[e];
+    const int *cp = net.cut_pos + (size_t)e * net.cut_cap;
+    const int *ce = net.cut_elem + (size_t)e * net.cut_cap;
+    const int *cs = net.cut_sign + (size_t)e * net.cut_cap;
+    for (int c = lane; c < nc; c += 32) {
+      double sum = 0.0;
+      for (int k = cp[c] + 1; k < n; k++) sum += wk[k];
+      atomicAdd(&gq[ce[c]], -(double)cs[c] * sum);
+    }
+  }
+}
+
+// The evaluation kernel transposed: every point carries a weight w (the
+// adjoint of the value eval_kernel writes there); every source element of the
+// point's fracture receives w times the derivative of that value with respect
+// to its coefficients (complex pairs), its discharge (log term; sweep only)
+// and the fracture constant (phi points of the sweep).  Sweep points exclude
+// their own element, as eval_kernel does.  RHS: the head-vector points, whose
+// weight is mu of the row times the row's factor (-1/(D t0), +1/(D t1) for the
+// two sides of an intersection, -1/D for constant-head lines and wells);
+// series terms only.  Each thread holds ADJ_PPT points; per source and
+// coefficient a warp reduces its lanes' sums into shared memory, which is
+// added to global memory once per source chunk.
+template <bool RHS>
+__global__ void __launch_bounds__(EVAL_THREADS) adj_eval_kernel(Net net, const Item *__restrict__ items,
+                                                                  const int2 *__restrict__ pts,
+                                                                  const Group *__restrict__ groups,
+                                                                  const double *__restrict__ wsw,
+                                                                  const double *__restrict__ mu, cd *gc, double *gq,
+                                                                  double *gC, int chunk, const AdjState *as) {
+  if (as->s.done) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int MC = net.MC;
+  Src *src = reinterpret_cast<Src *>(smem_raw);
+  cd *sacc = reinterpret_cast<cd *>(smem_raw + sizeof(Src) * chunk);
+  double *sq = reinterpret_cast<double *>(sacc + (size_t)chunk * MC);
+  __shared__ double s_cw[EVAL_THREADS / 32];
+  const Item it = items[blockIdx.x];
+  const int f = it.frac;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  cd z[ADJ_PPT];
+  double w[ADJ_PPT];
+  int excl[ADJ_PPT], kind[ADJ_PPT];
+  double cw = 0.0;
+#pragma unroll
+  for (int i = 0; i < ADJ_PPT; i++) {
+    const int p = it.p0 + threadIdx.x + i * EVAL_THREADS;
+    z[i] = mk(0.0, 0.0);
+    w[i] = 0.0;
+    excl[i] = -1;
+    kind[i] = KIND_PHI;
+    if (p < it.p1) {
+      const int2 gk = pts[p];
+      const Group g = groups[gk.x];
+      if (RHS) {
+        const int j = g.elem;
+        const int e = net.de_ids[j];
+        const double m = mu[j];
+        if (net.type[e] == 0)
+          w[i] = g.side ? m / (net.D * net.t[net.frac1[e]]) : -m / (net.D * net.t[net.frac0[e]]);
+        else
+          w[i] = -m / net.D;
+        z[i] = (g.side ? net.zint1 : net.zint0)[(size_t)j * net.D + gk.y];
+      } else {
+        w[i] = wsw[g.out + gk.y];
+        excl[i] = g.elem;
+        kind[i] = g.kind;
+        z[i] = sweep_point(net, g.elem, g.side, gk.y);
+        if (g.kind == KIND_PHI) cw += w[i];
+      }
+    }
+  }
+  const int e0 = net.fptr[f], e1 = net.fptr[f + 1];
+  for (int base = e0; base < e1; base += chunk) {
+    const int cnt = min(chunk, e1 - base);
+    __syncthreads();
+    for (int s = threadIdx.x; s < cnt; s += blockDim.x) {
+      const int el = net.felem[base + s];
+      Src h;
+      h.id = el;
+      h.type = net.type[el];
+      h.m = net.ncoef[el];
+      h.pad = (h.type == 0 && net.frac0[el] != f) ? 1 : 0;  // frac1 side of an intersection: -c, -q
+      h.qk = 0.0;
+      h.pad2 = 0.0;
+      if (h.type == 0 || h.type == 3 || h.type == 5) {
+        const cd *ep = h.pad ? net.ep1 + 2 * el : net.ep0 + 2 * el;
+        cd a = ep[0], b = ep[1];
+        cd inv = recip(b - a);
+        h.p0 = 2.0 * inv;
+        cd ab = a + b;
+        h.p1 = mk(-(ab.re * inv.re - ab.im * inv.im), -(ab.re * inv.im + ab.im * inv.re));
+      } else {
+        h.p0 = (h.type == 1) ? mk(0.0, 0.0) : net.center[el];
+        h.p1 = mk(1.0 / net.radius[el], 0.0);
+      }
+      src[s] = h;
+      sq[s] = 0.0;
+    }
+    for (int idx = threadIdx.x; idx < cnt * MC; idx += blockDim.x) sacc[idx] = mk(0.0, 0.0);
+    __syncthreads();
+    for (int s = 0; s < cnt; s++) {
+      const Src h = src[s];
+      const double sg = h.pad ? -1.0 : 1.0;
+      cd rt[ADJ_PPT], pw[ADJ_PPT];
+      double wv[ADJ_PPT];
+      double qc = 0.0;
+#pragma unroll
+      for (int i = 0; i < ADJ_PPT; i++) {
+        rt[i] = mk(0.0, 0.0);
+        pw[i] = mk(1.0, 0.0);
+        wv[i] = 0.0;
+        if (w[i] == 0.0 || h.id == excl[i]) continue;
+        cd chi;
+        if (h.type == 0 || h.type == 3 || h.type == 5) {
+          chi = exterior_chi(fma_c(h.p0, z[i], h.p1));
+          rt[i] = recip(chi);
+        } else if (h.type == 1) {
+          chi = h.p1.re * z[i];
+          rt[i] = chi;
+        } else {
+          chi = h.p1.re * (z[i] - h.p0);
+          if (h.type == 4) rt[i] = recip(chi);
+        }
+        wv[i] = w[i] * sg;
+        if (!RHS && (h.type == 0 || h.type == 2 || h.type == 3)) {
+          const double lg = (kind[i] == KIND_PSI) ? atan2(chi.im, chi.re) : 0.5 * log(norm2(chi));
+          qc += wv[i] / (2 * PI) * lg;
+        }
+      }
+      if (!RHS && (h.type == 0 || h.type == 2 || h.type == 3)) {
+        qc = warp_sum(qc);
+        if (lane == 0) atomicAdd(&sq[s], qc);
+      }
+      for (int j = 0; j < h.m; j++) {
+        double ar = 0.0, ai = 0.0;
+#pragma unroll
+        for (int i = 0; i < ADJ_PPT; i++) {
+          // d(value)/d(Re c_j, Im c_j) = conj(x^j) (phi) or i conj(x^j) (psi), x^j = pw
+          const double cr = wv[i] * pw[i].re, ci = wv[i] * pw[i].im;
+          if (kind[i] == KIND_PSI) {
+            ar += ci;
+            ai += cr;
+          } else {
+            ar += cr;
+            ai -= ci;
+          }
+          pw[i] = mk(pw[i].re * rt[i].re - pw[i].im * rt[i].im, pw[i].re * rt[i].im + pw[i].im * rt[i].re);
+        }
+        ar = warp_sum(ar);
+        ai = warp_sum(ai);
+        if (lane == 0) {
+          atomicAdd(&sacc[s * MC + j].re, ar);
+          atomicAdd(&sacc[s * MC + j].im, ai);
+        }
+      }
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < cnt * MC; idx += blockDim.x) {
+      const int s = idx / MC, j = idx - s * MC;
+      if (j >= src[s].m) continue;
+      const cd v = sacc[idx];
+      cd *g = gc + (size_t)src[s].id * MC + j;
+      atomicAdd(&g->re, v.re);
+      atomicAdd(&g->im, v.im);
+    }
+    if (!RHS)
+      for (int s = threadIdx.x; s < cnt; s += blockDim.x)
+        if (sq[s] != 0.0) atomicAdd(&gq[src[s].id], sq[s]);
+  }
+  if (!RHS) {
+    cw = warp_sum(cw);
+    if (lane == 0) s_cw[warp] = cw;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int k = 0; k < EVAL_THREADS / 32; k++) t += s_cw[k];
+      if (t != 0.0) atomicAdd(&gC[f], t);
+    }
+  }
+}
+
+// Right-hand side of the transposed discharge solve: dJ/dd + Phi_d^T lam.
+__global__ void adj_rhs_kernel(Net net, const double *gd, const double *gq, const double *gC, double *b,
+                               const AdjState *as) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (as->s.done || g >= net.N) return;
+  const int d = net.row_de[g];
+  b[g] = gd[g] + (d >= 0 ? gq[net.de_ids[d]] : gC[net.row_frac[g]]);
+}
+
+// dJ/dd in system-row order from the caller's dJ/dq and dJ/dC.
+__global__ void adj_gd_kernel(Net net, const double *gq_user, const double *gC_user, double *gd) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= net.N) return;
+  const int d = net.row_de[g];
+  gd[g] = d >= 0 ? gq_user[net.de_ids[d]] : gC_user[net.row_frac[g]];
+}
+
+// lam <- lam + omega (dJ/dc + Phi_c^T lam + b_c^T mu - lam), restricted to the
+// coefficient parts the update can change (imaginary parts of intersections
+// and constant-head lines, real parts of impermeable lines and c_0 of all but
+// bounding circles stay 0); per element max |delta| and max |lam|.
+__global__ void adj_update_kernel(Net net, cd *lam, const cd *gobj, const cd *gc, double *emax, const AdjState *as) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (as->s.done || e >= net.ne) return;
+  const int type = net.type[e], m = net.ncoef[e], MC = net.MC;
+  const double om = as->omega;
+  double dmax = 0.0, lmax = 0.0;
+  for (int j = 0; j < MC; j++) {
+    const size_t i = (size_t)e * MC + j;
+    cd v = mk(0.0, 0.0);
+    if (type != 2 && j < m && !(j == 0 && type != 1)) {
+      const cd l = lam[i], go = gobj[i], g = gc[i];
+      v = mk(l.re + om * (go.re + g.re - l.re), l.im + om * (go.im + g.im - l.im));
+      if (type == 0 || type == 3) v.im = 0.0;
+      if (type == 5) v.re = 0.0;
+      double dd = hypot(v.re - l.re, v.im - l.im);
+      if (!(dd == dd)) dd = INFINITY;
+      dmax = fmax(dmax, dd);
+      lmax = fmax(lmax, hypot(v.re, v.im));
+    }
+    lam[i] = v;
+  }
+  emax[2 * e] = dmax;
+  emax[2 * e + 1] = lmax;
+}
+
+__global__ void __launch_bounds__(1024) adj_reduce_kernel(Net net, const double *emax, AdjState *as) {
+  if (as->s.done) return;
+  __shared__ double sd[32], sl[32];
+  double d = 0.0, l = 0.0;
+  for (int e = threadIdx.x; e < net.ne; e += blockDim.x) {
+    d = fmax(d, emax[2 * e]);
+    l = fmax(l, emax[2 * e + 1]);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    d = fmax(d, __shfl_xor_sync(0xffffffffu, d, o));
+    l = fmax(l, __shfl_xor_sync(0xffffffffu, l, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    sd[threadIdx.x >> 5] = d;
+    sl[threadIdx.x >> 5] = l;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < (int)(blockDim.x >> 5); k++) {
+      d = fmax(d, sd[k]);
+      l = fmax(l, sl[k]);
+    }
+    as->s.nit += 1;
+    as->delta = d;
+    as->lam = l;
+    if (isinf(d) || !(l == l)) as->nonfinite = 1;
+    if (as->nonfinite || (as->s.nit >= 2 && d <= as->tol * l) || as->s.nit >= as->max_it) as->s.done = 1;
+  }
+}
+
+// lam^T Phi_theta: for every intersection, sum_j>=1 lam_j.re (Re a0_j + Re a1_j)
+// times t0 t1 / (t0 + t1)^2, added to theta of frac0 and subtracted from
+// theta of frac1 (a0, a1: the DFTs of the two sides' values at convergence).
+__global__ void adj_theta_kernel(Net net, const cd *lam, const int *group_of, const Group *groups,
+                                 const double *sweep_vals, double *gtheta) {
+  const int e = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (e >= net.ne || net.type[e] != 0) return;
+  const int n = net.nint[e], m = net.ncoef[e];
+  const double *v0 = sweep_vals + groups[group_of[2 * e]].out;
+  const double *v1 = sweep_vals + groups[group_of[2 * e + 1]].out;
+  double s = 0.0;
+  for (int j = 1 + lane; j < m; j += 32) {
+    cd a0, a1;
+    dft_lane(v0, n, 0, j, false, a0);
+    dft_lane(v1, n, 0, j, false, a1);
+    s += lam[(size_t)e * net.MC + j].re * (a0.re + a1.re);
+  }
+  s = warp_sum(s);
+  if (lane == 0) {
+    const int f0 = net.frac0[e], f1 = net.frac1[e];
+    const double t0 = net.t[f0], t1 = net.t[f1];
+    const double K = t0 * t1 / ((t0 + t1) * (t0 + t1));
+    atomicAdd(&gtheta[f0], s * K);
+    atomicAdd(&gtheta[f1], -s * K);
+  }
+}
+
+// Mean of Re Omega over the D points of each side of each discharge element.
+__global__ void adj_obar_kernel(Net net, double *obar) {
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (w >= 2 * net.n_de) return;
+  const int j = w >> 1, side = w & 1;
+  const int e = net.de_ids[j];
+  if (side && net.type[e] != 0) {
+    if (lane == 0) obar[w] = 0.0;
+    return;
+  }
+  const int f = side ? net.frac1[e] : net.frac0[e];
+  const cd *z = (side ? net.zint1 : net.zint0) + (size_t)j * net.D;
+  double s = 0.0;
+  for (int k = lane; k < net.D; k += 32) s += omega_at(net, f, z[k]).re;
+  s = warp_sum(s);
+  if (lane == 0) obar[w] = s / net.D;
+}
+
+// Heads Re Omega_f(z) / t_f at device-resident points.
+__global__ void heads_dev_kernel(Net net, const int64_t *__restrict__ frac, const cd *__restrict__ z, int n,
+                                 double *out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int f = (int)frac[i];
+  out[i] = omega_at(net, f, z[i]).re / net.t[f];
+}
+
+// Vector-Jacobian product of heads_dev_kernel: given dJ/dh per point, adds
+// dJ/d(coef) ([ne][mco] complex pairs), dJ/dq, dJ/dC and the explicit
+// dJ/dlog t (h = Re Omega / t, so dh/dlog t = -h) of the current state.
+__global__ void heads_vjp_kernel(Net net, const int64_t *__restrict__ frac, const cd *__restrict__ z, int n,
+                                 const double *__restrict__ gh, double *gcoef, int mco, double *gq, double *gC,
+                                 double *glogt) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double g = gh[i];
+  if (g == 0.0) return;
+  const int f = (int)frac[i];
+  const cd zz = z[i];
+  const double t = net.t[f];
+  const double w = g / t;
+  const double h = omega_at(net, f, zz).re / t;
+  if (!(h == h)) return;
+  atomicAdd(&glogt[f], -g * h);
+  atomicAdd(&gC[f], w);
+  for (int k = net.fptr[f]; k < net.fptr[f + 1]; k++) {
+    const int el = net.felem[k];
+    const int ty = net.type[el];
+    const int m = min(net.ncoef[el], mco);
+    const bool neg = (ty == 0 && net.frac0[el] != f);
+    const double sg = neg ? -1.0 : 1.0;
+    cd chi, rt = mk(0.0, 0.0);
+    if (ty == 0 || ty == 3 || ty == 5) {
+      const cd *ep = neg ? net.ep1 + 2 * el : net.ep0 + 2 * el;
+      cd inv = recip(ep[1] - ep[0]);
+      cd ab = ep[0] + ep[1];
+      chi = exterior_chi(
+          fma_c(2.0 * inv, zz, mk(-(ab.re * inv.re - ab.im * inv.im), -(ab.re * inv.im + ab.im * inv.re))));
+      rt = recip(chi);
+    } else if (ty == 1) {
+      chi = (1.0 / net.radius[el]) * zz;
+      rt = chi;
+    } else {
+      chi = (1.0 / net.radius[el]) * (zz - net.center[el]);
+      if (ty == 4) rt = recip(chi);
+    }
+    if (ty == 0 || ty == 2 || ty == 3) atomicAdd(&gq[el], w * sg / (2 * PI) * (0.5 * log(norm2(chi))));
+    cd pw = mk(1.0, 0.0);
+    for (int j = 0; j < m; j++) {
+      double *gp = gcoef + 2 * ((size_t)el * mco + j);
+      atomicAdd(gp, w * sg * pw.re);
+      atomicAdd(gp + 1, -w * sg * pw.im);
+      pw = mk(pw.re * rt.re - pw.im * rt.im, pw.re * rt.im + pw.im * rt.re);
+    }
+  }
+}
+
+}  // namespace andfn
+
+namespace andfn {
+
+// Point tables of the transposed evaluation: the forward point lists (same
+// order), cut into items of at most ADJ_ITEM points of one fracture.
+static void adj_items(const std::vector<Group> &groups, const std::vector<int2> &pts, std::vector<Item> &items) {
+  items.clear();
+  size_t p = 0;
+  while (p < pts.size()) {
+    const int f = groups[pts[p].x].frac;
+    size_t q = p;
+    while (q < pts.size() && groups[pts[q].x].frac == f) q++;
+    for (size_t a = p; a < q; a += ADJ_ITEM) {
+      Item it;
+      it.frac = f;
+      it.p0 = (int)a;
+      it.p1 = (int)std::min(q, a + ADJ_ITEM);
+      it.pad = 0;
+      items.push_back(it);
+    }
+    p = q;
+  }
+}
+
+// Transposed factors of the last run's LU (P A Q = L U, so A^T = Q U^T L^T P):
+// the lower solve is U^T (rows scaled by 1/U(i,i)), the upper one L^T (unit);
+// the dense tail's lower part is (D^-1 U22)^T followed by D^-1, its upper
+// part L22^T; y = Q^T b on entry, x = P^T y on exit.
+static int adj_build_factors(AndfnHandle *H) {
+  AdjBufs &A = *H->adj;
+  const LuFactors &F = H->lu_keep;
+  const int n = F.n, K = F.dense, m0 = n - K;
+  cudaStream_t s = H->stream;
+  auto transpose = [n](const std::vector<int> &ptr, const std::vector<int> &col, const std::vector<double> &val,
+                       std::vector<int> &tp, std::vector<int> &tc, std::vector<double> &tv) {
+    tp.assign(n + 1, 0);
+    for (int c : col) tp[c + 1]++;
+    for (int i = 0; i < n; i++) tp[i + 1] += tp[i];
+    tc.resize(col.size());
+    tv.resize(col.size());
+    std::vector<int> fill(tp.begin(), tp.end() - 1);
+    for (int r = 0; r < n; r++)
+      for (int p = ptr[r]; p < ptr[r + 1]; p++) {
+        const int c = col[p];
+        tc[fill[c]] = r;
+        tv[fill[c]++] = val[p];
+      }
+  };
+  std::vector<int> ut_p, ut_c, lt_p, lt_c;
+  std::vector<double> ut_v, lt_v;
+  transpose(F.u_ptr, F.u_col, F.u_val, ut_p, ut_c, ut_v);  // U^T: strictly lower
+  transpose(F.l_ptr, F.l_col, F.l_val, lt_p, lt_c, lt_v);  // L^T: strictly upper
+  TriDesc td;
+  std::memset(&td, 0, sizeof(td));
+  LevelSolve *ls[4] = {&td.Lf, &td.Lx, &td.Ux, &td.Ub};
+  A.max_nlev = 1;
+  for (int k = 0; k < 4; k++) {
+    std::vector<int> lev, rows, eptr, ecol;
+    std::vector<double> ev, esc;
+    const bool lower = (k <= 1);
+    int rlo = 0, rhi = m0, clo = 0, chi = m0;
+    if (k == 1) rlo = m0, rhi = n;
+    if (k == 2) clo = m0, chi = n;
+    if (K == 0 && (k == 1 || k == 2)) rlo = rhi = 0;
+    if (lower)
+      build_levels(n, ut_p, ut_c, ut_v, k == 0 ? &F.u_inv_diag : nullptr, true, rlo, rhi, clo, chi, k == 1, lev, rows,
+                   eptr, ecol, ev, esc);
+    else
+      build_levels(n, lt_p, lt_c, lt_v, nullptr, false, rlo, rhi, clo, chi, k == 2, lev, rows, eptr, ecol, ev, esc);
+    const int nslots = (int)rows.size();
+    const int group = group_for(eptr);
+    rows.push_back(0);
+    if (ecol.empty()) {
+      ecol.push_back(0);
+      ev.push_back(0.0);
+    }
+    CK(upload(A.lev[k], lev, s));
+    CK(upload(A.rows[k], rows, s));
+    CK(upload(A.eptr[k], eptr, s));
+    CK(upload(A.col[k], ecol, s));
+    CK(upload(A.val[k], ev, s));
+    if (k == 0) {
+      esc.push_back(1.0);
+      CK(upload(A.scale0, esc, s));
+    }
+    LevelSolve &L = *ls[k];
+    L.lev_ptr = A.lev[k].p;
+    L.rows = A.rows[k].p;
+    L.eptr = A.eptr[k].p;
+    L.col = A.col[k].p;
+    L.val = A.val[k].p;
+    L.scale = (k == 0) ? A.scale0.p : nullptr;
+    L.nlev = (int)lev.size() - 1;
+    L.nslots = nslots;
+    L.group = group;
+    A.max_nlev = std::max(A.max_nlev, L.nlev);
+  }
+  std::vector<double> tl((size_t)std::max(1, K * K)), tu((size_t)std::max(1, K * K)), ones(std::max(1, K), 1.0),
+      lsc(std::max(1, K), 1.0);
+  for (int j = 0; j < K; j++)
+    for (int i = 0; i < K; i++) {
+      tl[(size_t)j * K + i] = F.u22[(size_t)i * K + j] * F.u_inv_diag[m0 + j];
+      tu[(size_t)j * K + i] = F.l22[(size_t)i * K + j];
+    }
+  for (int i = 0; i < K; i++) lsc[i] = F.u_inv_diag[m0 + i];
+  CK(upload(A.tl, tl, s));
+  CK(upload(A.tu, tu, s));
+  CK(upload(A.tones, ones, s));
+  CK(upload(A.tlscale, lsc, s));
+  td.T.K = K;
+  td.T.L = A.tl.p;
+  td.T.U = A.tu.p;
+  td.T.uinv = A.tones.p;
+  td.T.lscale = A.tlscale.p;
+  std::vector<int> qinv(n), pinvinv(n);
+  for (int k = 0; k < n; k++) qinv[F.q[k]] = k;
+  for (int i = 0; i < n; i++) pinvinv[F.pinv[i]] = i;
+  CK(upload(A.pinv, qinv, s));
+  CK(upload(A.qcol, pinvinv, s));
+  td.pinv = A.pinv.p;
+  td.qcol = A.qcol.p;
+  td.row0 = 0;
+  td.n = n;
+  std::vector<TriDesc> tdv(1, td);
+  CK(upload(A.tri, tdv, s));
+  CK(cudaStreamSynchronize(s));
+  H->adj_factors_ready = true;
+  return 0;
+}
+
+static void launch_trisolve_adj(AndfnHandle *H, const Net &net, cudaStream_t s) {
+  const size_t ybytes = sizeof(double) * (size_t)H->max_n;
+  const int use_smem = ybytes <= 150 * 1024 ? H->max_n : 0;
+  const int cap_levptr = std::min(H->adj->max_nlev + 1, 10240);
+  size_t solve_smem = (use_smem ? ybytes : 0) + sizeof(int) * (size_t)cap_levptr;
+  const size_t meta_bytes = sizeof(int) * 2 * ((size_t)H->max_n + 1);
+  const int meta_cap = (solve_smem + meta_bytes <= 200 * 1024) ? H->max_n + 1 : 0;
+  if (meta_cap) solve_smem += meta_bytes;
+  trisolve_kernel<true><<<1, H->solve_threads, solve_smem, s>>>(net, use_smem, cap_levptr, meta_cap);
+}
+
+static constexpr int ADJ_LAUNCHES = 10;  // per adjoint iteration (3 memsets + 7 kernels)
+
+static void adj_enqueue_iteration(AndfnHandle *H, const Net &net, const Net &net_t, cudaStream_t s) {
+  AdjBufs &A = *H->adj;
+  const int ne = (int)H->ne, nf = (int)H->nf, N = H->N, MC = H->MC;
+  cudaMemsetAsync(A.gc.p, 0, sizeof(cd) * (size_t)ne * MC, s);
+  cudaMemsetAsync(A.gq.p, 0, sizeof(double) * ne, s);
+  cudaMemsetAsync(A.gC.p, 0, sizeof(double) * nf, s);
+  adj_fit_kernel<<<(ne + UPDATE_WARPS - 1) / UPDATE_WARPS, UPDATE_WARPS * 32, sizeof(double) * H->nvmax * UPDATE_WARPS,
+                   s>>>(net, A.lam.p, H->group_of.p, H->d_groups.p, A.wsw.p, A.gq.p, H->nvmax, A.st.p);
+  if (A.n_items_sw > 0)
+    adj_eval_kernel<false><<<A.n_items_sw, EVAL_THREADS, A.smem, s>>>(net, A.items_sw.p, H->sweep_pts.p,
+                                                                       H->d_groups.p, A.wsw.p, A.mu.p, A.gc.p,
+                                                                       A.gq.p, A.gC.p, A.chunk, A.st.p);
+  adj_rhs_kernel<<<(N + 255) / 256, 256, 0, s>>>(net, A.gd.p, A.gq.p, A.gC.p, A.b.p, A.st.p);
+  launch_trisolve_adj(H, net_t, s);
+  if (A.n_items_rhs > 0)
+    adj_eval_kernel<true><<<A.n_items_rhs, EVAL_THREADS, A.smem, s>>>(net, A.items_rhs.p, H->rhs_pts.p,
+                                                                      H->d_groups.p, A.wsw.p, A.mu.p, A.gc.p,
+                                                                      A.gq.p, A.gC.p, A.chunk, A.st.p);
+  adj_update_kernel<<<(ne + 255) / 256, 256, 0, s>>>(net, A.lam.p, A.gobj.p, A.gc.p, A.emax.p, A.st.p);
+  adj_reduce_kernel<<<1, 1024, 0, s>>>(net, A.emax.p, A.st.p);
+}
+
+static int adjoint_impl(AndfnHandle *H, const double *gcoef, int64_t mco, const double *gq_user,
+                        const double *gC_user, double tol, int64_t max_it, double *glogt, AndfnAdjointStats *S) {
+  auto t0 = std::chrono::steady_clock::now();
+  if (H->R != 1) {
+    set_error("the adjoint needs a single-network handle");
+    return ANDFN_BAD_INPUT;
+  }
+  if (!H->have_solution || H->lu_keep.n != H->N) {
+    set_error("the adjoint needs a completed run() on this handle (and no reset since)");
+    return ANDFN_BAD_INPUT;
+  }
+  if (!gcoef || !gq_user || !gC_user || !glogt || mco < 0 || !(tol > 0) || max_it < 1) {
+    set_error("adjoint: bad pointers, mco, tol or max_iterations");
+    return ANDFN_BAD_INPUT;
+  }
+  cudaStream_t s = H->stream;
+  if (!H->adj) H->adj = new AdjBufs();
+  AdjBufs &A = *H->adj;
+  const int ne = (int)H->ne, nf = (int)H->nf, N = H->N, MC = H->MC, n_de = (int)H->h.de_ids.size();
+  if (!H->adj_factors_ready) {
+    int rc = adj_build_factors(H);
+    if (rc) return rc;
+  }
+  // point tables: the forward lists (rebuilt in the same order), in items of
+  // up to ADJ_ITEM points
+  {
+    std::vector<Group> groups;
+    std::vector<int> go, rg;
+    std::vector<Item> si, ri, items;
+    std::vector<int2> spts, rpts;
+    int nsv = 0, nrv = 0;
+    build_tables(H, false, groups, go, si, spts, nsv);
+    build_tables(H, true, groups, rg, ri, rpts, nrv);
+    adj_items(groups, spts, items);
+    CK(upload(A.items_sw, items, s));
+    A.n_items_sw = (int)items.size();
+    adj_items(groups, rpts, items);
+    CK(upload(A.items_rhs, items, s));
+    A.n_items_rhs = (int)items.size();
+    CK(A.wsw.alloc(std::max(1, nsv)));
+    int maxnf = 1;
+    for (int f = 0; f < nf; f++) maxnf = std::max(maxnf, H->h.fptr[f + 1] - H->h.fptr[f]);
+    const size_t per = sizeof(Src) + sizeof(cd) * MC + sizeof(double);
+    A.chunk = std::max(1, std::min((int)(96 * 1024 / per), maxnf));
+    A.smem = per * A.chunk;
+    CK(cudaFuncSetAttribute(adj_eval_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    CK(cudaFuncSetAttribute(adj_eval_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+  }
+  CK(A.st.alloc(1));
+  CK(A.st_eval.alloc(1));
+  CK(A.lam.alloc((size_t)ne * MC));
+  CK(A.gobj.alloc((size_t)ne * MC));
+  CK(A.gc.alloc((size_t)ne * MC));
+  CK(A.gq.alloc(ne));
+  CK(A.gC.alloc(nf));
+  CK(A.gd.alloc(N));
+  CK(A.b.alloc(N));
+  CK(A.mu.alloc(N));
+  CK(A.emax.alloc(2 * (size_t)ne));
+  CK(A.gtheta.alloc(nf));
+  CK(A.obar.alloc(2 * (size_t)std::max(1, n_de)));
+  // objective gradients
+  CK(cudaMemsetAsync(A.gobj.p, 0, sizeof(cd) * (size_t)ne * MC, s));
+  const int64_t w = std::min<int64_t>(mco, MC);
+  if (w > 0)
+    CK(cudaMemcpy2DAsync(A.gobj.p, sizeof(cd) * MC, gcoef, sizeof(cd) * mco, sizeof(cd) * w, ne,
+                         cudaMemcpyDeviceToDevice, s));
+  Net net = H->net();
+  adj_gd_kernel<<<(N + 255) / 256, 256, 0, s>>>(net, gq_user, gC_user, A.gd.p);
+  // sweep values at the converged state (for lam^T Phi_theta)
+  SolveState se;
+  std::memset(&se, 0, sizeof(se));
+  se.solve_q = 1;
+  CK(cudaMemcpyAsync(A.st_eval.p, &se, sizeof(se), cudaMemcpyHostToDevice, s));
+  Net net_e = net;
+  net_e.st = A.st_eval.p;
+  if (H->n_sweep_items > 0)
+    eval_kernel<false><<<H->n_sweep_items, EVAL_THREADS, H->eval_smem, s>>>(
+        net_e, H->sweep_items.p, H->sweep_pts.p, H->d_groups.p, H->sweep_vals.p, H->chunk);
+  // loop state
+  AdjState as0;
+  std::memset(&as0, 0, sizeof(as0));
+  const double d = H->last_damping;
+  as0.omega = 1.0 - (1.0 - d) * (1.0 - d);
+  as0.tol = tol;
+  as0.max_it = (int)std::min<int64_t>(max_it, 1 << 30);
+  CK(cudaMemcpyAsync(A.st.p, &as0, sizeof(as0), cudaMemcpyHostToDevice, s));
+  CK(cudaMemsetAsync(A.lam.p, 0, sizeof(cd) * (size_t)ne * MC, s));
+  CK(cudaMemsetAsync(A.mu.p, 0, sizeof(double) * N, s));
+  CK(cudaStreamSynchronize(s));
+  CK(cudaGetLastError());
+  const double ms_setup = ms_since(t0);
+  auto t1 = std::chrono::steady_clock::now();
+  Net net_t = net;  // the transposed discharge solve: b -> mu
+  net_t.st = reinterpret_cast<SolveState *>(A.st.p);
+  net_t.bvec = A.b.p;
+  net_t.disc = A.mu.p;
+  net_t.tri = A.tri.p;
+  if (A.graph) {
+    cudaGraphExecDestroy(A.graph);
+    A.graph = nullptr;
+  }
+  {
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    for (int b = 0; b < ITER_BATCH; b++) adj_enqueue_iteration(H, net, net_t, s);
+    CK(cudaStreamEndCapture(s, &g));
+    CK(cudaGraphInstantiate(&A.graph, g, 0));
+    cudaGraphDestroy(g);
+  }
+  AdjState fin;
+  int guard = 0;
+  int64_t launches = 4;
+  while (true) {
+    CK(cudaGraphLaunch(A.graph, s));
+    CK(cudaMemcpyAsync(&fin, A.st.p, sizeof(fin), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    launches += ITER_BATCH * ADJ_LAUNCHES;
+    if (fin.s.done) break;
+    if (++guard > as0.max_it / ITER_BATCH + 2) break;
+  }
+  // lam^T Phi_theta and the mean potentials of the discharge rows
+  CK(cudaMemsetAsync(A.gtheta.p, 0, sizeof(double) * nf, s));
+  adj_theta_kernel<<<(ne * 32 + 127) / 128, 128, 0, s>>>(net, A.lam.p, H->group_of.p, H->d_groups.p,
+                                                          H->sweep_vals.p, A.gtheta.p);
+  if (n_de > 0) adj_obar_kernel<<<(2 * n_de * 32 + 127) / 128, 128, 0, s>>>(net, A.obar.p);
+  launches += 2;
+  std::vector<double> mu(N), obar(2 * (size_t)std::max(1, n_de)), gth(nf), tt(nf);
+  CK(cudaMemcpyAsync(mu.data(), A.mu.p, sizeof(double) * N, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(obar.data(), A.obar.p, sizeof(double) * obar.size(), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(gth.data(), A.gtheta.p, sizeof(double) * nf, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(tt.data(), H->t.p, sizeof(double) * nf, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  CK(cudaGetLastError());
+  // mu^T (b_theta - A_theta d): an intersection row gives mu * mean(Re Omega)
+  // / t on each side (+ on frac0, - on frac1); a constant-head line or well
+  // row gives mu * head * t
+  const HostNet &h = H->h;
+  for (int j = 0; j < n_de; j++) {
+    const int e = h.de_ids[j];
+    const int f0 = h.frac0[e];
+    if (h.type[e] == 0) {
+      const int f1 = h.frac1[e];
+      gth[f0] += mu[j] * obar[2 * j] / tt[f0];
+      gth[f1] -= mu[j] * obar[2 * j + 1] / tt[f1];
+    } else {
+      gth[f0] += mu[j] * h.head[e] * tt[f0];
+    }
+  }
+  CK(cudaMemcpyAsync(glogt, gth.data(), sizeof(double) * nf, cudaMemcpyHostToDevice, s));
+  CK(cudaStreamSynchronize(s));
+  int status = ANDFN_OK;
+  if (fin.nonfinite)
+    status = ANDFN_NONFINITE;
+  else if (!(fin.delta <= tol * fin.lam))
+    status = ANDFN_MAX_ITERATIONS;
+  if (S) {
+    std::memset(S, 0, sizeof(*S));
+    S->iterations = fin.s.nit;
+    S->delta = fin.delta;
+    S->lam = fin.lam;
+    S->omega = as0.omega;
+    S->ms_setup = ms_setup;
+    S->ms_iterate = ms_since(t1);
+    S->ms_total = ms_since(t0);
+    S->gpu_launches = launches;
+    S->status = status;
+  }
+  return status;
+}
+
+static int set_transmissivity_impl(AndfnHandle *H, const double *t) {
+  for (int64_t f = 0; f < H->nf; f++)
+    if (!(t[f] > 0) || !std::isfinite(t[f])) {
+      set_error("transmissivity must be positive and finite");
+      return ANDFN_BAD_INPUT;
+    }
+  HostNet &h = H->h;
+  for (int64_t f = 0; f < H->nf; f++) h.t[f] = t[f];
+  // phi = head * t of constant-head lines and wells (Fracture.phi_from_head)
+  for (int64_t e = 0; e < H->ne; e++)
+    if (h.type[e] == 2 || h.type[e] == 3) h.phi[e] = h.head[e] * h.t[h.frac0[e]];
+  cudaStream_t s = H->stream;
+  CK(cudaMemcpyAsync(H->t.p, h.t.data(), sizeof(double) * H->nf, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(H->phi.p, h.phi.data(), sizeof(double) * H->ne, cudaMemcpyHostToDevice, s));
+  CK(cudaStreamSynchronize(s));
+  H->have_solution = false;
+  return 0;
+}
+
+}  // namespace andfn
+
+extern "C" {
+
+int andfn_b200_set_transmissivity(AndfnHandle *H, const double *t) {
+  if (!H || !t) return ANDFN_BAD_INPUT;
+  CK(cudaSetDevice(H->device));
+  return set_transmissivity_impl(H, t);
+}
+
+int andfn_b200_state_device(AndfnHandle *H, double *coef, int64_t mco, double *q, double *constant) {
+  if (!H || mco < 0 || (mco > 0 && !coef) || !q || !constant) return ANDFN_BAD_INPUT;
+  CK(cudaSetDevice(H->device));
+  cudaStream_t s = H->stream;
+  const int64_t w = std::min<int64_t>(mco, H->MC);
+  if (mco > 0) {
+    CK(cudaMemsetAsync(coef, 0, sizeof(cd) * mco * H->ne, s));
+    if (w > 0)
+      CK(cudaMemcpy2DAsync(coef, sizeof(cd) * mco, H->coef.p, sizeof(cd) * H->MC, sizeof(cd) * w, H->ne,
+                           cudaMemcpyDeviceToDevice, s));
+  }
+  CK(cudaMemcpyAsync(q, H->q.p, sizeof(double) * H->ne, cudaMemcpyDeviceToDevice, s));
+  CK(cudaMemcpyAsync(constant, H->constant.p, sizeof(double) * H->nf, cudaMemcpyDeviceToDevice, s));
+  CK(cudaStreamSynchronize(s));
+  return 0;
+}
+
+int andfn_b200_heads_device(AndfnHandle *H, const int64_t *frac, const double *z, int64_t npts, double *out) {
+  if (!H || npts < 0 || (npts > 0 && (!frac || !z || !out)) || npts > (1LL << 31) - 1) return ANDFN_BAD_INPUT;
+  if (H->R != 1) {
+    set_error("heads_device needs a single-network handle");
+    return ANDFN_BAD_INPUT;
+  }
+  if (npts == 0) return 0;
+  CK(cudaSetDevice(H->device));
+  heads_dev_kernel<<<(unsigned)((npts + 127) / 128), 128, 0, H->stream>>>(H->net(), frac, (const cd *)z, (int)npts,
+                                                                           out);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(H->stream));
+  return 0;
+}
+
+int andfn_b200_heads_vjp(AndfnHandle *H, const int64_t *frac, const double *z, int64_t npts, const double *gh,
+                         double *gcoef, int64_t mco, double *gq, double *gC, double *glogt) {
+  if (!H || npts < 0 || (npts > 0 && (!frac || !z || !gh)) || !gcoef || !gq || !gC || !glogt || mco < 0 ||
+      npts > (1LL << 31) - 1)
+    return ANDFN_BAD_INPUT;
+  if (H->R != 1) {
+    set_error("heads_vjp needs a single-network handle");
+    return ANDFN_BAD_INPUT;
+  }
+  if (npts == 0) return 0;
+  CK(cudaSetDevice(H->device));
+  heads_vjp_kernel<<<(unsigned)((npts + 127) / 128), 128, 0, H->stream>>>(H->net(), frac, (const cd *)z, (int)npts,
+                                                                           gh, gcoef, (int)mco, gq, gC, glogt);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(H->stream));
+  return 0;
+}
+
+int andfn_b200_adjoint(AndfnHandle *H, const double *gcoef, int64_t mco, const double *gq, const double *gC,
+                       double tol, int64_t max_iterations, double *glogt, AndfnAdjointStats *stats) {
+  if (!H) return ANDFN_BAD_INPUT;
+  CK(cudaSetDevice(H->device));
+  return adjoint_impl(H, gcoef, mco, gq, gC, tol, max_iterations, glogt, stats);
+}
+
+}  // extern "C"

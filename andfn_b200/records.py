@@ -98,6 +98,16 @@ class AndfnSolveStats(ctypes.Structure):
         d["tri_cycles"] = list(self.tri_cycles)
         return d
 
+class AndfnAdjointStats(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int64), ("delta", ctypes.c_double), ("lam", ctypes.c_double),
+                ("omega", ctypes.c_double), ("ms_setup", ctypes.c_double), ("ms_iterate", ctypes.c_double),
+                ("ms_total", ctypes.c_double), ("gpu_launches", ctypes.c_int64), ("status", ctypes.c_int32),
+                ("pad", ctypes.c_int32)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_ if name != "pad"}
+
+
 _INT_FIELDS = ("_id", "_type", "frac0", "frac1", "ncoef", "nint")
 
 

@@ -199,6 +199,60 @@ int andfn_b200_fp64_peak(int32_t device, double *tflops);
 int andfn_b200_eval_heads_noalloc(AndfnHandle *h, const int64_t *frac,
                                   const double *z, int64_t npts, double *out);
 
+/* ---- adjoint: gradient with respect to log-transmissivity ---------------
+ * No reference counterpart (the reference computes no derivatives).  For an
+ * objective J(coef, q, C, log t) of the converged solve of a single-network
+ * handle, andfn_b200_adjoint returns dJ/dlog t_f (natural log) for every
+ * fracture, given the partial derivatives of J with respect to the solved
+ * state.  It runs the transposed fixed-point iteration of the solve (no
+ * forward iterates are stored) with the transposed factors of the last run;
+ * it stops when max|delta lam| <= tol * max|lam| or after max_iterations.
+ * All array arguments of the functions in this block are DEVICE pointers on
+ * the handle's device; complex values are (re, im) double pairs:
+ *   gcoef [ne][mco][2]  dJ/d(Re, Im) coef (entries beyond ncoef are ignored)
+ *   gq    [ne]          dJ/dq (read for the discharge elements only:
+ *                       intersections, constant-head lines, wells)
+ *   gC    [nf]          dJ/dC (fracture constants)
+ *   glogt [nf]          output, overwritten: the part of dJ/dlog t that
+ *                       flows through the solve (add the explicit part of J,
+ *                       e.g. from andfn_b200_heads_vjp)
+ * Requires a completed andfn_b200_run on the handle (with MAX_NCOEF =
+ * ncoef, so that no coefficients grow) and no reset since.  Returns 0, or
+ * ANDFN_MAX_ITERATIONS when the tolerance was not reached (the gradient of
+ * the last iterate is still written). */
+typedef struct {
+  int64_t iterations;
+  double delta;           /* final max |delta lam|            */
+  double lam;             /* final max |lam|                   */
+  double omega;           /* damping of the transposed loop    */
+  double ms_setup, ms_iterate, ms_total;
+  int64_t gpu_launches;
+  int32_t status;
+  int32_t pad;
+} AndfnAdjointStats;
+int andfn_b200_adjoint(AndfnHandle *h, const double *gcoef, int64_t mco,
+                       const double *gq, const double *gC, double tol,
+                       int64_t max_iterations, double *glogt,
+                       AndfnAdjointStats *stats);
+/* Replaces the fractures' transmissivities (host array [nf]) and with them
+ * phi = head * t of constant-head lines and wells (the reference sets phi
+ * once, at construction: andfn/const_head.py:45, andfn/well.py:38); the next
+ * run() solves with them. */
+int andfn_b200_set_transmissivity(AndfnHandle *h, const double *t);
+/* Copies the solved state to device arrays: coef [ne][mco][2] (zero beyond
+ * the handle's capacity), q [ne], C [nf]. */
+int andfn_b200_state_device(AndfnHandle *h, double *coef, int64_t mco,
+                            double *q, double *C);
+/* Heads at device-resident points (frac int64 [n], z complex [n][2], out [n])
+ * and the vector-Jacobian product of that map: given gh = dJ/dh, ADDS
+ * dJ/d(coef, q, C) of the current state and the explicit dJ/dlog t
+ * (-h gh) into gcoef [ne][mco][2], gq [ne], gC [nf], glogt [nf]. */
+int andfn_b200_heads_device(AndfnHandle *h, const int64_t *frac,
+                            const double *z, int64_t npts, double *out);
+int andfn_b200_heads_vjp(AndfnHandle *h, const int64_t *frac, const double *z,
+                         int64_t npts, const double *gh, double *gcoef,
+                         int64_t mco, double *gq, double *gC, double *glogt);
+
 /* Thread-local text of the last error. */
 const char *andfn_b200_last_error(void);
 /* Library version string. */

@@ -1,0 +1,149 @@
+"""Adjoint gradients d J / d log t against central finite differences.
+
+J is the objective of the gradient workload: the squared misfit of heads at
+observation points (observed = forward heads + N(0, 0.01)) plus the
+discharge through the head-0 face (sum of q of the constant-head lines with
+head 0).  Finite differences run the solve itself at t * exp(+-h) per
+fracture: the GPU forward (every fracture) and the oracle (the reference's
+algorithm on the CPU, a sample of fractures).  The solves run a fixed,
+large number of iterations (MAX_ERROR below round-off), so J of the
+iterate is a smooth function of log t and its difference quotient converges
+to the fixed point's derivative.
+
+Tolerance: |g_adjoint - g_fd| <= 1e-5 * max |g_fd| + 1e-12 * scale, the
+north-star bound (1e-5 relative) taken against the largest gradient entry,
+because entries of fractures that barely touch the flow are pure round-off
+in the difference quotient.
+"""
+import numpy as np
+import pytest
+
+from conftest import load_golden
+
+pytestmark = pytest.mark.gpu
+
+H_FD = 1e-5
+
+
+def _constants(ncoef, its=1500):
+    from andfn_b200.records import default_constants
+    return default_constants(MAX_ITERATIONS=its, MAX_ERROR=1e-300, MAX_NCOEF=ncoef)
+
+
+def _points(F, n, seed):
+    rng = np.random.default_rng(seed)
+    fr = rng.integers(0, len(F), n)
+    z = F["radius"][fr] * 0.9 * np.sqrt(rng.uniform(size=n)) * np.exp(2j * np.pi * rng.uniform(size=n))
+    return fr, z
+
+
+class Problem:
+    def __init__(self, case, q_weight=1.0, seed=0):
+        import torch
+        from andfn_b200.adjoint import DFNModel
+        g = load_golden(case)
+        self.F, self.E = g["F_in"].copy(), g["E_in"].copy()
+        self.c = _constants(int(self.E["ncoef"].max()))
+        self.model = DFNModel(self.F.copy(), self.E.copy(), self.c, 50)
+        self.logt0 = np.log(self.F["t"].astype(np.float64))
+        fr, z = _points(self.F, 50, seed)
+        self.fr_np, self.z_np = fr, z
+        self.fr = torch.tensor(fr, dtype=torch.int64, device="cuda")
+        self.z = torch.tensor(z, dtype=torch.complex128, device="cuda")
+        self.outlet = np.nonzero((self.E["_type"] == 3) & (self.E["head"] == 0.0))[0]
+        self.q_weight = q_weight
+        h0 = self.heads_np(self.logt0)
+        rng = np.random.default_rng(seed + 1)
+        self.hobs = h0 + rng.normal(0.0, 0.01, len(h0))
+
+    def heads_np(self, logt):
+        import torch
+        lt = torch.tensor(logt, dtype=torch.float64, device="cuda")
+        coef, q, C = self.model.solve(lt)
+        return self.model.heads(coef, q, C, lt, self.fr, self.z).cpu().numpy()
+
+    def J_gpu(self, logt):
+        import torch
+        lt = torch.tensor(logt, dtype=torch.float64, device="cuda")
+        coef, q, C = self.model.solve(lt)
+        h = self.model.heads(coef, q, C, lt, self.fr, self.z)
+        hobs = torch.tensor(self.hobs, device="cuda")
+        return float(((h - hobs) ** 2).sum() + self.q_weight * q[self.outlet].sum())
+
+    def grad_adjoint(self):
+        import torch
+        lt = torch.tensor(self.logt0, dtype=torch.float64, device="cuda", requires_grad=True)
+        coef, q, C = self.model.solve(lt)
+        h = self.model.heads(coef, q, C, lt, self.fr, self.z)
+        hobs = torch.tensor(self.hobs, device="cuda")
+        J = ((h - hobs) ** 2).sum() + self.q_weight * q[torch.tensor(self.outlet, device="cuda")].sum()
+        J.backward()
+        return lt.grad.cpu().numpy()
+
+    def J_oracle(self, logt):
+        from oracle import oracle as orc
+        F, E = self.F.copy(), self.E.copy()
+        t = np.exp(logt)
+        F["t"] = t
+        m = np.isin(E["_type"], (2, 3))
+        E["phi"][m] = E["head"][m] * t[E["frac0"][m]]
+        orc.solve(F, E, 50, self.c)
+        h = orc.eval_heads(F, E, self.fr_np, self.z_np)
+        return float(((h - self.hobs) ** 2).sum() + self.q_weight * E["q"][self.outlet].sum())
+
+
+def _fd(J, logt0, fracs):
+    g = np.zeros(len(fracs))
+    for i, f in enumerate(fracs):
+        lp, lm = logt0.copy(), logt0.copy()
+        lp[f] += H_FD
+        lm[f] -= H_FD
+        g[i] = (J(lp) - J(lm)) / (2 * H_FD)
+    return g
+
+
+def _check(ga, gf, tag):
+    err = np.abs(ga - gf)
+    bound = 1e-5 * np.abs(gf).max() + 1e-30
+    assert np.all(err <= bound), (tag, float(err.max() / np.abs(gf).max()), ga, gf)
+
+
+@pytest.mark.parametrize("case", ["c1_seed3", "mixed"])
+def test_adjoint_matches_gpu_finite_differences(case):
+    P = Problem(case)
+    ga = P.grad_adjoint()
+    st = P.model.adjoint_stats
+    assert st["status"] == 0, st
+    fracs = np.arange(len(P.F))
+    gf = _fd(P.J_gpu, P.logt0, fracs)
+    _check(ga, gf, (case, "gpu"))
+
+
+def test_adjoint_discharge_objective_matches_gpu_finite_differences():
+    """J = discharge through the head-0 face only (the q path of the adjoint)."""
+    P = Problem("c1_seed3", q_weight=1.0)
+
+    import torch
+
+    def J(logt):
+        lt = torch.tensor(logt, dtype=torch.float64, device="cuda")
+        coef, q, C = P.model.solve(lt)
+        return float(q[P.outlet].sum())
+
+    lt = torch.tensor(P.logt0, dtype=torch.float64, device="cuda", requires_grad=True)
+    coef, q, C = P.model.solve(lt)
+    q[torch.tensor(P.outlet, device="cuda")].sum().backward()
+    ga = lt.grad.cpu().numpy()
+    gf = _fd(J, P.logt0, np.arange(len(P.F)))
+    _check(ga, gf, "discharge")
+
+
+def test_adjoint_matches_oracle_finite_differences():
+    """The same gradient against finite differences of the oracle solve (a
+    sample of fractures, the largest gradients first)."""
+    P = Problem("c1_seed3")
+    ga = P.grad_adjoint()
+    fracs = np.argsort(-np.abs(ga))[:6]
+    gf = _fd(P.J_oracle, P.logt0, fracs)
+    err = np.abs(ga[fracs] - gf)
+    assert np.all(err <= 1e-5 * np.abs(ga).max()), (err / np.abs(ga).max(), ga[fracs], gf)
