@@ -12,9 +12,9 @@ fracture) and returns the solved state as torch tensors:
 ``model.heads(coef, q, C, logt, frac, z)`` evaluates heads Re Omega_f(z)/t_f
 (andfn/hpc/hpc_fracture.py:205-252) at device-resident points.  Both are
 ``torch.autograd.Function``s: ``J.backward()`` of any objective built from
-them runs the library's adjoint (the transposed fixed-point iteration of the
-solve, no stored iterates; include/andfn_b200.h) and the transposed head
-evaluation, and leaves dJ/dlogt in ``logt.grad``.
+them runs the library's adjoint (a GMRES solve whose operator is one
+transposed sweep of the solve, no stored iterates; include/andfn_b200.h) and
+the transposed head evaluation, and leaves dJ/dlogt in ``logt.grad``.
 
 The reference has no derivatives; its solve is what is differentiated
 (hpc_solve.solve, andfn/hpc/hpc_solve.py:55-257, with the transmissivities
@@ -44,7 +44,7 @@ def _ptr(t: torch.Tensor):
 
 class DFNModel:
     def __init__(self, fractures: np.ndarray, elements: np.ndarray, constants, discharge_int: int = 50,
-                 device: int = 0, adjoint_tol: float = 1e-11, adjoint_max_iterations: int = 20000):
+                 device: int = 0, adjoint_tol: float = 1e-10, adjoint_max_iterations: int = 5000):
         self.device = torch.device("cuda", device)
         self.solver = Solver(fractures, elements, discharge_int, device=device)
         self.constants = constants

@@ -1462,7 +1462,6 @@ struct AndfnHandle {
   LuFactors lu_keep;
   bool adj_factors_ready = false;
   bool have_solution = false;
-  double last_damping = 0.5;
   AdjBufs *adj = nullptr;
 
   Net net() const {
@@ -2480,7 +2479,6 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
     if (rct) return rct;
   }
   H->have_solution = false;
-  H->last_damping = C->damping;
   int rc = reset_impl(H);
   if (rc) return rc;
   Net net = H->net();
@@ -3188,19 +3186,20 @@ extern "C" int andfn_b200_eval_heads_noalloc(AndfnHandle *H, const int64_t *frac
 //     mu  = A^-T (dJ/dd + Phi_d^T lam)
 //     lam = dJ/dc + Phi_c^T lam + b_c^T mu
 // and dJ/dtheta = J_theta + lam^T Phi_theta + mu^T (b_theta - A_theta d).
-// lam is found by the transposed fixed-point iteration, damped like the
-// forward loop (omega = 1 - (1 - DAMPING)^2, the weight of the forward
-// loop's two blends), whose iteration operator has the forward one's
-// eigenvalues; no forward iterate is stored.  Each iteration runs the
-// transposes of the forward kernels:
+// Eliminating mu, lam solves the linear system (I - T^T) lam = F(0), T^T the
+// transpose of the forward loop's (undamped) iteration operator; it is
+// solved by restarted GMRES whose operator is one transposed sweep, so no
+// forward iterate is stored.  A transposed sweep runs the transposes of the
+// forward kernels:
 //   adj_fit_kernel        the DFT fit and per-type update transposed: lam ->
 //                         weights at the collocation points (+ the q terms of
 //                         the stream-function branch-cut unwrapping)
-//   adj_eval_kernel<0>    the sweep evaluation transposed: point weights ->
+//   adj_sweep_kernel      the sweep evaluation transposed: point weights ->
 //                         dJ/d(coef, q, C) of the source elements
 //   trisolve_kernel<1>    A^-T with the transposed factors of the last run
-//   adj_eval_kernel<1>    the head-vector evaluation transposed (b_c^T mu)
-//   adj_update / reduce   damped update of lam and the relative stop test
+//   adj_rhs_gather_kernel the head-vector evaluation transposed (b_c^T mu),
+//                         from power sums precomputed by rhs_sums_kernel
+//   adj_combine_kernel    (I - T^T) x, or the residual F(x) - x
 // theta enters Phi only through the intersection update
 // (t0 c1 - t1 c0) / (t0 + t1), b through 1/t of the intersection rows and
 // phi = t * head of constant-head lines and wells, and A through 1/t of the
@@ -3208,13 +3207,12 @@ extern "C" int andfn_b200_eval_heads_noalloc(AndfnHandle *H, const int64_t *frac
 // ==========================================================================
 namespace andfn {
 
-static constexpr int ADJ_PPT = 4;  // points per thread in adj_eval_kernel
-static constexpr int ADJ_ITEM = EVAL_THREADS * ADJ_PPT;
+static constexpr int ADJ_ITEM = EVAL_THREADS * 4;  // points of one adj_sweep_kernel item
 
+// The kernels shared with the forward loop return at entry when s.done is set;
+// the adjoint keeps it 0.
 struct AdjState {
-  SolveState s;  // s.done / s.nit belong to the adjoint loop (trisolve_kernel<true> reads s.done)
-  double tol, omega, delta, lam;
-  int max_it, nonfinite;
+  SolveState s;
 };
 
 struct AdjBufs {
@@ -3222,9 +3220,16 @@ struct AdjBufs {
   DBuf<SolveState> st_eval;
   DBuf<cd> lam, gobj, gc;          // [ne][MC]
   DBuf<double> gq, gC, gd, b, mu;  // [ne], [nf], [N], [N], [N]
-  DBuf<double> wsw, emax, gtheta, obar;
-  DBuf<Item> items_sw, items_rhs;
-  int n_items_sw = 0, n_items_rhs = 0;
+  DBuf<double> wsw, gtheta, obar, gd0, hbuf;
+  DBuf<cd> V, xin, wv;  // Krylov basis [restart + 1][ne][MC], sweep input and output
+  DBuf<Item> items_sw;
+  int n_items_sw = 0;
+  // head-vector power sums: pairs (row side g = 2 j + side, source element)
+  DBuf<int> pair_g, pair_src, pair_off, src_ptr, src_pairs;
+  DBuf<cd> S;
+  DBuf<double> fac;  // [2 n_de] weight of a row side per unit mu
+  int npairs = 0;
+  std::vector<int> sums_ncoef;  // ncoef the sums were computed for
   int chunk = 1;
   size_t smem = 0;
   // transposed factors
@@ -3233,9 +3238,10 @@ struct AdjBufs {
   DBuf<int> pinv, qcol;
   DBuf<TriDesc> tri;
   int max_nlev = 1;
-  cudaGraphExec_t graph = nullptr;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};  // one transposed sweep, mode 0 / 1
   ~AdjBufs() {
-    if (graph) cudaGraphExecDestroy(graph);
+    for (auto g : graph)
+      if (g) cudaGraphExecDestroy(g);
   }
 };
 
@@ -3318,40 +3324,38 @@ __global__ void __launch_bounds__(UPDATE_WARPS * 32) adj_fit_kernel(Net net, con
   }
 }
 
-// The evaluation kernel transposed: every point carries a weight w (the
-// adjoint of the value eval_kernel writes there); every source element of the
-// point's fracture receives w times the derivative of that value with respect
-// to its coefficients (complex pairs), its discharge (log term; sweep only)
-// and the fracture constant (phi points of the sweep).  Sweep points exclude
-// their own element, as eval_kernel does.  RHS: the head-vector points, whose
-// weight is mu of the row times the row's factor (-1/(D t0), +1/(D t1) for the
-// two sides of an intersection, -1/D for constant-head lines and wells);
-// series terms only.  Each thread holds ADJ_PPT points; per source and
-// coefficient a warp reduces its lanes' sums into shared memory, which is
-// added to global memory once per source chunk.
-template <bool RHS>
-__global__ void __launch_bounds__(EVAL_THREADS) adj_eval_kernel(Net net, const Item *__restrict__ items,
-                                                                  const int2 *__restrict__ pts,
-                                                                  const Group *__restrict__ groups,
-                                                                  const double *__restrict__ wsw,
-                                                                  const double *__restrict__ mu, cd *gc, double *gq,
-                                                                  double *gC, int chunk, const AdjState *as) {
-  if (as->s.done) return;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+// The sweep evaluation transposed: every collocation point carries a weight
+// w (the adjoint of the value eval_kernel writes there); every source element
+// of the point's fracture except the point's own element receives w times the
+// derivative of that value with respect to its coefficients (complex pairs),
+// its discharge (log term) and the fracture constant (phi points).  An item
+// holds up to EVAL_THREADS * P points of one fracture, P = 1, 2 or 4 (in
+// item.pad), each thread P of them.  Per source and coefficient every lane
+// sums its points, the lanes' sums go to a per-warp shared-memory table and
+// lane j adds up column j, so a warp spends one table write per coefficient
+// instead of a shuffle reduction; the block's sums go to global memory once
+// per source chunk.
+static constexpr int ADJ_RED_STRIDE = 33;  // lanes + 1 (bank spread)
+
+template <int P>
+__device__ __forceinline__ void adj_sweep_body(const Net &net, const Item &it, const int2 *__restrict__ pts,
+                                               const Group *__restrict__ groups, const double *__restrict__ wsw,
+                                               cd *gc, double *gq, double *gC, int chunk, unsigned char *smem) {
   const int MC = net.MC;
-  Src *src = reinterpret_cast<Src *>(smem_raw);
-  cd *sacc = reinterpret_cast<cd *>(smem_raw + sizeof(Src) * chunk);
-  double *sq = reinterpret_cast<double *>(sacc + (size_t)chunk * MC);
-  __shared__ double s_cw[EVAL_THREADS / 32];
-  const Item it = items[blockIdx.x];
-  const int f = it.frac;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  cd z[ADJ_PPT];
-  double w[ADJ_PPT];
-  int excl[ADJ_PPT], kind[ADJ_PPT];
+  Src *src = reinterpret_cast<Src *>(smem);
+  cd *sacc = reinterpret_cast<cd *>(smem + sizeof(Src) * chunk);
+  double *sq = reinterpret_cast<double *>(sacc + (size_t)chunk * MC);
+  double *red_re = sq + chunk + (size_t)warp * 2 * MC * ADJ_RED_STRIDE;
+  double *red_im = red_re + (size_t)MC * ADJ_RED_STRIDE;
+  __shared__ double s_cw[EVAL_THREADS / 32];
+  const int f = it.frac;
+  cd z[P];
+  double w[P];
+  int excl[P], kind[P];
   double cw = 0.0;
 #pragma unroll
-  for (int i = 0; i < ADJ_PPT; i++) {
+  for (int i = 0; i < P; i++) {
     const int p = it.p0 + threadIdx.x + i * EVAL_THREADS;
     z[i] = mk(0.0, 0.0);
     w[i] = 0.0;
@@ -3360,22 +3364,11 @@ __global__ void __launch_bounds__(EVAL_THREADS) adj_eval_kernel(Net net, const I
     if (p < it.p1) {
       const int2 gk = pts[p];
       const Group g = groups[gk.x];
-      if (RHS) {
-        const int j = g.elem;
-        const int e = net.de_ids[j];
-        const double m = mu[j];
-        if (net.type[e] == 0)
-          w[i] = g.side ? m / (net.D * net.t[net.frac1[e]]) : -m / (net.D * net.t[net.frac0[e]]);
-        else
-          w[i] = -m / net.D;
-        z[i] = (g.side ? net.zint1 : net.zint0)[(size_t)j * net.D + gk.y];
-      } else {
-        w[i] = wsw[g.out + gk.y];
-        excl[i] = g.elem;
-        kind[i] = g.kind;
-        z[i] = sweep_point(net, g.elem, g.side, gk.y);
-        if (g.kind == KIND_PHI) cw += w[i];
-      }
+      w[i] = wsw[g.out + gk.y];
+      excl[i] = g.elem;
+      kind[i] = g.kind;
+      z[i] = sweep_point(net, g.elem, g.side, gk.y);
+      if (g.kind == KIND_PHI) cw += w[i];
     }
   }
   const int e0 = net.fptr[f], e1 = net.fptr[f + 1];
@@ -3410,11 +3403,11 @@ __global__ void __launch_bounds__(EVAL_THREADS) adj_eval_kernel(Net net, const I
     for (int s = 0; s < cnt; s++) {
       const Src h = src[s];
       const double sg = h.pad ? -1.0 : 1.0;
-      cd rt[ADJ_PPT], pw[ADJ_PPT];
-      double wv[ADJ_PPT];
+      cd rt[P], pw[P];
+      double wv[P];
       double qc = 0.0;
 #pragma unroll
-      for (int i = 0; i < ADJ_PPT; i++) {
+      for (int i = 0; i < P; i++) {
         rt[i] = mk(0.0, 0.0);
         pw[i] = mk(1.0, 0.0);
         wv[i] = 0.0;
@@ -3431,19 +3424,20 @@ __global__ void __launch_bounds__(EVAL_THREADS) adj_eval_kernel(Net net, const I
           if (h.type == 4) rt[i] = recip(chi);
         }
         wv[i] = w[i] * sg;
-        if (!RHS && (h.type == 0 || h.type == 2 || h.type == 3)) {
+        if (h.type == 0 || h.type == 2 || h.type == 3) {
           const double lg = (kind[i] == KIND_PSI) ? atan2(chi.im, chi.re) : 0.5 * log(norm2(chi));
           qc += wv[i] / (2 * PI) * lg;
         }
       }
-      if (!RHS && (h.type == 0 || h.type == 2 || h.type == 3)) {
+      if (h.type == 0 || h.type == 2 || h.type == 3) {
         qc = warp_sum(qc);
         if (lane == 0) atomicAdd(&sq[s], qc);
       }
+      if (h.m == 0) continue;
       for (int j = 0; j < h.m; j++) {
         double ar = 0.0, ai = 0.0;
 #pragma unroll
-        for (int i = 0; i < ADJ_PPT; i++) {
+        for (int i = 0; i < P; i++) {
           // d(value)/d(Re c_j, Im c_j) = conj(x^j) (phi) or i conj(x^j) (psi), x^j = pw
           const double cr = wv[i] * pw[i].re, ci = wv[i] * pw[i].im;
           if (kind[i] == KIND_PSI) {
@@ -3455,13 +3449,20 @@ __global__ void __launch_bounds__(EVAL_THREADS) adj_eval_kernel(Net net, const I
           }
           pw[i] = mk(pw[i].re * rt[i].re - pw[i].im * rt[i].im, pw[i].re * rt[i].im + pw[i].im * rt[i].re);
         }
-        ar = warp_sum(ar);
-        ai = warp_sum(ai);
-        if (lane == 0) {
-          atomicAdd(&sacc[s * MC + j].re, ar);
-          atomicAdd(&sacc[s * MC + j].im, ai);
-        }
+        red_re[j * ADJ_RED_STRIDE + lane] = ar;
+        red_im[j * ADJ_RED_STRIDE + lane] = ai;
       }
+      __syncwarp();
+      for (int j = lane; j < h.m; j += 32) {
+        double sr = 0.0, si = 0.0;
+        for (int l = 0; l < 32; l++) {
+          sr += red_re[j * ADJ_RED_STRIDE + l];
+          si += red_im[j * ADJ_RED_STRIDE + l];
+        }
+        atomicAdd(&sacc[s * MC + j].re, sr);
+        atomicAdd(&sacc[s * MC + j].im, si);
+      }
+      __syncwarp();
     }
     __syncthreads();
     for (int idx = threadIdx.x; idx < cnt * MC; idx += blockDim.x) {
@@ -3472,20 +3473,126 @@ __global__ void __launch_bounds__(EVAL_THREADS) adj_eval_kernel(Net net, const I
       atomicAdd(&g->re, v.re);
       atomicAdd(&g->im, v.im);
     }
-    if (!RHS)
-      for (int s = threadIdx.x; s < cnt; s += blockDim.x)
-        if (sq[s] != 0.0) atomicAdd(&gq[src[s].id], sq[s]);
+    for (int s = threadIdx.x; s < cnt; s += blockDim.x)
+      if (sq[s] != 0.0) atomicAdd(&gq[src[s].id], sq[s]);
   }
-  if (!RHS) {
-    cw = warp_sum(cw);
-    if (lane == 0) s_cw[warp] = cw;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double t = 0.0;
-      for (int k = 0; k < EVAL_THREADS / 32; k++) t += s_cw[k];
-      if (t != 0.0) atomicAdd(&gC[f], t);
+  cw = warp_sum(cw);
+  if (lane == 0) s_cw[warp] = cw;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int k = 0; k < EVAL_THREADS / 32; k++) t += s_cw[k];
+    if (t != 0.0) atomicAdd(&gC[f], t);
+  }
+}
+
+__global__ void __launch_bounds__(EVAL_THREADS) adj_sweep_kernel(Net net, const Item *__restrict__ items,
+                                                                   const int2 *__restrict__ pts,
+                                                                   const Group *__restrict__ groups,
+                                                                   const double *__restrict__ wsw, cd *gc, double *gq,
+                                                                   double *gC, int chunk, const AdjState *as) {
+  if (as->s.done) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const Item it = items[blockIdx.x];
+  if (it.pad == 1)
+    adj_sweep_body<1>(net, it, pts, groups, wsw, gc, gq, gC, chunk, smem_raw);
+  else if (it.pad == 2)
+    adj_sweep_body<2>(net, it, pts, groups, wsw, gc, gq, gC, chunk, smem_raw);
+  else
+    adj_sweep_body<4>(net, it, pts, groups, wsw, gc, gq, gC, chunk, smem_raw);
+}
+
+// The head-vector evaluation transposed.  Its points carry one weight per
+// discharge row and side (mu of the row times -1/(D t0), +1/(D t1) for the
+// sides of an intersection, -1/D for a constant-head line or well), so the
+// sums over a side's D points of the series terms depend on the geometry
+// only: rhs_sums_kernel computes them once, S[pair][j] = sign * sum_k x_k^j
+// for every (row side, source element of that side's fracture) pair (one warp
+// per pair), and each iteration gathers gc[s][j] += sum over the pairs of s of
+// weight * conj(S[pair][j]) (one thread per source coefficient).
+__global__ void rhs_sums_kernel(Net net, const int *__restrict__ pair_g, const int *__restrict__ pair_src,
+                                const int *__restrict__ pair_off, int npairs, cd *S) {
+  const int pr = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (pr >= npairs) return;
+  const int g = pair_g[pr], el = pair_src[pr];
+  const int j = g >> 1, side = g & 1;
+  const int e = net.de_ids[j];
+  const int f = side ? net.frac1[e] : net.frac0[e];
+  const cd *zp = (side ? net.zint1 : net.zint0) + (size_t)j * net.D;
+  const int type = net.type[el], m = net.ncoef[el];
+  const bool neg = (type == 0 && net.frac0[el] != f);
+  const double sg = neg ? -1.0 : 1.0;
+  cd p0, p1;
+  if (type == 0 || type == 3 || type == 5) {
+    const cd *ep = neg ? net.ep1 + 2 * el : net.ep0 + 2 * el;
+    cd inv = recip(ep[1] - ep[0]);
+    cd ab = ep[0] + ep[1];
+    p0 = 2.0 * inv;
+    p1 = mk(-(ab.re * inv.re - ab.im * inv.im), -(ab.re * inv.im + ab.im * inv.re));
+  } else {
+    p0 = (type == 1) ? mk(0.0, 0.0) : net.center[el];
+    p1 = mk(1.0 / net.radius[el], 0.0);
+  }
+  cd *out = S + pair_off[pr];
+  // lanes take points k, k + 32, ... (KP per pass); powers advance per coefficient
+  constexpr int KP = 4;
+  for (int k0 = 0; k0 < net.D; k0 += 32 * KP) {
+    cd pw[KP], rt[KP];
+#pragma unroll
+    for (int i = 0; i < KP; i++) {
+      const int k = k0 + lane + 32 * i;
+      pw[i] = mk(0.0, 0.0);
+      rt[i] = mk(0.0, 0.0);
+      if (k < net.D) {
+        const cd zz = zp[k];
+        cd chi;
+        if (type == 0 || type == 3 || type == 5) {
+          chi = exterior_chi(fma_c(p0, zz, p1));
+          rt[i] = recip(chi);
+        } else if (type == 1) {
+          chi = p1.re * zz;
+          rt[i] = chi;
+        } else {
+          chi = p1.re * (zz - p0);
+          rt[i] = recip(chi);
+        }
+        pw[i] = mk(sg, 0.0);
+      }
+    }
+    for (int jj = 0; jj < m; jj++) {
+      double ar = 0.0, ai = 0.0;
+#pragma unroll
+      for (int i = 0; i < KP; i++) {
+        ar += pw[i].re;
+        ai += pw[i].im;
+        pw[i] = mk(pw[i].re * rt[i].re - pw[i].im * rt[i].im, pw[i].re * rt[i].im + pw[i].im * rt[i].re);
+      }
+      ar = warp_sum(ar);
+      ai = warp_sum(ai);
+      if (lane == 0) out[jj] = (k0 == 0) ? mk(ar, ai) : mk(out[jj].re + ar, out[jj].im + ai);
     }
   }
+}
+
+__global__ void adj_rhs_gather_kernel(Net net, const int *__restrict__ src_ptr, const int *__restrict__ src_pairs,
+                                      const int *__restrict__ pair_g, const int *__restrict__ pair_off,
+                                      const cd *__restrict__ S, const double *__restrict__ mu,
+                                      const double *__restrict__ fac, cd *gc, const AdjState *as) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (as->s.done || i >= (long long)net.ne * net.MC) return;
+  const int el = (int)(i / net.MC), j = (int)(i - (long long)el * net.MC);
+  if (j >= net.ncoef[el]) return;
+  double ar = 0.0, ai = 0.0;
+  for (int k = src_ptr[el]; k < src_ptr[el + 1]; k++) {
+    const int pr = src_pairs[k];
+    const int g = pair_g[pr];
+    const double wg = mu[g >> 1] * fac[g];
+    const cd v = S[pair_off[pr] + j];
+    ar += wg * v.re;  // weight * conj(S): the derivative of a phi value
+    ai -= wg * v.im;
+  }
+  gc[i].re += ar;
+  gc[i].im += ai;
 }
 
 // Right-hand side of the transposed discharge solve: dJ/dd + Phi_d^T lam.
@@ -3505,63 +3612,72 @@ __global__ void adj_gd_kernel(Net net, const double *gq_user, const double *gC_u
   gd[g] = d >= 0 ? gq_user[net.de_ids[d]] : gC_user[net.row_frac[g]];
 }
 
-// lam <- lam + omega (dJ/dc + Phi_c^T lam + b_c^T mu - lam), restricted to the
-// coefficient parts the update can change (imaginary parts of intersections
-// and constant-head lines, real parts of impermeable lines and c_0 of all but
-// bounding circles stay 0); per element max |delta| and max |lam|.
-__global__ void adj_update_kernel(Net net, cd *lam, const cd *gobj, const cd *gc, double *emax, const AdjState *as) {
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (as->s.done || e >= net.ne) return;
-  const int type = net.type[e], m = net.ncoef[e], MC = net.MC;
-  const double om = as->omega;
-  double dmax = 0.0, lmax = 0.0;
-  for (int j = 0; j < MC; j++) {
-    const size_t i = (size_t)e * MC + j;
-    cd v = mk(0.0, 0.0);
-    if (type != 2 && j < m && !(j == 0 && type != 1)) {
-      const cd l = lam[i], go = gobj[i], g = gc[i];
-      v = mk(l.re + om * (go.re + g.re - l.re), l.im + om * (go.im + g.im - l.im));
-      if (type == 0 || type == 3) v.im = 0.0;
-      if (type == 5) v.re = 0.0;
-      double dd = hypot(v.re - l.re, v.im - l.im);
-      if (!(dd == dd)) dd = INFINITY;
-      dmax = fmax(dmax, dd);
-      lmax = fmax(lmax, hypot(v.re, v.im));
-    }
-    lam[i] = v;
-  }
-  emax[2 * e] = dmax;
-  emax[2 * e + 1] = lmax;
+// The multiplier components the update can change: every coefficient below
+// ncoef, except the imaginary parts of intersections and constant-head lines
+// (real coefficients), the real parts of impermeable lines and c_0 of all
+// types but bounding circles (fixed at 0); wells have none.
+__device__ __forceinline__ cd adj_mask(const Net &net, int e, int j, cd v) {
+  const int type = net.type[e];
+  if (type == 2 || j >= net.ncoef[e] || (j == 0 && type != 1)) return mk(0.0, 0.0);
+  if (type == 0 || type == 3) v.im = 0.0;
+  if (type == 5) v.re = 0.0;
+  return v;
 }
 
-__global__ void __launch_bounds__(1024) adj_reduce_kernel(Net net, const double *emax, AdjState *as) {
-  if (as->s.done) return;
-  __shared__ double sd[32], sl[32];
-  double d = 0.0, l = 0.0;
-  for (int e = threadIdx.x; e < net.ne; e += blockDim.x) {
-    d = fmax(d, emax[2 * e]);
-    l = fmax(l, emax[2 * e + 1]);
+// With gc = Phi_c^T x + b_c^T mu(x) from one transposed sweep at lam = x:
+//   mode 0 (sweep with dJ/dd = 0):    y = mask(x - gc)          = (I - T^T) x
+//   mode 1 (sweep with the real dJ/dd): y = mask(dJ/dc + gc) - x = F(x) - x,
+// the residual of the multiplier equation lam = F(lam) (the right-hand side
+// when x = 0).
+__global__ void adj_combine_kernel(Net net, const cd *x, const cd *gc, const cd *gobj, cd *y, int mode) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= (long long)net.ne * net.MC) return;
+  const int e = (int)(i / net.MC), j = (int)(i - (long long)e * net.MC);
+  const cd xv = x[i], g = gc[i];
+  if (mode == 0) {
+    y[i] = adj_mask(net, e, j, mk(xv.re - g.re, xv.im - g.im));
+  } else {
+    const cd f = adj_mask(net, e, j, mk(gobj[i].re + g.re, gobj[i].im + g.im));
+    y[i] = mk(f.re - xv.re, f.im - xv.im);
   }
-  for (int o = 16; o > 0; o >>= 1) {
-    d = fmax(d, __shfl_xor_sync(0xffffffffu, d, o));
-    l = fmax(l, __shfl_xor_sync(0xffffffffu, l, o));
-  }
-  if ((threadIdx.x & 31) == 0) {
-    sd[threadIdx.x >> 5] = d;
-    sl[threadIdx.x >> 5] = l;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    for (int k = 0; k < (int)(blockDim.x >> 5); k++) {
-      d = fmax(d, sd[k]);
-      l = fmax(l, sl[k]);
+}
+
+// Dense vector kernels of the Krylov solve (vectors of n doubles, a basis of
+// nv vectors at stride `stride`): h[i] += V_i . w, w += sign sum_i h[i] V_i,
+// out = a w.
+__global__ void vec_mdot_kernel(const double *__restrict__ V, long long stride, int nv, const double *__restrict__ w,
+                                long long n, double *h) {
+  __shared__ double red[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int i = 0; i < nv; i++) {
+    const double *v = V + (size_t)i * stride;
+    double acc = 0.0;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+      acc = fma(v[k], w[k], acc);
+    acc = warp_sum(acc);
+    if (lane == 0) red[warp] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int k = 0; k < (int)(blockDim.x >> 5); k++) t += red[k];
+      atomicAdd(&h[i], t);
     }
-    as->s.nit += 1;
-    as->delta = d;
-    as->lam = l;
-    if (isinf(d) || !(l == l)) as->nonfinite = 1;
-    if (as->nonfinite || (as->s.nit >= 2 && d <= as->tol * l) || as->s.nit >= as->max_it) as->s.done = 1;
+    __syncthreads();
   }
+}
+
+__global__ void vec_update_kernel(double *w, const double *__restrict__ V, long long stride, int nv,
+                                  const double *__restrict__ h, double sign, long long n) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    double acc = 0.0;
+    for (int i = 0; i < nv; i++) acc = fma(h[i], V[(size_t)i * stride + k], acc);
+    w[k] = fma(sign, acc, w[k]);
+  }
+}
+
+__global__ void vec_scale_kernel(const double *w, double *out, double a, long long n) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+    out[k] = a * w[k];
 }
 
 // lam^T Phi_theta: for every intersection, sum_j>=1 lam_j.re (Re a0_j + Re a1_j)
@@ -3686,7 +3802,8 @@ static void adj_items(const std::vector<Group> &groups, const std::vector<int2> 
       it.frac = f;
       it.p0 = (int)a;
       it.p1 = (int)std::min(q, a + ADJ_ITEM);
-      it.pad = 0;
+      const int np = it.p1 - it.p0;
+      it.pad = np <= EVAL_THREADS ? 1 : (np <= 2 * EVAL_THREADS ? 2 : 4);  // points per thread
       items.push_back(it);
     }
     p = q;
@@ -3810,28 +3927,30 @@ static void launch_trisolve_adj(AndfnHandle *H, const Net &net, cudaStream_t s) 
   trisolve_kernel<true><<<1, H->solve_threads, solve_smem, s>>>(net, use_smem, cap_levptr, meta_cap);
 }
 
-static constexpr int ADJ_LAUNCHES = 10;  // per adjoint iteration (3 memsets + 7 kernels)
+static constexpr int ADJ_SWEEP_LAUNCHES = 9;  // per transposed sweep (3 memsets + 6 kernels)
+static constexpr int ADJ_RESTART = 40;        // Krylov basis size before a restart
 
-static void adj_enqueue_iteration(AndfnHandle *H, const Net &net, const Net &net_t, cudaStream_t s) {
+// One transposed sweep at lam = x: gc = Phi_c^T x + b_c^T A^-T (gd + Phi_d^T x),
+// then y = (I - T^T) x (mode 0, gd = 0) or y = F(x) - x (mode 1, the real dJ/dd).
+static void adj_enqueue_sweep(AndfnHandle *H, const Net &net, const Net &net_t, cudaStream_t s, const cd *x,
+                              const double *gd, cd *y, int mode) {
   AdjBufs &A = *H->adj;
   const int ne = (int)H->ne, nf = (int)H->nf, N = H->N, MC = H->MC;
+  const unsigned ce = (unsigned)(((long long)ne * MC + 255) / 256);
   cudaMemsetAsync(A.gc.p, 0, sizeof(cd) * (size_t)ne * MC, s);
   cudaMemsetAsync(A.gq.p, 0, sizeof(double) * ne, s);
   cudaMemsetAsync(A.gC.p, 0, sizeof(double) * nf, s);
   adj_fit_kernel<<<(ne + UPDATE_WARPS - 1) / UPDATE_WARPS, UPDATE_WARPS * 32, sizeof(double) * H->nvmax * UPDATE_WARPS,
-                   s>>>(net, A.lam.p, H->group_of.p, H->d_groups.p, A.wsw.p, A.gq.p, H->nvmax, A.st.p);
+                   s>>>(net, x, H->group_of.p, H->d_groups.p, A.wsw.p, A.gq.p, H->nvmax, A.st.p);
   if (A.n_items_sw > 0)
-    adj_eval_kernel<false><<<A.n_items_sw, EVAL_THREADS, A.smem, s>>>(net, A.items_sw.p, H->sweep_pts.p,
-                                                                       H->d_groups.p, A.wsw.p, A.mu.p, A.gc.p,
-                                                                       A.gq.p, A.gC.p, A.chunk, A.st.p);
-  adj_rhs_kernel<<<(N + 255) / 256, 256, 0, s>>>(net, A.gd.p, A.gq.p, A.gC.p, A.b.p, A.st.p);
+    adj_sweep_kernel<<<A.n_items_sw, EVAL_THREADS, A.smem, s>>>(net, A.items_sw.p, H->sweep_pts.p, H->d_groups.p,
+                                                                 A.wsw.p, A.gc.p, A.gq.p, A.gC.p, A.chunk, A.st.p);
+  adj_rhs_kernel<<<(N + 255) / 256, 256, 0, s>>>(net, gd, A.gq.p, A.gC.p, A.b.p, A.st.p);
   launch_trisolve_adj(H, net_t, s);
-  if (A.n_items_rhs > 0)
-    adj_eval_kernel<true><<<A.n_items_rhs, EVAL_THREADS, A.smem, s>>>(net, A.items_rhs.p, H->rhs_pts.p,
-                                                                      H->d_groups.p, A.wsw.p, A.mu.p, A.gc.p,
-                                                                      A.gq.p, A.gC.p, A.chunk, A.st.p);
-  adj_update_kernel<<<(ne + 255) / 256, 256, 0, s>>>(net, A.lam.p, A.gobj.p, A.gc.p, A.emax.p, A.st.p);
-  adj_reduce_kernel<<<1, 1024, 0, s>>>(net, A.emax.p, A.st.p);
+  if (A.npairs > 0)
+    adj_rhs_gather_kernel<<<ce, 256, 0, s>>>(net, A.src_ptr.p, A.src_pairs.p, A.pair_g.p, A.pair_off.p, A.S.p,
+                                             A.mu.p, A.fac.p, A.gc.p, A.st.p);
+  adj_combine_kernel<<<ce, 256, 0, s>>>(net, x, A.gc.p, A.gobj.p, y, mode);
 }
 
 static int adjoint_impl(AndfnHandle *H, const double *gcoef, int64_t mco, const double *gq_user,
@@ -3857,30 +3976,88 @@ static int adjoint_impl(AndfnHandle *H, const double *gcoef, int64_t mco, const 
     int rc = adj_build_factors(H);
     if (rc) return rc;
   }
-  // point tables: the forward lists (rebuilt in the same order), in items of
-  // up to ADJ_ITEM points
+  // sweep point tables: the forward list (rebuilt in the same order), in
+  // items of up to ADJ_ITEM points of one fracture
   {
     std::vector<Group> groups;
-    std::vector<int> go, rg;
-    std::vector<Item> si, ri, items;
-    std::vector<int2> spts, rpts;
-    int nsv = 0, nrv = 0;
+    std::vector<int> go;
+    std::vector<Item> si, items;
+    std::vector<int2> spts;
+    int nsv = 0;
     build_tables(H, false, groups, go, si, spts, nsv);
-    build_tables(H, true, groups, rg, ri, rpts, nrv);
     adj_items(groups, spts, items);
     CK(upload(A.items_sw, items, s));
     A.n_items_sw = (int)items.size();
-    adj_items(groups, rpts, items);
-    CK(upload(A.items_rhs, items, s));
-    A.n_items_rhs = (int)items.size();
     CK(A.wsw.alloc(std::max(1, nsv)));
     int maxnf = 1;
     for (int f = 0; f < nf; f++) maxnf = std::max(maxnf, H->h.fptr[f + 1] - H->h.fptr[f]);
+    const size_t red = sizeof(double) * 2 * MC * ADJ_RED_STRIDE * (EVAL_THREADS / 32);
     const size_t per = sizeof(Src) + sizeof(cd) * MC + sizeof(double);
-    A.chunk = std::max(1, std::min((int)(96 * 1024 / per), maxnf));
-    A.smem = per * A.chunk;
-    CK(cudaFuncSetAttribute(adj_eval_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    CK(cudaFuncSetAttribute(adj_eval_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    const size_t budget = 100 * 1024 > red + per ? 100 * 1024 - red : per;
+    A.chunk = std::max(1, std::min((int)(budget / per), maxnf));
+    A.smem = per * A.chunk + red;
+    if (A.smem > 200 * 1024) {
+      set_error("adjoint: coefficient capacity too large for the transposed evaluation");
+      return ANDFN_BAD_INPUT;
+    }
+    CK(cudaFuncSetAttribute(adj_sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+  }
+  // head-vector power sums (geometry and ncoef only: computed once per handle)
+  if (A.sums_ncoef != H->cur_ncoef) {
+    const HostNet &h = H->h;
+    std::vector<int> pg, ps, po;
+    std::vector<std::vector<int>> by_src(ne);
+    int off = 0;
+    for (int j = 0; j < n_de; j++) {
+      const int e = h.de_ids[j];
+      const int sides = (h.type[e] == 0) ? 2 : 1;
+      for (int sd = 0; sd < sides; sd++) {
+        const int f = sd ? h.frac1[e] : h.frac0[e];
+        for (int k = h.fptr[f]; k < h.fptr[f + 1]; k++) {
+          const int el = h.felem[k];
+          const int m = H->cur_ncoef[el];
+          if (h.type[el] == 2 || m <= 0) continue;
+          by_src[el].push_back((int)pg.size());
+          pg.push_back(2 * j + sd);
+          ps.push_back(el);
+          po.push_back(off);
+          off += m;
+        }
+      }
+    }
+    std::vector<int> sp(ne + 1, 0), spairs;
+    for (int el = 0; el < ne; el++) {
+      sp[el + 1] = sp[el] + (int)by_src[el].size();
+      spairs.insert(spairs.end(), by_src[el].begin(), by_src[el].end());
+    }
+    A.npairs = (int)pg.size();
+    if (A.npairs > 0) {
+      CK(upload(A.pair_g, pg, s));
+      CK(upload(A.pair_src, ps, s));
+      CK(upload(A.pair_off, po, s));
+      CK(upload(A.src_ptr, sp, s));
+      CK(upload(A.src_pairs, spairs, s));
+      CK(A.S.alloc(std::max(1, off)));
+      rhs_sums_kernel<<<(A.npairs * 32 + 127) / 128, 128, 0, s>>>(H->net(), A.pair_g.p, A.pair_src.p,
+                                                                   A.pair_off.p, A.npairs, A.S.p);
+      CK(cudaGetLastError());
+    }
+    A.sums_ncoef = H->cur_ncoef;
+  }
+  {
+    // row-side weights per unit mu (t may have changed since the sums)
+    const HostNet &h = H->h;
+    std::vector<double> fac(2 * (size_t)std::max(1, n_de), 0.0);
+    for (int j = 0; j < n_de; j++) {
+      const int e = h.de_ids[j];
+      if (h.type[e] == 0) {
+        fac[2 * j] = -1.0 / (H->D * h.t[h.frac0[e]]);
+        fac[2 * j + 1] = 1.0 / (H->D * h.t[h.frac1[e]]);
+      } else {
+        fac[2 * j] = -1.0 / H->D;
+      }
+    }
+    CK(upload(A.fac, fac, s));
   }
   CK(A.st.alloc(1));
   CK(A.st_eval.alloc(1));
@@ -3892,7 +4069,6 @@ static int adjoint_impl(AndfnHandle *H, const double *gcoef, int64_t mco, const 
   CK(A.gd.alloc(N));
   CK(A.b.alloc(N));
   CK(A.mu.alloc(N));
-  CK(A.emax.alloc(2 * (size_t)ne));
   CK(A.gtheta.alloc(nf));
   CK(A.obar.alloc(2 * (size_t)std::max(1, n_de)));
   // objective gradients
@@ -3913,15 +4089,23 @@ static int adjoint_impl(AndfnHandle *H, const double *gcoef, int64_t mco, const 
   if (H->n_sweep_items > 0)
     eval_kernel<false><<<H->n_sweep_items, EVAL_THREADS, H->eval_smem, s>>>(
         net_e, H->sweep_items.p, H->sweep_pts.p, H->d_groups.p, H->sweep_vals.p, H->chunk);
-  // loop state
+  // The multipliers solve the linear system (I - T^T) lam = F(0), F(lam) =
+  // mask(dJ/dc + gc(lam)) with gc from one transposed sweep (the damped
+  // fixed-point iteration lam <- F(lam) contracts only as fast as the forward
+  // loop).  Restarted GMRES with this operator, classical Gram-Schmidt
+  // applied twice; the start vector is 0.
   AdjState as0;
   std::memset(&as0, 0, sizeof(as0));
-  const double d = H->last_damping;
-  as0.omega = 1.0 - (1.0 - d) * (1.0 - d);
-  as0.tol = tol;
-  as0.max_it = (int)std::min<int64_t>(max_it, 1 << 30);
   CK(cudaMemcpyAsync(A.st.p, &as0, sizeof(as0), cudaMemcpyHostToDevice, s));
-  CK(cudaMemsetAsync(A.lam.p, 0, sizeof(cd) * (size_t)ne * MC, s));
+  const long long nd = (long long)ne * MC, n2 = 2 * nd;
+  const int mk_ = ADJ_RESTART;
+  CK(A.V.alloc((size_t)(mk_ + 1) * nd));
+  CK(A.xin.alloc(nd));
+  CK(A.wv.alloc(nd));
+  CK(A.gd0.alloc(N));
+  CK(A.hbuf.alloc(2 * (size_t)(mk_ + 2)));
+  CK(cudaMemsetAsync(A.gd0.p, 0, sizeof(double) * N, s));
+  CK(cudaMemsetAsync(A.lam.p, 0, sizeof(cd) * nd, s));
   CK(cudaMemsetAsync(A.mu.p, 0, sizeof(double) * N, s));
   CK(cudaStreamSynchronize(s));
   CK(cudaGetLastError());
@@ -3932,29 +4116,123 @@ static int adjoint_impl(AndfnHandle *H, const double *gcoef, int64_t mco, const 
   net_t.bvec = A.b.p;
   net_t.disc = A.mu.p;
   net_t.tri = A.tri.p;
-  if (A.graph) {
-    cudaGraphExecDestroy(A.graph);
-    A.graph = nullptr;
-  }
-  {
+  for (auto &g : A.graph)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+  for (int mode = 0; mode < 2; mode++) {
     cudaGraph_t g;
     CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-    for (int b = 0; b < ITER_BATCH; b++) adj_enqueue_iteration(H, net, net_t, s);
+    adj_enqueue_sweep(H, net, net_t, s, A.xin.p, mode ? A.gd.p : A.gd0.p, A.wv.p, mode);
     CK(cudaStreamEndCapture(s, &g));
-    CK(cudaGraphInstantiate(&A.graph, g, 0));
+    CK(cudaGraphInstantiate(&A.graph[mode], g, 0));
     cudaGraphDestroy(g);
   }
-  AdjState fin;
-  int guard = 0;
-  int64_t launches = 4;
-  while (true) {
-    CK(cudaGraphLaunch(A.graph, s));
-    CK(cudaMemcpyAsync(&fin, A.st.p, sizeof(fin), cudaMemcpyDeviceToHost, s));
+  double *V = reinterpret_cast<double *>(A.V.p);
+  double *wv = reinterpret_cast<double *>(A.wv.p);
+  double *hd = A.hbuf.p;
+  const int vb = 4 * 148, vt = 256;
+  int64_t matvecs = 0, launches = 4;
+  // |w|^2 on the device into hd[0], read back
+  auto norm2_of = [&](const double *w, double &out) -> int {
+    CK(cudaMemsetAsync(hd, 0, sizeof(double), s));
+    vec_mdot_kernel<<<vb, vt, 0, s>>>(w, 0, 1, w, n2, hd);
+    CK(cudaMemcpyAsync(&out, hd, sizeof(double), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
-    launches += ITER_BATCH * ADJ_LAUNCHES;
-    if (fin.s.done) break;
-    if (++guard > as0.max_it / ITER_BATCH + 2) break;
+    launches += 1;
+    return 0;
+  };
+  auto sweep = [&](const double *x, int mode) -> int {  // wv = (I - T^T) x or F(x) - x
+    CK(cudaMemcpyAsync(A.xin.p, x, sizeof(double) * n2, cudaMemcpyDeviceToDevice, s));
+    CK(cudaGraphLaunch(A.graph[mode], s));
+    matvecs++;
+    launches += ADJ_SWEEP_LAUNCHES;
+    return 0;
+  };
+  double bnorm = 0.0, rel = 1.0;
+  int nonfinite = 0;
+  std::vector<double> Hm((size_t)(mk_ + 1) * mk_), cs(mk_), sn(mk_), gv(mk_ + 1), hh(2 * (mk_ + 2));
+  while (true) {
+    // residual r = F(x) - x
+    if (sweep(reinterpret_cast<const double *>(A.lam.p), 1)) return ANDFN_CUDA_ERROR;
+    double r2 = 0.0;
+    if (norm2_of(wv, r2)) return ANDFN_CUDA_ERROR;
+    const double beta = std::sqrt(r2);
+    if (!std::isfinite(beta)) {
+      nonfinite = 1;
+      break;
+    }
+    if (matvecs == 1) bnorm = beta;
+    if (bnorm == 0.0) {
+      rel = 0.0;
+      break;
+    }
+    rel = beta / bnorm;
+    if (rel <= tol || matvecs >= max_it) break;
+    vec_scale_kernel<<<vb, vt, 0, s>>>(wv, V, 1.0 / beta, n2);
+    std::fill(gv.begin(), gv.end(), 0.0);
+    gv[0] = beta;
+    int k = 0;
+    for (int j = 0; j < mk_; j++) {
+      if (sweep(V + (size_t)j * n2, 0)) return ANDFN_CUDA_ERROR;
+      CK(cudaMemsetAsync(hd, 0, sizeof(double) * 2 * (mk_ + 2), s));
+      for (int pass = 0; pass < 2; pass++) {
+        double *hp = hd + pass * (mk_ + 2);
+        vec_mdot_kernel<<<vb, vt, 0, s>>>(V, n2, j + 1, wv, n2, hp);
+        vec_update_kernel<<<vb, vt, 0, s>>>(wv, V, n2, j + 1, hp, -1.0, n2);
+      }
+      vec_mdot_kernel<<<vb, vt, 0, s>>>(wv, 0, 1, wv, n2, hd + 2 * (mk_ + 2) - 1);
+      launches += 5;
+      CK(cudaMemcpyAsync(hh.data(), hd, sizeof(double) * 2 * (mk_ + 2), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      const double hn = std::sqrt(hh[2 * (mk_ + 2) - 1]);
+      for (int i = 0; i <= j; i++) Hm[(size_t)i * mk_ + j] = hh[i] + hh[mk_ + 2 + i];
+      Hm[(size_t)(j + 1) * mk_ + j] = hn;
+      // previous rotations, then a new one that zeroes H(j+1, j)
+      for (int i = 0; i < j; i++) {
+        const double a = Hm[(size_t)i * mk_ + j], b = Hm[(size_t)(i + 1) * mk_ + j];
+        Hm[(size_t)i * mk_ + j] = cs[i] * a + sn[i] * b;
+        Hm[(size_t)(i + 1) * mk_ + j] = -sn[i] * a + cs[i] * b;
+      }
+      const double a = Hm[(size_t)j * mk_ + j], b = hn;
+      const double r = std::hypot(a, b);
+      cs[j] = r > 0 ? a / r : 1.0;
+      sn[j] = r > 0 ? b / r : 0.0;
+      Hm[(size_t)j * mk_ + j] = r;
+      Hm[(size_t)(j + 1) * mk_ + j] = 0.0;
+      gv[j + 1] = -sn[j] * gv[j];
+      gv[j] = cs[j] * gv[j];
+      k = j + 1;
+      if (!std::isfinite(hn) || !std::isfinite(gv[j + 1])) {
+        nonfinite = 1;
+        break;
+      }
+      rel = std::fabs(gv[j + 1]) / bnorm;
+      if (hn > 0.0) vec_scale_kernel<<<vb, vt, 0, s>>>(wv, V + (size_t)(j + 1) * n2, 1.0 / hn, n2);
+      if (rel <= tol || matvecs >= max_it || hn == 0.0) break;
+    }
+    if (nonfinite) break;
+    // x += V y, H y = g (upper triangular k x k)
+    std::vector<double> y(k, 0.0);
+    for (int i = k - 1; i >= 0; i--) {
+      double t = gv[i];
+      for (int c = i + 1; c < k; c++) t -= Hm[(size_t)i * mk_ + c] * y[c];
+      y[i] = t / Hm[(size_t)i * mk_ + i];
+    }
+    CK(cudaMemcpyAsync(hd, y.data(), sizeof(double) * k, cudaMemcpyHostToDevice, s));
+    vec_update_kernel<<<vb, vt, 0, s>>>(reinterpret_cast<double *>(A.lam.p), V, n2, k, hd, 1.0, n2);
+    CK(cudaStreamSynchronize(s));
+    launches += 1;
   }
+  // the multiplier of the discharge system at the final lam, and the true
+  // residual of the final lam (mode 1 sweep)
+  if (sweep(reinterpret_cast<const double *>(A.lam.p), 1)) return ANDFN_CUDA_ERROR;
+  double rf2 = 0.0;
+  if (norm2_of(wv, rf2)) return ANDFN_CUDA_ERROR;
+  const double rel_true = bnorm > 0 ? std::sqrt(rf2) / bnorm : 0.0;
+  double l2 = 0.0;
+  if (norm2_of(reinterpret_cast<const double *>(A.lam.p), l2)) return ANDFN_CUDA_ERROR;
   // lam^T Phi_theta and the mean potentials of the discharge rows
   CK(cudaMemsetAsync(A.gtheta.p, 0, sizeof(double) * nf, s));
   adj_theta_kernel<<<(ne * 32 + 127) / 128, 128, 0, s>>>(net, A.lam.p, H->group_of.p, H->d_groups.p,
@@ -3986,16 +4264,16 @@ static int adjoint_impl(AndfnHandle *H, const double *gcoef, int64_t mco, const 
   CK(cudaMemcpyAsync(glogt, gth.data(), sizeof(double) * nf, cudaMemcpyHostToDevice, s));
   CK(cudaStreamSynchronize(s));
   int status = ANDFN_OK;
-  if (fin.nonfinite)
+  if (nonfinite || !std::isfinite(rel_true))
     status = ANDFN_NONFINITE;
-  else if (!(fin.delta <= tol * fin.lam))
+  else if (!(rel_true <= 10.0 * tol))
     status = ANDFN_MAX_ITERATIONS;
   if (S) {
     std::memset(S, 0, sizeof(*S));
-    S->iterations = fin.s.nit;
-    S->delta = fin.delta;
-    S->lam = fin.lam;
-    S->omega = as0.omega;
+    S->iterations = matvecs;
+    S->residual = rel_true;
+    S->lam_norm = std::sqrt(l2);
+    S->restart = ADJ_RESTART;
     S->ms_setup = ms_setup;
     S->ms_iterate = ms_since(t1);
     S->ms_total = ms_since(t0);

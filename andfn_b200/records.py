@@ -99,8 +99,8 @@ class AndfnSolveStats(ctypes.Structure):
         return d
 
 class AndfnAdjointStats(ctypes.Structure):
-    _fields_ = [("iterations", ctypes.c_int64), ("delta", ctypes.c_double), ("lam", ctypes.c_double),
-                ("omega", ctypes.c_double), ("ms_setup", ctypes.c_double), ("ms_iterate", ctypes.c_double),
+    _fields_ = [("iterations", ctypes.c_int64), ("residual", ctypes.c_double), ("lam_norm", ctypes.c_double),
+                ("restart", ctypes.c_int64), ("ms_setup", ctypes.c_double), ("ms_iterate", ctypes.c_double),
                 ("ms_total", ctypes.c_double), ("gpu_launches", ctypes.c_int64), ("status", ctypes.c_int32),
                 ("pad", ctypes.c_int32)]
 

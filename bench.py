@@ -320,6 +320,7 @@ def run_gpu(args):
             ev[k] = {"achieved_tflops": fl / (per[k] * 1e-3) / 1e12, "frac_of_fp64": fl / (per[k] * 1e-3) / 1e12 / fp64_tflops,
                      "avg_us": per[k] * 1e3}
     batched = None if args.no_batch else run_batched(args, device, flush)
+    adjoint = None if args.no_adjoint else run_adjoint(args, device, F, E)
     if rank == 0:
         cpu = None
         if not args.no_cpu:
@@ -339,7 +340,8 @@ def run_gpu(args):
                 "gpu_launches": int(launches), "roofline": roof, "kernels_us": {k: (v * 1e3 if v else None) for k, v in per.items()},
                 "kernel_share": {k: kt[k][0] / max(1e-12, sum(v[0] for v in kt.values())) for k in kt},
                 "eval_roofline": ev, "phase_ms": {k: stats[k] for k in ("ms_setup", "ms_factor", "ms_iterate")},
-                "fp64_peak_tflops": fp64_tflops, "clocks": clk, "cpu_baseline": cpu, "batched": batched}
+                "fp64_peak_tflops": fp64_tflops, "clocks": clk, "cpu_baseline": cpu, "batched": batched,
+                "adjoint": adjoint}
         print(json.dumps(line), flush=True)
     solver.close()
     if ws > 1:
@@ -420,6 +422,95 @@ def run_batched(args, device, flush, sample=32):
             "kernels_ms_per_step": {k: v[0] / args.steps for k, v in kt.items()}}
 
 
+ADJ_WORKLOAD = ("adjoint: the plain-solve network + 50 observation points (uniform on random fractures, seed 7), "
+                "h_obs = forward heads + N(0, 0.01); J = sum (h - h_obs)^2 + discharge through the x = L face; "
+                "dJ/dlog t of every fracture through torch.autograd")
+
+
+def run_adjoint(args, device, F, E, fd_fracs=10, fd_its=400, steps_fd=(1e-6, 1e-4)):
+    """Gradient of the head-misfit + outflow objective w.r.t. log t of all
+    fractures: time of the backward pass against the forward solve, and a
+    central finite-difference check of the fd_fracs largest gradient entries
+    (forward solves of a fixed fd_its iterations for the check, so J is a
+    smooth function of log t), at each step in steps_fd."""
+    import torch
+    from andfn_b200.adjoint import DFNModel
+    from andfn_b200.records import default_constants
+    D = 50
+    dev = f"cuda:{device}"
+    rng = np.random.default_rng(7)
+    n_obs = 50
+    fr = rng.integers(0, len(F), n_obs)
+    z = F["radius"][fr] * 0.9 * np.sqrt(rng.uniform(size=n_obs)) * np.exp(2j * np.pi * rng.uniform(size=n_obs))
+    frt = torch.tensor(fr, dtype=torch.int64, device=dev)
+    zt = torch.tensor(z, dtype=torch.complex128, device=dev)
+    outlet = torch.tensor(np.nonzero((E["_type"] == 3) & (E["head"] == 0.0))[0], device=dev)
+    logt0 = np.log(F["t"].astype(np.float64))
+
+    def objective(model, hobs, lt):
+        coef, q, C = model.solve(lt)
+        h = model.heads(coef, q, C, lt, frt, zt)
+        return ((h - hobs) ** 2).sum() + q[outlet].sum(), h
+
+    out = {"workload": ADJ_WORKLOAD, "observations": n_obs}
+    model = DFNModel(F.copy(), E.copy(), constants(), D, device=device, adjoint_tol=1e-8)
+    lt = torch.tensor(logt0, dtype=torch.float64, device=dev)
+    with torch.no_grad():
+        _, h0 = objective(model, torch.zeros(n_obs, dtype=torch.float64, device=dev), lt)
+    hobs = h0 + torch.tensor(rng.normal(0.0, 0.01, n_obs), device=dev)
+    fwd, bwd, its, adj_its = [], [], [], []
+    for i in range(args.warmup + args.steps):
+        ltg = lt.clone().requires_grad_(True)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        J, _ = objective(model, hobs, ltg)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        J.backward()
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        if i >= args.warmup:
+            fwd.append(t1 - t0)
+            bwd.append(t2 - t1)
+            its.append(model.stats["iterations"])
+            adj_its.append(model.adjoint_stats["iterations"])
+    g = ltg.grad.detach().cpu().numpy()
+    out.update({"forward_ms": 1e3 * float(np.mean(fwd)), "gradient_ms": 1e3 * float(np.mean(bwd)),
+                "gradient_over_forward": float(np.mean(bwd) / np.mean(fwd)),
+                "forward_iterations": int(its[-1]), "adjoint_iterations": int(adj_its[-1]),
+                "adjoint_tol": 1e-8, "adjoint_status": int(model.adjoint_stats["status"]),
+                "grad_norm": float(np.linalg.norm(g))})
+    model.close()
+    if fd_fracs > 0:
+        cfd = default_constants(MAX_ITERATIONS=fd_its, MAX_ERROR=1e-300, MAX_NCOEF=20)
+        m2 = DFNModel(F.copy(), E.copy(), cfd, D, device=device, adjoint_tol=1e-10)
+        ltg = lt.clone().requires_grad_(True)
+        J, _ = objective(m2, hobs, ltg)
+        J.backward()
+        ga = ltg.grad.detach().cpu().numpy()
+        sel = np.argsort(-np.abs(ga))[:fd_fracs]
+        checks = []
+        with torch.no_grad():
+            for h_fd in steps_fd:
+                gf = np.zeros(fd_fracs)
+                for k, f in enumerate(sel):
+                    vals = []
+                    for sgn in (1.0, -1.0):
+                        l2 = logt0.copy()
+                        l2[f] += sgn * h_fd
+                        Jv, _ = objective(m2, hobs, torch.tensor(l2, dtype=torch.float64, device=dev))
+                        vals.append(float(Jv))
+                    gf[k] = (vals[0] - vals[1]) / (2 * h_fd)
+                rel = np.abs(ga[sel] - gf) / np.abs(gf)
+                checks.append({"step": h_fd, "max_rel_err": float(rel.max()), "median_rel_err": float(np.median(rel)),
+                               "max_err_over_max_grad": float(np.abs(ga[sel] - gf).max() / np.abs(ga).max())})
+        out["fd_check"] = {"fractures": int(fd_fracs), "selection": "largest |dJ/dlog t|",
+                           "forward_iterations": fd_its, "adjoint_iterations": int(m2.adjoint_stats["iterations"]),
+                           "adjoint_status": int(m2.adjoint_stats["status"]), "steps": checks}
+        m2.close()
+    return out
+
+
 def aggregate_ranks(total_ms: float, steps: int, world_size: int, device=None) -> tuple[float, float]:
     """Slowest rank's timed milliseconds (all-reduce MAX) and the whole-job
     value: every rank solves its own network, so value = world_size * steps
@@ -451,6 +542,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-realizations measurement")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint (gradient) measurement")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

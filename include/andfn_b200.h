@@ -204,9 +204,13 @@ int andfn_b200_eval_heads_noalloc(AndfnHandle *h, const int64_t *frac,
  * objective J(coef, q, C, log t) of the converged solve of a single-network
  * handle, andfn_b200_adjoint returns dJ/dlog t_f (natural log) for every
  * fracture, given the partial derivatives of J with respect to the solved
- * state.  It runs the transposed fixed-point iteration of the solve (no
- * forward iterates are stored) with the transposed factors of the last run;
- * it stops when max|delta lam| <= tol * max|lam| or after max_iterations.
+ * state.  The multipliers of the solve's two equations (element sweep and
+ * discharge system) solve a linear system whose operator is one transposed
+ * sweep (the transposes of the sweep evaluation, the DFT fit and the
+ * discharge solve, with the transposed factors of the last run); it is
+ * solved by restarted GMRES, so no forward iterate is stored.  The solve
+ * stops when the relative residual |F(lam) - lam| / |F(0)| <= tol or after
+ * max_iterations transposed sweeps.
  * All array arguments of the functions in this block are DEVICE pointers on
  * the handle's device; complex values are (re, im) double pairs:
  *   gcoef [ne][mco][2]  dJ/d(Re, Im) coef (entries beyond ncoef are ignored)
@@ -218,13 +222,13 @@ int andfn_b200_eval_heads_noalloc(AndfnHandle *h, const int64_t *frac,
  *                       e.g. from andfn_b200_heads_vjp)
  * Requires a completed andfn_b200_run on the handle (with MAX_NCOEF =
  * ncoef, so that no coefficients grow) and no reset since.  Returns 0, or
- * ANDFN_MAX_ITERATIONS when the tolerance was not reached (the gradient of
- * the last iterate is still written). */
+ * ANDFN_MAX_ITERATIONS when the final residual is above 10 tol (the gradient
+ * of the last iterate is still written). */
 typedef struct {
-  int64_t iterations;
-  double delta;           /* final max |delta lam|            */
-  double lam;             /* final max |lam|                   */
-  double omega;           /* damping of the transposed loop    */
+  int64_t iterations;     /* transposed sweeps (operator applications) */
+  double residual;        /* final relative residual                  */
+  double lam_norm;        /* |lam|                                     */
+  int64_t restart;        /* Krylov basis size between restarts        */
   double ms_setup, ms_iterate, ms_total;
   int64_t gpu_launches;
   int32_t status;
