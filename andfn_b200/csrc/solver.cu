@@ -824,10 +824,35 @@ __global__ void rhs_reduce_kernel(Net net, const double *__restrict__ rhs_vals, 
 // 32 rows.  One warp solves the panel's triangle with its 32 rows in
 // registers (shuffle broadcast of each solved value), then the whole CTA
 // updates the rows below (lower) / above (upper) with coalesced column reads.
+// One panel's contribution to row i of a dense tail: sum_j<nb M(i, r0 + j) p_j
+// (col points at M(i, r0), column-major), all nb loads issued first.
+__device__ __forceinline__ double panel_dot(const double *__restrict__ col, int K, const double *pv, int nb) {
+  double v[32];
+#pragma unroll
+  for (int j = 0; j < 32; j++) v[j] = (j < nb) ? __ldg(col + (size_t)j * K) : 0.0;
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+#pragma unroll
+  for (int j = 0; j < 32; j += 4) {
+    a0 = fma(v[j], pv[j], a0);
+    a1 = fma(v[j + 1], pv[j + 1], a1);
+    a2 = fma(v[j + 2], pv[j + 2], a2);
+    a3 = fma(v[j + 3], pv[j + 3], a3);
+  }
+  return (a0 + a1) + (a2 + a3);
+}
+
+// The panels are pipelined: after the barrier that publishes panel p, warp 0
+// first updates the 32 rows of the next panel and goes straight on to that
+// panel's triangle, while the other warps update the remaining rows with
+// panel p; one barrier per panel.  The solved panel values go to a
+// double-buffered shared array (zero padded), so a warp still reading panel p
+// never sees panel p + 1.
 __device__ void dense_lower_solve(const double *__restrict__ Lcm, int K, double *y) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int r0 = 0; r0 < K; r0 += 32) {
-    const int nb = min(32, K - r0);
+  __shared__ double s_pan[2][32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, bd = blockDim.x;
+  const int npan = (K + 31) / 32;
+  for (int p = 0; p < npan; p++) {
+    const int r0 = p * 32, nb = min(32, K - r0);
     if (warp == 0) {
       double row[32];
 #pragma unroll
@@ -840,25 +865,30 @@ __device__ void dense_lower_solve(const double *__restrict__ Lcm, int K, double 
         if (lane > j) yi = fma(-row[j], yj, yi);
       }
       if (lane < nb) y[r0 + lane] = yi;
+      s_pan[p & 1][lane] = (lane < nb) ? yi : 0.0;
     }
     __syncthreads();
-    for (int i = r0 + nb + threadIdx.x; i < K; i += blockDim.x) {
-      double acc = 0.0;
-      const double *col = Lcm + (size_t)r0 * K + i;
-#pragma unroll 8
-      for (int j = 0; j < nb; j++) acc = fma(__ldg(col + (size_t)j * K), y[r0 + j], acc);
-      y[i] -= acc;
+    const double *pv = s_pan[p & 1];
+    if (warp == 0) {
+      const int i = r0 + 32 + lane;
+      if (i < K) y[i] -= panel_dot(Lcm + (size_t)r0 * K + i, K, pv, nb);
+      if (bd == 32)
+        for (int k = r0 + 64 + lane; k < K; k += 32) y[k] -= panel_dot(Lcm + (size_t)r0 * K + k, K, pv, nb);
+      __syncwarp();
+    } else {
+      for (int i = r0 + 64 + threadIdx.x - 32; i < K; i += bd - 32)
+        y[i] -= panel_dot(Lcm + (size_t)r0 * K + i, K, pv, nb);
     }
-    __syncthreads();
   }
+  __syncthreads();
 }
 
 __device__ void dense_upper_solve(const double *__restrict__ Ucm, const double *__restrict__ uinv, int K, double *y) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __shared__ double s_pan[2][32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, bd = blockDim.x;
   const int npan = (K + 31) / 32;
-  for (int pi = npan - 1; pi >= 0; pi--) {
-    const int r0 = pi * 32;
-    const int nb = min(32, K - r0);
+  for (int p = npan - 1; p >= 0; p--) {
+    const int r0 = p * 32, nb = min(32, K - r0);
     if (warp == 0) {
       double row[32];
 #pragma unroll
@@ -873,17 +903,23 @@ __device__ void dense_upper_solve(const double *__restrict__ Ucm, const double *
         if (lane < j) yi = fma(-row[j], xj, yi);
       }
       if (lane < nb) y[r0 + lane] = yi;
+      s_pan[p & 1][lane] = (lane < nb) ? yi : 0.0;
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < r0; i += blockDim.x) {
-      double acc = 0.0;
-      const double *col = Ucm + (size_t)r0 * K + i;
-#pragma unroll 8
-      for (int j = 0; j < nb; j++) acc = fma(__ldg(col + (size_t)j * K), y[r0 + j], acc);
-      y[i] -= acc;
+    const double *pv = s_pan[p & 1];
+    if (warp == 0) {
+      if (p > 0) {
+        const int i = r0 - 32 + lane;
+        y[i] -= panel_dot(Ucm + (size_t)r0 * K + i, K, pv, nb);
+      }
+      if (bd == 32)
+        for (int k = lane; k < r0 - 32; k += 32) y[k] -= panel_dot(Ucm + (size_t)r0 * K + k, K, pv, nb);
+      __syncwarp();
+    } else {
+      for (int i = threadIdx.x - 32; i < r0 - 32; i += bd - 32) y[i] -= panel_dot(Ucm + (size_t)r0 * K + i, K, pv, nb);
     }
-    __syncthreads();
   }
+  __syncthreads();
 }
 
 struct DenseTail {
