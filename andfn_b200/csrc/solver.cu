@@ -639,7 +639,7 @@ struct LevelSolve {
   const double *scale;  // [nslots] per-slot multiplier (1/U(i,i)) or null
   int nlev;
   int nslots;           // rows in this solve (rows[] has nslots, eptr[] nslots + 1 entries)
-  int group;            // lanes per row: 8, 16 or 32
+  int group;            // lanes per row: 4, 8, 16 or 32
 };
 
 static constexpr int PF = 4;  // factor entries per lane kept in registers
@@ -780,7 +780,9 @@ __device__ void level_solve_g(const LevelSolve &F, double *y, int *s_levptr, int
 
 __device__ void level_solve(const LevelSolve &F, double *y, int *s_levptr, int cap_levptr, int *s_meta,
                             int meta_cap) {
-  if (F.group == 8)
+  if (F.group == 4)
+    level_solve_g<4>(F, y, s_levptr, cap_levptr, s_meta, meta_cap);
+  else if (F.group == 8)
     level_solve_g<8>(F, y, s_levptr, cap_levptr, s_meta, meta_cap);
   else if (F.group == 16)
     level_solve_g<16>(F, y, s_levptr, cap_levptr, s_meta, meta_cap);
@@ -1416,6 +1418,21 @@ struct LevelParts {
 struct AdjBufs;
 static void destroy_adj(AdjBufs *a);
 
+// Power sums of the head-vector points: for every (discharge row side g =
+// 2 j + side, source element of that side's fracture with coefficients) pair,
+// S[x] = sign * sum over the side's D points of x^k (k < ncoef of the
+// source; x the source's 1/chi or chi).  They depend on the geometry and ncoef
+// only, so they are computed once per handle; the head vector is then
+// b = sum Re(coef * S) / D per row side, and its transpose reuses them.
+struct HeadSums {
+  DBuf<int> pair_g, pair_src, pair_off, src_ptr, src_pairs, gptr, sidx;
+  DBuf<cd> S;
+  int npairs = 0;
+  bool valid = false;
+  int mc = 0;
+  std::vector<int> ncoef;  // the ncoef the sums were computed for
+};
+
 }  // namespace andfn
 
 using namespace andfn;
@@ -1499,6 +1516,8 @@ struct AndfnHandle {
   bool adj_factors_ready = false;
   bool have_solution = false;
   AdjBufs *adj = nullptr;
+  HeadSums hs;
+  bool use_head_sums = false;
 
   Net net() const {
     Net n;
@@ -2161,9 +2180,16 @@ static void build_levels(int n, const std::vector<int> &ptr, const std::vector<i
 }
 
 // Lanes per factor row: the smallest group whose registers hold a mean row.
-static int group_for(const std::vector<int> &eptr) {
+// A single-level part (the coupling terms, independent rows) takes narrower
+// groups, so more rows are in flight at once.
+static int group_for(const std::vector<int> &eptr, bool single = false) {
   const int n = (int)eptr.size() - 1;
   const double mean = n > 0 ? (double)eptr[n] / n : 0.0;
+  if (single) {
+    if (mean <= 16.0 * PF) return 4;
+    if (mean <= 32.0 * PF) return 8;
+    return 16;
+  }
   if (mean <= 8.0 * PF) return 8;
   if (mean <= 16.0 * PF) return 16;
   return 32;
@@ -2239,7 +2265,7 @@ static int factor_all(AndfnHandle *H, const std::vector<double> &mv) {
       off[r][k] = {(int)P.lev.size(), (int)P.rows.size(), (int)P.col.size()};
       nlev[r][k] = (int)lev.size() - 1;
       nslots[r][k] = (int)rows.size();
-      grp[r][k] = group_for(eptr);
+      grp[r][k] = group_for(eptr, sp.single);
       H->max_nlev = std::max(H->max_nlev, nlev[r][k]);
       P.lev.insert(P.lev.end(), lev.begin(), lev.end());
       P.rows.insert(P.rows.end(), rows.begin(), rows.end());
@@ -2327,6 +2353,10 @@ static int factor_all(AndfnHandle *H, const std::vector<double> &mv) {
   return 0;
 }
 
+static int build_head_sums(AndfnHandle *H);
+__global__ void head_vector_kernel(Net net, const int *__restrict__ gptr, const int *__restrict__ sidx,
+                                   const cd *__restrict__ S);
+
 static void launch_trisolve(AndfnHandle *H, cudaStream_t s) {
   Net net = H->net();
   const size_t ybytes = sizeof(double) * (size_t)H->max_n;
@@ -2346,10 +2376,15 @@ static inline void mark(AndfnHandle *H, cudaStream_t s, int b, int c, int w) {
 static int enqueue_iteration(AndfnHandle *H, cudaStream_t s, int blend_mode, int b = -1) {
   Net net = H->net();
   mark(H, s, b, K_RHS, 0);
-  if (H->n_rhs_items > 0)
-    eval_kernel<true><<<H->n_rhs_items, EVAL_THREADS, H->eval_smem, s>>>(net, H->rhs_items.p, H->rhs_pts.p,
-                                                                          H->d_groups.p, H->rhs_vals.p, H->chunk);
-  rhs_reduce_kernel<<<(H->N * 32 + 255) / 256, 256, 0, s>>>(net, H->rhs_vals.p, H->rhs_group.p, H->d_groups.p);
+  if (H->use_head_sums) {
+    head_vector_kernel<<<(H->N * 32 + 255) / 256, 256, 0, s>>>(net, H->hs.gptr.p, H->hs.sidx.p, H->hs.S.p);
+  } else {
+    if (H->n_rhs_items > 0)
+      eval_kernel<true><<<H->n_rhs_items, EVAL_THREADS, H->eval_smem, s>>>(net, H->rhs_items.p, H->rhs_pts.p,
+                                                                            H->d_groups.p, H->rhs_vals.p, H->chunk);
+    rhs_reduce_kernel<<<(H->N * 32 + 255) / 256, 256, 0, s>>>(net, H->rhs_vals.p, H->rhs_group.p, H->d_groups.p);
+    H->launches += 1;
+  }
   mark(H, s, b, K_RHS, 1);
   mark(H, s, b, K_TRISOLVE, 0);
   launch_trisolve(H, s);
@@ -2369,7 +2404,7 @@ static int enqueue_iteration(AndfnHandle *H, cudaStream_t s, int blend_mode, int
   mark(H, s, b, K_REDUCE, 0);
   reduce_kernel<<<H->R, 1024, 0, s>>>(net);
   mark(H, s, b, K_REDUCE, 1);
-  H->launches += 6;
+  H->launches += 5;
   return 0;
 }
 
@@ -2536,6 +2571,13 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
   const int n_de = (int)H->h.de_ids.size();
   if (n_de > 0) zint_kernel<<<std::max(1, std::min(1184, (int)((n_de * H->D + 255) / 256))), 256, 0, s>>>(net);
   if (H->n_psi > 0) cuts_kernel<<<(H->n_psi * 32 + 127) / 128, 128, 0, s>>>(net, H->psi_list.p, H->n_psi);
+  // head vector from power sums, unless coefficients may grow
+  H->use_head_sums = false;
+  if (!growth_possible) {
+    int rch = build_head_sums(H);
+    if (rch) return rch;
+    H->use_head_sums = true;
+  }
   const long long nent = (long long)H->ent_row.size();
   if (nent > 0)
     matrix_values_kernel<<<(unsigned)((nent * 32 + 255) / 256), 256, 0, s>>>(
@@ -2581,14 +2623,15 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
       CK(cudaGraphInstantiate(&H->graph_exec, g, 0));
       cudaGraphDestroy(g);
     }
-    H->launches -= ITER_BATCH * 6;  // capture does not launch
+    const int per_it = H->use_head_sums ? 5 : 6;  // kernels of one captured iteration
+  H->launches -= ITER_BATCH * per_it;           // capture does not launch
     int guard = 0;
     int nit_before = 0;
     while (true) {
       CK(cudaGraphLaunch(H->graph_exec, s));
       CK(cudaMemcpyAsync(H->h_ndone, H->ndone.p, sizeof(int), cudaMemcpyDeviceToHost, s));
       CK(cudaStreamSynchronize(s));
-      H->launches += ITER_BATCH * 6;
+      H->launches += ITER_BATCH * per_it;
       if (H->profiling) {
         // only the iterations that did work (later ones return at entry)
         int rcs = read_states(H);
@@ -3260,12 +3303,7 @@ struct AdjBufs {
   DBuf<cd> V, xin, wv;  // Krylov basis [restart + 1][ne][MC], sweep input and output
   DBuf<Item> items_sw;
   int n_items_sw = 0;
-  // head-vector power sums: pairs (row side g = 2 j + side, source element)
-  DBuf<int> pair_g, pair_src, pair_off, src_ptr, src_pairs;
-  DBuf<cd> S;
   DBuf<double> fac;  // [2 n_de] weight of a row side per unit mu
-  int npairs = 0;
-  std::vector<int> sums_ncoef;  // ncoef the sums were computed for
   int chunk = 1;
   size_t smem = 0;
   // transposed factors
@@ -3610,6 +3648,41 @@ __global__ void rhs_sums_kernel(Net net, const int *__restrict__ pair_g, const i
   }
 }
 
+// Head vector from the power sums (replaces the evaluation of the head-vector
+// points): one warp per system row, b = (S1 / D) / t1 - (S0 / D) / t0 for an
+// intersection, phi - S0 / D for a constant-head line or well, 0 for a
+// continuity row, with S_side = sum over the side's pairs of Re(coef * S).
+__global__ void head_vector_kernel(Net net, const int *__restrict__ gptr, const int *__restrict__ sidx,
+                                   const cd *__restrict__ S) {
+  const int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (g >= net.N) return;
+  const SolveState *st = net.st + net.real_row[g];
+  if (st->done || !st->solve_q) return;
+  const int r = net.row_de[g];
+  if (r < 0) {
+    if (lane == 0) net.bvec[g] = 0.0;
+    return;
+  }
+  const int e = net.de_ids[r];
+  double sum[2] = {0.0, 0.0};
+  const int sides = (net.type[e] == 0) ? 2 : 1;
+  for (int sd = 0; sd < sides; sd++) {
+    double a = 0.0;
+    for (int x = gptr[2 * r + sd] + lane; x < gptr[2 * r + sd + 1]; x += 32) {
+      const cd c = net.coef[sidx[x]], v = S[x];
+      a = fma(c.re, v.re, fma(-c.im, v.im, a));
+    }
+    sum[sd] = warp_sum(a);
+  }
+  if (lane == 0) {
+    const double D = net.D;
+    if (sides == 2)
+      net.bvec[g] = (sum[1] / D) / net.t[net.frac1[e]] - (sum[0] / D) / net.t[net.frac0[e]];
+    else
+      net.bvec[g] = net.phi[e] - sum[0] / D;
+  }
+}
+
 __global__ void adj_rhs_gather_kernel(Net net, const int *__restrict__ src_ptr, const int *__restrict__ src_pairs,
                                       const int *__restrict__ pair_g, const int *__restrict__ pair_off,
                                       const cd *__restrict__ S, const double *__restrict__ mu,
@@ -3846,6 +3919,63 @@ static void adj_items(const std::vector<Group> &groups, const std::vector<int2> 
   }
 }
 
+// Builds the head-vector power sums for the current ncoef (once per handle;
+// again only if ncoef or the coefficient capacity changed).  Needs z_int.
+static int build_head_sums(AndfnHandle *H) {
+  HeadSums &hs = H->hs;
+  if (hs.valid && hs.ncoef == H->cur_ncoef && hs.mc == H->MC) return 0;
+  const HostNet &h = H->h;
+  const int ne = (int)H->ne, n_de = (int)h.de_ids.size(), MC = H->MC;
+  cudaStream_t s = H->stream;
+  std::vector<int> pg, ps, po, gptr(2 * (size_t)n_de + 1, 0), sidx;
+  std::vector<std::vector<int>> by_src(ne);
+  int off = 0;
+  for (int j = 0; j < n_de; j++) {
+    const int e = h.de_ids[j];
+    const int sides = (h.type[e] == 0) ? 2 : 1;
+    for (int sd = 0; sd < 2; sd++) {
+      gptr[2 * j + sd] = off;
+      if (sd >= sides) continue;
+      const int f = sd ? h.frac1[e] : h.frac0[e];
+      for (int k = h.fptr[f]; k < h.fptr[f + 1]; k++) {
+        const int el = h.felem[k];
+        const int m = H->cur_ncoef[el];
+        if (h.type[el] == 2 || m <= 0) continue;
+        by_src[el].push_back((int)pg.size());
+        pg.push_back(2 * j + sd);
+        ps.push_back(el);
+        po.push_back(off);
+        for (int jj = 0; jj < m; jj++) sidx.push_back(el * MC + jj);
+        off += m;
+      }
+    }
+  }
+  gptr[2 * (size_t)n_de] = off;
+  std::vector<int> sp(ne + 1, 0), spairs;
+  for (int el = 0; el < ne; el++) {
+    sp[el + 1] = sp[el] + (int)by_src[el].size();
+    spairs.insert(spairs.end(), by_src[el].begin(), by_src[el].end());
+  }
+  hs.npairs = (int)pg.size();
+  CK(upload(hs.gptr, gptr, s));
+  if (hs.npairs > 0) {
+    CK(upload(hs.pair_g, pg, s));
+    CK(upload(hs.pair_src, ps, s));
+    CK(upload(hs.pair_off, po, s));
+    CK(upload(hs.src_ptr, sp, s));
+    CK(upload(hs.src_pairs, spairs, s));
+    CK(upload(hs.sidx, sidx, s));
+    CK(hs.S.alloc(std::max(1, off)));
+    rhs_sums_kernel<<<(hs.npairs * 32 + 127) / 128, 128, 0, s>>>(H->net(), hs.pair_g.p, hs.pair_src.p,
+                                                                  hs.pair_off.p, hs.npairs, hs.S.p);
+    CK(cudaGetLastError());
+  }
+  hs.ncoef = H->cur_ncoef;
+  hs.mc = MC;
+  hs.valid = true;
+  return 0;
+}
+
 // Transposed factors of the last run's LU (P A Q = L U, so A^T = Q U^T L^T P):
 // the lower solve is U^T (rows scaled by 1/U(i,i)), the upper one L^T (unit);
 // the dense tail's lower part is (D^-1 U22)^T followed by D^-1, its upper
@@ -3892,7 +4022,7 @@ static int adj_build_factors(AndfnHandle *H) {
     else
       build_levels(n, lt_p, lt_c, lt_v, nullptr, false, rlo, rhi, clo, chi, k == 2, lev, rows, eptr, ecol, ev, esc);
     const int nslots = (int)rows.size();
-    const int group = group_for(eptr);
+    const int group = group_for(eptr, k == 1 || k == 2);
     rows.push_back(0);
     if (ecol.empty()) {
       ecol.push_back(0);
@@ -3983,9 +4113,9 @@ static void adj_enqueue_sweep(AndfnHandle *H, const Net &net, const Net &net_t, 
                                                                  A.wsw.p, A.gc.p, A.gq.p, A.gC.p, A.chunk, A.st.p);
   adj_rhs_kernel<<<(N + 255) / 256, 256, 0, s>>>(net, gd, A.gq.p, A.gC.p, A.b.p, A.st.p);
   launch_trisolve_adj(H, net_t, s);
-  if (A.npairs > 0)
-    adj_rhs_gather_kernel<<<ce, 256, 0, s>>>(net, A.src_ptr.p, A.src_pairs.p, A.pair_g.p, A.pair_off.p, A.S.p,
-                                             A.mu.p, A.fac.p, A.gc.p, A.st.p);
+  if (H->hs.npairs > 0)
+    adj_rhs_gather_kernel<<<ce, 256, 0, s>>>(net, H->hs.src_ptr.p, H->hs.src_pairs.p, H->hs.pair_g.p,
+                                             H->hs.pair_off.p, H->hs.S.p, A.mu.p, A.fac.p, A.gc.p, A.st.p);
   adj_combine_kernel<<<ce, 256, 0, s>>>(net, x, A.gc.p, A.gobj.p, y, mode);
 }
 
@@ -4038,47 +4168,9 @@ static int adjoint_impl(AndfnHandle *H, const double *gcoef, int64_t mco, const 
     }
     CK(cudaFuncSetAttribute(adj_sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
   }
-  // head-vector power sums (geometry and ncoef only: computed once per handle)
-  if (A.sums_ncoef != H->cur_ncoef) {
-    const HostNet &h = H->h;
-    std::vector<int> pg, ps, po;
-    std::vector<std::vector<int>> by_src(ne);
-    int off = 0;
-    for (int j = 0; j < n_de; j++) {
-      const int e = h.de_ids[j];
-      const int sides = (h.type[e] == 0) ? 2 : 1;
-      for (int sd = 0; sd < sides; sd++) {
-        const int f = sd ? h.frac1[e] : h.frac0[e];
-        for (int k = h.fptr[f]; k < h.fptr[f + 1]; k++) {
-          const int el = h.felem[k];
-          const int m = H->cur_ncoef[el];
-          if (h.type[el] == 2 || m <= 0) continue;
-          by_src[el].push_back((int)pg.size());
-          pg.push_back(2 * j + sd);
-          ps.push_back(el);
-          po.push_back(off);
-          off += m;
-        }
-      }
-    }
-    std::vector<int> sp(ne + 1, 0), spairs;
-    for (int el = 0; el < ne; el++) {
-      sp[el + 1] = sp[el] + (int)by_src[el].size();
-      spairs.insert(spairs.end(), by_src[el].begin(), by_src[el].end());
-    }
-    A.npairs = (int)pg.size();
-    if (A.npairs > 0) {
-      CK(upload(A.pair_g, pg, s));
-      CK(upload(A.pair_src, ps, s));
-      CK(upload(A.pair_off, po, s));
-      CK(upload(A.src_ptr, sp, s));
-      CK(upload(A.src_pairs, spairs, s));
-      CK(A.S.alloc(std::max(1, off)));
-      rhs_sums_kernel<<<(A.npairs * 32 + 127) / 128, 128, 0, s>>>(H->net(), A.pair_g.p, A.pair_src.p,
-                                                                   A.pair_off.p, A.npairs, A.S.p);
-      CK(cudaGetLastError());
-    }
-    A.sums_ncoef = H->cur_ncoef;
+  {
+    int rcs = build_head_sums(H);
+    if (rcs) return rcs;
   }
   {
     // row-side weights per unit mu (t may have changed since the sums)
