@@ -8,7 +8,7 @@ from __future__ import annotations
 import ctypes
 import os
 
-from .records import AndfnAdjointStats, AndfnConstants, AndfnLayout, AndfnSolveStats
+from .records import AndfnAdjointStats, AndfnConstants, AndfnLayout, AndfnResidual, AndfnSolveStats
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libandfn_b200.so")
@@ -20,7 +20,8 @@ EXPORTS = ("andfn_b200_solve", "andfn_b200_create", "andfn_b200_upload_state", "
            "andfn_b200_batch_solve", "andfn_b200_batch_create", "andfn_b200_batch_run",
            "andfn_b200_batch_download", "andfn_b200_batch_eval_heads", "andfn_b200_realizations",
            "andfn_b200_eval_heads_noalloc", "andfn_b200_adjoint", "andfn_b200_set_transmissivity",
-           "andfn_b200_state_device", "andfn_b200_heads_device", "andfn_b200_heads_vjp")
+           "andfn_b200_state_device", "andfn_b200_heads_device", "andfn_b200_heads_vjp",
+           "andfn_b200_bc_residual")
 
 STATUS = {0: "ok", 1: "max_iterations", 2: "nonfinite", 3: "singular", 10: "bad_layout", 11: "bad_input",
           12: "cuda_error", 13: "no_device", 14: "out_of_memory"}
@@ -75,6 +76,7 @@ def lib() -> ctypes.CDLL:
         ("andfn_b200_state_device", ctypes.c_int, [P, P, I64, P, P]),
         ("andfn_b200_heads_device", ctypes.c_int, [P, P, P, I64, P]),
         ("andfn_b200_heads_vjp", ctypes.c_int, [P, P, P, I64, P, P, I64, P, P, P]),
+        ("andfn_b200_bc_residual", ctypes.c_int, [P, P, P, ctypes.POINTER(AndfnResidual)]),
     ):
         fn = getattr(L, name)
         fn.restype = res

@@ -4498,3 +4498,141 @@ int andfn_b200_adjoint(AndfnHandle *H, const double *gcoef, int64_t mco, const d
 }
 
 }  // extern "C"
+
+// ==========================================================================
+// Boundary-condition residual and flux balance of the current state (no
+// reference counterpart for the residual; the flux balance is
+// Fracture.check_discharge, andfn/fracture.py:377-394).
+//   intersection:   max_k |h0(z_k) - h1(z_k)| / h_scale at its collocation
+//                   points (h = Re Omega_f / t_f, both sides)
+//   constant head:  max_k |h(z_k) - head| / h_scale
+//   well:           max over 16 points on its circle of |h - head| / h_scale
+//   bounding circle, impermeable circle / line: (max_k - min_k) psi'_k /
+//                   q_scale, psi' the stream function unwrapped across the
+//                   branch cuts (the no-flow condition makes it constant)
+// h_scale = max |head| of the constant-head lines and wells (1 if none);
+// q_scale = the largest total |q| of a fracture's discharge elements
+// (get_total_discharge, andfn/fracture.py:365-375), the network's flow scale.
+// ==========================================================================
+namespace andfn {
+
+__global__ void bc_residual_kernel(Net net, double hscale, double qscale, double *res) {
+  const int e = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (e >= net.ne) return;
+  const int type = net.type[e];
+  const int f0 = net.frac0[e];
+  double r = 0.0;
+  if (type == 0 || type == 3) {
+    const int n = net.nint[e];
+    const double t0 = net.t[f0];
+    const double head = (type == 3) ? net.phi[e] / t0 : 0.0;
+    for (int k = lane; k < n; k += 32) {
+      const double h0 = omega_at(net, f0, sweep_point(net, e, 0, k)).re / t0;
+      double d;
+      if (type == 0) {
+        const int f1 = net.frac1[e];
+        d = h0 - omega_at(net, f1, sweep_point(net, e, 1, k)).re / net.t[f1];
+      } else {
+        d = h0 - head;
+      }
+      r = fmax(r, fabs(d) / hscale);
+    }
+  } else if (type == 2) {
+    const double t0 = net.t[f0], head = net.phi[e] / t0;
+    if (lane < 16) {
+      double sn, cs;
+      sincos(2 * PI * lane / 16, &sn, &cs);
+      const cd z = mk(net.center[e].re + net.radius[e] * cs, net.center[e].im + net.radius[e] * sn);
+      r = fabs(omega_at(net, f0, z).re / t0 - head) / hscale;
+    }
+  } else {
+    const int n = net.nint[e];
+    const int nc = net.cut_n[e];
+    const int *cp = net.cut_pos + (size_t)e * net.cut_cap;
+    const int *ce = net.cut_elem + (size_t)e * net.cut_cap;
+    const int *cs = net.cut_sign + (size_t)e * net.cut_cap;
+    double mx = -INFINITY, mn = INFINITY;
+    for (int k = lane; k < n; k += 32) {
+      double cum = 0.0;
+      for (int c = 0; c < nc; c++)
+        if (cp[c] < k) cum += net.q[ce[c]] * (double)cs[c];
+      const double psi = omega_at(net, f0, sweep_point(net, e, 0, k)).im - cum;
+      mx = fmax(mx, psi);
+      mn = fmin(mn, psi);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+      mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+    }
+    r = (mx >= mn) ? (mx - mn) / qscale : 0.0;
+  }
+  for (int o = 16; o > 0; o >>= 1) r = fmax(r, __shfl_xor_sync(0xffffffffu, r, o));
+  if (lane == 0) res[e] = r;
+}
+
+}  // namespace andfn
+
+extern "C" int andfn_b200_bc_residual(AndfnHandle *H, double *elem_res, double *frac_flux, AndfnResidual *out) {
+  if (!H || !out) return ANDFN_BAD_INPUT;
+  if (H->R != 1) {
+    set_error("bc_residual needs a single-network handle");
+    return ANDFN_BAD_INPUT;
+  }
+  CK(cudaSetDevice(H->device));
+  const HostNet &h = H->h;
+  const int ne = (int)H->ne, nf = (int)H->nf;
+  cudaStream_t s = H->stream;
+  std::vector<double> tt(nf), phi(ne), q(ne);
+  CK(cudaMemcpyAsync(tt.data(), H->t.p, sizeof(double) * nf, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(phi.data(), H->phi.p, sizeof(double) * ne, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(q.data(), H->q.p, sizeof(double) * ne, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  double hscale = 0.0;
+  for (int e = 0; e < ne; e++)
+    if (h.type[e] == 2 || h.type[e] == 3) hscale = std::max(hscale, std::fabs(phi[e] / tt[h.frac0[e]]));
+  if (!(hscale > 0.0)) hscale = 1.0;
+  // flow scale and the per-fracture balance (check_discharge,
+  // andfn/fracture.py:377-394)
+  std::vector<double> fsum(nf, 0.0), ftot(nf, 0.0);
+  double qscale = 0.0;
+  for (int f = 0; f < nf; f++) {
+    for (int k = h.fptr[f]; k < h.fptr[f + 1]; k++) {
+      const int el = h.felem[k], ty = h.type[el];
+      if (ty != 0 && ty != 2 && ty != 3) continue;
+      fsum[f] += (ty == 0 && h.frac1[el] == f) ? -q[el] : q[el];
+      ftot[f] += std::fabs(q[el]);
+    }
+    qscale = std::max(qscale, ftot[f]);
+  }
+  if (!(qscale > 0.0)) qscale = 1.0;
+  DBuf<double> dres;
+  CK(dres.alloc(ne));
+  // branch cuts of the current nint (also valid for a handle that has not run)
+  if (H->n_psi > 0) cuts_kernel<<<(H->n_psi * 32 + 127) / 128, 128, 0, s>>>(H->net(), H->psi_list.p, H->n_psi);
+  bc_residual_kernel<<<(ne * 32 + 127) / 128, 128, 0, s>>>(H->net(), hscale, qscale, dres.p);
+  CK(cudaGetLastError());
+  std::vector<double> res(ne);
+  CK(cudaMemcpyAsync(res.data(), dres.p, sizeof(double) * ne, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  std::memset(out, 0, sizeof(*out));
+  out->h_scale = hscale;
+  out->bc_worst = -1;
+  for (int e = 0; e < ne; e++)
+    if (!(res[e] <= out->bc_max)) {  // NaN propagates
+      out->bc_max = res[e];
+      out->bc_worst = e;
+      if (!(res[e] == res[e])) break;
+    }
+  out->q_scale = qscale;
+  out->flux_worst = -1;
+  for (int f = 0; f < nf; f++) {
+    const double rel = std::fabs(fsum[f]) / qscale;
+    if (frac_flux) frac_flux[f] = std::fabs(fsum[f]);
+    if (rel > out->flux_max) {
+      out->flux_max = rel;
+      out->flux_worst = f;
+    }
+  }
+  if (elem_res) std::memcpy(elem_res, res.data(), sizeof(double) * ne);
+  return 0;
+}

@@ -108,6 +108,14 @@ class AndfnAdjointStats(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_ if name != "pad"}
 
 
+class AndfnResidual(ctypes.Structure):
+    _fields_ = [("bc_max", ctypes.c_double), ("bc_worst", ctypes.c_int64), ("flux_max", ctypes.c_double),
+                ("flux_worst", ctypes.c_int64), ("h_scale", ctypes.c_double), ("q_scale", ctypes.c_double)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 _INT_FIELDS = ("_id", "_type", "frac0", "frac1", "ncoef", "nint")
 
 

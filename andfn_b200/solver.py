@@ -109,6 +109,20 @@ class Solver:
                                                            out.ctypes.data_as(ctypes.c_void_p)))
         return out
 
+    def bc_residual(self) -> dict:
+        """Boundary-condition residual per element and flux balance per
+        fracture of the current state (include/andfn_b200.h)."""
+        from .records import AndfnResidual
+        res = np.empty(len(self.elements))
+        flux = np.empty(len(self.fractures))
+        out = AndfnResidual()
+        _ffi.check(_ffi.lib().andfn_b200_bc_residual(self._h, res.ctypes.data_as(ctypes.c_void_p),
+                                                    flux.ctypes.data_as(ctypes.c_void_p), ctypes.byref(out)))
+        d = out.as_dict()
+        d["elem"] = res
+        d["flux"] = flux
+        return d
+
     def eval_omega(self, frac_idx, z) -> np.ndarray:
         """Omega_f(z) (andfn/hpc/hpc_fracture.py:52-94)."""
         frac_idx = np.ascontiguousarray(frac_idx, np.int64)

@@ -257,6 +257,28 @@ int andfn_b200_heads_vjp(AndfnHandle *h, const int64_t *frac, const double *z,
                          int64_t npts, const double *gh, double *gcoef,
                          int64_t mco, double *gq, double *gC, double *glogt);
 
+/* ---- boundary-condition residual and flux balance -----------------------
+ * Of the handle's current state (single network; after run() or download()).
+ * Per element, the relative boundary-condition error at its collocation
+ * points (no reference counterpart): intersections |h0 - h1|, constant-head
+ * lines and wells |h - head|, both over h_scale = max |prescribed head|;
+ * bounding circles and impermeable elements the spread of the stream
+ * function unwrapped across branch cuts, over q_scale = the largest total
+ * |q| of a fracture (get_total_discharge, andfn/fracture.py:365-375).  Per
+ * fracture, |sum of signed discharges| as Fracture.check_discharge
+ * (andfn/fracture.py:377-394); the summary gives its maximum over q_scale.
+ * elem_res [ne] and frac_flux [nf] are host arrays or NULL. */
+typedef struct {
+  double bc_max;        /* max element residual                 */
+  int64_t bc_worst;     /* its element                          */
+  double flux_max;      /* max flux imbalance / q_scale         */
+  int64_t flux_worst;   /* its fracture                         */
+  double h_scale;       /* head scale of the residual           */
+  double q_scale;       /* discharge scale                      */
+} AndfnResidual;
+int andfn_b200_bc_residual(AndfnHandle *h, double *elem_res, double *frac_flux,
+                           AndfnResidual *out);
+
 /* Thread-local text of the last error. */
 const char *andfn_b200_last_error(void);
 /* Library version string. */

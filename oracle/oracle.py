@@ -302,3 +302,72 @@ def num_threads() -> int:
 if __name__ == "__main__":
     print(build(force=True))
     print("threads", num_threads(), "scipy", scipy_version(), "pid", os.getpid())
+
+
+# --- boundary-condition residual and flux balance (test/report restatement) ---
+def collocation_points(elements, e, side=0):
+    """The element's collocation points: z = map_chi_to_z(exp(i theta_k))
+    (andfn/hpc/hpc_math_functions.py:279-284, 674-699)."""
+    E = elements
+    ty, n = int(E["_type"][e]), int(E["nint"][e])
+    k = np.arange(n)
+    th = 2 * np.pi * k / n if ty == 1 else (k + 0.5) * np.pi / n
+    chi = np.exp(1j * th)
+    if ty in (1, 4):
+        return E["radius"][e] * chi + E["center"][e]
+    ep = E["endpoints1"][e] if side else E["endpoints0"][e]
+    a, b = ep[0], ep[1]
+    return 0.5 * (0.5 * (chi + 1 / chi) * (b - a) + a + b)
+
+
+def bc_residual(fractures, elements):
+    """Per-element boundary-condition residual and per-fracture flux balance
+    of a solved state, as andfn_b200_bc_residual defines them (the flux
+    balance is Fracture.check_discharge, andfn/fracture.py:377-394)."""
+    F, E = fractures, elements
+    ty = E["_type"]
+    t = F["t"]
+    heads = np.abs(E["phi"] / t[E["frac0"]])[np.isin(ty, (2, 3))]
+    hs = heads.max() if len(heads) and heads.max() > 0 else 1.0
+    ne = len(E)
+    res = np.zeros(ne)
+    disch = np.isin(ty, (0, 2, 3))
+    flux = np.zeros(len(F))
+    ftot = np.zeros(len(F))
+    for f in range(len(F)):
+        els = F["elements"][f, : F["nelements"][f]]
+        s = tot = 0.0
+        for el in els:
+            if not disch[el]:
+                continue
+            s += -E["q"][el] if (ty[el] == 0 and E["frac1"][el] == f) else E["q"][el]
+            tot += abs(E["q"][el])
+        flux[f] = abs(s)
+        ftot[f] = tot
+    qs = ftot.max() if len(ftot) and ftot.max() > 0 else 1.0
+    for e in range(ne):
+        f0 = int(E["frac0"][e])
+        if ty[e] in (0, 3):
+            z0 = collocation_points(E, e, 0)
+            h0 = eval_omega(F, E, np.full(len(z0), f0), z0).real / t[f0]
+            if ty[e] == 0:
+                f1 = int(E["frac1"][e])
+                z1 = collocation_points(E, e, 1)
+                h1 = eval_omega(F, E, np.full(len(z1), f1), z1).real / t[f1]
+                d = h0 - h1
+            else:
+                d = h0 - E["phi"][e] / t[f0]
+            res[e] = np.abs(d).max() / hs if len(d) else 0.0
+        elif ty[e] == 2:
+            z = E["center"][e] + E["radius"][e] * np.exp(2j * np.pi * np.arange(16) / 16)
+            h = eval_omega(F, E, np.full(16, f0), z).real / t[f0]
+            res[e] = np.abs(h - E["phi"][e] / t[f0]).max() / hs
+        else:
+            z = collocation_points(E, e, 0)
+            n = len(z)
+            psi = eval_omega(F, E, np.full(n, f0), z).imag
+            corr = np.concatenate([[0.0], np.cumsum(E["dpsi_corr"][e][: n - 1])])
+            psi = psi - corr
+            res[e] = (psi.max() - psi.min()) / qs
+    return {"elem": res, "flux": flux, "h_scale": hs, "q_scale": qs, "bc_max": float(res.max()),
+            "flux_max": float(flux.max() / qs)}
