@@ -752,6 +752,19 @@ __device__ void level_solve_g(const LevelSolve &F, double *y, int *s_levptr, int
     hb = lp[1] + gid < lp[2];
     load_row<G>(b, F, M, lp[1] + gid, hb, sub);
   }
+  // A level with at most 32 / G rows is solved by warp 0 alone (rows go to
+  // groups in order); between two such levels a warp barrier suffices, and the
+  // other warps run ahead to the next block barrier.  The condition depends on
+  // the level pointers only, so every thread takes the same barriers.
+  constexpr int WG = 32 / G;
+  auto level_sync = [&](int l) {
+    const bool small = lp[l + 1] - lp[l] <= WG;
+    const bool small_next = l + 1 < F.nlev && lp[l + 2] - lp[l + 1] <= WG;
+    if (small && small_next)
+      __syncwarp();
+    else
+      __syncthreads();
+  };
   for (int l = 0; l < F.nlev; l += 2) {
     {
       const int r0 = lp[l], r1 = lp[l + 1];
@@ -762,7 +775,7 @@ __device__ void level_solve_g(const LevelSolve &F, double *y, int *s_levptr, int
         ha = lp[l + 2] + gid < lp[l + 3];
         load_row<G>(a, F, M, lp[l + 2] + gid, ha, sub);
       }
-      __syncthreads();
+      level_sync(l);
     }
     if (l + 1 < F.nlev) {
       const int r0 = lp[l + 1], r1 = lp[l + 2];
@@ -773,13 +786,171 @@ __device__ void level_solve_g(const LevelSolve &F, double *y, int *s_levptr, int
         hb = lp[l + 3] + gid < lp[l + 4];
         load_row<G>(b, F, M, lp[l + 3] + gid, hb, sub);
       }
-      __syncthreads();
+      level_sync(l + 1);
     }
   }
 }
 
+static constexpr int RING_SLOTS = 4;  // staged levels in flight + 1 (see level_solve_staged)
+
+// Byte offsets into the dynamic shared memory of the trisolve kernel (y at 0).
+struct Ring {
+  int levptr_off, meta_off, meta_cap;
+  int val_off, scale_off, col_off;  // [RING_SLOTS][cap] values, [RING_SLOTS][rcap] scales, [RING_SLOTS][cap] columns
+  int cap, rcap;
+};
+
+__device__ __forceinline__ void cp_async4(void *dst, const void *src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *dst, const void *src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Copies level l's entries (and row scales) into ring slot l % RING_SLOTS
+// when they fit; called by the staging threads (warps 1 and up), each of which
+// commits one group per call.
+__device__ __forceinline__ void stage_level(const LevelSolve &F, const int *lp, const int *meptr, int l,
+                                            const Ring &R, unsigned char *smem, int t, int nt) {
+  if (l < F.nlev) {
+    const int s0 = lp[l], s1 = lp[l + 1];
+    const int e0 = meptr[s0], e1 = meptr[s1];
+    if (e1 - e0 <= R.cap && s1 - s0 <= R.rcap) {
+      const int slot = l % RING_SLOTS;
+      int *dc = reinterpret_cast<int *>(smem + R.col_off) + slot * R.cap;
+      double *dv = reinterpret_cast<double *>(smem + R.val_off) + slot * R.cap;
+      for (int i = t; i < e1 - e0; i += nt) {
+        cp_async4(dc + i, F.col + e0 + i);
+        cp_async8(dv + i, F.val + e0 + i);
+      }
+      if (F.scale) {
+        double *ds = reinterpret_cast<double *>(smem + R.scale_off) + slot * R.rcap;
+        for (int i = t; i < s1 - s0; i += nt) cp_async8(ds + i, F.scale + s0 + i);
+      }
+    }
+  }
+  cp_async_commit();
+}
+
+// The rows of one level: groups of G lanes, one row per group and pass; the
+// pass count depends on the level only, so the shuffles stay converged.
+// Column/value/scale pointers are indexed by entry / slot position; the row's
+// own value and scale are loaded before its entries, off the critical path.
+// STAGED (the pointers are shared memory) and !STAGED (global) are separate
+// instantiations so that each has one address space.
+template <int G, bool STAGED>
+__device__ __forceinline__ void solve_level_rows(double *y, const int *mrows, const int *meptr, int s0, int s1,
+                                                 const int *cc, const double *vv, const double *sc) {
+  const int lane = threadIdx.x & 31, sub = lane % G;
+  const int gid = threadIdx.x / G, ng = blockDim.x / G;
+  for (int base = s0; base < s1; base += ng) {
+    const int r = base + gid;
+    const bool valid = r < s1;
+    int row = 0, beg = 0, end = 0;
+    if (valid) {
+      row = mrows[r];
+      beg = meptr[r];
+      end = meptr[r + 1];
+    }
+    const double yr = (valid && sub == 0) ? y[row] : 0.0;
+    const double scl = (valid && sub == 0 && sc) ? sc[r] : 1.0;
+    double a0 = 0.0, a1 = 0.0;
+    int p = beg + sub;
+    for (; p + G < end; p += 2 * G) {
+      a0 = fma(vv[p], y[cc[p]], a0);
+      a1 = fma(vv[p + G], y[cc[p + G]], a1);
+    }
+    if (p < end) a0 = fma(vv[p], y[cc[p]], a0);
+    double acc = a0 + a1;
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (valid && sub == 0) y[row] = (yr - acc) * scl;
+  }
+}
+
+// Lanes per row for a level of nrows rows: as many as keep the level to one
+// pass of the row warps (the warps below the staging warps; rows go to groups
+// in order, so a level that fits stays off the staging warps), at least 4.
+template <bool STAGED>
+__device__ __forceinline__ void solve_level_any(double *y, const int *mrows, const int *meptr, int s0, int s1,
+                                                const int *cc, const double *vv, const double *sc, int nw) {
+  const int nr = s1 - s0;
+  if (nr <= nw)
+    solve_level_rows<32, STAGED>(y, mrows, meptr, s0, s1, cc, vv, sc);
+  else if (nr <= 2 * nw)
+    solve_level_rows<16, STAGED>(y, mrows, meptr, s0, s1, cc, vv, sc);
+  else if (nr <= 4 * nw)
+    solve_level_rows<8, STAGED>(y, mrows, meptr, s0, s1, cc, vv, sc);
+  else
+    solve_level_rows<4, STAGED>(y, mrows, meptr, s0, s1, cc, vv, sc);
+}
+
+// Staged level solve.  A deep level has few rows, so its cost is the latency
+// of fetching its factor entries; here the entries (and row scales) of the
+// next RING_SLOTS - 1 levels are copied into a shared-memory ring with
+// asynchronous copies (cp.async) by warps 1 and up while the current level is
+// solved, and a level reads only shared memory on its critical path (y, the
+// slot metadata and the ring all live in the kernel's shared memory, so the
+// loads are shared-space loads).  The copies are issued by the last warps,
+// which small levels' rows do not reach.  Levels larger than the ring's capacity read global
+// memory directly.
+__device__ void level_solve_staged(const LevelSolve &F, const Ring &R) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double *y = reinterpret_cast<double *>(smem_raw);
+  const int *lp = reinterpret_cast<const int *>(smem_raw + R.levptr_off);
+  const int *mrows = reinterpret_cast<const int *>(smem_raw + R.meta_off);
+  const int *meptr = mrows + R.meta_cap;
+  // the last STAGE_WARPS warps copy; the others solve the rows of small levels
+  const int nwarps = blockDim.x >> 5;
+  const int nst = nwarps >= 8 ? 4 : 1;
+  const int nrow_w = nwarps - nst;
+  const bool stager = (int)(threadIdx.x >> 5) >= nrow_w;
+  const int t = threadIdx.x - nrow_w * 32, nt = nst * 32;
+  if (stager) {
+    for (int l = 0; l < RING_SLOTS - 1; l++) stage_level(F, lp, meptr, l, R, smem_raw, t, nt);
+    cp_async_wait<RING_SLOTS - 2>();
+  }
+  __syncthreads();
+  for (int l = 0; l < F.nlev; l++) {
+    if (stager) stage_level(F, lp, meptr, l + RING_SLOTS - 1, R, smem_raw, t, nt);  // slot of level l - 1
+    const int s0 = lp[l], s1 = lp[l + 1];
+    const int e0 = meptr[s0], e1 = meptr[s1];
+    if (e1 - e0 <= R.cap && s1 - s0 <= R.rcap) {
+      const int slot = l % RING_SLOTS;
+      const int *cc = reinterpret_cast<const int *>(smem_raw + R.col_off) + slot * R.cap - e0;
+      const double *vv = reinterpret_cast<const double *>(smem_raw + R.val_off) + slot * R.cap - e0;
+      const double *sc =
+          F.scale ? reinterpret_cast<const double *>(smem_raw + R.scale_off) + slot * R.rcap - s0 : nullptr;
+      solve_level_any<true>(y, mrows, meptr, s0, s1, cc, vv, sc, nrow_w);
+    } else {
+      solve_level_any<false>(y, mrows, meptr, s0, s1, F.col, F.val, F.scale, nrow_w);
+    }
+    if (stager) cp_async_wait<RING_SLOTS - 2>();  // level l + 1's slot is complete
+    __syncthreads();
+  }
+  if (stager) cp_async_wait<0>();
+}
+
 __device__ void level_solve(const LevelSolve &F, double *y, int *s_levptr, int cap_levptr, int *s_meta,
-                            int meta_cap) {
+                            int meta_cap, const Ring &R) {
+  const bool lev_in_smem = F.nlev + 1 <= cap_levptr;
+  const bool meta_in_smem = F.nslots + 1 <= meta_cap;
+  if (R.cap > 0 && lev_in_smem && meta_in_smem && blockDim.x >= 64) {
+    __syncthreads();
+    for (int i = threadIdx.x; i <= F.nlev; i += blockDim.x) s_levptr[i] = F.lev_ptr[i];
+    for (int i = threadIdx.x; i < F.nslots; i += blockDim.x) s_meta[i] = F.rows[i];
+    for (int i = threadIdx.x; i <= F.nslots; i += blockDim.x) s_meta[meta_cap + i] = F.eptr[i];
+    __syncthreads();
+    level_solve_staged(F, R);
+    return;
+  }
   if (F.group == 4)
     level_solve_g<4>(F, y, s_levptr, cap_levptr, s_meta, meta_cap);
   else if (F.group == 8)
@@ -945,8 +1116,8 @@ struct TriDesc {
 // ADJ: the transposed solve of the adjoint (the factor parts passed in
 // net.tri are those of A^T): reads net.bvec, writes net.disc only.
 template <bool ADJ>
-__global__ void __launch_bounds__(SOLVE_THREADS) trisolve_kernel(Net net, int use_smem, int cap_levptr,
-                                                                  int meta_cap) {
+__global__ void __launch_bounds__(SOLVE_THREADS, 1) trisolve_kernel(Net net, int use_smem, int cap_levptr,
+                                                                     int meta_cap, int ring_cap) {
   const int r = blockIdx.x;
   SolveState *st = net.st + r;
   if (st->done) return;
@@ -958,6 +1129,21 @@ __global__ void __launch_bounds__(SOLVE_THREADS) trisolve_kernel(Net net, int us
   double *y = use_smem ? reinterpret_cast<double *>(smem_raw) : net.work + row0;
   int *s_levptr = reinterpret_cast<int *>(smem_raw + sizeof(double) * ycap);
   int *s_meta = s_levptr + cap_levptr;
+  // factor-entry ring after the slot metadata (16-byte aligned); the staged
+  // path needs y, the level pointers and the metadata in shared memory
+  Ring ring{0, 0, 0, 0, 0, 0, 0, 0};
+  if (ring_cap > 0 && use_smem) {
+    const int off =
+        (int)((sizeof(double) * ycap + sizeof(int) * ((size_t)cap_levptr + 2 * (size_t)meta_cap) + 15) & ~(size_t)15);
+    ring.levptr_off = (int)(sizeof(double) * ycap);
+    ring.meta_off = ring.levptr_off + (int)sizeof(int) * cap_levptr;
+    ring.meta_cap = meta_cap;
+    ring.val_off = off;
+    ring.scale_off = off + (int)sizeof(double) * RING_SLOTS * ring_cap;
+    ring.col_off = ring.scale_off + (int)sizeof(double) * RING_SLOTS * (ring_cap / 2);
+    ring.cap = ring_cap;
+    ring.rcap = ring_cap / 2;
+  }
   if (!ADJ) {
     if (threadIdx.x == 0) st->nit += 1;
     if (!st->solve_q) return;  // uniform: solve_q is written only by reduce_kernel
@@ -975,10 +1161,10 @@ __global__ void __launch_bounds__(SOLVE_THREADS) trisolve_kernel(Net net, int us
   for (int i = threadIdx.x; i < N; i += blockDim.x) y[TD.pinv[i]] = net.bvec[row0 + i];
   phase(0);
   // L: sparse leading rows, coupling of the trailing rows to them, dense tail
-  level_solve(TD.Lf, y, s_levptr, cap_levptr, s_meta, meta_cap);
+  level_solve(TD.Lf, y, s_levptr, cap_levptr, s_meta, meta_cap, ring);
   phase(1);
   if (TD.T.K > 0) {
-    level_solve(TD.Lx, y, s_levptr, cap_levptr, s_meta, meta_cap);
+    level_solve(TD.Lx, y, s_levptr, cap_levptr, s_meta, meta_cap, ring);
     phase(2);
     dense_lower_solve(TD.T.L, TD.T.K, y + (N - TD.T.K));
     if (TD.T.lscale) {
@@ -989,10 +1175,10 @@ __global__ void __launch_bounds__(SOLVE_THREADS) trisolve_kernel(Net net, int us
     // U: dense tail, coupling of the leading rows to it, sparse leading rows
     dense_upper_solve(TD.T.U, TD.T.uinv, TD.T.K, y + (N - TD.T.K));
     phase(4);
-    level_solve(TD.Ux, y, s_levptr, cap_levptr, s_meta, meta_cap);
+    level_solve(TD.Ux, y, s_levptr, cap_levptr, s_meta, meta_cap, ring);
     phase(5);
   }
-  level_solve(TD.Ub, y, s_levptr, cap_levptr, s_meta, meta_cap);  // scale = 1/U(i,i)
+  level_solve(TD.Ub, y, s_levptr, cap_levptr, s_meta, meta_cap, ring);  // scale = 1/U(i,i)
   phase(6);
   // x = Q y; error_q = max|x - x_old| / (max|x_old| + 1e-16) (hpc_solve.py:169-174)
   __shared__ double s_d[32], s_o[32];
@@ -2353,6 +2539,25 @@ static int factor_all(AndfnHandle *H, const std::vector<double> &mv) {
   return 0;
 }
 
+// Factor-entry ring of the staged level solve: entries per slot (even), from
+// the shared memory left under 200 KB; 0 (unstaged path) when y or the slot
+// metadata are not in shared memory.
+static size_t ring_bytes(int cap) {
+  return (size_t)RING_SLOTS * (sizeof(double) * cap + sizeof(double) * (cap / 2) + sizeof(int) * cap);
+}
+static int ring_capacity(size_t used, int use_smem, int meta_cap) {
+  if (!use_smem || !meta_cap) return 0;
+  const size_t budget = 190 * 1024;
+  const size_t base = (used + 15) & ~(size_t)15;
+  if (base >= budget) return 0;
+  // per entry: value and column in every slot, a row scale per two entries
+  const size_t per_entry = (size_t)RING_SLOTS * (sizeof(double) + sizeof(int) + sizeof(double) / 2);
+  int cap = (int)((budget - base) / per_entry) & ~1;
+  cap = std::min(cap, 2048);
+  if (cap < 64 || base + ring_bytes(cap) > budget) return 0;
+  return cap;
+}
+
 static int build_head_sums(AndfnHandle *H);
 __global__ void head_vector_kernel(Net net, const int *__restrict__ gptr, const int *__restrict__ sidx,
                                    const cd *__restrict__ S);
@@ -2366,7 +2571,13 @@ static void launch_trisolve(AndfnHandle *H, cudaStream_t s) {
   const size_t meta_bytes = sizeof(int) * 2 * ((size_t)H->max_n + 1);
   const int meta_cap = (solve_smem + meta_bytes <= 200 * 1024) ? H->max_n + 1 : 0;
   if (meta_cap) solve_smem += meta_bytes;
-  trisolve_kernel<false><<<H->R, H->solve_threads, solve_smem, s>>>(net, use_smem, cap_levptr, meta_cap);
+  const int ring_cap = ring_capacity(solve_smem, use_smem, meta_cap);
+  if (ring_cap) solve_smem = ((solve_smem + 15) & ~(size_t)15) + ring_bytes(ring_cap);
+  trisolve_kernel<false><<<H->R, H->solve_threads, solve_smem, s>>>(net, use_smem, cap_levptr, meta_cap, ring_cap);
+  const cudaError_t le = cudaGetLastError();
+  if (le != cudaSuccess)
+    set_error(std::string("trisolve_kernel launch (shared memory ") + std::to_string(solve_smem) +
+              " B, ring " + std::to_string(ring_cap) + "): " + cudaGetErrorString(le));
 }
 
 static inline void mark(AndfnHandle *H, cudaStream_t s, int b, int c, int w) {
@@ -2619,7 +2830,13 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
             for (auto &e : c) CK(cudaEventCreate(&e));
       CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
       for (int b = 0; b < ITER_BATCH; b++) enqueue_iteration(H, s, 0, b);
-      CK(cudaStreamEndCapture(s, &g));
+      {
+        const cudaError_t ec = cudaStreamEndCapture(s, &g);
+        if (ec != cudaSuccess) {
+          set_error(std::string("capture of the iteration graph: ") + cudaGetErrorString(ec) + "; " + g_last_error);
+          return ANDFN_CUDA_ERROR;
+        }
+      }
       CK(cudaGraphInstantiate(&H->graph_exec, g, 0));
       cudaGraphDestroy(g);
     }
@@ -4090,7 +4307,9 @@ static void launch_trisolve_adj(AndfnHandle *H, const Net &net, cudaStream_t s) 
   const size_t meta_bytes = sizeof(int) * 2 * ((size_t)H->max_n + 1);
   const int meta_cap = (solve_smem + meta_bytes <= 200 * 1024) ? H->max_n + 1 : 0;
   if (meta_cap) solve_smem += meta_bytes;
-  trisolve_kernel<true><<<1, H->solve_threads, solve_smem, s>>>(net, use_smem, cap_levptr, meta_cap);
+  const int ring_cap = ring_capacity(solve_smem, use_smem, meta_cap);
+  if (ring_cap) solve_smem = ((solve_smem + 15) & ~(size_t)15) + ring_bytes(ring_cap);
+  trisolve_kernel<true><<<1, H->solve_threads, solve_smem, s>>>(net, use_smem, cap_levptr, meta_cap, ring_cap);
 }
 
 static constexpr int ADJ_SWEEP_LAUNCHES = 9;  // per transposed sweep (3 memsets + 6 kernels)
