@@ -448,3 +448,44 @@ def batch_realization(seed, L=40.0, nf_range=(200, 800), wells=4, ncoef=15, nint
     net = power_law_fisher(seed, nf, L, ncoef=ncoef, nint=nint, keep="all", **kw)
     place_wells(net, rng, wells)
     return _prune(net, "connected")
+
+
+def place_impermeable_circles(net, rng, n, rmin=1.0, rmax=3.0, ncoef=30, nint=60, clearance=1.2, tries=500):
+    """n impermeable circles (radius U[rmin, rmax]) at random points of random
+    fractures, inside the fracture and clear of its line elements and of the
+    other circles."""
+    nf = len(net.radii)
+    placed = 0
+    for _ in range(tries * n):
+        if placed == n:
+            break
+        f = int(rng.integers(0, nf))
+        R = float(net.radii[f])
+        r = float(rng.uniform(rmin, rmax))
+        if R < 2.5 * r:
+            continue
+        z = (R - 1.5 * r) * np.sqrt(rng.uniform()) * np.exp(2j * np.pi * rng.uniform())
+        ok = True
+        for el in net.frac_elems[f]:
+            e = net.elements[el]
+            if e.type in (0, 3, 5):
+                ep = e.ep1 if (e.type == 0 and e.frac1 == f) else e.ep0
+                ok = _seg_dist(z, complex(ep[0]), complex(ep[1])) > clearance * r
+            elif e.type in (2, 4):
+                ok = abs(z - e.center) > clearance * (r + e.radius)
+            if not ok:
+                break
+        if ok:
+            add_impermeable_circle(net, f, z, r, ncoef, nint)
+            placed += 1
+    return placed
+
+
+def large_network(seed=11, nf=20000, L=200.0, n_imp=100, ncoef=30, nint=60):
+    """The large single-network workload: nf power-law/Fisher discs (radii
+    1-40 m) in an L cube, the largest cluster joining both head planes, plus
+    n_imp impermeable circles (radius 1-3 m) on random fractures of it."""
+    net = power_law_fisher(seed, nf, L, rmin=1.0, rmax=40.0, ncoef=ncoef, nint=nint)
+    rng = np.random.default_rng([seed, 13])
+    place_impermeable_circles(net, rng, n_imp, ncoef=ncoef, nint=nint)
+    return net

@@ -346,6 +346,7 @@ def run_gpu(args):
     ev["trisolve"] = {"bytes": tri_bytes, "dense_tail": K}
     batched = None if args.no_batch else run_batched(args, device, flush)
     adjoint = None if args.no_adjoint else run_adjoint(args, device, F, E)
+    large = None if args.no_large else run_large(args, device)
     if rank == 0:
         cpu = None
         if not args.no_cpu:
@@ -372,7 +373,7 @@ def run_gpu(args):
                                 "q_scale": resid["q_scale"],
                                 "note": "series truncation residual at the collocation points (ncoef 20); "
                                         "convergence uses the reference's MAX_ERROR rule"},
-                "adjoint": adjoint}
+                "adjoint": adjoint, "large": large}
         print(json.dumps(line), flush=True)
     solver.close()
     if ws > 1:
@@ -543,6 +544,62 @@ def run_adjoint(args, device, F, E, fd_fracs=10, fd_its=400, steps_fd=(1e-6, 1e-
     return out
 
 
+LARGE_WORKLOAD = ("large: 20,000 power-law/Fisher discs (radii 1-40 m) in a 200 m cube (seed 11), largest cluster "
+                  "joining both head planes (2,588 fractures), 100 impermeable circles (radius 1-3 m), bounding "
+                  "circles on every fracture, ncoef 30, nint 60, MAX_ERROR 1e-8; forward solve + gradient of 50 "
+                  "observation heads + outflow w.r.t. log t")
+
+
+def run_large(args, device):
+    """Forward solve and log-transmissivity gradient of the large network."""
+    import torch
+    from andfn_b200 import network as nw
+    from andfn_b200.adjoint import DFNModel
+    from andfn_b200.records import default_constants
+    F, E = nw.to_records(nw.large_network())
+    c = default_constants(MAX_ITERATIONS=300, MAX_ERROR=MAX_ERROR, MAX_NCOEF=30)
+    dev = f"cuda:{device}"
+    rng = np.random.default_rng(17)
+    fr = rng.integers(0, len(F), 50)
+    z = F["radius"][fr] * 0.8 * np.sqrt(rng.uniform(size=50)) * np.exp(2j * np.pi * rng.uniform(size=50))
+    frt = torch.tensor(fr, dtype=torch.int64, device=dev)
+    zt = torch.tensor(z, dtype=torch.complex128, device=dev)
+    outlet = torch.tensor(np.nonzero((E["_type"] == 3) & (E["head"] == 0.0))[0], device=dev)
+    free0, total = torch.cuda.mem_get_info(device)
+    model = DFNModel(F.copy(), E.copy(), c, 50, device=device, adjoint_tol=1e-8)
+    lt0 = torch.tensor(np.log(F["t"]), dtype=torch.float64, device=dev)
+    with torch.no_grad():
+        coef, q, C = model.solve(lt0)
+        hobs = model.heads(coef, q, C, lt0, frt, zt) + torch.tensor(rng.normal(0, 0.01, 50), device=dev)
+    fwd, bwd = [], []
+    for i in range(1 + max(1, min(args.steps, 2))):
+        lt = lt0.clone().requires_grad_(True)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        coef, q, C = model.solve(lt)
+        h = model.heads(coef, q, C, lt, frt, zt)
+        J = ((h - hobs) ** 2).sum() + q[outlet].sum()
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        J.backward()
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        if i:
+            fwd.append(t1 - t0)
+            bwd.append(t2 - t1)
+    free1, _ = torch.cuda.mem_get_info(device)
+    st, ast = model.stats, model.adjoint_stats
+    model.close()
+    return {"workload": LARGE_WORKLOAD, "fractures": int(len(F)), "elements": int(len(E)),
+            "n_unknowns": int(st["n_unknowns"]), "dense_tail": int(st["dense_tail"]),
+            "forward_iterations": int(st["iterations"]), "forward_status": int(st["status"]),
+            "forward_ms": 1e3 * float(np.mean(fwd)), "gradient_ms": 1e3 * float(np.mean(bwd)),
+            "gradient_over_forward": float(np.mean(bwd) / np.mean(fwd)),
+            "adjoint_sweeps": int(ast["iterations"]), "adjoint_residual": float(ast["residual"]),
+            "adjoint_status": int(ast["status"]), "device_memory_mb": (free0 - free1) / 2**20,
+            "grad_norm": float(torch.linalg.norm(lt.grad).item())}
+
+
 def aggregate_ranks(total_ms: float, steps: int, world_size: int, device=None) -> tuple[float, float]:
     """Slowest rank's timed milliseconds (all-reduce MAX) and the whole-job
     value: every rank solves its own network, so value = world_size * steps
@@ -575,6 +632,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-realizations measurement")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint (gradient) measurement")
+    ap.add_argument("--no-large", action="store_true", help="skip the large-network forward + gradient run")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
