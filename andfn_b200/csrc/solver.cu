@@ -18,6 +18,7 @@
 // reads a device status word first and returns once the loop is finished, so
 // iterations are launched in batches (CUDA graphs) without a host round trip
 // per iteration.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -1095,13 +1096,224 @@ __device__ void dense_upper_solve(const double *__restrict__ Ucm, const double *
   __syncthreads();
 }
 
+namespace cg = cooperative_groups;
+
+// W = U^-1 L^-1 of a dense tail (L unit lower, U upper with 1/U(i,i) in
+// uinv, both K x K column-major), column-major: the blocked solve of
+// L U W = I.  A CTA takes nc (<= 16) columns of W and keeps them in shared
+// memory (row-major [K][nc]); forward substitution with L and backward
+// substitution with U go panel by panel (32 rows): a warp solves a panel's
+// triangle for one column, then the CTA subtracts the panel from the rows
+// below (L) or above (U).  Computed once per factorisation.
+static constexpr int DINV_NC = 16;
+static constexpr int CLUSTER_MIN_K = 256;  // dense tails this large use the cluster path
+
+__global__ void __launch_bounds__(256) dense_inverse_kernel(const double *__restrict__ L, const double *__restrict__ U,
+                                                            const double *__restrict__ uinv, int K, int nc,
+                                                            double *__restrict__ W) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double *X = reinterpret_cast<double *>(smem_raw);
+  const int c0 = blockIdx.x * nc;
+  const int ncl = min(nc, K - c0);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int idx = threadIdx.x; idx < K * nc; idx += blockDim.x) {
+    const int i = idx / nc, c = idx - i * nc;
+    X[idx] = (c < ncl && i == c0 + c) ? 1.0 : 0.0;
+  }
+  __syncthreads();
+  for (int r0 = (c0 / 32) * 32; r0 < K; r0 += 32) {
+    const int nb = min(32, K - r0);
+    double row[32];
+#pragma unroll
+    for (int j = 0; j < 32; j++) row[j] = (lane < nb && j < lane) ? L[(size_t)(r0 + j) * K + r0 + lane] : 0.0;
+    for (int c = warp; c < ncl; c += nw) {
+      double x = (lane < nb) ? X[(r0 + lane) * nc + c] : 0.0;
+#pragma unroll
+      for (int j = 0; j < 32; j++) {
+        const double xj = __shfl_sync(0xffffffffu, x, j);
+        if (lane > j) x = fma(-row[j], xj, x);
+      }
+      if (lane < nb) X[(r0 + lane) * nc + c] = x;
+    }
+    __syncthreads();
+    for (int i = r0 + nb + threadIdx.x; i < K; i += blockDim.x) {
+      double acc[DINV_NC];
+#pragma unroll
+      for (int c = 0; c < DINV_NC; c++) acc[c] = 0.0;
+      for (int j = 0; j < nb; j++) {
+        const double l = L[(size_t)(r0 + j) * K + i];
+        const double *xr = X + (r0 + j) * nc;
+#pragma unroll
+        for (int c = 0; c < DINV_NC; c++)
+          if (c < ncl) acc[c] = fma(l, xr[c], acc[c]);
+      }
+#pragma unroll
+      for (int c = 0; c < DINV_NC; c++)
+        if (c < ncl) X[i * nc + c] -= acc[c];
+    }
+    __syncthreads();
+  }
+  for (int p = (K + 31) / 32 - 1; p >= 0; p--) {
+    const int r0 = p * 32, nb = min(32, K - r0);
+    double row[32];
+#pragma unroll
+    for (int j = 0; j < 32; j++) row[j] = (lane < nb && j > lane && j < nb) ? U[(size_t)(r0 + j) * K + r0 + lane] : 0.0;
+    const double di = (lane < nb) ? uinv[r0 + lane] : 0.0;
+    for (int c = warp; c < ncl; c += nw) {
+      double x = (lane < nb) ? X[(r0 + lane) * nc + c] : 0.0;
+#pragma unroll
+      for (int j = 31; j >= 0; j--) {
+        if (lane == j) x *= di;
+        const double xj = __shfl_sync(0xffffffffu, x, j);
+        if (lane < j) x = fma(-row[j], xj, x);
+      }
+      if (lane < nb) X[(r0 + lane) * nc + c] = x;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < r0; i += blockDim.x) {
+      double acc[DINV_NC];
+#pragma unroll
+      for (int c = 0; c < DINV_NC; c++) acc[c] = 0.0;
+      for (int j = 0; j < nb; j++) {
+        const double u = U[(size_t)(r0 + j) * K + i];
+        const double *xr = X + (r0 + j) * nc;
+#pragma unroll
+        for (int c = 0; c < DINV_NC; c++)
+          if (c < ncl) acc[c] = fma(u, xr[c], acc[c]);
+      }
+#pragma unroll
+      for (int c = 0; c < DINV_NC; c++)
+        if (c < ncl) X[i * nc + c] -= acc[c];
+    }
+    __syncthreads();
+  }
+  for (int idx = threadIdx.x; idx < K * ncl; idx += blockDim.x) {
+    const int c = idx / K, i = idx - c * K;
+    W[(size_t)(c0 + c) * K + i] = X[i * nc + c];
+  }
+}
+
+// out = in^T for K x K column-major matrices.
+__global__ void transpose_kernel(const double *__restrict__ in, double *__restrict__ out, int K) {
+  __shared__ double tile[32][33];
+  const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const int r = bx + threadIdx.x, c = by + k;
+    if (r < K && c < K) tile[k][threadIdx.x] = in[(size_t)c * K + r];
+  }
+  __syncthreads();
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const int r = by + threadIdx.x, c = bx + k;
+    if (r < K && c < K) out[(size_t)c * K + r] = tile[threadIdx.x][k];
+  }
+}
+
 struct DenseTail {
   int K;                 // trailing block size (0 = none)
   const double *L;       // K x K column-major, strictly lower part
   const double *U;       // K x K column-major, strictly upper part
   const double *uinv;    // [K] 1 / U(i,i)
   const double *lscale;  // [K] multiplier after the unit lower solve, or null
+  const double *W;       // K x K column-major inverse (cluster path), or null
 };
+
+namespace cg = cooperative_groups;
+
+// Rows [i0, i1) of a column-major K x K product, restricted to the columns
+// [jlo(i), jhi(i)) that mode selects (0: all, 1: j > i, 2: j < i):
+// out[i] = sum_j M(i, j) v[j].  Threads take (row, part) pairs; the parts of
+// a row (strided columns) are added through shared memory red[].
+__device__ void slice_gemv(const double *__restrict__ M, int K, int i0, int i1, const double *v, int mode,
+                           double *out, double *red) {
+  const int nr = i1 - i0;
+  if (nr <= 0) {
+    __syncthreads();
+    __syncthreads();
+    return;
+  }
+  const int parts = max(1, min(32, (int)blockDim.x / nr));
+  const int t = threadIdx.x;
+  const int row = t % nr, part = t / nr;
+  double acc = 0.0;
+  if (part < parts) {
+    const int i = i0 + row;
+    const double *col = M + i;
+    const int jlo = (mode == 1) ? i + 1 : 0, jhi = (mode == 2) ? i : K;
+    int j = jlo + ((part - jlo % parts) % parts + parts) % parts;  // first j >= jlo with j % parts == part
+    double a[4] = {0.0, 0.0, 0.0, 0.0};
+    for (; j + 3 * parts < jhi; j += 4 * parts) {
+      const double m0 = __ldg(col + (size_t)j * K), m1 = __ldg(col + (size_t)(j + parts) * K),
+                   m2 = __ldg(col + (size_t)(j + 2 * parts) * K), m3 = __ldg(col + (size_t)(j + 3 * parts) * K);
+      a[0] = fma(m0, v[j], a[0]);
+      a[1] = fma(m1, v[j + parts], a[1]);
+      a[2] = fma(m2, v[j + 2 * parts], a[2]);
+      a[3] = fma(m3, v[j + 3 * parts], a[3]);
+    }
+    for (; j < jhi; j += parts) a[0] = fma(__ldg(col + (size_t)j * K), v[j], a[0]);
+    acc = (a[0] + a[1]) + (a[2] + a[3]);
+    red[part * nr + row] = acc;
+  }
+  __syncthreads();
+  if (t < nr) {
+    double s = 0.0;
+    for (int p = 0; p < parts; p++) s += red[p * nr + t];
+    out[t] = s;
+  }
+  __syncthreads();
+}
+
+// The dense tail across a thread-block cluster: x = W b with one step of
+// iterative refinement through the factors, r = b - L (U x0), x = x0 + W r
+// (W = U^-1 L^-1 computed once per factorisation; applying an inverse alone
+// loses accuracy on an ill-conditioned Schur complement, the refinement
+// step restores the triangular solves' accuracy).  Each of the csize CTAs
+// computes a slice of rows of every product and writes it into every CTA's
+// copy of the vector through distributed shared memory; one cluster barrier
+// per product, no sequential panel chain.  The adjoint passes W^T and the
+// transposed factors: L = (D^-1 U)^T with lscale = D^-1, U = L^T (unit), so
+// the residual product divides by lscale between the two triangles.
+// buf holds b, x0, t, r (K each) and the reduction scratch.
+__device__ void cluster_dense_refined(const DenseTail &T, double *y2, double *buf, cg::cluster_group &cluster,
+                                      int csize, int crank) {
+  const int K = T.K;
+  double *b = buf, *x0 = buf + K, *tt = buf + 2 * K, *rr = buf + 3 * K, *red = buf + 4 * K;
+  const int per = (K + csize - 1) / csize;
+  const int i0 = min(K, crank * per), i1 = min(K, i0 + per);
+  double *sl = red + 512;  // slice result scratch [per] (red holds parts x rows <= 512)
+  for (int i = threadIdx.x; i < K; i += blockDim.x) b[i] = y2[i];
+  __syncthreads();
+  auto publish = [&](double *dst) {
+    for (int c = 0; c < csize; c++) {
+      double *d = (c == crank) ? dst : cluster.map_shared_rank(dst, c);
+      for (int k = threadIdx.x; k < i1 - i0; k += blockDim.x) d[i0 + k] = sl[k];
+    }
+    cluster.sync();
+  };
+  // x0 = W b
+  slice_gemv(T.W, K, i0, i1, b, 0, sl, red);
+  publish(x0);
+  // t = U x0 (strict upper part + diagonal 1/uinv), then / lscale
+  slice_gemv(T.U, K, i0, i1, x0, 1, sl, red);
+  for (int k = threadIdx.x; k < i1 - i0; k += blockDim.x) {
+    const int i = i0 + k;
+    double v = sl[k] + x0[i] / T.uinv[i];
+    if (T.lscale) v /= T.lscale[i];
+    sl[k] = v;
+  }
+  __syncthreads();
+  publish(tt);
+  // r = b - L t (unit lower)
+  slice_gemv(T.L, K, i0, i1, tt, 2, sl, red);
+  for (int k = threadIdx.x; k < i1 - i0; k += blockDim.x) sl[k] = b[i0 + k] - (tt[i0 + k] + sl[k]);
+  __syncthreads();
+  publish(rr);
+  // x = x0 + W r, into every copy of the tail (CTA 0's is its solve vector)
+  slice_gemv(T.W, K, i0, i1, rr, 0, sl, red);
+  for (int k = threadIdx.x; k < i1 - i0; k += blockDim.x) sl[k] += x0[i0 + k];
+  __syncthreads();
+  publish(y2);
+}
+
 
 // The factorised discharge system of one realization (its rows are the
 // global rows row0 .. row0 + n - 1; all indices inside are local).
@@ -1118,7 +1330,12 @@ struct TriDesc {
 template <bool ADJ>
 __global__ void __launch_bounds__(SOLVE_THREADS, 1) trisolve_kernel(Net net, int use_smem, int cap_levptr,
                                                                      int meta_cap, int ring_cap) {
-  const int r = blockIdx.x;
+  // launched either one CTA per realization or, for one network with a large
+  // dense tail, as a cluster whose CTAs 1.. join only the dense phase
+  cg::cluster_group cluster = cg::this_cluster();
+  const int csize = (int)cluster.num_blocks();
+  const int crank = (int)cluster.block_rank();
+  const int r = blockIdx.x / csize;
   SolveState *st = net.st + r;
   if (st->done) return;
   const TriDesc &TD = net.tri[r];
@@ -1144,6 +1361,24 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 1) trisolve_kernel(Net net, int
     ring.cap = ring_cap;
     ring.rcap = ring_cap / 2;
   }
+  // the cluster path keeps b, x0, t, r and scratch in the ring's shared memory
+  double *dense_buf = reinterpret_cast<double *>(smem_raw + ring.val_off);
+  const int dense_per = (TD.T.K + csize - 1) / csize;
+  const bool coop = csize > 1 && TD.T.K > 0 && use_smem && TD.T.W && ring.cap > 0 &&
+                    (size_t)64 * ring.cap >= sizeof(double) * (4 * (size_t)TD.T.K + 512 + dense_per);
+  if (crank != 0) {
+    if (!ADJ && !st->solve_q) return;  // the same exits as CTA 0, so the cluster barriers pair up
+    if (!coop) return;
+    const int K = TD.T.K;
+    double *y2 = y + (N - K);
+    cluster.sync();  // CTA 0 has finished the sparse L part and the coupling rows
+    const double *src = cluster.map_shared_rank(y2, 0);
+    for (int i = threadIdx.x; i < K; i += blockDim.x) y2[i] = src[i];
+    cluster.sync();  // every copy is taken
+    cluster_dense_refined(TD.T, y2, dense_buf, cluster, csize, crank);
+    cluster.sync();  // no CTA leaves while another may still write into its shared memory
+    return;
+  }
   if (!ADJ) {
     if (threadIdx.x == 0) st->nit += 1;
     if (!st->solve_q) return;  // uniform: solve_q is written only by reduce_kernel
@@ -1166,15 +1401,25 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 1) trisolve_kernel(Net net, int
   if (TD.T.K > 0) {
     level_solve(TD.Lx, y, s_levptr, cap_levptr, s_meta, meta_cap, ring);
     phase(2);
-    dense_lower_solve(TD.T.L, TD.T.K, y + (N - TD.T.K));
-    if (TD.T.lscale) {
-      for (int i = threadIdx.x; i < TD.T.K; i += blockDim.x) y[N - TD.T.K + i] *= TD.T.lscale[i];
-      __syncthreads();
+    if (coop) {
+      double *y2 = y + (N - TD.T.K);
+      cluster.sync();  // the helpers copy y2 after this
+      cluster.sync();  // ... and have copied it
+      cluster_dense_refined(TD.T, y2, dense_buf, cluster, csize, crank);
+      phase(3);
+      cluster.sync();
+      phase(4);
+    } else {
+      dense_lower_solve(TD.T.L, TD.T.K, y + (N - TD.T.K));
+      if (TD.T.lscale) {
+        for (int i = threadIdx.x; i < TD.T.K; i += blockDim.x) y[N - TD.T.K + i] *= TD.T.lscale[i];
+        __syncthreads();
+      }
+      phase(3);
+      // U: dense tail, coupling of the leading rows to it, sparse leading rows
+      dense_upper_solve(TD.T.U, TD.T.uinv, TD.T.K, y + (N - TD.T.K));
+      phase(4);
     }
-    phase(3);
-    // U: dense tail, coupling of the leading rows to it, sparse leading rows
-    dense_upper_solve(TD.T.U, TD.T.uinv, TD.T.K, y + (N - TD.T.K));
-    phase(4);
     level_solve(TD.Ux, y, s_levptr, cap_levptr, s_meta, meta_cap, ring);
     phase(5);
   }
@@ -1655,10 +1900,11 @@ struct AndfnHandle {
   DBuf<double> lf_val, ub_val, ub_scale;
   DBuf<int> lx_lev, lx_rows, lx_eptr, lx_col, ux_lev, ux_rows, ux_eptr, ux_col;
   DBuf<double> lx_val, ux_val;
-  DBuf<double> tail_l, tail_u, tail_uinv;
+  DBuf<double> tail_l, tail_u, tail_uinv, tail_w;
   DBuf<int> pinv, qcol;
   DBuf<TriDesc> tri;
-  int max_n = 0, max_nlev = 0;
+  int max_n = 0, max_nlev = 0, max_k = 0;
+  int cluster_fwd = -1, cluster_adj = -1;  // CTAs of the dense-tail cluster (1: no cluster; -1: not yet chosen)
   int64_t nnz_factors = 0;
   // evaluation tables
   std::vector<Group> groups;
@@ -2290,6 +2536,7 @@ static int create_impl(AndfnHandle *H, int R, const char *const *F, const int64_
   CK(cudaFuncSetAttribute(eval_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
   CK(cudaFuncSetAttribute(trisolve_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
   CK(cudaFuncSetAttribute(trisolve_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+  CK(cudaFuncSetAttribute(dense_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
   CK(cudaFuncSetAttribute(update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
   rc = reset_impl(H);
   if (rc) return rc;
@@ -2417,12 +2664,15 @@ static int factor_all(AndfnHandle *H, const std::vector<double> &mv) {
   std::vector<size_t> toff(R), tuoff(R);
   std::vector<int> pinv, qcol;
   H->nnz_factors = 0;
+  H->max_k = 0;
+  H->cluster_fwd = H->cluster_adj = -1;
   H->max_n = 0;
   H->max_nlev = 1;
   for (int r = 0; r < R; r++) {
     const LuFactors &F = LU[r];
     const int n = F.n, K = F.dense, m0 = n - K;
     H->max_n = std::max(H->max_n, n);
+    H->max_k = std::max(H->max_k, K);
     H->nnz_factors += F.nnz() + 2LL * K * K;
     pinv.insert(pinv.end(), F.pinv.begin(), F.pinv.end());
     qcol.insert(qcol.end(), F.q.begin(), F.q.end());
@@ -2499,6 +2749,17 @@ static int factor_all(AndfnHandle *H, const std::vector<double> &mv) {
   CK(upload(H->tail_l, tl, s));
   CK(upload(H->tail_u, tu, s));
   CK(upload(H->tail_uinv, tui, s));
+  // explicit inverse of a large dense tail of one network, for the cluster
+  // path of the discharge solve (applied with one refinement step)
+  const bool want_w = R == 1 && LU[0].dense >= CLUSTER_MIN_K;
+  if (want_w) {
+    const int K = LU[0].dense;
+    CK(H->tail_w.alloc((size_t)K * K));
+    const int nc = std::max(1, std::min(DINV_NC, (int)(200 * 1024 / (sizeof(double) * (size_t)K))));
+    dense_inverse_kernel<<<(K + nc - 1) / nc, 256, sizeof(double) * (size_t)K * nc, s>>>(
+        H->tail_l.p, H->tail_u.p, H->tail_uinv.p, K, nc, H->tail_w.p);
+    CK(cudaGetLastError());
+  }
   CK(upload(H->pinv, pinv, s));
   CK(upload(H->qcol, qcol, s));
   std::vector<TriDesc> td(R);
@@ -2523,6 +2784,7 @@ static int factor_all(AndfnHandle *H, const std::vector<double> &mv) {
     td[r].T.U = H->tail_u.p + toff[r];
     td[r].T.uinv = H->tail_uinv.p + tuoff[r];
     td[r].T.lscale = nullptr;
+    td[r].T.W = want_w ? H->tail_w.p : nullptr;
     td[r].pinv = H->pinv.p + H->h.roff[r];
     td[r].qcol = H->qcol.p + H->h.roff[r];
     td[r].row0 = H->h.roff[r];
@@ -2558,6 +2820,56 @@ static int ring_capacity(size_t used, int use_smem, int meta_cap) {
   return cap;
 }
 
+// One network with a dense tail of at least CLUSTER_MIN_K rows: the trisolve
+// runs as a cluster of CLUSTER_CTAS CTAs (the dense tail spread over their
+// SMs) when the device can co-schedule such a cluster with this much shared
+// memory per CTA; otherwise one CTA.
+static constexpr int CLUSTER_CTAS = 8;
+
+template <bool ADJ>
+static int choose_cluster(AndfnHandle *H, size_t smem, int use_smem) {
+  if (H->R != 1 || H->max_k < CLUSTER_MIN_K || !use_smem) return 1;
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = CLUSTER_CTAS;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.gridDim = dim3(CLUSTER_CTAS);
+  cfg.blockDim = dim3(H->solve_threads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int n = 0;
+  if (cudaOccupancyMaxActiveClusters(&n, trisolve_kernel<ADJ>, &cfg) != cudaSuccess) {
+    cudaGetLastError();
+    return 1;
+  }
+  return n >= 1 ? CLUSTER_CTAS : 1;
+}
+
+template <bool ADJ>
+static void launch_trisolve_kernel(AndfnHandle *H, const Net &net, cudaStream_t s, int csize, size_t smem,
+                                   int use_smem, int cap_levptr, int meta_cap, int ring_cap) {
+  if (csize > 1) {
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = csize;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(csize);
+    cfg.blockDim = dim3(H->solve_threads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, trisolve_kernel<ADJ>, net, use_smem, cap_levptr, meta_cap, ring_cap);
+  } else {
+    trisolve_kernel<ADJ><<<H->R, H->solve_threads, smem, s>>>(net, use_smem, cap_levptr, meta_cap, ring_cap);
+  }
+}
+
 static int build_head_sums(AndfnHandle *H);
 __global__ void head_vector_kernel(Net net, const int *__restrict__ gptr, const int *__restrict__ sidx,
                                    const cd *__restrict__ S);
@@ -2573,7 +2885,8 @@ static void launch_trisolve(AndfnHandle *H, cudaStream_t s) {
   if (meta_cap) solve_smem += meta_bytes;
   const int ring_cap = ring_capacity(solve_smem, use_smem, meta_cap);
   if (ring_cap) solve_smem = ((solve_smem + 15) & ~(size_t)15) + ring_bytes(ring_cap);
-  trisolve_kernel<false><<<H->R, H->solve_threads, solve_smem, s>>>(net, use_smem, cap_levptr, meta_cap, ring_cap);
+  if (H->cluster_fwd < 0) H->cluster_fwd = choose_cluster<false>(H, solve_smem, use_smem);
+  launch_trisolve_kernel<false>(H, net, s, H->cluster_fwd, solve_smem, use_smem, cap_levptr, meta_cap, ring_cap);
   const cudaError_t le = cudaGetLastError();
   if (le != cudaSuccess)
     set_error(std::string("trisolve_kernel launch (shared memory ") + std::to_string(solve_smem) +
@@ -3525,7 +3838,7 @@ struct AdjBufs {
   size_t smem = 0;
   // transposed factors
   DBuf<int> lev[4], rows[4], eptr[4], col[4];
-  DBuf<double> val[4], scale0, tl, tu, tones, tlscale;
+  DBuf<double> val[4], scale0, tl, tu, tones, tlscale, tw;
   DBuf<int> pinv, qcol;
   DBuf<TriDesc> tri;
   int max_nlev = 1;
@@ -4283,6 +4596,13 @@ static int adj_build_factors(AndfnHandle *H) {
   td.T.U = A.tu.p;
   td.T.uinv = A.tones.p;
   td.T.lscale = A.tlscale.p;
+  td.T.W = nullptr;
+  if (K >= CLUSTER_MIN_K && H->tail_w.p && H->tail_w.n == (size_t)K * K) {  // (L U)^-T = W^T
+    CK(A.tw.alloc((size_t)K * K));
+    transpose_kernel<<<dim3((K + 31) / 32, (K + 31) / 32), dim3(32, 8), 0, s>>>(H->tail_w.p, A.tw.p, K);
+    CK(cudaGetLastError());
+    td.T.W = A.tw.p;
+  }
   std::vector<int> qinv(n), pinvinv(n);
   for (int k = 0; k < n; k++) qinv[F.q[k]] = k;
   for (int i = 0; i < n; i++) pinvinv[F.pinv[i]] = i;
@@ -4309,7 +4629,8 @@ static void launch_trisolve_adj(AndfnHandle *H, const Net &net, cudaStream_t s) 
   if (meta_cap) solve_smem += meta_bytes;
   const int ring_cap = ring_capacity(solve_smem, use_smem, meta_cap);
   if (ring_cap) solve_smem = ((solve_smem + 15) & ~(size_t)15) + ring_bytes(ring_cap);
-  trisolve_kernel<true><<<1, H->solve_threads, solve_smem, s>>>(net, use_smem, cap_levptr, meta_cap, ring_cap);
+  if (H->cluster_adj < 0) H->cluster_adj = choose_cluster<true>(H, solve_smem, use_smem);
+  launch_trisolve_kernel<true>(H, net, s, H->cluster_adj, solve_smem, use_smem, cap_levptr, meta_cap, ring_cap);
 }
 
 static constexpr int ADJ_SWEEP_LAUNCHES = 9;  // per transposed sweep (3 memsets + 6 kernels)

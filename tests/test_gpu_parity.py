@@ -137,3 +137,21 @@ def test_generated_network_matches_oracle_with_dense_tail():
         Fo, Eo = F0.copy(), E0.copy()
         orc.solve(Fo, Eo, 50, c)
         _compare(E, F, Eo, Fo, ("generated", its))
+
+
+def test_generated_network_with_cluster_dense_tail_matches_oracle():
+    """A 588-fracture network with a 364-row dense tail (the dense tail runs
+    as a CTA cluster: inverse + one refinement step), 120 iterations (the
+    network converges at 146; a fixed count keeps the comparison exact):
+    coefficients vs the oracle."""
+    from andfn_b200 import network as nw
+    from andfn_b200.records import default_constants
+    from oracle import oracle as orc
+    F0, E0 = nw.to_records(nw.power_law_fisher(3, nf=1500, L=30.0, ncoef=10, nint=20))
+    c = default_constants(MAX_ITERATIONS=120, MAX_ERROR=1e-300, MAX_NCOEF=10)
+    F, E = F0.copy(), E0.copy()
+    st = _gpu_solve(F, E, 50, c)
+    assert st["dense_tail"] >= 256 and st["iterations"] == 120, st
+    Fo, Eo = F0.copy(), E0.copy()
+    orc.solve(Fo, Eo, 50, c)
+    _compare(E, F, Eo, Fo, ("cluster tail", 120))
