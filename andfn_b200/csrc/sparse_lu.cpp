@@ -241,8 +241,11 @@ static int dense_lu(double *S, int n, std::vector<int> &piv, double &min_piv) {
   return 0;
 }
 
+static int finish_factors(LuFactors &F, LuPending &W, const std::vector<int> &dpiv, const double *S,
+                          const double *tail_diag);
+
 int sparse_lu_factor(const CscMatrix &A, const std::vector<int> &q, double pivot_threshold, LuFactors &F,
-                     int dense) {
+                     int dense, bool defer_dense) {
   const int n = A.n;
   if (dense < 0 || dense > n) dense = 0;
   const int m0 = n - dense;
@@ -266,21 +269,10 @@ int sparse_lu_factor(const CscMatrix &A, const std::vector<int> &q, double pivot
   std::vector<int> tail_row;           // dense-block row of each original row (or -1)
   std::vector<double> S;               // Schur complement, column-major dense x dense
   std::vector<int> tail_rows;          // original rows of the dense block, in block order
-  for (int k = 0; k < n; k++) {
+  for (int k = 0; k < m0; k++) {
     const int col = q[k];
     pattern.clear();
     topo.clear();
-    if (k == m0 && dense > 0) {
-      // rows not pivoted yet form the dense block
-      tail_row.assign(n, -1);
-      for (int r = 0; r < n; r++)
-        if (F.pinv[r] < 0) {
-          tail_row[r] = (int)tail_rows.size();
-          tail_rows.push_back(r);
-        }
-      if ((int)tail_rows.size() != dense) return 3;
-      S.assign((size_t)dense * dense, 0.0);
-    }
     // Scatter A(:, col) and find the reach of its pivoted rows in L's graph.
     for (int p = A.colptr[col]; p < A.colptr[col + 1]; p++) {
       int r = A.rowind[p];
@@ -348,14 +340,6 @@ int sparse_lu_factor(const CscMatrix &A, const std::vector<int> &q, double pivot
       }
     }
     Ucp.push_back((int)Uri.size());
-    if (k >= m0) {
-      // dense block column: the not-yet-pivoted rows
-      double *sc = S.data() + (size_t)(k - m0) * dense;
-      for (int r : pattern)
-        if (F.pinv[r] < 0) sc[tail_row[r]] = x[r];
-      Lcp.push_back((int)Lri.size());
-      continue;
-    }
     // Partial pivoting over the not-yet-pivoted rows.
     int piv = -1;
     double amax = 0.0;
@@ -382,33 +366,176 @@ int sparse_lu_factor(const CscMatrix &A, const std::vector<int> &q, double pivot
     Lcp.push_back((int)Lri.size());
   }
   if (dense > 0) {
-    std::vector<int> dpiv;
-    if (dense_lu(S.data(), dense, dpiv, min_piv)) return 3;
+    // The dense block: the rows not pivoted yet.  Its columns (the Schur
+    // complement) depend only on the finished leading columns of L, so they
+    // are formed in parallel, each with its own workspace, by the same steps
+    // (and the same arithmetic order) as the leading columns.
+    tail_row.assign(n, -1);
+    for (int r = 0; r < n; r++)
+      if (F.pinv[r] < 0) {
+        tail_row[r] = (int)tail_rows.size();
+        tail_rows.push_back(r);
+      }
+    if ((int)tail_rows.size() != dense) return 3;
+    S.assign((size_t)dense * dense, 0.0);
+    std::vector<std::vector<int>> u_rows(dense);
+    std::vector<std::vector<double>> u_vals(dense);
+#pragma omp parallel
+    {
+      std::vector<double> xw(n, 0.0);
+      std::vector<int> tw(n, -1), vw(n, -1), pat, tp, stk, cpos;
+      pat.reserve(n);
+      tp.reserve(n);
+#pragma omp for schedule(dynamic, 4)
+      for (int k = m0; k < n; k++) {
+        const int col = q[k];
+        pat.clear();
+        tp.clear();
+        for (int p = A.colptr[col]; p < A.colptr[col + 1]; p++) {
+          int r = A.rowind[p];
+          if (tw[r] != k) {
+            tw[r] = k;
+            pat.push_back(r);
+            xw[r] = 0.0;
+          }
+          xw[r] += A.val[p];
+          int j = F.pinv[r];
+          if (j >= 0 && vw[j] != k) {
+            stk.clear();
+            cpos.clear();
+            stk.push_back(j);
+            cpos.push_back(Lcp[j]);
+            vw[j] = k;
+            while (!stk.empty()) {
+              int jj = stk.back();
+              int &cp = cpos.back();
+              bool pushed = false;
+              while (cp < Lcp[jj + 1]) {
+                int rr = Lri[cp++];
+                int j2 = F.pinv[rr];
+                if (j2 >= 0 && vw[j2] != k) {
+                  vw[j2] = k;
+                  stk.push_back(j2);
+                  cpos.push_back(Lcp[j2]);
+                  pushed = true;
+                  break;
+                }
+              }
+              if (!pushed) {
+                tp.push_back(jj);
+                stk.pop_back();
+                cpos.pop_back();
+              }
+            }
+          }
+        }
+        for (int t = (int)tp.size() - 1; t >= 0; t--) {
+          int j = tp[t];
+          const int rj = prow[j];
+          double xj = (tw[rj] == k) ? xw[rj] : 0.0;
+          if (xj == 0.0) continue;
+          for (int p = Lcp[j]; p < Lcp[j + 1]; p++) {
+            int r = Lri[p];
+            if (tw[r] != k) {
+              tw[r] = k;
+              pat.push_back(r);
+              xw[r] = 0.0;
+            }
+            xw[r] -= Lv[p] * xj;
+          }
+        }
+        std::vector<int> &ur = u_rows[k - m0];
+        std::vector<double> &uv = u_vals[k - m0];
+        for (int t = (int)tp.size() - 1; t >= 0; t--) {
+          int j = tp[t];
+          const int rj = prow[j];
+          double v = (tw[rj] == k) ? xw[rj] : 0.0;
+          if (v != 0.0) {
+            ur.push_back(j);
+            uv.push_back(v);
+          }
+        }
+        double *sc = S.data() + (size_t)(k - m0) * dense;
+        for (int r : pat)
+          if (F.pinv[r] < 0) sc[tail_row[r]] = xw[r];
+      }
+    }
+    for (int k = m0; k < n; k++) {
+      Uri.insert(Uri.end(), u_rows[k - m0].begin(), u_rows[k - m0].end());
+      Uv.insert(Uv.end(), u_vals[k - m0].begin(), u_vals[k - m0].end());
+      Ucp.push_back((int)Uri.size());
+      Lcp.push_back((int)Lri.size());
+    }
+  }
+  LuPending W;
+  W.Lcp = std::move(Lcp);
+  W.Lri = std::move(Lri);
+  W.Lv = std::move(Lv);
+  W.Ucp = std::move(Ucp);
+  W.Uri = std::move(Uri);
+  W.Uv = std::move(Uv);
+  W.diag = std::move(diag);
+  W.prow = std::move(prow);
+  W.tail_rows = std::move(tail_rows);
+  W.min_piv = min_piv;
+  if (dense > 0 && defer_dense) {
+    F.schur = std::move(S);
+    F.pending = std::move(W);
+    return 0;
+  }
+  std::vector<int> dpiv;
+  if (dense > 0 && dense_lu(S.data(), dense, dpiv, W.min_piv)) return 3;
+  return finish_factors(F, W, dpiv, dense > 0 ? S.data() : nullptr, nullptr);
+}
+
+int sparse_lu_finish(LuFactors &F, const std::vector<int> &dpiv, const std::vector<double> &tail_diag) {
+  if ((int)dpiv.size() != F.dense || (int)tail_diag.size() != F.dense) return 3;
+  for (double d : tail_diag)
+    if (!(d != 0.0) || !std::isfinite(d)) return 3;
+  const int rc = finish_factors(F, F.pending, dpiv, nullptr, tail_diag.data());
+  F.pending = LuPending();
+  F.schur.clear();
+  F.schur.shrink_to_fit();
+  return rc;
+}
+
+// The row permutation of the dense block from its pivots, the dense block's
+// triangles (when factorised here) and the row-oriented factors.
+static int finish_factors(LuFactors &F, LuPending &W, const std::vector<int> &dpiv, const double *S,
+                          const double *tail_diag) {
+  const int n = F.n, dense = F.dense, m0 = n - dense;
+  std::vector<int> &Lcp = W.Lcp, &Lri = W.Lri, &Ucp = W.Ucp, &Uri = W.Uri, &prow = W.prow;
+  std::vector<double> &Lv = W.Lv, &Uv = W.Uv, &diag = W.diag;
+  if (dense > 0) {
     // block row order after the dense pivoting
     std::vector<int> order(dense);
     for (int i = 0; i < dense; i++) order[i] = i;
     for (int j = 0; j < dense; j++) std::swap(order[j], order[dpiv[j]]);
     for (int i = 0; i < dense; i++) {
-      const int r = tail_rows[order[i]];
+      const int r = W.tail_rows[order[i]];
       F.pinv[r] = m0 + i;
       prow[m0 + i] = r;
     }
-    F.l22.assign((size_t)dense * dense, 0.0);
-    F.u22.assign((size_t)dense * dense, 0.0);
-    for (int c = 0; c < dense; c++)
-      for (int i = 0; i < dense; i++) {
-        const double v = S[(size_t)c * dense + i];
-        if (i > c)
-          F.l22[(size_t)c * dense + i] = v;
-        else if (i < c)
-          F.u22[(size_t)c * dense + i] = v;
-        else
-          diag[m0 + i] = v;
-      }
+    if (S) {
+      F.l22.assign((size_t)dense * dense, 0.0);
+      F.u22.assign((size_t)dense * dense, 0.0);
+      for (int c = 0; c < dense; c++)
+        for (int i = 0; i < dense; i++) {
+          const double v = S[(size_t)c * dense + i];
+          if (i > c)
+            F.l22[(size_t)c * dense + i] = v;
+          else if (i < c)
+            F.u22[(size_t)c * dense + i] = v;
+          else
+            diag[m0 + i] = v;
+        }
+    } else {
+      for (int i = 0; i < dense; i++) diag[m0 + i] = tail_diag[i];
+    }
   }
-  F.min_abs_pivot = min_piv;
+  F.min_abs_pivot = W.min_piv;
   // Row-oriented factors in pivot-step indices (entries inside the dense
-  // block are kept only in l22 / u22).
+  // block are kept only in the dense block).
   F.l_ptr.assign(n + 1, 0);
   for (int k = 0; k < m0; k++)
     for (int p = Lcp[k]; p < Lcp[k + 1]; p++) F.l_ptr[F.pinv[Lri[p]] + 1]++;

@@ -19,6 +19,14 @@ struct CscMatrix {
   std::vector<double> val;
 };
 
+// State of a factorisation whose dense block is factorised elsewhere
+// (sparse_lu_factor(..., defer_dense = true) then sparse_lu_finish).
+struct LuPending {
+  std::vector<int> Lcp, Lri, Ucp, Uri, prow, tail_rows;
+  std::vector<double> Lv, Uv, diag;
+  double min_piv = 0.0;
+};
+
 struct LuFactors {
   int n = 0;
   // Dense trailing block: the last `dense` pivot steps are factorised as a
@@ -37,6 +45,10 @@ struct LuFactors {
   std::vector<double> u_inv_diag; // 1 / U(k,k)
   int64_t nnz() const { return (int64_t)l_val.size() + (int64_t)u_val.size() + n; }
   double min_abs_pivot = 0.0;
+  // deferred dense block: the Schur complement (column-major dense x dense,
+  // row order = block order) and the state sparse_lu_finish needs
+  std::vector<double> schur;
+  LuPending pending;
 };
 
 // Column ordering: minimum degree on the column-intersection graph of A,
@@ -54,7 +66,15 @@ std::vector<int> column_min_degree_order(const CscMatrix &A, int *dense_tail = n
 // with partial pivoting (OpenMP).  Returns 0 on success, 3 (singular) if a
 // column has no nonzero pivot.
 int sparse_lu_factor(const CscMatrix &A, const std::vector<int> &q, double pivot_threshold, LuFactors &out,
-                     int dense = 0);
+                     int dense = 0, bool defer_dense = false);
+
+// With defer_dense, sparse_lu_factor stops after forming the Schur complement
+// (out.schur); once it is factorised in place elsewhere (partial pivoting,
+// dpiv[j] = block row swapped with row j, unit lower L below the diagonal, U
+// on and above it), sparse_lu_finish completes the row order and the
+// row-oriented factors from the pivots and U's diagonal (l22 / u22 stay
+// empty: the factorised block lives where it was factorised).
+int sparse_lu_finish(LuFactors &F, const std::vector<int> &dpiv, const std::vector<double> &tail_diag);
 
 // Reference triangular solve on the host (used for checks): x = A^-1 b.
 void sparse_lu_solve_host(const LuFactors &F, const double *b, double *x);
