@@ -24,6 +24,7 @@
 #include <algorithm>
 #include <array>
 #include <chrono>
+#include <cfloat>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -1208,6 +1209,244 @@ __global__ void transpose_kernel(const double *__restrict__ in, double *__restri
   }
 }
 
+// Dense-tail factors of the adjoint from the forward ones (one K x K
+// column-major matrix holding L strictly below and U on and above the
+// diagonal): out(i, j) = S(j, i) / U(j, j) below the diagonal ((D^-1 U)^T),
+// S(j, i) above it (L^T), 0 on it.
+__global__ void adj_tail_kernel(const double *__restrict__ S, const double *__restrict__ uinv, int K,
+                                double *__restrict__ out) {
+  __shared__ double tile[32][33];
+  const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const int r = bx + threadIdx.x, c = by + k;
+    if (r < K && c < K) tile[k][threadIdx.x] = S[(size_t)c * K + r];
+  }
+  __syncthreads();
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const int i = by + threadIdx.x, j = bx + k;
+    if (i < K && j < K) {
+      const double v = tile[threadIdx.x][k];
+      out[(size_t)j * K + i] = (i > j) ? v * uinv[j] : (i < j ? v : 0.0);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Dense LU of the Schur complement on the device (right-looking, partial
+// pivoting, panels of DLU_NB columns), in place on a K x K column-major
+// matrix: unit lower L below the diagonal, U on and above it, the pivot rule
+// of the host factorisation (largest magnitude, first row on a tie).  Per
+// panel: the panel kernel factorises the panel columns (one CTA; the panel's
+// rows in shared memory when they fit), the update kernel applies the
+// panel's row interchanges to every other column and solves U12 = L11^-1 A12,
+// the GEMM kernel updates the trailing block A22 -= L21 U12.
+static constexpr int DLU_NB = 16;
+static constexpr int DLU_THREADS = 1024;
+static constexpr int DLU_MIN_K = 64;
+static constexpr size_t DLU_SMEM_MAX = 220 * 1024;
+
+struct DluScratch {
+  int *piv;       // [K] block row swapped with row j at step j
+  double *diag;   // [K] U(j, j)
+  int *swap_src;  // [2 DLU_NB] composite interchange of the last panel:
+  int *swap_dst;  //   row swap_dst[k] receives the old row swap_src[k]
+  int *swap_cnt;  // [1]
+  int *flag;      // [1] first zero / non-finite pivot column + 1 (0 = none)
+};
+
+__global__ void __launch_bounds__(DLU_THREADS) dlu_panel_kernel(double *__restrict__ S, int K, int j0, int nb,
+                                                                int use_smem, DluScratch D) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ double s_wv[32];
+  __shared__ int s_wi[32];
+  __shared__ int s_piv[DLU_NB];
+  const int tid = threadIdx.x, bd = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = bd >> 5;
+  const int m = K - j0;
+  double *P;
+  size_t rs, cs;
+  if (use_smem) {
+    P = reinterpret_cast<double *>(smem_raw);
+    rs = DLU_NB + 1;
+    cs = 1;
+    for (int idx = tid; idx < m * nb; idx += bd) {
+      const int c = idx / m, i = idx - c * m;
+      P[i * rs + c] = S[(size_t)(j0 + c) * K + j0 + i];
+    }
+    __syncthreads();
+  } else {
+    P = S + (size_t)j0 * K + j0;
+    rs = 1;
+    cs = K;
+  }
+  for (int jj = 0; jj < nb; jj++) {
+    double best = -1.0;
+    int bi = m;
+    int bad = 0;
+    for (int i = jj + tid; i < m; i += bd) {
+      const double v = fabs(P[i * rs + jj * cs]);
+      if (!(v <= DBL_MAX)) bad = 1;
+      if (v > best) {
+        best = v;
+        bi = i;
+      }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      const double ov = __shfl_down_sync(0xffffffffu, best, off);
+      const int oi = __shfl_down_sync(0xffffffffu, bi, off);
+      if (ov > best || (ov == best && oi < bi)) {
+        best = ov;
+        bi = oi;
+      }
+    }
+    if (lane == 0) {
+      s_wv[warp] = best;
+      s_wi[warp] = bi;
+    }
+    bad = __syncthreads_or(bad);
+    if (warp == 0) {
+      best = (lane < nw) ? s_wv[lane] : -1.0;
+      bi = (lane < nw) ? s_wi[lane] : m;
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        const double ov = __shfl_down_sync(0xffffffffu, best, off);
+        const int oi = __shfl_down_sync(0xffffffffu, bi, off);
+        if (ov > best || (ov == best && oi < bi)) {
+          best = ov;
+          bi = oi;
+        }
+      }
+      if (lane == 0) {
+        if (bi >= m) bi = jj;  // every entry NaN: keep the diagonal, flagged below
+        s_piv[jj] = bi;
+        D.piv[j0 + jj] = j0 + bi;
+        if ((bad || !(best > 0.0)) && *D.flag == 0) *D.flag = j0 + jj + 1;
+      }
+    }
+    __syncthreads();
+    const int p = s_piv[jj];
+    if (p != jj && tid < nb) {
+      const double a = P[jj * rs + tid * cs], b = P[p * rs + tid * cs];
+      P[jj * rs + tid * cs] = b;
+      P[p * rs + tid * cs] = a;
+    }
+    __syncthreads();
+    const double piv = P[jj * rs + jj * cs];
+    if (tid == 0) D.diag[j0 + jj] = piv;
+    const double inv = (piv != 0.0) ? 1.0 / piv : 0.0;
+    for (int i = jj + 1 + tid; i < m; i += bd) {
+      const double l = P[i * rs + jj * cs] * inv;
+      P[i * rs + jj * cs] = l;
+      for (int c = jj + 1; c < nb; c++) P[i * rs + c * cs] = fma(-l, P[jj * rs + c * cs], P[i * rs + c * cs]);
+    }
+    __syncthreads();
+  }
+  if (use_smem) {
+    for (int idx = tid; idx < m * nb; idx += bd) {
+      const int c = idx / m, i = idx - c * m;
+      S[(size_t)(j0 + c) * K + j0 + i] = P[i * rs + c];
+    }
+  }
+  if (tid == 0) {
+    // the panel's interchanges as one permutation of at most 2 nb rows
+    int rows[2 * DLU_NB], orig[2 * DLU_NB], cnt = 0;
+    auto find = [&](int r) {
+      for (int k = 0; k < cnt; k++)
+        if (rows[k] == r) return k;
+      rows[cnt] = r;
+      orig[cnt] = r;
+      return cnt++;
+    };
+    for (int jj = 0; jj < nb; jj++) {
+      const int a = j0 + jj, b = j0 + s_piv[jj];
+      if (a == b) continue;
+      const int ka = find(a), kb = find(b);
+      const int t = orig[ka];
+      orig[ka] = orig[kb];
+      orig[kb] = t;
+    }
+    for (int k = 0; k < cnt; k++) {
+      D.swap_dst[k] = rows[k];
+      D.swap_src[k] = orig[k];
+    }
+    *D.swap_cnt = cnt;
+  }
+}
+
+// One warp per column outside the panel: the panel's interchanges, then for
+// the trailing columns U12 = L11^-1 A12 (unit lower triangle of the panel).
+__global__ void __launch_bounds__(256) dlu_update_kernel(double *__restrict__ S, int K, int j0, int nb, DluScratch D) {
+  __shared__ double L11[DLU_NB][DLU_NB + 1];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int idx = threadIdx.x; idx < nb * nb; idx += blockDim.x) {
+    const int c = idx / nb, r = idx - c * nb;
+    L11[r][c] = (r > c) ? S[(size_t)(j0 + c) * K + j0 + r] : 0.0;
+  }
+  __syncthreads();
+  const int cidx = blockIdx.x * (blockDim.x >> 5) + warp;
+  if (cidx >= K - nb) return;
+  const int c = (cidx < j0) ? cidx : cidx + nb;
+  double *col = S + (size_t)c * K;
+  const int cnt = *D.swap_cnt;
+  double v = 0.0;
+  if (lane < cnt) v = col[D.swap_src[lane]];
+  __syncwarp();
+  if (lane < cnt) col[D.swap_dst[lane]] = v;
+  __syncwarp();
+  if (c < j0 + nb) return;
+  double x = (lane < nb) ? col[j0 + lane] : 0.0;
+#pragma unroll
+  for (int j = 0; j < DLU_NB; j++) {
+    const double xj = __shfl_sync(0xffffffffu, x, j);
+    if (lane > j && lane < nb) x = fma(-L11[lane][j], xj, x);
+  }
+  if (lane < nb) col[j0 + lane] = x;
+}
+
+// A22 -= L21 U12 over 64 x 64 tiles of the trailing block (4 x 4 outputs a
+// thread; the thread's rows are 16 apart so the column-major stores coalesce).
+__global__ void __launch_bounds__(256) dlu_gemm_kernel(double *__restrict__ S, int K, int j0, int nb) {
+  __shared__ double As[DLU_NB][64], Bs[DLU_NB][65];
+  const int c0 = j0 + nb, m = K - c0;
+  const int rb = blockIdx.x * 64, cb = blockIdx.y * 64;
+  for (int idx = threadIdx.x; idx < DLU_NB * 64; idx += blockDim.x) {
+    const int k = idx / 64, i = idx - k * 64;
+    As[k][i] = (k < nb && rb + i < m) ? S[(size_t)(j0 + k) * K + c0 + rb + i] : 0.0;
+    const int c = idx / DLU_NB, kk = idx - c * DLU_NB;
+    Bs[kk][c] = (kk < nb && cb + c < m) ? S[(size_t)(c0 + cb + c) * K + j0 + kk] : 0.0;
+  }
+  __syncthreads();
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  double acc[4][4];
+#pragma unroll
+  for (int r = 0; r < 4; r++)
+#pragma unroll
+    for (int q = 0; q < 4; q++) acc[r][q] = 0.0;
+#pragma unroll
+  for (int k = 0; k < DLU_NB; k++) {
+    double a[4], b[4];
+#pragma unroll
+    for (int r = 0; r < 4; r++) a[r] = As[k][tx + 16 * r];
+#pragma unroll
+    for (int q = 0; q < 4; q++) b[q] = Bs[k][ty + 16 * q];
+#pragma unroll
+    for (int r = 0; r < 4; r++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) acc[r][q] = fma(a[r], b[q], acc[r][q]);
+  }
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int c = cb + ty + 16 * q;
+    if (c >= m) continue;
+    double *col = S + (size_t)(c0 + c) * K + c0;
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+      const int i = rb + tx + 16 * r;
+      if (i < m) col[i] -= acc[r][q];
+    }
+  }
+}
+
 struct DenseTail {
   int K;                 // trailing block size (0 = none)
   const double *L;       // K x K column-major, strictly lower part
@@ -1900,7 +2139,11 @@ struct AndfnHandle {
   DBuf<double> lf_val, ub_val, ub_scale;
   DBuf<int> lx_lev, lx_rows, lx_eptr, lx_col, ux_lev, ux_rows, ux_eptr, ux_col;
   DBuf<double> lx_val, ux_val;
-  DBuf<double> tail_l, tail_u, tail_uinv, tail_w;
+  // dense tails: L strictly below and U on and above the diagonal in one
+  // K x K column-major matrix per realization (diagonal of U in tail_uinv)
+  DBuf<double> tail_l, tail_uinv, tail_w;
+  DBuf<int> dlu_i;  // device dense-LU scratch
+  DBuf<double> dlu_d;
   DBuf<int> pinv, qcol;
   DBuf<TriDesc> tri;
   int max_n = 0, max_nlev = 0, max_k = 0;
@@ -2537,6 +2780,7 @@ static int create_impl(AndfnHandle *H, int R, const char *const *F, const int64_
   CK(cudaFuncSetAttribute(trisolve_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
   CK(cudaFuncSetAttribute(trisolve_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
   CK(cudaFuncSetAttribute(dense_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+  CK(cudaFuncSetAttribute(dlu_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DLU_SMEM_MAX));
   CK(cudaFuncSetAttribute(update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
   rc = reset_impl(H);
   if (rc) return rc;
@@ -2631,22 +2875,63 @@ static int group_for(const std::vector<int> &eptr, bool single = false) {
 // Factorises every realization's system (in parallel over realizations) and
 // uploads the level-ordered factor parts, dense tails, permutations and one
 // TriDesc per realization.
+// Factorises the Schur complement F.schur on the device into H->tail_l
+// (panels of DLU_NB columns, three launches each) and completes F from the
+// pivots and U's diagonal.  Returns 3 for a singular block.
+static int gpu_dense_lu(AndfnHandle *H, LuFactors &F) {
+  const int K = F.dense;
+  cudaStream_t s = H->stream;
+  CK(upload(H->tail_l, F.schur, s));
+  CK(H->dlu_i.alloc((size_t)K + 4 * DLU_NB + 2));
+  CK(H->dlu_d.alloc((size_t)K));
+  int *ib = H->dlu_i.p;
+  DluScratch D{ib, H->dlu_d.p, ib + K, ib + K + 2 * DLU_NB, ib + K + 4 * DLU_NB, ib + K + 4 * DLU_NB + 1};
+  CK(cudaMemsetAsync(D.flag, 0, sizeof(int), s));
+  double *S = H->tail_l.p;
+  for (int j0 = 0; j0 < K; j0 += DLU_NB) {
+    const int nb = std::min(DLU_NB, K - j0), m = K - j0, mt = m - nb;
+    const size_t sm = sizeof(double) * (size_t)m * (DLU_NB + 1);
+    const int use_smem = sm <= DLU_SMEM_MAX;
+    dlu_panel_kernel<<<1, DLU_THREADS, use_smem ? sm : 0, s>>>(S, K, j0, nb, use_smem, D);
+    if (K > nb) dlu_update_kernel<<<(K - nb + 7) / 8, 256, 0, s>>>(S, K, j0, nb, D);
+    if (mt > 0) dlu_gemm_kernel<<<dim3((mt + 63) / 64, (mt + 63) / 64), 256, 0, s>>>(S, K, j0, nb);
+  }
+  CK(cudaGetLastError());
+  std::vector<int> piv(K), flag(1);
+  std::vector<double> dg(K);
+  CK(cudaMemcpyAsync(piv.data(), D.piv, sizeof(int) * K, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(dg.data(), D.diag, sizeof(double) * K, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(flag.data(), D.flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+  g_d2h_bytes += (int64_t)(12 * K + 4);
+  CK(cudaStreamSynchronize(s));
+  if (flag[0]) return 3;
+  return sparse_lu_finish(F, piv, dg);
+}
+
 static int factor_all(AndfnHandle *H, const std::vector<double> &mv) {
   const int R = H->R;
   cudaStream_t s = H->stream;
   std::vector<LuFactors> LU(R);
   std::vector<int> rcs(R, 0);
-  // one realization: the dense Schur LU inside uses the host threads; several:
-  // one realization per thread
+  // one realization: the Schur complement's columns use the host threads and
+  // a large dense block is factorised on the device; several: one
+  // realization per thread, dense blocks on the host
+  const bool defer = R == 1 && H->sys[0].dense_k >= DLU_MIN_K;
   auto factor_one = [&](int r) {
     CscMatrix A = system_csc(H->sys[r], mv.data());
-    rcs[r] = sparse_lu_factor(A, H->sys[r].colorder, 1.0, LU[r], H->sys[r].dense_k);
+    rcs[r] = sparse_lu_factor(A, H->sys[r].colorder, 1.0, LU[r], H->sys[r].dense_k, defer);
   };
   if (R == 1) {
     factor_one(0);
   } else {
 #pragma omp parallel for schedule(dynamic, 1)
     for (int r = 0; r < R; r++) factor_one(r);
+  }
+  const bool dev_tail = defer && rcs[0] == 0 && !LU[0].schur.empty();
+  if (dev_tail) {
+    const int rc = gpu_dense_lu(H, LU[0]);
+    if (rc != 0 && rc != 3) return rc;
+    rcs[0] = rc;
   }
   for (int r = 0; r < R; r++)
     if (rcs[r]) {
@@ -2660,7 +2945,7 @@ static int factor_all(AndfnHandle *H, const std::vector<double> &mv) {
   LevelParts parts[4];  // lf, lx, ux, ub
   std::vector<std::array<PartOff, 4>> off(R);
   std::vector<std::array<int, 4>> nlev(R), nslots(R), grp(R);
-  std::vector<double> tl, tu, tui;
+  std::vector<double> tl, tui;
   std::vector<size_t> toff(R), tuoff(R);
   std::vector<int> pinv, qcol;
   H->nnz_factors = 0;
@@ -2716,8 +3001,10 @@ static int factor_all(AndfnHandle *H, const std::vector<double> &mv) {
     }
     toff[r] = tl.size();
     tuoff[r] = tui.size();
-    tl.insert(tl.end(), F.l22.begin(), F.l22.end());
-    tu.insert(tu.end(), F.u22.begin(), F.u22.end());
+    if (!dev_tail) {  // L and U (zero diagonals, disjoint parts) in one matrix
+      tl.insert(tl.end(), F.l22.begin(), F.l22.end());
+      for (size_t k = 0; k < F.u22.size(); k++) tl[toff[r] + k] += F.u22[k];
+    }
     tui.insert(tui.end(), F.u_inv_diag.begin() + m0, F.u_inv_diag.end());
     H->sys[r].tail_k = K;
     H->sys[r].nlev_l = nlev[r][0];
@@ -2741,13 +3028,11 @@ static int factor_all(AndfnHandle *H, const std::vector<double> &mv) {
     CK(upload(*dval[k], parts[k].val, s));
   }
   CK(upload(H->ub_scale, parts[3].scale, s));
-  if (tl.empty()) {
-    tl.push_back(0.0);
-    tu.push_back(0.0);
-    tui.push_back(0.0);
+  if (tui.empty()) tui.push_back(0.0);
+  if (!dev_tail) {
+    if (tl.empty()) tl.push_back(0.0);
+    CK(upload(H->tail_l, tl, s));
   }
-  CK(upload(H->tail_l, tl, s));
-  CK(upload(H->tail_u, tu, s));
   CK(upload(H->tail_uinv, tui, s));
   // explicit inverse of a large dense tail of one network, for the cluster
   // path of the discharge solve (applied with one refinement step)
@@ -2757,7 +3042,7 @@ static int factor_all(AndfnHandle *H, const std::vector<double> &mv) {
     CK(H->tail_w.alloc((size_t)K * K));
     const int nc = std::max(1, std::min(DINV_NC, (int)(200 * 1024 / (sizeof(double) * (size_t)K))));
     dense_inverse_kernel<<<(K + nc - 1) / nc, 256, sizeof(double) * (size_t)K * nc, s>>>(
-        H->tail_l.p, H->tail_u.p, H->tail_uinv.p, K, nc, H->tail_w.p);
+        H->tail_l.p, H->tail_l.p, H->tail_uinv.p, K, nc, H->tail_w.p);
     CK(cudaGetLastError());
   }
   CK(upload(H->pinv, pinv, s));
@@ -2781,7 +3066,7 @@ static int factor_all(AndfnHandle *H, const std::vector<double> &mv) {
     }
     td[r].T.K = K;
     td[r].T.L = H->tail_l.p + toff[r];
-    td[r].T.U = H->tail_u.p + toff[r];
+    td[r].T.U = H->tail_l.p + toff[r];
     td[r].T.uinv = H->tail_uinv.p + tuoff[r];
     td[r].T.lscale = nullptr;
     td[r].T.W = want_w ? H->tail_w.p : nullptr;
@@ -3838,7 +4123,7 @@ struct AdjBufs {
   size_t smem = 0;
   // transposed factors
   DBuf<int> lev[4], rows[4], eptr[4], col[4];
-  DBuf<double> val[4], scale0, tl, tu, tones, tlscale, tw;
+  DBuf<double> val[4], scale0, tl, tones, tw;
   DBuf<int> pinv, qcol;
   DBuf<TriDesc> tri;
   int max_nlev = 1;
@@ -4579,23 +4864,20 @@ static int adj_build_factors(AndfnHandle *H) {
     L.group = group;
     A.max_nlev = std::max(A.max_nlev, L.nlev);
   }
-  std::vector<double> tl((size_t)std::max(1, K * K)), tu((size_t)std::max(1, K * K)), ones(std::max(1, K), 1.0),
-      lsc(std::max(1, K), 1.0);
-  for (int j = 0; j < K; j++)
-    for (int i = 0; i < K; i++) {
-      tl[(size_t)j * K + i] = F.u22[(size_t)i * K + j] * F.u_inv_diag[m0 + j];
-      tu[(size_t)j * K + i] = F.l22[(size_t)i * K + j];
-    }
-  for (int i = 0; i < K; i++) lsc[i] = F.u_inv_diag[m0 + i];
-  CK(upload(A.tl, tl, s));
-  CK(upload(A.tu, tu, s));
+  // the forward tail (one network: offset 0) transposed on the device
+  std::vector<double> ones(std::max(1, K), 1.0);
+  CK(A.tl.alloc((size_t)std::max(1, K * K)));
+  if (K > 0) {
+    adj_tail_kernel<<<dim3((K + 31) / 32, (K + 31) / 32), dim3(32, 8), 0, s>>>(H->tail_l.p, H->tail_uinv.p, K,
+                                                                                 A.tl.p);
+    CK(cudaGetLastError());
+  }
   CK(upload(A.tones, ones, s));
-  CK(upload(A.tlscale, lsc, s));
   td.T.K = K;
   td.T.L = A.tl.p;
-  td.T.U = A.tu.p;
+  td.T.U = A.tl.p;
   td.T.uinv = A.tones.p;
-  td.T.lscale = A.tlscale.p;
+  td.T.lscale = H->tail_uinv.p;
   td.T.W = nullptr;
   if (K >= CLUSTER_MIN_K && H->tail_w.p && H->tail_w.n == (size_t)K * K) {  // (L U)^-T = W^T
     CK(A.tw.alloc((size_t)K * K));

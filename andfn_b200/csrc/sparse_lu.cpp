@@ -490,8 +490,10 @@ int sparse_lu_factor(const CscMatrix &A, const std::vector<int> &q, double pivot
 
 int sparse_lu_finish(LuFactors &F, const std::vector<int> &dpiv, const std::vector<double> &tail_diag) {
   if ((int)dpiv.size() != F.dense || (int)tail_diag.size() != F.dense) return 3;
-  for (double d : tail_diag)
+  for (double d : tail_diag) {
     if (!(d != 0.0) || !std::isfinite(d)) return 3;
+    F.pending.min_piv = std::min(F.pending.min_piv, std::fabs(d));
+  }
   const int rc = finish_factors(F, F.pending, dpiv, nullptr, tail_diag.data());
   F.pending = LuPending();
   F.schur.clear();
