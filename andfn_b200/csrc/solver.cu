@@ -1713,6 +1713,264 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 1) trisolve_kernel(Net net, int
 }
 
 // ------------------------------------------------------------------------
+// Explicit inverse of the discharge system of one network
+// ------------------------------------------------------------------------
+// X = (P A Q)^-1 = U^-1 L^-1 in pivot order, row-major with rows padded to
+// ldw (a multiple of 32), formed once per factorisation from the
+// level-ordered factors: the unit lower solve on the identity (one CTA per 32
+// right-hand sides, lane = right-hand side, warps over the rows of a level;
+// L^-1 is lower triangular, so rows and entries left of a CTA's columns are
+// skipped), the dense tail's rows as W22 T with the tail inverse
+// W22 = U22^-1 L22^-1 (one FP64 GEMM), then the upper solve.  A discharge
+// solve is then x0 = Q X P b, r = b - A x0, x = x0 + Q X P r: two streaming
+// passes over X and one over A instead of the level-by-level dependency
+// chain; the refinement step makes the result as accurate as the inverse's
+// condition allows (the triangular solves' own accuracy or better).
+static constexpr int WINV_THREADS = 512;
+static constexpr int WINV_MAX_N = 16384;
+
+// sum over the entries e of slot sl with col(e) >= cmin of val(e) X(col(e), c)
+__device__ __forceinline__ double winv_row_dot(const LevelSolve &F, int sl, const double *X, int ldw, int c,
+                                               int cmin) {
+  const int e0 = __ldg(F.eptr + sl), e1 = __ldg(F.eptr + sl + 1);
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+  int e = e0;
+  for (; e + 3 < e1; e += 4) {
+    const int j0 = __ldg(F.col + e), j1 = __ldg(F.col + e + 1), j2 = __ldg(F.col + e + 2), j3 = __ldg(F.col + e + 3);
+    const double v0 = __ldg(F.val + e), v1 = __ldg(F.val + e + 1), v2 = __ldg(F.val + e + 2),
+                 v3 = __ldg(F.val + e + 3);
+    const double x0 = (j0 >= cmin) ? X[(size_t)j0 * ldw + c] : 0.0;
+    const double x1 = (j1 >= cmin) ? X[(size_t)j1 * ldw + c] : 0.0;
+    const double x2 = (j2 >= cmin) ? X[(size_t)j2 * ldw + c] : 0.0;
+    const double x3 = (j3 >= cmin) ? X[(size_t)j3 * ldw + c] : 0.0;
+    a0 = fma(v0, x0, a0);
+    a1 = fma(v1, x1, a1);
+    a2 = fma(v2, x2, a2);
+    a3 = fma(v3, x3, a3);
+  }
+  for (; e < e1; e++) {
+    const int j = __ldg(F.col + e);
+    if (j >= cmin) a0 = fma(__ldg(F.val + e), X[(size_t)j * ldw + c], a0);
+  }
+  return (a0 + a1) + (a2 + a3);
+}
+
+// X = L^-1 on the leading rows (X zeroed beforehand); T = the trailing rows
+// before the dense tail's solve (K x ldw, row-major).
+__global__ void __launch_bounds__(WINV_THREADS) winv_lower_kernel(TriDesc TD, double *__restrict__ X, int ldw,
+                                                                  double *__restrict__ T) {
+  const int N = TD.n, K = TD.T.K;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int c0 = blockIdx.x * 32, c = c0 + lane;
+  const LevelSolve &F = TD.Lf;
+  for (int l = 0; l < F.nlev; l++) {
+    const int s0 = __ldg(F.lev_ptr + l), s1 = __ldg(F.lev_ptr + l + 1);
+    for (int sl = s0 + warp; sl < s1; sl += nw) {
+      const int i = __ldg(F.rows + sl);
+      if (i < c0) continue;  // X(i, c) = 0 for i < c
+      const double acc = winv_row_dot(F, sl, X, ldw, c, c0);
+      X[(size_t)i * ldw + c] = ((i == c) ? 1.0 : 0.0) - acc;
+    }
+    __syncthreads();
+  }
+  if (K > 0) {
+    const LevelSolve &G = TD.Lx;  // independent rows (entries in the leading columns only)
+    for (int sl = warp; sl < G.nslots; sl += nw) {
+      const int i = __ldg(G.rows + sl);
+      const double acc = winv_row_dot(G, sl, X, ldw, c, c0);
+      T[(size_t)(i - (N - K)) * ldw + c] = ((i == c) ? 1.0 : 0.0) - acc;
+    }
+  }
+}
+
+// C (K x ldw, row-major) = W (K x K, column-major) T (K x ldw, row-major):
+// 64 x 64 tiles, 16-deep slices of W and T in shared memory, 4 x 4 outputs a
+// thread (rows and columns 16 apart, so loads and stores coalesce).
+__global__ void __launch_bounds__(256) winv_gemm_kernel(const double *__restrict__ W, int K,
+                                                        const double *__restrict__ T, int ldw,
+                                                        double *__restrict__ C) {
+  __shared__ double As[16][64], Bs[16][64];
+  const int rb = blockIdx.x * 64, cb = blockIdx.y * 64;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  double acc[4][4];
+#pragma unroll
+  for (int r = 0; r < 4; r++)
+#pragma unroll
+    for (int q = 0; q < 4; q++) acc[r][q] = 0.0;
+  for (int k0 = 0; k0 < K; k0 += 16) {
+    for (int idx = threadIdx.x; idx < 16 * 64; idx += blockDim.x) {
+      const int kk = idx >> 6, i = idx & 63;
+      const bool kv = k0 + kk < K;
+      As[kk][i] = (kv && rb + i < K) ? __ldg(W + (size_t)(k0 + kk) * K + rb + i) : 0.0;
+      Bs[kk][i] = (kv && cb + i < ldw) ? __ldg(T + (size_t)(k0 + kk) * ldw + cb + i) : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < 16; kk++) {
+      double a[4], b[4];
+#pragma unroll
+      for (int r = 0; r < 4; r++) a[r] = As[kk][ty + 16 * r];
+#pragma unroll
+      for (int q = 0; q < 4; q++) b[q] = Bs[kk][tx + 16 * q];
+#pragma unroll
+      for (int r = 0; r < 4; r++)
+#pragma unroll
+        for (int q = 0; q < 4; q++) acc[r][q] = fma(a[r], b[q], acc[r][q]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+    const int i = rb + ty + 16 * r;
+    if (i >= K) continue;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int c = cb + tx + 16 * q;
+      if (c < ldw) C[(size_t)i * ldw + c] = acc[r][q];
+    }
+  }
+}
+
+// X = U^-1 X on the leading rows: coupling to the (final) trailing rows, then
+// the sparse upper levels with 1/U(i,i).
+__global__ void __launch_bounds__(WINV_THREADS) winv_upper_kernel(TriDesc TD, double *__restrict__ X, int ldw) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int c = blockIdx.x * 32 + lane;
+  if (TD.T.K > 0) {
+    const LevelSolve &G = TD.Ux;  // independent rows
+    for (int sl = warp; sl < G.nslots; sl += nw) {
+      const int i = __ldg(G.rows + sl);
+      const double acc = winv_row_dot(G, sl, X, ldw, c, 0);
+      X[(size_t)i * ldw + c] -= acc;
+    }
+    __syncthreads();
+  }
+  const LevelSolve &F = TD.Ub;
+  for (int l = 0; l < F.nlev; l++) {
+    const int s0 = __ldg(F.lev_ptr + l), s1 = __ldg(F.lev_ptr + l + 1);
+    for (int sl = s0 + warp; sl < s1; sl += nw) {
+      const int i = __ldg(F.rows + sl);
+      const double acc = winv_row_dot(F, sl, X, ldw, c, 0);
+      const double sc = F.scale ? __ldg(F.scale + sl) : 1.0;
+      X[(size_t)i * ldw + c] = (X[(size_t)i * ldw + c] - acc) * sc;
+    }
+    __syncthreads();
+  }
+}
+
+// One pass over X: y(k) = sum_j X(k, j) v(j) with v = P src (src in equation
+// order, permuted into pivot order in shared memory), one warp per row k,
+// X streamed past the L2.  STAGE 0: x0(Q k) = y(k) (and the loop counter,
+// as trisolve_kernel counts it).  STAGE 1: x(Q k) = x0(Q k) + y(k), written
+// to the discharges / constants with the max-change error of the solve; the
+// last CTA to finish turns the grid's maxima into error_q.
+template <int STAGE>
+__global__ void __launch_bounds__(WINV_THREADS) winv_gemv_kernel(Net net, const double *__restrict__ X, int ldw,
+                                                                 const double *__restrict__ src,
+                                                                 double *__restrict__ x0,
+                                                                 unsigned long long *__restrict__ acc) {
+  SolveState *st = net.st;
+  if (st->done) return;
+  if (STAGE == 0 && blockIdx.x == 0 && threadIdx.x == 0) {
+    st->nit += 1;
+    acc[0] = 0ull;
+    acc[1] = 0ull;
+    acc[2] = 0ull;
+  }
+  if (!st->solve_q) return;  // uniform: solve_q is written only by reduce_kernel
+  const TriDesc &TD = net.tri[0];
+  const int N = TD.n;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double *v = reinterpret_cast<double *>(smem_raw);
+  for (int i = threadIdx.x; i < N; i += blockDim.x) v[__ldg(TD.pinv + i)] = src[i];
+  for (int i = N + threadIdx.x; i < ldw; i += blockDim.x) v[i] = 0.0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const double2 *vv = reinterpret_cast<const double2 *>(v);
+  const int n2 = ldw / 2;
+  double md = 0.0, mo = 0.0;
+  for (int k = blockIdx.x * nw + warp; k < N; k += gridDim.x * nw) {
+    const double2 *row = reinterpret_cast<const double2 *>(X + (size_t)k * ldw);
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    int j = lane;
+    for (; j + 96 < n2; j += 128) {
+      const double2 w0 = __ldcs(row + j), w1 = __ldcs(row + j + 32), w2 = __ldcs(row + j + 64),
+                    w3 = __ldcs(row + j + 96);
+      const double2 b0 = vv[j], b1 = vv[j + 32], b2 = vv[j + 64], b3 = vv[j + 96];
+      a0 = fma(w0.y, b0.y, fma(w0.x, b0.x, a0));
+      a1 = fma(w1.y, b1.y, fma(w1.x, b1.x, a1));
+      a2 = fma(w2.y, b2.y, fma(w2.x, b2.x, a2));
+      a3 = fma(w3.y, b3.y, fma(w3.x, b3.x, a3));
+    }
+    for (; j < n2; j += 32) {
+      const double2 w0 = __ldcs(row + j), b0 = vv[j];
+      a0 = fma(w0.y, b0.y, fma(w0.x, b0.x, a0));
+    }
+    const double y = warp_sum((a0 + a1) + (a2 + a3));
+    if (lane == 0) {
+      const int cc = __ldg(TD.qcol + k);
+      if (STAGE == 0) {
+        x0[cc] = y;
+      } else {
+        const double xv = x0[cc] + y;
+        const double xo = net.disc[cc];
+        double dd = fabs(xv - xo);
+        if (!(dd == dd)) dd = INFINITY;
+        md = fmax(md, dd);
+        mo = fmax(mo, fabs(xo));
+        net.disc[cc] = xv;
+        const int d = net.row_de[cc];
+        if (d >= 0)
+          net.q[net.de_ids[d]] = xv;
+        else
+          net.constant[net.row_frac[cc]] = xv;
+      }
+    }
+  }
+  if (STAGE == 0) return;
+  __shared__ double s_d[32], s_o[32];
+  __shared__ int s_last;
+  if (lane == 0) {
+    s_d[warp] = md;
+    s_o[warp] = mo;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0, b = 0.0;
+    for (int k = 0; k < nw; k++) {
+      a = fmax(a, s_d[k]);
+      b = fmax(b, s_o[k]);
+    }
+    // non-negative doubles order like their bit patterns
+    atomicMax(acc, (unsigned long long)__double_as_longlong(a));
+    atomicMax(acc + 1, (unsigned long long)__double_as_longlong(b));
+    __threadfence();
+    s_last = atomicAdd(acc + 2, 1ull) == (unsigned long long)(gridDim.x - 1);
+  }
+  __syncthreads();
+  if (s_last && threadIdx.x == 0) {
+    __threadfence();
+    const double a = __longlong_as_double((long long)atomicAdd(acc, 0ull));
+    const double b = __longlong_as_double((long long)atomicAdd(acc + 1, 0ull));
+    st->error_q = a / (b + 1e-16);
+  }
+}
+
+// r = b - A x0 (A's rows in equation order, one warp per row).
+__global__ void winv_resid_kernel(Net net, const int *__restrict__ rp, const int *__restrict__ cols,
+                                  const double *__restrict__ vals, const double *__restrict__ x0,
+                                  double *__restrict__ r, int N) {
+  const SolveState *st = net.st;
+  if (st->done || !st->solve_q) return;
+  const int i = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (i >= N) return;
+  double sum = 0.0;
+  for (int p = __ldg(rp + i) + lane; p < __ldg(rp + i + 1); p += 32) sum = fma(__ldg(vals + p), x0[__ldg(cols + p)], sum);
+  sum = warp_sum(sum);
+  if (lane == 0) r[i] = net.bvec[i] - sum;
+}
+
+// ------------------------------------------------------------------------
 // Setup kernels
 // ------------------------------------------------------------------------
 // numba np.linspace(a, b, D + 2)[1:D+1] (np.divide of a complex by an int is
@@ -2144,6 +2402,14 @@ struct AndfnHandle {
   DBuf<double> tail_l, tail_uinv, tail_w;
   DBuf<int> dlu_i;  // device dense-LU scratch
   DBuf<double> dlu_d;
+  // explicit inverse of a single network's system (pivot order, rows padded
+  // to winv_ldw), the system's CSR pattern and the solve's work arrays
+  DBuf<double> winv, winv_t, wx0, wr;
+  DBuf<int> a_ptr, a_col;
+  DBuf<unsigned long long> wacc;
+  int winv_ldw = 0, num_sms = 148;
+  bool winv_ready = false;
+  bool winv_enabled = true;
   DBuf<int> pinv, qcol;
   DBuf<TriDesc> tri;
   int max_n = 0, max_nlev = 0, max_k = 0;
@@ -2781,6 +3047,10 @@ static int create_impl(AndfnHandle *H, int R, const char *const *F, const int64_
   CK(cudaFuncSetAttribute(trisolve_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
   CK(cudaFuncSetAttribute(dense_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
   CK(cudaFuncSetAttribute(dlu_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DLU_SMEM_MAX));
+  CK(cudaFuncSetAttribute(winv_gemv_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)(sizeof(double) * WINV_MAX_N)));
+  CK(cudaFuncSetAttribute(winv_gemv_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)(sizeof(double) * WINV_MAX_N)));
   CK(cudaFuncSetAttribute(update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
   rc = reset_impl(H);
   if (rc) return rc;
@@ -2906,6 +3176,42 @@ static int gpu_dense_lu(AndfnHandle *H, LuFactors &F) {
   CK(cudaStreamSynchronize(s));
   if (flag[0]) return 3;
   return sparse_lu_finish(F, piv, dg);
+}
+
+// Forms the explicit inverse of a single network's factorised system (its
+// TriDesc, dense-tail inverse in H->tail_w) when the device has room for it,
+// and the CSR pattern of the system for the refinement step.
+static int build_inverse(AndfnHandle *H, const TriDesc &td) {
+  cudaStream_t s = H->stream;
+  const int N = td.n, K = td.T.K, m0 = N - K;
+  const int ldw = (N + 31) / 32 * 32;
+  const size_t xbytes = sizeof(double) * (size_t)N * ldw, tbytes = sizeof(double) * (size_t)std::max(1, K) * ldw;
+  size_t fr = 0, tot = 0;
+  CK(cudaMemGetInfo(&fr, &tot));
+  const size_t have = fr + sizeof(double) * (H->winv.cap + H->winv_t.cap);
+  if (xbytes + tbytes + ((size_t)1 << 30) > have) return 0;  // keep the triangular solves
+  CK(H->winv.alloc((size_t)N * ldw));
+  CK(H->winv_t.alloc((size_t)std::max(1, K) * ldw));
+  CK(cudaMemsetAsync(H->winv.p, 0, xbytes, s));
+  const int nchunk = ldw / 32;
+  winv_lower_kernel<<<nchunk, WINV_THREADS, 0, s>>>(td, H->winv.p, ldw, H->winv_t.p);
+  if (K > 0)
+    winv_gemm_kernel<<<dim3((K + 63) / 64, (ldw + 63) / 64), 256, 0, s>>>(H->tail_w.p, K, H->winv_t.p, ldw,
+                                                                         H->winv.p + (size_t)m0 * ldw);
+  winv_upper_kernel<<<nchunk, WINV_THREADS, 0, s>>>(td, H->winv.p, ldw);
+  CK(cudaGetLastError());
+  H->launches += K > 0 ? 3 : 2;
+  const RealSys &S = H->sys[0];
+  if (H->a_ptr.n != S.mrow_ptr.size() || H->a_col.n != S.mcol.size()) {
+    CK(upload(H->a_ptr, S.mrow_ptr, s));
+    CK(upload(H->a_col, S.mcol, s));
+  }
+  CK(H->wx0.alloc(N));
+  CK(H->wr.alloc(N));
+  CK(H->wacc.alloc(3));
+  H->winv_ldw = ldw;
+  H->winv_ready = true;
+  return 0;
 }
 
 static int factor_all(AndfnHandle *H, const std::vector<double> &mv) {
@@ -3036,7 +3342,8 @@ static int factor_all(AndfnHandle *H, const std::vector<double> &mv) {
   CK(upload(H->tail_uinv, tui, s));
   // explicit inverse of a large dense tail of one network, for the cluster
   // path of the discharge solve (applied with one refinement step)
-  const bool want_w = R == 1 && LU[0].dense >= CLUSTER_MIN_K;
+  const bool want_winv = R == 1 && H->winv_enabled && LU[0].n <= WINV_MAX_N;
+  const bool want_w = R == 1 && LU[0].dense > 0 && (LU[0].dense >= CLUSTER_MIN_K || want_winv);
   if (want_w) {
     const int K = LU[0].dense;
     CK(H->tail_w.alloc((size_t)K * K));
@@ -3076,6 +3383,11 @@ static int factor_all(AndfnHandle *H, const std::vector<double> &mv) {
     td[r].n = n;
   }
   CK(upload(H->tri, td, s));
+  H->winv_ready = false;
+  if (want_winv) {
+    const int rc = build_inverse(H, td[0]);
+    if (rc) return rc;
+  }
   CK(cudaStreamSynchronize(s));
   // the adjoint solves with the transposed factors of a single network
   H->adj_factors_ready = false;
@@ -3159,8 +3471,23 @@ static int build_head_sums(AndfnHandle *H);
 __global__ void head_vector_kernel(Net net, const int *__restrict__ gptr, const int *__restrict__ sidx,
                                    const cd *__restrict__ S);
 
+// Kernels one discharge solve launches.
+static int tri_launches(const AndfnHandle *H) { return H->winv_ready ? 3 : 1; }
+
 static void launch_trisolve(AndfnHandle *H, cudaStream_t s) {
   Net net = H->net();
+  if (H->winv_ready) {
+    const int N = H->N, ldw = H->winv_ldw;
+    const size_t vsm = sizeof(double) * (size_t)ldw;
+    const int grid = 2 * H->num_sms;  // two CTAs of 512 threads per SM
+    winv_gemv_kernel<0><<<grid, WINV_THREADS, vsm, s>>>(net, H->winv.p, ldw, net.bvec, H->wx0.p, H->wacc.p);
+    winv_resid_kernel<<<(N * 32 + 255) / 256, 256, 0, s>>>(net, H->a_ptr.p, H->a_col.p,
+                                                          H->d_mvals.p + H->sys[0].ent0, H->wx0.p, H->wr.p, N);
+    winv_gemv_kernel<1><<<grid, WINV_THREADS, vsm, s>>>(net, H->winv.p, ldw, H->wr.p, H->wx0.p, H->wacc.p);
+    const cudaError_t le = cudaGetLastError();
+    if (le != cudaSuccess) set_error(std::string("explicit-inverse solve launch: ") + cudaGetErrorString(le));
+    return;
+  }
   const size_t ybytes = sizeof(double) * (size_t)H->max_n;
   const int use_smem = ybytes <= 150 * 1024 ? H->max_n : 0;
   const int cap_levptr = std::min(H->max_nlev + 1, 10240);
@@ -3213,7 +3540,7 @@ static int enqueue_iteration(AndfnHandle *H, cudaStream_t s, int blend_mode, int
   mark(H, s, b, K_REDUCE, 0);
   reduce_kernel<<<H->R, 1024, 0, s>>>(net);
   mark(H, s, b, K_REDUCE, 1);
-  H->launches += 5;
+  H->launches += 4 + tri_launches(H);
   return 0;
 }
 
@@ -3248,7 +3575,7 @@ static int run_adaptive(AndfnHandle *H, const AndfnConstants *C) {
     int ngrow = 0;
     CK(cudaMemcpyAsync(&ngrow, H->grow_count.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
-    H->launches += 7;
+    H->launches += 6 + tri_launches(H);
     if (ngrow > 0) {
       std::vector<int> grown(ngrow);
       CK(cudaMemcpy(grown.data(), H->grow_list.p, sizeof(int) * ngrow, cudaMemcpyDeviceToHost));
@@ -3438,7 +3765,7 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
       CK(cudaGraphInstantiate(&H->graph_exec, g, 0));
       cudaGraphDestroy(g);
     }
-    const int per_it = H->use_head_sums ? 5 : 6;  // kernels of one captured iteration
+    const int per_it = (H->use_head_sums ? 4 : 5) + tri_launches(H);  // kernels of one captured iteration
   H->launches -= ITER_BATCH * per_it;           // capture does not launch
     int guard = 0;
     int nit_before = 0;
@@ -3519,6 +3846,7 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
     st.nnz_matrix = (int64_t)H->sys[r].mcol.size();
     st.nnz_factors = H->sys[r].nnz;
     st.dense_tail = H->sys[r].tail_k;
+    st.explicit_inverse = H->winv_ready ? 1 : 0;
     st.levels_l = H->sys[r].nlev_l;
     st.levels_u = H->sys[r].nlev_u;
     for (int i = 0; i < 8; i++) st.tri_cycles[i] = f.tri_cycles[i];
@@ -3686,6 +4014,7 @@ int andfn_b200_batch_create(AndfnHandle **out, int64_t R, void *const *frac_recs
   cudaGetDevice(&H->device);
   cudaDeviceProp prop;
   cudaGetDeviceProperties(&prop, H->device);
+  H->num_sms = prop.multiProcessorCount;
   if (prop.major < 10) {
     delete H;
     set_error("an sm_100 (Blackwell) device is required");
@@ -3702,6 +4031,7 @@ int andfn_b200_batch_create(AndfnHandle **out, int64_t R, void *const *frac_recs
     if (t >= 32 && t <= SOLVE_THREADS && t % 32 == 0) H->solve_threads = t;
   }
   H->D = discharge_int;
+  if (const char *v = getenv("ANDFN_B200_EXPLICIT_INVERSE")) H->winv_enabled = atoi(v) != 0;
   int rc = create_impl(H, (int)R, (const char *const *)frac_recs, nf, (const char *const *)elem_recs, ne);
   if (rc) {
     delete H;

@@ -91,7 +91,8 @@ class AndfnSolveStats(ctypes.Structure):
                 ("h2d_bytes", ctypes.c_int64), ("d2h_bytes", ctypes.c_int64), ("dense_tail", ctypes.c_int64),
                 ("levels_l", ctypes.c_int64), ("levels_u", ctypes.c_int64),
                 ("ms_create_upload", ctypes.c_double), ("ms_create_tables", ctypes.c_double),
-                ("ms_create_order", ctypes.c_double), ("tri_cycles", ctypes.c_int64 * 8)]
+                ("ms_create_order", ctypes.c_double), ("tri_cycles", ctypes.c_int64 * 8),
+                ("explicit_inverse", ctypes.c_int64)]
 
     def as_dict(self) -> dict:
         d = {name: getattr(self, name) for name, _ in self._fields_}

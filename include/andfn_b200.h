@@ -94,6 +94,9 @@ typedef struct AndfnSolveStats {
   int64_t tri_cycles[8]; /* SM cycles of the discharge-solve phases, summed over iterations:
                             head vector, L sparse, L coupling, L dense, U dense,
                             U coupling, U sparse, scatter */
+  int64_t explicit_inverse; /* 1: each discharge solve applied the system's explicit inverse
+                               (formed once per factorisation) with one refinement step;
+                               0: level-scheduled triangular solves */
 } AndfnSolveStats;
 
 /* ---- one-call drop-in (replaces andfn/hpc/hpc_solve.py:55 solve) --------

@@ -52,7 +52,12 @@ def test_batch_matches_reference_golden():
     assert np.array_equal(nets[0][1]["coef"], nets[3][1]["coef"])
 
 
-def test_batch_equals_separate_solves_bitwise():
+def test_batch_equals_separate_solves_bitwise(monkeypatch):
+    """Every realization of a batch runs the same arithmetic as its own
+    single-network solve through the triangular solves (a single network
+    otherwise applies the explicit inverse of its system, a different
+    summation order)."""
+    monkeypatch.setenv("ANDFN_B200_EXPLICIT_INVERSE", "0")
     import andfn_b200
     from andfn_b200.records import default_constants
     recs = _generated(range(1, 9))

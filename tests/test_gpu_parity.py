@@ -121,10 +121,13 @@ def test_heads_10k_points_after_gpu_solve():
     assert np.all(np.abs(hg - ho) <= 1e-9 * np.maximum(1.0, np.abs(ho)))
 
 
-def test_generated_network_matches_oracle_with_dense_tail():
+@pytest.mark.parametrize("inverse", [1, 0])
+def test_generated_network_matches_oracle_with_dense_tail(inverse, monkeypatch):
     """A 551-fracture power-law/Fisher network (N = 1398 unknowns): large
-    enough that the LU has a dense trailing block, which the GPU solves with
-    dense panels.  GPU vs oracle after 3 and 10 iterations."""
+    enough that the LU has a dense trailing block.  Discharge solves through
+    the explicit inverse (1) or the triangular solves with dense panels (0).
+    GPU vs oracle after 3 and 10 iterations."""
+    monkeypatch.setenv("ANDFN_B200_EXPLICIT_INVERSE", str(inverse))
     from andfn_b200 import network as nw
     from andfn_b200.records import default_constants
     from oracle import oracle as orc
@@ -133,17 +136,20 @@ def test_generated_network_matches_oracle_with_dense_tail():
         c = default_constants(MAX_ITERATIONS=its, MAX_ERROR=1e-8, MAX_NCOEF=10)
         F, E = F0.copy(), E0.copy()
         st = _gpu_solve(F, E, 50, c)
-        assert st["dense_tail"] >= 64, st
+        assert st["dense_tail"] >= 64 and st["explicit_inverse"] == inverse, st
         Fo, Eo = F0.copy(), E0.copy()
         orc.solve(Fo, Eo, 50, c)
         _compare(E, F, Eo, Fo, ("generated", its))
 
 
-def test_generated_network_with_cluster_dense_tail_matches_oracle():
-    """A 588-fracture network with a 364-row dense tail (the dense tail runs
-    as a CTA cluster: inverse + one refinement step), 120 iterations (the
+@pytest.mark.parametrize("inverse", [1, 0])
+def test_generated_network_with_cluster_dense_tail_matches_oracle(inverse, monkeypatch):
+    """A 588-fracture network with a 364-row dense tail, 120 iterations (the
     network converges at 146; a fixed count keeps the comparison exact):
-    coefficients vs the oracle."""
+    coefficients vs the oracle, with the explicit inverse of the whole system
+    (1) and with the triangular solves whose dense tail runs as a CTA cluster
+    (tail inverse + one refinement step) (0)."""
+    monkeypatch.setenv("ANDFN_B200_EXPLICIT_INVERSE", str(inverse))
     from andfn_b200 import network as nw
     from andfn_b200.records import default_constants
     from oracle import oracle as orc
@@ -151,7 +157,7 @@ def test_generated_network_with_cluster_dense_tail_matches_oracle():
     c = default_constants(MAX_ITERATIONS=120, MAX_ERROR=1e-300, MAX_NCOEF=10)
     F, E = F0.copy(), E0.copy()
     st = _gpu_solve(F, E, 50, c)
-    assert st["dense_tail"] >= 256 and st["iterations"] == 120, st
+    assert st["dense_tail"] >= 256 and st["iterations"] == 120 and st["explicit_inverse"] == inverse, st
     Fo, Eo = F0.copy(), E0.copy()
     orc.solve(Fo, Eo, 50, c)
     _compare(E, F, Eo, Fo, ("cluster tail", 120))
