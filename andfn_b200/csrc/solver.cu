@@ -1735,6 +1735,25 @@ __device__ __forceinline__ double winv_row_dot(const LevelSolve &F, int sl, cons
   const int e0 = __ldg(F.eptr + sl), e1 = __ldg(F.eptr + sl + 1);
   double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
   int e = e0;
+  for (; e + 7 < e1; e += 8) {  // eight loads of X in flight
+    int j[8];
+    double v[8], x[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      j[u] = __ldg(F.col + e + u);
+      v[u] = __ldg(F.val + e + u);
+    }
+#pragma unroll
+    for (int u = 0; u < 8; u++) x[u] = (j[u] >= cmin) ? X[(size_t)j[u] * ldw + c] : 0.0;
+    a0 = fma(v[0], x[0], a0);
+    a1 = fma(v[1], x[1], a1);
+    a2 = fma(v[2], x[2], a2);
+    a3 = fma(v[3], x[3], a3);
+    a0 = fma(v[4], x[4], a0);
+    a1 = fma(v[5], x[5], a1);
+    a2 = fma(v[6], x[6], a2);
+    a3 = fma(v[7], x[7], a3);
+  }
   for (; e + 3 < e1; e += 4) {
     const int j0 = __ldg(F.col + e), j1 = __ldg(F.col + e + 1), j2 = __ldg(F.col + e + 2), j3 = __ldg(F.col + e + 3);
     const double v0 = __ldg(F.val + e), v1 = __ldg(F.val + e + 1), v2 = __ldg(F.val + e + 2),
@@ -1755,17 +1774,22 @@ __device__ __forceinline__ double winv_row_dot(const LevelSolve &F, int sl, cons
   return (a0 + a1) + (a2 + a3);
 }
 
+// The level kernels give a CTA WINV_CW right-hand sides: each half-warp
+// solves one row of a level for them, so a warp has two rows in flight.
+static constexpr int WINV_CW = 16;
+
 // X = L^-1 on the leading rows (X zeroed beforehand); T = the trailing rows
 // before the dense tail's solve (K x ldw, row-major).
 __global__ void __launch_bounds__(WINV_THREADS) winv_lower_kernel(TriDesc TD, double *__restrict__ X, int ldw,
                                                                   double *__restrict__ T) {
   const int N = TD.n, K = TD.T.K;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const int c0 = blockIdx.x * 32, c = c0 + lane;
+  const int sub = lane / WINV_CW, hw = 2 * warp + sub, nhw = 2 * nw;
+  const int c0 = blockIdx.x * WINV_CW, c = c0 + lane % WINV_CW;
   const LevelSolve &F = TD.Lf;
   for (int l = 0; l < F.nlev; l++) {
     const int s0 = __ldg(F.lev_ptr + l), s1 = __ldg(F.lev_ptr + l + 1);
-    for (int sl = s0 + warp; sl < s1; sl += nw) {
+    for (int sl = s0 + hw; sl < s1; sl += nhw) {
       const int i = __ldg(F.rows + sl);
       if (i < c0) continue;  // X(i, c) = 0 for i < c
       const double acc = winv_row_dot(F, sl, X, ldw, c, c0);
@@ -1775,7 +1799,7 @@ __global__ void __launch_bounds__(WINV_THREADS) winv_lower_kernel(TriDesc TD, do
   }
   if (K > 0) {
     const LevelSolve &G = TD.Lx;  // independent rows (entries in the leading columns only)
-    for (int sl = warp; sl < G.nslots; sl += nw) {
+    for (int sl = hw; sl < G.nslots; sl += nhw) {
       const int i = __ldg(G.rows + sl);
       const double acc = winv_row_dot(G, sl, X, ldw, c, c0);
       T[(size_t)(i - (N - K)) * ldw + c] = ((i == c) ? 1.0 : 0.0) - acc;
@@ -1831,24 +1855,32 @@ __global__ void __launch_bounds__(256) winv_gemm_kernel(const double *__restrict
   }
 }
 
-// X = U^-1 X on the leading rows: coupling to the (final) trailing rows, then
-// the sparse upper levels with 1/U(i,i).
+// X(i, :) -= sum_j U(i, j) X(j, :) for the leading rows i and the (final)
+// trailing rows j: independent rows, so a CTA takes WINV_COUPLE_ROWS rows
+// for one slab of 256 columns (every entry's row of X is read as one
+// coalesced 2 KB slab, mostly from L2).
+static constexpr int WINV_COUPLE_ROWS = 8;
+__global__ void __launch_bounds__(256) winv_coupling_kernel(LevelSolve G, double *__restrict__ X, int ldw) {
+  const int c = blockIdx.y * 256 + threadIdx.x;
+  if (c >= ldw) return;
+  const int s0 = blockIdx.x * WINV_COUPLE_ROWS, s1 = min(G.nslots, s0 + WINV_COUPLE_ROWS);
+  for (int sl = s0; sl < s1; sl++) {
+    const int i = __ldg(G.rows + sl);
+    const double acc = winv_row_dot(G, sl, X, ldw, c, 0);
+    X[(size_t)i * ldw + c] -= acc;
+  }
+}
+
+// X = U^-1 X on the leading rows after the coupling: the sparse upper levels
+// with 1/U(i,i).
 __global__ void __launch_bounds__(WINV_THREADS) winv_upper_kernel(TriDesc TD, double *__restrict__ X, int ldw) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const int c = blockIdx.x * 32 + lane;
-  if (TD.T.K > 0) {
-    const LevelSolve &G = TD.Ux;  // independent rows
-    for (int sl = warp; sl < G.nslots; sl += nw) {
-      const int i = __ldg(G.rows + sl);
-      const double acc = winv_row_dot(G, sl, X, ldw, c, 0);
-      X[(size_t)i * ldw + c] -= acc;
-    }
-    __syncthreads();
-  }
+  const int sub = lane / WINV_CW, hw = 2 * warp + sub, nhw = 2 * nw;
+  const int c = blockIdx.x * WINV_CW + lane % WINV_CW;
   const LevelSolve &F = TD.Ub;
   for (int l = 0; l < F.nlev; l++) {
     const int s0 = __ldg(F.lev_ptr + l), s1 = __ldg(F.lev_ptr + l + 1);
-    for (int sl = s0 + warp; sl < s1; sl += nw) {
+    for (int sl = s0 + hw; sl < s1; sl += nhw) {
       const int i = __ldg(F.rows + sl);
       const double acc = winv_row_dot(F, sl, X, ldw, c, 0);
       const double sc = F.scale ? __ldg(F.scale + sl) : 1.0;
@@ -1859,77 +1891,104 @@ __global__ void __launch_bounds__(WINV_THREADS) winv_upper_kernel(TriDesc TD, do
 }
 
 // One pass over X: y(k) = sum_j X(k, j) v(j) with v = P src (src in equation
-// order, permuted into pivot order in shared memory), one warp per row k,
-// X streamed past the L2.  STAGE 0: x0(Q k) = y(k) (and the loop counter,
-// as trisolve_kernel counts it).  STAGE 1: x(Q k) = x0(Q k) + y(k), written
-// to the discharges / constants with the max-change error of the solve; the
-// last CTA to finish turns the grid's maxima into error_q.
-template <int STAGE>
+// order, permuted into pivot order in shared memory), X streamed past the L2.
+// Each CTA owns a contiguous block of at most WINV_RPC rows; its 16 warps
+// split every row into equal segments, two rows in flight at a time, and the
+// segment sums are added in a fixed order (deterministic).  STAGE 0:
+// x0(Q k) = y(k) (and the loop counter, as trisolve_kernel counts it).
+// STAGE 1: x(Q k) = x0(Q k) + y(k).  The forward pass writes x to the
+// discharges / constants with the max-change error of the solve (the last
+// CTA to finish turns the grid's maxima into error_q); the adjoint (ADJ: X
+// holds the transposed inverse, P and Q those of the transposed system)
+// writes net.disc only.
+static constexpr int WINV_RPC = 64;
+static_assert(WINV_THREADS == 512, "16 warps split each row of X");
+
+template <int STAGE, bool ADJ>
 __global__ void __launch_bounds__(WINV_THREADS) winv_gemv_kernel(Net net, const double *__restrict__ X, int ldw,
                                                                  const double *__restrict__ src,
                                                                  double *__restrict__ x0,
                                                                  unsigned long long *__restrict__ acc) {
   SolveState *st = net.st;
   if (st->done) return;
-  if (STAGE == 0 && blockIdx.x == 0 && threadIdx.x == 0) {
-    st->nit += 1;
-    acc[0] = 0ull;
-    acc[1] = 0ull;
-    acc[2] = 0ull;
+  if (!ADJ) {
+    if (STAGE == 0 && blockIdx.x == 0 && threadIdx.x == 0) {
+      st->nit += 1;
+      acc[0] = 0ull;
+      acc[1] = 0ull;
+      acc[2] = 0ull;
+    }
+    if (!st->solve_q) return;  // uniform: solve_q is written only by reduce_kernel
   }
-  if (!st->solve_q) return;  // uniform: solve_q is written only by reduce_kernel
   const TriDesc &TD = net.tri[0];
   const int N = TD.n;
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ double s_part[WINV_RPC][16];
   double *v = reinterpret_cast<double *>(smem_raw);
   for (int i = threadIdx.x; i < N; i += blockDim.x) v[__ldg(TD.pinv + i)] = src[i];
   for (int i = N + threadIdx.x; i < ldw; i += blockDim.x) v[i] = 0.0;
   __syncthreads();
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const double2 *vv = reinterpret_cast<const double2 *>(v);
-  const int n2 = ldw / 2;
-  double md = 0.0, mo = 0.0;
-  for (int k = blockIdx.x * nw + warp; k < N; k += gridDim.x * nw) {
-    const double2 *row = reinterpret_cast<const double2 *>(X + (size_t)k * ldw);
-    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-    int j = lane;
-    for (; j + 96 < n2; j += 128) {
-      const double2 w0 = __ldcs(row + j), w1 = __ldcs(row + j + 32), w2 = __ldcs(row + j + 64),
-                    w3 = __ldcs(row + j + 96);
-      const double2 b0 = vv[j], b1 = vv[j + 32], b2 = vv[j + 64], b3 = vv[j + 96];
-      a0 = fma(w0.y, b0.y, fma(w0.x, b0.x, a0));
-      a1 = fma(w1.y, b1.y, fma(w1.x, b1.x, a1));
-      a2 = fma(w2.y, b2.y, fma(w2.x, b2.x, a2));
-      a3 = fma(w3.y, b3.y, fma(w3.x, b3.x, a3));
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int rpc = (N + gridDim.x - 1) / gridDim.x;  // <= WINV_RPC (grid size chosen by the host)
+  const int r0 = min(N, (int)blockIdx.x * rpc), r1 = min(N, r0 + rpc);
+  const int seg = ldw / 32;  // double2 per warp and row
+  const double2 *vs = reinterpret_cast<const double2 *>(v) + warp * seg;
+  const double2 zero2 = make_double2(0.0, 0.0);
+  for (int k = r0; k < r1; k += 2) {
+    const bool two = k + 1 < r1;
+    const double2 *ra = reinterpret_cast<const double2 *>(X + (size_t)k * ldw) + warp * seg;
+    const double2 *rb = two ? ra + ldw / 2 : ra;
+    double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0;
+#pragma unroll 2
+    for (int j = lane; j < seg; j += 64) {
+      const bool h = j + 32 < seg;
+      const double2 wa0 = __ldcs(ra + j), wb0 = __ldcs(rb + j);
+      const double2 wa1 = h ? __ldcs(ra + j + 32) : zero2, wb1 = h ? __ldcs(rb + j + 32) : zero2;
+      const double2 x0v = vs[j], x1v = h ? vs[j + 32] : zero2;
+      a0 = fma(wa0.y, x0v.y, fma(wa0.x, x0v.x, a0));
+      b0 = fma(wb0.y, x0v.y, fma(wb0.x, x0v.x, b0));
+      a1 = fma(wa1.y, x1v.y, fma(wa1.x, x1v.x, a1));
+      b1 = fma(wb1.y, x1v.y, fma(wb1.x, x1v.x, b1));
     }
-    for (; j < n2; j += 32) {
-      const double2 w0 = __ldcs(row + j), b0 = vv[j];
-      a0 = fma(w0.y, b0.y, fma(w0.x, b0.x, a0));
-    }
-    const double y = warp_sum((a0 + a1) + (a2 + a3));
+    const double sa = warp_sum(a0 + a1), sb = warp_sum(b0 + b1);
     if (lane == 0) {
-      const int cc = __ldg(TD.qcol + k);
-      if (STAGE == 0) {
-        x0[cc] = y;
-      } else {
-        const double xv = x0[cc] + y;
-        const double xo = net.disc[cc];
-        double dd = fabs(xv - xo);
-        if (!(dd == dd)) dd = INFINITY;
-        md = fmax(md, dd);
-        mo = fmax(mo, fabs(xo));
-        net.disc[cc] = xv;
-        const int d = net.row_de[cc];
-        if (d >= 0)
-          net.q[net.de_ids[d]] = xv;
-        else
-          net.constant[net.row_frac[cc]] = xv;
-      }
+      s_part[k - r0][warp] = sa;
+      if (two) s_part[k + 1 - r0][warp] = sb;
     }
   }
-  if (STAGE == 0) return;
+  __syncthreads();
+  double md = 0.0, mo = 0.0;
+  for (int t = threadIdx.x; t < r1 - r0; t += blockDim.x) {
+    double y = 0.0;
+#pragma unroll
+    for (int w = 0; w < 16; w++) y += s_part[t][w];
+    const int cc = __ldg(TD.qcol + r0 + t);
+    if (STAGE == 0) {
+      x0[cc] = y;
+    } else if (ADJ) {
+      net.disc[cc] = x0[cc] + y;
+    } else {
+      const double xv = x0[cc] + y;
+      const double xo = net.disc[cc];
+      double dd = fabs(xv - xo);
+      if (!(dd == dd)) dd = INFINITY;
+      md = fmax(md, dd);
+      mo = fmax(mo, fabs(xo));
+      net.disc[cc] = xv;
+      const int d = net.row_de[cc];
+      if (d >= 0)
+        net.q[net.de_ids[d]] = xv;
+      else
+        net.constant[net.row_frac[cc]] = xv;
+    }
+  }
+  if (STAGE == 0 || ADJ) return;
   __shared__ double s_d[32], s_o[32];
   __shared__ int s_last;
+  for (int o = 16; o > 0; o >>= 1) {
+    md = fmax(md, __shfl_xor_sync(0xffffffffu, md, o));
+    mo = fmax(mo, __shfl_xor_sync(0xffffffffu, mo, o));
+  }
   if (lane == 0) {
     s_d[warp] = md;
     s_o[warp] = mo;
@@ -1937,7 +1996,7 @@ __global__ void __launch_bounds__(WINV_THREADS) winv_gemv_kernel(Net net, const 
   __syncthreads();
   if (threadIdx.x == 0) {
     double a = 0.0, b = 0.0;
-    for (int k = 0; k < nw; k++) {
+    for (int k = 0; k < 16; k++) {
       a = fmax(a, s_d[k]);
       b = fmax(b, s_o[k]);
     }
@@ -1956,18 +2015,38 @@ __global__ void __launch_bounds__(WINV_THREADS) winv_gemv_kernel(Net net, const 
   }
 }
 
-// r = b - A x0 (A's rows in equation order, one warp per row).
+// r = b - M x0 with M's rows in CSR form (one warp per row): M = A (vals in
+// entry order, map null) or A^T (CSC of A; map gives each entry's index in
+// A's entry order).  The adjoint's state has no solve_q gate.
+template <bool ADJ>
 __global__ void winv_resid_kernel(Net net, const int *__restrict__ rp, const int *__restrict__ cols,
-                                  const double *__restrict__ vals, const double *__restrict__ x0,
-                                  double *__restrict__ r, int N) {
+                                  const int *__restrict__ map, const double *__restrict__ vals,
+                                  const double *__restrict__ x0, double *__restrict__ r, int N) {
   const SolveState *st = net.st;
-  if (st->done || !st->solve_q) return;
+  if (st->done || (!ADJ && !st->solve_q)) return;
   const int i = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
   if (i >= N) return;
   double sum = 0.0;
-  for (int p = __ldg(rp + i) + lane; p < __ldg(rp + i + 1); p += 32) sum = fma(__ldg(vals + p), x0[__ldg(cols + p)], sum);
+  for (int p = __ldg(rp + i) + lane; p < __ldg(rp + i + 1); p += 32)
+    sum = fma(__ldg(vals + (map ? __ldg(map + p) : p)), x0[__ldg(cols + p)], sum);
   sum = warp_sum(sum);
   if (lane == 0) r[i] = net.bvec[i] - sum;
+}
+
+// out (cols x ldo, row-major) = in^T for in (rows x ldi, row-major).
+__global__ void transpose_ld_kernel(const double *__restrict__ in, int ldi, int rows, int cols,
+                                    double *__restrict__ out, int ldo) {
+  __shared__ double tile[32][33];
+  const int rb = blockIdx.y * 32, cb = blockIdx.x * 32;
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const int r = rb + k, c = cb + threadIdx.x;
+    if (r < rows && c < cols) tile[k][threadIdx.x] = in[(size_t)r * ldi + c];
+  }
+  __syncthreads();
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const int c = cb + k, r = rb + threadIdx.x;
+    if (r < rows && c < cols) out[(size_t)c * ldo + r] = tile[threadIdx.x][k];
+  }
 }
 
 // ------------------------------------------------------------------------
@@ -2408,6 +2487,7 @@ struct AndfnHandle {
   DBuf<int> a_ptr, a_col;
   DBuf<unsigned long long> wacc;
   int winv_ldw = 0, num_sms = 148;
+  double ms_fac[4] = {};  // factorisation phases of the last run (see AndfnSolveStats)
   bool winv_ready = false;
   bool winv_enabled = true;
   DBuf<int> pinv, qcol;
@@ -3047,9 +3127,13 @@ static int create_impl(AndfnHandle *H, int R, const char *const *F, const int64_
   CK(cudaFuncSetAttribute(trisolve_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
   CK(cudaFuncSetAttribute(dense_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
   CK(cudaFuncSetAttribute(dlu_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DLU_SMEM_MAX));
-  CK(cudaFuncSetAttribute(winv_gemv_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  CK(cudaFuncSetAttribute(winv_gemv_kernel<0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)(sizeof(double) * WINV_MAX_N)));
-  CK(cudaFuncSetAttribute(winv_gemv_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  CK(cudaFuncSetAttribute(winv_gemv_kernel<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)(sizeof(double) * WINV_MAX_N)));
+  CK(cudaFuncSetAttribute(winv_gemv_kernel<0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)(sizeof(double) * WINV_MAX_N)));
+  CK(cudaFuncSetAttribute(winv_gemv_kernel<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)(sizeof(double) * WINV_MAX_N)));
   CK(cudaFuncSetAttribute(update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
   rc = reset_impl(H);
@@ -3193,14 +3277,18 @@ static int build_inverse(AndfnHandle *H, const TriDesc &td) {
   CK(H->winv.alloc((size_t)N * ldw));
   CK(H->winv_t.alloc((size_t)std::max(1, K) * ldw));
   CK(cudaMemsetAsync(H->winv.p, 0, xbytes, s));
-  const int nchunk = ldw / 32;
+  const int nchunk = ldw / WINV_CW;
   winv_lower_kernel<<<nchunk, WINV_THREADS, 0, s>>>(td, H->winv.p, ldw, H->winv_t.p);
-  if (K > 0)
+  if (K > 0) {
     winv_gemm_kernel<<<dim3((K + 63) / 64, (ldw + 63) / 64), 256, 0, s>>>(H->tail_w.p, K, H->winv_t.p, ldw,
                                                                          H->winv.p + (size_t)m0 * ldw);
+    if (td.Ux.nslots > 0)
+      winv_coupling_kernel<<<dim3((td.Ux.nslots + WINV_COUPLE_ROWS - 1) / WINV_COUPLE_ROWS, (ldw + 255) / 256), 256,
+                             0, s>>>(td.Ux, H->winv.p, ldw);
+  }
   winv_upper_kernel<<<nchunk, WINV_THREADS, 0, s>>>(td, H->winv.p, ldw);
   CK(cudaGetLastError());
-  H->launches += K > 0 ? 3 : 2;
+  H->launches += K > 0 ? 4 : 2;
   const RealSys &S = H->sys[0];
   if (H->a_ptr.n != S.mrow_ptr.size() || H->a_col.n != S.mcol.size()) {
     CK(upload(H->a_ptr, S.mrow_ptr, s));
@@ -3227,18 +3315,24 @@ static int factor_all(AndfnHandle *H, const std::vector<double> &mv) {
     CscMatrix A = system_csc(H->sys[r], mv.data());
     rcs[r] = sparse_lu_factor(A, H->sys[r].colorder, 1.0, LU[r], H->sys[r].dense_k, defer);
   };
+  auto tf0 = std::chrono::steady_clock::now();
   if (R == 1) {
     factor_one(0);
   } else {
 #pragma omp parallel for schedule(dynamic, 1)
     for (int r = 0; r < R; r++) factor_one(r);
   }
+  H->ms_fac[0] = ms_since(tf0);
+  auto tf1 = std::chrono::steady_clock::now();
+  H->ms_fac[1] = H->ms_fac[3] = 0.0;
   const bool dev_tail = defer && rcs[0] == 0 && !LU[0].schur.empty();
   if (dev_tail) {
     const int rc = gpu_dense_lu(H, LU[0]);
     if (rc != 0 && rc != 3) return rc;
     rcs[0] = rc;
+    H->ms_fac[1] = ms_since(tf1);
   }
+  auto tf2 = std::chrono::steady_clock::now();
   for (int r = 0; r < R; r++)
     if (rcs[r]) {
       set_error("discharge system of realization " + std::to_string(r) +
@@ -3347,7 +3441,8 @@ static int factor_all(AndfnHandle *H, const std::vector<double> &mv) {
   if (want_w) {
     const int K = LU[0].dense;
     CK(H->tail_w.alloc((size_t)K * K));
-    const int nc = std::max(1, std::min(DINV_NC, (int)(200 * 1024 / (sizeof(double) * (size_t)K))));
+    // about one CTA per SM (nc columns of the inverse each)
+    const int nc = std::max(1, std::min({DINV_NC, (int)(200 * 1024 / (sizeof(double) * (size_t)K)), K / H->num_sms}));
     dense_inverse_kernel<<<(K + nc - 1) / nc, 256, sizeof(double) * (size_t)K * nc, s>>>(
         H->tail_l.p, H->tail_l.p, H->tail_uinv.p, K, nc, H->tail_w.p);
     CK(cudaGetLastError());
@@ -3384,11 +3479,15 @@ static int factor_all(AndfnHandle *H, const std::vector<double> &mv) {
   }
   CK(upload(H->tri, td, s));
   H->winv_ready = false;
+  CK(cudaStreamSynchronize(s));
+  H->ms_fac[2] = ms_since(tf2);
   if (want_winv) {
+    auto tf3 = std::chrono::steady_clock::now();
     const int rc = build_inverse(H, td[0]);
     if (rc) return rc;
+    CK(cudaStreamSynchronize(s));
+    H->ms_fac[3] = ms_since(tf3);
   }
-  CK(cudaStreamSynchronize(s));
   // the adjoint solves with the transposed factors of a single network
   H->adj_factors_ready = false;
   if (R == 1)
@@ -3474,16 +3573,26 @@ __global__ void head_vector_kernel(Net net, const int *__restrict__ gptr, const 
 // Kernels one discharge solve launches.
 static int tri_launches(const AndfnHandle *H) { return H->winv_ready ? 3 : 1; }
 
+// A discharge solve through the explicit inverse X (forward) or its
+// transpose (ADJ): x0 = Q X P b, r = b - M x0, x = x0 + Q X P r, with M = A
+// or A^T in CSR form (map: value index of each entry, null = entry order).
+template <bool ADJ>
+static void launch_winv_solve(AndfnHandle *H, const Net &net, cudaStream_t s, const double *X, const int *rp,
+                              const int *cols, const int *map) {
+  const int N = H->N, ldw = H->winv_ldw;
+  const size_t vsm = sizeof(double) * (size_t)ldw;
+  // two CTAs of 512 threads per SM, at most WINV_RPC rows per CTA
+  const int grid = std::max(2 * H->num_sms, (N + WINV_RPC - 1) / WINV_RPC);
+  winv_gemv_kernel<0, ADJ><<<grid, WINV_THREADS, vsm, s>>>(net, X, ldw, net.bvec, H->wx0.p, H->wacc.p);
+  winv_resid_kernel<ADJ><<<(N * 32 + 255) / 256, 256, 0, s>>>(net, rp, cols, map, H->d_mvals.p + H->sys[0].ent0,
+                                                             H->wx0.p, H->wr.p, N);
+  winv_gemv_kernel<1, ADJ><<<grid, WINV_THREADS, vsm, s>>>(net, X, ldw, H->wr.p, H->wx0.p, H->wacc.p);
+}
+
 static void launch_trisolve(AndfnHandle *H, cudaStream_t s) {
   Net net = H->net();
   if (H->winv_ready) {
-    const int N = H->N, ldw = H->winv_ldw;
-    const size_t vsm = sizeof(double) * (size_t)ldw;
-    const int grid = 2 * H->num_sms;  // two CTAs of 512 threads per SM
-    winv_gemv_kernel<0><<<grid, WINV_THREADS, vsm, s>>>(net, H->winv.p, ldw, net.bvec, H->wx0.p, H->wacc.p);
-    winv_resid_kernel<<<(N * 32 + 255) / 256, 256, 0, s>>>(net, H->a_ptr.p, H->a_col.p,
-                                                          H->d_mvals.p + H->sys[0].ent0, H->wx0.p, H->wr.p, N);
-    winv_gemv_kernel<1><<<grid, WINV_THREADS, vsm, s>>>(net, H->winv.p, ldw, H->wr.p, H->wx0.p, H->wacc.p);
+    launch_winv_solve<false>(H, net, s, H->winv.p, H->a_ptr.p, H->a_col.p, nullptr);
     const cudaError_t le = cudaGetLastError();
     if (le != cudaSuccess) set_error(std::string("explicit-inverse solve launch: ") + cudaGetErrorString(le));
     return;
@@ -3737,6 +3846,10 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
   rc = factor_all(H, mv);
   if (rc) return rc;
   base.ms_factor = ms_since(t_fac);
+  base.ms_factor_sparse = H->ms_fac[0];
+  base.ms_factor_dense = H->ms_fac[1];
+  base.ms_factor_levels = H->ms_fac[2];
+  base.ms_inverse = H->ms_fac[3];
   // iterations, in graph batches
   auto t_it = std::chrono::steady_clock::now();
   if (growth_possible) {
@@ -4446,6 +4559,11 @@ struct AdjBufs {
   DBuf<double> gq, gC, gd, b, mu;  // [ne], [nf], [N], [N], [N]
   DBuf<double> wsw, gtheta, obar, gd0, hbuf;
   DBuf<cd> V, xin, wv;  // Krylov basis [restart + 1][ne][MC], sweep input and output
+  // transposed explicit inverse (rows padded like the forward one) and A^T
+  // in CSR form (value index of each entry in A's entry order)
+  DBuf<double> xt;
+  DBuf<int> at_ptr, at_col, at_map;
+  bool use_winv = false;
   DBuf<Item> items_sw;
   int n_items_sw = 0;
   DBuf<double> fac;  // [2 n_de] weight of a row side per unit mu
@@ -5209,6 +5327,35 @@ static int adj_build_factors(AndfnHandle *H) {
   td.T.uinv = A.tones.p;
   td.T.lscale = H->tail_uinv.p;
   td.T.W = nullptr;
+  A.use_winv = false;
+  if (H->winv_ready) {  // A^-T = (Q X P)^T: X^T with the transposed system's P and Q
+    const int ldw = H->winv_ldw;
+    size_t fr = 0, tot = 0;
+    CK(cudaMemGetInfo(&fr, &tot));
+    const size_t xbytes = sizeof(double) * (size_t)n * ldw;
+    if (xbytes + ((size_t)1 << 30) <= fr + sizeof(double) * A.xt.cap) {
+      CK(A.xt.alloc((size_t)n * ldw));
+      CK(cudaMemsetAsync(A.xt.p, 0, xbytes, s));
+      transpose_ld_kernel<<<dim3((n + 31) / 32, (n + 31) / 32), dim3(32, 8), 0, s>>>(H->winv.p, ldw, n, n, A.xt.p,
+                                                                                     ldw);
+      CK(cudaGetLastError());
+      const RealSys &S = H->sys[0];
+      std::vector<int> cp(n + 1, 0), ri(S.mcol.size()), mp(S.mcol.size());
+      for (int c : S.mcol) cp[c + 1]++;
+      for (int i = 0; i < n; i++) cp[i + 1] += cp[i];
+      std::vector<int> fill(cp.begin(), cp.end() - 1);
+      for (int rr = 0; rr < n; rr++)
+        for (int p = S.mrow_ptr[rr]; p < S.mrow_ptr[rr + 1]; p++) {
+          const int c = S.mcol[p];
+          ri[fill[c]] = rr;
+          mp[fill[c]++] = p;
+        }
+      CK(upload(A.at_ptr, cp, s));
+      CK(upload(A.at_col, ri, s));
+      CK(upload(A.at_map, mp, s));
+      A.use_winv = true;
+    }
+  }
   if (K >= CLUSTER_MIN_K && H->tail_w.p && H->tail_w.n == (size_t)K * K) {  // (L U)^-T = W^T
     CK(A.tw.alloc((size_t)K * K));
     transpose_kernel<<<dim3((K + 31) / 32, (K + 31) / 32), dim3(32, 8), 0, s>>>(H->tail_w.p, A.tw.p, K);
@@ -5232,6 +5379,11 @@ static int adj_build_factors(AndfnHandle *H) {
 }
 
 static void launch_trisolve_adj(AndfnHandle *H, const Net &net, cudaStream_t s) {
+  if (H->adj->use_winv) {
+    const AdjBufs &A = *H->adj;
+    launch_winv_solve<true>(H, net, s, A.xt.p, A.at_ptr.p, A.at_col.p, A.at_map.p);
+    return;
+  }
   const size_t ybytes = sizeof(double) * (size_t)H->max_n;
   const int use_smem = ybytes <= 150 * 1024 ? H->max_n : 0;
   const int cap_levptr = std::min(H->adj->max_nlev + 1, 10240);
@@ -5245,7 +5397,8 @@ static void launch_trisolve_adj(AndfnHandle *H, const Net &net, cudaStream_t s) 
   launch_trisolve_kernel<true>(H, net, s, H->cluster_adj, solve_smem, use_smem, cap_levptr, meta_cap, ring_cap);
 }
 
-static constexpr int ADJ_SWEEP_LAUNCHES = 9;  // per transposed sweep (3 memsets + 6 kernels)
+// per transposed sweep: 3 memsets + 5 kernels + the transposed discharge solve
+static int adj_sweep_launches(const AndfnHandle *H) { return 8 + (H->adj->use_winv ? 3 : 1); }
 static constexpr int ADJ_RESTART = 40;        // Krylov basis size before a restart
 
 // One transposed sweep at lam = x: gc = Phi_c^T x + b_c^T A^-T (gd + Phi_d^T x),
@@ -5427,7 +5580,7 @@ static int adjoint_impl(AndfnHandle *H, const double *gcoef, int64_t mco, const 
     CK(cudaMemcpyAsync(A.xin.p, x, sizeof(double) * n2, cudaMemcpyDeviceToDevice, s));
     CK(cudaGraphLaunch(A.graph[mode], s));
     matvecs++;
-    launches += ADJ_SWEEP_LAUNCHES;
+    launches += adj_sweep_launches(H);
     return 0;
   };
   double bnorm = 0.0, rel = 1.0;

@@ -92,7 +92,9 @@ class AndfnSolveStats(ctypes.Structure):
                 ("levels_l", ctypes.c_int64), ("levels_u", ctypes.c_int64),
                 ("ms_create_upload", ctypes.c_double), ("ms_create_tables", ctypes.c_double),
                 ("ms_create_order", ctypes.c_double), ("tri_cycles", ctypes.c_int64 * 8),
-                ("explicit_inverse", ctypes.c_int64)]
+                ("explicit_inverse", ctypes.c_int64), ("ms_factor_sparse", ctypes.c_double),
+                ("ms_factor_dense", ctypes.c_double), ("ms_factor_levels", ctypes.c_double),
+                ("ms_inverse", ctypes.c_double)]
 
     def as_dict(self) -> dict:
         d = {name: getattr(self, name) for name, _ in self._fields_}

@@ -365,7 +365,9 @@ def run_gpu(args):
                         "phases_ms": e2e_phases},
                 "gpu_launches": int(launches), "roofline": roof, "kernels_us": {k: (v * 1e3 if v else None) for k, v in per.items()},
                 "kernel_share": {k: kt[k][0] / max(1e-12, sum(v[0] for v in kt.values())) for k in kt},
-                "eval_roofline": ev, "phase_ms": {k: stats[k] for k in ("ms_setup", "ms_factor", "ms_iterate")},
+                "eval_roofline": ev, "phase_ms": {k: stats[k] for k in ("ms_setup", "ms_factor", "ms_factor_sparse",
+                                                                 "ms_factor_dense", "ms_factor_levels",
+                                                                 "ms_inverse", "ms_iterate")},
                 "fp64_peak_tflops": fp64_tflops, "clocks": clk, "cpu_baseline": cpu, "batched": batched,
                 "bc_residual": {"max": resid["bc_max"], "worst_element": int(resid["bc_worst"]),
                                 "element_type": int(E["_type"][resid["bc_worst"]]) if resid["bc_worst"] >= 0 else None,

@@ -97,6 +97,10 @@ typedef struct AndfnSolveStats {
   int64_t explicit_inverse; /* 1: each discharge solve applied the system's explicit inverse
                                (formed once per factorisation) with one refinement step;
                                0: level-scheduled triangular solves */
+  double ms_factor_sparse;  /* ms_factor parts: sparse LU + Schur complement (host),          */
+  double ms_factor_dense;   /*   dense LU of the Schur complement (device, incl. its upload), */
+  double ms_factor_levels;  /*   level-ordered factor tables + dense-tail inverse,            */
+  double ms_inverse;        /*   explicit inverse of the system (device)                      */
 } AndfnSolveStats;
 
 /* ---- one-call drop-in (replaces andfn/hpc/hpc_solve.py:55 solve) --------

@@ -149,12 +149,15 @@ def test_adjoint_matches_oracle_finite_differences():
     assert np.all(err <= 1e-5 * np.abs(ga).max()), (err / np.abs(ga).max(), ga[fracs], gf)
 
 
-def test_adjoint_with_dense_tail_matches_gpu_finite_differences():
+@pytest.mark.parametrize("inverse", [1, 0])
+def test_adjoint_with_dense_tail_matches_gpu_finite_differences(inverse, monkeypatch):
     """A 588-fracture generated network (converges in 146 iterations) whose LU
-    has a 364-row dense tail (the discharge solves then run the dense-tail
-    code as a CTA cluster, forward and transposed): gradient vs central
-    differences of the GPU forward solve on the five largest entries (step
-    1e-4, fixed-iteration forward solves)."""
+    has a 364-row dense tail.  Discharge solves, forward and transposed,
+    through the explicit inverse of the system and its transpose (1) or the
+    triangular solves with the dense tail as a CTA cluster (0): gradient vs
+    central differences of the GPU forward solve on the five largest entries
+    (step 1e-4, fixed-iteration forward solves)."""
+    monkeypatch.setenv("ANDFN_B200_EXPLICIT_INVERSE", str(inverse))
     import torch
     from andfn_b200 import network as nw
     from andfn_b200.adjoint import DFNModel
