@@ -29,6 +29,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/andfn_b200.h"
@@ -1243,6 +1244,7 @@ __global__ void adj_tail_kernel(const double *__restrict__ S, const double *__re
 static constexpr int DLU_NB = 16;
 static constexpr int DLU_THREADS = 1024;
 static constexpr int DLU_MIN_K = 64;
+static constexpr int DLU_MAX_K = 16384;  // int panel indices: K * DLU_NB + K < 2^31
 static constexpr size_t DLU_SMEM_MAX = 220 * 1024;
 
 struct DluScratch {
@@ -1254,36 +1256,38 @@ struct DluScratch {
   int *flag;      // [1] first zero / non-finite pivot column + 1 (0 = none)
 };
 
+// Panel element (i, c) (rows from j0, columns from j0): shared memory
+// row-major with a padded row, or the matrix itself (column-major).
+template <bool SMEM>
+__device__ __forceinline__ int dlu_at(int i, int c, int K) {
+  return SMEM ? i * (DLU_NB + 1) + c : i + c * K;
+}
+
+template <bool SMEM>
 __global__ void __launch_bounds__(DLU_THREADS) dlu_panel_kernel(double *__restrict__ S, int K, int j0, int nb,
-                                                                int use_smem, DluScratch D) {
+                                                                DluScratch D) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double s_wv[32];
   __shared__ int s_wi[32];
   __shared__ int s_piv[DLU_NB];
   const int tid = threadIdx.x, bd = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = bd >> 5;
   const int m = K - j0;
+  double *const Sp = S + (size_t)j0 * K + j0;
   double *P;
-  size_t rs, cs;
-  if (use_smem) {
+  if (SMEM) {
     P = reinterpret_cast<double *>(smem_raw);
-    rs = DLU_NB + 1;
-    cs = 1;
-    for (int idx = tid; idx < m * nb; idx += bd) {
-      const int c = idx / m, i = idx - c * m;
-      P[i * rs + c] = S[(size_t)(j0 + c) * K + j0 + i];
-    }
+    for (int c = 0; c < nb; c++)
+      for (int i = tid; i < m; i += bd) P[dlu_at<true>(i, c, K)] = Sp[i + c * K];
     __syncthreads();
   } else {
-    P = S + (size_t)j0 * K + j0;
-    rs = 1;
-    cs = K;
+    P = Sp;
   }
   for (int jj = 0; jj < nb; jj++) {
     double best = -1.0;
     int bi = m;
     int bad = 0;
     for (int i = jj + tid; i < m; i += bd) {
-      const double v = fabs(P[i * rs + jj * cs]);
+      const double v = fabs(P[dlu_at<SMEM>(i, jj, K)]);
       if (!(v <= DBL_MAX)) bad = 1;
       if (v > best) {
         best = v;
@@ -1326,26 +1330,24 @@ __global__ void __launch_bounds__(DLU_THREADS) dlu_panel_kernel(double *__restri
     __syncthreads();
     const int p = s_piv[jj];
     if (p != jj && tid < nb) {
-      const double a = P[jj * rs + tid * cs], b = P[p * rs + tid * cs];
-      P[jj * rs + tid * cs] = b;
-      P[p * rs + tid * cs] = a;
+      const double a = P[dlu_at<SMEM>(jj, tid, K)], b = P[dlu_at<SMEM>(p, tid, K)];
+      P[dlu_at<SMEM>(jj, tid, K)] = b;
+      P[dlu_at<SMEM>(p, tid, K)] = a;
     }
     __syncthreads();
-    const double piv = P[jj * rs + jj * cs];
+    const double piv = P[dlu_at<SMEM>(jj, jj, K)];
     if (tid == 0) D.diag[j0 + jj] = piv;
     const double inv = (piv != 0.0) ? 1.0 / piv : 0.0;
     for (int i = jj + 1 + tid; i < m; i += bd) {
-      const double l = P[i * rs + jj * cs] * inv;
-      P[i * rs + jj * cs] = l;
-      for (int c = jj + 1; c < nb; c++) P[i * rs + c * cs] = fma(-l, P[jj * rs + c * cs], P[i * rs + c * cs]);
+      const double l = P[dlu_at<SMEM>(i, jj, K)] * inv;
+      P[dlu_at<SMEM>(i, jj, K)] = l;
+      for (int c = jj + 1; c < nb; c++) P[dlu_at<SMEM>(i, c, K)] = fma(-l, P[dlu_at<SMEM>(jj, c, K)], P[dlu_at<SMEM>(i, c, K)]);
     }
     __syncthreads();
   }
-  if (use_smem) {
-    for (int idx = tid; idx < m * nb; idx += bd) {
-      const int c = idx / m, i = idx - c * m;
-      S[(size_t)(j0 + c) * K + j0 + i] = P[i * rs + c];
-    }
+  if (SMEM) {
+    for (int c = 0; c < nb; c++)
+      for (int i = tid; i < m; i += bd) Sp[i + c * K] = P[dlu_at<true>(i, c, K)];
   }
   if (tid == 0) {
     // the panel's interchanges as one permutation of at most 2 nb rows
@@ -2469,6 +2471,10 @@ struct AndfnHandle {
   DBuf<int> d_ent_row, d_ent_src, d_ent_side, d_ent_kind;
   DBuf<double> d_mvals;
   double ms_create_upload = 0, ms_create_tables = 0, ms_create_order = 0;
+  // the column orders are computed on this host thread while the evaluation
+  // tables are built and the first run's device set-up goes on; joined
+  // before the first factorisation (and on destruction)
+  std::thread order_thread;
   DBuf<double> disc, work, bvec;
   DBuf<int> ready;
   // factors of all realizations (level-ordered parts, dense tails, permutations)
@@ -2604,6 +2610,7 @@ struct AndfnHandle {
     return n;
   }
   ~AndfnHandle() {
+    if (order_thread.joinable()) order_thread.join();
     andfn::destroy_adj(adj);
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
     for (auto &b : ev)
@@ -3087,6 +3094,30 @@ static int create_impl(AndfnHandle *H, int R, const char *const *F, const int64_
   CK(H->cut_pos.alloc((size_t)nel * H->cut_cap));
   CK(H->cut_elem.alloc((size_t)nel * H->cut_cap));
   CK(H->cut_sign.alloc((size_t)nel * H->cut_cap));
+  // discharge systems: patterns, then fill-reducing column orders from the
+  // patterns alone, computed once per network (in parallel over
+  // realizations) on a host thread of their own; nothing before the first
+  // factorisation reads them
+  H->sys.assign(R, RealSys());
+  H->ent_row.clear();
+  H->ent_src.clear();
+  H->ent_side.clear();
+  H->ent_kind.clear();
+  for (int r = 0; r < R; r++) build_pattern(H, r);
+  H->order_thread = std::thread([H, R]() {
+    auto tc2 = std::chrono::steady_clock::now();
+#pragma omp parallel for schedule(dynamic, 1) if (R > 1)
+    for (int r = 0; r < R; r++) {
+      CscMatrix P = system_csc(H->sys[r], nullptr);
+      H->sys[r].colorder = column_min_degree_order(P, &H->sys[r].dense_k);
+    }
+    H->ms_create_order = ms_since(tc2);
+  });
+  CK(upload(H->d_ent_row, H->ent_row, s));
+  CK(upload(H->d_ent_src, H->ent_src, s));
+  CK(upload(H->d_ent_side, H->ent_side, s));
+  CK(upload(H->d_ent_kind, H->ent_kind, s));
+  CK(H->d_mvals.alloc(std::max<size_t>(1, H->ent_row.size())));
   H->ms_create_upload = ms_since(tc0);
   auto tc1 = std::chrono::steady_clock::now();
   H->cur_ncoef = h.ncoef;
@@ -3094,26 +3125,6 @@ static int create_impl(AndfnHandle *H, int R, const char *const *F, const int64_
   int rc = build_eval_tables(H);
   if (rc) return rc;
   H->ms_create_tables = ms_since(tc1);
-  // discharge systems: patterns, then fill-reducing column orders from the
-  // patterns alone, computed once per network (in parallel over realizations)
-  H->sys.assign(R, RealSys());
-  H->ent_row.clear();
-  H->ent_src.clear();
-  H->ent_side.clear();
-  H->ent_kind.clear();
-  for (int r = 0; r < R; r++) build_pattern(H, r);
-  CK(upload(H->d_ent_row, H->ent_row, s));
-  CK(upload(H->d_ent_src, H->ent_src, s));
-  CK(upload(H->d_ent_side, H->ent_side, s));
-  CK(upload(H->d_ent_kind, H->ent_kind, s));
-  CK(H->d_mvals.alloc(std::max<size_t>(1, H->ent_row.size())));
-  auto tc2 = std::chrono::steady_clock::now();
-#pragma omp parallel for schedule(dynamic, 1) if (R > 1)
-  for (int r = 0; r < R; r++) {
-    CscMatrix P = system_csc(H->sys[r], nullptr);
-    H->sys[r].colorder = column_min_degree_order(P, &H->sys[r].dense_k);
-  }
-  H->ms_create_order = ms_since(tc2);
   CK(H->disc.alloc(H->N));
   CK(H->work.alloc(H->N));
   CK(H->bvec.alloc(H->N));
@@ -3126,7 +3137,7 @@ static int create_impl(AndfnHandle *H, int R, const char *const *F, const int64_
   CK(cudaFuncSetAttribute(trisolve_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
   CK(cudaFuncSetAttribute(trisolve_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
   CK(cudaFuncSetAttribute(dense_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-  CK(cudaFuncSetAttribute(dlu_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DLU_SMEM_MAX));
+  CK(cudaFuncSetAttribute(dlu_panel_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DLU_SMEM_MAX));
   CK(cudaFuncSetAttribute(winv_gemv_kernel<0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)(sizeof(double) * WINV_MAX_N)));
   CK(cudaFuncSetAttribute(winv_gemv_kernel<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -3246,7 +3257,10 @@ static int gpu_dense_lu(AndfnHandle *H, LuFactors &F) {
     const int nb = std::min(DLU_NB, K - j0), m = K - j0, mt = m - nb;
     const size_t sm = sizeof(double) * (size_t)m * (DLU_NB + 1);
     const int use_smem = sm <= DLU_SMEM_MAX;
-    dlu_panel_kernel<<<1, DLU_THREADS, use_smem ? sm : 0, s>>>(S, K, j0, nb, use_smem, D);
+    if (use_smem)
+      dlu_panel_kernel<true><<<1, DLU_THREADS, sm, s>>>(S, K, j0, nb, D);
+    else
+      dlu_panel_kernel<false><<<1, DLU_THREADS, 0, s>>>(S, K, j0, nb, D);
     if (K > nb) dlu_update_kernel<<<(K - nb + 7) / 8, 256, 0, s>>>(S, K, j0, nb, D);
     if (mt > 0) dlu_gemm_kernel<<<dim3((mt + 63) / 64, (mt + 63) / 64), 256, 0, s>>>(S, K, j0, nb);
   }
@@ -3310,7 +3324,7 @@ static int factor_all(AndfnHandle *H, const std::vector<double> &mv) {
   // one realization: the Schur complement's columns use the host threads and
   // a large dense block is factorised on the device; several: one
   // realization per thread, dense blocks on the host
-  const bool defer = R == 1 && H->sys[0].dense_k >= DLU_MIN_K;
+  const bool defer = R == 1 && H->sys[0].dense_k >= DLU_MIN_K && H->sys[0].dense_k <= DLU_MAX_K;
   auto factor_one = [&](int r) {
     CscMatrix A = system_csc(H->sys[r], mv.data());
     rcs[r] = sparse_lu_factor(A, H->sys[r].colorder, 1.0, LU[r], H->sys[r].dense_k, defer);
@@ -3843,6 +3857,7 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
   base.ms_setup = ms_since(t_setup);
   // factorisation (host)
   auto t_fac = std::chrono::steady_clock::now();
+  if (H->order_thread.joinable()) H->order_thread.join();
   rc = factor_all(H, mv);
   if (rc) return rc;
   base.ms_factor = ms_since(t_fac);

@@ -90,7 +90,9 @@ typedef struct AndfnSolveStats {
   int64_t dense_tail;    /* pivot steps solved as a dense trailing block  */
   int64_t levels_l;      /* dependency levels of the sparse part of L     */
   int64_t levels_u;      /* dependency levels of the sparse part of U     */
-  double ms_create_upload, ms_create_tables, ms_create_order; /* handle creation phases */
+  double ms_create_upload, ms_create_tables, ms_create_order; /* handle creation phases (the column
+                            ordering runs on a host thread of its own, alongside the tables and the first
+                            run's device set-up; ms_create_order is that thread's time) */
   int64_t tri_cycles[8]; /* SM cycles of the discharge-solve phases, summed over iterations:
                             head vector, L sparse, L coupling, L dense, U dense,
                             U coupling, U sparse, scatter */
