@@ -4053,6 +4053,89 @@ static int download_impl(AndfnHandle *H, char *const *F, char *const *E) {
   return 0;
 }
 
+// Complex discharge vector w at points (andfn/hpc/hpc_fracture.py:139-175):
+// the sum over the fracture's intersections and constant-head lines
+// (derivative of the Laurent series and the log term times dchi/dz,
+// hpc_intersection.py:179-225, hpc_const_head_line.py:135-164), bounding
+// circle (derivative of the Taylor series in chi = z / R as the reference
+// writes it, without dchi/dz, hpc_bounding_circle.py:97-115) and wells
+// (hpc_well.py:89-108); impermeable elements do not contribute.
+// With u = 1/chi and P(u) = sum_{k>=1} k c_k u^(k-1), the line term is
+// sg (u^2 P - q u / (2 pi)) * 2 / (1 - u^2) * 2 / (b - a).
+__global__ void points_w_kernel(Net net, const int *__restrict__ frac, const cd *__restrict__ z, int npts,
+                                cd *__restrict__ out_w) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= npts) return;
+  const int f = frac[i];
+  const cd zz = z[i];
+  cd w = mk(0.0, 0.0);
+  for (int k = net.fptr[f]; k < net.fptr[f + 1]; k++) {
+    const int el = net.felem[k];
+    const int ty = net.type[el];
+    const int m = net.ncoef[el];
+    const cd *c = net.coef + (size_t)el * net.MC;
+    if (ty == 0 || ty == 3) {
+      const bool neg = (ty == 0 && net.frac0[el] != f);
+      const double sg = neg ? -1.0 : 1.0;
+      const cd *ep = neg ? net.ep1 + 2 * el : net.ep0 + 2 * el;
+      const cd inv = recip(ep[1] - ep[0]);
+      const cd ab = ep[0] + ep[1];
+      const cd Z = fma_c(2.0 * inv, zz, mk(-(ab.re * inv.re - ab.im * inv.im), -(ab.re * inv.im + ab.im * inv.re)));
+      const cd u = recip(exterior_chi(Z));
+      cd P = mk(0.0, 0.0);
+      if (m >= 2) {
+        P = (double)(m - 1) * c[m - 1];
+        for (int j = m - 2; j >= 1; j--) P = fma_c(P, u, (double)j * c[j]);
+      }
+      const cd u2 = u * u;
+      const cd t = u2 * P - (net.q[el] / (2 * PI)) * u;
+      const cd fac = recip(mk(1.0 - u2.re, -u2.im)) * (4.0 * inv);  // 2 / (1 - u^2) * 2 / (b - a)
+      w = w + (sg * t) * fac;
+    } else if (ty == 1) {
+      const cd chi = (1.0 / net.radius[el]) * zz;
+      cd P = (net.MC > 1) ? c[1] : mk(0.0, 0.0);  // m < 2: the reference reads the record's slot 1
+      if (m >= 2) {
+        P = (double)(m - 1) * c[m - 1];
+        for (int j = m - 2; j >= 1; j--) P = fma_c(P, chi, (double)j * c[j]);
+      }
+      w = w + P;
+    } else if (ty == 2) {
+      const double r = net.radius[el];
+      const cd u = recip((1.0 / r) * (zz - net.center[el]));
+      w = w + (-net.q[el] / (2 * PI * r)) * u;
+    }
+  }
+  out_w[i] = w;
+}
+
+// Complex discharge vectors at the points of realization 0.
+static int eval_w_impl(AndfnHandle *H, const int64_t *frac, const cd *z, int64_t npts, cd *out) {
+  if (npts <= 0) return 0;
+  if (npts > (1LL << 31) - 1) return ANDFN_BAD_INPUT;
+  const int nfr = H->h.foff[1] - H->h.foff[0];
+  std::vector<int> fr(npts);
+  for (int64_t i = 0; i < npts; i++) {
+    if (frac[i] < 0 || frac[i] >= nfr) {
+      set_error("point fracture index out of range");
+      return ANDFN_BAD_INPUT;
+    }
+    fr[i] = (int)frac[i];
+  }
+  cudaStream_t s = H->stream;
+  DBuf<int> dfr;
+  DBuf<cd> dz, dw;
+  CK(dfr.alloc(npts));
+  CK(dz.alloc(npts));
+  CK(dw.alloc(npts));
+  CK(cudaMemcpyAsync(dfr.p, fr.data(), sizeof(int) * npts, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(dz.p, z, sizeof(cd) * npts, cudaMemcpyHostToDevice, s));
+  points_w_kernel<<<(unsigned)((npts + 127) / 128), 128, 0, s>>>(H->net(), dfr.p, dz.p, (int)npts, dw.p);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, dw.p, sizeof(cd) * npts, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return 0;
+}
+
 // Points of realization r (fracture indices local to it).
 static int eval_points_impl(AndfnHandle *H, int64_t r, const int64_t *frac, const double *z, int64_t npts,
                             double *omega, double *head) {
@@ -4275,6 +4358,12 @@ int andfn_b200_eval_omega(AndfnHandle *H, const int64_t *frac, const double *z, 
   if (!H || (npts > 0 && (!frac || !z || !out))) return ANDFN_BAD_INPUT;
   cudaSetDevice(H->device);
   return eval_points_impl(H, 0, frac, z, npts, out, nullptr);
+}
+
+int andfn_b200_eval_w(AndfnHandle *H, const int64_t *frac, const double *z, int64_t npts, double *out) {
+  if (!H || (npts > 0 && (!frac || !z || !out))) return ANDFN_BAD_INPUT;
+  cudaSetDevice(H->device);
+  return eval_w_impl(H, frac, reinterpret_cast<const cd *>(z), npts, reinterpret_cast<cd *>(out));
 }
 
 void andfn_b200_destroy(AndfnHandle *H) {

@@ -132,3 +132,13 @@ class Solver:
                                                    z.ctypes.data_as(ctypes.c_void_p), len(z),
                                                    out.ctypes.data_as(ctypes.c_void_p)))
         return out
+
+    def eval_w(self, frac_idx, z) -> np.ndarray:
+        """Complex discharge vector w_f(z) (andfn/hpc/hpc_fracture.py:139-175)."""
+        frac_idx = np.ascontiguousarray(frac_idx, np.int64)
+        z = np.ascontiguousarray(z, np.complex128)
+        out = np.empty(len(z), np.complex128)
+        _ffi.check(_ffi.lib().andfn_b200_eval_w(self._h, frac_idx.ctypes.data_as(ctypes.c_void_p),
+                                               z.ctypes.data_as(ctypes.c_void_p), len(z),
+                                               out.ctypes.data_as(ctypes.c_void_p)))
+        return out

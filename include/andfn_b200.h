@@ -139,6 +139,12 @@ int andfn_b200_eval_heads(AndfnHandle *h, const int64_t *frac, const double *z,
  * exclude = -1).  out: complex128 [npts]. */
 int andfn_b200_eval_omega(AndfnHandle *h, const int64_t *frac, const double *z,
                           int64_t npts, double *out);
+/* Complex discharge vector w at npts points of fracture frac[i] of a
+ * single-network handle (replaces andfn/hpc/hpc_fracture.py:139-175 calc_w,
+ * exclude = -1; the velocity magnitude of Fracture.calc_velocity,
+ * andfn/fracture.py:481-497, is |w| / aperture).  z, out: complex128 [npts]. */
+int andfn_b200_eval_w(AndfnHandle *h, const int64_t *frac, const double *z,
+                      int64_t npts, double *out);
 void andfn_b200_destroy(AndfnHandle *h);
 
 /* CUDA stream the handle launches on (cudaStream_t as void*). */

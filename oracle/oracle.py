@@ -371,3 +371,79 @@ def bc_residual(fractures, elements):
             res[e] = (psi.max() - psi.min()) / qs
     return {"elem": res, "flux": flux, "h_scale": hs, "q_scale": qs, "bc_max": float(res.max()),
             "flux_max": float(flux.max() / qs)}
+
+
+# ---------------------------------------------------------------------------
+# Flow-field evaluations (test infrastructure: restatements the GPU results
+# are checked against; pure Python, small cases).
+# ---------------------------------------------------------------------------
+def sunflower_spiral(n_in: int, n_bnd: int) -> np.ndarray:
+    """Unit-disc sample points (andfn/hpc/hpc_fracture.py:20-49): n_in points on
+    a golden-angle spiral, r = sqrt((i + 1/2) / n_in), theta = pi (1 + sqrt 5)
+    (i + 1/2), then n_bnd points exp(i theta) at linspace(0, 2 pi, n_bnd)."""
+    idx = np.arange(0, n_in, dtype=np.float64) + 0.5
+    r = np.sqrt(idx / n_in)
+    th = np.pi * (1 + 5 ** 0.5) * idx
+    z = r * np.cos(th) + 1j * r * np.sin(th)
+    return np.concatenate((z, np.exp(1j * np.linspace(0, 2 * np.pi, n_bnd))))
+
+
+def _line_chi(z, ep):
+    # andfn/hpc/hpc_geometry_functions.py:12-31
+    big_z = (2 * z - ep[0] - ep[1]) / (ep[1] - ep[0])
+    return big_z + np.sqrt(big_z - 1) * np.sqrt(big_z + 1)
+
+
+def _asym_d1(chi, coef):
+    # andfn/hpc/hpc_math_functions.py:76-100: d/dchi sum_k c_k chi^-k
+    res = 0j
+    n = len(coef)
+    for k in range(n):
+        res -= coef[n - k - 1] * (n - k - 1)
+        res /= chi
+    return res
+
+
+def _taylor_d1(chi, coef):
+    # andfn/hpc/hpc_math_functions.py:164-190: d/dchi sum_k c_k chi^k
+    res = 0j
+    n = len(coef)
+    for k in range(n - 2):
+        res += coef[n - k - 1] * (n - k - 1)
+        res *= chi
+    return res + coef[1]
+
+
+def calc_w(fractures, elements, f: int, z: complex) -> complex:
+    """Complex discharge vector of fracture f at z (andfn/hpc/hpc_fracture.py:139-175):
+    the sum over its intersections (hpc_intersection.py:179-225, the second
+    fracture's side with -coef, +q/(2 pi chi) and its own endpoints), bounding
+    circle (hpc_bounding_circle.py:97-115: derivative of the Taylor series in
+    chi = z / R, no chain-rule factor, center ignored), wells (hpc_well.py:89-108)
+    and constant-head lines (hpc_const_head_line.py:135-164); impermeable
+    elements do not contribute."""
+    fr = fractures[f]
+    w = 0j
+    for k in range(int(fr["nelements"])):
+        el = elements[int(fr["elements"][k])]
+        t = int(el["_type"])
+        if t == 0 or t == 3:
+            side1 = t == 0 and int(fr["_id"]) != int(el["frac0"])
+            ep = el["endpoints1"] if side1 else el["endpoints0"]
+            chi = complex(_line_chi(complex(z), ep))
+            c = el["coef"][: int(el["ncoef"])]
+            if side1:
+                ww = -_asym_d1(chi, -c) + el["q"] / (2 * np.pi * chi)
+            else:
+                ww = -_asym_d1(chi, c) - el["q"] / (2 * np.pi * chi)
+            ww *= 2 * chi ** 2 / (chi ** 2 - 1) * 2 / (ep[1] - ep[0])
+        elif t == 1:
+            chi = complex(z) / el["radius"]
+            ww = _taylor_d1(chi, el["coef"][: int(el["ncoef"])])
+        elif t == 2:
+            chi = (complex(z) - el["center"]) / el["radius"]
+            ww = -el["q"] / (2 * np.pi * chi) / el["radius"]
+        else:
+            continue
+        w += ww
+    return complex(w)
