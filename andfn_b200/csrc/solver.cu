@@ -4656,6 +4656,16 @@ struct AdjState {
   SolveState s;
 };
 
+// GMRES cycle state of the adjoint on the device (see gm_givens_kernel).
+static constexpr int GM_MK = 40;  // Krylov basis size before a restart
+struct GmresDev {
+  int j, stop, k, nonfinite;
+  long long matvecs, max_it;
+  double bnorm, tol, rel, scale;
+  double cs[GM_MK], sn[GM_MK], gv[GM_MK + 1];
+  double Hm[(GM_MK + 1) * GM_MK];  // row-major (GM_MK + 1) x GM_MK
+};
+
 struct AdjBufs {
   DBuf<AdjState> st;
   DBuf<SolveState> st_eval;
@@ -4663,6 +4673,8 @@ struct AdjBufs {
   DBuf<double> gq, gC, gd, b, mu;  // [ne], [nf], [N], [N], [N]
   DBuf<double> wsw, gtheta, obar, gd0, hbuf;
   DBuf<cd> V, xin, wv;  // Krylov basis [restart + 1][ne][MC], sweep input and output
+  DBuf<GmresDev> gm;    // GMRES cycle state
+  cudaGraphExec_t step_graph = nullptr;  // one Arnoldi step
   // transposed explicit inverse (rows padded like the forward one) and A^T
   // in CSR form (value index of each entry in A's entry order)
   DBuf<double> xt;
@@ -4683,6 +4695,7 @@ struct AdjBufs {
   ~AdjBufs() {
     for (auto g : graph)
       if (g) cudaGraphExecDestroy(g);
+    if (step_graph) cudaGraphExecDestroy(step_graph);
   }
 };
 
@@ -5156,6 +5169,123 @@ __global__ void vec_scale_kernel(const double *w, double *out, double a, long lo
     out[k] = a * w[k];
 }
 
+// ---------------------------------------------------------------------------
+// GMRES cycle state on the device.  One Arnoldi step (basis copy, transposed
+// sweep, two classical Gram-Schmidt passes, norm, Givens update, scaling) is
+// one captured graph whose kernels read the step index j and the stop flag
+// from here, so the host launches several steps between synchronisations;
+// the steps after a stop return at entry (the sweep's kernels through the
+// adjoint state's done flag, which the Givens kernel sets with stop).
+
+// Start of a cycle: V_0 = r / beta was written by the host; j = 0.
+__global__ void gm_reset_kernel(GmresDev *g, AdjState *as, double beta, double bnorm, double tol,
+                                long long matvecs, long long max_it) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  g->j = 0;
+  g->stop = 0;
+  g->k = 0;
+  g->nonfinite = 0;
+  g->matvecs = matvecs;
+  g->max_it = max_it;
+  g->bnorm = bnorm;
+  g->tol = tol;
+  g->rel = beta / bnorm;
+  g->scale = 0.0;
+  for (int i = 0; i <= GM_MK; i++) g->gv[i] = 0.0;
+  g->gv[0] = beta;
+  as->s.done = 0;
+}
+
+// xin = V_j
+__global__ void gm_copy_kernel(const GmresDev *g, const double *__restrict__ V, double *__restrict__ xin, long long n) {
+  if (g->stop) return;
+  const double *v = V + (size_t)g->j * n;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+    xin[k] = v[k];
+}
+
+// h[i] += <V_i, w> for i <= j (nv1: one vector only, V itself)
+__global__ void gm_mdot_kernel(const GmresDev *g, const double *__restrict__ V, long long stride, int nv1,
+                               const double *__restrict__ w, long long n, double *h) {
+  if (g->stop) return;
+  __shared__ double red[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nv = nv1 ? 1 : g->j + 1;
+  for (int i = 0; i < nv; i++) {
+    const double *v = V + (size_t)i * stride;
+    double acc = 0.0;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+      acc = fma(v[k], w[k], acc);
+    acc = warp_sum(acc);
+    if (lane == 0) red[warp] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int k = 0; k < (int)(blockDim.x >> 5); k++) t += red[k];
+      atomicAdd(&h[i], t);
+    }
+    __syncthreads();
+  }
+}
+
+// w -= sum_{i <= j} h[i] V_i
+__global__ void gm_update_kernel(const GmresDev *g, double *w, const double *__restrict__ V, long long stride,
+                                 const double *__restrict__ h, long long n) {
+  if (g->stop) return;
+  const int nv = g->j + 1;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    double acc = 0.0;
+    for (int i = 0; i < nv; i++) acc = fma(h[i], V[(size_t)i * stride + k], acc);
+    w[k] -= acc;
+  }
+}
+
+// Hessenberg column j from the two Gram-Schmidt passes (hd[0..], hd[GM_MK + 2 ..])
+// and |w|^2 (hd[2 GM_MK + 3]), the previous rotations, a new one zeroing
+// H(j+1, j), the residual estimate, and the decision to stop the cycle.
+__global__ void gm_givens_kernel(GmresDev *g, const double *hd, AdjState *as) {
+  if (threadIdx.x != 0 || blockIdx.x != 0 || g->stop) return;
+  const int j = g->j;
+  g->matvecs += 1;
+  const double hn = sqrt(hd[2 * (GM_MK + 2) - 1]);
+  double *Hm = g->Hm;
+  for (int i = 0; i <= j; i++) Hm[i * GM_MK + j] = hd[i] + hd[GM_MK + 2 + i];
+  Hm[(j + 1) * GM_MK + j] = hn;
+  for (int i = 0; i < j; i++) {
+    const double a = Hm[i * GM_MK + j], b = Hm[(i + 1) * GM_MK + j];
+    Hm[i * GM_MK + j] = g->cs[i] * a + g->sn[i] * b;
+    Hm[(i + 1) * GM_MK + j] = -g->sn[i] * a + g->cs[i] * b;
+  }
+  const double a = Hm[j * GM_MK + j], b = hn;
+  const double r = hypot(a, b);
+  g->cs[j] = r > 0 ? a / r : 1.0;
+  g->sn[j] = r > 0 ? b / r : 0.0;
+  Hm[j * GM_MK + j] = r;
+  Hm[(j + 1) * GM_MK + j] = 0.0;
+  g->gv[j + 1] = -g->sn[j] * g->gv[j];
+  g->gv[j] = g->cs[j] * g->gv[j];
+  g->k = j + 1;
+  const bool bad = !isfinite(hn) || !isfinite(g->gv[j + 1]);
+  g->rel = fabs(g->gv[j + 1]) / g->bnorm;
+  g->scale = hn > 0.0 ? 1.0 / hn : 0.0;
+  if (bad || g->rel <= g->tol || g->matvecs >= g->max_it || hn == 0.0 || j + 1 == GM_MK) {
+    g->nonfinite = bad ? 1 : 0;
+    g->stop = 1;
+    as->s.done = 1;
+  } else {
+    g->j = j + 1;
+  }
+}
+
+// V_{j+1} = w / |w| (j already advanced)
+__global__ void gm_scale_kernel(const GmresDev *g, const double *__restrict__ w, double *V, long long n) {
+  if (g->stop) return;
+  double *v = V + (size_t)g->j * n;
+  const double a = g->scale;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+    v[k] = a * w[k];
+}
+
 // lam^T Phi_theta: for every intersection, sum_j>=1 lam_j.re (Re a0_j + Re a1_j)
 // times t0 t1 / (t0 + t1)^2, added to theta of frac0 and subtracted from
 // theta of frac1 (a0, a1: the DFTs of the two sides' values at convergence).
@@ -5503,7 +5633,7 @@ static void launch_trisolve_adj(AndfnHandle *H, const Net &net, cudaStream_t s) 
 
 // per transposed sweep: 3 memsets + 5 kernels + the transposed discharge solve
 static int adj_sweep_launches(const AndfnHandle *H) { return 8 + (H->adj->use_winv ? 3 : 1); }
-static constexpr int ADJ_RESTART = 40;        // Krylov basis size before a restart
+static constexpr int ADJ_RESTART = GM_MK;     // Krylov basis size before a restart
 
 // One transposed sweep at lam = x: gc = Phi_c^T x + b_c^T A^-T (gd + Phi_d^T x),
 // then y = (I - T^T) x (mode 0, gd = 0) or y = F(x) - x (mode 1, the real dJ/dd).
@@ -5670,6 +5800,38 @@ static int adjoint_impl(AndfnHandle *H, const double *gcoef, int64_t mco, const 
   double *wv = reinterpret_cast<double *>(A.wv.p);
   double *hd = A.hbuf.p;
   const int vb = 4 * 148, vt = 256;
+  // one Arnoldi step as a graph (its kernels read j and stop from A.gm)
+  CK(A.gm.alloc(1));
+  if (A.step_graph) {
+    cudaGraphExecDestroy(A.step_graph);
+    A.step_graph = nullptr;
+  }
+  {
+    GmresDev *gd = A.gm.p;
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    gm_copy_kernel<<<vb, vt, 0, s>>>(gd, V, reinterpret_cast<double *>(A.xin.p), n2);
+    adj_enqueue_sweep(H, net, net_t, s, A.xin.p, A.gd0.p, A.wv.p, 0);
+    cudaMemsetAsync(hd, 0, sizeof(double) * 2 * (GM_MK + 2), s);
+    for (int pass = 0; pass < 2; pass++) {
+      double *hp = hd + pass * (GM_MK + 2);
+      gm_mdot_kernel<<<vb, vt, 0, s>>>(gd, V, n2, 0, wv, n2, hp);
+      gm_update_kernel<<<vb, vt, 0, s>>>(gd, wv, V, n2, hp, n2);
+    }
+    gm_mdot_kernel<<<vb, vt, 0, s>>>(gd, wv, 0, 1, wv, n2, hd + 2 * (GM_MK + 2) - 1);
+    gm_givens_kernel<<<1, 32, 0, s>>>(gd, hd, A.st.p);
+    gm_scale_kernel<<<vb, vt, 0, s>>>(gd, wv, V, n2);
+    const cudaError_t ec = cudaStreamEndCapture(s, &g);
+    if (ec != cudaSuccess) {
+      set_error(std::string("capture of the Arnoldi step: ") + cudaGetErrorString(ec));
+      return ANDFN_CUDA_ERROR;
+    }
+    CK(cudaGraphInstantiate(&A.step_graph, g, 0));
+    cudaGraphDestroy(g);
+  }
+  // kernels of one Arnoldi step: copy + sweep + memset + 5 + Givens + scale
+  const int step_launches = 1 + adj_sweep_launches(H) + 1 + 5 + 2;
+  constexpr int STEPS_PER_SYNC = 8;
   int64_t matvecs = 0, launches = 4;
   // |w|^2 on the device into hd[0], read back
   auto norm2_of = [&](const double *w, double &out) -> int {
@@ -5689,7 +5851,7 @@ static int adjoint_impl(AndfnHandle *H, const double *gcoef, int64_t mco, const 
   };
   double bnorm = 0.0, rel = 1.0;
   int nonfinite = 0;
-  std::vector<double> Hm((size_t)(mk_ + 1) * mk_), cs(mk_), sn(mk_), gv(mk_ + 1), hh(2 * (mk_ + 2));
+  std::vector<double> Hm((size_t)(mk_ + 1) * mk_), gv(mk_ + 1);
   while (true) {
     // residual r = F(x) - x
     if (sweep(reinterpret_cast<const double *>(A.lam.p), 1)) return ANDFN_CUDA_ERROR;
@@ -5708,48 +5870,34 @@ static int adjoint_impl(AndfnHandle *H, const double *gcoef, int64_t mco, const 
     rel = beta / bnorm;
     if (rel <= tol || matvecs >= max_it) break;
     vec_scale_kernel<<<vb, vt, 0, s>>>(wv, V, 1.0 / beta, n2);
-    std::fill(gv.begin(), gv.end(), 0.0);
-    gv[0] = beta;
-    int k = 0;
-    for (int j = 0; j < mk_; j++) {
-      if (sweep(V + (size_t)j * n2, 0)) return ANDFN_CUDA_ERROR;
-      CK(cudaMemsetAsync(hd, 0, sizeof(double) * 2 * (mk_ + 2), s));
-      for (int pass = 0; pass < 2; pass++) {
-        double *hp = hd + pass * (mk_ + 2);
-        vec_mdot_kernel<<<vb, vt, 0, s>>>(V, n2, j + 1, wv, n2, hp);
-        vec_update_kernel<<<vb, vt, 0, s>>>(wv, V, n2, j + 1, hp, -1.0, n2);
-      }
-      vec_mdot_kernel<<<vb, vt, 0, s>>>(wv, 0, 1, wv, n2, hd + 2 * (mk_ + 2) - 1);
-      launches += 5;
-      CK(cudaMemcpyAsync(hh.data(), hd, sizeof(double) * 2 * (mk_ + 2), cudaMemcpyDeviceToHost, s));
+    gm_reset_kernel<<<1, 32, 0, s>>>(A.gm.p, A.st.p, beta, bnorm, tol, matvecs, max_it);
+    launches += 2;
+    // Arnoldi steps in batches; the device stops the cycle
+    GmresDev gh;
+    for (int done_steps = 0; done_steps < mk_;) {
+      const int nb = std::min(STEPS_PER_SYNC, mk_ - done_steps);
+      for (int b = 0; b < nb; b++) CK(cudaGraphLaunch(A.step_graph, s));
+      launches += (int64_t)nb * step_launches;
+      done_steps += nb;
+      CK(cudaMemcpyAsync(&gh, A.gm.p, sizeof(GmresDev), cudaMemcpyDeviceToHost, s));
       CK(cudaStreamSynchronize(s));
-      const double hn = std::sqrt(hh[2 * (mk_ + 2) - 1]);
-      for (int i = 0; i <= j; i++) Hm[(size_t)i * mk_ + j] = hh[i] + hh[mk_ + 2 + i];
-      Hm[(size_t)(j + 1) * mk_ + j] = hn;
-      // previous rotations, then a new one that zeroes H(j+1, j)
-      for (int i = 0; i < j; i++) {
-        const double a = Hm[(size_t)i * mk_ + j], b = Hm[(size_t)(i + 1) * mk_ + j];
-        Hm[(size_t)i * mk_ + j] = cs[i] * a + sn[i] * b;
-        Hm[(size_t)(i + 1) * mk_ + j] = -sn[i] * a + cs[i] * b;
-      }
-      const double a = Hm[(size_t)j * mk_ + j], b = hn;
-      const double r = std::hypot(a, b);
-      cs[j] = r > 0 ? a / r : 1.0;
-      sn[j] = r > 0 ? b / r : 0.0;
-      Hm[(size_t)j * mk_ + j] = r;
-      Hm[(size_t)(j + 1) * mk_ + j] = 0.0;
-      gv[j + 1] = -sn[j] * gv[j];
-      gv[j] = cs[j] * gv[j];
-      k = j + 1;
-      if (!std::isfinite(hn) || !std::isfinite(gv[j + 1])) {
-        nonfinite = 1;
-        break;
-      }
-      rel = std::fabs(gv[j + 1]) / bnorm;
-      if (hn > 0.0) vec_scale_kernel<<<vb, vt, 0, s>>>(wv, V + (size_t)(j + 1) * n2, 1.0 / hn, n2);
-      if (rel <= tol || matvecs >= max_it || hn == 0.0) break;
+      if (gh.stop) break;
     }
-    if (nonfinite) break;
+    matvecs = gh.matvecs;
+    rel = gh.rel;
+    const int k = gh.k;
+    if (gh.nonfinite) {
+      nonfinite = 1;
+      break;
+    }
+    for (int i = 0; i <= k && i <= mk_; i++) gv[i] = gh.gv[i];
+    for (int i = 0; i < k; i++)
+      for (int c = 0; c < k; c++) Hm[(size_t)i * mk_ + c] = gh.Hm[i * GM_MK + c];
+    // the sweeps of the next cycle (or the final residual) run again
+    {
+      const int zero = 0;
+      CK(cudaMemcpyAsync(&A.st.p->s.done, &zero, sizeof(int), cudaMemcpyHostToDevice, s));
+    }
     // x += V y, H y = g (upper triangular k x k)
     std::vector<double> y(k, 0.0);
     for (int i = k - 1; i >= 0; i--) {
