@@ -76,23 +76,39 @@ std::vector<int> column_min_degree_order(const CscMatrix &A, int *dense_tail, do
     std::sort(Ei[j].begin(), Ei[j].end());
     Ei[j].erase(std::unique(Ei[j].begin(), Ei[j].end()), Ei[j].end());
   }
-  std::vector<char> elem_active(2 * (size_t)n + 1, 0), alive(n, 1);
-  for (int r = 0; r < n; r++) elem_active[r] = !Le[r].empty();
-  std::vector<int> mark(n, -1), wstamp(2 * (size_t)n + 1, -1), w(2 * (size_t)n + 1, 0);
-  DegreeBuckets queue(n);
-  // Exact initial degree |union of row cliques containing j| - 1.
-  for (int j = 0; j < n; j++) {
-    int d = 0;
-    for (int e : Ei[j])
-      for (int v : Le[e])
-        if (v != j && mark[v] != j) {
-          mark[v] = j;
-          d++;
-        }
-    queue.insert(j, std::min(d, n - 1));
+  // per element: the stamp and value of w (below), its list length and
+  // whether it is active, side by side (one cache line per visit)
+  struct ElemInfo {
+    int stamp, w, len, active;
+  };
+  std::vector<ElemInfo> ei(2 * (size_t)n + 1, ElemInfo{-1, 0, 0, 0});
+  std::vector<char> alive(n, 1);
+  for (int r = 0; r < n; r++) {
+    ei[r].active = !Le[r].empty();
+    ei[r].len = (int)Le[r].size();
   }
+  std::vector<int> mark(n, -1);
+  DegreeBuckets queue(n);
+  // Exact initial degree |union of row cliques containing j| - 1 (columns in
+  // parallel, each thread with its own marks), inserted in column order.
+  std::vector<int> deg0(n);
+#pragma omp parallel
+  {
+    std::vector<int> mk(n, -1);
+#pragma omp for schedule(static, 64)
+    for (int j = 0; j < n; j++) {
+      int d = 0;
+      for (int e : Ei[j])
+        for (int v : Le[e])
+          if (v != j && mk[v] != j) {
+            mk[v] = j;
+            d++;
+          }
+      deg0[j] = std::min(d, n - 1);
+    }
+  }
+  for (int j = 0; j < n; j++) queue.insert(j, deg0[j]);
   queue.mindeg = 0;
-  std::fill(mark.begin(), mark.end(), -1);
 
   std::vector<int> order;
   order.reserve(n);
@@ -120,13 +136,13 @@ std::vector<int> column_min_degree_order(const CscMatrix &A, int *dense_tail, do
     stamp++;
     Lp.clear();
     for (int e : Ei[p]) {
-      if (!elem_active[e]) continue;
+      if (!ei[e].active) continue;
       for (int v : Le[e])
         if (v != p && alive[v] && mark[v] != stamp) {
           mark[v] = stamp;
           Lp.push_back(v);
         }
-      elem_active[e] = 0;  // absorbed into the new element
+      ei[e].active = 0;  // absorbed into the new element
       std::vector<int>().swap(Le[e]);
     }
     std::vector<int>().swap(Ei[p]);
@@ -134,28 +150,29 @@ std::vector<int> column_min_degree_order(const CscMatrix &A, int *dense_tail, do
     if (Lp.empty()) continue;
     std::sort(Lp.begin(), Lp.end());
     Le[ne] = Lp;
-    elem_active[ne] = 1;
+    ei[ne].active = 1;
+    ei[ne].len = (int)Lp.size();
     const int lp = (int)Lp.size();
-    // Prune absorbed elements from the neighbours' lists, add the new one.
+    // Prune absorbed elements from the neighbours' lists and add the new one;
+    // w(e) = |Le \ Lp| for every other element touching Lp (one pass).
+    const int wst = k;
     for (int i : Lp) {
       auto &E = Ei[i];
       size_t o = 0;
-      for (size_t a = 0; a < E.size(); a++)
-        if (elem_active[E[a]]) E[o++] = E[a];
+      for (size_t a = 0; a < E.size(); a++) {
+        const int e = E[a];
+        ElemInfo &x = ei[e];
+        if (!x.active) continue;
+        E[o++] = e;
+        if (x.stamp != wst) {
+          x.stamp = wst;
+          x.w = x.len;
+        }
+        x.w -= 1;
+      }
       E.resize(o);
       E.push_back(ne);
     }
-    // w(e) = |Le \ Lp| for every other element touching Lp.
-    int wst = k;
-    for (int i : Lp)
-      for (int e : Ei[i]) {
-        if (e == ne) continue;
-        if (wstamp[e] != wst) {
-          wstamp[e] = wst;
-          w[e] = (int)Le[e].size();
-        }
-        w[e] -= 1;
-      }
     // Aggressive absorption of elements contained in Lp, then degrees.
     const int rem = n - k - 1;
     for (int i : Lp) {
@@ -164,16 +181,17 @@ std::vector<int> column_min_degree_order(const CscMatrix &A, int *dense_tail, do
       long d = lp - 1;
       for (size_t a = 0; a < E.size(); a++) {
         int e = E[a];
-        if (e != ne && wstamp[e] == wst && w[e] == 0) {
-          if (elem_active[e]) {
-            elem_active[e] = 0;
+        ElemInfo &x = ei[e];
+        if (e != ne && x.stamp == wst && x.w == 0) {
+          if (x.active) {
+            x.active = 0;
             std::vector<int>().swap(Le[e]);
           }
           continue;
         }
-        if (!elem_active[e]) continue;
+        if (!x.active) continue;
         E[o++] = e;
-        if (e != ne) d += w[e];
+        if (e != ne) d += x.w;
       }
       E.resize(o);
       long bound = (long)queue.deg[i] + lp - 1;
