@@ -1276,8 +1276,14 @@ __global__ void __launch_bounds__(DLU_THREADS) dlu_panel_kernel(double *__restri
   double *P;
   if (SMEM) {
     P = reinterpret_cast<double *>(smem_raw);
-    for (int c = 0; c < nb; c++)
-      for (int i = tid; i < m; i += bd) P[dlu_at<true>(i, c, K)] = Sp[i + c * K];
+    for (int i = tid; i < m; i += bd) {  // a row's columns loaded together
+      double v[DLU_NB];
+#pragma unroll
+      for (int c = 0; c < DLU_NB; c++) v[c] = (c < nb) ? Sp[i + c * K] : 0.0;
+#pragma unroll
+      for (int c = 0; c < DLU_NB; c++)
+        if (c < nb) P[dlu_at<true>(i, c, K)] = v[c];
+    }
     __syncthreads();
   } else {
     P = Sp;
@@ -1349,29 +1355,38 @@ __global__ void __launch_bounds__(DLU_THREADS) dlu_panel_kernel(double *__restri
     for (int c = 0; c < nb; c++)
       for (int i = tid; i < m; i += bd) Sp[i + c * K] = P[dlu_at<true>(i, c, K)];
   }
-  if (tid == 0) {
-    // the panel's interchanges as one permutation of at most 2 nb rows
-    int rows[2 * DLU_NB], orig[2 * DLU_NB], cnt = 0;
-    auto find = [&](int r) {
-      for (int k = 0; k < cnt; k++)
-        if (rows[k] == r) return k;
-      rows[cnt] = r;
-      orig[cnt] = r;
-      return cnt++;
-    };
+  if (warp == 0) {
+    // the panel's interchanges as one permutation of at most 2 nb rows:
+    // lane k holds slot k (its row, and the row whose old content it gets)
+    __syncwarp();
+    int row = -1, org = -1, cnt = 0;
     for (int jj = 0; jj < nb; jj++) {
       const int a = j0 + jj, b = j0 + s_piv[jj];
       if (a == b) continue;
-      const int ka = find(a), kb = find(b);
-      const int t = orig[ka];
-      orig[ka] = orig[kb];
-      orig[kb] = t;
+      int ka, kb;
+      const unsigned ma = __ballot_sync(0xffffffffu, row == a);
+      if (ma) {
+        ka = __ffs(ma) - 1;
+      } else {
+        ka = cnt++;
+        if (lane == ka) row = org = a;
+      }
+      const unsigned mb = __ballot_sync(0xffffffffu, row == b);
+      if (mb) {
+        kb = __ffs(mb) - 1;
+      } else {
+        kb = cnt++;
+        if (lane == kb) row = org = b;
+      }
+      const int oa = __shfl_sync(0xffffffffu, org, ka), ob = __shfl_sync(0xffffffffu, org, kb);
+      if (lane == ka) org = ob;
+      if (lane == kb) org = oa;
     }
-    for (int k = 0; k < cnt; k++) {
-      D.swap_dst[k] = rows[k];
-      D.swap_src[k] = orig[k];
+    if (lane < cnt) {
+      D.swap_dst[lane] = row;
+      D.swap_src[lane] = org;
     }
-    *D.swap_cnt = cnt;
+    if (lane == 0) *D.swap_cnt = cnt;
   }
 }
 
