@@ -1142,7 +1142,8 @@ __global__ void __launch_bounds__(256) dense_inverse_kernel(const double *__rest
       double acc[DINV_NC];
 #pragma unroll
       for (int c = 0; c < DINV_NC; c++) acc[c] = 0.0;
-      for (int j = 0; j < nb; j++) {
+#pragma unroll 8
+      for (int j = 0; j < nb; j++) {  // eight L loads in flight
         const double l = L[(size_t)(r0 + j) * K + i];
         const double *xr = X + (r0 + j) * nc;
 #pragma unroll
@@ -1176,7 +1177,8 @@ __global__ void __launch_bounds__(256) dense_inverse_kernel(const double *__rest
       double acc[DINV_NC];
 #pragma unroll
       for (int c = 0; c < DINV_NC; c++) acc[c] = 0.0;
-      for (int j = 0; j < nb; j++) {
+#pragma unroll 8
+      for (int j = 0; j < nb; j++) {  // eight U loads in flight
         const double u = U[(size_t)(r0 + j) * K + i];
         const double *xr = X + (r0 + j) * nc;
 #pragma unroll
@@ -3047,6 +3049,25 @@ static int create_impl(AndfnHandle *H, int R, const char *const *F, const int64_
   H->ne = h.eoff[R];
   H->nf = h.foff[R];
   H->N = h.roff[R];
+  // discharge systems: patterns, then fill-reducing column orders from the
+  // patterns alone, computed once per network (in parallel over
+  // realizations) on a host thread of their own; nothing before the first
+  // factorisation reads them
+  H->sys.assign(R, RealSys());
+  H->ent_row.clear();
+  H->ent_src.clear();
+  H->ent_side.clear();
+  H->ent_kind.clear();
+  for (int r = 0; r < R; r++) build_pattern(H, r);
+  H->order_thread = std::thread([H, R]() {
+    auto tc2 = std::chrono::steady_clock::now();
+#pragma omp parallel for schedule(dynamic, 1) if (R > 1)
+    for (int r = 0; r < R; r++) {
+      CscMatrix P = system_csc(H->sys[r], nullptr);
+      H->sys[r].colorder = column_min_degree_order(P, &H->sys[r].dense_k);
+    }
+    H->ms_create_order = ms_since(tc2);
+  });
   h.coef.assign((size_t)H->ne * H->MC, mk(0.0, 0.0));
   for (int r = 0; r < R; r++) read_coefs(H, r, E[r]);
   cudaStream_t s = H->stream;
@@ -3109,25 +3130,6 @@ static int create_impl(AndfnHandle *H, int R, const char *const *F, const int64_
   CK(H->cut_pos.alloc((size_t)nel * H->cut_cap));
   CK(H->cut_elem.alloc((size_t)nel * H->cut_cap));
   CK(H->cut_sign.alloc((size_t)nel * H->cut_cap));
-  // discharge systems: patterns, then fill-reducing column orders from the
-  // patterns alone, computed once per network (in parallel over
-  // realizations) on a host thread of their own; nothing before the first
-  // factorisation reads them
-  H->sys.assign(R, RealSys());
-  H->ent_row.clear();
-  H->ent_src.clear();
-  H->ent_side.clear();
-  H->ent_kind.clear();
-  for (int r = 0; r < R; r++) build_pattern(H, r);
-  H->order_thread = std::thread([H, R]() {
-    auto tc2 = std::chrono::steady_clock::now();
-#pragma omp parallel for schedule(dynamic, 1) if (R > 1)
-    for (int r = 0; r < R; r++) {
-      CscMatrix P = system_csc(H->sys[r], nullptr);
-      H->sys[r].colorder = column_min_degree_order(P, &H->sys[r].dense_k);
-    }
-    H->ms_create_order = ms_since(tc2);
-  });
   CK(upload(H->d_ent_row, H->ent_row, s));
   CK(upload(H->d_ent_src, H->ent_src, s));
   CK(upload(H->d_ent_side, H->ent_side, s));
