@@ -3301,10 +3301,14 @@ static int build_inverse(AndfnHandle *H, const TriDesc &td) {
   const int N = td.n, K = td.T.K, m0 = N - K;
   const int ldw = (N + 31) / 32 * 32;
   const size_t xbytes = sizeof(double) * (size_t)N * ldw, tbytes = sizeof(double) * (size_t)std::max(1, K) * ldw;
-  size_t fr = 0, tot = 0;
-  CK(cudaMemGetInfo(&fr, &tot));
-  const size_t have = fr + sizeof(double) * (H->winv.cap + H->winv_t.cap);
-  if (xbytes + tbytes + ((size_t)1 << 30) > have) return 0;  // keep the triangular solves
+  // free device memory is queried only when the buffers have to grow (a
+  // driver query per run would contend with monitoring tools)
+  if (H->winv.cap < (size_t)N * ldw || H->winv_t.cap < (size_t)std::max(1, K) * ldw) {
+    size_t fr = 0, tot = 0;
+    CK(cudaMemGetInfo(&fr, &tot));
+    const size_t have = fr + sizeof(double) * (H->winv.cap + H->winv_t.cap);
+    if (xbytes + tbytes + ((size_t)1 << 30) > have) return 0;  // keep the triangular solves
+  }
   CK(H->winv.alloc((size_t)N * ldw));
   CK(H->winv_t.alloc((size_t)std::max(1, K) * ldw));
   CK(cudaMemsetAsync(H->winv.p, 0, xbytes, s));
@@ -5064,12 +5068,23 @@ __global__ void head_vector_kernel(Net net, const int *__restrict__ gptr, const 
   double sum[2] = {0.0, 0.0};
   const int sides = (net.type[e] == 0) ? 2 : 1;
   for (int sd = 0; sd < sides; sd++) {
-    double a = 0.0;
-    for (int x = gptr[2 * r + sd] + lane; x < gptr[2 * r + sd + 1]; x += 32) {
-      const cd c = net.coef[sidx[x]], v = S[x];
-      a = fma(c.re, v.re, fma(-c.im, v.im, a));
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    const int x1 = gptr[2 * r + sd + 1];
+    int x = gptr[2 * r + sd] + lane;
+    for (; x + 96 < x1; x += 128) {  // four index -> coefficient chains in flight
+      const int i0 = sidx[x], i1 = sidx[x + 32], i2 = sidx[x + 64], i3 = sidx[x + 96];
+      const cd v0 = S[x], v1 = S[x + 32], v2 = S[x + 64], v3 = S[x + 96];
+      const cd c0 = net.coef[i0], c1 = net.coef[i1], c2 = net.coef[i2], c3 = net.coef[i3];
+      a0 = fma(c0.re, v0.re, fma(-c0.im, v0.im, a0));
+      a1 = fma(c1.re, v1.re, fma(-c1.im, v1.im, a1));
+      a2 = fma(c2.re, v2.re, fma(-c2.im, v2.im, a2));
+      a3 = fma(c3.re, v3.re, fma(-c3.im, v3.im, a3));
     }
-    sum[sd] = warp_sum(a);
+    for (; x < x1; x += 32) {
+      const cd c = net.coef[sidx[x]], v = S[x];
+      a0 = fma(c.re, v.re, fma(-c.im, v.im, a0));
+    }
+    sum[sd] = warp_sum((a0 + a1) + (a2 + a3));
   }
   if (lane == 0) {
     const double D = net.D;
@@ -5088,17 +5103,38 @@ __global__ void adj_rhs_gather_kernel(Net net, const int *__restrict__ src_ptr, 
   if (as->s.done || i >= (long long)net.ne * net.MC) return;
   const int el = (int)(i / net.MC), j = (int)(i - (long long)el * net.MC);
   if (j >= net.ncoef[el]) return;
-  double ar = 0.0, ai = 0.0;
-  for (int k = src_ptr[el]; k < src_ptr[el + 1]; k++) {
+  // weight * conj(S) per pair: the derivative of a phi value; four pair
+  // chains (pair -> row side, offset -> weight, S) in flight
+  double ar[4] = {0.0, 0.0, 0.0, 0.0}, ai[4] = {0.0, 0.0, 0.0, 0.0};
+  const int k1 = src_ptr[el + 1];
+  int k = src_ptr[el];
+  for (; k + 3 < k1; k += 4) {
+    int pr[4], g[4], off[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) pr[u] = src_pairs[k + u];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      g[u] = pair_g[pr[u]];
+      off[u] = pair_off[pr[u]];
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const double wg = mu[g[u] >> 1] * fac[g[u]];
+      const cd v = S[off[u] + j];
+      ar[u] += wg * v.re;
+      ai[u] -= wg * v.im;
+    }
+  }
+  for (; k < k1; k++) {
     const int pr = src_pairs[k];
     const int g = pair_g[pr];
     const double wg = mu[g >> 1] * fac[g];
     const cd v = S[pair_off[pr] + j];
-    ar += wg * v.re;  // weight * conj(S): the derivative of a phi value
-    ai -= wg * v.im;
+    ar[0] += wg * v.re;
+    ai[0] -= wg * v.im;
   }
-  gc[i].re += ar;
-  gc[i].im += ai;
+  gc[i].re += (ar[0] + ar[1]) + (ar[2] + ar[3]);
+  gc[i].im += (ai[0] + ai[1]) + (ai[2] + ai[3]);
 }
 
 // Right-hand side of the transposed discharge solve: dJ/dd + Phi_d^T lam.
@@ -5581,10 +5617,10 @@ static int adj_build_factors(AndfnHandle *H) {
   A.use_winv = false;
   if (H->winv_ready) {  // A^-T = (Q X P)^T: X^T with the transposed system's P and Q
     const int ldw = H->winv_ldw;
-    size_t fr = 0, tot = 0;
-    CK(cudaMemGetInfo(&fr, &tot));
     const size_t xbytes = sizeof(double) * (size_t)n * ldw;
-    if (xbytes + ((size_t)1 << 30) <= fr + sizeof(double) * A.xt.cap) {
+    size_t fr = 0, tot = 0;
+    if (A.xt.cap < (size_t)n * ldw) CK(cudaMemGetInfo(&fr, &tot));
+    if (A.xt.cap >= (size_t)n * ldw || xbytes + ((size_t)1 << 30) <= fr + sizeof(double) * A.xt.cap) {
       CK(A.xt.alloc((size_t)n * ldw));
       CK(cudaMemsetAsync(A.xt.p, 0, xbytes, s));
       transpose_ld_kernel<<<dim3((n + 31) / 32, (n + 31) / 32), dim3(32, 8), 0, s>>>(H->winv.p, ldw, n, n, A.xt.p,
