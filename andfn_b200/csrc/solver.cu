@@ -42,7 +42,7 @@ static constexpr double PI = 3.141592653589793115997963468544185161590576171875;
 static constexpr int EVAL_THREADS = 128;
 static constexpr int UPDATE_WARPS = 4;
 static constexpr int SOLVE_THREADS = 512;
-static constexpr int ITER_BATCH = 4;  // iterations per graph launch
+static constexpr int ITER_BATCH = 8;  // iterations per graph launch (one host status read each)
 
 enum GroupKind { KIND_PHI = 0, KIND_PSI = 1 };
 // kernel classes of one outer iteration, in launch order
@@ -546,7 +546,8 @@ __global__ void __launch_bounds__(1024) reduce_kernel(Net net) {
   double best = -INFINITY, bec = -INFINITY;
   int bidx = 0x7fffffff, nonfin = 0;
   const int e0 = net.eoff[r], e1 = net.eoff[r + 1];
-  for (int i = e0 + threadIdx.x; i < e1; i += blockDim.x) {
+#pragma unroll 4
+  for (int i = e0 + threadIdx.x; i < e1; i += blockDim.x) {  // loads of four elements in flight
     double e = net.err[i], ec = net.err_coef[i];
     if (!(e == e)) {  // NaN wins (np.max / np.argmax semantics)
       if (best == best || i < bidx) {
