@@ -330,16 +330,26 @@ def run_gpu(args):
         tri_bytes = 12.0 * (nnz - 2.0 * K * K - N) + 8.0 * K * K + 24.0 * N
         tri_note = "latency-bound dependency chain (levels of L and U)"
     roof = {}
+    # DRAM bytes (read + write) of one launch on this workload, from the ncu
+    # captures summarised in profiles/ (sweep: eval_kernels_2118_fractures.md;
+    # discharge solve: two winv_gemv passes, winv_gemv_2118_fractures.md)
+    measured_traffic = {"eval_sweep": 5274112.0 + 0.0,
+                        "trisolve": 2.0 * (231307520.0 + 3308800.0) if inverse else None}
     if dom in ("eval_sweep", "eval_rhs"):
         fl = work["eval_sweep_flops"] if dom == "eval_sweep" else work["eval_rhs_flops"]
         ach = fl / (per[dom] * 1e-3) / 1e12
         roof = {"kernel": dom, "bound": "fp64", "achieved": ach, "peak": fp64_tflops, "unit": "TFLOP/s",
-                "frac": ach / fp64_tflops, "traffic": None, "peak_source": "measured FP64 FMA probe"}
+                "frac": ach / fp64_tflops,
+                "traffic": measured_traffic.get(dom) if F is not None and len(F) == 2118 else None,
+                "traffic_unit": "B per launch (ncu dram read + write)",
+                "peak_source": "measured FP64 FMA probe"}
     else:
         bytes_ = tri_bytes if dom == "trisolve" else 0.0
         ach = bytes_ / (per[dom] * 1e-3) / 1e9
         roof = {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
-                "traffic": None, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
+                "traffic": measured_traffic.get(dom) if len(F) == 2118 else None,
+                "traffic_unit": "B per launch (ncu dram read + write)",
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)",
                 "note": tri_note if dom == "trisolve" else ""}
     ev = {}
     if per.get("eval_sweep"):
