@@ -2511,6 +2511,7 @@ struct AndfnHandle {
   DBuf<int> a_ptr, a_col;
   DBuf<unsigned long long> wacc;
   int winv_ldw = 0, num_sms = 148;
+  cudaEvent_t dlu_ev = nullptr;  // the dense LU's pivots are on the host
   double ms_fac[4] = {};  // factorisation phases of the last run (see AndfnSolveStats)
   bool winv_ready = false;
   bool winv_enabled = true;
@@ -2629,6 +2630,7 @@ struct AndfnHandle {
   }
   ~AndfnHandle() {
     if (order_thread.joinable()) order_thread.join();
+    if (dlu_ev) cudaEventDestroy(dlu_ev);
     andfn::destroy_adj(adj);
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
     for (auto &b : ev)
@@ -3261,7 +3263,30 @@ static int group_for(const std::vector<int> &eptr, bool single = false) {
 // Factorises the Schur complement F.schur on the device into H->tail_l
 // (panels of DLU_NB columns, three launches each) and completes F from the
 // pivots and U's diagonal.  Returns 3 for a singular block.
-static int gpu_dense_lu(AndfnHandle *H, LuFactors &F) {
+__global__ void recip_kernel(const double *__restrict__ d, double *__restrict__ out, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = 1.0 / d[i];
+}
+
+// W = (L U)^-1 of a single network's dense tail (H->tail_l, 1/U(i,i) in
+// H->tail_uinv) into H->tail_w.
+static int launch_tail_inverse(AndfnHandle *H, int K) {
+  cudaStream_t s = H->stream;
+  CK(H->tail_w.alloc((size_t)K * K));
+  // about one CTA per SM (nc columns of the inverse each)
+  const int nc = std::max(1, std::min({DINV_NC, (int)(200 * 1024 / (sizeof(double) * (size_t)K)), K / H->num_sms}));
+  dense_inverse_kernel<<<(K + nc - 1) / nc, 256, sizeof(double) * (size_t)K * nc, s>>>(H->tail_l.p, H->tail_l.p,
+                                                                                       H->tail_uinv.p, K, nc,
+                                                                                       H->tail_w.p);
+  CK(cudaGetLastError());
+  return 0;
+}
+
+// With want_w the tail inverse is launched right after the LU (1/U(i,i)
+// computed on the device, the same IEEE quotients as the host's), and the
+// host waits only for the pivots, so the inverse runs while the host
+// completes the factors and builds the level tables.
+static int gpu_dense_lu(AndfnHandle *H, LuFactors &F, bool want_w) {
   const int K = F.dense;
   cudaStream_t s = H->stream;
   CK(upload(H->tail_l, F.schur, s));
@@ -3283,13 +3308,21 @@ static int gpu_dense_lu(AndfnHandle *H, LuFactors &F) {
     if (mt > 0) dlu_gemm_kernel<<<dim3((mt + 63) / 64, (mt + 63) / 64), 256, 0, s>>>(S, K, j0, nb);
   }
   CK(cudaGetLastError());
+  CK(H->tail_uinv.alloc((size_t)K));
+  recip_kernel<<<(K + 255) / 256, 256, 0, s>>>(D.diag, H->tail_uinv.p, K);
   std::vector<int> piv(K), flag(1);
   std::vector<double> dg(K);
   CK(cudaMemcpyAsync(piv.data(), D.piv, sizeof(int) * K, cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(dg.data(), D.diag, sizeof(double) * K, cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(flag.data(), D.flag, sizeof(int), cudaMemcpyDeviceToHost, s));
   g_d2h_bytes += (int64_t)(12 * K + 4);
-  CK(cudaStreamSynchronize(s));
+  if (!H->dlu_ev) CK(cudaEventCreateWithFlags(&H->dlu_ev, cudaEventDisableTiming));
+  CK(cudaEventRecord(H->dlu_ev, s));
+  if (want_w) {
+    const int rc = launch_tail_inverse(H, K);
+    if (rc) return rc;
+  }
+  CK(cudaEventSynchronize(H->dlu_ev));
   if (flag[0]) return 3;
   return sparse_lu_finish(F, piv, dg);
 }
@@ -3362,8 +3395,13 @@ static int factor_all(AndfnHandle *H, const std::vector<double> &mv) {
   auto tf1 = std::chrono::steady_clock::now();
   H->ms_fac[1] = H->ms_fac[3] = 0.0;
   const bool dev_tail = defer && rcs[0] == 0 && !LU[0].schur.empty();
+  // explicit inverse of the whole system (one network), and of a dense tail
+  // of one network (the inverse's tail rows; the cluster path of the
+  // triangular solves, applied with one refinement step)
+  const bool want_winv = R == 1 && H->winv_enabled && LU[0].n <= WINV_MAX_N;
+  const bool want_w = R == 1 && LU[0].dense > 0 && (LU[0].dense >= CLUSTER_MIN_K || want_winv);
   if (dev_tail) {
-    const int rc = gpu_dense_lu(H, LU[0]);
+    const int rc = gpu_dense_lu(H, LU[0], want_w);
     if (rc != 0 && rc != 3) return rc;
     rcs[0] = rc;
     H->ms_fac[1] = ms_since(tf1);
@@ -3469,19 +3507,10 @@ static int factor_all(AndfnHandle *H, const std::vector<double> &mv) {
     if (tl.empty()) tl.push_back(0.0);
     CK(upload(H->tail_l, tl, s));
   }
-  CK(upload(H->tail_uinv, tui, s));
-  // explicit inverse of a large dense tail of one network, for the cluster
-  // path of the discharge solve (applied with one refinement step)
-  const bool want_winv = R == 1 && H->winv_enabled && LU[0].n <= WINV_MAX_N;
-  const bool want_w = R == 1 && LU[0].dense > 0 && (LU[0].dense >= CLUSTER_MIN_K || want_winv);
-  if (want_w) {
-    const int K = LU[0].dense;
-    CK(H->tail_w.alloc((size_t)K * K));
-    // about one CTA per SM (nc columns of the inverse each)
-    const int nc = std::max(1, std::min({DINV_NC, (int)(200 * 1024 / (sizeof(double) * (size_t)K)), K / H->num_sms}));
-    dense_inverse_kernel<<<(K + nc - 1) / nc, 256, sizeof(double) * (size_t)K * nc, s>>>(
-        H->tail_l.p, H->tail_l.p, H->tail_uinv.p, K, nc, H->tail_w.p);
-    CK(cudaGetLastError());
+  if (!dev_tail) CK(upload(H->tail_uinv, tui, s));  // on the device already (gpu_dense_lu)
+  if (want_w && !dev_tail) {
+    const int rc = launch_tail_inverse(H, LU[0].dense);
+    if (rc) return rc;
   }
   CK(upload(H->pinv, pinv, s));
   CK(upload(H->qcol, qcol, s));
