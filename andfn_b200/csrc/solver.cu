@@ -42,6 +42,13 @@ static constexpr double PI = 3.141592653589793115997963468544185161590576171875;
 static constexpr int EVAL_THREADS = 128;
 static constexpr int UPDATE_WARPS = 4;
 static constexpr int SOLVE_THREADS = 512;
+// The explicit-inverse solve alone is as accurate as the triangular solves
+// (~1e-10 relative on an ill-conditioned system); its refinement step
+// (accurate to ~1e-15) is applied once both the discharges and the mean
+// coefficients change by less than this between iterations: the iterations
+// that set the converged state (earlier solve errors have been damped by the
+// contraction of the iteration by then).
+static constexpr double WINV_REFINE_BELOW = 1e-6;
 static constexpr int ITER_BATCH = 8;  // iterations per graph launch (one host status read each)
 
 enum GroupKind { KIND_PHI = 0, KIND_PSI = 1 };
@@ -72,6 +79,9 @@ struct SolveState {
   double error_q, error, error_coef, pad;
   double max_error, damping;
   int max_it, fused_blend2;
+  // explicit-inverse solves: 1 once the refinement step is applied (from the
+  // iteration after error_q and error_coef first fell below WINV_REFINE_BELOW)
+  int refine, pad_refine;
   // SM clock cycles spent in the phases of trisolve_kernel, summed over
   // launches (thread 0's view): gather, L sparse, L coupling, L dense,
   // U dense, U coupling, U sparse, scatter
@@ -613,6 +623,7 @@ __global__ void __launch_bounds__(1024) reduce_kernel(Net net) {
     if (!(st->error_q == st->error_q)) nf = 1;
     if (nf) st->nonfinite = 1;
     // hpc_solve.py:237-239
+    if (fmax(st->error_q, ec) < WINV_REFINE_BELOW) st->refine = 1;  // sticky
     if (ec < st->max_error && st->error_q < st->max_error) {
       st->cnt_error += 1;
       st->error_q = 1e30;
@@ -1914,13 +1925,15 @@ __global__ void __launch_bounds__(WINV_THREADS) winv_upper_kernel(TriDesc TD, do
 // order, permuted into pivot order in shared memory), X streamed past the L2.
 // Each CTA owns a contiguous block of at most WINV_RPC rows; its 16 warps
 // split every row into equal segments, two rows in flight at a time, and the
-// segment sums are added in a fixed order (deterministic).  STAGE 0:
-// x0(Q k) = y(k) (and the loop counter, as trisolve_kernel counts it).
-// STAGE 1: x(Q k) = x0(Q k) + y(k).  The forward pass writes x to the
-// discharges / constants with the max-change error of the solve (the last
-// CTA to finish turns the grid's maxima into error_q); the adjoint (ADJ: X
-// holds the transposed inverse, P and Q those of the transposed system)
-// writes net.disc only.
+// segment sums are added in a fixed order (deterministic).  STAGE 0 counts
+// the loop iteration (as trisolve_kernel does) and, when the state asks for
+// the refinement step, writes x0(Q k) = y(k); otherwise it is the final pass.
+// STAGE 1 (refinement only): x(Q k) = x0(Q k) + y(k).  The final forward
+// pass writes x to the discharges / constants with the max-change error of
+// the solve (the last CTA to finish turns the grid's maxima into error_q and
+// zeroes them for the next solve); the adjoint (ADJ: X holds the transposed
+// inverse, P and Q those of the transposed system, no refinement) writes
+// net.disc only.
 static constexpr int WINV_RPC = 64;
 static_assert(WINV_THREADS == 512, "16 warps split each row of X");
 
@@ -1931,14 +1944,14 @@ __global__ void __launch_bounds__(WINV_THREADS) winv_gemv_kernel(Net net, const 
                                                                  unsigned long long *__restrict__ acc) {
   SolveState *st = net.st;
   if (st->done) return;
+  // forward: without refinement (refine is written by reduce_kernel only)
+  // the first pass writes the result itself and the second does not run;
+  // the adjoint's solves are not refined
+  const bool fin = ADJ ? true : (STAGE == 1 || !st->refine);
   if (!ADJ) {
-    if (STAGE == 0 && blockIdx.x == 0 && threadIdx.x == 0) {
-      st->nit += 1;
-      acc[0] = 0ull;
-      acc[1] = 0ull;
-      acc[2] = 0ull;
-    }
+    if (STAGE == 0 && blockIdx.x == 0 && threadIdx.x == 0) st->nit += 1;
     if (!st->solve_q) return;  // uniform: solve_q is written only by reduce_kernel
+    if (STAGE == 1 && !st->refine) return;
   }
   const TriDesc &TD = net.tri[0];
   const int N = TD.n;
@@ -1983,12 +1996,12 @@ __global__ void __launch_bounds__(WINV_THREADS) winv_gemv_kernel(Net net, const 
 #pragma unroll
     for (int w = 0; w < 16; w++) y += s_part[t][w];
     const int cc = __ldg(TD.qcol + r0 + t);
-    if (STAGE == 0) {
+    if (!fin) {
       x0[cc] = y;
     } else if (ADJ) {
-      net.disc[cc] = x0[cc] + y;
+      net.disc[cc] = (STAGE == 1 ? x0[cc] : 0.0) + y;
     } else {
-      const double xv = x0[cc] + y;
+      const double xv = (STAGE == 1 ? x0[cc] : 0.0) + y;
       const double xo = net.disc[cc];
       double dd = fabs(xv - xo);
       if (!(dd == dd)) dd = INFINITY;
@@ -2002,7 +2015,7 @@ __global__ void __launch_bounds__(WINV_THREADS) winv_gemv_kernel(Net net, const 
         net.constant[net.row_frac[cc]] = xv;
     }
   }
-  if (STAGE == 0 || ADJ) return;
+  if (!fin || ADJ) return;
   __shared__ double s_d[32], s_o[32];
   __shared__ int s_last;
   for (int o = 16; o > 0; o >>= 1) {
@@ -2032,6 +2045,9 @@ __global__ void __launch_bounds__(WINV_THREADS) winv_gemv_kernel(Net net, const 
     const double a = __longlong_as_double((long long)atomicAdd(acc, 0ull));
     const double b = __longlong_as_double((long long)atomicAdd(acc + 1, 0ull));
     st->error_q = a / (b + 1e-16);
+    acc[0] = 0ull;  // every other CTA is done with them: zero for the next solve
+    acc[1] = 0ull;
+    acc[2] = 0ull;
   }
 }
 
@@ -2043,7 +2059,7 @@ __global__ void winv_resid_kernel(Net net, const int *__restrict__ rp, const int
                                   const int *__restrict__ map, const double *__restrict__ vals,
                                   const double *__restrict__ x0, double *__restrict__ r, int N) {
   const SolveState *st = net.st;
-  if (st->done || (!ADJ && !st->solve_q)) return;
+  if (st->done || (!ADJ && (!st->solve_q || !st->refine))) return;
   const int i = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
   if (i >= N) return;
   double sum = 0.0;
@@ -3366,6 +3382,7 @@ static int build_inverse(AndfnHandle *H, const TriDesc &td) {
   CK(H->wx0.alloc(N));
   CK(H->wr.alloc(N));
   CK(H->wacc.alloc(3));
+  CK(cudaMemsetAsync(H->wacc.p, 0, sizeof(unsigned long long) * 3, s));
   H->winv_ldw = ldw;
   H->winv_ready = true;
   return 0;
@@ -3649,6 +3666,7 @@ static void launch_winv_solve(AndfnHandle *H, const Net &net, cudaStream_t s, co
   // two CTAs of 512 threads per SM, at most WINV_RPC rows per CTA
   const int grid = std::max(2 * H->num_sms, (N + WINV_RPC - 1) / WINV_RPC);
   winv_gemv_kernel<0, ADJ><<<grid, WINV_THREADS, vsm, s>>>(net, X, ldw, net.bvec, H->wx0.p, H->wacc.p);
+  if (ADJ) return;  // the transposed solves are not refined
   winv_resid_kernel<ADJ><<<(N * 32 + 255) / 256, 256, 0, s>>>(net, rp, cols, map, H->d_mvals.p + H->sys[0].ent0,
                                                              H->wx0.p, H->wr.p, N);
   winv_gemv_kernel<1, ADJ><<<grid, WINV_THREADS, vsm, s>>>(net, X, ldw, H->wr.p, H->wx0.p, H->wacc.p);
@@ -3871,6 +3889,7 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
   st0.max_it = (int)C->max_iterations;
   st0.fused_blend2 = growth_possible ? 0 : 1;
   st0.solve_q = 1;
+  st0.refine = 0;
   st0.done = (C->max_iterations <= 0) ? 1 : 0;
   std::vector<SolveState> st_init(R, st0);
   CK(cudaMemcpyAsync(H->st.p, st_init.data(), sizeof(SolveState) * R, cudaMemcpyHostToDevice, s));
@@ -5715,7 +5734,7 @@ static void launch_trisolve_adj(AndfnHandle *H, const Net &net, cudaStream_t s) 
 }
 
 // per transposed sweep: 3 memsets + 5 kernels + the transposed discharge solve
-static int adj_sweep_launches(const AndfnHandle *H) { return 8 + (H->adj->use_winv ? 3 : 1); }
+static int adj_sweep_launches(const AndfnHandle *) { return 8 + 1; }
 static constexpr int ADJ_RESTART = GM_MK;     // Krylov basis size before a restart
 
 // One transposed sweep at lam = x: gc = Phi_c^T x + b_c^T A^-T (gd + Phi_d^T x),
