@@ -263,7 +263,7 @@ static int finish_factors(LuFactors &F, LuPending &W, const std::vector<int> &dp
                           const double *tail_diag);
 
 int sparse_lu_factor(const CscMatrix &A, const std::vector<int> &q, double pivot_threshold, LuFactors &F,
-                     int dense, bool defer_dense) {
+                     int dense, bool defer_dense, double *schur_buf) {
   const int n = A.n;
   if (dense < 0 || dense > n) dense = 0;
   const int m0 = n - dense;
@@ -285,7 +285,10 @@ int sparse_lu_factor(const CscMatrix &A, const std::vector<int> &q, double pivot
   topo.reserve(n);
   double min_piv = INFINITY;
   std::vector<int> tail_row;           // dense-block row of each original row (or -1)
-  std::vector<double> S;               // Schur complement, column-major dense x dense
+  // Schur complement, column-major dense x dense (columns zeroed by the
+  // thread that forms them)
+  std::unique_ptr<double[]> S_own;
+  double *S = nullptr;
   std::vector<int> tail_rows;          // original rows of the dense block, in block order
   for (int k = 0; k < m0; k++) {
     const int col = q[k];
@@ -395,7 +398,12 @@ int sparse_lu_factor(const CscMatrix &A, const std::vector<int> &q, double pivot
         tail_rows.push_back(r);
       }
     if ((int)tail_rows.size() != dense) return 3;
-    S.assign((size_t)dense * dense, 0.0);
+    if (defer_dense && schur_buf) {
+      S = schur_buf;
+    } else {
+      S_own.reset(new double[(size_t)dense * dense]);
+      S = S_own.get();
+    }
     std::vector<std::vector<int>> u_rows(dense);
     std::vector<std::vector<double>> u_vals(dense);
 #pragma omp parallel
@@ -473,7 +481,8 @@ int sparse_lu_factor(const CscMatrix &A, const std::vector<int> &q, double pivot
             uv.push_back(v);
           }
         }
-        double *sc = S.data() + (size_t)(k - m0) * dense;
+        double *sc = S + (size_t)(k - m0) * dense;
+        std::fill(sc, sc + dense, 0.0);
         for (int r : pat)
           if (F.pinv[r] < 0) sc[tail_row[r]] = xw[r];
       }
@@ -497,13 +506,14 @@ int sparse_lu_factor(const CscMatrix &A, const std::vector<int> &q, double pivot
   W.tail_rows = std::move(tail_rows);
   W.min_piv = min_piv;
   if (dense > 0 && defer_dense) {
-    F.schur = std::move(S);
+    F.schur = S;
+    F.schur_own = std::move(S_own);
     F.pending = std::move(W);
     return 0;
   }
   std::vector<int> dpiv;
-  if (dense > 0 && dense_lu(S.data(), dense, dpiv, W.min_piv)) return 3;
-  return finish_factors(F, W, dpiv, dense > 0 ? S.data() : nullptr, nullptr);
+  if (dense > 0 && dense_lu(S, dense, dpiv, W.min_piv)) return 3;
+  return finish_factors(F, W, dpiv, dense > 0 ? S : nullptr, nullptr);
 }
 
 int sparse_lu_finish(LuFactors &F, const std::vector<int> &dpiv, const std::vector<double> &tail_diag) {
@@ -514,8 +524,8 @@ int sparse_lu_finish(LuFactors &F, const std::vector<int> &dpiv, const std::vect
   }
   const int rc = finish_factors(F, F.pending, dpiv, nullptr, tail_diag.data());
   F.pending = LuPending();
-  F.schur.clear();
-  F.schur.shrink_to_fit();
+  F.schur = nullptr;
+  F.schur_own.reset();
   return rc;
 }
 

@@ -9,6 +9,7 @@
 // dependency-driven kernel (see solver.cu).
 #pragma once
 #include <cstdint>
+#include <memory>
 #include <vector>
 
 namespace andfn {
@@ -47,7 +48,9 @@ struct LuFactors {
   double min_abs_pivot = 0.0;
   // deferred dense block: the Schur complement (column-major dense x dense,
   // row order = block order) and the state sparse_lu_finish needs
-  std::vector<double> schur;
+  double *schur = nullptr;            // dense x dense, in schur_own or a caller's buffer
+  std::unique_ptr<double[]> schur_own;
+  const double *schur_data() const { return schur; }
   LuPending pending;
 };
 
@@ -66,10 +69,12 @@ std::vector<int> column_min_degree_order(const CscMatrix &A, int *dense_tail = n
 // with partial pivoting (OpenMP).  Returns 0 on success, 3 (singular) if a
 // column has no nonzero pivot.
 int sparse_lu_factor(const CscMatrix &A, const std::vector<int> &q, double pivot_threshold, LuFactors &out,
-                     int dense = 0, bool defer_dense = false);
+                     int dense = 0, bool defer_dense = false, double *schur_buf = nullptr);
 
 // With defer_dense, sparse_lu_factor stops after forming the Schur complement
-// (out.schur); once it is factorised in place elsewhere (partial pivoting,
+// (out.schur: schur_buf when given, dense x dense doubles, e.g. page-locked
+// memory for the upload, else memory of its own); once it is factorised in
+// place elsewhere (partial pivoting,
 // dpiv[j] = block row swapped with row j, unit lower L below the diagonal, U
 // on and above it), sparse_lu_finish completes the row order and the
 // row-oriented factors from the pivots and U's diagonal (l22 / u22 stay
