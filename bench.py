@@ -384,7 +384,8 @@ def run_gpu(args):
                    "sample": f"oracle: assembly + LU + {SAMPLE_ITS} iterations ({r['sample_seconds']:.1f} s), "
                              f"scaled to {stats['iterations']} iterations"}
         line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+                "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+                "step_ms": [round(x, 3) for x in step_ms], "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
                 "config": {"workload": WORKLOAD, "fractures": int(len(F)), "elements": int(len(E)),
                            "iterations": int(stats["iterations"]), "n_unknowns": int(N), "nnz_lu": int(nnz),
