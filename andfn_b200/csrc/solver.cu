@@ -81,7 +81,7 @@ struct SolveState {
   int max_it, fused_blend2;
   // explicit-inverse solves: 1 once the refinement step is applied (from the
   // iteration after error_q and error_coef first fell below WINV_REFINE_BELOW)
-  int refine, pad_refine;
+  int refine, n_refined;  // n_refined: solves that took the refinement step
   // SM clock cycles spent in the phases of trisolve_kernel, summed over
   // launches (thread 0's view): gather, L sparse, L coupling, L dense,
   // U dense, U coupling, U sparse, scatter
@@ -1952,6 +1952,7 @@ __global__ void __launch_bounds__(WINV_THREADS) winv_gemv_kernel(Net net, const 
     if (STAGE == 0 && blockIdx.x == 0 && threadIdx.x == 0) st->nit += 1;
     if (!st->solve_q) return;  // uniform: solve_q is written only by reduce_kernel
     if (STAGE == 1 && !st->refine) return;
+    if (STAGE == 1 && blockIdx.x == 0 && threadIdx.x == 0) st->n_refined += 1;
   }
   const TriDesc &TD = net.tri[0];
   const int N = TD.n;
@@ -3914,6 +3915,7 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
   st0.fused_blend2 = growth_possible ? 0 : 1;
   st0.solve_q = 1;
   st0.refine = 0;
+  st0.n_refined = 0;
   st0.done = (C->max_iterations <= 0) ? 1 : 0;
   std::vector<SolveState> st_init(R, st0);
   CK(cudaMemcpyAsync(H->st.p, st_init.data(), sizeof(SolveState) * R, cudaMemcpyHostToDevice, s));
@@ -4069,6 +4071,7 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
     st.nnz_factors = H->sys[r].nnz;
     st.dense_tail = H->sys[r].tail_k;
     st.explicit_inverse = H->winv_ready ? 1 : 0;
+    st.refined_solves = H->winv_ready ? f.n_refined : 0;
     st.levels_l = H->sys[r].nlev_l;
     st.levels_u = H->sys[r].nlev_u;
     for (int i = 0; i < 8; i++) st.tri_cycles[i] = f.tri_cycles[i];

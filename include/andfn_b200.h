@@ -103,6 +103,7 @@ typedef struct AndfnSolveStats {
   double ms_factor_dense;   /*   dense LU of the Schur complement (device, incl. its upload), */
   double ms_factor_levels;  /*   level-ordered factor tables + dense-tail inverse,            */
   double ms_inverse;        /*   explicit inverse of the system (device)                      */
+  int64_t refined_solves;   /* explicit-inverse solves that took the refinement step */
 } AndfnSolveStats;
 
 /* ---- one-call drop-in (replaces andfn/hpc/hpc_solve.py:55 solve) --------
