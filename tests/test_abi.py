@@ -83,3 +83,34 @@ def test_batch_records_must_share_dtypes():
     E2 = np.zeros(len(E), element_dtype(12))
     with pytest.raises(ValueError):
         andfn_b200.solve_batch([(F, E), (F.copy(), E2)], 50, g["constants_1"])
+
+
+def test_record_structs_match_the_header(tmp_path):
+    """Every struct of include/andfn_b200.h has the size and field offsets of
+    its ctypes mirror in andfn_b200/records.py (gcc compiles a probe)."""
+    import json
+    import shutil
+    import subprocess
+    from andfn_b200 import records
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    names = ["AndfnLayout", "AndfnConstants", "AndfnSolveStats", "AndfnAdjointStats", "AndfnResidual"]
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "andfn_b200.h"', 'int main(void) {',
+             'printf("{");']
+    for k, n in enumerate(names):
+        cls = getattr(records, n)
+        lines.append(f'printf("{"," if k else ""}\\"{n}\\": [%zu", sizeof({n}));')
+        for f, _ in cls._fields_:
+            lines.append(f'printf(", %zu", offsetof({n}, {f}));')
+        lines.append('printf("]");')
+    lines += ['printf("}\\n");', "return 0;", "}"]
+    src = tmp_path / "probe.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "probe"
+    subprocess.run([cc, "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = json.loads(subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout)
+    for n in names:
+        cls = getattr(records, n)
+        want = [ctypes.sizeof(cls)] + [getattr(cls, f).offset for f, _ in cls._fields_]
+        assert got[n] == want, (n, got[n], want)
