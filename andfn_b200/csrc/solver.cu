@@ -5333,25 +5333,35 @@ __global__ void gm_copy_kernel(const GmresDev *g, const double *__restrict__ V, 
     xin[k] = v[k];
 }
 
-// h[i] += <V_i, w> for i <= j (nv1: one vector only, V itself)
+// h[i] += <V_i, w> for i <= j (nv1: one vector only, V itself); eight
+// basis vectors per pass over w, their block sums reduced together.
+static constexpr int GM_GROUP = 8;
 __global__ void gm_mdot_kernel(const GmresDev *g, const double *__restrict__ V, long long stride, int nv1,
                                const double *__restrict__ w, long long n, double *h) {
   if (g->stop) return;
-  __shared__ double red[32];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __shared__ double red[GM_GROUP][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
   const int nv = nv1 ? 1 : g->j + 1;
-  for (int i = 0; i < nv; i++) {
-    const double *v = V + (size_t)i * stride;
-    double acc = 0.0;
-    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
-      acc = fma(v[k], w[k], acc);
-    acc = warp_sum(acc);
-    if (lane == 0) red[warp] = acc;
+  for (int i0 = 0; i0 < nv; i0 += GM_GROUP) {
+    double acc[GM_GROUP];
+#pragma unroll
+    for (int u = 0; u < GM_GROUP; u++) acc[u] = 0.0;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+      const double wk = w[k];
+#pragma unroll
+      for (int u = 0; u < GM_GROUP; u++)
+        if (i0 + u < nv) acc[u] = fma(V[(size_t)(i0 + u) * stride + k], wk, acc[u]);
+    }
+#pragma unroll
+    for (int u = 0; u < GM_GROUP; u++) {
+      const double a = warp_sum(acc[u]);
+      if (lane == 0) red[u][warp] = a;
+    }
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < GM_GROUP && i0 + (int)threadIdx.x < nv) {
       double t = 0.0;
-      for (int k = 0; k < (int)(blockDim.x >> 5); k++) t += red[k];
-      atomicAdd(&h[i], t);
+      for (int k = 0; k < nwarp; k++) t += red[threadIdx.x][k];
+      atomicAdd(&h[i0 + threadIdx.x], t);
     }
     __syncthreads();
   }
