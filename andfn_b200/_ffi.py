@@ -21,7 +21,8 @@ EXPORTS = ("andfn_b200_solve", "andfn_b200_create", "andfn_b200_upload_state", "
            "andfn_b200_batch_download", "andfn_b200_batch_eval_heads", "andfn_b200_realizations",
            "andfn_b200_eval_heads_noalloc", "andfn_b200_adjoint", "andfn_b200_set_transmissivity",
            "andfn_b200_state_device", "andfn_b200_heads_device", "andfn_b200_heads_vjp",
-           "andfn_b200_bc_residual", "andfn_b200_eval_w")
+           "andfn_b200_bc_residual", "andfn_b200_eval_w", "andfn_b200_eval_w_object",
+           "andfn_b200_track")
 
 STATUS = {0: "ok", 1: "max_iterations", 2: "nonfinite", 3: "singular", 10: "bad_layout", 11: "bad_input",
           12: "cuda_error", 13: "no_device", 14: "out_of_memory"}
@@ -57,6 +58,9 @@ def lib() -> ctypes.CDLL:
         ("andfn_b200_eval_heads", ctypes.c_int, [P, P, P, I64, P]),
         ("andfn_b200_eval_omega", ctypes.c_int, [P, P, P, I64, P]),
         ("andfn_b200_eval_w", ctypes.c_int, [P, P, P, I64, P]),
+        ("andfn_b200_eval_w_object", ctypes.c_int, [P, P, P, I64, P]),
+        ("andfn_b200_track", ctypes.c_int, [P, P, I64, P, I64, P, P, P, ctypes.c_double, I64, I32, I64,
+                                            P, P, P, P, P, P, P]),
         ("andfn_b200_destroy", None, [P]),
         ("andfn_b200_stream", P, [P]),
         ("andfn_b200_last_error", ctypes.c_char_p, []),

@@ -12,7 +12,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "libandfn_b200.so")
 SOURCES = [os.path.join(HERE, "csrc", f) for f in ("solver.cu", "sparse_lu.cpp")]
-DEPS = SOURCES + [os.path.join(HERE, "csrc", f) for f in ("dmath.cuh", "sparse_lu.h")] + [
+DEPS = SOURCES + [os.path.join(HERE, "csrc", f) for f in ("dmath.cuh", "sparse_lu.h", "track.cuh")] + [
     os.path.join(os.path.dirname(HERE), "include", "andfn_b200.h")]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC,-O3,-fopenmp", "-shared", "-diag-suppress", "550", "-lgomp"]

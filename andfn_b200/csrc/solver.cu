@@ -35,6 +35,7 @@
 #include "../../include/andfn_b200.h"
 #include "dmath.cuh"
 #include "sparse_lu.h"
+#include "track.cuh"
 
 namespace andfn {
 
@@ -4233,6 +4234,162 @@ static int eval_w_impl(AndfnHandle *H, const int64_t *frac, const cd *z, int64_t
   return 0;
 }
 
+// ---------------------------------------------------------------------------
+// Streamline tracking (track.cuh): one thread per particle, each tracing its
+// whole streamline through the fractures it passes.
+static TrackView track_view(const Net &n, const double *fgeo, const double *aperture) {
+  TrackView v;
+  v.MC = n.MC;
+  v.type = n.type;
+  v.frac0 = n.frac0;
+  v.frac1 = n.frac1;
+  v.ncoef = n.ncoef;
+  v.ep0 = n.ep0;
+  v.ep1 = n.ep1;
+  v.radius = n.radius;
+  v.center = n.center;
+  v.q = n.q;
+  v.coef = n.coef;
+  v.fptr = n.fptr;
+  v.felem = n.felem;
+  v.fgeo = fgeo;
+  v.aperture = aperture;
+  return v;
+}
+
+__global__ void track_kernel(TrackView tv, int npart, const int *__restrict__ pf, const cd *__restrict__ pz,
+                             const double *__restrict__ pe, double ds, int max_length, int backward, int cap,
+                             cd *oz, double *ov, int *oseg, int *ofr, int *on, int *oelem, int *ostat) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= npart) return;
+  const size_t b = (size_t)i * (size_t)cap;
+  int n = 0, el = -1;
+  ostat[i] = t_track(tv, pf[i], pz[i], pe[i], ds, max_length, backward != 0, cap, oz + b, ov + b, oseg + b, ofr + b,
+                     &n, &el);
+  on[i] = n;
+  oelem[i] = el;
+}
+
+// Object-layer w (Fracture.calc_w, andfn/fracture.py:453-478) at points.
+__global__ void points_w_object_kernel(TrackView tv, const int *__restrict__ frac, const cd *__restrict__ z, int npts,
+                                       cd *__restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= npts) return;
+  out[i] = t_frac_w(tv, frac[i], z[i]);
+}
+
+static int check_frac_ids(AndfnHandle *H, const int64_t *frac, int64_t n, std::vector<int> &out) {
+  if (H->R != 1) {
+    set_error("tracking and object-layer fields need a single-network handle");
+    return ANDFN_BAD_INPUT;
+  }
+  const int nfr = H->h.foff[1] - H->h.foff[0];
+  out.resize(n);
+  for (int64_t i = 0; i < n; i++) {
+    if (frac[i] < 0 || frac[i] >= nfr) {
+      set_error("point fracture index out of range");
+      return ANDFN_BAD_INPUT;
+    }
+    out[i] = (int)frac[i];
+  }
+  return 0;
+}
+
+static int eval_w_object_impl(AndfnHandle *H, const int64_t *frac, const cd *z, int64_t npts, cd *out) {
+  if (npts <= 0) return 0;
+  if (npts > (1LL << 31) - 1) return ANDFN_BAD_INPUT;
+  std::vector<int> fr;
+  if (int rc = check_frac_ids(H, frac, npts, fr)) return rc;
+  cudaStream_t s = H->stream;
+  DBuf<int> dfr;
+  DBuf<cd> dz, dw;
+  CK(dfr.alloc(npts));
+  CK(dz.alloc(npts));
+  CK(dw.alloc(npts));
+  CK(cudaMemcpyAsync(dfr.p, fr.data(), sizeof(int) * npts, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(dz.p, z, sizeof(cd) * npts, cudaMemcpyHostToDevice, s));
+  points_w_object_kernel<<<(unsigned)((npts + 127) / 128), 128, 0, s>>>(track_view(H->net(), nullptr, nullptr), dfr.p,
+                                                                         dz.p, (int)npts, dw.p);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, dw.p, sizeof(cd) * npts, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return 0;
+}
+
+static int track_impl(AndfnHandle *H, const void *frac_recs, int64_t nf, const double *aperture, int64_t npart,
+                      const int64_t *frac, const cd *z, const double *elev, double ds, int64_t max_length,
+                      int backward, int64_t cap, cd *out_z, double *out_v, int64_t *out_seg, int64_t *out_frac,
+                      int64_t *out_n, int64_t *out_elem, int32_t *out_status) {
+  if (npart <= 0) return 0;
+  std::vector<int> pf;
+  if (int rc = check_frac_ids(H, frac, npart, pf)) return rc;
+  if (nf != H->h.foff[1] - H->h.foff[0]) {
+    set_error("fracture count differs from the handle's network");
+    return ANDFN_BAD_INPUT;
+  }
+  if (cap < 2 || cap > (1LL << 30) || max_length < 0 || max_length > (1LL << 30) || npart > (1LL << 30) ||
+      npart * cap > (1LL << 31)) {
+    set_error("track: cap, max_length or the particle count out of range");
+    return ANDFN_BAD_INPUT;
+  }
+  const AndfnLayout &L = H->L;
+  std::vector<double> geo((size_t)nf * TRACK_FGEO);
+  for (int64_t f = 0; f < nf; f++) {
+    const char *rec = static_cast<const char *>(frac_recs) + f * L.frac_size;
+    double *g = &geo[(size_t)f * TRACK_FGEO];
+    std::memcpy(g, rec + L.f_radius, 8);
+    std::memcpy(g + 1, rec + L.f_center, 24);
+    std::memcpy(g + 4, rec + L.f_x_vector, 24);
+    std::memcpy(g + 7, rec + L.f_y_vector, 24);
+    std::memcpy(g + 10, rec + L.f_normal, 24);
+  }
+  cudaStream_t s = H->stream;
+  const size_t slots = (size_t)npart * (size_t)cap;
+  DBuf<double> dgeo, dap, dpe, dov;
+  DBuf<int> dpf, dseg, dfr, dn, del, dst;
+  DBuf<cd> dpz, doz;
+  CK(dgeo.alloc(geo.size()));
+  CK(dap.alloc(nf));
+  CK(dpe.alloc(npart));
+  CK(dpf.alloc(npart));
+  CK(dpz.alloc(npart));
+  CK(doz.alloc(slots));
+  CK(dov.alloc(slots));
+  CK(dseg.alloc(slots));
+  CK(dfr.alloc(slots));
+  CK(dn.alloc(npart));
+  CK(del.alloc(npart));
+  CK(dst.alloc(npart));
+  CK(cudaMemcpyAsync(dgeo.p, geo.data(), sizeof(double) * geo.size(), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(dap.p, aperture, sizeof(double) * nf, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(dpe.p, elev, sizeof(double) * npart, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(dpf.p, pf.data(), sizeof(int) * npart, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(dpz.p, z, sizeof(cd) * npart, cudaMemcpyHostToDevice, s));
+  track_kernel<<<(unsigned)((npart + 63) / 64), 64, 0, s>>>(track_view(H->net(), dgeo.p, dap.p), (int)npart, dpf.p,
+                                                            dpz.p, dpe.p, ds, (int)max_length, backward, (int)cap,
+                                                            doz.p, dov.p, dseg.p, dfr.p, dn.p, del.p, dst.p);
+  CK(cudaGetLastError());
+  std::vector<int> seg(slots), fr(slots), n(npart), el(npart);
+  CK(cudaMemcpyAsync(out_z, doz.p, sizeof(cd) * slots, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(out_v, dov.p, sizeof(double) * slots, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(seg.data(), dseg.p, sizeof(int) * slots, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(fr.data(), dfr.p, sizeof(int) * slots, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(n.data(), dn.p, sizeof(int) * npart, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(el.data(), del.p, sizeof(int) * npart, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(out_status, dst.p, sizeof(int32_t) * npart, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  for (int64_t i = 0; i < npart; i++) {
+    out_n[i] = n[i];
+    out_elem[i] = el[i];
+    const size_t b = (size_t)i * (size_t)cap;
+    for (int k = 0; k < n[i]; k++) {
+      out_seg[b + k] = seg[b + k];
+      out_frac[b + k] = fr[b + k];
+    }
+  }
+  return 0;
+}
+
 // Points of realization r (fracture indices local to it).
 static int eval_points_impl(AndfnHandle *H, int64_t r, const int64_t *frac, const double *z, int64_t npts,
                             double *omega, double *head) {
@@ -4461,6 +4618,25 @@ int andfn_b200_eval_w(AndfnHandle *H, const int64_t *frac, const double *z, int6
   if (!H || (npts > 0 && (!frac || !z || !out))) return ANDFN_BAD_INPUT;
   cudaSetDevice(H->device);
   return eval_w_impl(H, frac, reinterpret_cast<const cd *>(z), npts, reinterpret_cast<cd *>(out));
+}
+
+int andfn_b200_eval_w_object(AndfnHandle *H, const int64_t *frac, const double *z, int64_t npts, double *out) {
+  if (!H || (npts > 0 && (!frac || !z || !out))) return ANDFN_BAD_INPUT;
+  cudaSetDevice(H->device);
+  return eval_w_object_impl(H, frac, reinterpret_cast<const cd *>(z), npts, reinterpret_cast<cd *>(out));
+}
+
+int andfn_b200_track(AndfnHandle *H, const void *frac_recs, int64_t nf, const double *aperture, int64_t npart,
+                     const int64_t *frac, const double *z, const double *elevation, double ds, int64_t max_length,
+                     int32_t backward, int64_t cap, double *out_z, double *out_v, int64_t *out_seg,
+                     int64_t *out_frac, int64_t *out_n, int64_t *out_elem, int32_t *out_status) {
+  if (!H || (npart > 0 && (!frac_recs || !aperture || !frac || !z || !elevation || !out_z || !out_v || !out_seg ||
+                           !out_frac || !out_n || !out_elem || !out_status)))
+    return ANDFN_BAD_INPUT;
+  cudaSetDevice(H->device);
+  return track_impl(H, frac_recs, nf, aperture, npart, frac, reinterpret_cast<const cd *>(z), elevation, ds,
+                    max_length, backward, cap, reinterpret_cast<cd *>(out_z), out_v, out_seg, out_frac, out_n,
+                    out_elem, out_status);
 }
 
 void andfn_b200_destroy(AndfnHandle *H) {

@@ -146,6 +146,34 @@ int andfn_b200_eval_omega(AndfnHandle *h, const int64_t *frac, const double *z,
  * andfn/fracture.py:481-497, is |w| / aperture).  z, out: complex128 [npts]. */
 int andfn_b200_eval_w(AndfnHandle *h, const int64_t *frac, const double *z,
                       int64_t npts, double *out);
+/* The discharge vector of the reference's object layer, which its streamline
+ * tracking uses: Fracture.calc_w (andfn/fracture.py:453-478), where bounding
+ * circles carry -1/R (bounding.py:91-108) and are NaN beyond |z/R| > 1 + 1e-5,
+ * wells and impermeable circles are NaN inside, and impermeable elements
+ * contribute (impermeable_object.py:131-156, 205-224).  Single-network handle;
+ * z, out: complex128 [npts]. */
+int andfn_b200_eval_w_object(AndfnHandle *h, const int64_t *frac, const double *z,
+                             int64_t npts, double *out);
+/* Streamline tracking of npart particles on the handle's solved single network
+ * (replaces DFN.streamline_tracking, andfn/dfn.py:2643-2722, called per start
+ * point and elevation as DFN.plot_streamline_tracking does, dfn.py:2558-2641).
+ * frac_recs: the nf fracture records of the handle (their frames are read with
+ * the handle's layout); aperture: [nf] (the Fracture objects' aperture, which the
+ * records do not hold).  Particle i starts at z[i] (complex128) on fracture
+ * frac[i] with elevation[i]; ds is the step as a fraction of the fracture
+ * radius, max_length the reference's point limit, backward != 0 traces against
+ * the flow.  Outputs, cap slots per particle: out_z (complex128 [npart][cap]),
+ * out_v (velocity |w| / aperture), out_seg (segment index of the point),
+ * out_frac (fracture of the point); out_n [npart] points written, out_elem
+ * [npart] the element the trace ended on (-1 = the reference's False),
+ * out_status [npart] 0 = done, 1 = cap slots were not enough (trace cut). */
+int andfn_b200_track(AndfnHandle *h, const void *frac_recs, int64_t nf,
+                     const double *aperture, int64_t npart, const int64_t *frac,
+                     const double *z, const double *elevation, double ds,
+                     int64_t max_length, int32_t backward, int64_t cap,
+                     double *out_z, double *out_v, int64_t *out_seg,
+                     int64_t *out_frac, int64_t *out_n, int64_t *out_elem,
+                     int32_t *out_status);
 void andfn_b200_destroy(AndfnHandle *h);
 
 /* CUDA stream the handle launches on (cudaStream_t as void*). */

@@ -39,6 +39,37 @@ def mirrors(F, E, f, z):
     return out
 
 
+def assert_trace_matches(F, E, t, i, gold_i, s, sf, v, e, ztol=1e-12, vtol=1e-11, ttol=1e-12):
+    """Trace i of a golden case against (segments, fractures, velocities,
+    element) from an implementation.  Positions within ztol x the largest
+    radius, velocities within vtol relative, travel time and length within ttol
+    relative (of the golden points, with any mirrored start substituted)."""
+    assert e == int(t["element"][i])
+    assert len(s) == len(gold_i)
+    used = []
+    for j, ((gs, gv, gf), ss, vv, ff) in enumerate(zip(gold_i, s, v, sf)):
+        assert ff == gf and len(ss) == len(gs)
+        tol = ztol * F["radius"].max()
+        if j > 0 and abs(ss[0] - gs[0]) > tol:
+            # The start of a segment after a transfer is the point just off the
+            # intersection on the chi side of the crossing point, which lies ON the
+            # line: one rounding bit of the trace decides that side, so the mirror
+            # image across an intersection of the fracture is accepted there.
+            assert any(abs(ss[0] - m) <= 1e-9 * F["radius"].max() for m in mirrors(F, E, gf, gs[0]))
+            gs = np.concatenate(([ss[0]], gs[1:]))
+        np.testing.assert_allclose(ss, gs, rtol=0, atol=tol)
+        used.append(gs)
+        # A segment that ends on an element ends ON its line or circle, where w is
+        # singular (the branch cut of the line map): the last rounding bit of the
+        # complex square root picks the side there, so that one velocity is not
+        # compared.  Travel times use v[:-1] and never read it.
+        on_element = j < len(s) - 1 or e >= 0
+        n = len(vv) - 1 if on_element else len(vv)
+        np.testing.assert_allclose(vv[:n], gv[:n], rtol=vtol, equal_nan=True)
+    tt, tl = ot.travel_time_and_length(s, v)
+    np.testing.assert_allclose([tt, tl], ot.travel_time_and_length(used, [g[1] for g in gold_i]), rtol=ttol)
+
+
 @pytest.mark.parametrize("name", ["mixed", "c1_seed3"])
 def test_oracle_traces_match_reference(name):
     t, F, E = load_case(name)
@@ -47,30 +78,7 @@ def test_oracle_traces_match_reference(name):
         s, sf, v, e = ot.streamline_tracking(F, E, t["aperture"], t["start_z"][i], int(t["start_frac"][i]),
                                              float(t["start_elev"][i]), float(t["ds"]), int(t["max_length"]),
                                              bool(t["backward"][i]))
-        assert e == int(t["element"][i])
-        assert len(s) == len(gold[i])
-        used = []
-        for j, ((gs, gv, gf), ss, vv, ff) in enumerate(zip(gold[i], s, v, sf)):
-            assert ff == gf and len(ss) == len(gs)
-            tol = 1e-12 * F["radius"].max()
-            if j > 0 and abs(ss[0] - gs[0]) > tol:
-                # The start of a segment after a transfer is the point just off the
-                # intersection on the chi side of the crossing point, which lies ON the
-                # line: one rounding bit of the trace decides that side, so the mirror
-                # image across an intersection of the fracture is accepted there.
-                assert any(abs(ss[0] - m) <= 1e-9 * F["radius"].max() for m in mirrors(F, E, gf, gs[0]))
-                gs = np.concatenate(([ss[0]], gs[1:]))
-            np.testing.assert_allclose(ss, gs, rtol=0, atol=tol)
-            used.append(gs)
-            # A segment that ends on an element ends ON its line or circle, where w is
-            # singular (the branch cut of the line map): the last rounding bit of the
-            # complex square root picks the side there, so that one velocity is not
-            # compared.  Travel times use v[:-1] and never read it.
-            on_element = j < len(s) - 1 or e >= 0
-            n = len(vv) - 1 if on_element else len(vv)
-            np.testing.assert_allclose(vv[:n], gv[:n], rtol=1e-11, equal_nan=True)
-        tt, tl = ot.travel_time_and_length(s, v)
-        np.testing.assert_allclose([tt, tl], ot.travel_time_and_length(used, [g[1] for g in gold[i]]), rtol=1e-12)
+        assert_trace_matches(F, E, t, i, gold[i], s, sf, v, e)
         np.testing.assert_allclose(ot.travel_time_and_length([g[0] for g in gold[i]], [g[1] for g in gold[i]]),
                                    [t["travel_time"][i], t["travel_length"][i]], rtol=1e-12)
 
