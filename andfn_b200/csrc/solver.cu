@@ -4235,8 +4235,8 @@ static int eval_w_impl(AndfnHandle *H, const int64_t *frac, const cd *z, int64_t
 }
 
 // ---------------------------------------------------------------------------
-// Streamline tracking (track.cuh): one thread per particle, each tracing its
-// whole streamline through the fractures it passes.
+// Streamline tracking (track.cuh): a group of TRACK_GROUP lanes per particle,
+// tracing its whole streamline through the fractures it passes.
 static TrackView track_view(const Net &n, const double *fgeo, const double *aperture) {
   TrackView v;
   v.MC = n.MC;
@@ -4260,14 +4260,22 @@ static TrackView track_view(const Net &n, const double *fgeo, const double *aper
 __global__ void track_kernel(TrackView tv, int npart, const int *__restrict__ pf, const cd *__restrict__ pz,
                              const double *__restrict__ pe, double ds, int max_length, int backward, int cap,
                              cd *oz, double *ov, int *oseg, int *ofr, int *on, int *oelem, int *ostat) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  // blockDim.x is a multiple of 32, so the TRACK_GROUP lanes of a particle sit
+  // in one warp and leave (i >= npart) together.
+  const int i = (blockIdx.x * blockDim.x + threadIdx.x) / TRACK_GROUP;
   if (i >= npart) return;
+  const int lane = threadIdx.x & (TRACK_GROUP - 1);
+  const int base = (threadIdx.x & 31) & ~(TRACK_GROUP - 1);
+  const GroupW<TRACK_GROUP> wf{tv, lane, ((1u << TRACK_GROUP) - 1u) << base};
   const size_t b = (size_t)i * (size_t)cap;
   int n = 0, el = -1;
-  ostat[i] = t_track(tv, pf[i], pz[i], pe[i], ds, max_length, backward != 0, cap, oz + b, ov + b, oseg + b, ofr + b,
-                     &n, &el);
-  on[i] = n;
-  oelem[i] = el;
+  const int st = t_track(tv, wf, lane == 0, pf[i], pz[i], pe[i], ds, max_length, backward != 0, cap, oz + b, ov + b,
+                         oseg + b, ofr + b, &n, &el);
+  if (lane == 0) {
+    ostat[i] = st;
+    on[i] = n;
+    oelem[i] = el;
+  }
 }
 
 // Object-layer w (Fracture.calc_w, andfn/fracture.py:453-478) at points.
@@ -4327,7 +4335,7 @@ static int track_impl(AndfnHandle *H, const void *frac_recs, int64_t nf, const d
     set_error("fracture count differs from the handle's network");
     return ANDFN_BAD_INPUT;
   }
-  if (cap < 2 || cap > (1LL << 30) || max_length < 0 || max_length > (1LL << 30) || npart > (1LL << 30) ||
+  if (cap < 2 || cap > (1LL << 30) || max_length < 0 || max_length > (1LL << 30) || npart > (1LL << 27) ||
       npart * cap > (1LL << 31)) {
     set_error("track: cap, max_length or the particle count out of range");
     return ANDFN_BAD_INPUT;
@@ -4365,7 +4373,8 @@ static int track_impl(AndfnHandle *H, const void *frac_recs, int64_t nf, const d
   CK(cudaMemcpyAsync(dpe.p, elev, sizeof(double) * npart, cudaMemcpyHostToDevice, s));
   CK(cudaMemcpyAsync(dpf.p, pf.data(), sizeof(int) * npart, cudaMemcpyHostToDevice, s));
   CK(cudaMemcpyAsync(dpz.p, z, sizeof(cd) * npart, cudaMemcpyHostToDevice, s));
-  track_kernel<<<(unsigned)((npart + 63) / 64), 64, 0, s>>>(track_view(H->net(), dgeo.p, dap.p), (int)npart, dpf.p,
+  track_kernel<<<(unsigned)((npart * TRACK_GROUP + 127) / 128), 128, 0, s>>>(track_view(H->net(), dgeo.p, dap.p),
+                                                                              (int)npart, dpf.p,
                                                             dpz.p, dpe.p, ds, (int)max_length, backward, (int)cap,
                                                             doz.p, dov.p, dseg.p, dfr.p, dn.p, del.p, dst.p);
   CK(cudaGetLastError());

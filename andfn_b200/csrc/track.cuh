@@ -1,4 +1,6 @@
-// Streamline (particle) tracking on a solved network: one thread per particle.
+// Streamline (particle) tracking on a solved network: a group of TRACK_GROUP
+// lanes per particle, which share the sum over the fracture's elements in every
+// evaluation of w and otherwise run the same steps in lockstep.
 //
 // Follows the object layer of the reference, which is what DFN.streamline_tracking
 // (andfn/dfn.py:2643-2722) runs on:
@@ -37,6 +39,7 @@ struct TrackView {
   const double *aperture;       // [nf]
 };
 static constexpr int TRACK_FGEO = 13;
+static constexpr int TRACK_GROUP = 8;  // lanes that trace one particle together
 static constexpr double TRACK_PI = 3.141592653589793;
 
 // Status of one particle.
@@ -49,14 +52,18 @@ __host__ __device__ __forceinline__ cd t_mul(cd a, cd b) {
   return mk(a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re);
 }
 
-// d/dchi of sum_k s c_k chi^-k by the reference's Horner form
-// (andfn/hpc/hpc_math_functions.py:76-100).
+// 1 / chi by Smith's quotient.
+__host__ __device__ __forceinline__ cd t_recip(cd a) { return cdiv_ref(mk(1.0, 0.0), a); }
+
+// d/dchi of sum_k s c_k chi^-k in the reference's Horner order
+// (andfn/hpc/hpc_math_functions.py:76-100), each division by chi taken as a
+// product with u = 1 / chi.
 __host__ __device__ inline cd t_asym_d1(cd chi, const cd *c, int m, double s) {
+  const cd u = t_recip(chi);
   cd res = mk(0.0, 0.0);
   for (int k = 0; k < m; k++) {
     const double n = (double)(m - 1 - k);
-    res = res - t_scale(c[m - 1 - k], s * n);
-    res = cdiv_ref(res, chi);
+    res = t_mul(res - t_scale(c[m - 1 - k], s * n), u);
   }
   return res;
 }
@@ -119,18 +126,61 @@ __host__ __device__ inline cd t_frac_w(const TrackView &v, int f, cd z) {
   return w;
 }
 
-__host__ __device__ __forceinline__ double t_velocity(const TrackView &v, int f, cd z) {
-  return t_abs(t_frac_w(v, f, z)) / v.aperture[f];
+// The share of lane `lane` of a group of G lanes: elements lane, lane + G, ...
+__host__ __device__ inline cd t_frac_w_part(const TrackView &v, int f, cd z, int lane, int G) {
+  cd w = mk(0.0, 0.0);
+  for (int k = v.fptr[f] + lane; k < v.fptr[f + 1]; k += G) w = w + t_element_w(v, f, v.felem[k], z);
+  return w;
 }
+
+// w of a fracture summed by a group of G lanes that trace one particle
+// together: each lane sums its share, then a butterfly (lane l adds the value
+// of lane l ^ o for o = G/2 ... 1) leaves the same total, bit for bit, in
+// every lane (a + b == b + a), so all lanes take the same decisions.
+#ifdef __CUDACC__
+template <int G>
+struct GroupW {
+  TrackView v;
+  int lane;
+  unsigned mask;  // the G lanes of this group within the warp
+  __device__ cd operator()(int f, cd z) const {
+    cd w = t_frac_w_part(v, f, z, lane, G);
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) {
+      const double re = __shfl_xor_sync(mask, w.re, o, G);
+      const double im = __shfl_xor_sync(mask, w.im, o, G);
+      w = w + mk(re, im);
+    }
+    return w;
+  }
+};
+#endif
+
+// The same sum on the host, lane by lane, in the butterfly's order.
+template <int G>
+struct HostGroupW {
+  const TrackView *v;
+  cd operator()(int f, cd z) const {
+    cd p[G], q[G];
+    for (int l = 0; l < G; l++) p[l] = t_frac_w_part(*v, f, z, l, G);
+    for (int o = G / 2; o > 0; o >>= 1) {
+      for (int l = 0; l < G; l++) q[l] = p[l] + p[l ^ o];
+      for (int l = 0; l < G; l++) p[l] = q[l];
+    }
+    return p[0];
+  }
+};
 
 __host__ __device__ __forceinline__ bool t_isnan(cd z) { return isnan(z.re) || isnan(z.im); }
 
 // Unit step along conj(w) with up to max_it trapezoidal corrections; points
 // beyond the fracture radius are pulled back inside (andfn/dfn.py:2797-2846).
-__host__ __device__ inline cd t_runge_kutta(const TrackView &v, int f, cd z0, double ds, bool backward) {
+// w0 is w at z0, which the caller has already evaluated for the velocity there.
+template <class W>
+__host__ __device__ inline cd t_runge_kutta(const TrackView &v, const W &wf, int f, cd z0, cd w0, double ds,
+                                            bool backward) {
   const double R = v.fgeo[(size_t)f * TRACK_FGEO];
   if (backward) ds = -ds;
-  const cd w0 = t_frac_w(v, f, z0);
   if (isnan(w0.re)) return t_nan();
   const double a0 = t_abs(w0);
   cd z1 = z0 + t_scale(mk(w0.re / a0, -w0.im / a0), ds);
@@ -139,7 +189,7 @@ __host__ __device__ inline cd t_runge_kutta(const TrackView &v, int f, cd z0, do
   double dz = 1e99;
   int it = 0;
   while (dz > 1e-6 && it < 10) {
-    const cd w1 = t_frac_w(v, f, z1);
+    const cd w1 = wf(f, z1);
     if (isnan(w1.re)) break;
     const cd sw = w0 + w1;
     const double as = t_abs(sw);
@@ -247,8 +297,9 @@ __host__ __device__ __forceinline__ cd t_chi_to_z_line(cd chi, cd a, cd b) {
 // The particle crosses intersection e from fracture f_old into f at p3: the two
 // points just off the line on either side, the split of the flow by |w| there,
 // and the side that the elevation selects (andfn/dfn.py:2743-2795).
-__host__ __device__ inline void t_exit_intersection(const TrackView &v, const double p3[3], int e, int f, int f_old,
-                                                    double *elevation, cd *z_next, cd *z_start) {
+template <class W>
+__host__ __device__ inline void t_exit_intersection(const TrackView &v, const W &wf, const double p3[3], int e, int f,
+                                                    int f_old, double *elevation, cd *z_next, cd *z_start) {
   const cd *ep = (f == v.frac0[e]) ? v.ep0 + 2 * e : v.ep1 + 2 * e;
   const cd z = t_to_2d(v, f, p3);
   const cd chi0 = map_z_line_to_chi_ref(z, ep[0], ep[1]);
@@ -256,7 +307,7 @@ __host__ __device__ inline void t_exit_intersection(const TrackView &v, const do
   const double dchi = 1e-4;
   const cd za = t_chi_to_z_line(t_scale(chi0, 1 + dchi), ep[0], ep[1]);
   const cd zb = t_chi_to_z_line(t_scale(chi1, 1 + dchi), ep[0], ep[1]);
-  const double a0 = t_abs(t_frac_w(v, f, za)), a1 = t_abs(t_frac_w(v, f, zb));
+  const double a0 = t_abs(wf(f, za)), a1 = t_abs(wf(f, zb));
   double divide = a0 / (a0 + a1);
   double pa[3];
   t_to_3d(v, f, za, pa);
@@ -286,25 +337,31 @@ __host__ __device__ inline void t_exit_intersection(const TrackView &v, const do
 // oz / ov / oseg / ofr (point, velocity, segment index, fracture); *n_out is
 // the number of points, *elem_out the element the trace ended on (-1: none,
 // the reference's False).  A segment whose first step is NaN is dropped, as in
-// the reference.  TRACK_TRUNCATED when cap points did not suffice.
-__host__ __device__ inline int t_track(const TrackView &v, int f, cd z0, double elevation, double ds, int max_length,
-                                       bool backward, int cap, cd *oz, double *ov, int *oseg, int *ofr, int *n_out,
-                                       int *elem_out) {
+// the reference.  TRACK_TRUNCATED when cap points did not suffice.  Only a
+// `writer` stores; the other lanes of a group compute the same values.
+template <class W>
+__host__ __device__ inline int t_track(const TrackView &v, const W &wf, bool writer, int f, cd z0, double elevation,
+                                       double ds, int max_length, bool backward, int cap, cd *oz, double *ov,
+                                       int *oseg, int *ofr, int *n_out, int *elem_out) {
   int n = 0, nseg = 0, element = -1, status = TRACK_DONE;
   cd z_start = z0;
   for (;;) {
     const double ds_frac = v.fgeo[(size_t)f * TRACK_FGEO] * ds;
+    const double ap = v.aperture[f];
     const int length = n;
     if (n >= cap) {
       status = TRACK_TRUNCATED;
       break;
     }
     int np = 1;
-    oz[n] = z_start;
-    ov[n] = t_velocity(v, f, z0);
-    oseg[n] = nseg;
-    ofr[n] = f;
-    cd z1 = t_runge_kutta(v, f, z0, ds_frac, backward);
+    cd w0 = wf(f, z0);
+    if (writer) {
+      oz[n] = z_start;
+      ov[n] = t_abs(w0) / ap;
+      oseg[n] = nseg;
+      ofr[n] = f;
+    }
+    cd z1 = t_runge_kutta(v, wf, f, z0, w0, ds_frac, backward);
     if (t_isnan(z1)) break;
     cd z3;
     element = t_check_exit(v, f, z0, z1, &z3);
@@ -314,13 +371,16 @@ __host__ __device__ inline int t_track(const TrackView &v, int f, cd z0, double 
         status = TRACK_TRUNCATED;
         break;
       }
-      oz[n + np] = z1;
-      ov[n + np] = t_velocity(v, f, z1);
-      oseg[n + np] = nseg;
-      ofr[n + np] = f;
+      w0 = wf(f, z1);
+      if (writer) {
+        oz[n + np] = z1;
+        ov[n + np] = t_abs(w0) / ap;
+        oseg[n + np] = nseg;
+        ofr[n + np] = f;
+      }
       np++;
       z0 = z1;
-      z1 = t_runge_kutta(v, f, z0, ds_frac, backward);
+      z1 = t_runge_kutta(v, wf, f, z0, w0, ds_frac, backward);
       if (t_isnan(z1)) {
         z3 = z0;
         break;
@@ -338,10 +398,13 @@ __host__ __device__ inline int t_track(const TrackView &v, int f, cd z0, double 
       element = -1;
       break;
     }
-    oz[n + np] = z3;
-    ov[n + np] = t_velocity(v, f, z3);
-    oseg[n + np] = nseg;
-    ofr[n + np] = f;
+    const cd w3 = wf(f, z3);
+    if (writer) {
+      oz[n + np] = z3;
+      ov[n + np] = t_abs(w3) / ap;
+      oseg[n + np] = nseg;
+      ofr[n + np] = f;
+    }
     n += np + 1;
     nseg++;
     if (element < 0 || v.type[element] != 0) break;
@@ -349,7 +412,7 @@ __host__ __device__ inline int t_track(const TrackView &v, int f, cd z0, double 
     t_to_3d(v, f, z3, p3);
     const int f_old = f;
     f = (f == v.frac0[element]) ? v.frac1[element] : v.frac0[element];
-    t_exit_intersection(v, p3, element, f, f_old, &elevation, &z0, &z_start);
+    t_exit_intersection(v, wf, p3, element, f, f_old, &elevation, &z0, &z_start);
   }
   *n_out = n;
   *elem_out = element;

@@ -255,6 +255,14 @@ def run_gpu(args):
         solver.reset()
         solver.run(c)
     torch.cuda.synchronize()
+    if args.track_only:
+        # streamline tracking alone on the solved network (a profiling case)
+        if rank == 0:
+            print(json.dumps({"tracking": run_tracking(solver, F, E, reps=1, cpu_particles=0,
+                                                       n=args.track_particles, max_length=args.track_max_length)}),
+                  flush=True)
+        solver.close()
+        return
     clocks = ClockSampler(device)
     clocks.start()
     if ws > 1:
@@ -378,6 +386,12 @@ def run_gpu(args):
     if per.get("trisolve"):
         gbs = tri_bytes / (per["trisolve"] * 1e-3) / 1e9
         ev["discharge_solve"].update({"avg_us": per["trisolve"] * 1e3, "achieved_gbs": gbs, "frac_of_hbm": gbs / hbm})
+    tracking = None
+    if not args.no_track and rank == 0:
+        try:
+            tracking = run_tracking(solver, F, E)
+        except Exception as exc:  # reported in the line; the solve numbers stand without it
+            tracking = {"error": f"{type(exc).__name__}: {exc}"}
     batched = None if args.no_batch else run_batched(args, device, flush)
     adjoint = None if args.no_adjoint else run_adjoint(args, device, F, E)
     large = None if args.no_large else run_large(args, device)
@@ -410,7 +424,7 @@ def run_gpu(args):
                                 "q_scale": resid["q_scale"],
                                 "note": "series truncation residual at the collocation points (ncoef 20); "
                                         "convergence uses the reference's MAX_ERROR rule"},
-                "adjoint": adjoint, "large": large}
+                "adjoint": adjoint, "large": large, "tracking": tracking}
         print(json.dumps(line), flush=True)
     solver.close()
     if ws > 1:
@@ -642,6 +656,49 @@ def run_large(args, device):
             "grad_norm": float(torch.linalg.norm(lt.grad).item())}
 
 
+TRACK_PARTICLES, TRACK_MAX_LENGTH, TRACK_DS = 8192, 1000, 1e-2
+
+
+def run_tracking(solver, F, E, reps=3, cpu_particles=2, seed=9, n=TRACK_PARTICLES, max_length=TRACK_MAX_LENGTH):
+    """Streamline tracking on the solved plain-solve network: TRACK_PARTICLES
+    particles (seeded starts at r <= 0.9 R on random fractures, elevations
+    U(0, 1), apertures 10^U(-4, -3)) traced forward, up to TRACK_MAX_LENGTH
+    points each, by one andfn_b200_track launch.  Timed end to end through the
+    public call (host buffers, copies and allocation inside; the call returns
+    after its stream has synchronised), median of reps.  CPU leg: the oracle's
+    tracker (a pure-Python port of the reference's pure-Python tracking) on the
+    first cpu_particles particles."""
+    from andfn_b200.track import track
+    from oracle import track as ot
+    rng = np.random.default_rng(seed)
+    ap = 10 ** rng.uniform(-4, -3, len(F))
+    fr = rng.integers(0, len(F), n)
+    z = np.sqrt(rng.uniform(0, 0.81, n)) * F["radius"][fr] * np.exp(1j * rng.uniform(0, 2 * np.pi, n))
+    el = rng.uniform(0, 1, n)
+    track(solver, ap, fr[:64], z[:64], el[:64], TRACK_DS, max_length)
+    ms = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        tr = track(solver, ap, fr, z, el, TRACK_DS, max_length)
+        ms.append((time.perf_counter() - t0) * 1e3)
+    med = float(np.median(ms))
+    pts = int(tr.npoints.sum())
+    Fs, Es = F.copy(), E.copy()
+    solver.download(Fs, Es)
+    t0 = time.perf_counter()
+    cpu_pts = 0
+    for i in range(cpu_particles):
+        seg, _, _, _ = ot.streamline_tracking(Fs, Es, ap, z[i], int(fr[i]), float(el[i]), TRACK_DS, max_length)
+        cpu_pts += sum(len(x) for x in seg)
+    cpu_s = max(time.perf_counter() - t0, 1e-9)
+    return {"particles": n, "max_length": max_length, "ds": TRACK_DS, "points": pts,
+            "ms": [round(x, 2) for x in ms], "particles_per_s": n / (med * 1e-3), "points_per_s": pts / (med * 1e-3),
+            "statistic": "median, end to end through andfn_b200_track (host buffers)",
+            "truncated": int((tr.status != 0).sum()), "ended_on_element": int((tr.element >= 0).sum()),
+            "cpu_baseline": {"points_per_s": cpu_pts / cpu_s, "particles": cpu_particles, "points": cpu_pts,
+                             "cores": 1, "kind": "port", "sample": "oracle/track.py on the first particles"}}
+
+
 def aggregate_ranks(total_ms: float, steps: int, world_size: int, device=None) -> tuple[float, float]:
     """Slowest rank's timed milliseconds (all-reduce MAX) and the whole-job
     value: every rank solves its own network, so value = world_size * steps
@@ -675,6 +732,10 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-realizations measurement")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint (gradient) measurement")
     ap.add_argument("--no-large", action="store_true", help="skip the large-network forward + gradient run")
+    ap.add_argument("--no-track", action="store_true", help="skip the streamline-tracking measurement")
+    ap.add_argument("--track-only", action="store_true", help="only solve once and time streamline tracking")
+    ap.add_argument("--track-particles", type=int, default=TRACK_PARTICLES)
+    ap.add_argument("--track-max-length", type=int, default=TRACK_MAX_LENGTH)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

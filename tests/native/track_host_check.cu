@@ -54,8 +54,9 @@ extern "C" void track_host(int MC, const int *type, const int *frac0, const int 
   for (int i = 0; i < npart; i++) {
     const size_t b = (size_t)i * (size_t)cap;
     int n = 0, el = -1;
-    ostat[i] = t_track(v, pf[i], mk(pz[2 * i], pz[2 * i + 1]), pe[i], ds, max_length, backward != 0, cap,
-                       reinterpret_cast<cd *>(oz) + b, ov + b, oseg + b, ofr + b, &n, &el);
+    ostat[i] = t_track(v, HostGroupW<TRACK_GROUP>{&v}, true, pf[i], mk(pz[2 * i], pz[2 * i + 1]), pe[i], ds,
+                       max_length, backward != 0, cap, reinterpret_cast<cd *>(oz) + b, ov + b, oseg + b, ofr + b, &n,
+                       &el);
     on[i] = n;
     oelem[i] = el;
   }
