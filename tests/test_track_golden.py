@@ -94,3 +94,31 @@ def test_golden_cases_cover_every_exit():
             seen.add(int(E["_type"][e]) if e >= 0 else (-1 if n else -2))
             multi += ns > 1
     assert {2, 3, -1, -2} <= seen and multi >= 5
+
+
+def test_product_travel_time_matches_reference():
+    """andfn_b200.track.get_travel_time_and_length on the reference's traces
+    gives the reference's DFN.get_travel_time_and_length values."""
+    from andfn_b200.track import get_travel_time_and_length
+    for name in ("mixed", "c1_seed3"):
+        t, F, E = load_case(name)
+        for i, g in enumerate(golden_traces(t)):
+            if not g:
+                continue
+            got = get_travel_time_and_length([x[0] for x in g], [x[1] for x in g])
+            np.testing.assert_allclose(got, [t["travel_time"][i], t["travel_length"][i]], rtol=1e-14)
+
+
+def test_traces_split_into_reference_segments():
+    """Traces.trace turns the per-slot arrays of a launch into the reference's
+    (segments, fractures, velocities, element) form, empty traces included."""
+    from andfn_b200.track import Traces
+    cap = 6
+    z = np.arange(2 * cap, dtype=np.complex128).reshape(2, cap)
+    seg = np.array([[0, 0, 1, 1, 1, 0], [0] * cap])
+    fr = np.array([[3, 3, 5, 5, 5, 0], [0] * cap])
+    tr = Traces(z, z.real.copy(), seg, fr, np.array([5, 0]), np.array([7, -1]), np.zeros(2, np.int32))
+    s, sf, v, e = tr.trace(0)
+    assert [list(x.real) for x in s] == [[0, 1], [2, 3, 4]] and sf == [3, 5] and e == 7
+    assert [list(x) for x in v] == [[0, 1], [2, 3, 4]]
+    assert tr.trace(1) == ([], [], [], -1)
