@@ -7,7 +7,7 @@ arguments and results:
 * ``get_flow_nets(F, n_points, n_boundary_points, E)``   hpc_fracture.py:254-300
 * ``get_heads(F, E, z_array)``                            hpc_fracture.py:303-343
 * ``calc_w(F, E, frac_idx, z)``                           hpc_fracture.py:139-175 (vectorised over points)
-* ``calc_velocity(F, E, frac_idx, z, aperture)``          andfn/fracture.py:481-497
+* ``calc_velocity(F, E, frac_idx, z, aperture)``          andfn/fracture.py:481-497 (object-layer w)
 
 The point evaluations run in the library (``andfn_b200_eval_omega``,
 ``andfn_b200_eval_heads``, ``andfn_b200_eval_w``): one GPU thread per point,
@@ -98,8 +98,14 @@ def calc_w(fracture_struc_array, element_struc_array, frac_idx, z, *, solver: So
 
 def calc_velocity(fracture_struc_array, element_struc_array, frac_idx, z, aperture, *,
                   solver: Solver | None = None, discharge_int: int = 50) -> np.ndarray:
-    """|w| / aperture (Fracture.calc_velocity; the aperture is an attribute of the
-    reference's Fracture objects, not of the records, so it is passed in:
-    a scalar or one value per point)."""
-    w = calc_w(fracture_struc_array, element_struc_array, frac_idx, z, solver=solver, discharge_int=discharge_int)
+    """Fracture.calc_velocity (andfn/fracture.py:481-497): |w| / aperture, with w
+    the discharge vector of the reference's Fracture objects (Fracture.calc_w,
+    andfn/fracture.py:453-478: bounding circles with -1/R and NaN outside, wells
+    and impermeable circles NaN inside, impermeable elements included), which
+    differs from the consolidated ``calc_w`` above.  The aperture is an attribute
+    of the Fracture objects, not of the records, so it is passed in: a scalar or
+    one value per point."""
+    from .track import calc_w_object
+    w = calc_w_object(fracture_struc_array, element_struc_array, frac_idx, z, solver=solver,
+                      discharge_int=discharge_int)
     return np.abs(w) / np.asarray(aperture, np.float64)
