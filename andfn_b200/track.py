@@ -12,9 +12,9 @@ a solved network:
 * ``get_travel_time_and_length(streamline, velocity)``
                                       DFN.get_travel_time_and_length, andfn/dfn.py:2848-2903
 
-All particles are traced by one kernel launch (``andfn_b200_track``), one
-GPU thread per particle following its streamline through every fracture it
-enters.  The field is the object layer's Fracture.calc_w (andfn/fracture.py:
+All particles are traced by one kernel launch (``andfn_b200_track``): a group
+of 8 GPU lanes per particle, which share each sum over the fracture's elements,
+follows its streamline through every fracture it enters.  The field is the object layer's Fracture.calc_w (andfn/fracture.py:
 453-478), which differs from the consolidated calc_w of andfn.hpc at bounding
 circles and impermeable elements; ``calc_w_object`` evaluates it at points.
 Fracture apertures belong to the reference's Fracture objects, not to the
@@ -24,14 +24,13 @@ Elements are referred to by record index; -1 stands for the reference's False.
 """
 from __future__ import annotations
 
-import contextlib
 import ctypes
 from dataclasses import dataclass
 
 import numpy as np
 
 from . import _ffi
-from .fracture import map_2d_to_3d
+from .fracture import _handle, map_2d_to_3d
 from .solver import Solver
 
 TRACK_DONE, TRACK_TRUNCATED = 0, 1
@@ -66,18 +65,6 @@ def _aperture(fractures, aperture) -> np.ndarray:
         raise ValueError("fracture apertures are needed for velocities (Fracture.aperture)")
     a = np.broadcast_to(np.asarray(aperture, np.float64), (len(fractures),))
     return np.ascontiguousarray(a)
-
-
-@contextlib.contextmanager
-def _handle(fractures, elements, solver, discharge_int):
-    if solver is not None:
-        yield solver
-        return
-    s = Solver(np.ascontiguousarray(fractures), np.ascontiguousarray(elements), discharge_int)
-    try:
-        yield s
-    finally:
-        s.close()
 
 
 def track(solver: Solver, aperture, frac, z0, elevation=0.0, ds: float = 1e-2, max_length: int = 1000,
