@@ -1,7 +1,8 @@
 """Writes the golden vectors of streamline tracking by running the reference itself.
 
 Run in a container where the reference source tree is available (its path is
-the first argument, default /root/reference); the GPU machines never run this
+the first argument, default /root/reference; further arguments name the cases
+to write, all by default); the GPU machines never run this
 script, they only read the ``track_*.npz`` files it writes next to itself.
 
 For the converged state of two solve cases (the last k of ``mixed.npz``, which
@@ -28,17 +29,20 @@ sys.path.insert(0, HERE)
 
 from make_golden import build_c1, build_mixed, consolidated, import_reference  # noqa: E402
 
-CASES = (("mixed", 21, 12, 0.02, 150), ("c1_seed3", 22, 16, 0.01, 300))
+CASES = (("mixed", 21, 12, 0.02, 150), ("c1_seed3", 22, 16, 0.01, 300), ("c1_seed13", 23, 16, 0.01, 300))
 
 
 def main():
     ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    only = set(sys.argv[2:])  # case names to (re)write; all when none are given
     andfn = import_reference(ref)
     from andfn.hpc.hpc_solve import solve as hpc_solve
     for name, seed, npart, ds, max_length in CASES:
+        if only and name not in only:
+            continue
         g = np.load(os.path.join(HERE, f"{name}.npz"), allow_pickle=True)
         k = int(np.asarray(g["its"]).max())
-        dfn = build_mixed(andfn) if name == "mixed" else build_c1(andfn, 3)
+        dfn = build_mixed(andfn) if name == "mixed" else build_c1(andfn, int(name.split("seed")[1]))
         F, E = consolidated(dfn)
         c = g[f"constants_{k}"][()]
         hpc_solve(F, E, int(g["D"]), c, dfn.ntype_element)

@@ -70,7 +70,7 @@ def assert_trace_matches(F, E, t, i, gold_i, s, sf, v, e, ztol=1e-12, vtol=1e-11
     np.testing.assert_allclose([tt, tl], ot.travel_time_and_length(used, [g[1] for g in gold_i]), rtol=ttol)
 
 
-@pytest.mark.parametrize("name", ["mixed", "c1_seed3"])
+@pytest.mark.parametrize("name", ["mixed", "c1_seed3", "c1_seed13"])
 def test_oracle_traces_match_reference(name):
     t, F, E = load_case(name)
     gold = golden_traces(t)
@@ -88,7 +88,7 @@ def test_golden_cases_cover_every_exit():
     NaN step, and several pass through intersections."""
     seen = set()
     multi = 0
-    for name in ("mixed", "c1_seed3"):
+    for name in ("mixed", "c1_seed3", "c1_seed13"):
         t, F, E = load_case(name)
         for e, n, ns in zip(t["element"], t["npoints"], t["nseg"]):
             seen.add(int(E["_type"][e]) if e >= 0 else (-1 if n else -2))
@@ -100,7 +100,7 @@ def test_product_travel_time_matches_reference():
     """andfn_b200.track.get_travel_time_and_length on the reference's traces
     gives the reference's DFN.get_travel_time_and_length values."""
     from andfn_b200.track import get_travel_time_and_length
-    for name in ("mixed", "c1_seed3"):
+    for name in ("mixed", "c1_seed3", "c1_seed13"):
         t, F, E = load_case(name)
         for i, g in enumerate(golden_traces(t)):
             if not g:

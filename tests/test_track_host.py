@@ -76,7 +76,7 @@ def host_track(lib, F, E, aperture, frac, z0, elev, ds, max_length, backward, ca
                   ost)
 
 
-@pytest.mark.parametrize("name", ["mixed", "c1_seed3"])
+@pytest.mark.parametrize("name", ["mixed", "c1_seed3", "c1_seed13"])
 def test_host_compiled_tracker_matches_reference(host_lib, name):
     t, F, E = load_case(name)
     gold = golden_traces(t)
