@@ -128,8 +128,11 @@ class _SolveFn(torch.autograd.Function):
 class _HeadsFn(torch.autograd.Function):
     @staticmethod
     def forward(ctx, coef, q, C, logt, model, frac, z):
-        frac = frac.to(torch.int64).contiguous()
-        z = z.to(torch.complex128).contiguous()
+        frac = frac.to(device=model.device, dtype=torch.int64).contiguous()
+        z = z.to(device=model.device, dtype=torch.complex128).contiguous()
+        if frac.ndim != 1 or frac.shape != z.shape:
+            raise ValueError(f"frac and z must be 1-d tensors of one length (got {tuple(frac.shape)} and "
+                             f"{tuple(z.shape)})")
         out = torch.empty(len(frac), dtype=torch.float64, device=model.device)
         model._sync()
         _ffi.check(model._lib().andfn_b200_heads_device(model.solver._h, _ptr(frac), _ptr(z), len(frac),

@@ -20,6 +20,7 @@ import numpy as np
 
 from . import _ffi
 from .records import AndfnSolveStats, constants_struct, layout_of
+from .solver import points_args
 
 
 def _pointers(networks):
@@ -123,8 +124,7 @@ class BatchSolver:
 
     def eval_heads(self, r: int, frac_idx, z) -> np.ndarray:
         """Heads of realization r (andfn/hpc/hpc_fracture.py:205-252)."""
-        frac_idx = np.ascontiguousarray(frac_idx, np.int64)
-        z = np.ascontiguousarray(z, np.complex128)
+        frac_idx, z = points_args(frac_idx, z)
         out = np.empty(len(z))
         _ffi.check(_ffi.lib().andfn_b200_batch_eval_heads(self._h, int(r), frac_idx.ctypes.data_as(ctypes.c_void_p),
                                                          z.ctypes.data_as(ctypes.c_void_p), len(z),

@@ -326,6 +326,238 @@ __global__ void __launch_bounds__(EVAL_THREADS) eval_kernel(Net net, const Item 
 }
 
 // ------------------------------------------------------------------------
+// Pair tables of the sweep.  Within one solve the collocation points and the
+// element geometry are fixed, so for every (collocation point, source
+// element of the point's fracture) pair the map value the series needs and
+// the log term are the same in every iteration:
+//   x = 1/chi  (Laurent types 0, 3, 4, 5)   or   chi = z / R  (bounding
+//       circle, type 1; Taylor series);
+//   l = 0.5 log|chi|^2 (point of a phi element) or atan2(chi) (psi element)
+//       for the discharge types 0, 2, 3, else 0; NaN where the reference's
+//       potential is NaN (inside a well or an impermeable circle).
+// The sweep then evaluates sum_k c_k x^k + qk * l per pair: the Horner chain
+// alone instead of two square roots, a reciprocal and a logarithm.
+// Layout, per fracture f: [source slot s][point of f] (points contiguous,
+// so a warp's loads for one source are coalesced), from tab_off[f]; the
+// points of f are the flattened sweep points [fpt0[f], fpt0[f] + fnp[f]).
+// The values are computed with the same expressions as eval_kernel<false>,
+// so both sweeps give the same results bit for bit.
+// ------------------------------------------------------------------------
+__device__ __forceinline__ void line_map_coeffs(const Net &net, int el, int f, cd &p0, cd &p1) {
+  // Z = p0 z + p1 = (2 z - a - b) / (b - a) on the side of el that lies in f
+  const int side = (net.type[el] == 0 && net.frac0[el] != f) ? 1 : 0;
+  const cd *ep = side ? net.ep1 + 2 * el : net.ep0 + 2 * el;
+  cd a = ep[0], b = ep[1];
+  cd inv = recip(b - a);
+  p0 = 2.0 * inv;
+  cd ab = a + b;
+  p1 = mk(-(ab.re * inv.re - ab.im * inv.im), -(ab.re * inv.im + ab.im * inv.re));
+}
+
+__global__ void __launch_bounds__(EVAL_THREADS) pair_table_kernel(Net net, const Item *__restrict__ items,
+                                                                    const int2 *__restrict__ pts,
+                                                                    const Group *__restrict__ groups,
+                                                                    const int *__restrict__ fpt0,
+                                                                    const int *__restrict__ fnp,
+                                                                    const long long *__restrict__ tab_off,
+                                                                    cd *__restrict__ tw, double *__restrict__ tl) {
+  const Item it = items[blockIdx.x];
+  const int p = it.p0 + threadIdx.x;
+  if (p >= it.p1) return;
+  const int f = it.frac;
+  const int2 gk = pts[p];
+  const Group g = groups[gk.x];
+  const int exclude = g.elem, kind = g.kind;
+  const cd z = sweep_point(net, g.elem, g.side, gk.y);
+  const int np = fnp[f];
+  const long long base = tab_off[f] + (p - fpt0[f]);
+  const int e0 = net.fptr[f], e1 = net.fptr[f + 1];
+  for (int s = 0; s < e1 - e0; s++) {
+    const int el = net.felem[e0 + s];
+    const int type = net.type[el];
+    cd x = mk(0.0, 0.0);
+    double l = 0.0;
+    if (el != exclude) {
+      if (type == 0 || type == 3 || type == 5) {
+        cd p0, p1;
+        line_map_coeffs(net, el, f, p0, p1);
+        const cd chi = exterior_chi(fma_c(p0, z, p1));
+        x = recip(chi);
+        if (type != 5) l = (kind == KIND_PSI) ? atan2(chi.im, chi.re) : 0.5 * log(norm2(chi));
+      } else if (type == 1) {
+        const double ir = 1.0 / net.radius[el];
+        x = ir * z;
+      } else {
+        const double ir = 1.0 / net.radius[el];
+        const cd chi = ir * (z - net.center[el]);
+        if (type == 2) {
+          const double thr = (1.0 - 1e-12) * (1.0 - 1e-12);
+          if (norm2(chi) < thr)
+            l = NAN;
+          else
+            l = (kind == KIND_PSI) ? atan2(chi.im, chi.re) : 0.5 * log(norm2(chi));
+        } else {  // type 4
+          const double thr = (1.0 - 1e-10) * (1.0 - 1e-10);
+          if (norm2(chi) < thr)
+            l = NAN;
+          else
+            x = recip(chi);
+        }
+      }
+    }
+    tw[base + (long long)s * np] = x;
+    tl[base + (long long)s * np] = l;
+  }
+}
+
+// One Horner chain sum_k c_k x^k over mm coefficients (c zero beyond the
+// source's own ncoef, so a longer chain gives the same value).
+__device__ __forceinline__ cd horner(const cd *__restrict__ c, int mm, cd x) {
+  cd r = c[mm - 1];
+  for (int k = mm - 2; k >= 0; k--) r = fma_c(r, x, c[k]);
+  return r;
+}
+
+// The sweep from the pair tables: one thread per collocation point of one
+// item (fracture, <= EVAL_THREADS points); the item's sources are staged in
+// shared memory (signed coefficients, zero-padded to MC, ncoef, q / 2 pi,
+// id), and every thread walks them two at a time (two independent Horner
+// chains), loading the next pair's table entries before the current pair's
+// chains run.  Output as eval_kernel<false>.
+struct TabSrc {
+  int id, m;
+  double qk;
+};
+__global__ void __launch_bounds__(EVAL_THREADS) sweep_table_kernel(Net net, const Item *__restrict__ items,
+                                                                     const int2 *__restrict__ pts,
+                                                                     const Group *__restrict__ groups,
+                                                                     const int *__restrict__ fpt0,
+                                                                     const int *__restrict__ fnp,
+                                                                     const long long *__restrict__ tab_off,
+                                                                     const cd *__restrict__ tw,
+                                                                     const double *__restrict__ tl,
+                                                                     double *__restrict__ out, int chunk) {
+  const Item it = items[blockIdx.x];
+  const int f = it.frac;
+  if (net.st[net.real_frac[f]].done) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  TabSrc *src = reinterpret_cast<TabSrc *>(smem_raw);
+  cd *scoef = reinterpret_cast<cd *>(smem_raw + sizeof(TabSrc) * chunk);
+  const int MC = net.MC;
+  const int p = it.p0 + threadIdx.x;
+  const bool active = p < it.p1;
+  int exclude = -1, kind = KIND_PHI, gout = 0;
+  long long base = 0;
+  const int np = fnp[f];
+  if (active) {
+    const int2 gk = pts[p];
+    const Group g = groups[gk.x];
+    gout = g.out + gk.y;
+    exclude = g.elem;
+    kind = g.kind;
+    base = tab_off[f] + (p - fpt0[f]);
+  }
+  const int e0 = net.fptr[f], e1 = net.fptr[f + 1];
+  double acc_re = 0.0, acc_im = 0.0;
+  for (int c0 = e0; c0 < e1; c0 += chunk) {
+    const int cnt = min(chunk, e1 - c0);
+    __syncthreads();
+    for (int s = threadIdx.x; s < cnt; s += blockDim.x) {
+      const int el = net.felem[c0 + s];
+      const int type = net.type[el];
+      const double sg = (type == 0 && net.frac0[el] != f) ? -1.0 : 1.0;
+      TabSrc h;
+      h.id = el;
+      h.m = net.ncoef[el];
+      h.qk = sg * net.q[el] / (2 * PI);
+      src[s] = h;
+    }
+    for (int idx = threadIdx.x; idx < cnt * MC; idx += blockDim.x) {
+      const int s = idx / MC, k = idx - s * MC;
+      const int el = net.felem[c0 + s];
+      const int m = net.ncoef[el];
+      const bool neg = (net.type[el] == 0 && net.frac0[el] != f);
+      cd c = (k < m) ? net.coef[(size_t)el * MC + k] : mk(0.0, 0.0);
+      if (neg) c = mk(-c.re, -c.im);
+      scoef[idx] = c;
+    }
+    __syncthreads();
+    if (!active) continue;
+    const cd *__restrict__ xw = tw + base + (long long)(c0 - e0) * np;
+    const double *__restrict__ xl = tl + base + (long long)(c0 - e0) * np;
+    int s = 0;
+    cd xa = mk(0.0, 0.0), xb = mk(0.0, 0.0);
+    double la = 0.0, lb = 0.0;
+    if (cnt >= 2) {
+      xa = xw[0];
+      la = xl[0];
+      xb = xw[np];
+      lb = xl[np];
+    }
+    for (; s + 1 < cnt; s += 2) {
+      // next pair's table entries, in flight while this pair's chains run
+      cd na = mk(0.0, 0.0), nb = mk(0.0, 0.0);
+      double nla = 0.0, nlb = 0.0;
+      if (s + 3 < cnt) {
+        na = xw[(long long)(s + 2) * np];
+        nla = xl[(long long)(s + 2) * np];
+        nb = xw[(long long)(s + 3) * np];
+        nlb = xl[(long long)(s + 3) * np];
+      }
+      const TabSrc ha = src[s], hb = src[s + 1];
+      const int mm = max(ha.m, hb.m);
+      cd ra = mk(0.0, 0.0), rb = mk(0.0, 0.0);
+      if (mm > 0) {
+        const cd *ca = scoef + s * MC, *cb = ca + MC;
+        ra = ca[mm - 1];
+        rb = cb[mm - 1];
+        for (int k = mm - 2; k >= 0; k--) {
+          ra = fma_c(ra, xa, ca[k]);
+          rb = fma_c(rb, xb, cb[k]);
+        }
+      }
+      if (ha.id != exclude) {
+        acc_re += ra.re;
+        acc_im += ra.im;
+        if (kind == KIND_PSI)
+          acc_im += ha.qk * la;
+        else
+          acc_re += ha.qk * la;
+      }
+      if (hb.id != exclude) {
+        acc_re += rb.re;
+        acc_im += rb.im;
+        if (kind == KIND_PSI)
+          acc_im += hb.qk * lb;
+        else
+          acc_re += hb.qk * lb;
+      }
+      xa = na;
+      la = nla;
+      xb = nb;
+      lb = nlb;
+    }
+    if (s < cnt) {  // odd source count: the last one alone
+      const TabSrc h = src[s];
+      if (h.id != exclude) {
+        const cd x = xw[(long long)s * np];
+        const double l = xl[(long long)s * np];
+        if (h.m > 0) {
+          const cd r = horner(scoef + s * MC, h.m, x);
+          acc_re += r.re;
+          acc_im += r.im;
+        }
+        if (kind == KIND_PSI)
+          acc_im += h.qk * l;
+        else
+          acc_re += h.qk * l;
+      }
+    }
+  }
+  if (active) out[gout] = (kind == KIND_PSI) ? acc_im : (acc_re + net.constant[f]);
+}
+
+// ------------------------------------------------------------------------
 // Per-element fit: Cauchy-integral DFT, per-type transform, errors, blends.
 // One warp per element.  vals holds phi (or psi) at the collocation points.
 // ------------------------------------------------------------------------
@@ -2233,14 +2465,10 @@ __global__ void cuts_kernel(Net net, const int *__restrict__ elist, int nlist) {
   if (lane == 0) net.cut_n[e] = min(total, net.cut_cap);
 }
 
-// Omega_f(z) at arbitrary points (hpc_fracture.py:52-94, exclude = -1), one
-// thread per point; used for heads (hpc_fracture.py:205-252).
-__global__ void points_kernel(Net net, const int *__restrict__ frac, const cd *__restrict__ z, int npts,
-                              cd *__restrict__ out_omega, double *__restrict__ out_head) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= npts) return;
-  const int f = frac[i];
-  const cd zz = z[i];
+// Omega_f(z) of one point: C_f plus the potential of every element of
+// fracture f (hpc_fracture.py:52-94, exclude = -1).  Shared by every
+// point-evaluation kernel (heads, Omega), so they evaluate one formula.
+__device__ __forceinline__ cd omega_at(const Net &net, int f, cd zz) {
   double ar = net.constant[f], ai = 0.0;
   for (int k = net.fptr[f]; k < net.fptr[f + 1]; k++) {
     const int el = net.felem[k];
@@ -2298,8 +2526,19 @@ __global__ void points_kernel(Net net, const int *__restrict__ frac, const cd *_
       }
     }
   }
-  if (out_omega) out_omega[i] = mk(ar, ai);
-  if (out_head) out_head[i] = ar / net.t[f];
+  return mk(ar, ai);
+}
+
+// Omega_f(z) at arbitrary points, one thread per point; used for heads
+// (hpc_fracture.py:205-252).
+__global__ void points_kernel(Net net, const int *__restrict__ frac, const cd *__restrict__ z, int npts,
+                              cd *__restrict__ out_omega, double *__restrict__ out_head) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= npts) return;
+  const int f = frac[i];
+  const cd om = omega_at(net, f, z[i]);
+  if (out_omega) out_omega[i] = om;
+  if (out_head) out_head[i] = om.re / net.t[f];
 }
 
 // Average discharge term of source element ee over the D points of row j
@@ -2550,6 +2789,17 @@ struct AndfnHandle {
   DBuf<int> group_of;   // [ne][2] -> sweep group
   DBuf<int> rhs_group;  // [n_de][2] -> rhs group
   DBuf<double> sweep_vals, rhs_vals;
+  // sweep pair tables (see pair_table_kernel): layout, values, and whether
+  // the values belong to this run's geometry and points
+  DBuf<long long> tab_off;
+  DBuf<int> tab_fpt0, tab_fnp;
+  std::vector<int> h_tab_fpt0, h_tab_fnp;
+  DBuf<cd> tab_w;
+  DBuf<double> tab_l;
+  long long tab_pairs = 0;
+  int tab_chunk = 2;
+  size_t tab_smem = 0;
+  bool tab_valid = false, use_tab = false;
   DBuf<int> upd_list, psi_list;
   int n_upd = 0, n_psi = 0;
   int nvmax = 0;
@@ -2903,7 +3153,8 @@ static CscMatrix system_csc(const RealSys &S, const double *vals) {
 
 static void build_tables(AndfnHandle *H, bool rhs, std::vector<Group> &groups, std::vector<int> &index_of,
                          std::vector<Item> &items, std::vector<int2> &pts, int &nvals,
-                         const std::vector<char> *only = nullptr) {
+                         const std::vector<char> *only = nullptr, std::vector<int> *fpt0 = nullptr,
+                         std::vector<int> *fnp = nullptr) {
   const HostNet &h = H->h;
   const std::vector<int> &cnint = H->cur_nint;
   const std::vector<int> &cncoef = H->cur_ncoef;
@@ -2970,6 +3221,8 @@ static void build_tables(AndfnHandle *H, bool rhs, std::vector<Group> &groups, s
     for (int gi : gl)
       for (int k = 0; k < groups[gi].npts; k++) pts.push_back(make_int2(gi, k));
     const int end = (int)pts.size();
+    if (fpt0) fpt0->push_back(start);
+    if (fnp) fnp->push_back(end - start);
     double work_per_pt = 0.0;
     for (int k = h.fptr[f]; k < h.fptr[f + 1]; k++) work_per_pt += 30.0 + 4.0 * cncoef[h.felem[k]];
     for (int p = start; p < end; p += EVAL_THREADS) {
@@ -2998,8 +3251,25 @@ static int build_eval_tables(AndfnHandle *H) {
   std::vector<Item> sitems, ritems;
   std::vector<int2> spts, rpts;
   int nsv = 0, nrv = 0;
-  build_tables(H, false, groups, group_of, sitems, spts, nsv);
+  std::vector<int> fpt0, fnp;
+  build_tables(H, false, groups, group_of, sitems, spts, nsv, nullptr, &fpt0, &fnp);
   build_tables(H, true, groups, rhs_group, ritems, rpts, nrv);
+  // pair tables: per fracture, (sources) x (points of the fracture)
+  {
+    const int nf = (int)H->nf;
+    std::vector<long long> off(nf + 1, 0);
+    for (int f = 0; f < nf; f++) off[f + 1] = off[f] + (long long)(h.fptr[f + 1] - h.fptr[f]) * fnp[f];
+    H->tab_pairs = off[nf];
+    CK(upload(H->tab_off, off, s));
+    CK(upload(H->tab_fpt0, fpt0, s));
+    CK(upload(H->tab_fnp, fnp, s));
+    H->h_tab_fpt0 = fpt0;
+    H->h_tab_fnp = fnp;
+    const size_t np = (size_t)std::max<long long>(1, H->tab_pairs);
+    if (H->tab_w.cap < np) CK(H->tab_w.alloc(np));
+    if (H->tab_l.cap < np) CK(H->tab_l.alloc(np));
+    H->tab_valid = false;
+  }
   H->groups = groups;
   CK(upload(H->d_groups, groups, s));
   CK(upload(H->group_of, group_of, s));
@@ -3032,6 +3302,12 @@ static int build_eval_tables(AndfnHandle *H) {
   chunk = std::max(1, std::min(chunk, maxnf));
   H->chunk = chunk;
   H->eval_smem = (sizeof(Src) + sizeof(cd) * H->MC) * chunk;
+  // table sweep staging: at most 48 KB of sources per CTA (four CTAs an SM
+  // when every fracture's sources fit)
+  int tchunk = (int)((48 * 1024) / (sizeof(TabSrc) + sizeof(cd) * H->MC));
+  tchunk = std::max(2, std::min(tchunk, maxnf));
+  H->tab_chunk = tchunk;
+  H->tab_smem = (sizeof(TabSrc) + sizeof(cd) * H->MC) * tchunk;
   CK(cudaStreamSynchronize(s));
   H->tables_dirty = false;
   return 0;
@@ -3176,6 +3452,7 @@ static int create_impl(AndfnHandle *H, int R, const char *const *F, const int64_
   if (!H->h_ndone) CK(cudaMallocHost(&H->h_ndone, sizeof(int)));
   CK(cudaFuncSetAttribute(eval_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
   CK(cudaFuncSetAttribute(eval_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+  CK(cudaFuncSetAttribute(sweep_table_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
   CK(cudaFuncSetAttribute(trisolve_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
   CK(cudaFuncSetAttribute(trisolve_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
   CK(cudaFuncSetAttribute(dense_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
@@ -3727,6 +4004,33 @@ static inline void mark(AndfnHandle *H, cudaStream_t s, int b, int c, int w) {
   if (H->profiling && b >= 0) cudaEventRecordWithFlags(H->ev[b][c][w], s, cudaEventRecordExternal);
 }
 
+// The sweep evaluation into sweep_vals: from the pair tables when this run
+// has them (fixed ncoef and nint), else the full evaluation.
+static void launch_sweep(AndfnHandle *H, const Net &net, cudaStream_t s) {
+  if (H->n_sweep_items <= 0) return;
+  if (H->use_tab && H->tab_valid)
+    sweep_table_kernel<<<H->n_sweep_items, EVAL_THREADS, H->tab_smem, s>>>(
+        net, H->sweep_items.p, H->sweep_pts.p, H->d_groups.p, H->tab_fpt0.p, H->tab_fnp.p, H->tab_off.p, H->tab_w.p,
+        H->tab_l.p, H->sweep_vals.p, H->tab_chunk);
+  else
+    eval_kernel<false><<<H->n_sweep_items, EVAL_THREADS, H->eval_smem, s>>>(net, H->sweep_items.p, H->sweep_pts.p,
+                                                                             H->d_groups.p, H->sweep_vals.p, H->chunk);
+}
+
+// The pair tables of the current points and geometry (once per run).
+static int build_pair_table(AndfnHandle *H) {
+  H->tab_valid = false;
+  if (H->n_sweep_items > 0 && H->tab_pairs > 0) {
+    pair_table_kernel<<<H->n_sweep_items, EVAL_THREADS, 0, H->stream>>>(
+        H->net(), H->sweep_items.p, H->sweep_pts.p, H->d_groups.p, H->tab_fpt0.p, H->tab_fnp.p, H->tab_off.p,
+        H->tab_w.p, H->tab_l.p);
+    CK(cudaGetLastError());
+    H->launches += 1;
+  }
+  H->tab_valid = true;
+  return 0;
+}
+
 static int enqueue_iteration(AndfnHandle *H, cudaStream_t s, int blend_mode, int b = -1) {
   Net net = H->net();
   mark(H, s, b, K_RHS, 0);
@@ -3744,9 +4048,7 @@ static int enqueue_iteration(AndfnHandle *H, cudaStream_t s, int blend_mode, int
   launch_trisolve(H, s);
   mark(H, s, b, K_TRISOLVE, 1);
   mark(H, s, b, K_SWEEP, 0);
-  if (H->n_sweep_items > 0)
-    eval_kernel<false><<<H->n_sweep_items, EVAL_THREADS, H->eval_smem, s>>>(
-        net, H->sweep_items.p, H->sweep_pts.p, H->d_groups.p, H->sweep_vals.p, H->chunk);
+  launch_sweep(H, net, s);
   mark(H, s, b, K_SWEEP, 1);
   const int ub = (H->n_upd + UPDATE_WARPS - 1) / UPDATE_WARPS;
   const size_t usmem = sizeof(double) * 2 * H->nvmax * UPDATE_WARPS;
@@ -3927,12 +4229,20 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
   const int n_de = (int)H->h.de_ids.size();
   if (n_de > 0) zint_kernel<<<std::max(1, std::min(1184, (int)((n_de * H->D + 255) / 256))), 256, 0, s>>>(net);
   if (H->n_psi > 0) cuts_kernel<<<(H->n_psi * 32 + 127) / 128, 128, 0, s>>>(net, H->psi_list.p, H->n_psi);
-  // head vector from power sums, unless coefficients may grow
+  // head vector from power sums and the sweep from pair tables, unless
+  // coefficients may grow (then the points and series lengths change)
   H->use_head_sums = false;
+  H->use_tab = false;
+  H->tab_valid = false;
   if (!growth_possible) {
     int rch = build_head_sums(H);
     if (rch) return rch;
     H->use_head_sums = true;
+    if (const char *v = getenv("ANDFN_B200_PAIR_TABLES"); !v || atoi(v) != 0) {
+      int rcp = build_pair_table(H);
+      if (rcp) return rcp;
+      H->use_tab = true;
+    }
   }
   const long long nent = (long long)H->ent_row.size();
   if (nent > 0)
@@ -4036,9 +4346,7 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
     if (any) {
       net = H->net();
       CK(cudaMemcpyAsync(H->st.p, tmp.data(), sizeof(SolveState) * R, cudaMemcpyHostToDevice, s));
-      if (H->n_sweep_items > 0)
-        eval_kernel<false><<<H->n_sweep_items, EVAL_THREADS, H->eval_smem, s>>>(
-            net, H->sweep_items.p, H->sweep_pts.p, H->d_groups.p, H->sweep_vals.p, H->chunk);
+      launch_sweep(H, net, s);
       const int ub = (H->n_upd + UPDATE_WARPS - 1) / UPDATE_WARPS;
       const size_t usmem = sizeof(double) * 2 * H->nvmax * UPDATE_WARPS;
       if (ub > 0)
@@ -4760,7 +5068,9 @@ int andfn_b200_solve(void *frac_recs, int64_t nf, void *elem_recs, int64_t ne, c
 //
 // * The first call on a device looks up the array's address
 //   (cudaGetSymbolAddress, with that device current) and caches it; make
-//   that first call before any stream capture on the device.
+//   that first call before any stream capture on the device.  The address
+//   belongs to the device's primary context: the cache assumes that context
+//   lives as long as the library (no cudaDeviceReset in between).
 // * Nothing in the array has to start at zero: every entry the kernel reads
 //   is copied in by the same call first, and the kernel writes every result
 //   entry that is copied out.
@@ -4779,69 +5089,6 @@ struct NoAllocScratch {
 };
 
 static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
-
-// Omega_f(z) of one point: the series of every element of fracture f, as
-// points_kernel evaluates them (hpc_fracture.py:52-94, exclude = -1).
-__device__ __forceinline__ cd omega_at(const Net &net, int f, cd zz) {
-  double ar = net.constant[f], ai = 0.0;
-  for (int k = net.fptr[f]; k < net.fptr[f + 1]; k++) {
-    const int el = net.felem[k];
-    const int ty = net.type[el];
-    const int m = net.ncoef[el];
-    const cd *c = net.coef + (size_t)el * net.MC;
-    const bool neg = (ty == 0 && net.frac0[el] != f);
-    const double sg = neg ? -1.0 : 1.0;
-    const double qk = sg * net.q[el] / (2 * PI);
-    if (ty == 0 || ty == 3 || ty == 5) {
-      const cd *ep = neg ? net.ep1 + 2 * el : net.ep0 + 2 * el;
-      cd inv = recip(ep[1] - ep[0]);
-      cd ab = ep[0] + ep[1];
-      cd Z = fma_c(2.0 * inv, zz, mk(-(ab.re * inv.re - ab.im * inv.im), -(ab.re * inv.im + ab.im * inv.re)));
-      cd chi = exterior_chi(Z);
-      if (m > 0) {
-        cd w = recip(chi);
-        cd r = sg * c[m - 1];
-        for (int j = m - 2; j >= 0; j--) r = fma_c(r, w, sg * c[j]);
-        ar += r.re;
-        ai += r.im;
-      }
-      if (ty != 5) {
-        ar += qk * 0.5 * log(norm2(chi));
-        ai += qk * atan2(chi.im, chi.re);
-      }
-    } else if (ty == 1) {
-      cd chi = (1.0 / net.radius[el]) * zz;
-      if (m > 0) {
-        cd r = c[m - 1];
-        for (int j = m - 2; j >= 0; j--) r = fma_c(r, chi, c[j]);
-        ar += r.re;
-        ai += r.im;
-      }
-    } else if (ty == 2) {
-      cd chi = (1.0 / net.radius[el]) * (zz - net.center[el]);
-      if (norm2(chi) < (1.0 - 1e-12) * (1.0 - 1e-12)) {
-        ar = NAN;
-        ai = NAN;
-      } else {
-        ar += qk * 0.5 * log(norm2(chi));
-        ai += qk * atan2(chi.im, chi.re);
-      }
-    } else if (ty == 4) {
-      cd chi = (1.0 / net.radius[el]) * (zz - net.center[el]);
-      if (norm2(chi) < (1.0 - 1e-10) * (1.0 - 1e-10)) {
-        ar = NAN;
-        ai = NAN;
-      } else if (m > 0) {
-        cd w = recip(chi);
-        cd r = c[m - 1];
-        for (int j = m - 2; j >= 0; j--) r = fma_c(r, w, c[j]);
-        ar += r.re;
-        ai += r.im;
-      }
-    }
-  }
-  return mk(ar, ai);
-}
 
 // One thread per point; fracture indices are local to the realization whose
 // fractures start at f0.
@@ -4964,6 +5211,8 @@ struct AdjBufs {
   bool use_winv = false;
   DBuf<Item> items_sw;
   int n_items_sw = 0;
+  DBuf<Item> items_tab;  // items of adj_sweep_table_kernel (ADJ_TAB_PTS points of one fracture)
+  int n_items_tab = 0;
   DBuf<double> fac;  // [2 n_de] weight of a row side per unit mu
   int chunk = 1;
   size_t smem = 0;
@@ -5236,6 +5485,107 @@ __global__ void __launch_bounds__(EVAL_THREADS) adj_sweep_kernel(Net net, const 
     adj_sweep_body<2>(net, it, pts, groups, wsw, gc, gq, gC, chunk, smem_raw);
   else
     adj_sweep_body<4>(net, it, pts, groups, wsw, gc, gq, gC, chunk, smem_raw);
+}
+
+// The sweep evaluation transposed, from the forward sweep's pair tables
+// (pair_table_kernel): for every source s of fracture f and every weighted
+// collocation point p of f,
+//   d/d(Re c_sj, Im c_sj) += w_p sg (Re x^j, -Im x^j)   (phi point)
+//                         or w_p sg (Im x^j,  Re x^j)   (psi point)
+//   d/dq_s += w_p sg l / (2 pi)                         (discharge types)
+// with x, l the pair's table entries.  One item is up to ADJ_TAB_PTS points
+// of one fracture; each warp takes sources round-robin, its lanes split the
+// points, keep the MM coefficient sums of the source in registers and reduce
+// them over the warp once per source (no shared-memory reduction tables).
+static constexpr int ADJ_TAB_PTS = 256;
+template <int MM>
+__global__ void __launch_bounds__(EVAL_THREADS) adj_sweep_table_kernel(
+    Net net, const Item *__restrict__ items, const int2 *__restrict__ pts, const Group *__restrict__ groups,
+    const int *__restrict__ fpt0, const int *__restrict__ fnp, const long long *__restrict__ tab_off,
+    const cd *__restrict__ tw, const double *__restrict__ tl, const double *__restrict__ wsw, cd *gc, double *gq,
+    double *gC, const AdjState *as) {
+  if (as->s.done) return;
+  __shared__ double s_w[ADJ_TAB_PTS];
+  __shared__ int s_ex[ADJ_TAB_PTS];
+  __shared__ int s_psi[ADJ_TAB_PTS];
+  __shared__ double s_cw[EVAL_THREADS / 32];
+  const Item it = items[blockIdx.x];
+  const int f = it.frac;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int npt = it.p1 - it.p0;
+  double cw = 0.0;
+  for (int i = threadIdx.x; i < ADJ_TAB_PTS; i += EVAL_THREADS) {
+    double w = 0.0;
+    int ex = -1, psi = 0;
+    if (i < npt) {
+      const int2 gk = pts[it.p0 + i];
+      const Group g = groups[gk.x];
+      w = wsw[g.out + gk.y];
+      ex = g.elem;
+      psi = (g.kind == KIND_PSI) ? 1 : 0;
+      if (!psi) cw += w;
+    }
+    s_w[i] = w;
+    s_ex[i] = ex;
+    s_psi[i] = psi;
+  }
+  cw = warp_sum(cw);
+  if (lane == 0) s_cw[warp] = cw;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int k = 0; k < EVAL_THREADS / 32; k++) t += s_cw[k];
+    if (t != 0.0) atomicAdd(&gC[f], t);
+  }
+  const int np = fnp[f];
+  const long long base = tab_off[f] + (it.p0 - fpt0[f]);
+  const int e0 = net.fptr[f], nsrc = net.fptr[f + 1] - e0;
+  const int MC = net.MC;
+  for (int s = warp; s < nsrc; s += EVAL_THREADS / 32) {
+    const int el = net.felem[e0 + s];
+    const int type = net.type[el];
+    const int m = net.ncoef[el];
+    const double sg = (type == 0 && net.frac0[el] != f) ? -1.0 : 1.0;
+    const bool disch = (type == 0 || type == 2 || type == 3);
+    const cd *__restrict__ xs = tw + base + (long long)s * np;
+    const double *__restrict__ ls = tl + base + (long long)s * np;
+    double ar[MM], ai[MM];
+#pragma unroll
+    for (int j = 0; j < MM; j++) ar[j] = ai[j] = 0.0;
+    double qc = 0.0;
+    for (int i = lane; i < npt; i += 32) {
+      const double w = s_w[i];
+      if (w == 0.0 || s_ex[i] == el) continue;
+      const cd x = xs[i];
+      const double wv = w * sg;
+      if (disch) qc += wv / (2 * PI) * ls[i];
+      const bool psi = s_psi[i] != 0;
+      cd pw = mk(1.0, 0.0);
+#pragma unroll
+      for (int j = 0; j < MM; j++) {
+        if (j < m) {
+          const double cr = wv * pw.re, ci = wv * pw.im;
+          ar[j] += psi ? ci : cr;
+          ai[j] += psi ? cr : -ci;
+          pw = mk(pw.re * x.re - pw.im * x.im, pw.re * x.im + pw.im * x.re);
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < MM; j++) {
+      if (j < m) {
+        const double r = warp_sum(ar[j]), im = warp_sum(ai[j]);
+        if (lane == 0 && (r != 0.0 || im != 0.0)) {
+          atomicAdd(&gc[(size_t)el * MC + j].re, r);
+          atomicAdd(&gc[(size_t)el * MC + j].im, im);
+        }
+      }
+    }
+    if (disch) {
+      qc = warp_sum(qc);
+      if (lane == 0 && qc != 0.0) atomicAdd(&gq[el], qc);
+    }
+  }
 }
 
 // The head-vector evaluation transposed.  Its points carry one weight per
@@ -5971,9 +6321,22 @@ static void adj_enqueue_sweep(AndfnHandle *H, const Net &net, const Net &net_t, 
   cudaMemsetAsync(A.gC.p, 0, sizeof(double) * nf, s);
   adj_fit_kernel<<<(ne + UPDATE_WARPS - 1) / UPDATE_WARPS, UPDATE_WARPS * 32, sizeof(double) * H->nvmax * UPDATE_WARPS,
                    s>>>(net, x, H->group_of.p, H->d_groups.p, A.wsw.p, A.gq.p, H->nvmax, A.st.p);
-  if (A.n_items_sw > 0)
+  if (H->use_tab && H->tab_valid && MC <= 32 && A.n_items_tab > 0) {
+#define ANDFN_ADJ_TAB(MMV)                                                                                      \
+  adj_sweep_table_kernel<MMV><<<A.n_items_tab, EVAL_THREADS, 0, s>>>(                                          \
+      net, A.items_tab.p, H->sweep_pts.p, H->d_groups.p, H->tab_fpt0.p, H->tab_fnp.p, H->tab_off.p, H->tab_w.p, \
+      H->tab_l.p, A.wsw.p, A.gc.p, A.gq.p, A.gC.p, A.st.p)
+    if (MC <= 16)
+      ANDFN_ADJ_TAB(16);
+    else if (MC <= 24)
+      ANDFN_ADJ_TAB(24);
+    else
+      ANDFN_ADJ_TAB(32);
+#undef ANDFN_ADJ_TAB
+  } else if (A.n_items_sw > 0) {
     adj_sweep_kernel<<<A.n_items_sw, EVAL_THREADS, A.smem, s>>>(net, A.items_sw.p, H->sweep_pts.p, H->d_groups.p,
                                                                  A.wsw.p, A.gc.p, A.gq.p, A.gC.p, A.chunk, A.st.p);
+  }
   adj_rhs_kernel<<<(N + 255) / 256, 256, 0, s>>>(net, gd, A.gq.p, A.gC.p, A.b.p, A.st.p);
   launch_trisolve_adj(H, net_t, s);
   if (H->hs.npairs > 0)
@@ -6030,6 +6393,19 @@ static int adjoint_impl(AndfnHandle *H, const double *gcoef, int64_t mco, const 
       return ANDFN_BAD_INPUT;
     }
     CK(cudaFuncSetAttribute(adj_sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    // items of the table-driven transposed sweep
+    std::vector<Item> ti;
+    for (int f = 0; f < nf && f < (int)H->h_tab_fpt0.size(); f++)
+      for (int a = 0; a < H->h_tab_fnp[f]; a += ADJ_TAB_PTS) {
+        Item it;
+        it.frac = f;
+        it.p0 = H->h_tab_fpt0[f] + a;
+        it.p1 = H->h_tab_fpt0[f] + std::min(H->h_tab_fnp[f], a + ADJ_TAB_PTS);
+        it.pad = 0;
+        ti.push_back(it);
+      }
+    CK(upload(A.items_tab, ti, s));
+    A.n_items_tab = (int)ti.size();
   }
   {
     int rcs = build_head_sums(H);
@@ -6077,9 +6453,7 @@ static int adjoint_impl(AndfnHandle *H, const double *gcoef, int64_t mco, const 
   CK(cudaMemcpyAsync(A.st_eval.p, &se, sizeof(se), cudaMemcpyHostToDevice, s));
   Net net_e = net;
   net_e.st = A.st_eval.p;
-  if (H->n_sweep_items > 0)
-    eval_kernel<false><<<H->n_sweep_items, EVAL_THREADS, H->eval_smem, s>>>(
-        net_e, H->sweep_items.p, H->sweep_pts.p, H->d_groups.p, H->sweep_vals.p, H->chunk);
+  launch_sweep(H, net_e, s);
   // The multipliers solve the linear system (I - T^T) lam = F(0), F(lam) =
   // mask(dJ/dc + gc(lam)) with gc from one transposed sweep (the damped
   // fixed-point iteration lam <- F(lam) contracts only as fast as the forward

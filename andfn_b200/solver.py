@@ -14,6 +14,29 @@ from . import _ffi
 from .records import AndfnSolveStats, constants_struct, layout_of
 
 
+def points_args(frac_idx, z):
+    """(frac_idx, z) as C-contiguous 1-d int64 / complex128 arrays of one
+    length; the C entry points read len(z) entries of both."""
+    frac_idx = np.ascontiguousarray(frac_idx, np.int64)
+    z = np.ascontiguousarray(z, np.complex128)
+    if frac_idx.ndim != 1 or z.ndim != 1 or frac_idx.shape != z.shape:
+        raise ValueError(f"frac_idx and z must be 1-d arrays of one length (got shapes {frac_idx.shape} "
+                         f"and {z.shape})")
+    return frac_idx, z
+
+
+def out_array(out, n, dtype=np.float64):
+    """A caller's output array the C call writes n entries into: it must be a
+    writeable, C-contiguous 1-d ndarray of dtype and length n (it cannot be
+    converted, since the results must land in the caller's own array)."""
+    if out is None:
+        return np.empty(n, dtype)
+    if (not isinstance(out, np.ndarray) or out.dtype != np.dtype(dtype) or out.ndim != 1 or out.shape[0] != n
+            or not out.flags.c_contiguous or not out.flags.writeable):
+        raise ValueError(f"out must be a writeable C-contiguous 1-d {np.dtype(dtype)} array of length {n}")
+    return out
+
+
 class Solver:
     def __init__(self, fractures: np.ndarray, elements: np.ndarray, discharge_int: int = 50, device: int = -1):
         if not (fractures.flags.c_contiguous and elements.flags.c_contiguous):
@@ -85,8 +108,7 @@ class Solver:
 
     def eval_heads(self, frac_idx, z) -> np.ndarray:
         """Heads Re(Omega_f(z))/t_f (andfn/hpc/hpc_fracture.py:205-252)."""
-        frac_idx = np.ascontiguousarray(frac_idx, np.int64)
-        z = np.ascontiguousarray(z, np.complex128)
+        frac_idx, z = points_args(frac_idx, z)
         out = np.empty(len(z))
         _ffi.check(_ffi.lib().andfn_b200_eval_heads(self._h, frac_idx.ctypes.data_as(ctypes.c_void_p),
                                                    z.ctypes.data_as(ctypes.c_void_p), len(z),
@@ -99,11 +121,10 @@ class Solver:
         """Heads through the entry point that allocates no device memory
         (at most NOALLOC_MAX_POINTS points per call; calls on one device must
         not overlap in time).  Pass C-contiguous int64 / complex128 arrays and
-        an out array to avoid host-side copies as well."""
-        frac_idx = np.ascontiguousarray(frac_idx, np.int64)
-        z = np.ascontiguousarray(z, np.complex128)
-        if out is None:
-            out = np.empty(len(z))
+        an out array (a writeable C-contiguous float64 array of len(z)) to
+        avoid host-side copies as well."""
+        frac_idx, z = points_args(frac_idx, z)
+        out = out_array(out, len(z))
         _ffi.check(_ffi.lib().andfn_b200_eval_heads_noalloc(self._h, frac_idx.ctypes.data_as(ctypes.c_void_p),
                                                            z.ctypes.data_as(ctypes.c_void_p), len(z),
                                                            out.ctypes.data_as(ctypes.c_void_p)))
@@ -125,8 +146,7 @@ class Solver:
 
     def eval_omega(self, frac_idx, z) -> np.ndarray:
         """Omega_f(z) (andfn/hpc/hpc_fracture.py:52-94)."""
-        frac_idx = np.ascontiguousarray(frac_idx, np.int64)
-        z = np.ascontiguousarray(z, np.complex128)
+        frac_idx, z = points_args(frac_idx, z)
         out = np.empty(len(z), np.complex128)
         _ffi.check(_ffi.lib().andfn_b200_eval_omega(self._h, frac_idx.ctypes.data_as(ctypes.c_void_p),
                                                    z.ctypes.data_as(ctypes.c_void_p), len(z),
@@ -135,8 +155,7 @@ class Solver:
 
     def eval_w(self, frac_idx, z) -> np.ndarray:
         """Complex discharge vector w_f(z) (andfn/hpc/hpc_fracture.py:139-175)."""
-        frac_idx = np.ascontiguousarray(frac_idx, np.int64)
-        z = np.ascontiguousarray(z, np.complex128)
+        frac_idx, z = points_args(frac_idx, z)
         out = np.empty(len(z), np.complex128)
         _ffi.check(_ffi.lib().andfn_b200_eval_w(self._h, frac_idx.ctypes.data_as(ctypes.c_void_p),
                                                z.ctypes.data_as(ctypes.c_void_p), len(z),

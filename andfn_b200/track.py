@@ -31,7 +31,7 @@ import numpy as np
 
 from . import _ffi
 from .fracture import _handle, map_2d_to_3d
-from .solver import Solver
+from .solver import Solver, points_args
 
 TRACK_DONE, TRACK_TRUNCATED = 0, 1
 
@@ -94,8 +94,7 @@ def track(solver: Solver, aperture, frac, z0, elevation=0.0, ds: float = 1e-2, m
 def calc_w_object(fracture_struc_array, element_struc_array, frac_idx, z, *, solver: Solver | None = None,
                   discharge_int: int = 50) -> np.ndarray:
     """Fracture.calc_w of the object layer (andfn/fracture.py:453-478) at points."""
-    frac_idx = np.ascontiguousarray(np.atleast_1d(frac_idx), np.int64)
-    z = np.ascontiguousarray(np.atleast_1d(z), np.complex128)
+    frac_idx, z = points_args(np.atleast_1d(frac_idx), np.atleast_1d(z))
     out = np.empty(len(z), np.complex128)
     P = ctypes.c_void_p
     with _handle(fracture_struc_array, element_struc_array, solver, discharge_int) as s:

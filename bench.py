@@ -15,8 +15,8 @@ CUDA events on the library's stream, L2 flushed (256 MiB write) between steps.
 e2e:   solves/s through the one-call C ABI (andfn_b200_solve) from host
 records, host<->device copies included.
 --impl reference: the CPU oracle (a C + OpenMP restatement of the reference's
-Numba solver with SciPy's SuperLU) on all host cores, each step a bounded
-sample (10 outer iterations) scaled to a full solve.
+Numba solver with SciPy's SuperLU) on all host cores, each step one complete
+solve of the same network (about 8 s on 16 cores).
 
 Multi-GPU (torchrun): every rank solves its own copy of the network
 (independent replicas; the solve has no exchange step).
@@ -40,7 +40,6 @@ METRIC = "batched vs plain DFN solves/s at 1e-8 BC residual; adjoint/forward tim
 WORKLOAD = ("plain solve: 2,118-fracture spanning cluster of 5,500 power-law/Fisher discs in a 50 m cube "
             "(seed 5), ncoef 20, nint 40, discharge_int 50, MAX_ERROR 1e-8")
 MAX_ERROR = 1e-8
-SAMPLE_ITS = 10
 
 
 def build_network(seed=5):
@@ -182,49 +181,49 @@ def measured_peaks():
         return {}
 
 
-def cpu_sample(F, E, D, c, iterations_full, threads=None):
-    """The oracle on a bounded sample: assembly + LU + SAMPLE_ITS iterations,
-    scaled to a full solve of iterations_full iterations."""
+def cpu_solve(F, E, D, c, threads=None):
+    """One complete solve of the network by the oracle (assembly, SuperLU
+    factorisation, iterations to convergence) on the host cores; wall time."""
     from oracle import oracle as orc
     if threads:
         orc.set_num_threads(threads)
-    cc = c.copy()
-    cc["MAX_ITERATIONS"] = SAMPLE_ITS
     Fs, Es = F.copy(), E.copy()
     st = {}
     t0 = time.perf_counter()
-    orc.solve(Fs, Es, D, cc, stats=st)
+    orc.solve(Fs, Es, D, c, stats=st)
     wall = time.perf_counter() - t0
-    per_it = (st["s_discharge"] + st["s_elements"]) / st["iterations"]
-    est = st["s_matrix"] + st["s_lu"] + per_it * iterations_full
-    return {"seconds_per_solve": est, "sample_seconds": wall, "threads": st["threads"]}
+    return {"seconds_per_solve": wall, "threads": st["threads"], "iterations": int(st["iterations"]),
+            "status": int(st.get("status", 0))}
 
 
 def run_reference(args):
+    """The reference arm: the CPU oracle (a C + OpenMP restatement of the
+    reference's Numba solve, with SciPy's SuperLU) solving the plain-solve
+    network completely in every step, on all host cores."""
     ws, rank, _ = dist_env()
     if rank != 0:
         return
     F, E = build_network()
     c = constants()
     D = 50
-    its_full = 90  # outer iterations of this network to MAX_ERROR 1e-8 (GPU and oracle agree)
     for _ in range(args.warmup):
-        cpu_sample(F, E, D, c, its_full)
+        cpu_solve(F, E, D, c)
     secs = []
-    thr = None
+    r = {}
     for _ in range(args.steps):
-        r = cpu_sample(F, E, D, c, its_full)
+        r = cpu_solve(F, E, D, c)
         secs.append(r["seconds_per_solve"])
-        thr = r["threads"]
-    v = 1.0 / float(np.mean(secs))
-    sample = (f"oracle (C+OpenMP restatement of the reference's Numba solve, SciPy SuperLU): assembly, LU and "
-              f"{SAMPLE_ITS} outer iterations per step, scaled to {its_full} iterations")
+    v = args.steps / float(np.sum(secs))
+    sample = (f"oracle (C+OpenMP restatement of the reference's Numba solve, SciPy SuperLU): one complete solve "
+              f"per step (assembly, LU, {r['iterations']} outer iterations to MAX_ERROR 1e-8)")
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
             "config": {"workload": WORKLOAD, "parallelism": "cpu threads"},
-            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": thr, "kind": "port", "sample": sample},
-            "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": r["threads"], "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "step_s": [round(x, 3) for x in secs]}
     print(json.dumps(line), flush=True)
 
 
@@ -349,9 +348,9 @@ def run_gpu(args):
         tri_bytes = 12.0 * (nnz - 2.0 * K * K - N) + 8.0 * K * K + 24.0 * N
         tri_note = "latency-bound dependency chain (levels of L and U)"
     roof = {}
-    # DRAM bytes (read + write) of one launch on this workload, from the ncu
-    # captures summarised in profiles/ (sweep: eval_kernels_2118_fractures.md;
-    # discharge solve: two winv_gemv passes, winv_gemv_2118_fractures.md)
+    # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch
+    # on this workload, from one ncu capture of the plain-solve profile case
+    # (discharge solve: one winv_gemv pass, times the passes a solve makes)
     measured_traffic = {"eval_sweep": 5274112.0 + 0.0,
                         "trisolve": (1.0 + frac_ref) * (231307520.0 + 3308800.0) if inverse else None}
     if dom in ("eval_sweep", "eval_rhs"):
@@ -398,10 +397,10 @@ def run_gpu(args):
     if rank == 0:
         cpu = None
         if not args.no_cpu:
-            r = cpu_sample(F, E, D, c, int(stats["iterations"]))
+            r = cpu_solve(F, E, D, c)
             cpu = {"value": 1.0 / r["seconds_per_solve"], "unit": "solves/s", "cores": r["threads"], "kind": "port",
-                   "sample": f"oracle: assembly + LU + {SAMPLE_ITS} iterations ({r['sample_seconds']:.1f} s), "
-                             f"scaled to {stats['iterations']} iterations"}
+                   "sample": f"oracle: one complete solve ({r['seconds_per_solve']:.1f} s, {r['iterations']} "
+                             f"iterations, status {r['status']})"}
         line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
                 "step_ms": [round(x, 3) for x in step_ms], "higher_is_better": True,
@@ -425,10 +424,36 @@ def run_gpu(args):
                                 "note": "series truncation residual at the collocation points (ncoef 20); "
                                         "convergence uses the reference's MAX_ERROR rule"},
                 "adjoint": adjoint, "large": large, "tracking": tracking}
+        # the north-star ratios, last so that a truncated copy of the line keeps them
+        line["north_star"] = north_star_summary(value, e2e_val, cpu, roof, batched, adjoint, large)
         print(json.dumps(line), flush=True)
     solver.close()
     if ws > 1:
         torch.distributed.destroy_process_group()
+
+
+def north_star_summary(value, e2e, cpu, roof, batched, adjoint, large):
+    """Plain GPU vs CPU solves/s (device-resident and end to end), batched
+    per-realization rate vs the plain single-network rate, gradient time vs
+    forward time, the finite-difference check and the dominant kernel's
+    roofline fraction."""
+    out = {"plain_solves_per_s": value, "e2e_solves_per_s": e2e}
+    if cpu:
+        out.update({"cpu_solves_per_s": cpu["value"], "value_over_cpu": value / cpu["value"],
+                    "e2e_over_cpu": e2e / cpu["value"], "cpu_cores": cpu["cores"]})
+    if batched:
+        out.update({"batched_realizations_per_s": batched["value"],
+                    "batched_speedup_vs_plain": batched["speedup_vs_plain"]})
+    if adjoint:
+        out["gradient_over_forward"] = adjoint["gradient_over_forward"]
+        fd = adjoint.get("fd_check")
+        if fd:
+            out["fd_max_rel_err"] = {str(x["step"]): x["max_rel_err"] for x in fd["steps"]}
+    if large:
+        out["large_gradient_over_forward"] = large["gradient_over_forward"]
+    if roof:
+        out["roofline"] = {"kernel": roof.get("kernel"), "frac": roof.get("frac")}
+    return out
 
 
 def run_batched(args, device, flush, sample=32):
@@ -505,7 +530,8 @@ def run_batched(args, device, flush, sample=32):
             "iterations": {"max": int(its.max()), "mean": float(its.mean())},
             "status_counts": {str(k): int(v) for k, v in zip(*np.unique(status, return_counts=True))},
             "phase_ms": {k: st[0][k] for k in ("ms_setup", "ms_factor", "ms_iterate")},
-            "kernels_ms_per_step": {k: v[0] / args.steps for k, v in kt.items()}}
+            "kernels_ms_per_run": {k: v[0] / 2 for k, v in kt.items()},
+            "kernels_note": "per-kernel device time of one batched run (two untimed runs with event profiling)"}
 
 
 ADJ_WORKLOAD = ("adjoint: the plain-solve network + 50 observation points (uniform on random fractures, seed 7), "
@@ -699,6 +725,53 @@ def run_tracking(solver, F, E, reps=3, cpu_particles=2, seed=9, n=TRACK_PARTICLE
                              "cores": 1, "kind": "port", "sample": "oracle/track.py on the first particles"}}
 
 
+def run_profile_case(args):
+    """One untimed run of a bench workload, the command profiler captures
+    wrap: ``plain`` (one solve of the plain-solve network through the one-call
+    C ABI), ``adjoint`` (one forward solve plus the gradient of the head-misfit
+    + outflow objective w.r.t. log t) or ``batch`` (one batched solve of the
+    256 realizations).  --profile-iterations caps MAX_ITERATIONS."""
+    import andfn_b200
+    its = args.profile_iterations
+    if args.profile_case == "batch":
+        recs = build_batch()
+        c = batch_constants()
+        if its:
+            c["MAX_ITERATIONS"] = its
+        st = andfn_b200.solve_batch(recs, 50, c)
+        it = [s["iterations"] for s in st]
+        print(f"realizations {len(st)} iterations max {max(it)} mean {np.mean(it):.1f}", flush=True)
+        return
+    F, E = build_network()
+    c = constants()
+    if its:
+        c["MAX_ITERATIONS"] = its
+    if args.profile_case == "adjoint":
+        import torch
+        from andfn_b200.adjoint import DFNModel
+        rng = np.random.default_rng(7)
+        fr = rng.integers(0, len(F), 50)
+        z = F["radius"][fr] * 0.9 * np.sqrt(rng.uniform(size=50)) * np.exp(2j * np.pi * rng.uniform(size=50))
+        dev = "cuda:0"
+        frt = torch.tensor(fr, device=dev)
+        zt = torch.tensor(z, dtype=torch.complex128, device=dev)
+        outlet = torch.tensor(np.nonzero((E["_type"] == 3) & (E["head"] == 0.0))[0], device=dev)
+        m = DFNModel(F.copy(), E.copy(), c, 50, adjoint_tol=1e-8)
+        lt = torch.tensor(np.log(F["t"]), device=dev, requires_grad=True)
+        coef, q, C = m.solve(lt)
+        h = m.heads(coef, q, C, lt, frt, zt)
+        J = ((h - 0.5) ** 2).sum() + q[outlet].sum()
+        J.backward()
+        print(f"forward iterations {m.stats['iterations']} adjoint sweeps {m.adjoint_stats['iterations']} "
+              f"residual {m.adjoint_stats['residual']:.2e}", flush=True)
+        m.close()
+        return
+    andfn_b200.solve(F, E, 50, c)
+    st = andfn_b200.last_stats
+    print(f"iterations {st['iterations']} status {st['status']} factor {st['ms_factor']:.1f} ms "
+          f"iterate {st['ms_iterate']:.1f} ms", flush=True)
+
+
 def aggregate_ranks(total_ms: float, steps: int, world_size: int, device=None) -> tuple[float, float]:
     """Slowest rank's timed milliseconds (all-reduce MAX) and the whole-job
     value: every rank solves its own network, so value = world_size * steps
@@ -736,8 +809,13 @@ def main():
     ap.add_argument("--track-only", action="store_true", help="only solve once and time streamline tracking")
     ap.add_argument("--track-particles", type=int, default=TRACK_PARTICLES)
     ap.add_argument("--track-max-length", type=int, default=TRACK_MAX_LENGTH)
+    ap.add_argument("--profile-case", choices=["plain", "adjoint", "batch"], default=None,
+                    help="one untimed run of that workload (the command a profiler capture wraps); no JSON line")
+    ap.add_argument("--profile-iterations", type=int, default=None, help="MAX_ITERATIONS of --profile-case")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.profile_case:
+        run_profile_case(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_gpu(args)

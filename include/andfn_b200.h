@@ -235,7 +235,10 @@ int andfn_b200_fp64_peak(int32_t device, double *tflops);
  *   - npts is at most ANDFN_NOALLOC_MAX_POINTS; larger calls are refused
  *     with ANDFN_BAD_INPUT (split them, or use andfn_b200_eval_heads);
  *   - the first call on a device looks the array up and caches its address:
- *     make it before any stream capture on that device;
+ *     make it before any stream capture on that device.  The cached address
+ *     belongs to the device's primary context, so it assumes that context
+ *     lives as long as the library is loaded: after cudaDeviceReset the
+ *     library must not be used again in that process;
  *   - the array is shared by all handles on a device: calls that overlap in
  *     time on one device race on it and must be serialised by the caller.
  * Fracture indices are those of the handle's first (or only) network. */

@@ -1,7 +1,7 @@
 """Writes the golden vectors of the flow-field evaluations by running the reference itself.
 
 Run in a container where the reference source tree is available (its path is
-the first argument, default /root/reference); the GPU machines never run this
+the first argument, or $ANDFN_REFERENCE); the GPU machines never run this
 script, they only read the ``flow_*.npz`` files it writes next to itself.
 
 For a converged state of the solve cases (the last k of ``mixed.npz``, which
@@ -26,7 +26,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 
-from make_golden import import_reference  # noqa: E402
+from make_golden import import_reference, reference_path  # noqa: E402
 
 N_IN, N_BND, N_W = 40, 12, 400
 
@@ -38,8 +38,7 @@ def case_state(name):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
-    import_reference(ref)
+    import_reference(reference_path(sys.argv[:2]))
     from andfn.hpc import hpc_fracture as hf
     for name, seed in (("mixed", 11), ("c1_seed3", 12)):
         F, E, k = case_state(name)

@@ -1,8 +1,9 @@
 """Writes the golden vectors of the solve by running the reference itself.
 
-Run in a container where the reference source tree is available (its path is
-the first argument, default /root/reference); the GPU machines never run
-this script, they only read the .npz files it writes next to itself.
+Run in a container where the reference source tree is available: its path
+is the first argument, or the environment variable ANDFN_REFERENCE when no
+argument is given.  The GPU machines never run this script; they only read
+the .npz files it writes next to itself.
 
 For every case the reference builds a seeded network through its public API
 (Fracture, DFN.get_fracture_intersections, set_constant_head_boundary,
@@ -28,6 +29,15 @@ import types
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def reference_path(argv):
+    """The reference source tree: argv[1], else $ANDFN_REFERENCE."""
+    path = argv[1] if len(argv) > 1 else os.environ.get("ANDFN_REFERENCE")
+    if not path or not os.path.isdir(os.path.join(path, "andfn")):
+        sys.exit(f"usage: {os.path.basename(argv[0])} REFERENCE_TREE (or set ANDFN_REFERENCE); "
+                 f"the tree must contain the andfn package (got {path!r})")
+    return path
 
 
 def import_reference(path):
@@ -195,8 +205,7 @@ def run_case(andfn, name, dfn, its, max_error=1e-8, max_ncoef=None, D=50, nheads
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
-    andfn = import_reference(ref)
+    andfn = import_reference(reference_path(sys.argv))
     # Seeds of the 30-disc recipe: flowing networks (one cluster joins both
     # heads) and one whose clusters touch a single head each (q = 0).
     seeds, trivial = [], []

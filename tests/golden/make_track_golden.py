@@ -1,7 +1,7 @@
 """Writes the golden vectors of streamline tracking by running the reference itself.
 
 Run in a container where the reference source tree is available (its path is
-the first argument, default /root/reference; further arguments name the cases
+the first argument, or $ANDFN_REFERENCE; further arguments name the cases
 to write, all by default); the GPU machines never run this
 script, they only read the ``track_*.npz`` files it writes next to itself.
 
@@ -27,15 +27,14 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 
-from make_golden import build_c1, build_mixed, consolidated, import_reference  # noqa: E402
+from make_golden import build_c1, build_mixed, consolidated, import_reference, reference_path  # noqa: E402
 
 CASES = (("mixed", 21, 12, 0.02, 150), ("c1_seed3", 22, 16, 0.01, 300), ("c1_seed13", 23, 16, 0.01, 300))
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     only = set(sys.argv[2:])  # case names to (re)write; all when none are given
-    andfn = import_reference(ref)
+    andfn = import_reference(reference_path(sys.argv[:2]))
     from andfn.hpc.hpc_solve import solve as hpc_solve
     for name, seed, npart, ds, max_length in CASES:
         if only and name not in only:

@@ -1,0 +1,142 @@
+"""GPU parity on the networks the benchmark measures.
+
+  * the plain-solve network (2,118 fractures, 5,376 elements, ncoef 20,
+    nint 40): the GPU after 1 and 3 iterations and at convergence against
+    the reference's own outputs (tests/golden/bench_c2.npz: full q, fracture
+    constants and errors, coefficients of 256 sampled elements); the GPU
+    against the oracle (pinned bit for bit to those outputs,
+    test_oracle_bench_golden.py) on every coefficient after 3 and 10
+    iterations and at convergence, with equal iteration counts; heads at the
+    fixture's 10,000 points against the reference's heads;
+  * the large network (2,588 fractures, 100 impermeable circles, ncoef 30,
+    nint 60): the GPU after 1 and 2 iterations against the reference's
+    outputs, and after 3 iterations against the oracle.
+
+Tolerances (as test_gpu_parity): coefficients, q, constants, dpsi_corr and
+error_coef within 1e-10 * P, P the potential scale of the network (largest
+|coef|, |phi|, |constant|); ncoef and nint exact; heads within
+1e-9 * max(1, |h|).  Each comparison also reports the per-coefficient
+relative error |gpu - ref| / |ref| over the coefficients above 1e-6 P (a
+coefficient far below the potential scale carries few significant digits
+of the scale-sized sums it is fitted from) and requires it below 1e-6.
+"""
+import numpy as np
+import pytest
+
+from conftest import potential_scale
+from test_gpu_parity import _compare
+from test_oracle_bench_golden import golden_and_records
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-10
+
+
+def _gpu_solve(F, E, c):
+    import andfn_b200
+    andfn_b200.solve(F, E, 50, c)
+    return dict(andfn_b200.last_stats)
+
+
+def coef_relative_error(a, b, P):
+    """Largest |a - b| / |b| over the coefficients with |b| > 1e-6 P, and the
+    count of such coefficients."""
+    mag = np.abs(b)
+    sel = mag > 1e-6 * P
+    if not sel.any():
+        return 0.0, 0
+    return float((np.abs(a - b)[sel] / mag[sel]).max()), int(sel.sum())
+
+
+def _compare_fingerprint(g, k, F, E, tag):
+    """GPU state against the reference's stored outputs after k iterations."""
+    p = f"k{k}_"
+    s = g["sample"]
+    assert np.array_equal(E["ncoef"], g[p + "ncoef"]) and np.array_equal(E["nint"], g[p + "nint"]), tag
+    cs = g[p + "coef_sample"]
+    P = float(max(np.abs(cs).max(), np.abs(E["phi"]).max(), np.abs(g[p + "constant"]).max()))
+    for name, a, b in (("coef (sampled elements)", E["coef"][s], cs), ("q", E["q"], g[p + "q"]),
+                       ("constant", F["constant"], g[p + "constant"]),
+                       ("dpsi_corr (sampled elements)", E["dpsi_corr"][s], g[p + "dpsi_corr_sample"]),
+                       ("error_coef", E["error_coef"], g[p + "error_coef"])):
+        d = float(np.abs(a - b).max())
+        assert d <= TOL * P, (tag, name, d / P)
+    rel, n = coef_relative_error(E["coef"][s], cs, P)
+    print(f"{tag}: max |dcoef|/P {np.abs(E['coef'][s] - cs).max() / P:.2e}, per-coefficient relative {rel:.2e} "
+          f"over {n} sampled coefficients")
+    assert rel < 1e-6, (tag, rel)
+
+
+def _compare_oracle(E, F, Eo, Fo, tag):
+    _compare(E, F, Eo, Fo, tag)
+    P = potential_scale(Eo, Fo)
+    rel, n = coef_relative_error(E["coef"], Eo["coef"], P)
+    print(f"{tag}: max |dcoef|/P {np.abs(E['coef'] - Eo['coef']).max() / P:.2e}, per-coefficient relative "
+          f"{rel:.2e} over {n} coefficients")
+    assert rel < 1e-6, (tag, rel)
+
+
+def test_plain_network_matches_reference_outputs():
+    g, F0, E0 = golden_and_records("bench_c2")
+    for k in g["its"]:
+        F, E = F0.copy(), E0.copy()
+        st = _gpu_solve(F, E, g[f"k{k}_constants"])
+        assert st["status"] in (0, 1), st
+        _compare_fingerprint(g, int(k), F, E, ("bench_c2 vs reference", int(k)))
+
+
+@pytest.mark.parametrize("k", [3, 10])
+def test_plain_network_matches_oracle_at_fixed_iterations(k):
+    from andfn_b200.records import default_constants
+    from oracle import oracle as orc
+    _, F0, E0 = golden_and_records("bench_c2")
+    c = default_constants(MAX_ITERATIONS=k, MAX_ERROR=1e-300, MAX_NCOEF=20)
+    F, E = F0.copy(), E0.copy()
+    st = _gpu_solve(F, E, c)
+    assert st["iterations"] == k, st
+    Fo, Eo = F0.copy(), E0.copy()
+    orc.solve(Fo, Eo, 50, c)
+    _compare_oracle(E, F, Eo, Fo, ("bench_c2 vs oracle", k))
+
+
+def test_plain_network_converges_like_the_oracle_and_heads_match_reference():
+    """To convergence at MAX_ERROR 1e-8 (the benchmark's stopping rule):
+    iteration counts equal, every coefficient within the bound, and heads at
+    the fixture's 10,000 points against the reference's heads."""
+    import andfn_b200
+    from oracle import oracle as orc
+    g, F0, E0 = golden_and_records("bench_c2")
+    k = int(g["heads_k"])
+    c = g[f"k{k}_constants"]
+    F, E = F0.copy(), E0.copy()
+    st = _gpu_solve(F, E, c)
+    Fo, Eo = F0.copy(), E0.copy()
+    sto = {}
+    orc.solve(Fo, Eo, 50, c, stats=sto)
+    assert st["status"] == 0 and st["iterations"] == sto["iterations"], (st, sto)
+    assert st["cnt_error"] == sto["cnt_error"]
+    _compare_oracle(E, F, Eo, Fo, ("bench_c2 converged vs oracle", st["iterations"]))
+    with andfn_b200.Solver(F, E, 50) as s:
+        h = s.eval_heads(g["heads_frac"], g["heads_z"])
+    ref = g["heads_ref"]
+    err = np.abs(h - ref) / np.maximum(1.0, np.abs(ref))
+    print(f"bench_c2 heads at {len(ref)} points: max relative error {err.max():.2e}")
+    assert np.all(err <= 1e-9)
+
+
+def test_large_network_matches_reference_and_oracle():
+    from andfn_b200.records import default_constants
+    from oracle import oracle as orc
+    g, F0, E0 = golden_and_records("bench_c5")
+    assert (E0["_type"] == 4).sum() == 100
+    for k in g["its"]:
+        F, E = F0.copy(), E0.copy()
+        st = _gpu_solve(F, E, g[f"k{k}_constants"])
+        assert st["status"] in (0, 1), st
+        _compare_fingerprint(g, int(k), F, E, ("bench_c5 vs reference", int(k)))
+    c = default_constants(MAX_ITERATIONS=3, MAX_ERROR=1e-300, MAX_NCOEF=30)
+    F, E = F0.copy(), E0.copy()
+    _gpu_solve(F, E, c)
+    Fo, Eo = F0.copy(), E0.copy()
+    orc.solve(Fo, Eo, 50, c)
+    _compare_oracle(E, F, Eo, Fo, ("bench_c5 vs oracle", 3))
