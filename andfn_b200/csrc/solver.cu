@@ -43,13 +43,12 @@ static constexpr double PI = 3.141592653589793115997963468544185161590576171875;
 static constexpr int EVAL_THREADS = 128;
 static constexpr int UPDATE_WARPS = 4;
 static constexpr int SOLVE_THREADS = 512;
-// The explicit-inverse solve alone is as accurate as the triangular solves
-// (~1e-10 relative on an ill-conditioned system); its refinement step
-// (accurate to ~1e-15) is applied once both the discharges and the mean
-// coefficients change by less than this between iterations: the iterations
-// that set the converged state (earlier solve errors have been damped by the
-// contraction of the iteration by then).
-static constexpr double WINV_REFINE_BELOW = 1e-6;
+// Discharge solves through the explicit inverse X take one refinement step
+// in every iteration: x0 = X b alone carries errors of a few 1e-9 of the
+// potential scale in the fracture constants of an ill-conditioned system
+// (condition ~6e12 on the 2,118-fracture network), which show in the
+// iterates of the first iterations; x0 + X (b - A x0) is accurate to
+// round-off, so every iterate follows the reference's to 1e-13 or better.
 static constexpr int ITER_BATCH = 8;  // iterations per graph launch (one host status read each)
 
 enum GroupKind { KIND_PHI = 0, KIND_PSI = 1 };
@@ -80,8 +79,8 @@ struct SolveState {
   double error_q, error, error_coef, pad;
   double max_error, damping;
   int max_it, fused_blend2;
-  // explicit-inverse solves: 1 once the refinement step is applied (from the
-  // iteration after error_q and error_coef first fell below WINV_REFINE_BELOW)
+  // explicit-inverse solves: 1 when the refinement step is applied (set at
+  // the start of a run)
   int refine, n_refined;  // n_refined: solves that took the refinement step
   // SM clock cycles spent in the phases of trisolve_kernel, summed over
   // launches (thread 0's view): gather, L sparse, L coupling, L dense,
@@ -134,6 +133,8 @@ struct Net {
   const int *row_frac;       // [N] fracture of a continuity row, -1 otherwise
   int *ndone;                // realizations whose loop has finished
   const struct TriDesc *tri; // [R]
+  // known part of the head vector [N] (wells with a prescribed discharge), or null
+  const double *bknown;
 };
 
 // ------------------------------------------------------------------------
@@ -410,6 +411,12 @@ __global__ void __launch_bounds__(EVAL_THREADS) pair_table_kernel(Net net, const
   }
 }
 
+// A complex128 load with the streaming (evict-first) cache policy.
+__device__ __forceinline__ cd ldcs_cd(const cd *p) {
+  const double2 v = __ldcs(reinterpret_cast<const double2 *>(p));
+  return mk(v.x, v.y);
+}
+
 // One Horner chain sum_k c_k x^k over mm coefficients (c zero beyond the
 // source's own ncoef, so a longer chain gives the same value).
 __device__ __forceinline__ cd horner(const cd *__restrict__ c, int mm, cd x) {
@@ -488,21 +495,23 @@ __global__ void __launch_bounds__(EVAL_THREADS) sweep_table_kernel(Net net, cons
     int s = 0;
     cd xa = mk(0.0, 0.0), xb = mk(0.0, 0.0);
     double la = 0.0, lb = 0.0;
+    // the tables are read once per sweep: streaming (evict-first) loads keep
+    // the L2-resident data of the other kernels (power sums, coefficients)
     if (cnt >= 2) {
-      xa = xw[0];
-      la = xl[0];
-      xb = xw[np];
-      lb = xl[np];
+      xa = ldcs_cd(xw);
+      la = __ldcs(xl);
+      xb = ldcs_cd(xw + np);
+      lb = __ldcs(xl + np);
     }
     for (; s + 1 < cnt; s += 2) {
       // next pair's table entries, in flight while this pair's chains run
       cd na = mk(0.0, 0.0), nb = mk(0.0, 0.0);
       double nla = 0.0, nlb = 0.0;
       if (s + 3 < cnt) {
-        na = xw[(long long)(s + 2) * np];
-        nla = xl[(long long)(s + 2) * np];
-        nb = xw[(long long)(s + 3) * np];
-        nlb = xl[(long long)(s + 3) * np];
+        na = ldcs_cd(xw + (long long)(s + 2) * np);
+        nla = __ldcs(xl + (long long)(s + 2) * np);
+        nb = ldcs_cd(xw + (long long)(s + 3) * np);
+        nlb = __ldcs(xl + (long long)(s + 3) * np);
       }
       const TabSrc ha = src[s], hb = src[s + 1];
       const int mm = max(ha.m, hb.m);
@@ -540,8 +549,8 @@ __global__ void __launch_bounds__(EVAL_THREADS) sweep_table_kernel(Net net, cons
     if (s < cnt) {  // odd source count: the last one alone
       const TabSrc h = src[s];
       if (h.id != exclude) {
-        const cd x = xw[(long long)s * np];
-        const double l = xl[(long long)s * np];
+        const cd x = ldcs_cd(xw + (long long)s * np);
+        const double l = __ldcs(xl + (long long)s * np);
         if (h.m > 0) {
           const cd r = horner(scoef + s * MC, h.m, x);
           acc_re += r.re;
@@ -856,7 +865,6 @@ __global__ void __launch_bounds__(1024) reduce_kernel(Net net) {
     if (!(st->error_q == st->error_q)) nf = 1;
     if (nf) st->nonfinite = 1;
     // hpc_solve.py:237-239
-    if (fmax(st->error_q, ec) < WINV_REFINE_BELOW) st->refine = 1;  // sticky
     if (ec < st->max_error && st->error_q < st->max_error) {
       st->cnt_error += 1;
       st->error_q = 1e30;
@@ -1220,11 +1228,12 @@ __global__ void rhs_reduce_kernel(Net net, const double *__restrict__ rhs_vals, 
   if (st->done || !st->solve_q) return;
   const int r = net.row_de[g];
   if (r < 0) {
-    if (lane == 0) net.bvec[g] = 0.0;
+    if (lane == 0) net.bvec[g] = net.bknown ? net.bknown[g] : 0.0;
     return;
   }
   const int D = net.D;
   const int e = net.de_ids[r];
+  const double bk = net.bknown ? net.bknown[g] : 0.0;
   const Group g0 = groups[rhs_group[2 * r]];
   double s0 = 0.0;
   for (int k = lane; k < D; k += 32) s0 += rhs_vals[g0.out + k];
@@ -1234,9 +1243,9 @@ __global__ void rhs_reduce_kernel(Net net, const double *__restrict__ rhs_vals, 
     double s1 = 0.0;
     for (int k = lane; k < D; k += 32) s1 += rhs_vals[g1.out + k];
     s1 = warp_sum(s1);
-    if (lane == 0) net.bvec[g] = (s1 / D) / net.t[net.frac1[e]] - (s0 / D) / net.t[net.frac0[e]];
+    if (lane == 0) net.bvec[g] = ((s1 / D) / net.t[net.frac1[e]] - (s0 / D) / net.t[net.frac0[e]]) + bk;
   } else if (lane == 0) {
-    net.bvec[g] = net.phi[e] - s0 / D;
+    net.bvec[g] = (net.phi[e] - s0 / D) + bk;
   }
 }
 
@@ -2177,7 +2186,7 @@ __global__ void __launch_bounds__(WINV_THREADS) winv_gemv_kernel(Net net, const 
                                                                  unsigned long long *__restrict__ acc) {
   SolveState *st = net.st;
   if (st->done) return;
-  // forward: without refinement (refine is written by reduce_kernel only)
+  // forward: without refinement (refine is set when the run starts)
   // the first pass writes the result itself and the second does not run;
   // the adjoint's solves are not refined
   const bool fin = ADJ ? true : (STAGE == 1 || !st->refine);
@@ -2679,6 +2688,8 @@ struct HostNet {
   std::vector<int> eoff, foff, doff, roff;
   std::vector<int> real_elem, real_frac, real_row, row_de, row_frac;
   std::vector<double> head;  // prescribed head of constant-head lines and wells
+  // wells whose discharge is prescribed (NaN head): not unknowns of the system
+  std::vector<char> spec_q;
 };
 
 // Discharge system of one realization (local row / column indices).
@@ -2743,6 +2754,13 @@ struct AndfnHandle {
   int N = 0;  // rows of all realizations
   std::vector<RealSys> sys;
   std::vector<int> ent_row, ent_src, ent_side, ent_kind;
+  // known terms of wells with a prescribed discharge: matrix-like entries
+  // (row, source well, side; their values follow the pattern entries in the
+  // assembly arrays from known0 on) and continuity-row terms (row, well)
+  std::vector<int> known_row, known_src, known_side, known_cont_row, known_cont_src;
+  int known0 = 0;
+  bool has_spec = false;
+  DBuf<double> bknown;
   DBuf<int> d_ent_row, d_ent_src, d_ent_side, d_ent_kind;
   DBuf<double> d_mvals;
   double ms_create_upload = 0, ms_create_tables = 0, ms_create_order = 0;
@@ -2897,6 +2915,7 @@ struct AndfnHandle {
     n.row_frac = row_frac.p;
     n.ndone = ndone.p;
     n.tri = tri.p;
+    n.bknown = has_spec ? bknown.p : nullptr;
     return n;
   }
   ~AndfnHandle() {
@@ -2998,6 +3017,11 @@ static int parse_records(AndfnHandle *H, int r, const char *F, int64_t nf, const
     h.err_old2.push_back(rd_f64(rec, L.e_error_old2));
     h.err_coef.push_back(rd_f64(rec, L.e_error_coef));
     h.head.push_back(rd_f64(rec, L.e_head));
+    h.spec_q.push_back(ty == 2 && std::isnan(h.head.back()) ? 1 : 0);
+    if (h.spec_q.back() && !std::isfinite(h.q.back())) {
+      set_error("a well with a prescribed discharge (NaN head) needs a finite q");
+      return ANDFN_BAD_INPUT;
+    }
     h.real_elem.push_back(r);
   }
   H->MC = std::max(H->MC, std::max(1, maxm));
@@ -3030,7 +3054,7 @@ static int parse_records(AndfnHandle *H, int r, const char *F, int64_t nf, const
   const int d0 = (int)h.de_ids.size();
   for (int64_t i = 0; i < ne; i++) {
     const int ty = h.type[e0 + i];
-    if (ty == 0 || ty == 2 || ty == 3) {
+    if ((ty == 0 || ty == 2 || ty == 3) && !h.spec_q[e0 + i]) {
       h.elem_de[e0 + i] = (int)h.de_ids.size();
       h.de_ids.push_back(e0 + (int)i);
     }
@@ -3100,6 +3124,12 @@ static void build_pattern(AndfnHandle *H, int r) {
       for (int k = h.fptr[f]; k < h.fptr[f + 1]; k++) {
         const int ee = h.felem[k];
         if (ee == e || !disch(h.type[ee])) continue;
+        if (h.spec_q[ee]) {  // prescribed discharge: a known term of the row
+          H->known_row.push_back(row0 + j);
+          H->known_src.push_back(ee);
+          H->known_side.push_back(s);
+          continue;
+        }
         S.mcol.push_back(h.elem_de[ee] - d0);
         H->ent_row.push_back(row0 + j);
         H->ent_src.push_back(ee);
@@ -3121,6 +3151,11 @@ static void build_pattern(AndfnHandle *H, int r) {
     for (int k = h.fptr[f]; k < h.fptr[f + 1]; k++) {
       const int el = h.felem[k];
       if (!disch(h.type[el])) continue;
+      if (h.spec_q[el]) {  // +q of the well in its fracture's continuity row
+        H->known_cont_row.push_back(row0 + n_de + (f - f0));
+        H->known_cont_src.push_back(el);
+        continue;
+      }
       S.mcol.push_back(h.elem_de[el] - d0);
       H->ent_row.push_back(row0 + n_de + (f - f0));
       H->ent_src.push_back(el);
@@ -3360,6 +3395,14 @@ static int create_impl(AndfnHandle *H, int R, const char *const *F, const int64_
   H->ent_side.clear();
   H->ent_kind.clear();
   for (int r = 0; r < R; r++) build_pattern(H, r);
+  H->known0 = (int)H->ent_row.size();
+  for (size_t k = 0; k < H->known_row.size(); k++) {
+    H->ent_row.push_back(H->known_row[k]);
+    H->ent_src.push_back(H->known_src[k]);
+    H->ent_side.push_back(H->known_side[k]);
+    H->ent_kind.push_back(0);
+  }
+  for (char c : H->h.spec_q) H->has_spec |= (c != 0);
   H->order_thread = std::thread([H, R]() {
     auto tc2 = std::chrono::steady_clock::now();
 #pragma omp parallel for schedule(dynamic, 1) if (R > 1)
@@ -4217,7 +4260,7 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
   st0.max_it = (int)C->max_iterations;
   st0.fused_blend2 = growth_possible ? 0 : 1;
   st0.solve_q = 1;
-  st0.refine = 0;
+  st0.refine = 1;  // the refinement step in every explicit-inverse solve
   st0.n_refined = 0;
   st0.done = (C->max_iterations <= 0) ? 1 : 0;
   std::vector<SolveState> st_init(R, st0);
@@ -4261,6 +4304,16 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
   CK(cudaMemcpyAsync(H->disc.p, disc0.data(), sizeof(double) * H->N, cudaMemcpyHostToDevice, s));
   g_h2d_bytes += 8 * (int64_t)H->N;
   CK(cudaStreamSynchronize(s));
+  if (H->has_spec) {
+    // the prescribed discharges' terms move to the right-hand side: minus
+    // the entry times q in the rows, minus q in the continuity rows
+    std::vector<double> bk(H->N, 0.0);
+    for (size_t k = 0; k < H->known_row.size(); k++)
+      bk[H->known_row[k]] -= mv[H->known0 + k] * H->h.q[H->known_src[k]];
+    for (size_t k = 0; k < H->known_cont_row.size(); k++) bk[H->known_cont_row[k]] -= H->h.q[H->known_cont_src[k]];
+    CK(upload(H->bknown, bk, s));
+    g_h2d_bytes += 8 * (int64_t)H->N;
+  }
   base.ms_setup = ms_since(t_setup);
   // factorisation (host)
   auto t_fac = std::chrono::steady_clock::now();
@@ -5556,9 +5609,9 @@ __global__ void __launch_bounds__(EVAL_THREADS) adj_sweep_table_kernel(
     for (int i = lane; i < npt; i += 32) {
       const double w = s_w[i];
       if (w == 0.0 || s_ex[i] == el) continue;
-      const cd x = xs[i];
+      const cd x = ldcs_cd(xs + i);
       const double wv = w * sg;
-      if (disch) qc += wv / (2 * PI) * ls[i];
+      if (disch) qc += wv / (2 * PI) * __ldcs(ls + i);
       const bool psi = s_psi[i] != 0;
       cd pw = mk(1.0, 0.0);
 #pragma unroll
@@ -5672,7 +5725,7 @@ __global__ void head_vector_kernel(Net net, const int *__restrict__ gptr, const 
   if (st->done || !st->solve_q) return;
   const int r = net.row_de[g];
   if (r < 0) {
-    if (lane == 0) net.bvec[g] = 0.0;
+    if (lane == 0) net.bvec[g] = net.bknown ? net.bknown[g] : 0.0;
     return;
   }
   const int e = net.de_ids[r];
@@ -5699,10 +5752,12 @@ __global__ void head_vector_kernel(Net net, const int *__restrict__ gptr, const 
   }
   if (lane == 0) {
     const double D = net.D;
+    double b;
     if (sides == 2)
-      net.bvec[g] = (sum[1] / D) / net.t[net.frac1[e]] - (sum[0] / D) / net.t[net.frac0[e]];
+      b = (sum[1] / D) / net.t[net.frac1[e]] - (sum[0] / D) / net.t[net.frac0[e]];
     else
-      net.bvec[g] = net.phi[e] - sum[0] / D;
+      b = net.phi[e] - sum[0] / D;
+    net.bvec[g] = net.bknown ? b + net.bknown[g] : b;
   }
 }
 
@@ -6352,6 +6407,10 @@ static int adjoint_impl(AndfnHandle *H, const double *gcoef, int64_t mco, const 
     set_error("the adjoint needs a single-network handle");
     return ANDFN_BAD_INPUT;
   }
+  if (H->has_spec) {
+    set_error("the adjoint does not cover wells with a prescribed discharge (NaN head)");
+    return ANDFN_BAD_INPUT;
+  }
   if (!H->have_solution || H->lu_keep.n != H->N) {
     set_error("the adjoint needs a completed run() on this handle (and no reset since)");
     return ANDFN_BAD_INPUT;
@@ -6794,7 +6853,7 @@ __global__ void bc_residual_kernel(Net net, double hscale, double qscale, double
     }
   } else if (type == 2) {
     const double t0 = net.t[f0], head = net.phi[e] / t0;
-    if (lane < 16) {
+    if (lane < 16 && head == head) {  // a NaN head: the well's discharge is prescribed instead
       double sn, cs;
       sincos(2 * PI * lane / 16, &sn, &cs);
       const cd z = mk(net.center[e].re + net.radius[e] * cs, net.center[e].im + net.radius[e] * sn);

@@ -42,6 +42,7 @@ class Element:
     head: float = 0.0
     ncoef: int = 0
     nint: int = 0
+    q: float = 0.0
 
 
 @dataclass
@@ -248,7 +249,7 @@ def _prune(net, keep):
     root = _clusters(net)
     bnd = {}
     for e in net.elements:
-        if e.type in (2, 3):
+        if e.type in (2, 3) and not np.isnan(e.head):  # a NaN head: prescribed discharge, no head boundary
             bnd.setdefault(root[e.frac0], set()).add(e.head)
     if keep == "connected":
         keep_roots = set(bnd)
@@ -283,9 +284,15 @@ def _prune(net, keep):
     return out
 
 
-def add_well(net, frac, center, radius, head):
-    """A head-specified well on a fracture (andfn/well.py)."""
-    net.elements.append(Element(type=2, frac0=frac, radius=radius, center=complex(center), head=head))
+def add_well(net, frac, center, radius, head, q=None):
+    """A well on a fracture: head-specified (andfn/well.py), or, with q given,
+    with that prescribed discharge (head NaN; an extension of the reference,
+    whose wells prescribe a head)."""
+    if q is None:
+        e = Element(type=2, frac0=frac, radius=radius, center=complex(center), head=head)
+    else:
+        e = Element(type=2, frac0=frac, radius=radius, center=complex(center), head=float("nan"), q=float(q))
+    net.elements.append(e)
     net.frac_elems[frac].append(len(net.elements) - 1)
 
 
@@ -332,6 +339,7 @@ def to_records(net, max_ncoef=None, max_elements=None):
         r["center"] = e.center
         r["head"] = e.head
         r["phi"] = e.head * net.t[e.frac0] if e.type in (2, 3) else 0.0  # Fracture.phi_from_head
+        r["q"] = e.q
         r["ncoef"] = e.ncoef
         r["nint"] = e.nint
     F["_id"] = np.arange(nf)
@@ -412,10 +420,11 @@ def _seg_dist(z, a, b):
     return abs(z - (a + t * d))
 
 
-def place_wells(net, rng, n, radius=0.05, head=(0.0, 1.0), clearance=10.0, rim=0.8, tries=200):
-    """n head-specified wells at uniform random points (inside rim * R) of
-    random fractures, at least clearance * radius away from every line
-    element of that fracture and from the other wells."""
+def place_wells(net, rng, n, radius=0.05, head=(0.0, 1.0), clearance=10.0, rim=0.8, tries=200, q=None):
+    """n wells at uniform random points (inside rim * R) of random fractures,
+    at least clearance * radius away from every line element of that fracture
+    and from the other wells; head-specified with head U[head], or, when q is
+    a range, with a prescribed discharge U[q]."""
     nf = len(net.radii)
     for _ in range(n):
         for _t in range(tries):
@@ -433,21 +442,32 @@ def place_wells(net, rng, n, radius=0.05, head=(0.0, 1.0), clearance=10.0, rim=0
                 if not ok:
                     break
             if ok:
-                add_well(net, f, z, radius, float(rng.uniform(*head)))
+                if q is None:
+                    add_well(net, f, z, radius, float(rng.uniform(*head)))
+                else:
+                    add_well(net, f, z, radius, float("nan"), q=float(rng.uniform(*q)))
                 break
 
 
-def batch_realization(seed, L=40.0, nf_range=(200, 800), wells=4, ncoef=15, nint=30, **kw):
+def batch_realization(seed, L=40.0, nf_range=(200, 800), wells=4, ncoef=15, nint=30, well_q=(-1e-4, 1e-4), **kw):
     """One realization of the batched workload: N_gen ~ U{200..800} discs drawn
     as power_law_fisher in an L cube, head planes 1 / 0 at x = 0 / L, then
-    `wells` head-specified wells (radius 0.05 m, head U[0, 1]) on random
-    fractures; the fractures connected to a head boundary (plane or well) are
-    kept, as check_connectivity does."""
+    `wells` wells (radius 0.05 m) with a prescribed discharge U[well_q]
+    (m^3/s) at random points of random fractures of the clusters that touch
+    a head plane (the fractures kept, as check_connectivity does: a well in a
+    cluster without a head boundary would have no steady state).  With
+    well_q=None the wells are head-specified (head U[0, 1]) and placed before
+    the pruning, so clusters joined to a well are kept too."""
     rng = np.random.default_rng([seed, 7])
     nf = int(rng.integers(nf_range[0], nf_range[1] + 1))
     net = power_law_fisher(seed, nf, L, ncoef=ncoef, nint=nint, keep="all", **kw)
-    place_wells(net, rng, wells)
-    return _prune(net, "connected")
+    if well_q is None:
+        place_wells(net, rng, wells)
+        return _prune(net, "connected")
+    net = _prune(net, "connected")
+    if len(net.radii):
+        place_wells(net, rng, wells, q=well_q)
+    return net
 
 
 def place_impermeable_circles(net, rng, n, rmin=1.0, rmax=3.0, ncoef=30, nint=60, clearance=1.2, tries=500):

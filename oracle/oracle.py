@@ -118,6 +118,14 @@ def discharge_element_ids(elements: np.ndarray) -> np.ndarray:
     return np.nonzero((t == 0) | (t == 2) | (t == 3))[0].astype(np.int64)
 
 
+def specified_discharge_wells(elements: np.ndarray) -> np.ndarray:
+    """Mask of the wells whose discharge is prescribed (an extension: the
+    reference's wells prescribe a head, andfn/well.py:38, and their q is an
+    unknown of the discharge system, hpc_solve.py:1451-1459).  Such a well is
+    marked by a NaN head; its record's q is the prescribed discharge."""
+    return (elements["_type"] == 2) & np.isnan(elements["head"])
+
+
 class Oracle:
     """State of one oracle solve (the reference's work_array and tables)."""
 
@@ -224,8 +232,31 @@ def solve(fracture_struc_array, element_struc_array, discharge_int, constants, n
     discharges[: o.n_de] = E["q"][o.de]
     discharges[o.n_de: o.n_de + o.nf] = F["constant"]
     discharges = discharges[:size] if len(discharges) >= size else np.pad(discharges, (0, size - len(discharges)))
-    discharges_old = np.zeros(size)
     A = o.build_matrix()
+    # Wells with a prescribed discharge (specified_discharge_wells): their
+    # rows and columns leave the system, and their known discharge moves to
+    # the right-hand side of the other rows (the matrix entry times q, and
+    # the well's +q in its fracture's continuity row).
+    spec = np.zeros(size, bool)
+    spec[: o.n_de] = specified_discharge_wells(E)[o.de]
+    keep = ~spec
+    q_spec = E["q"][o.de[spec[: o.n_de]]].copy()
+    b_known = None
+    if spec.any():
+        A = A.tocsr()
+        b_known = -(A[keep][:, np.nonzero(spec)[0]] @ q_spec)
+        A = A[keep][:, keep].tocsc()
+        discharges = discharges[keep]
+    discharges_old = np.zeros(len(discharges))
+
+    def scatter(x):
+        if b_known is None:
+            return x
+        full = np.zeros(size)
+        full[keep] = x
+        full[spec] = q_spec
+        return full
+
     t_mat = time.perf_counter()
     lu = spla.splu(A)
     t_lu = time.perf_counter()
@@ -244,8 +275,10 @@ def solve(fracture_struc_array, element_struc_array, discharge_int, constants, n
         if error_q > max_error / 1e30:
             discharges_old[:] = discharges[:]
             head = o.head_vector()
+            if b_known is not None:
+                head = head[keep] + b_known
             discharges[:] = lu.solve(head)
-            o.post_solve(discharges)
+            o.post_solve(scatter(discharges))
             error_q = np.max(np.abs(discharges - discharges_old) / (np.max(np.abs(discharges_old)) + 1e-16))
         t1 = time.perf_counter()
         o.element_solver2(max_error, nit, coef_ratio, max_coef, coef_increase, damping)
@@ -262,7 +295,7 @@ def solve(fracture_struc_array, element_struc_array, discharge_int, constants, n
             error_q = 1e30
     if stats is not None:
         stats.update(dict(iterations=nit, cnt_error=cnt_error, error=error, error_coef=error_coef,
-                          error_q=float(error_q), worst_element=_id, n_unknowns=size, nnz_matrix=A.nnz,
+                          error_q=float(error_q), worst_element=_id, n_unknowns=A.shape[0], nnz_matrix=A.nnz,
                           nnz_factors=int(lu.L.nnz + lu.U.nnz), s_matrix=t_mat - t_start, s_lu=t_lu - t_mat,
                           s_discharge=t_q, s_elements=t_e, s_total=time.perf_counter() - t_start,
                           threads=lib().oracle_num_threads()))

@@ -158,8 +158,8 @@ def test_generated_network_with_cluster_dense_tail_matches_oracle(inverse, monke
     F, E = F0.copy(), E0.copy()
     st = _gpu_solve(F, E, 50, c)
     assert st["dense_tail"] >= 256 and st["iterations"] == 120 and st["explicit_inverse"] == inverse, st
-    if inverse:  # unrefined solves early, refined ones once the changes fall below 1e-6
-        assert 0 < st["refined_solves"] < 120, st
+    if inverse:  # every explicit-inverse solve takes the refinement step
+        assert st["refined_solves"] == 120, st
     Fo, Eo = F0.copy(), E0.copy()
     orc.solve(Fo, Eo, 50, c)
     _compare(E, F, Eo, Fo, ("cluster tail", 120))
