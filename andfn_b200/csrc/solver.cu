@@ -28,6 +28,8 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -417,36 +419,26 @@ __device__ __forceinline__ cd ldcs_cd(const cd *p) {
   return mk(v.x, v.y);
 }
 
-// One Horner chain sum_k c_k x^k over mm coefficients (c zero beyond the
-// source's own ncoef, so a longer chain gives the same value).
-__device__ __forceinline__ cd horner(const cd *__restrict__ c, int mm, cd x) {
-  cd r = c[mm - 1];
-  for (int k = mm - 2; k >= 0; k--) r = fma_c(r, x, c[k]);
-  return r;
-}
-
-// The sweep from the pair tables: one thread per collocation point of one
-// item (fracture, <= EVAL_THREADS points); the item's sources are staged in
-// shared memory (signed coefficients, zero-padded to MC, ncoef, q / 2 pi,
-// id), and every thread walks them two at a time (two independent Horner
-// chains), loading the next pair's table entries before the current pair's
-// chains run.  Output as eval_kernel<false>.
+// The sweep from the pair tables, one item (fracture, <= EVAL_THREADS
+// collocation points; one thread per point).  The item's sources are staged
+// in shared memory (signed coefficients, zero-padded to MC, ncoef,
+// q / 2 pi, id), and every thread walks them two at a time (two independent
+// Horner chains), loading the next pair's table entries before the current
+// pair's chains run.  The table loads are streaming (evict-first): the
+// tables are read once per sweep, and the power sums and coefficients of the
+// other kernels should stay in L2.  Output as eval_kernel<false>.
 struct TabSrc {
   int id, m;
   double qk;
 };
-__global__ void __launch_bounds__(EVAL_THREADS) sweep_table_kernel(Net net, const Item *__restrict__ items,
-                                                                     const int2 *__restrict__ pts,
-                                                                     const Group *__restrict__ groups,
-                                                                     const int *__restrict__ fpt0,
-                                                                     const int *__restrict__ fnp,
-                                                                     const long long *__restrict__ tab_off,
-                                                                     const cd *__restrict__ tw,
-                                                                     const double *__restrict__ tl,
-                                                                     double *__restrict__ out, int chunk) {
-  const Item it = items[blockIdx.x];
+
+__device__ __forceinline__ void sweep_table_item(const Net &net, const Item it, const int2 *__restrict__ pts,
+                                                 const Group *__restrict__ groups, const int *__restrict__ fpt0,
+                                                 const int *__restrict__ fnp, const long long *__restrict__ tab_off,
+                                                 const cd *__restrict__ tw, const double *__restrict__ tl,
+                                                 double *__restrict__ out, int chunk) {
   const int f = it.frac;
-  if (net.st[net.real_frac[f]].done) return;
+  if (net.st[net.real_frac[f]].done) return;  // uniform over the CTA
   extern __shared__ __align__(16) unsigned char smem_raw[];
   TabSrc *src = reinterpret_cast<TabSrc *>(smem_raw);
   cd *scoef = reinterpret_cast<cd *>(smem_raw + sizeof(TabSrc) * chunk);
@@ -495,8 +487,6 @@ __global__ void __launch_bounds__(EVAL_THREADS) sweep_table_kernel(Net net, cons
     int s = 0;
     cd xa = mk(0.0, 0.0), xb = mk(0.0, 0.0);
     double la = 0.0, lb = 0.0;
-    // the tables are read once per sweep: streaming (evict-first) loads keep
-    // the L2-resident data of the other kernels (power sums, coefficients)
     if (cnt >= 2) {
       xa = ldcs_cd(xw);
       la = __ldcs(xl);
@@ -504,7 +494,7 @@ __global__ void __launch_bounds__(EVAL_THREADS) sweep_table_kernel(Net net, cons
       lb = __ldcs(xl + np);
     }
     for (; s + 1 < cnt; s += 2) {
-      // next pair's table entries, in flight while this pair's chains run
+      // the next pair's table entries, in flight while this pair's chains run
       cd na = mk(0.0, 0.0), nb = mk(0.0, 0.0);
       double nla = 0.0, nlb = 0.0;
       if (s + 3 < cnt) {
@@ -552,7 +542,9 @@ __global__ void __launch_bounds__(EVAL_THREADS) sweep_table_kernel(Net net, cons
         const cd x = ldcs_cd(xw + (long long)s * np);
         const double l = __ldcs(xl + (long long)s * np);
         if (h.m > 0) {
-          const cd r = horner(scoef + s * MC, h.m, x);
+          const cd *c = scoef + s * MC;
+          cd r = c[h.m - 1];
+          for (int k = h.m - 2; k >= 0; k--) r = fma_c(r, x, c[k]);
           acc_re += r.re;
           acc_im += r.im;
         }
@@ -564,6 +556,50 @@ __global__ void __launch_bounds__(EVAL_THREADS) sweep_table_kernel(Net net, cons
     }
   }
   if (active) out[gout] = (kind == KIND_PSI) ? acc_im : (acc_re + net.constant[f]);
+}
+
+// One CTA per item (the hardware block scheduler hands out the items, which
+// are sorted by estimated cost, largest first).
+__global__ void __launch_bounds__(EVAL_THREADS) sweep_table_kernel(Net net, const Item *__restrict__ items,
+                                                                     const int2 *__restrict__ pts,
+                                                                     const Group *__restrict__ groups,
+                                                                     const int *__restrict__ fpt0,
+                                                                     const int *__restrict__ fnp,
+                                                                     const long long *__restrict__ tab_off,
+                                                                     const cd *__restrict__ tw,
+                                                                     const double *__restrict__ tl,
+                                                                     double *__restrict__ out, int chunk) {
+  sweep_table_item(net, items[blockIdx.x], pts, groups, fpt0, fnp, tab_off, tw, tl, out, chunk);
+}
+
+// Persistent form: a grid of a few CTAs per SM takes the items (largest
+// first) from a device work queue, one atomic fetch per item; the last CTA
+// to finish resets the queue for the next launch.
+struct WorkQueue {
+  int next, done;
+};
+__global__ void __launch_bounds__(EVAL_THREADS) sweep_table_queue_kernel(
+    Net net, const Item *__restrict__ items, int n_items, const int2 *__restrict__ pts,
+    const Group *__restrict__ groups, const int *__restrict__ fpt0, const int *__restrict__ fnp,
+    const long long *__restrict__ tab_off, const cd *__restrict__ tw, const double *__restrict__ tl,
+    double *__restrict__ out, int chunk, WorkQueue *q) {
+  __shared__ int s_next;
+  while (true) {
+    if (threadIdx.x == 0) s_next = atomicAdd(&q->next, 1);
+    __syncthreads();
+    const int i = s_next;
+    __syncthreads();  // every thread has read s_next before thread 0 fetches again
+    if (i >= n_items) break;
+    sweep_table_item(net, items[i], pts, groups, fpt0, fnp, tab_off, tw, tl, out, chunk);
+  }
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(&q->done, 1) == (int)gridDim.x - 1) {  // every CTA has stopped fetching
+      q->next = 0;
+      q->done = 0;
+      __threadfence();
+    }
+  }
 }
 
 // ------------------------------------------------------------------------
@@ -714,6 +750,8 @@ __global__ void __launch_bounds__(UPDATE_WARPS * 32) update_kernel(Net net, cons
     cd w = neww[j], c = cc[j];
     for (int b = 0; b < nb; b++) c = mk(d * w.re + (1 - d) * c.re, d * w.im + (1 - d) * c.im);
     cc[j] = c;
+    // a non-finite leading coefficient ends the realization's loop (read by reduce_kernel)
+    if (j == 0 && !isfinite(c.re)) st->nonfinite = 1;
   }
 }
 
@@ -818,7 +856,6 @@ __global__ void __launch_bounds__(1024) reduce_kernel(Net net) {
     } else if (bec == bec && ec > bec) {
       bec = ec;
     }
-    if (!isfinite(net.coef[(size_t)i * net.MC].re)) nonfin = 1;
   }
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   for (int o = 16; o > 0; o >>= 1) {
@@ -2313,6 +2350,426 @@ __global__ void winv_resid_kernel(Net net, const int *__restrict__ rp, const int
 }
 
 // out (cols x ldo, row-major) = in^T for in (rows x ldi, row-major).
+// ------------------------------------------------------------------------
+// Batched realizations: an explicit inverse per realization.  A batch's
+// systems are small (tens to a few hundred unknowns), and a level-scheduled
+// triangular solve of one is a chain of dependent levels in one CTA; their
+// inverses (26 MB for the 256 realizations of the batched workload) stay in
+// L2, and each solve is two matrix-vector products of one CTA.
+//
+// batch_inverse_kernel: one CTA per realization forms X = A^-1 by in-place
+// Gauss-Jordan elimination with partial pivoting (the largest |a_ik| of the
+// column, the first row on a tie; the row interchanges are undone as column
+// interchanges in reverse order at the end), in shared memory when the
+// matrix fits, else in place in the output (global memory, L2-resident).  A
+// zero or non-finite pivot marks the realization singular.  The dense A is
+// scattered from the assembled entries (CSR: row g's entries [ptr[g],
+// ptr[g+1]) of vals, local columns in col).
+// ------------------------------------------------------------------------
+static constexpr int BINV_THREADS = 512;
+static constexpr int BINV_SOLVE_THREADS = 512;
+static constexpr int BINV_MAX_N = 4096;  // three n-vectors of the solve kernel in shared memory
+
+__global__ void __launch_bounds__(BINV_THREADS) batch_inverse_kernel(const int *__restrict__ order,
+                                                                     const int *__restrict__ roff,
+                                                                     const long long *__restrict__ xoff,
+                                                                     double *__restrict__ Xall,
+                                                                     const int *__restrict__ ptr,
+                                                                     const int *__restrict__ col,
+                                                                     const double *__restrict__ vals, int *sing,
+                                                                     int smem_n) {
+  const int r = order[blockIdx.x];
+  const int row0 = roff[r], n = roff[r + 1] - row0;
+  double *Xg = Xall + xoff[r];
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double *sm = reinterpret_cast<double *>(smem_raw);
+  const bool in_smem = n <= smem_n;
+  double *A = in_smem ? sm : Xg;
+  double *rowk = in_smem ? sm + (size_t)n * n : sm;
+  double *colk = rowk + n;
+  int *ip = reinterpret_cast<int *>(colk + n);
+  __shared__ double s_best[BINV_THREADS / 32];
+  __shared__ int s_idx[BINV_THREADS / 32];
+  __shared__ int s_p, s_bad;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = BINV_THREADS / 32;
+  for (long long i = tid; i < (long long)n * n; i += BINV_THREADS) A[i] = 0.0;
+  if (tid == 0) s_bad = 0;
+  __syncthreads();
+  for (int i = tid; i < n; i += BINV_THREADS)
+    for (int p = ptr[row0 + i]; p < ptr[row0 + i + 1]; p++) A[(size_t)i * n + col[p]] += vals[p];
+  __syncthreads();
+  for (int k = 0; k < n; k++) {
+    // pivot: the largest |a_ik|, i >= k; the first such row on a tie; a
+    // NaN anywhere in the column marks the system singular
+    double best = -1.0;
+    int bi = n, nan_seen = 0;
+    for (int i = k + tid; i < n; i += BINV_THREADS) {
+      const double v = fabs(A[(size_t)i * n + k]);
+      if (!(v == v))
+        nan_seen = 1;
+      else if (v > best) {  // rows ascend per thread: strict > keeps the first
+        best = v;
+        bi = i;
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      nan_seen |= __shfl_xor_sync(0xffffffffu, nan_seen, o);
+      if (ob > best || (ob == best && oi < bi)) {
+        best = ob;
+        bi = oi;
+      }
+    }
+    if (lane == 0) {
+      s_best[warp] = best;
+      s_idx[warp] = bi;
+      if (nan_seen) s_bad = 1;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      double b = s_best[0];
+      int p = s_idx[0];
+      for (int w = 1; w < nw; w++)
+        if (s_best[w] > b || (s_best[w] == b && s_idx[w] < p)) {
+          b = s_best[w];
+          p = s_idx[w];
+        }
+      if (!(b > 0.0) || !(b < INFINITY) || p >= n) s_bad = 1;  // zero or infinite pivot
+      s_p = p;
+      ip[k] = p;
+    }
+    __syncthreads();
+    if (s_bad) break;
+    const int p = s_p;
+    if (p != k)
+      for (int j = tid; j < n; j += BINV_THREADS) {
+        const double t = A[(size_t)k * n + j];
+        A[(size_t)k * n + j] = A[(size_t)p * n + j];
+        A[(size_t)p * n + j] = t;
+      }
+    __syncthreads();
+    const double inv = 1.0 / A[(size_t)k * n + k];
+    for (int j = tid; j < n; j += BINV_THREADS) {
+      rowk[j] = (j == k ? 1.0 : A[(size_t)k * n + j]) * inv;
+      colk[j] = A[(size_t)j * n + k];
+    }
+    __syncthreads();
+    for (int i = warp; i < n; i += nw) {
+      double *Ai = A + (size_t)i * n;
+      if (i == k) {
+        for (int j = lane; j < n; j += 32) Ai[j] = rowk[j];
+      } else {
+        const double ci = colk[i];
+        for (int j = lane; j < n; j += 32) Ai[j] = (j == k) ? -ci * inv : fma(-ci, rowk[j], Ai[j]);
+      }
+    }
+    __syncthreads();
+  }
+  if (s_bad) {
+    if (tid == 0) sing[r] = 1;
+    return;
+  }
+  // undo the row interchanges: columns k and ip[k], in reverse order
+  for (int k = n - 1; k >= 0; k--) {
+    const int p = ip[k];
+    if (p != k)
+      for (int i = tid; i < n; i += BINV_THREADS) {
+        const double t = A[(size_t)i * n + k];
+        A[(size_t)i * n + k] = A[(size_t)i * n + p];
+        A[(size_t)i * n + p] = t;
+      }
+    __syncthreads();
+  }
+  if (in_smem)
+    for (long long i = tid; i < (long long)n * n; i += BINV_THREADS) Xg[i] = A[i];
+  if (tid == 0) sing[r] = 0;
+}
+
+// The same Gauss-Jordan elimination for a realization too large for one
+// CTA's shared memory: a cluster of BINV_CLUSTER CTAs holds the matrix in
+// their shared memories, CTA c the rows [c rpc, (c + 1) rpc), rpc =
+// ceil(n / BINV_CLUSTER).  Pivot step k:
+//   1. each CTA finds the largest |a_ik| of its rows i >= k (first on a tie;
+//      NaN flags the system) and publishes it; cluster barrier;
+//   2. every CTA reads the BINV_CLUSTER candidates (distributed shared
+//      memory) and takes the same pivot row p;
+//   3. every CTA copies the old row p into its own buffer, and p's owner
+//      copies the old row k; cluster barrier (no row is written before every
+//      remote read of it is done);
+//   4. each CTA forms the scaled pivot row from its copy, p's owner stores
+//      the old row k as row p, and every CTA updates its own rows (row k
+//      becomes the scaled pivot row).
+// A step's writes to a row happen after the step's second barrier, and the
+// next step's remote reads after the next step's first barrier, which every
+// CTA reaches only after finishing this step.  All CTAs take the same
+// decisions (from the same candidates), so they pass the same barriers.
+static constexpr int BINV_CLUSTER = 8;
+static constexpr size_t BINV_CLUSTER_SMEM_MAX = 220 * 1024;
+
+__host__ __device__ __forceinline__ size_t binv_cluster_smem(int n) {
+  const size_t rpc = (size_t)(n + BINV_CLUSTER - 1) / BINV_CLUSTER;
+  return sizeof(double) * (rpc * n + 3 * (size_t)n) + sizeof(int) * (size_t)n + 16;
+}
+
+__global__ void __launch_bounds__(BINV_THREADS) batch_inverse_cluster_kernel(
+    const int *__restrict__ big, const int *__restrict__ roff, const long long *__restrict__ xoff,
+    double *__restrict__ Xall, const int *__restrict__ ptr, const int *__restrict__ col,
+    const double *__restrict__ vals, int *sing) {
+  cg::cluster_group cluster = cg::this_cluster();
+  const int crank = (int)cluster.block_rank();
+  const int r = big[blockIdx.x / BINV_CLUSTER];
+  const int row0 = roff[r], n = roff[r + 1] - row0;
+  const int rpc = (n + BINV_CLUSTER - 1) / BINV_CLUSTER;
+  const int my0 = min(n, crank * rpc), my1 = min(n, my0 + rpc);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double *A = reinterpret_cast<double *>(smem_raw);  // my rows, row-major (rpc x n)
+  double *prow = A + (size_t)rpc * n;                // old pivot row
+  double *rowk = prow + n;                           // scaled pivot row
+  double *rkold = rowk + n;                          // old row k (p's owner)
+  int *ip = reinterpret_cast<int *>(rkold + n);
+  __shared__ double s_cv[2];
+  __shared__ int s_ci[2];
+  __shared__ double s_best[BINV_THREADS / 32];
+  __shared__ int s_idx[BINV_THREADS / 32];
+  __shared__ int s_p, s_bad, s_nan;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = BINV_THREADS / 32;
+  for (long long i = tid; i < (long long)rpc * n; i += BINV_THREADS) A[i] = 0.0;
+  if (tid == 0) {
+    s_bad = 0;
+    s_nan = 0;
+  }
+  __syncthreads();
+  for (int i = my0 + tid; i < my1; i += BINV_THREADS)
+    for (int p = ptr[row0 + i]; p < ptr[row0 + i + 1]; p++) A[(size_t)(i - my0) * n + col[p]] += vals[p];
+  __syncthreads();
+  int bad = 0;
+  for (int k = 0; k < n; k++) {
+    const int par = k & 1;
+    // 1. this CTA's candidate
+    double best = -1.0;
+    int bi = n, nan_seen = 0;
+    for (int i = max(k, my0) + tid; i < my1; i += BINV_THREADS) {
+      const double v = fabs(A[(size_t)(i - my0) * n + k]);
+      if (!(v == v))
+        nan_seen = 1;
+      else if (v > best) {
+        best = v;
+        bi = i;
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      nan_seen |= __shfl_xor_sync(0xffffffffu, nan_seen, o);
+      if (ob > best || (ob == best && oi < bi)) {
+        best = ob;
+        bi = oi;
+      }
+    }
+    if (lane == 0) {
+      s_best[warp] = best;
+      s_idx[warp] = bi;
+      if (nan_seen) s_nan = 1;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      double b = s_best[0];
+      int p = s_idx[0];
+      for (int w = 1; w < nw; w++)
+        if (s_best[w] > b || (s_best[w] == b && s_idx[w] < p)) {
+          b = s_best[w];
+          p = s_idx[w];
+        }
+      s_cv[par] = s_nan ? NAN : b;
+      s_ci[par] = p;
+    }
+    cluster.sync();
+    // 2. the pivot, from every CTA's candidate
+    if (tid == 0) {
+      double b = -1.0;
+      int p = n, anynan = 0;
+      for (int c = 0; c < BINV_CLUSTER; c++) {
+        const double cv = *cluster.map_shared_rank(&s_cv[par], c);
+        const int ci = *cluster.map_shared_rank(&s_ci[par], c);
+        if (!(cv == cv))
+          anynan = 1;
+        else if (cv > b || (cv == b && ci < p)) {
+          b = cv;
+          p = ci;
+        }
+      }
+      s_bad = (anynan || !(b > 0.0) || !(b < INFINITY) || p >= n) ? 1 : 0;
+      s_p = p;
+    }
+    __syncthreads();
+    if (s_bad) {
+      bad = 1;
+      break;
+    }
+    const int p = s_p;
+    const int ownk = k / rpc, ownp = p / rpc;
+    // 3. copies of the old rows p (every CTA) and k (p's owner)
+    {
+      const double *rp = cluster.map_shared_rank(A, ownp) + (size_t)(p - ownp * rpc) * n;
+      for (int j = tid; j < n; j += BINV_THREADS) prow[j] = rp[j];
+      if (crank == ownp && p != k) {
+        const double *rk = cluster.map_shared_rank(A, ownk) + (size_t)(k - ownk * rpc) * n;
+        for (int j = tid; j < n; j += BINV_THREADS) rkold[j] = rk[j];
+      }
+    }
+    cluster.sync();
+    // 4. the scaled pivot row, the interchange, the update of this CTA's rows
+    const double inv = 1.0 / prow[k];
+    for (int j = tid; j < n; j += BINV_THREADS) rowk[j] = (j == k ? 1.0 : prow[j]) * inv;
+    if (crank == ownp && p != k)
+      for (int j = tid; j < n; j += BINV_THREADS) A[(size_t)(p - my0) * n + j] = rkold[j];
+    if (tid == 0) ip[k] = p;
+    __syncthreads();
+    for (int i = my0 + warp; i < my1; i += nw) {
+      double *Ai = A + (size_t)(i - my0) * n;
+      if (i == k) {
+        for (int j = lane; j < n; j += 32) Ai[j] = rowk[j];
+      } else {
+        const double ci = Ai[k];
+        __syncwarp();
+        for (int j = lane; j < n; j += 32) Ai[j] = (j == k) ? -ci * inv : fma(-ci, rowk[j], Ai[j]);
+      }
+    }
+    __syncthreads();
+  }
+  if (!bad) {
+    // undo the row interchanges: columns k and ip[k] of this CTA's rows, in reverse order
+    for (int k = n - 1; k >= 0; k--) {
+      const int p = ip[k];
+      if (p != k)
+        for (int i = my0 + tid; i < my1; i += BINV_THREADS) {
+          double *Ai = A + (size_t)(i - my0) * n;
+          const double t = Ai[k];
+          Ai[k] = Ai[p];
+          Ai[p] = t;
+        }
+      __syncthreads();
+    }
+    double *Xg = Xall + xoff[r];
+    for (long long i = tid; i < (long long)(my1 - my0) * n; i += BINV_THREADS) Xg[(size_t)my0 * n + i] = A[i];
+  }
+  cluster.sync();  // no CTA leaves while another may still read its shared memory
+  if (crank == 0 && tid == 0) sing[r] = bad;
+}
+
+// One discharge solve of every realization, one CTA each: x0 = X b,
+// r = b - A x0 (the assembled entries), x = x0 + X r; then, as the
+// triangular solve's epilogue, error_q = max|x - x_old| / (max|x_old| + 1e-16)
+// (hpc_solve.py:169-174) and the scatter of q and the fracture constants
+// (post_matrix_solve, hpc_solve.py:721-761).
+// out = X v for an n x n row-major X (L2-resident) and v in shared memory:
+// each warp takes four rows at a time, its lanes split the columns, eight
+// independent loads in flight per lane.
+__device__ __forceinline__ void binv_gemv(const double *__restrict__ X, int n, const double *v, double *out) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = BINV_SOLVE_THREADS / 32;
+  for (int i0 = warp * 4; i0 < n; i0 += nw * 4) {
+    const double *X0 = X + (size_t)i0 * n;
+    const bool h1 = i0 + 1 < n, h2 = i0 + 2 < n, h3 = i0 + 3 < n;
+    const double *X1 = h1 ? X0 + n : X0, *X2 = h2 ? X0 + 2 * (size_t)n : X0, *X3 = h3 ? X0 + 3 * (size_t)n : X0;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0, b0 = 0.0, b1 = 0.0, b2 = 0.0, b3 = 0.0;
+    int j = lane;
+    for (; j + 32 < n; j += 64) {
+      const double v0 = v[j], v1 = v[j + 32];
+      const double x00 = __ldg(X0 + j), x10 = __ldg(X1 + j), x20 = __ldg(X2 + j), x30 = __ldg(X3 + j);
+      const double x01 = __ldg(X0 + j + 32), x11 = __ldg(X1 + j + 32), x21 = __ldg(X2 + j + 32),
+                   x31 = __ldg(X3 + j + 32);
+      a0 = fma(x00, v0, a0);
+      a1 = fma(x10, v0, a1);
+      a2 = fma(x20, v0, a2);
+      a3 = fma(x30, v0, a3);
+      b0 = fma(x01, v1, b0);
+      b1 = fma(x11, v1, b1);
+      b2 = fma(x21, v1, b2);
+      b3 = fma(x31, v1, b3);
+    }
+    if (j < n) {
+      const double v0 = v[j];
+      a0 = fma(__ldg(X0 + j), v0, a0);
+      a1 = fma(__ldg(X1 + j), v0, a1);
+      a2 = fma(__ldg(X2 + j), v0, a2);
+      a3 = fma(__ldg(X3 + j), v0, a3);
+    }
+    const double s0 = warp_sum(a0 + b0), s1 = warp_sum(a1 + b1), s2 = warp_sum(a2 + b2), s3 = warp_sum(a3 + b3);
+    if (lane == 0) {
+      out[i0] = s0;
+      if (h1) out[i0 + 1] = s1;
+      if (h2) out[i0 + 2] = s2;
+      if (h3) out[i0 + 3] = s3;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(BINV_SOLVE_THREADS) batch_winv_solve_kernel(
+    Net net, const int *__restrict__ order, const int *__restrict__ roff, const long long *__restrict__ xoff,
+    const double *__restrict__ Xall, const int *__restrict__ ptr, const int *__restrict__ col,
+    const double *__restrict__ vals) {
+  const int r = order[blockIdx.x];
+  SolveState *st = net.st + r;
+  if (st->done) return;
+  if (threadIdx.x == 0) st->nit += 1;
+  if (!st->solve_q) return;  // uniform: solve_q is written only by reduce_kernel
+  const int row0 = roff[r], n = roff[r + 1] - row0;
+  const double *X = Xall + xoff[r];
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double *b = reinterpret_cast<double *>(smem_raw);
+  double *x0 = b + n;
+  double *res = x0 + n;
+  for (int i = threadIdx.x; i < n; i += BINV_SOLVE_THREADS) b[i] = net.bvec[row0 + i];
+  __syncthreads();
+  binv_gemv(X, n, b, x0);
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += BINV_SOLVE_THREADS) {
+    double s = b[i];
+    for (int p = ptr[row0 + i]; p < ptr[row0 + i + 1]; p++) s = fma(-vals[p], x0[col[p]], s);
+    res[i] = s;
+  }
+  __syncthreads();
+  binv_gemv(X, n, res, b);  // b now holds the correction X r
+  __syncthreads();
+  __shared__ double s_d[BINV_SOLVE_THREADS / 32], s_o[BINV_SOLVE_THREADS / 32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double md = 0.0, mo = 0.0;
+  for (int i = threadIdx.x; i < n; i += BINV_SOLVE_THREADS) {
+    const int c = row0 + i;
+    const double xv = x0[i] + b[i];
+    const double xo = net.disc[c];
+    double dd = fabs(xv - xo);
+    if (!(dd == dd)) dd = INFINITY;
+    md = fmax(md, dd);
+    mo = fmax(mo, fabs(xo));
+    net.disc[c] = xv;
+    const int d = net.row_de[c];
+    if (d >= 0)
+      net.q[net.de_ids[d]] = xv;
+    else
+      net.constant[net.row_frac[c]] = xv;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    md = fmax(md, __shfl_xor_sync(0xffffffffu, md, o));
+    mo = fmax(mo, __shfl_xor_sync(0xffffffffu, mo, o));
+  }
+  if (lane == 0) {
+    s_d[warp] = md;
+    s_o[warp] = mo;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0, bb = 0.0;
+    for (int k = 0; k < BINV_SOLVE_THREADS / 32; k++) {
+      a = fmax(a, s_d[k]);
+      bb = fmax(bb, s_o[k]);
+    }
+    st->error_q = a / (bb + 1e-16);
+    st->n_refined += 1;
+  }
+}
+
 __global__ void transpose_ld_kernel(const double *__restrict__ in, int ldi, int rows, int cols,
                                     double *__restrict__ out, int ldo) {
   __shared__ double tile[32][33];
@@ -2793,6 +3250,13 @@ struct AndfnHandle {
   double ms_fac[4] = {};  // factorisation phases of the last run (see AndfnSolveStats)
   bool winv_ready = false;
   bool winv_enabled = true;
+  // batches: one explicit inverse per realization (batch_inverse_kernel)
+  bool binv_ready = false;
+  DBuf<double> binv;
+  DBuf<long long> binv_off;
+  DBuf<int> binv_order, binv_roff, bcsr_ptr, bcsr_col, bsing, binv_small, binv_big;
+  int binv_maxn = 0, binv_nsmall = 0, binv_nbig = 0, binv_smem_n = 0, binv_bign = 0;
+  bool bcsr_built = false;
   DBuf<int> pinv, qcol;
   DBuf<TriDesc> tri;
   int max_n = 0, max_nlev = 0, max_k = 0;
@@ -2818,6 +3282,10 @@ struct AndfnHandle {
   int tab_chunk = 2;
   size_t tab_smem = 0;
   bool tab_valid = false, use_tab = false;
+  // launch form of the table sweep (SWEEP_* below), picked by sweep_autotune
+  DBuf<WorkQueue> sweep_q;
+  int sweep_variant = -1;
+  bool tune_sweep = true;  // false: the one-call solve uses a cached choice or the default
   DBuf<int> upd_list, psi_list;
   int n_upd = 0, n_psi = 0;
   int nvmax = 0;
@@ -2836,6 +3304,9 @@ struct AndfnHandle {
   std::vector<SolveState> h_st;  // host copy of the R loop states
   int *h_ndone = nullptr;        // pinned
   cudaGraphExec_t graph_exec = nullptr;
+  // the whole iteration loop as one graph launch (a device-side while node)
+  cudaGraphExec_t loop_exec = nullptr;
+  DBuf<int> loop_count;
   int solve_threads = SOLVE_THREADS;
   // per-kernel timing: event pairs recorded as graph nodes around every
   // kernel of every captured iteration
@@ -2924,6 +3395,7 @@ struct AndfnHandle {
     if (pin_schur) cudaFreeHost(pin_schur);
     andfn::destroy_adj(adj);
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    if (loop_exec) cudaGraphExecDestroy(loop_exec);
     for (auto &b : ev)
       for (auto &c : b)
         for (auto &e : c)
@@ -3337,8 +3809,8 @@ static int build_eval_tables(AndfnHandle *H) {
   chunk = std::max(1, std::min(chunk, maxnf));
   H->chunk = chunk;
   H->eval_smem = (sizeof(Src) + sizeof(cd) * H->MC) * chunk;
-  // table sweep staging: at most 48 KB of sources per CTA (four CTAs an SM
-  // when every fracture's sources fit)
+  // table sweep staging: at most 48 KB of sources per CTA (every source of
+  // the largest fracture when they fit)
   int tchunk = (int)((48 * 1024) / (sizeof(TabSrc) + sizeof(cd) * H->MC));
   tchunk = std::max(2, std::min(tchunk, maxnf));
   H->tab_chunk = tchunk;
@@ -3403,12 +3875,20 @@ static int create_impl(AndfnHandle *H, int R, const char *const *F, const int64_
     H->ent_kind.push_back(0);
   }
   for (char c : H->h.spec_q) H->has_spec |= (c != 0);
-  H->order_thread = std::thread([H, R]() {
+  // batches whose realizations the device inverts need no column order; it
+  // is computed on first use if a run falls back to the sparse LU
+  int maxn_sys = 0;
+  for (int r = 0; r < R; r++) maxn_sys = std::max(maxn_sys, H->sys[r].n);
+  const bool skip_order =
+      R > 1 && H->winv_enabled && maxn_sys <= BINV_MAX_N && binv_cluster_smem(maxn_sys) <= BINV_CLUSTER_SMEM_MAX;
+  H->order_thread = std::thread([H, R, skip_order]() {
     auto tc2 = std::chrono::steady_clock::now();
+    if (!skip_order) {
 #pragma omp parallel for schedule(dynamic, 1) if (R > 1)
-    for (int r = 0; r < R; r++) {
-      CscMatrix P = system_csc(H->sys[r], nullptr);
-      H->sys[r].colorder = column_min_degree_order(P, &H->sys[r].dense_k);
+      for (int r = 0; r < R; r++) {
+        CscMatrix P = system_csc(H->sys[r], nullptr);
+        H->sys[r].colorder = column_min_degree_order(P, &H->sys[r].dense_k);
+      }
     }
     H->ms_create_order = ms_since(tc2);
   });
@@ -3716,9 +4196,147 @@ static int build_inverse(AndfnHandle *H, const TriDesc &td) {
   return 0;
 }
 
+// Batched realizations: X_r = A_r^-1 for every realization on the device
+// (batch_inverse_kernel), from the assembled entries already on the device.
+static int factor_batch_inverse(AndfnHandle *H) {
+  const int R = H->R;
+  cudaStream_t s = H->stream;
+  auto t0 = std::chrono::steady_clock::now();
+  const std::vector<int> &roff = H->h.roff;
+  if (!H->bcsr_built) {
+    // CSR of every realization's pattern over the global rows; entry p of
+    // realization r is assembly entry ent0_r + p
+    std::vector<int> ptr(H->N + 1, 0), col;
+    for (int r = 0; r < R; r++) {
+      const RealSys &S = H->sys[r];
+      for (int i = 0; i < S.n; i++) ptr[roff[r] + i + 1] = S.ent0 + S.mrow_ptr[i + 1];
+      if (S.n > 0) ptr[roff[r]] = S.ent0 + S.mrow_ptr[0];
+    }
+    col.assign(H->ent_row.size(), 0);
+    for (int r = 0; r < R; r++) {
+      const RealSys &S = H->sys[r];
+      for (size_t p = 0; p < S.mcol.size(); p++) col[S.ent0 + p] = S.mcol[p];
+    }
+    std::vector<int> order(R);
+    for (int r = 0; r < R; r++) order[r] = r;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return H->sys[a].n > H->sys[b].n; });
+    std::vector<long long> off(R);
+    long long tot = 0;
+    int maxn = 1;
+    for (int r = 0; r < R; r++) {
+      off[r] = tot;
+      tot += (long long)H->sys[r].n * H->sys[r].n;
+      maxn = std::max(maxn, H->sys[r].n);
+    }
+    CK(upload(H->bcsr_ptr, ptr, s));
+    CK(upload(H->bcsr_col, col, s));
+    CK(upload(H->binv_order, order, s));
+    CK(upload(H->binv_roff, roff, s));
+    CK(upload(H->binv_off, off, s));
+    CK(H->binv.alloc((size_t)std::max(1LL, tot)));
+    CK(H->bsing.alloc(R));
+    H->binv_maxn = maxn;
+    // realizations whose matrix fits one CTA's shared memory (n <= smem_n)
+    // are inverted by one CTA each, larger ones by a cluster
+    const size_t budget = 200 * 1024;
+    const size_t vec = 16 * (size_t)maxn + 4 * (size_t)maxn + 16;
+    int smem_n = 0;
+    if (budget > vec) smem_n = (int)std::floor(std::sqrt((double)(budget - vec) / 8.0));
+    smem_n = std::min(smem_n, maxn);
+    std::vector<int> small, big;
+    int bign = 0;
+    for (int r : order) {
+      if (H->sys[r].n <= smem_n) {
+        small.push_back(r);
+      } else {
+        big.push_back(r);
+        bign = std::max(bign, H->sys[r].n);
+      }
+    }
+    CK(upload(H->binv_small, small.empty() ? std::vector<int>{0} : small, s));
+    CK(upload(H->binv_big, big.empty() ? std::vector<int>{0} : big, s));
+    H->binv_nsmall = (int)small.size();
+    H->binv_nbig = (int)big.size();
+    H->binv_smem_n = smem_n;
+    H->binv_bign = bign;
+    H->bcsr_built = true;
+  }
+  const int maxn = H->binv_maxn;
+  const int smem_n = H->binv_smem_n;
+  const size_t smem = 8 * (size_t)smem_n * smem_n + 16 * (size_t)maxn + 4 * (size_t)maxn + 16;
+  CK(cudaFuncSetAttribute(batch_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CK(cudaFuncSetAttribute(batch_winv_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)(24 * (size_t)maxn)));
+  if (H->binv_nbig > 0) {
+    const size_t csmem = binv_cluster_smem(H->binv_bign);
+    CK(cudaFuncSetAttribute(batch_inverse_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csmem));
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = BINV_CLUSTER;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(BINV_CLUSTER * H->binv_nbig);
+    cfg.blockDim = dim3(BINV_THREADS);
+    cfg.dynamicSmemBytes = csmem;
+    cfg.stream = s;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    CK(cudaLaunchKernelEx(&cfg, batch_inverse_cluster_kernel, (const int *)H->binv_big.p, (const int *)H->binv_roff.p,
+                          (const long long *)H->binv_off.p, H->binv.p, (const int *)H->bcsr_ptr.p,
+                          (const int *)H->bcsr_col.p, (const double *)H->d_mvals.p, H->bsing.p));
+    H->launches += 1;
+  }
+  if (H->binv_nsmall > 0) {
+    batch_inverse_kernel<<<H->binv_nsmall, BINV_THREADS, smem, s>>>(H->binv_small.p, H->binv_roff.p, H->binv_off.p,
+                                                                    H->binv.p, H->bcsr_ptr.p, H->bcsr_col.p,
+                                                                    H->d_mvals.p, H->bsing.p, smem_n);
+    H->launches += 1;
+  }
+  CK(cudaGetLastError());
+  std::vector<int> sing(R, 0);
+  CK(cudaMemcpyAsync(sing.data(), H->bsing.p, sizeof(int) * R, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  for (int r = 0; r < R; r++)
+    if (sing[r]) {
+      set_error("discharge system of realization " + std::to_string(r) +
+                " is singular (a fracture without a head boundary?)");
+      return ANDFN_SINGULAR;
+    }
+  for (int r = 0; r < R; r++) {
+    H->sys[r].tail_k = 0;
+    H->sys[r].nlev_l = H->sys[r].nlev_u = 0;
+    H->sys[r].nnz = (int64_t)H->sys[r].n * H->sys[r].n;
+  }
+  H->nnz_factors = 0;
+  for (int r = 0; r < R; r++) H->nnz_factors += H->sys[r].nnz;
+  H->winv_ready = false;
+  H->binv_ready = true;
+  H->adj_factors_ready = false;
+  H->lu_keep = LuFactors();
+  H->ms_fac[0] = H->ms_fac[2] = H->ms_fac[3] = 0.0;
+  H->ms_fac[1] = ms_since(t0);
+  return 0;
+}
+
 static int factor_all(AndfnHandle *H, const std::vector<double> &mv) {
   const int R = H->R;
   cudaStream_t s = H->stream;
+  H->binv_ready = false;
+  if (R > 1 && H->winv_enabled) {
+    // batches: per-realization explicit inverses on the device when they are
+    // small enough (the host's sparse LU is then not needed)
+    int maxn = 0;
+    long long tot = 0;
+    for (int r = 0; r < R; r++) {
+      maxn = std::max(maxn, H->sys[r].n);
+      tot += (long long)H->sys[r].n * H->sys[r].n;
+    }
+    size_t fr = 0, totmem = 0;
+    cudaMemGetInfo(&fr, &totmem);
+    if (maxn <= BINV_MAX_N && binv_cluster_smem(maxn) <= BINV_CLUSTER_SMEM_MAX && 8.0 * (double)tot < 0.5 * (double)fr)
+      return factor_batch_inverse(H);
+  }
   std::vector<LuFactors> LU(R);
   std::vector<int> rcs(R, 0);
   // one realization: the Schur complement's columns use the host threads and
@@ -3744,6 +4362,10 @@ static int factor_all(AndfnHandle *H, const std::vector<double> &mv) {
   }
   H->factor_runs += 1;
   auto factor_one = [&](int r) {
+    if (H->sys[r].colorder.empty() && H->sys[r].n > 0) {  // column order not computed at creation
+      CscMatrix P = system_csc(H->sys[r], nullptr);
+      H->sys[r].colorder = column_min_degree_order(P, &H->sys[r].dense_k);
+    }
     CscMatrix A = system_csc(H->sys[r], mv.data());
     rcs[r] = sparse_lu_factor(A, H->sys[r].colorder, 1.0, LU[r], H->sys[r].dense_k, defer, schur_buf);
   };
@@ -3999,7 +4621,7 @@ __global__ void head_vector_kernel(Net net, const int *__restrict__ gptr, const 
                                    const cd *__restrict__ S);
 
 // Kernels one discharge solve launches.
-static int tri_launches(const AndfnHandle *H) { return H->winv_ready ? 3 : 1; }
+static int tri_launches(const AndfnHandle *H) { return H->winv_ready ? 3 : 1; }  // batched inverses: 1
 
 // A discharge solve through the explicit inverse X (forward) or its
 // transpose (ADJ): x0 = Q X P b, r = b - M x0, x = x0 + Q X P r, with M = A
@@ -4020,6 +4642,14 @@ static void launch_winv_solve(AndfnHandle *H, const Net &net, cudaStream_t s, co
 
 static void launch_trisolve(AndfnHandle *H, cudaStream_t s) {
   Net net = H->net();
+  if (H->binv_ready) {
+    batch_winv_solve_kernel<<<H->R, BINV_SOLVE_THREADS, 24 * (size_t)H->binv_maxn, s>>>(
+        net, H->binv_order.p, H->binv_roff.p, H->binv_off.p, H->binv.p, H->bcsr_ptr.p, H->bcsr_col.p,
+        H->d_mvals.p);
+    const cudaError_t le = cudaGetLastError();
+    if (le != cudaSuccess) set_error(std::string("batched explicit-inverse solve launch: ") + cudaGetErrorString(le));
+    return;
+  }
   if (H->winv_ready) {
     launch_winv_solve<false>(H, net, s, H->winv.p, H->a_ptr.p, H->a_col.p, nullptr);
     const cudaError_t le = cudaGetLastError();
@@ -4047,17 +4677,172 @@ static inline void mark(AndfnHandle *H, cudaStream_t s, int b, int c, int w) {
   if (H->profiling && b >= 0) cudaEventRecordWithFlags(H->ev[b][c][w], s, cudaEventRecordExternal);
 }
 
+static int enqueue_iteration(AndfnHandle *H, cudaStream_t s, int blend_mode, int b = -1);
+
+// Condition of the device-side iteration loop: another iteration while some
+// realization is still running, at most cap iterations (a bound independent
+// of the stopping logic).  One thread.
+__global__ void loop_cond_kernel(cudaGraphConditionalHandle h, const int *ndone, int R, int *count, int cap) {
+  const int c = ++(*count);
+  cudaGraphSetConditional(h, (*ndone < R && c < cap) ? 1u : 0u);
+}
+
+// The iteration loop as one graph launch: a while node whose body is one
+// outer iteration (enqueue_iteration) followed by loop_cond_kernel.  Returns
+// 0 and sets *ran when the loop ran; *ran = false (nothing launched) when the
+// runtime has no conditional graph nodes, so the caller falls back to
+// launching batches of iterations from the host.
+static int run_device_loop(AndfnHandle *H, const AndfnConstants *C, bool *ran, int *iterations_run) {
+  *ran = false;
+  cudaStream_t s = H->stream;
+  if (H->loop_exec) {
+    cudaGraphExecDestroy(H->loop_exec);
+    H->loop_exec = nullptr;
+  }
+  if (!H->loop_count.p) CK(H->loop_count.alloc(1));
+  cudaGraph_t g = nullptr;
+  CK(cudaGraphCreate(&g, 0));
+  cudaGraphConditionalHandle hc;
+  if (cudaGraphConditionalHandleCreate(&hc, g, 1, cudaGraphCondAssignDefault) != cudaSuccess) {
+    cudaGetLastError();
+    cudaGraphDestroy(g);
+    return 0;
+  }
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = hc;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t cnode;
+  if (cudaGraphAddNode(&cnode, g, nullptr, 0, &cp) != cudaSuccess) {
+    cudaGetLastError();
+    cudaGraphDestroy(g);
+    return 0;
+  }
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  const int64_t launches0 = H->launches;
+  CK(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  enqueue_iteration(H, s, 0, -1);
+  const int cap = (int)std::min<int64_t>(C->max_iterations + 2, (int64_t)1 << 30);
+  loop_cond_kernel<<<1, 1, 0, s>>>(hc, H->ndone.p, H->R, H->loop_count.p, cap);
+  {
+    const cudaError_t ec = cudaStreamEndCapture(s, &body);
+    if (ec != cudaSuccess) {
+      cudaGraphDestroy(g);
+      set_error(std::string("capture of the iteration loop: ") + cudaGetErrorString(ec) + "; " + g_last_error);
+      return ANDFN_CUDA_ERROR;
+    }
+  }
+  const int64_t per_it = H->launches - launches0 + 1;  // kernels of one iteration, the condition included
+  H->launches = launches0;                              // capture launches nothing
+  const cudaError_t ei = cudaGraphInstantiate(&H->loop_exec, g, 0);
+  cudaGraphDestroy(g);
+  if (ei != cudaSuccess) {
+    set_error(std::string("instantiation of the iteration loop: ") + cudaGetErrorString(ei));
+    return ANDFN_CUDA_ERROR;
+  }
+  CK(cudaMemsetAsync(H->loop_count.p, 0, sizeof(int), s));
+  CK(cudaGraphLaunch(H->loop_exec, s));
+  int count = 0;
+  CK(cudaMemcpyAsync(&count, H->loop_count.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  H->launches += per_it * count;
+  *iterations_run = count;
+  *ran = true;
+  return 0;
+}
+
+// Launch forms of the table sweep: one CTA per item, or persistent CTAs
+// (4 or 6 per SM) taking items from a device work queue.
+enum SweepVariant { SWEEP_PER_ITEM = 0, SWEEP_QUEUE4 = 1, SWEEP_QUEUE6 = 2, SWEEP_VARIANTS = 3 };
+
+static void launch_sweep_variant(AndfnHandle *H, const Net &net, cudaStream_t s, int v) {
+  if (v == SWEEP_PER_ITEM) {
+    sweep_table_kernel<<<H->n_sweep_items, EVAL_THREADS, H->tab_smem, s>>>(
+        net, H->sweep_items.p, H->sweep_pts.p, H->d_groups.p, H->tab_fpt0.p, H->tab_fnp.p, H->tab_off.p, H->tab_w.p,
+        H->tab_l.p, H->sweep_vals.p, H->tab_chunk);
+  } else {
+    const int per_sm = (v == SWEEP_QUEUE4) ? 4 : 6;
+    const int grid = std::min(H->n_sweep_items, per_sm * H->num_sms);
+    sweep_table_queue_kernel<<<grid, EVAL_THREADS, H->tab_smem, s>>>(
+        net, H->sweep_items.p, H->n_sweep_items, H->sweep_pts.p, H->d_groups.p, H->tab_fpt0.p, H->tab_fnp.p,
+        H->tab_off.p, H->tab_w.p, H->tab_l.p, H->sweep_vals.p, H->tab_chunk, H->sweep_q.p);
+  }
+}
+
 // The sweep evaluation into sweep_vals: from the pair tables when this run
 // has them (fixed ncoef and nint), else the full evaluation.
 static void launch_sweep(AndfnHandle *H, const Net &net, cudaStream_t s) {
   if (H->n_sweep_items <= 0) return;
   if (H->use_tab && H->tab_valid)
-    sweep_table_kernel<<<H->n_sweep_items, EVAL_THREADS, H->tab_smem, s>>>(
-        net, H->sweep_items.p, H->sweep_pts.p, H->d_groups.p, H->tab_fpt0.p, H->tab_fnp.p, H->tab_off.p, H->tab_w.p,
-        H->tab_l.p, H->sweep_vals.p, H->tab_chunk);
+    launch_sweep_variant(H, net, s, H->sweep_variant < 0 ? SWEEP_PER_ITEM : H->sweep_variant);
   else
     eval_kernel<false><<<H->n_sweep_items, EVAL_THREADS, H->eval_smem, s>>>(net, H->sweep_items.p, H->sweep_pts.p,
                                                                              H->d_groups.p, H->sweep_vals.p, H->chunk);
+}
+
+// Autotuner of the table sweep's launch form: each form runs on this run's
+// own tables (one warm-up launch, then three timed with CUDA events; the
+// outputs are overwritten by the first iteration), the fastest is kept for
+// the handle and cached for the process by the shape of the work (MC,
+// items and largest fracture, bucketed).  ANDFN_B200_SWEEP_VARIANT=0/1/2
+// forces a form.  A handle that may not tune (the one-call solve) takes a
+// cached choice or the per-item form.
+static std::mutex g_tune_mu;
+static std::map<std::array<int, 4>, int> g_tune_cache;
+
+static int sweep_autotune(AndfnHandle *H) {
+  if (H->sweep_variant >= 0) return 0;
+  if (const char *v = getenv("ANDFN_B200_SWEEP_VARIANT")) {
+    const int x = atoi(v);
+    if (x >= 0 && x < SWEEP_VARIANTS) {
+      H->sweep_variant = x;
+      return 0;
+    }
+  }
+  int maxnf = 1;
+  for (int f = 0; f < (int)H->nf; f++) maxnf = std::max(maxnf, H->h.fptr[f + 1] - H->h.fptr[f]);
+  const std::array<int, 4> key = {H->device, H->MC, H->n_sweep_items / 256, maxnf / 8};
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      H->sweep_variant = it->second;
+      return 0;
+    }
+  }
+  if (!H->tune_sweep || H->n_sweep_items <= 0) {
+    H->sweep_variant = SWEEP_PER_ITEM;
+    return 0;
+  }
+  cudaStream_t s = H->stream;
+  const Net net = H->net();
+  cudaEvent_t a, b;
+  CK(cudaEventCreate(&a));
+  CK(cudaEventCreate(&b));
+  float best = 1e30f;
+  int bestv = SWEEP_PER_ITEM;
+  for (int v = 0; v < SWEEP_VARIANTS; v++) {
+    launch_sweep_variant(H, net, s, v);
+    CK(cudaEventRecord(a, s));
+    for (int r = 0; r < 3; r++) launch_sweep_variant(H, net, s, v);
+    CK(cudaEventRecord(b, s));
+    CK(cudaEventSynchronize(b));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, a, b));
+    if (ms < best) {
+      best = ms;
+      bestv = v;
+    }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  CK(cudaGetLastError());
+  H->launches += 4 * SWEEP_VARIANTS;
+  H->sweep_variant = bestv;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune_cache[key] = bestv;
+  return 0;
 }
 
 // The pair tables of the current points and geometry (once per run).
@@ -4074,7 +4859,7 @@ static int build_pair_table(AndfnHandle *H) {
   return 0;
 }
 
-static int enqueue_iteration(AndfnHandle *H, cudaStream_t s, int blend_mode, int b = -1) {
+static int enqueue_iteration(AndfnHandle *H, cudaStream_t s, int blend_mode, int b) {
   Net net = H->net();
   mark(H, s, b, K_RHS, 0);
   if (H->use_head_sums) {
@@ -4285,6 +5070,12 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
       int rcp = build_pair_table(H);
       if (rcp) return rcp;
       H->use_tab = true;
+      if (!H->sweep_q.p) {
+        CK(H->sweep_q.alloc(1));
+        CK(cudaMemsetAsync(H->sweep_q.p, 0, sizeof(WorkQueue), s));
+      }
+      rcp = sweep_autotune(H);
+      if (rcp) return rcp;
     }
   }
   const long long nent = (long long)H->ent_row.size();
@@ -4327,10 +5118,23 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
   base.ms_inverse = H->ms_fac[3];
   // iterations, in graph batches
   auto t_it = std::chrono::steady_clock::now();
+  int64_t loop_launches = 0;
   if (growth_possible) {
     int rca = run_adaptive(H, C);
     if (rca) return rca;
   } else {
+    // the whole loop in one launch (not with per-kernel event profiling,
+    // whose event nodes a loop body cannot hold, nor with cluster-launched
+    // triangular solves)
+    bool looped = false;
+    const char *dl = getenv("ANDFN_B200_DEVICE_LOOP");
+    if (!H->profiling && (H->winv_ready || H->binv_ready) && !(dl && atoi(dl) == 0)) {
+      int its_run = 0;
+      int rcl = run_device_loop(H, C, &looped, &its_run);
+      if (rcl) return rcl;
+      if (looped) loop_launches = 1;
+    }
+    if (!looped) {
     if (H->graph_exec) {
       cudaGraphExecDestroy(H->graph_exec);
       H->graph_exec = nullptr;
@@ -4379,8 +5183,10 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
           }
         nit_before = nit_max;
       }
+      loop_launches += 1;
       if (*H->h_ndone >= R) break;
       if (++guard > 1 + C->max_iterations / ITER_BATCH + 2) break;
+    }
     }
   }
   rc = read_states(H);
@@ -4432,8 +5238,10 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
     st.nnz_matrix = (int64_t)H->sys[r].mcol.size();
     st.nnz_factors = H->sys[r].nnz;
     st.dense_tail = H->sys[r].tail_k;
-    st.explicit_inverse = H->winv_ready ? 1 : 0;
-    st.refined_solves = H->winv_ready ? f.n_refined : 0;
+    st.explicit_inverse = (H->winv_ready || H->binv_ready) ? 1 : 0;
+    st.refined_solves = (H->winv_ready || H->binv_ready) ? f.n_refined : 0;
+    st.sweep_variant = H->use_tab ? H->sweep_variant : -1;
+    st.loop_launches = loop_launches;
     st.levels_l = H->sys[r].nlev_l;
     st.levels_u = H->sys[r].nlev_u;
     for (int i = 0; i < 8; i++) st.tri_cycles[i] = f.tri_cycles[i];
@@ -5076,6 +5884,7 @@ int andfn_b200_batch_solve(int64_t R, void *const *frac_recs, const int64_t *nf,
   AndfnHandle *H = nullptr;
   int rc = andfn_b200_batch_create(&H, R, frac_recs, nf, elem_recs, ne, layout, discharge_int, -1);
   if (rc) return rc;
+  H->tune_sweep = false;  // a cached choice of an earlier handle, or the per-item form
   const double ms_up = ms_since(t0);
   rc = run_impl(H, constants, nullptr);
   double ms_down = 0;

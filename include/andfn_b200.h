@@ -104,6 +104,11 @@ typedef struct AndfnSolveStats {
   double ms_factor_levels;  /*   level-ordered factor tables + dense-tail inverse,            */
   double ms_inverse;        /*   explicit inverse of the system (device)                      */
   int64_t refined_solves;   /* explicit-inverse solves that took the refinement step */
+  int64_t sweep_variant;    /* launch form of the sweep from pair tables, picked by the autotuner:
+                               0 one CTA per work item, 1 / 2 persistent CTAs (4 / 6 per SM) on a
+                               device work queue; -1: no pair tables (adaptive coefficient growth) */
+  int64_t loop_launches;    /* graph launches of the iteration loop (1: the whole loop runs on the
+                               device in one launch) */
 } AndfnSolveStats;
 
 /* ---- one-call drop-in (replaces andfn/hpc/hpc_solve.py:55 solve) --------

@@ -208,11 +208,19 @@ def _const(constants, name):
 
 
 def solve(fracture_struc_array, element_struc_array, discharge_int, constants, ntype_elements=None,
-          stats: dict | None = None, max_iterations: int | None = None):
+          stats: dict | None = None, max_iterations: int | None = None, refine: bool = False):
     """Restatement of andfn/hpc/hpc_solve.py:55-257 (same in-place contract).
 
     ``constants`` is a dtype_constants record or a mapping with the keys
     MAX_ERROR, MAX_ITERATIONS, COEF_RATIO, MAX_NCOEF, COEF_INCREASE, DAMPING.
+
+    ``refine=True`` (not the reference's algorithm; off by default) adds one
+    step of iterative refinement to every discharge solve, x += LU^-1 (b - A x).
+    The reference's unrefined SuperLU solves of an ill-conditioned system
+    (condition ~1e12) carry round-off of ~1e-10 relative that changes with
+    every right-hand side, so a quantity of the solved state is a smooth
+    function of the inputs only down to that level; with the refinement it is
+    smooth to ~1e-15, which finite-difference checks of derivatives need.
     """
     import scipy.sparse.linalg as spla
 
@@ -278,6 +286,8 @@ def solve(fracture_struc_array, element_struc_array, discharge_int, constants, n
             if b_known is not None:
                 head = head[keep] + b_known
             discharges[:] = lu.solve(head)
+            if refine:
+                discharges += lu.solve(head - A @ discharges)
             o.post_solve(scatter(discharges))
             error_q = np.max(np.abs(discharges - discharges_old) / (np.max(np.abs(discharges_old)) + 1e-16))
         t1 = time.perf_counter()

@@ -201,10 +201,15 @@ def test_adjoint_config4_form_on_dense_tail_network():
     is dominated by the round-off of J itself (about 3e-9 of the largest
     entry, measured), not by the gradient's error.  GPU difference quotients
     use fixed-iteration solves from the zero state (500 iterations, so J is
-    smooth in log t); the oracle's start from its converged state at the
-    base point and run 150 more iterations at each perturbed point (the
-    fixed-point iteration contracts by about 0.8 per iteration, so the
-    start's influence is below round-off)."""
+    smooth in log t).  The oracle's discharge solves take one refinement step
+    (oracle.solve(refine=True)): the reference's unrefined SuperLU solves of
+    this system (condition ~1e12) leave J noisy at ~5e-9 relative (J changes
+    by 2e-11 between 150, 300 and 500 iterations, measured), which a step of
+    1e-6 turns into errors of ~1e-5 of the gradient; with the refinement J is
+    smooth to ~1e-15.  Its difference quotients start from its converged
+    state at the base point and run 250 iterations at each perturbed point
+    (the slowest mode of the iteration contracts by about 0.9 per iteration,
+    so the start's influence is ~1e-11)."""
     import torch
     from andfn_b200 import network as nw
     from andfn_b200.adjoint import DFNModel
@@ -245,8 +250,8 @@ def test_adjoint_config4_form_on_dense_tail_network():
     # the oracle: converged base state, then warm-started fixed-iteration solves
     cb = _constants(10, its=300)
     Fb, Eb = F.copy(), E.copy()
-    orc.solve(Fb, Eb, 50, cb)
-    cw = _constants(10, its=150)
+    orc.solve(Fb, Eb, 50, cb, refine=True)
+    cw = _constants(10, its=250)
 
     def J_oracle(logt):
         Fo, Eo = Fb.copy(), Eb.copy()
@@ -254,7 +259,7 @@ def test_adjoint_config4_form_on_dense_tail_network():
         Fo["t"] = t
         m = np.isin(Eo["_type"], (2, 3))
         Eo["phi"][m] = Eo["head"][m] * t[Eo["frac0"][m]]
-        orc.solve(Fo, Eo, 50, cw)
+        orc.solve(Fo, Eo, 50, cw, refine=True)
         hh = orc.eval_heads(Fo, Eo, fr, z)
         return float(((hh - hobs) ** 2).sum() + Eo["q"][outlet].sum())
 

@@ -91,6 +91,8 @@ def test_batch_matches_oracle_with_max_iterations_stop():
     c = default_constants(MAX_ITERATIONS=12, MAX_ERROR=1e-8, MAX_NCOEF=10)
     batch = [(F.copy(), E.copy()) for F, E in recs]
     st = andfn_b200.solve_batch(batch, 50, c)
+    # batches solve through per-realization explicit inverses, one refinement step each solve
+    assert all(s["explicit_inverse"] == 1 and s["refined_solves"] > 0 for s in st), st[0]
     for r, ((F0, E0), (Fb, Eb), s) in enumerate(zip(recs, batch, st)):
         Fo, Eo = F0.copy(), E0.copy()
         so = {}
@@ -147,9 +149,30 @@ def test_batch_realizations_with_wells_match_oracle():
     c = default_constants(MAX_ITERATIONS=200, MAX_ERROR=1e-8, MAX_NCOEF=15)
     batch = [(F.copy(), E.copy()) for F, E in recs]
     st = andfn_b200.solve_batch(batch, 50, c)
+    # batches solve through per-realization explicit inverses, one refinement step each solve
+    assert all(s["explicit_inverse"] == 1 and s["refined_solves"] > 0 for s in st), st[0]
     for r, ((F0, E0), (Fb, Eb), s) in enumerate(zip(recs, batch, st)):
         Fo, Eo = F0.copy(), E0.copy()
         so = {}
         orc.solve(Fo, Eo, 50, c, stats=so)
         assert s["iterations"] == so["iterations"], (r, s["iterations"], so["iterations"])
         _compare(Eb, Fb, Eo, Fo, ("wells", r))
+
+
+def test_batch_with_a_singular_realization_raises():
+    """A realization whose fracture has no head boundary (one disc with a
+    prescribed-discharge well only: its constant is undetermined) makes the
+    batched inversion report a singular system, as the single-network path
+    (SuperLU raises there, hpc_solve.py:121)."""
+    import andfn_b200
+    from andfn_b200 import _ffi
+    from andfn_b200 import network as nw
+    from andfn_b200.records import default_constants
+    lone = nw.build([[0.0, 0.0, 0.0]], [[0.0, 0.0, 1.0]], [2.0], [1e-5], 10, 20, keep="all")
+    nw.add_well(lone, 0, 0.3 + 0.2j, 0.05, float("nan"), q=1e-5)
+    good = nw.uniform_discs(3, nf=40, L=20.0)
+    recs = nw.to_records_batch([good, lone])
+    c = default_constants(MAX_ITERATIONS=20, MAX_ERROR=1e-8, MAX_NCOEF=10)
+    with pytest.raises(_ffi.AndfnError) as ei:
+        andfn_b200.solve_batch([(F.copy(), E.copy()) for F, E in recs], 50, c)
+    assert ei.value.code == 3 and "realization 1" in str(ei.value), str(ei.value)

@@ -5,7 +5,13 @@ FMA-based Horner scheme, so agreement is to rounding, not bit-exact):
   * coefficients, discharges q, fracture constants, dpsi_corr:
         max |gpu - ref| <= 1e-10 * P, with P the potential scale of the
         solved network (conftest.potential_scale: max |coef|, |phi|, |C|)
-  * error_coef: absolute 1e-10 * P (it is a mean |delta coef|)
+  * error_coef: absolute 1e-10 * P (it is a mean |delta coef|), except where
+    one side is exactly 0: calc_coef_error returns 0 when the sum of the old
+    coefficients' magnitudes is below 1e-15 (hpc_math_functions.py:647-670),
+    a threshold on a round-off-level sum, so an element whose old
+    coefficients sit at round-off can fall on either side; such a flip is
+    accepted when the nonzero value is below 1e-6 * P, for at most 0.1 % of
+    the elements
   * error (the truncation indicator | |S - S_10| / |S| - 1 |, S = sum of the
     element's new coefficients): coefficient differences of 1e-10 P move it by
     at most about m 1e-10 P / |S|, so per element the bound is
@@ -30,16 +36,26 @@ def _gpu_solve(F, E, D, c):
     return dict(andfn_b200.last_stats)
 
 
+def error_coef_mismatch(a, b, P):
+    """Elements whose error_coef differs by more than 1e-10 P, not counting
+    the threshold flips described in the module docstring; the number of
+    flips."""
+    d = np.abs(a - b)
+    flip = ((a == 0) != (b == 0)) & (np.maximum(np.abs(a), np.abs(b)) <= 1e-6 * P)
+    return np.nonzero((d > TOL * P) & ~flip)[0], int(flip.sum())
+
+
 def _compare(E, F, Eo, Fo, tag):
     assert np.array_equal(E["ncoef"], Eo["ncoef"]), tag
     assert np.array_equal(E["nint"], Eo["nint"]), tag
     assert np.array_equal(E["thetas"], Eo["thetas"]), tag
     P = potential_scale(Eo, Fo)
     for name, a, b in (("coef", E["coef"], Eo["coef"]), ("q", E["q"], Eo["q"]),
-                       ("constant", F["constant"], Fo["constant"]), ("dpsi_corr", E["dpsi_corr"], Eo["dpsi_corr"]),
-                       ("error_coef", E["error_coef"], Eo["error_coef"])):
+                       ("constant", F["constant"], Fo["constant"]), ("dpsi_corr", E["dpsi_corr"], Eo["dpsi_corr"])):
         d = float(np.abs(a - b).max())
         assert d <= TOL * P, (tag, name, d / P)
+    bad, flips = error_coef_mismatch(E["error_coef"], Eo["error_coef"], P)
+    assert len(bad) == 0 and flips <= max(1, len(E) // 1000), (tag, "error_coef", bad[:5], flips)
     if P > 1e3 * max(np.abs(Eo["coef"]).max(), 1e-300):
         return  # no flow: the truncation indicator is a ratio of round-off terms
     c = Eo["coef"]
