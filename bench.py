@@ -745,7 +745,10 @@ def run_profile_case(args):
     wrap: ``plain`` (one solve of the plain-solve network through the one-call
     C ABI), ``adjoint`` (one forward solve plus the gradient of the head-misfit
     + outflow objective w.r.t. log t) or ``batch`` (one batched solve of the
-    256 realizations).  --profile-iterations caps MAX_ITERATIONS."""
+    256 realizations).  --profile-iterations caps MAX_ITERATIONS.  The
+    iterations run as 8-iteration graph launches from the host (not the
+    single device-side loop), whose kernels a profiler attributes one by one."""
+    os.environ.setdefault("ANDFN_B200_DEVICE_LOOP", "0")
     import andfn_b200
     its = args.profile_iterations
     if args.profile_case == "batch":
