@@ -22,7 +22,8 @@ EXPORTS = ("andfn_b200_solve", "andfn_b200_create", "andfn_b200_upload_state", "
            "andfn_b200_eval_heads_noalloc", "andfn_b200_adjoint", "andfn_b200_set_transmissivity",
            "andfn_b200_state_device", "andfn_b200_heads_device", "andfn_b200_heads_vjp",
            "andfn_b200_bc_residual", "andfn_b200_eval_w", "andfn_b200_eval_w_object",
-           "andfn_b200_track")
+           "andfn_b200_track", "andfn_b200_disc_intersections", "andfn_b200_clusters",
+           "andfn_b200_geometry_last_error")
 
 STATUS = {0: "ok", 1: "max_iterations", 2: "nonfinite", 3: "singular", 10: "bad_layout", 11: "bad_input",
           12: "cuda_error", 13: "no_device", 14: "out_of_memory"}
@@ -82,6 +83,10 @@ def lib() -> ctypes.CDLL:
         ("andfn_b200_heads_device", ctypes.c_int, [P, P, P, I64, P]),
         ("andfn_b200_heads_vjp", ctypes.c_int, [P, P, P, I64, P, P, I64, P, P, P]),
         ("andfn_b200_bc_residual", ctypes.c_int, [P, P, P, ctypes.POINTER(AndfnResidual)]),
+        ("andfn_b200_disc_intersections", ctypes.c_int, [I32, I64, P, P, P, P, P, ctypes.c_double, I64, P, P, P,
+                                                         P]),
+        ("andfn_b200_clusters", ctypes.c_int, [I32, I64, I64, P, P]),
+        ("andfn_b200_geometry_last_error", ctypes.c_char_p, []),
     ):
         fn = getattr(L, name)
         fn.restype = res

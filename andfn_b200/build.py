@@ -11,7 +11,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "libandfn_b200.so")
-SOURCES = [os.path.join(HERE, "csrc", f) for f in ("solver.cu", "sparse_lu.cpp")]
+SOURCES = [os.path.join(HERE, "csrc", f) for f in ("solver.cu", "geometry.cu", "sparse_lu.cpp")]
 DEPS = SOURCES + [os.path.join(HERE, "csrc", f) for f in ("dmath.cuh", "sparse_lu.h", "track.cuh")] + [
     os.path.join(os.path.dirname(HERE), "include", "andfn_b200.h")]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",

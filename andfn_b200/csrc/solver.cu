@@ -3256,6 +3256,7 @@ struct AndfnHandle {
   DBuf<long long> binv_off;
   DBuf<int> binv_order, binv_roff, bcsr_ptr, bcsr_col, bsing, binv_small, binv_big;
   int binv_maxn = 0, binv_nsmall = 0, binv_nbig = 0, binv_smem_n = 0, binv_bign = 0;
+  double dense_frac = 0.4;  // ordering: dense tail once the minimum degree reaches this fraction
   bool bcsr_built = false;
   DBuf<int> pinv, qcol;
   DBuf<TriDesc> tri;
@@ -3881,13 +3882,21 @@ static int create_impl(AndfnHandle *H, int R, const char *const *F, const int64_
   for (int r = 0; r < R; r++) maxn_sys = std::max(maxn_sys, H->sys[r].n);
   const bool skip_order =
       R > 1 && H->winv_enabled && maxn_sys <= BINV_MAX_N && binv_cluster_smem(maxn_sys) <= BINV_CLUSTER_SMEM_MAX;
-  H->order_thread = std::thread([H, R, skip_order]() {
+  // the ordering hands the remaining columns to the dense tail once the
+  // minimum degree reaches this fraction of what remains
+  double dense_frac = 0.4;
+  if (const char *v = getenv("ANDFN_B200_DENSE_FRAC")) {
+    const double x = atof(v);
+    if (x > 0.0 && x <= 1.0) dense_frac = x;
+  }
+  H->dense_frac = dense_frac;
+  H->order_thread = std::thread([H, R, skip_order, dense_frac]() {
     auto tc2 = std::chrono::steady_clock::now();
     if (!skip_order) {
 #pragma omp parallel for schedule(dynamic, 1) if (R > 1)
       for (int r = 0; r < R; r++) {
         CscMatrix P = system_csc(H->sys[r], nullptr);
-        H->sys[r].colorder = column_min_degree_order(P, &H->sys[r].dense_k);
+        H->sys[r].colorder = column_min_degree_order(P, &H->sys[r].dense_k, dense_frac);
       }
     }
     H->ms_create_order = ms_since(tc2);
@@ -4364,7 +4373,7 @@ static int factor_all(AndfnHandle *H, const std::vector<double> &mv) {
   auto factor_one = [&](int r) {
     if (H->sys[r].colorder.empty() && H->sys[r].n > 0) {  // column order not computed at creation
       CscMatrix P = system_csc(H->sys[r], nullptr);
-      H->sys[r].colorder = column_min_degree_order(P, &H->sys[r].dense_k);
+      H->sys[r].colorder = column_min_degree_order(P, &H->sys[r].dense_k, H->dense_frac);
     }
     CscMatrix A = system_csc(H->sys[r], mv.data());
     rcs[r] = sparse_lu_factor(A, H->sys[r].colorder, 1.0, LU[r], H->sys[r].dense_k, defer, schur_buf);

@@ -165,14 +165,67 @@ def _candidate_pairs(centers, radii):
     return pairs[order]
 
 
+def gpu_disc_intersections(centers, normals, xv, yv, radii, se_factor, device=-1):
+    """Disc-disc intersection segments of every pair i < k on the GPU
+    (andfn_b200_disc_intersections): the pairs sorted by (i, k) and the
+    shortened endpoints in both discs' frames, bit for bit what
+    _candidate_pairs + plane_disc_intersections + shorten compute."""
+    import ctypes
+
+    from . import _ffi
+    L = _ffi.lib()
+    P = ctypes.c_void_p
+    arrs = [np.ascontiguousarray(a, np.float64) for a in (centers, normals, xv, yv)]
+    r = np.ascontiguousarray(radii, np.float64)
+    nf = len(r)
+    if any(a.shape != (nf, 3) for a in arrs):
+        raise ValueError("centers, normals, xv and yv must be nf x 3")
+    cap = max(16, 8 * nf)
+    for _ in range(2):
+        pairs = np.empty((cap, 2), np.int64)
+        e0 = np.empty((cap, 2), np.complex128)
+        e1 = np.empty((cap, 2), np.complex128)
+        n = ctypes.c_int64()
+        rc = L.andfn_b200_disc_intersections(int(device), nf, *[a.ctypes.data_as(P) for a in arrs],
+                                             r.ctypes.data_as(P), float(se_factor), cap, pairs.ctypes.data_as(P),
+                                             e0.ctypes.data_as(P), e1.ctypes.data_as(P), ctypes.byref(n))
+        if rc == 0:
+            return pairs[: n.value], e0[: n.value], e1[: n.value]
+        if rc == 11 and n.value > cap:
+            cap = n.value
+            continue
+        raise _ffi.AndfnError(rc, L.andfn_b200_geometry_last_error().decode())
+    raise RuntimeError("disc_intersections: segment count changed between calls")
+
+
+def gpu_clusters(nf, pairs, device=-1):
+    """Connected components of the fracture graph given by pairs (i, k) on the
+    GPU (andfn_b200_clusters): each fracture's label is the smallest fracture
+    index of its component."""
+    import ctypes
+
+    from . import _ffi
+    L = _ffi.lib()
+    P = ctypes.c_void_p
+    pr = np.ascontiguousarray(np.asarray(pairs, np.int64).reshape(-1, 2))
+    out = np.empty(int(nf), np.int64)
+    rc = L.andfn_b200_clusters(int(device), int(nf), len(pr), pr.ctypes.data_as(P), out.ctypes.data_as(P))
+    if rc:
+        raise _ffi.AndfnError(rc, L.andfn_b200_geometry_last_error().decode())
+    return out
+
+
 def build(centers, normals, radii, t, ncoef, nint, se_factor=0.9, heads=((0.0, 1.0),), axis=0, box=None,
-          keep="connected"):
+          keep="connected", device=None):
     """Intersections, constant-head boundaries and connectivity for given discs.
 
     heads: ((coordinate, head), ...) of planes normal to ``axis`` cutting the
     box (the reference's set_constant_head_boundary with a plane of radius L).
     keep: "connected" (reference check_connectivity), "largest_spanning"
     (only the largest cluster that joins two different heads), or "all".
+    device: None computes the disc-disc intersections on the host (numpy);
+    a CUDA ordinal (-1: the current one) computes them, and the clusters, on
+    the GPU, with the same results.
     """
     centers = np.asarray(centers, float)
     normals = np.asarray(normals, float)
@@ -187,20 +240,25 @@ def build(centers, normals, radii, t, ncoef, nint, se_factor=0.9, heads=((0.0, 1
         net.elements.append(Element(type=1, frac0=f, radius=float(radii[f]), ncoef=ncoef, nint=nint))
         net.frac_elems.append([f])
     # intersections
-    pairs = _candidate_pairs(centers, radii)
-    if len(pairs):
-        i, k = pairs[:, 0], pairs[:, 1]
-        valid, e0, e1 = plane_disc_intersections(centers[i], normals[i], xv[i], yv[i], radii[i],
-                                                 centers[k], normals[k], xv[k], yv[k], radii[k])
-        e0 = shorten(e0, se_factor)
-        e1 = shorten(e1, se_factor)
-        for p in np.nonzero(valid)[0]:
-            a, b = int(i[p]), int(k[p])
-            net.elements.append(Element(type=0, frac0=a, frac1=b, ep0=(e0[p, 0], e0[p, 1]),
-                                        ep1=(e1[p, 0], e1[p, 1]), ncoef=ncoef, nint=nint))
-            el = len(net.elements) - 1
-            net.frac_elems[a].append(el)
-            net.frac_elems[b].append(el)
+    if device is None:
+        pairs = _candidate_pairs(centers, radii)
+        if len(pairs):
+            i, k = pairs[:, 0], pairs[:, 1]
+            valid, e0, e1 = plane_disc_intersections(centers[i], normals[i], xv[i], yv[i], radii[i],
+                                                     centers[k], normals[k], xv[k], yv[k], radii[k])
+            e0 = shorten(e0, se_factor)
+            e1 = shorten(e1, se_factor)
+            sel = np.nonzero(valid)[0]
+            pairs, e0, e1 = pairs[sel], e0[sel], e1[sel]
+    else:
+        pairs, e0, e1 = gpu_disc_intersections(centers, normals, xv, yv, radii, se_factor, device)
+    for p in range(len(pairs)):
+        a, b = int(pairs[p, 0]), int(pairs[p, 1])
+        net.elements.append(Element(type=0, frac0=a, frac1=b, ep0=(e0[p, 0], e0[p, 1]),
+                                    ep1=(e1[p, 0], e1[p, 1]), ncoef=ncoef, nint=nint))
+        el = len(net.elements) - 1
+        net.frac_elems[a].append(el)
+        net.frac_elems[b].append(el)
     # constant-head planes (set_head_boundary): a disc of radius L normal to the axis
     if box is not None:
         L = float(box)
@@ -226,12 +284,17 @@ def build(centers, normals, radii, t, ncoef, nint, se_factor=0.9, heads=((0.0, 1
                                             ncoef=ncoef, nint=nint))
                 net.frac_elems[f].append(len(net.elements) - 1)
     if keep != "all":
-        net = _prune(net, keep)
+        net = _prune(net, keep, device)
     return net
 
 
-def _clusters(net):
+def _clusters(net, device=None):
+    """Cluster label of every fracture: the smallest fracture index of its
+    connected component (on the GPU with device set, andfn_b200_clusters)."""
     nf = len(net.radii)
+    if device is not None:
+        pairs = np.array([(e.frac0, e.frac1) for e in net.elements if e.type == 0], np.int64).reshape(-1, 2)
+        return gpu_clusters(nf, pairs, device)
     par = np.arange(nf)
 
     def find(x):
@@ -241,12 +304,13 @@ def _clusters(net):
         return x
     for e in net.elements:
         if e.type == 0:
-            par[find(e.frac0)] = find(e.frac1)
+            a, b = find(e.frac0), find(e.frac1)
+            par[max(a, b)] = min(a, b)  # the smaller index stays the root
     return np.array([find(f) for f in range(nf)])
 
 
-def _prune(net, keep):
-    root = _clusters(net)
+def _prune(net, keep, device=None):
+    root = _clusters(net, device)
     bnd = {}
     for e in net.elements:
         if e.type in (2, 3) and not np.isnan(e.head):  # a NaN head: prescribed discharge, no head boundary

@@ -251,6 +251,31 @@ int andfn_b200_fp64_peak(int32_t device, double *tflops);
 int andfn_b200_eval_heads_noalloc(AndfnHandle *h, const int64_t *frac,
                                   const double *z, int64_t npts, double *out);
 
+/* ---- network geometry on the device ---------------------------------------
+ * Replace the host steps that build a network before the solve:
+ * andfn_b200_disc_intersections is get_fracture_intersections
+ * (andfn/geometry_functions.py:623-713) with fracture_intersection (:302-356)
+ * and shorten_line (:974-993) by se_factor, for every pair of discs i < k
+ * with |c_i - c_k| <= r_i + r_k.  Inputs are nf x 3 arrays (centers,
+ * normals, the discs' in-plane x / y unit vectors as andfn/fracture.py:60-68
+ * builds them) and the radii.  Output, sorted by (i, k): out_pairs[j] =
+ * (i, k), out_ep0[j] / out_ep1[j] = the segment's two endpoints (complex,
+ * re/im interleaved) in disc i's / disc k's frame.  *out_n receives the
+ * number of segments; when it exceeds cap the call returns ANDFN_BAD_INPUT
+ * and writes nothing (call again with cap >= *out_n).  Every operation is
+ * rounded on its own in numpy's order, so the results equal the host
+ * restatement (andfn_b200/network.py) bit for bit.
+ * andfn_b200_clusters: the connected components of a pair list (the graph
+ * check_connectivity_hpc walks, :1121-1294); out_root[f] is the smallest
+ * fracture index of f's component.  device < 0: the current device.
+ * andfn_b200_geometry_last_error: message of the last failing call of the two. */
+int andfn_b200_disc_intersections(int32_t device, int64_t nf, const double *centers, const double *normals,
+                                  const double *xvec, const double *yvec, const double *radii, double se_factor,
+                                  int64_t cap, int64_t *out_pairs, double *out_ep0, double *out_ep1,
+                                  int64_t *out_n);
+int andfn_b200_clusters(int32_t device, int64_t nf, int64_t npairs, const int64_t *pairs, int64_t *out_root);
+const char *andfn_b200_geometry_last_error(void);
+
 /* ---- adjoint: gradient with respect to log-transmissivity ---------------
  * No reference counterpart (the reference computes no derivatives).  For an
  * objective J(coef, q, C, log t) of the converged solve of a single-network
