@@ -43,6 +43,7 @@ namespace andfn {
 
 static constexpr double PI = 3.141592653589793115997963468544185161590576171875;
 static constexpr int EVAL_THREADS = 128;
+static constexpr int HV_THREADS = 128;  // head_vector_kernel: one CTA per system row
 static constexpr int UPDATE_WARPS = 4;
 static constexpr int SOLVE_THREADS = 512;
 // Discharge solves through the explicit inverse X take one refinement step
@@ -666,14 +667,45 @@ __global__ void __launch_bounds__(UPDATE_WARPS * 32) update_kernel(Net net, cons
   if (psi) {
     // get_dpsi_corr (hpc_math_functions.py:407-447) and the unwrapping of
     // psi in cauchy_integral_domega(_line) (:496-505, :586-595):
-    // psi'_k = psi_k - sum_{i<k} dpsi_corr_i.
+    // psi'_k = psi_k - sum_{i<k} dpsi_corr_i.  The cuts are staged 32 at a
+    // time in shared memory (one load round by the warp's lanes); every lane
+    // then adds them in cut order, as one serial loop over the cuts would.
+    __shared__ int s_cp[UPDATE_WARPS][32];
+    __shared__ double s_qv[UPDATE_WARPS][32];
     const int nc = net.cut_n[e];
     const int *cp = net.cut_pos + (size_t)e * net.cut_cap;
     const int *ce = net.cut_elem + (size_t)e * net.cut_cap;
     const int *cs = net.cut_sign + (size_t)e * net.cut_cap;
     double *dc = net.dpsi_corr + (size_t)e * 2 * MC;
+    double cum0 = 0.0, here0 = 0.0, cum1 = 0.0, here1 = 0.0;  // points lane and lane + 32
+    const int k0 = lane, k1 = lane + 32;
+    for (int c0 = 0; c0 < nc; c0 += 32) {
+      const int cnt = min(32, nc - c0);
+      __syncwarp();
+      if (lane < cnt) {
+        s_cp[warp][lane] = cp[c0 + lane];
+        s_qv[warp][lane] = net.q[ce[c0 + lane]] * (double)cs[c0 + lane];
+      }
+      __syncwarp();
+      for (int c = 0; c < cnt; c++) {
+        const int pos = s_cp[warp][c];
+        const double qv = s_qv[warp][c];
+        if (pos < k0) cum0 += qv;
+        if (pos == k0) here0 += qv;
+        if (pos < k1) cum1 += qv;
+        if (pos == k1) here1 += qv;
+      }
+    }
     __syncwarp();
-    for (int k = lane; k < n; k += 32) {
+    if (k0 < n) {
+      if (k0 < n - 1) dc[k0] = here0;
+      v0[k0] -= cum0;
+    }
+    if (k1 < n) {
+      if (k1 < n - 1) dc[k1] = here1;
+      v0[k1] -= cum1;
+    }
+    for (int k = lane + 64; k < n; k += 32) {  // points beyond 64 (nint > 64), in the serial form
       double cum = 0.0, here = 0.0;
       for (int c = 0; c < nc; c++) {
         const double qv = net.q[ce[c]] * (double)cs[c];
@@ -3256,7 +3288,7 @@ struct AndfnHandle {
   DBuf<long long> binv_off;
   DBuf<int> binv_order, binv_roff, bcsr_ptr, bcsr_col, bsing, binv_small, binv_big;
   int binv_maxn = 0, binv_nsmall = 0, binv_nbig = 0, binv_smem_n = 0, binv_bign = 0;
-  double dense_frac = 0.4;  // ordering: dense tail once the minimum degree reaches this fraction
+  double dense_frac = 0.15;  // ordering: dense tail once the minimum degree reaches this fraction
   bool bcsr_built = false;
   DBuf<int> pinv, qcol;
   DBuf<TriDesc> tri;
@@ -3883,8 +3915,10 @@ static int create_impl(AndfnHandle *H, int R, const char *const *F, const int64_
   const bool skip_order =
       R > 1 && H->winv_enabled && maxn_sys <= BINV_MAX_N && binv_cluster_smem(maxn_sys) <= BINV_CLUSTER_SMEM_MAX;
   // the ordering hands the remaining columns to the dense tail once the
-  // minimum degree reaches this fraction of what remains
-  double dense_frac = 0.4;
+  // minimum degree reaches this fraction of what remains: 0.15 balances the
+  // host's serial sparse LU against the device's dense LU (2,118-fracture
+  // network: 41.6 ms a solve at 0.4, 38.5 ms at 0.15, 38.7 ms at 0.1)
+  double dense_frac = 0.15;
   if (const char *v = getenv("ANDFN_B200_DENSE_FRAC")) {
     const double x = atof(v);
     if (x > 0.0 && x <= 1.0) dense_frac = x;
@@ -4872,7 +4906,7 @@ static int enqueue_iteration(AndfnHandle *H, cudaStream_t s, int blend_mode, int
   Net net = H->net();
   mark(H, s, b, K_RHS, 0);
   if (H->use_head_sums) {
-    head_vector_kernel<<<(H->N * 32 + 255) / 256, 256, 0, s>>>(net, H->hs.gptr.p, H->hs.sidx.p, H->hs.S.p);
+    head_vector_kernel<<<H->N, HV_THREADS, 0, s>>>(net, H->hs.gptr.p, H->hs.sidx.p, H->hs.S.p);
   } else {
     if (H->n_rhs_items > 0)
       eval_kernel<true><<<H->n_rhs_items, EVAL_THREADS, H->eval_smem, s>>>(net, H->rhs_items.p, H->rhs_pts.p,
@@ -6535,15 +6569,33 @@ __global__ void rhs_sums_kernel(Net net, const int *__restrict__ pair_g, const i
 // points): one warp per system row, b = (S1 / D) / t1 - (S0 / D) / t0 for an
 // intersection, phi - S0 / D for a constant-head line or well, 0 for a
 // continuity row, with S_side = sum over the side's pairs of Re(coef * S).
-__global__ void head_vector_kernel(Net net, const int *__restrict__ gptr, const int *__restrict__ sidx,
-                                   const cd *__restrict__ S) {
-  const int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+// One CTA of HV_THREADS per system row: the row side's power-sum entries are
+// split over the CTA's threads (four index -> coefficient chains in flight
+// per thread) and summed with a fixed-order tree, so the result does not
+// depend on timing; the longest rows (1,700 entries) no longer sit on one
+// warp's dependent loads.
+__device__ __forceinline__ double hv_block_sum(double v, double *red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  v = warp_sum(v);
+  __syncthreads();  // red is free (a previous sum's readers are done)
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  double t = 0.0;
+#pragma unroll
+  for (int w = 0; w < HV_THREADS / 32; w++) t += red[w];
+  return t;
+}
+__global__ void __launch_bounds__(HV_THREADS) head_vector_kernel(Net net, const int *__restrict__ gptr,
+                                                                  const int *__restrict__ sidx,
+                                                                  const cd *__restrict__ S) {
+  __shared__ double red[HV_THREADS / 32];
+  const int g = blockIdx.x;
   if (g >= net.N) return;
   const SolveState *st = net.st + net.real_row[g];
   if (st->done || !st->solve_q) return;
   const int r = net.row_de[g];
   if (r < 0) {
-    if (lane == 0) net.bvec[g] = net.bknown ? net.bknown[g] : 0.0;
+    if (threadIdx.x == 0) net.bvec[g] = net.bknown ? net.bknown[g] : 0.0;
     return;
   }
   const int e = net.de_ids[r];
@@ -6552,23 +6604,24 @@ __global__ void head_vector_kernel(Net net, const int *__restrict__ gptr, const 
   for (int sd = 0; sd < sides; sd++) {
     double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
     const int x1 = gptr[2 * r + sd + 1];
-    int x = gptr[2 * r + sd] + lane;
-    for (; x + 96 < x1; x += 128) {  // four index -> coefficient chains in flight
-      const int i0 = sidx[x], i1 = sidx[x + 32], i2 = sidx[x + 64], i3 = sidx[x + 96];
-      const cd v0 = S[x], v1 = S[x + 32], v2 = S[x + 64], v3 = S[x + 96];
+    int x = gptr[2 * r + sd] + threadIdx.x;
+    constexpr int T = HV_THREADS;
+    for (; x + 3 * T < x1; x += 4 * T) {  // four index -> coefficient chains in flight
+      const int i0 = sidx[x], i1 = sidx[x + T], i2 = sidx[x + 2 * T], i3 = sidx[x + 3 * T];
+      const cd v0 = S[x], v1 = S[x + T], v2 = S[x + 2 * T], v3 = S[x + 3 * T];
       const cd c0 = net.coef[i0], c1 = net.coef[i1], c2 = net.coef[i2], c3 = net.coef[i3];
       a0 = fma(c0.re, v0.re, fma(-c0.im, v0.im, a0));
       a1 = fma(c1.re, v1.re, fma(-c1.im, v1.im, a1));
       a2 = fma(c2.re, v2.re, fma(-c2.im, v2.im, a2));
       a3 = fma(c3.re, v3.re, fma(-c3.im, v3.im, a3));
     }
-    for (; x < x1; x += 32) {
+    for (; x < x1; x += T) {
       const cd c = net.coef[sidx[x]], v = S[x];
       a0 = fma(c.re, v.re, fma(-c.im, v.im, a0));
     }
-    sum[sd] = warp_sum((a0 + a1) + (a2 + a3));
+    sum[sd] = hv_block_sum((a0 + a1) + (a2 + a3), red);
   }
-  if (lane == 0) {
+  if (threadIdx.x == 0) {
     const double D = net.D;
     double b;
     if (sides == 2)

@@ -60,7 +60,7 @@ struct LuFactors {
 // *dense_tail (optional) receives the number of trailing columns that remain
 // once the minimum degree reaches dense_frac of the remaining columns (the
 // graph is then nearly complete; 0 if that never happens with >= 64 left).
-std::vector<int> column_min_degree_order(const CscMatrix &A, int *dense_tail = nullptr, double dense_frac = 0.4,
+std::vector<int> column_min_degree_order(const CscMatrix &A, int *dense_tail = nullptr, double dense_frac = 0.15,
                                          int max_dense = 3072);
 
 // LU with partial pivoting: left-looking sparse (Gilbert-Peierls) for the
