@@ -2249,16 +2249,16 @@ static constexpr int WINV_RPC = 64;
 static_assert(WINV_THREADS == 512, "16 warps split each row of X");
 
 template <int STAGE, bool ADJ>
-__global__ void __launch_bounds__(WINV_THREADS) winv_gemv_kernel(Net net, const double *__restrict__ X, int ldw,
+__global__ void __launch_bounds__(WINV_THREADS, 2) winv_gemv_kernel(Net net, const double *__restrict__ X, int ldw,
                                                                  const double *__restrict__ src,
                                                                  double *__restrict__ x0,
                                                                  unsigned long long *__restrict__ acc) {
   SolveState *st = net.st;
   if (st->done) return;
-  // forward: without refinement (refine is set when the run starts)
-  // the first pass writes the result itself and the second does not run;
-  // the adjoint's solves are not refined
-  const bool fin = ADJ ? true : (STAGE == 1 || !st->refine);
+  // forward: without refinement (refine is set when the run starts) the
+  // first pass writes the result itself and the second does not run; the
+  // adjoint's transposed solves always take the refinement step
+  const bool fin = (STAGE == 1) || (!ADJ && !st->refine);
   if (!ADJ) {
     if (STAGE == 0 && blockIdx.x == 0 && threadIdx.x == 0) st->nit += 1;
     if (!st->solve_q) return;  // uniform: solve_q is written only by reduce_kernel
@@ -2279,26 +2279,36 @@ __global__ void __launch_bounds__(WINV_THREADS) winv_gemv_kernel(Net net, const 
   const int seg = ldw / 32;  // double2 per warp and row
   const double2 *vs = reinterpret_cast<const double2 *>(v) + warp * seg;
   const double2 zero2 = make_double2(0.0, 0.0);
-  for (int k = r0; k < r1; k += 2) {
-    const bool two = k + 1 < r1;
+  // four rows at a time: per lane 8 loads of 16 B in flight per round (each
+  // row's segment in two halves of 32 double2), half the latency rounds of
+  // two rows at a time; rows beyond r1 reread row k (results not stored)
+  for (int k = r0; k < r1; k += 4) {
     const double2 *ra = reinterpret_cast<const double2 *>(X + (size_t)k * ldw) + warp * seg;
-    const double2 *rb = two ? ra + ldw / 2 : ra;
-    double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0;
-#pragma unroll 2
+    const double2 *rb = (k + 1 < r1) ? ra + ldw / 2 : ra;
+    const double2 *rc = (k + 2 < r1) ? ra + ldw : ra;
+    const double2 *rd = (k + 3 < r1) ? ra + 3 * (size_t)(ldw / 2) : ra;
+    double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0, c0 = 0.0, c1 = 0.0, d0 = 0.0, d1 = 0.0;
     for (int j = lane; j < seg; j += 64) {
       const bool h = j + 32 < seg;
-      const double2 wa0 = __ldcs(ra + j), wb0 = __ldcs(rb + j);
+      const double2 wa0 = __ldcs(ra + j), wb0 = __ldcs(rb + j), wc0 = __ldcs(rc + j), wd0 = __ldcs(rd + j);
       const double2 wa1 = h ? __ldcs(ra + j + 32) : zero2, wb1 = h ? __ldcs(rb + j + 32) : zero2;
+      const double2 wc1 = h ? __ldcs(rc + j + 32) : zero2, wd1 = h ? __ldcs(rd + j + 32) : zero2;
       const double2 x0v = vs[j], x1v = h ? vs[j + 32] : zero2;
       a0 = fma(wa0.y, x0v.y, fma(wa0.x, x0v.x, a0));
       b0 = fma(wb0.y, x0v.y, fma(wb0.x, x0v.x, b0));
+      c0 = fma(wc0.y, x0v.y, fma(wc0.x, x0v.x, c0));
+      d0 = fma(wd0.y, x0v.y, fma(wd0.x, x0v.x, d0));
       a1 = fma(wa1.y, x1v.y, fma(wa1.x, x1v.x, a1));
       b1 = fma(wb1.y, x1v.y, fma(wb1.x, x1v.x, b1));
+      c1 = fma(wc1.y, x1v.y, fma(wc1.x, x1v.x, c1));
+      d1 = fma(wd1.y, x1v.y, fma(wd1.x, x1v.x, d1));
     }
-    const double sa = warp_sum(a0 + a1), sb = warp_sum(b0 + b1);
+    const double sa = warp_sum(a0 + a1), sb = warp_sum(b0 + b1), sc = warp_sum(c0 + c1), sd = warp_sum(d0 + d1);
     if (lane == 0) {
       s_part[k - r0][warp] = sa;
-      if (two) s_part[k + 1 - r0][warp] = sb;
+      if (k + 1 < r1) s_part[k + 1 - r0][warp] = sb;
+      if (k + 2 < r1) s_part[k + 2 - r0][warp] = sc;
+      if (k + 3 < r1) s_part[k + 3 - r0][warp] = sd;
     }
   }
   __syncthreads();
@@ -3142,6 +3152,10 @@ static void set_error(const std::string &s) { g_last_error = s; }
 // Device buffer that keeps its allocation when it is re-filled with no more
 // elements than it holds (cudaFree synchronises the device, so repeated
 // solves on one handle should not reallocate).
+// Host milliseconds spent in device allocation and release on this thread
+// (reported per solve as ms_alloc).
+static thread_local double g_alloc_ms = 0.0;
+
 template <class T>
 struct DBuf {
   T *p = nullptr;
@@ -3153,10 +3167,17 @@ struct DBuf {
     n = count;
     if (count == 0) return cudaSuccess;
     cap = count;
-    return cudaMalloc(&p, sizeof(T) * count);
+    const auto t0 = std::chrono::steady_clock::now();
+    const cudaError_t e = cudaMalloc(&p, sizeof(T) * count);
+    g_alloc_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return e;
   }
   void release() {
-    if (p) cudaFree(p);
+    if (p) {
+      const auto t0 = std::chrono::steady_clock::now();
+      cudaFree(p);
+      g_alloc_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
     p = nullptr;
     n = cap = 0;
   }
@@ -3213,6 +3234,7 @@ struct HeadSums {
   DBuf<cd> S;
   int npairs = 0;
   bool valid = false;
+  bool long_rows = false;  // > 256 entries a row on average: a CTA per row, else a warp
   int mc = 0;
   std::vector<int> ncoef;  // the ncoef the sums were computed for
 };
@@ -4660,6 +4682,7 @@ static void launch_trisolve_kernel(AndfnHandle *H, const Net &net, cudaStream_t 
 }
 
 static int build_head_sums(AndfnHandle *H);
+template <int T, int RPB>
 __global__ void head_vector_kernel(Net net, const int *__restrict__ gptr, const int *__restrict__ sidx,
                                    const cd *__restrict__ S);
 
@@ -4677,7 +4700,6 @@ static void launch_winv_solve(AndfnHandle *H, const Net &net, cudaStream_t s, co
   // two CTAs of 512 threads per SM, at most WINV_RPC rows per CTA
   const int grid = std::max(2 * H->num_sms, (N + WINV_RPC - 1) / WINV_RPC);
   winv_gemv_kernel<0, ADJ><<<grid, WINV_THREADS, vsm, s>>>(net, X, ldw, net.bvec, H->wx0.p, H->wacc.p);
-  if (ADJ) return;  // the transposed solves are not refined
   winv_resid_kernel<ADJ><<<(N * 32 + 255) / 256, 256, 0, s>>>(net, rp, cols, map, H->d_mvals.p + H->sys[0].ent0,
                                                              H->wx0.p, H->wr.p, N);
   winv_gemv_kernel<1, ADJ><<<grid, WINV_THREADS, vsm, s>>>(net, X, ldw, H->wr.p, H->wx0.p, H->wacc.p);
@@ -4906,7 +4928,10 @@ static int enqueue_iteration(AndfnHandle *H, cudaStream_t s, int blend_mode, int
   Net net = H->net();
   mark(H, s, b, K_RHS, 0);
   if (H->use_head_sums) {
-    head_vector_kernel<<<H->N, HV_THREADS, 0, s>>>(net, H->hs.gptr.p, H->hs.sidx.p, H->hs.S.p);
+    if (H->hs.long_rows)
+      head_vector_kernel<HV_THREADS, 1><<<H->N, HV_THREADS, 0, s>>>(net, H->hs.gptr.p, H->hs.sidx.p, H->hs.S.p);
+    else
+      head_vector_kernel<32, 4><<<(H->N + 3) / 4, 128, 0, s>>>(net, H->hs.gptr.p, H->hs.sidx.p, H->hs.S.p);
   } else {
     if (H->n_rhs_items > 0)
       eval_kernel<true><<<H->n_rhs_items, EVAL_THREADS, H->eval_smem, s>>>(net, H->rhs_items.p, H->rhs_pts.p,
@@ -5285,6 +5310,7 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
     st.refined_solves = (H->winv_ready || H->binv_ready) ? f.n_refined : 0;
     st.sweep_variant = H->use_tab ? H->sweep_variant : -1;
     st.loop_launches = loop_launches;
+    st.ms_alloc = g_alloc_ms;
     st.levels_l = H->sys[r].nlev_l;
     st.levels_u = H->sys[r].nlev_u;
     for (int i = 0; i < 8; i++) st.tri_cycles[i] = f.tri_cycles[i];
@@ -5924,6 +5950,7 @@ int andfn_b200_batch_solve(int64_t R, void *const *frac_recs, const int64_t *nf,
                            const AndfnConstants *constants, AndfnSolveStats *stats) {
   auto t0 = std::chrono::steady_clock::now();
   g_h2d_bytes = g_d2h_bytes = 0;
+  g_alloc_ms = 0.0;
   AndfnHandle *H = nullptr;
   int rc = andfn_b200_batch_create(&H, R, frac_recs, nf, elem_recs, ne, layout, discharge_int, -1);
   if (rc) return rc;
@@ -5948,6 +5975,8 @@ int andfn_b200_batch_solve(int64_t R, void *const *frac_recs, const int64_t *nf,
       stats[r].d2h_bytes = g_d2h_bytes;
     }
   andfn_b200_destroy(H);
+  if (stats)
+    for (int64_t r = 0; r < R; r++) stats[r].ms_alloc = g_alloc_ms;  // creation, run and destruction
   return rc;
 }
 
@@ -6569,33 +6598,39 @@ __global__ void rhs_sums_kernel(Net net, const int *__restrict__ pair_g, const i
 // points): one warp per system row, b = (S1 / D) / t1 - (S0 / D) / t0 for an
 // intersection, phi - S0 / D for a constant-head line or well, 0 for a
 // continuity row, with S_side = sum over the side's pairs of Re(coef * S).
-// One CTA of HV_THREADS per system row: the row side's power-sum entries are
-// split over the CTA's threads (four index -> coefficient chains in flight
-// per thread) and summed with a fixed-order tree, so the result does not
-// depend on timing; the longest rows (1,700 entries) no longer sit on one
-// warp's dependent loads.
-__device__ __forceinline__ double hv_block_sum(double v, double *red) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+// The head vector, a group of T threads per system row (RPB rows per CTA):
+// the row side's power-sum entries are split over the group's threads (four
+// index -> coefficient chains in flight per thread) and summed with a
+// fixed-order tree, so the result does not depend on timing.  Long rows
+// (one network: ~380 entries on average, 1,700 at most) take a 128-thread
+// CTA each, so they no longer sit on one warp's dependent loads; short rows
+// (batches of small realizations) a warp each, four to a CTA.
+template <int T>
+__device__ __forceinline__ double hv_group_sum(double v, double *red) {
   v = warp_sum(v);
+  if (T == 32) return v;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   __syncthreads();  // red is free (a previous sum's readers are done)
   if (lane == 0) red[warp] = v;
   __syncthreads();
   double t = 0.0;
 #pragma unroll
-  for (int w = 0; w < HV_THREADS / 32; w++) t += red[w];
+  for (int w = 0; w < T / 32; w++) t += red[w];
   return t;
 }
-__global__ void __launch_bounds__(HV_THREADS) head_vector_kernel(Net net, const int *__restrict__ gptr,
-                                                                  const int *__restrict__ sidx,
-                                                                  const cd *__restrict__ S) {
-  __shared__ double red[HV_THREADS / 32];
-  const int g = blockIdx.x;
-  if (g >= net.N) return;
+template <int T, int RPB>
+__global__ void __launch_bounds__(T * RPB) head_vector_kernel(Net net, const int *__restrict__ gptr,
+                                                               const int *__restrict__ sidx,
+                                                               const cd *__restrict__ S) {
+  __shared__ double red[T / 32 > 0 ? T / 32 : 1];
+  const int t = (T == 32) ? (threadIdx.x & 31) : threadIdx.x;
+  const int g = blockIdx.x * RPB + ((T == 32) ? (threadIdx.x >> 5) : 0);
+  if (g >= net.N) return;  // uniform over the row's group
   const SolveState *st = net.st + net.real_row[g];
   if (st->done || !st->solve_q) return;
   const int r = net.row_de[g];
   if (r < 0) {
-    if (threadIdx.x == 0) net.bvec[g] = net.bknown ? net.bknown[g] : 0.0;
+    if (t == 0) net.bvec[g] = net.bknown ? net.bknown[g] : 0.0;
     return;
   }
   const int e = net.de_ids[r];
@@ -6604,8 +6639,7 @@ __global__ void __launch_bounds__(HV_THREADS) head_vector_kernel(Net net, const 
   for (int sd = 0; sd < sides; sd++) {
     double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
     const int x1 = gptr[2 * r + sd + 1];
-    int x = gptr[2 * r + sd] + threadIdx.x;
-    constexpr int T = HV_THREADS;
+    int x = gptr[2 * r + sd] + t;
     for (; x + 3 * T < x1; x += 4 * T) {  // four index -> coefficient chains in flight
       const int i0 = sidx[x], i1 = sidx[x + T], i2 = sidx[x + 2 * T], i3 = sidx[x + 3 * T];
       const cd v0 = S[x], v1 = S[x + T], v2 = S[x + 2 * T], v3 = S[x + 3 * T];
@@ -6619,9 +6653,9 @@ __global__ void __launch_bounds__(HV_THREADS) head_vector_kernel(Net net, const 
       const cd c = net.coef[sidx[x]], v = S[x];
       a0 = fma(c.re, v.re, fma(-c.im, v.im, a0));
     }
-    sum[sd] = hv_block_sum((a0 + a1) + (a2 + a3), red);
+    sum[sd] = hv_group_sum<T>((a0 + a1) + (a2 + a3), red);
   }
-  if (threadIdx.x == 0) {
+  if (t == 0) {
     const double D = net.D;
     double b;
     if (sides == 2)
@@ -7054,6 +7088,7 @@ static int build_head_sums(AndfnHandle *H) {
     spairs.insert(spairs.end(), by_src[el].begin(), by_src[el].end());
   }
   hs.npairs = (int)pg.size();
+  hs.long_rows = off > 256LL * std::max(1, H->N);
   CK(upload(hs.gptr, gptr, s));
   if (hs.npairs > 0) {
     CK(upload(hs.pair_g, pg, s));
@@ -7232,7 +7267,9 @@ static void launch_trisolve_adj(AndfnHandle *H, const Net &net, cudaStream_t s) 
 }
 
 // per transposed sweep: 3 memsets + 5 kernels + the transposed discharge solve
-static int adj_sweep_launches(const AndfnHandle *) { return 8 + 1; }
+// operations of one transposed sweep (3 memsets, 5 kernels, the transposed
+// discharge solve: 3 kernels through X^T with its refinement step, else 1)
+static int adj_sweep_launches(const AndfnHandle *H) { return 8 + ((H->adj && H->adj->use_winv) ? 3 : 1); }
 static constexpr int ADJ_RESTART = GM_MK;     // Krylov basis size before a restart
 
 // One transposed sweep at lam = x: gc = Phi_c^T x + b_c^T A^-T (gd + Phi_d^T x),

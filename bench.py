@@ -314,7 +314,7 @@ def run_gpu(args):
         ls = andfn_b200.last_stats
         e2e_phases.append({k: round(ls[k], 2) for k in ("ms_upload", "ms_create_upload", "ms_create_tables",
                                                        "ms_create_order", "ms_setup", "ms_factor", "ms_iterate",
-                                                       "ms_download")})
+                                                       "ms_download", "ms_alloc", "ms_total")})
         h2d = ls["h2d_bytes"]
         d2h = ls["d2h_bytes"]
     # median: host-side phases share the box's CPUs with other jobs, so a

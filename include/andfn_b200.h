@@ -109,6 +109,9 @@ typedef struct AndfnSolveStats {
                                device work queue; -1: no pair tables (adaptive coefficient growth) */
   int64_t loop_launches;    /* graph launches of the iteration loop (1: the whole loop runs on the
                                device in one launch) */
+  double ms_alloc;          /* host milliseconds in device allocation and release on the calling
+                               thread (andfn_b200_solve: the whole call; a run: since the thread's
+                               previous one-call solve) */
 } AndfnSolveStats;
 
 /* ---- one-call drop-in (replaces andfn/hpc/hpc_solve.py:55 solve) --------
