@@ -18,6 +18,22 @@ __version__ = "0.1.0"
 _saved = {}
 
 
+def release_cached_memory():
+    """Free the device memory the library keeps for reuse between handles."""
+    from . import _ffi
+    _ffi.lib().andfn_b200_release_cached_memory()
+
+
+def cached_memory(device: int = 0) -> dict:
+    """Bytes of device memory cached on ``device``, and the cache's hits and
+    misses since the process started."""
+    import ctypes
+    from . import _ffi
+    b, h, m = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+    _ffi.check(_ffi.lib().andfn_b200_cached_memory(device, ctypes.byref(b), ctypes.byref(h), ctypes.byref(m)))
+    return {"bytes": b.value, "hits": h.value, "misses": m.value}
+
+
 def install():
     """Route ``andfn.DFN.solve`` through the GPU solve."""
     import andfn.dfn as dfn_mod
@@ -32,6 +48,6 @@ def uninstall():
         dfn_mod.hpc_solve = _saved.pop("hpc_solve")
 
 
-__all__ = ["solve", "install", "uninstall", "Solver", "BatchSolver", "solve_batch", "last_stats", "element_dtype", "fracture_dtype",
+__all__ = ["solve", "install", "uninstall", "release_cached_memory", "cached_memory", "Solver", "BatchSolver", "solve_batch", "last_stats", "element_dtype", "fracture_dtype",
            "constants_dtype", "default_constants", "layout_of", "AndfnLayout", "AndfnConstants",
            "AndfnSolveStats"]

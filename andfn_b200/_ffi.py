@@ -23,7 +23,7 @@ EXPORTS = ("andfn_b200_solve", "andfn_b200_create", "andfn_b200_upload_state", "
            "andfn_b200_state_device", "andfn_b200_heads_device", "andfn_b200_heads_vjp",
            "andfn_b200_bc_residual", "andfn_b200_eval_w", "andfn_b200_eval_w_object",
            "andfn_b200_track", "andfn_b200_disc_intersections", "andfn_b200_clusters",
-           "andfn_b200_geometry_last_error")
+           "andfn_b200_geometry_last_error", "andfn_b200_release_cached_memory", "andfn_b200_cached_memory")
 
 STATUS = {0: "ok", 1: "max_iterations", 2: "nonfinite", 3: "singular", 10: "bad_layout", 11: "bad_input",
           12: "cuda_error", 13: "no_device", 14: "out_of_memory"}
@@ -87,6 +87,8 @@ def lib() -> ctypes.CDLL:
                                                          P]),
         ("andfn_b200_clusters", ctypes.c_int, [I32, I64, I64, P, P]),
         ("andfn_b200_geometry_last_error", ctypes.c_char_p, []),
+        ("andfn_b200_release_cached_memory", None, []),
+        ("andfn_b200_cached_memory", ctypes.c_int, [I32, P, P, P]),
     ):
         fn = getattr(L, name)
         fn.restype = res

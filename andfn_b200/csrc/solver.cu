@@ -1789,6 +1789,332 @@ __global__ void __launch_bounds__(256) dlu_gemm_kernel(double *__restrict__ S, i
   }
 }
 
+// ---------------------------------------------------------------------------
+// The same dense LU in one cooperative launch with a look-ahead of one panel:
+// every panel step costs two grid barriers instead of three kernel launches,
+// and CTA 0 factorises panel k+1 while the other CTAs are still applying
+// panel k to the rest of the trailing block.
+//   phase S(k)  all CTAs, a warp per column outside panel k: the panel's row
+//               interchanges, then U12 = L11^-1 A12 (as dlu_update_kernel);
+//   barrier;
+//   phase G(k)  A22 -= L21 U12 in items of DLUC_TR rows x DLU_NB columns (as
+//               dlu_gemm_kernel); the items of panel k+1's columns come
+//               first and each bumps a counter;
+//   phase P(k+1) CTA 0, once that counter shows panel k+1's columns are
+//               updated: the panel factorisation (as dlu_panel_kernel, the
+//               pivot search of a column fused with the update by the
+//               column before);
+//   barrier.
+// Every product, quotient and fused multiply-add is the one the three-kernel
+// path computes, in the same order, so the factors are the same bit for bit.
+// Waits are bounded: a barrier or the counter wait that runs out sets
+// DluSync::err and every CTA returns at its next barrier.
+static constexpr int DLUC_THREADS = 512;
+static constexpr int DLUC_TR = 128;                 // rows of a G item
+static constexpr unsigned DLUC_SPIN_LIMIT = 1u << 24;  // polls of a wait (>= 1 s with the sleeps)
+
+// dynamic shared memory of dlu_coop_kernel for a K x K block
+static size_t dluc_smem(int K) {
+  return sizeof(double) * (DLU_NB + 1) * (size_t)std::max(K, DLUC_TR + 2 * DLU_NB);
+}
+
+struct DluSync {
+  unsigned count;  // CTAs arrived at the current barrier
+  unsigned gen;    // barrier generation
+  unsigned cb0;    // G items of the next panel's columns finished (all panels)
+  int err;         // a wait ran out
+};
+
+__device__ __forceinline__ bool dluc_barrier(DluSync *sy, unsigned nblocks) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned *gen = &sy->gen;
+    volatile int *err = &sy->err;
+    int ok = 1;
+    const unsigned g = *gen;
+    __threadfence();
+    if (atomicAdd(&sy->count, 1u) == nblocks - 1) {
+      atomicExch(&sy->count, 0u);
+      __threadfence();
+      atomicAdd(&sy->gen, 1u);
+    } else {
+      unsigned it = 0;
+      while (*gen == g) {
+        if (*err || ++it > DLUC_SPIN_LIMIT) {
+          atomicExch(&sy->err, 1);
+          ok = 0;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    s_ok = ok && !*err;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// Panel factorisation of columns j0 .. j0+nb-1 (rows j0 .. K-1) by one CTA in
+// shared memory P (m x (DLU_NB + 1), row-major); loads the panel with L2
+// loads (other CTAs wrote it), stores it back and writes the pivots, U's
+// diagonal, the composite interchange and the bad-pivot flag.
+__device__ void dluc_panel(double *__restrict__ S, int K, int j0, int nb, const DluScratch &D, double *P) {
+  __shared__ double s_wv[DLUC_THREADS / 32];
+  __shared__ int s_wi[DLUC_THREADS / 32];
+  __shared__ int s_bad[DLUC_THREADS / 32];
+  __shared__ int s_piv[DLU_NB];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  constexpr int NW = DLUC_THREADS / 32;
+  const int m = K - j0;
+  double *const Sp = S + (size_t)j0 * K + j0;
+  for (int i = tid; i < m; i += DLUC_THREADS) {
+    double v[DLU_NB];
+#pragma unroll
+    for (int c = 0; c < DLU_NB; c++) v[c] = (c < nb) ? __ldcg(Sp + i + (size_t)c * K) : 0.0;
+#pragma unroll
+    for (int c = 0; c < DLU_NB; c++)
+      if (c < nb) P[i * (DLU_NB + 1) + c] = v[c];
+  }
+  __syncthreads();
+  // candidate of column 0
+  double best = -1.0;
+  int bi = m, bad = 0;
+  for (int i = tid; i < m; i += DLUC_THREADS) {
+    const double v = fabs(P[i * (DLU_NB + 1)]);
+    if (!(v <= DBL_MAX)) bad = 1;
+    if (v > best) {
+      best = v;
+      bi = i;
+    }
+  }
+  for (int jj = 0; jj < nb; jj++) {
+    // block argmax of column jj (largest magnitude, first row on a tie);
+    // every warp reduces the warps' candidates itself
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      const double ov = __shfl_down_sync(0xffffffffu, best, off);
+      const int oi = __shfl_down_sync(0xffffffffu, bi, off);
+      if (ov > best || (ov == best && oi < bi)) {
+        best = ov;
+        bi = oi;
+      }
+    }
+    bad = __any_sync(0xffffffffu, bad);
+    if (lane == 0) {
+      s_wv[warp] = best;
+      s_wi[warp] = bi;
+      s_bad[warp] = bad;
+    }
+    __syncthreads();
+    best = (lane < NW) ? s_wv[lane] : -1.0;
+    bi = (lane < NW) ? s_wi[lane] : m;
+    bad = (lane < NW) ? s_bad[lane] : 0;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      const double ov = __shfl_down_sync(0xffffffffu, best, off);
+      const int oi = __shfl_down_sync(0xffffffffu, bi, off);
+      if (ov > best || (ov == best && oi < bi)) {
+        best = ov;
+        bi = oi;
+      }
+    }
+    bad = __any_sync(0xffffffffu, bad);
+    int p = __shfl_sync(0xffffffffu, bi, 0);
+    const double bv = __shfl_sync(0xffffffffu, best, 0);
+    if (p >= m) p = jj;  // every entry NaN: keep the diagonal, flagged below
+    if (tid == 0) {
+      s_piv[jj] = p;
+      D.piv[j0 + jj] = j0 + p;
+      if ((bad || !(bv > 0.0)) && *D.flag == 0) *D.flag = j0 + jj + 1;
+    }
+    if (p != jj && tid < nb) {
+      const double a = P[jj * (DLU_NB + 1) + tid], b = P[p * (DLU_NB + 1) + tid];
+      P[jj * (DLU_NB + 1) + tid] = b;
+      P[p * (DLU_NB + 1) + tid] = a;
+    }
+    __syncthreads();
+    const double piv = P[jj * (DLU_NB + 1) + jj];
+    if (tid == 0) D.diag[j0 + jj] = piv;
+    const double inv = (piv != 0.0) ? 1.0 / piv : 0.0;
+    // update by column jj, and the candidate of column jj + 1
+    best = -1.0;
+    bi = m;
+    bad = 0;
+    const int nx = jj + 1;
+    for (int i = jj + 1 + tid; i < m; i += DLUC_THREADS) {
+      double *Pi = P + i * (DLU_NB + 1);
+      const double l = Pi[jj] * inv;
+      Pi[jj] = l;
+      for (int c = jj + 1; c < nb; c++) Pi[c] = fma(-l, P[jj * (DLU_NB + 1) + c], Pi[c]);
+      if (nx < nb) {
+        const double v = fabs(Pi[nx]);
+        if (!(v <= DBL_MAX)) bad = 1;
+        if (v > best) {
+          best = v;
+          bi = i;
+        }
+      }
+    }
+    __syncthreads();
+  }
+  for (int c = 0; c < nb; c++)
+    for (int i = tid; i < m; i += DLUC_THREADS) Sp[i + (size_t)c * K] = P[i * (DLU_NB + 1) + c];
+  if (warp == 0) {
+    // the panel's interchanges as one permutation of at most 2 nb rows
+    int row = -1, org = -1, cnt = 0;
+    for (int jj = 0; jj < nb; jj++) {
+      const int a = j0 + jj, b = j0 + s_piv[jj];
+      if (a == b) continue;
+      int ka, kb;
+      const unsigned ma = __ballot_sync(0xffffffffu, row == a);
+      if (ma) {
+        ka = __ffs(ma) - 1;
+      } else {
+        ka = cnt++;
+        if (lane == ka) row = org = a;
+      }
+      const unsigned mb = __ballot_sync(0xffffffffu, row == b);
+      if (mb) {
+        kb = __ffs(mb) - 1;
+      } else {
+        kb = cnt++;
+        if (lane == kb) row = org = b;
+      }
+      const int oa = __shfl_sync(0xffffffffu, org, ka), ob = __shfl_sync(0xffffffffu, org, kb);
+      if (lane == ka) org = ob;
+      if (lane == kb) org = oa;
+    }
+    if (lane < cnt) {
+      D.swap_dst[lane] = row;
+      D.swap_src[lane] = org;
+    }
+    if (lane == 0) *D.swap_cnt = cnt;
+  }
+}
+
+__global__ void __launch_bounds__(DLUC_THREADS, 1) dlu_coop_kernel(double *__restrict__ S, int K, DluScratch D,
+                                                                   DluSync *sy) {
+  // one dynamic buffer, used by one phase at a time: the panel (CTA 0), or
+  // L11 (phase S), or an item's L21 rows and U12 block (phase G)
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double *const P = reinterpret_cast<double *>(smem_raw);
+  double(*const s_l)[DLU_NB + 1] = reinterpret_cast<double(*)[DLU_NB + 1]>(P);
+  double(*const s_u)[DLU_NB + 1] = reinterpret_cast<double(*)[DLU_NB + 1]>(P + DLUC_TR * (DLU_NB + 1));
+  double(*const L11)[DLU_NB + 1] =
+      reinterpret_cast<double(*)[DLU_NB + 1]>(P + (DLUC_TR + DLU_NB) * (DLU_NB + 1));
+  const unsigned G = gridDim.x;
+  const int cta = blockIdx.x, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int NW = DLUC_THREADS / 32;
+  const int np = (K + DLU_NB - 1) / DLU_NB;
+  if (cta == 0) dluc_panel(S, K, 0, min(DLU_NB, K), D, P);
+  if (!dluc_barrier(sy, G)) return;
+  unsigned cb0_target = 0;
+  for (int k = 0; k < np; k++) {
+    const int j0 = k * DLU_NB, nb = min(DLU_NB, K - j0), c0 = j0 + nb, mt = K - c0;
+    // S(k): interchanges for every column outside the panel, U12 for the trailing ones
+    for (int idx = threadIdx.x; idx < nb * nb; idx += DLUC_THREADS) {
+      const int c = idx / nb, r = idx - c * nb;
+      L11[r][c] = (r > c) ? __ldcg(S + (size_t)(j0 + c) * K + j0 + r) : 0.0;
+    }
+    __syncthreads();
+    const int cnt = __ldcg(D.swap_cnt);
+    const int sw_src = (lane < cnt) ? __ldcg(D.swap_src + lane) : 0;
+    const int sw_dst = (lane < cnt) ? __ldcg(D.swap_dst + lane) : 0;
+    for (int cidx = cta * NW + warp; cidx < K - nb; cidx += G * NW) {
+      const int c = (cidx < j0) ? cidx : cidx + nb;
+      double *col = S + (size_t)c * K;
+      double v = 0.0;
+      if (lane < cnt) v = __ldcg(col + sw_src);
+      __syncwarp();
+      if (lane < cnt) col[sw_dst] = v;
+      __syncwarp();
+      if (c < c0) continue;
+      double x = (lane < nb) ? __ldcg(col + j0 + lane) : 0.0;
+#pragma unroll
+      for (int j = 0; j < DLU_NB; j++) {
+        const double xj = __shfl_sync(0xffffffffu, x, j);
+        if (lane > j && lane < nb) x = fma(-L11[lane][j], xj, x);
+      }
+      if (lane < nb) col[j0 + lane] = x;
+    }
+    if (!dluc_barrier(sy, G)) return;
+    if (mt <= 0) break;
+    // G(k): items (row tile, column block); column block 0 = panel k+1
+    const int nrt = (mt + DLUC_TR - 1) / DLUC_TR, ncb = (mt + DLU_NB - 1) / DLU_NB;
+    const int nitems = nrt * ncb;
+    cb0_target += (unsigned)nrt;
+    const int first = (G > 1) ? cta - 1 : 0, stride = (G > 1) ? (int)G - 1 : 1;
+    if (G == 1 || cta > 0) {
+      for (int it = first; it < nitems; it += stride) {
+        const int cb = it / nrt, rt = it - cb * nrt;
+        const int r0 = rt * DLUC_TR, cc0 = cb * DLU_NB;
+        const int ncols = min(DLU_NB, mt - cc0);
+        __syncthreads();  // the previous item's reads of s_l / s_u are done
+        for (int idx = threadIdx.x; idx < DLUC_TR * DLU_NB; idx += DLUC_THREADS) {
+          const int kk = idx / DLUC_TR, i = idx - kk * DLUC_TR;
+          s_l[i][kk] = (kk < nb && r0 + i < mt) ? __ldcg(S + (size_t)(j0 + kk) * K + c0 + r0 + i) : 0.0;
+        }
+        for (int idx = threadIdx.x; idx < DLU_NB * DLU_NB; idx += DLUC_THREADS) {
+          const int c = idx / DLU_NB, kk = idx - c * DLU_NB;
+          s_u[kk][c] = (kk < nb && c < ncols) ? __ldcg(S + (size_t)(c0 + cc0 + c) * K + j0 + kk) : 0.0;
+        }
+        __syncthreads();
+        // thread: row r0 + (tid % DLUC_TR), columns 4 (tid / DLUC_TR) .. +3
+        const int i = threadIdx.x % DLUC_TR, q0 = 4 * (threadIdx.x / DLUC_TR);
+        if (r0 + i < mt) {
+          double acc[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+          for (int kk = 0; kk < DLU_NB; kk++) {
+            const double a = s_l[i][kk];
+#pragma unroll
+            for (int q = 0; q < 4; q++) acc[q] = fma(a, s_u[kk][q0 + q], acc[q]);
+          }
+#pragma unroll
+          for (int q = 0; q < 4; q++) {
+            const int c = q0 + q;
+            if (c < ncols) {
+              double *dst = S + (size_t)(c0 + cc0 + c) * K + c0 + r0 + i;
+              *dst = __ldcg(dst) - acc[q];
+            }
+          }
+        }
+        if (cb == 0) {
+          __syncthreads();
+          if (threadIdx.x == 0) {
+            __threadfence();
+            atomicAdd(&sy->cb0, 1u);
+          }
+        }
+      }
+    }
+    // P(k+1) on CTA 0 once panel k+1's columns are updated
+    if (cta == 0) {
+      __shared__ int s_go;
+      if (threadIdx.x == 0) {
+        volatile unsigned *cb0 = &sy->cb0;
+        volatile int *err = &sy->err;
+        unsigned it = 0;
+        int go = 1;
+        while (*cb0 < cb0_target) {
+          if (*err || ++it > DLUC_SPIN_LIMIT) {
+            atomicExch(&sy->err, 1);
+            go = 0;
+            break;
+          }
+          __nanosleep(64);
+        }
+        __threadfence();
+        s_go = go;
+      }
+      __syncthreads();
+      if (s_go) dluc_panel(S, K, c0, min(DLU_NB, mt), D, P);
+    }
+    if (!dluc_barrier(sy, G)) return;
+  }
+}
+
 struct DenseTail {
   int K;                 // trailing block size (0 = none)
   const double *L;       // K x K column-major, strictly lower part
@@ -2705,14 +3031,16 @@ __global__ void __launch_bounds__(BINV_THREADS) batch_inverse_cluster_kernel(
 // triangular solve's epilogue, error_q = max|x - x_old| / (max|x_old| + 1e-16)
 // (hpc_solve.py:169-174) and the scatter of q and the fracture constants
 // (post_matrix_solve, hpc_solve.py:721-761).
-// out = X v for an n x n row-major X (L2-resident) and v in shared memory:
+// out = X v for rows x n of a row-major X (L2-resident) with n columns and v
+// in shared memory (binv_gemv: the square case):
 // each warp takes four rows at a time, its lanes split the columns, eight
 // independent loads in flight per lane.
-__device__ __forceinline__ void binv_gemv(const double *__restrict__ X, int n, const double *v, double *out) {
+__device__ __forceinline__ void binv_gemv_rows(const double *__restrict__ X, int rows, int n, const double *v,
+                                               double *out) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = BINV_SOLVE_THREADS / 32;
-  for (int i0 = warp * 4; i0 < n; i0 += nw * 4) {
+  for (int i0 = warp * 4; i0 < rows; i0 += nw * 4) {
     const double *X0 = X + (size_t)i0 * n;
-    const bool h1 = i0 + 1 < n, h2 = i0 + 2 < n, h3 = i0 + 3 < n;
+    const bool h1 = i0 + 1 < rows, h2 = i0 + 2 < rows, h3 = i0 + 3 < rows;
     const double *X1 = h1 ? X0 + n : X0, *X2 = h2 ? X0 + 2 * (size_t)n : X0, *X3 = h3 ? X0 + 3 * (size_t)n : X0;
     double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0, b0 = 0.0, b1 = 0.0, b2 = 0.0, b3 = 0.0;
     int j = lane;
@@ -2745,6 +3073,10 @@ __device__ __forceinline__ void binv_gemv(const double *__restrict__ X, int n, c
       if (h3) out[i0 + 3] = s3;
     }
   }
+}
+
+__device__ __forceinline__ void binv_gemv(const double *__restrict__ X, int n, const double *v, double *out) {
+  binv_gemv_rows(X, n, n, v, out);
 }
 
 __global__ void __launch_bounds__(BINV_SOLVE_THREADS) batch_winv_solve_kernel(
@@ -2810,6 +3142,115 @@ __global__ void __launch_bounds__(BINV_SOLVE_THREADS) batch_winv_solve_kernel(
     st->error_q = a / (bb + 1e-16);
     st->n_refined += 1;
   }
+}
+
+// The same solve for a realization with many unknowns, spread over a
+// cluster of BINV_CLUSTER CTAs: CTA c computes the rows [c rpc, (c+1) rpc) of
+// x0 = X b, of the residual and of the correction X r; x0 and the residual
+// are gathered from every CTA's shared memory (distributed shared memory)
+// between the passes, and error_q is the maximum of the CTAs' partial maxima.
+// Every CTA takes the same exits (the loop state it reads is written by other
+// kernels only) and the same four cluster barriers:
+//   1. every CTA's rows of x0 are in its xp;
+//   2. every CTA's residual rows are in its rp and every copy of x0 is taken
+//      (so xp may take the correction);
+//   3. every CTA's partial maxima are written;
+//   4. CTA 0 has read them (no CTA leaves while its shared memory is read).
+__global__ void __launch_bounds__(BINV_SOLVE_THREADS) batch_winv_solve_cluster_kernel(
+    Net net, const int *__restrict__ big, const int *__restrict__ roff, const long long *__restrict__ xoff,
+    const double *__restrict__ Xall, const int *__restrict__ ptr, const int *__restrict__ col,
+    const double *__restrict__ vals) {
+  cg::cluster_group cluster = cg::this_cluster();
+  const int crank = (int)cluster.block_rank();
+  const int r = big[blockIdx.x / BINV_CLUSTER];
+  SolveState *st = net.st + r;
+  if (st->done) return;
+  if (crank == 0 && threadIdx.x == 0) st->nit += 1;
+  if (!st->solve_q) return;  // uniform: solve_q is written only by reduce_kernel
+  const int row0 = roff[r], n = roff[r + 1] - row0;
+  const int rpc = (n + BINV_CLUSTER - 1) / BINV_CLUSTER;
+  const int my0 = min(n, crank * rpc), my1 = min(n, my0 + rpc), mine = my1 - my0;
+  const double *X = Xall + xoff[r] + (size_t)my0 * n;  // this CTA's rows
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double *b = reinterpret_cast<double *>(smem_raw);  // n: b, later the whole residual
+  double *x0 = b + n;                                // n: the whole x0
+  double *xp = x0 + n;                               // rpc: this CTA's rows of x0, later of X r
+  double *rp = xp + rpc;                             // rpc: this CTA's rows of the residual
+  __shared__ double s_d[BINV_SOLVE_THREADS / 32], s_o[BINV_SOLVE_THREADS / 32];
+  __shared__ double s_md, s_mo;
+  for (int i = threadIdx.x; i < n; i += BINV_SOLVE_THREADS) b[i] = net.bvec[row0 + i];
+  __syncthreads();
+  binv_gemv_rows(X, mine, n, b, xp);
+  cluster.sync();  // 1
+  for (int i = threadIdx.x; i < n; i += BINV_SOLVE_THREADS) {
+    const int c = i / rpc;
+    x0[i] = *cluster.map_shared_rank(xp + (i - c * rpc), c);
+  }
+  __syncthreads();
+  for (int i = my0 + threadIdx.x; i < my1; i += BINV_SOLVE_THREADS) {
+    double sres = b[i];
+    for (int p = ptr[row0 + i]; p < ptr[row0 + i + 1]; p++) sres = fma(-vals[p], x0[col[p]], sres);
+    rp[i - my0] = sres;
+  }
+  cluster.sync();  // 2
+  for (int i = threadIdx.x; i < n; i += BINV_SOLVE_THREADS) {
+    const int c = i / rpc;
+    b[i] = *cluster.map_shared_rank(rp + (i - c * rpc), c);
+  }
+  __syncthreads();
+  binv_gemv_rows(X, mine, n, b, xp);  // the correction of this CTA's rows
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double md = 0.0, mo = 0.0;
+  for (int i = my0 + threadIdx.x; i < my1; i += BINV_SOLVE_THREADS) {
+    const int c = row0 + i;
+    const double xv = x0[i] + xp[i - my0];
+    const double xo = net.disc[c];
+    double dd = fabs(xv - xo);
+    if (!(dd == dd)) dd = INFINITY;
+    md = fmax(md, dd);
+    mo = fmax(mo, fabs(xo));
+    net.disc[c] = xv;
+    const int d = net.row_de[c];
+    if (d >= 0)
+      net.q[net.de_ids[d]] = xv;
+    else
+      net.constant[net.row_frac[c]] = xv;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    md = fmax(md, __shfl_xor_sync(0xffffffffu, md, o));
+    mo = fmax(mo, __shfl_xor_sync(0xffffffffu, mo, o));
+  }
+  if (lane == 0) {
+    s_d[warp] = md;
+    s_o[warp] = mo;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0, bb = 0.0;
+    for (int k = 0; k < BINV_SOLVE_THREADS / 32; k++) {
+      a = fmax(a, s_d[k]);
+      bb = fmax(bb, s_o[k]);
+    }
+    s_md = a;
+    s_mo = bb;
+  }
+  cluster.sync();  // 3
+  if (crank == 0 && threadIdx.x == 0) {
+    double a = 0.0, bb = 0.0;
+    for (int c = 0; c < BINV_CLUSTER; c++) {
+      a = fmax(a, *cluster.map_shared_rank(&s_md, c));
+      bb = fmax(bb, *cluster.map_shared_rank(&s_mo, c));
+    }
+    st->error_q = a / (bb + 1e-16);
+    st->n_refined += 1;
+  }
+  cluster.sync();  // 4
+}
+
+static size_t binv_solve_cluster_smem(int n) {
+  const int rpc = (n + BINV_CLUSTER - 1) / BINV_CLUSTER;
+  return sizeof(double) * (2 * (size_t)n + 2 * (size_t)rpc);
 }
 
 __global__ void transpose_ld_kernel(const double *__restrict__ in, int ldi, int rows, int cols,
@@ -3149,13 +3590,177 @@ static void set_error(const std::string &s) { g_last_error = s; }
     }                                                                                               \
   } while (0)
 
-// Device buffer that keeps its allocation when it is re-filled with no more
-// elements than it holds (cudaFree synchronises the device, so repeated
-// solves on one handle should not reallocate).
 // Host milliseconds spent in device allocation and release on this thread
 // (reported per solve as ms_alloc).
 static thread_local double g_alloc_ms = 0.0;
 
+// ------------------------------------------------------------------------
+// Device memory cache shared by every handle of the process.
+//
+// cudaMalloc and cudaFree of the large buffers (an explicit inverse of
+// hundreds of MB, the pair tables) cost milliseconds each, and cudaFree waits
+// for the whole device; a one-call solve that creates and destroys a handle
+// would pay that every call.  Released blocks are therefore kept and handed
+// to later buffers of any handle:
+//   * a block is released while the releasing thread has a handle's stream
+//     current (PoolStream, set by the entry points), and it is tagged with an
+//     event recorded on that stream; a later user waits for the event on its
+//     own current stream (cudaStreamWaitEvent) before touching the block, so
+//     reuse is ordered after every use of the earlier owner;
+//   * without a current stream a block is freed and allocated the plain way
+//     (cudaFree's device-wide wait keeps that safe);
+//   * a request takes the smallest cached block of at least its size and at
+//     most twice it (plus 1 MiB), and blocks are allocated in 256-byte steps;
+//   * the cache holds at most ANDFN_B200_POOL_MB MiB per device (default
+//     8192, 0 turns it off); a block that would exceed it is freed, and a
+//     failed cudaMalloc frees every cached block of the device and retries;
+//   * andfn_b200_release_cached_memory() returns every cached block.
+// ------------------------------------------------------------------------
+static thread_local cudaStream_t g_pool_stream = nullptr;
+static thread_local bool g_pool_stream_set = false;
+
+struct PoolStream {
+  cudaStream_t prev;
+  bool prev_set;
+  explicit PoolStream(cudaStream_t s) : prev(g_pool_stream), prev_set(g_pool_stream_set) {
+    g_pool_stream = s;
+    g_pool_stream_set = true;
+  }
+  ~PoolStream() {
+    g_pool_stream = prev;
+    g_pool_stream_set = prev_set;
+  }
+};
+
+struct PoolBlock {
+  void *p;
+  size_t bytes;
+  cudaEvent_t ev;
+};
+
+struct DevicePool {
+  std::mutex m;
+  std::multimap<size_t, PoolBlock> free_blocks[64];  // by device
+  size_t held[64] = {};
+  std::vector<cudaEvent_t> spare_events;
+  int64_t hits = 0, misses = 0;
+};
+
+static DevicePool &device_pool() {
+  static DevicePool *pool = new DevicePool();  // never destroyed: the driver may be gone at exit
+  return *pool;
+}
+
+static size_t pool_cap_bytes() {
+  static const size_t cap = [] {
+    long long mb = 8192;
+    if (const char *e = getenv("ANDFN_B200_POOL_MB")) mb = std::max(0LL, atoll(e));
+    return (size_t)mb << 20;
+  }();
+  return cap;
+}
+
+static size_t pool_round(size_t bytes) { return (bytes + 255) & ~(size_t)255; }
+
+// Frees every cached block of device dev (waiting for each block's event).
+static void pool_flush_device(DevicePool &P, int dev) {
+  for (auto &kv : P.free_blocks[dev]) {
+    if (kv.second.ev) {
+      cudaEventSynchronize(kv.second.ev);
+      P.spare_events.push_back(kv.second.ev);
+    }
+    cudaFree(kv.second.p);
+  }
+  P.free_blocks[dev].clear();
+  P.held[dev] = 0;
+}
+
+// The cache is used only with a current stream that is not being captured
+// into a graph (an event wait there would tie the graph to this moment).
+static bool pool_usable() {
+  if (!g_pool_stream_set || pool_cap_bytes() == 0) return false;
+  if (!g_pool_stream) return true;  // idle: the handle's stream has been synchronised
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(g_pool_stream, &cs) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return cs == cudaStreamCaptureStatusNone;
+}
+
+static cudaError_t pool_alloc(void **out, size_t bytes) {
+  bytes = pool_round(bytes);
+  int dev = 0;
+  cudaGetDevice(&dev);
+  DevicePool &P = device_pool();
+  if (dev >= 0 && dev < 64 && pool_usable()) {
+    std::lock_guard<std::mutex> lk(P.m);
+    auto &fb = P.free_blocks[dev];
+    auto it = fb.lower_bound(bytes);
+    if (it != fb.end() && it->first <= 2 * bytes + ((size_t)1 << 20)) {
+      PoolBlock b = it->second;
+      fb.erase(it);
+      P.held[dev] -= b.bytes;
+      if (b.ev) {
+        if (g_pool_stream)
+          cudaStreamWaitEvent(g_pool_stream, b.ev, 0);
+        else
+          cudaEventSynchronize(b.ev);
+        P.spare_events.push_back(b.ev);
+      }
+      *out = b.p;
+      P.hits++;
+      return cudaSuccess;
+    }
+    P.misses++;
+  }
+  cudaError_t e = cudaMalloc(out, bytes);
+  if (e == cudaErrorMemoryAllocation && dev >= 0 && dev < 64) {
+    cudaGetLastError();
+    {
+      std::lock_guard<std::mutex> lk(P.m);
+      pool_flush_device(P, dev);
+    }
+    e = cudaMalloc(out, bytes);
+  }
+  return e;
+}
+
+static void pool_release(void *p, size_t bytes) {
+  bytes = pool_round(bytes);
+  int dev = 0;
+  cudaGetDevice(&dev);
+  DevicePool &P = device_pool();
+  if (dev >= 0 && dev < 64 && pool_usable()) {
+    std::lock_guard<std::mutex> lk(P.m);
+    if (P.held[dev] + bytes <= pool_cap_bytes()) {
+      if (!g_pool_stream) {  // idle: nothing in flight uses the block
+        P.free_blocks[dev].emplace(bytes, PoolBlock{p, bytes, nullptr});
+        P.held[dev] += bytes;
+        return;
+      }
+      cudaEvent_t ev = nullptr;
+      if (!P.spare_events.empty()) {
+        ev = P.spare_events.back();
+        P.spare_events.pop_back();
+      } else if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+        ev = nullptr;
+      }
+      if (ev && cudaEventRecord(ev, g_pool_stream) == cudaSuccess) {
+        P.free_blocks[dev].emplace(bytes, PoolBlock{p, bytes, ev});
+        P.held[dev] += bytes;
+        return;
+      }
+      cudaGetLastError();
+      if (ev) P.spare_events.push_back(ev);
+    }
+  }
+  cudaFree(p);
+}
+
+// Device buffer that keeps its allocation when it is re-filled with no more
+// elements than it holds; its blocks come from, and go back to, the device
+// memory cache above.
 template <class T>
 struct DBuf {
   T *p = nullptr;
@@ -3168,14 +3773,20 @@ struct DBuf {
     if (count == 0) return cudaSuccess;
     cap = count;
     const auto t0 = std::chrono::steady_clock::now();
-    const cudaError_t e = cudaMalloc(&p, sizeof(T) * count);
+    void *q = nullptr;
+    const cudaError_t e = pool_alloc(&q, sizeof(T) * count);
+    p = static_cast<T *>(q);
+    if (e != cudaSuccess) {
+      p = nullptr;
+      cap = 0;
+    }
     g_alloc_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return e;
   }
   void release() {
     if (p) {
       const auto t0 = std::chrono::steady_clock::now();
-      cudaFree(p);
+      pool_release(p, sizeof(T) * cap);
       g_alloc_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     }
     p = nullptr;
@@ -3291,6 +3902,7 @@ struct AndfnHandle {
   DBuf<double> tail_l, tail_uinv, tail_w;
   DBuf<int> dlu_i;  // device dense-LU scratch
   DBuf<double> dlu_d;
+  DBuf<DluSync> dlu_sync;  // barrier state of the one-launch dense LU
   // explicit inverse of a single network's system (pivot order, rows padded
   // to winv_ldw), the system's CSR pattern and the solve's work arrays
   DBuf<double> winv, winv_t, wx0, wr;
@@ -3310,6 +3922,10 @@ struct AndfnHandle {
   DBuf<long long> binv_off;
   DBuf<int> binv_order, binv_roff, bcsr_ptr, bcsr_col, bsing, binv_small, binv_big;
   int binv_maxn = 0, binv_nsmall = 0, binv_nbig = 0, binv_smem_n = 0, binv_bign = 0;
+  // realizations (the largest, a prefix of binv_order) whose per-iteration
+  // solve runs on a cluster of CTAs, and binv_order on the host
+  int binv_ncsolve = 0;
+  std::vector<int> binv_order_h;
   double dense_frac = 0.15;  // ordering: dense tail once the minimum degree reaches this fraction
   bool bcsr_built = false;
   DBuf<int> pinv, qcol;
@@ -4185,7 +4801,27 @@ static int gpu_dense_lu(AndfnHandle *H, LuFactors &F, bool want_w) {
   DluScratch D{ib, H->dlu_d.p, ib + K, ib + K + 2 * DLU_NB, ib + K + 4 * DLU_NB, ib + K + 4 * DLU_NB + 1};
   CK(cudaMemsetAsync(D.flag, 0, sizeof(int), s));
   double *S = H->tail_l.p;
-  for (int j0 = 0; j0 < K; j0 += DLU_NB) {
+  // one cooperative launch when the panel fits one CTA's shared memory and
+  // every SM can hold a CTA (ANDFN_B200_DLU_COOP=0: the three launches a panel)
+  bool coop = sizeof(double) * (DLU_NB + 1) * (size_t)K <= DLU_SMEM_MAX;
+  if (const char *e = getenv("ANDFN_B200_DLU_COOP")) coop = coop && atoi(e) != 0;
+  if (coop) {
+    const size_t sm = dluc_smem(K);
+    CK(cudaFuncSetAttribute(dlu_coop_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dlu_coop_kernel, DLUC_THREADS, sm));
+    coop = per_sm >= 1;
+    if (coop) {
+      if (H->dlu_sync.cap < 1) CK(H->dlu_sync.alloc(1));
+      CK(cudaMemsetAsync(H->dlu_sync.p, 0, sizeof(DluSync), s));
+      DluSync *sy = H->dlu_sync.p;
+      int Kv = K;
+      void *args[] = {(void *)&S, (void *)&Kv, (void *)&D, (void *)&sy};
+      CK(cudaLaunchCooperativeKernel((void *)dlu_coop_kernel, dim3(H->num_sms), dim3(DLUC_THREADS), args, sm, s));
+      H->launches += 1;
+    }
+  }
+  for (int j0 = 0; j0 < K && !coop; j0 += DLU_NB) {
     const int nb = std::min(DLU_NB, K - j0), m = K - j0, mt = m - nb;
     const size_t sm = sizeof(double) * (size_t)m * (DLU_NB + 1);
     const int use_smem = sm <= DLU_SMEM_MAX;
@@ -4195,15 +4831,18 @@ static int gpu_dense_lu(AndfnHandle *H, LuFactors &F, bool want_w) {
       dlu_panel_kernel<false><<<1, DLU_THREADS, 0, s>>>(S, K, j0, nb, D);
     if (K > nb) dlu_update_kernel<<<(K - nb + 7) / 8, 256, 0, s>>>(S, K, j0, nb, D);
     if (mt > 0) dlu_gemm_kernel<<<dim3((mt + 63) / 64, (mt + 63) / 64), 256, 0, s>>>(S, K, j0, nb);
+    H->launches += 1 + (K > nb) + (mt > 0);
   }
   CK(cudaGetLastError());
   CK(H->tail_uinv.alloc((size_t)K));
   recip_kernel<<<(K + 255) / 256, 256, 0, s>>>(D.diag, H->tail_uinv.p, K);
   std::vector<int> piv(K), flag(1);
   std::vector<double> dg(K);
+  DluSync syh = {};
   CK(cudaMemcpyAsync(piv.data(), D.piv, sizeof(int) * K, cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(dg.data(), D.diag, sizeof(double) * K, cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(flag.data(), D.flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+  if (coop) CK(cudaMemcpyAsync(&syh, H->dlu_sync.p, sizeof(DluSync), cudaMemcpyDeviceToHost, s));
   g_d2h_bytes += (int64_t)(12 * K + 4);
   if (!H->dlu_ev) CK(cudaEventCreateWithFlags(&H->dlu_ev, cudaEventDisableTiming));
   CK(cudaEventRecord(H->dlu_ev, s));
@@ -4212,6 +4851,10 @@ static int gpu_dense_lu(AndfnHandle *H, LuFactors &F, bool want_w) {
     if (rc) return rc;
   }
   CK(cudaEventSynchronize(H->dlu_ev));
+  if (syh.err) {
+    set_error("dense LU of the Schur complement: a grid barrier wait ran out");
+    return ANDFN_CUDA_ERROR;
+  }
   if (flag[0]) return 3;
   return sparse_lu_finish(F, piv, dg);
 }
@@ -4296,6 +4939,7 @@ static int factor_batch_inverse(AndfnHandle *H) {
     CK(upload(H->bcsr_ptr, ptr, s));
     CK(upload(H->bcsr_col, col, s));
     CK(upload(H->binv_order, order, s));
+    H->binv_order_h = order;
     CK(upload(H->binv_roff, roff, s));
     CK(upload(H->binv_off, off, s));
     CK(H->binv.alloc((size_t)std::max(1LL, tot)));
@@ -4324,6 +4968,16 @@ static int factor_batch_inverse(AndfnHandle *H) {
     H->binv_nbig = (int)big.size();
     H->binv_smem_n = smem_n;
     H->binv_bign = bign;
+    // the per-iteration solve of a realization with at least
+    // ANDFN_B200_BINV_CLUSTER_SOLVE_N (default 128) unknowns is spread over
+    // a cluster: its two products with X then take 1/8 of the time and the
+    // largest realizations, which set the pace of a batch's last iterations,
+    // are not bound by one SM's share of L2 bandwidth
+    int csolve_n = 128;
+    if (const char *e = getenv("ANDFN_B200_BINV_CLUSTER_SOLVE_N")) csolve_n = std::max(1, atoi(e));
+    int nc = 0;
+    while (nc < R && H->sys[order[nc]].n >= csolve_n && H->sys[order[nc]].n >= BINV_CLUSTER) nc++;
+    H->binv_ncsolve = nc;
     H->bcsr_built = true;
   }
   const int maxn = H->binv_maxn;
@@ -4332,6 +4986,9 @@ static int factor_batch_inverse(AndfnHandle *H) {
   CK(cudaFuncSetAttribute(batch_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   CK(cudaFuncSetAttribute(batch_winv_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)(24 * (size_t)maxn)));
+  if (H->binv_ncsolve > 0)
+    CK(cudaFuncSetAttribute(batch_winv_solve_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)binv_solve_cluster_smem(maxn)));
   if (H->binv_nbig > 0) {
     const size_t csmem = binv_cluster_smem(H->binv_bign);
     CK(cudaFuncSetAttribute(batch_inverse_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csmem));
@@ -4708,9 +5365,35 @@ static void launch_winv_solve(AndfnHandle *H, const Net &net, cudaStream_t s, co
 static void launch_trisolve(AndfnHandle *H, cudaStream_t s) {
   Net net = H->net();
   if (H->binv_ready) {
-    batch_winv_solve_kernel<<<H->R, BINV_SOLVE_THREADS, 24 * (size_t)H->binv_maxn, s>>>(
-        net, H->binv_order.p, H->binv_roff.p, H->binv_off.p, H->binv.p, H->bcsr_ptr.p, H->bcsr_col.p,
-        H->d_mvals.p);
+    // binv_order lists the realizations by decreasing size: the first
+    // binv_ncsolve of them are solved by a cluster each, the rest by one CTA
+    const int nc = H->binv_ncsolve;
+    if (nc > 0) {
+      cudaLaunchConfig_t cfg = {};
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = BINV_CLUSTER;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cfg.gridDim = dim3(BINV_CLUSTER * nc);
+      cfg.blockDim = dim3(BINV_SOLVE_THREADS);
+      cfg.dynamicSmemBytes = binv_solve_cluster_smem(H->sys[H->binv_order_h[0]].n);
+      cfg.stream = s;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      const cudaError_t ce = cudaLaunchKernelEx(
+          &cfg, batch_winv_solve_cluster_kernel, net, (const int *)H->binv_order.p, (const int *)H->binv_roff.p,
+          (const long long *)H->binv_off.p, (const double *)H->binv.p, (const int *)H->bcsr_ptr.p,
+          (const int *)H->bcsr_col.p, (const double *)H->d_mvals.p);
+      if (ce != cudaSuccess) set_error(std::string("batched cluster solve launch: ") + cudaGetErrorString(ce));
+      H->launches += 1;
+    }
+    if (H->R > nc) {
+      batch_winv_solve_kernel<<<H->R - nc, BINV_SOLVE_THREADS, 24 * (size_t)H->binv_maxn, s>>>(
+          net, H->binv_order.p + nc, H->binv_roff.p, H->binv_off.p, H->binv.p, H->bcsr_ptr.p, H->bcsr_col.p,
+          H->d_mvals.p);
+      H->launches += 1;
+    }
     const cudaError_t le = cudaGetLastError();
     if (le != cudaSuccess) set_error(std::string("batched explicit-inverse solve launch: ") + cudaGetErrorString(le));
     return;
@@ -5737,6 +6420,7 @@ int andfn_b200_batch_create(AndfnHandle **out, int64_t R, void *const *frac_recs
     set_error("cudaStreamCreate failed");
     return ANDFN_CUDA_ERROR;
   }
+  PoolStream pool_scope(H->stream);
   H->L = *layout;
   if (const char *v = getenv("ANDFN_B200_SOLVE_THREADS")) {
     int t = atoi(v);
@@ -5769,6 +6453,7 @@ int andfn_b200_upload_state(AndfnHandle *H, const void *frac_recs, const void *e
   }
   H->have_solution = false;
   cudaSetDevice(H->device);
+  PoolStream pool_scope(H->stream);
   const char *E = (const char *)elem_recs;
   const char *F = (const char *)frac_recs;
   const AndfnLayout &L = H->L;
@@ -5805,6 +6490,7 @@ int andfn_b200_upload_state(AndfnHandle *H, const void *frac_recs, const void *e
 int andfn_b200_reset_state(AndfnHandle *H) {
   if (!H) return ANDFN_BAD_INPUT;
   cudaSetDevice(H->device);
+  PoolStream pool_scope(H->stream);
   H->have_solution = false;
   int rc = reset_impl(H);
   if (rc) return rc;
@@ -5815,6 +6501,7 @@ int andfn_b200_reset_state(AndfnHandle *H) {
 int andfn_b200_batch_run(AndfnHandle *H, const AndfnConstants *constants, AndfnSolveStats *stats) {
   if (!H || !constants) return ANDFN_BAD_INPUT;
   cudaSetDevice(H->device);
+  PoolStream pool_scope(H->stream);
   return run_impl(H, constants, stats);
 }
 
@@ -5825,18 +6512,21 @@ int andfn_b200_run(AndfnHandle *H, const AndfnConstants *constants, AndfnSolveSt
     return ANDFN_BAD_INPUT;
   }
   cudaSetDevice(H->device);
+  PoolStream pool_scope(H->stream);
   return run_impl(H, constants, stats);
 }
 
 int andfn_b200_batch_download(AndfnHandle *H, void *const *frac_recs, void *const *elem_recs) {
   if (!H || !frac_recs || !elem_recs) return ANDFN_BAD_INPUT;
   cudaSetDevice(H->device);
+  PoolStream pool_scope(H->stream);
   return download_impl(H, (char *const *)frac_recs, (char *const *)elem_recs);
 }
 
 int andfn_b200_download(AndfnHandle *H, void *frac_recs, void *elem_recs) {
   if (!H || !frac_recs || !elem_recs || H->R != 1) return ANDFN_BAD_INPUT;
   cudaSetDevice(H->device);
+  PoolStream pool_scope(H->stream);
   char *F[1] = {(char *)frac_recs};
   char *E[1] = {(char *)elem_recs};
   return download_impl(H, F, E);
@@ -5845,6 +6535,7 @@ int andfn_b200_download(AndfnHandle *H, void *frac_recs, void *elem_recs) {
 int andfn_b200_eval_heads(AndfnHandle *H, const int64_t *frac, const double *z, int64_t npts, double *out) {
   if (!H || (npts > 0 && (!frac || !z || !out))) return ANDFN_BAD_INPUT;
   cudaSetDevice(H->device);
+  PoolStream pool_scope(H->stream);
   return eval_points_impl(H, 0, frac, z, npts, nullptr, out);
 }
 
@@ -5852,24 +6543,28 @@ int andfn_b200_batch_eval_heads(AndfnHandle *H, int64_t r, const int64_t *frac, 
                                 double *out) {
   if (!H || (npts > 0 && (!frac || !z || !out))) return ANDFN_BAD_INPUT;
   cudaSetDevice(H->device);
+  PoolStream pool_scope(H->stream);
   return eval_points_impl(H, r, frac, z, npts, nullptr, out);
 }
 
 int andfn_b200_eval_omega(AndfnHandle *H, const int64_t *frac, const double *z, int64_t npts, double *out) {
   if (!H || (npts > 0 && (!frac || !z || !out))) return ANDFN_BAD_INPUT;
   cudaSetDevice(H->device);
+  PoolStream pool_scope(H->stream);
   return eval_points_impl(H, 0, frac, z, npts, out, nullptr);
 }
 
 int andfn_b200_eval_w(AndfnHandle *H, const int64_t *frac, const double *z, int64_t npts, double *out) {
   if (!H || (npts > 0 && (!frac || !z || !out))) return ANDFN_BAD_INPUT;
   cudaSetDevice(H->device);
+  PoolStream pool_scope(H->stream);
   return eval_w_impl(H, frac, reinterpret_cast<const cd *>(z), npts, reinterpret_cast<cd *>(out));
 }
 
 int andfn_b200_eval_w_object(AndfnHandle *H, const int64_t *frac, const double *z, int64_t npts, double *out) {
   if (!H || (npts > 0 && (!frac || !z || !out))) return ANDFN_BAD_INPUT;
   cudaSetDevice(H->device);
+  PoolStream pool_scope(H->stream);
   return eval_w_object_impl(H, frac, reinterpret_cast<const cd *>(z), npts, reinterpret_cast<cd *>(out));
 }
 
@@ -5881,6 +6576,7 @@ int andfn_b200_track(AndfnHandle *H, const void *frac_recs, int64_t nf, const do
                            !out_frac || !out_n || !out_elem || !out_status)))
     return ANDFN_BAD_INPUT;
   cudaSetDevice(H->device);
+  PoolStream pool_scope(H->stream);
   return track_impl(H, frac_recs, nf, aperture, npart, frac, reinterpret_cast<const cd *>(z), elevation, ds,
                     max_length, backward, cap, reinterpret_cast<cd *>(out_z), out_v, out_seg, out_frac, out_n,
                     out_elem, out_status);
@@ -5890,6 +6586,7 @@ void andfn_b200_destroy(AndfnHandle *H) {
   if (!H) return;
   cudaSetDevice(H->device);
   cudaStreamSynchronize(H->stream);
+  PoolStream pool_scope(nullptr);  // the stream is idle: blocks go back to the cache with no event
   delete H;
 }
 
@@ -5945,6 +6642,29 @@ int andfn_b200_fp64_peak(int32_t device, double *tflops) {
   return 0;
 }
 
+void andfn_b200_release_cached_memory(void) {
+  DevicePool &P = device_pool();
+  std::lock_guard<std::mutex> lk(P.m);
+  int cur = 0;
+  cudaGetDevice(&cur);
+  for (int d = 0; d < 64; d++) {
+    if (P.free_blocks[d].empty()) continue;
+    cudaSetDevice(d);
+    pool_flush_device(P, d);
+  }
+  cudaSetDevice(cur);
+}
+
+int andfn_b200_cached_memory(int32_t device, int64_t *bytes, int64_t *hits, int64_t *misses) {
+  if (device < 0 || device >= 64) return ANDFN_BAD_INPUT;
+  DevicePool &P = device_pool();
+  std::lock_guard<std::mutex> lk(P.m);
+  if (bytes) *bytes = (int64_t)P.held[device];
+  if (hits) *hits = P.hits;
+  if (misses) *misses = P.misses;
+  return 0;
+}
+
 int andfn_b200_batch_solve(int64_t R, void *const *frac_recs, const int64_t *nf, void *const *elem_recs,
                            const int64_t *ne, const AndfnLayout *layout, int64_t discharge_int,
                            const AndfnConstants *constants, AndfnSolveStats *stats) {
@@ -5955,6 +6675,7 @@ int andfn_b200_batch_solve(int64_t R, void *const *frac_recs, const int64_t *nf,
   int rc = andfn_b200_batch_create(&H, R, frac_recs, nf, elem_recs, ne, layout, discharge_int, -1);
   if (rc) return rc;
   H->tune_sweep = false;  // a cached choice of an earlier handle, or the per-item form
+  PoolStream pool_scope(H->stream);
   const double ms_up = ms_since(t0);
   rc = run_impl(H, constants, nullptr);
   double ms_down = 0;
@@ -6056,6 +6777,7 @@ extern "C" int andfn_b200_eval_heads_noalloc(AndfnHandle *H, const int64_t *frac
     return ANDFN_NO_DEVICE;
   }
   CK(cudaSetDevice(H->device));
+  PoolStream pool_scope(H->stream);
   NoAllocScratch *s = g_noalloc_ptr[H->device];
   if (!s) {  // first call on this device: look the array up once
     void *p = nullptr;
@@ -7659,12 +8381,14 @@ extern "C" {
 int andfn_b200_set_transmissivity(AndfnHandle *H, const double *t) {
   if (!H || !t) return ANDFN_BAD_INPUT;
   CK(cudaSetDevice(H->device));
+  PoolStream pool_scope(H->stream);
   return set_transmissivity_impl(H, t);
 }
 
 int andfn_b200_state_device(AndfnHandle *H, double *coef, int64_t mco, double *q, double *constant) {
   if (!H || mco < 0 || (mco > 0 && !coef) || !q || !constant) return ANDFN_BAD_INPUT;
   CK(cudaSetDevice(H->device));
+  PoolStream pool_scope(H->stream);
   cudaStream_t s = H->stream;
   const int64_t w = std::min<int64_t>(mco, H->MC);
   if (mco > 0) {
@@ -7687,6 +8411,7 @@ int andfn_b200_heads_device(AndfnHandle *H, const int64_t *frac, const double *z
   }
   if (npts == 0) return 0;
   CK(cudaSetDevice(H->device));
+  PoolStream pool_scope(H->stream);
   heads_dev_kernel<<<(unsigned)((npts + 127) / 128), 128, 0, H->stream>>>(H->net(), frac, (const cd *)z, (int)npts,
                                                                            out);
   CK(cudaGetLastError());
@@ -7705,6 +8430,7 @@ int andfn_b200_heads_vjp(AndfnHandle *H, const int64_t *frac, const double *z, i
   }
   if (npts == 0) return 0;
   CK(cudaSetDevice(H->device));
+  PoolStream pool_scope(H->stream);
   heads_vjp_kernel<<<(unsigned)((npts + 127) / 128), 128, 0, H->stream>>>(H->net(), frac, (const cd *)z, (int)npts,
                                                                            gh, gcoef, (int)mco, gq, gC, glogt);
   CK(cudaGetLastError());
@@ -7716,6 +8442,7 @@ int andfn_b200_adjoint(AndfnHandle *H, const double *gcoef, int64_t mco, const d
                        double tol, int64_t max_iterations, double *glogt, AndfnAdjointStats *stats) {
   if (!H) return ANDFN_BAD_INPUT;
   CK(cudaSetDevice(H->device));
+  PoolStream pool_scope(H->stream);
   return adjoint_impl(H, gcoef, mco, gq, gC, tol, max_iterations, glogt, stats);
 }
 
@@ -7801,6 +8528,7 @@ extern "C" int andfn_b200_bc_residual(AndfnHandle *H, double *elem_res, double *
     return ANDFN_BAD_INPUT;
   }
   CK(cudaSetDevice(H->device));
+  PoolStream pool_scope(H->stream);
   const HostNet &h = H->h;
   const int ne = (int)H->ne, nf = (int)H->nf;
   cudaStream_t s = H->stream;

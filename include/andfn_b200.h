@@ -234,6 +234,18 @@ int andfn_b200_kernel_times(AndfnHandle *h, double *ms, int64_t *launches, int n
  * the evaluation kernels' roofline). */
 int andfn_b200_fp64_peak(int32_t device, double *tflops);
 
+/* Device memory cache (no reference counterpart).  Device buffers released
+ * by handles (andfn_b200_destroy, or a buffer that grows) are kept by the
+ * library and reused by later handles of the process, so a one-call solve
+ * does not pay cudaMalloc / cudaFree for its large buffers every call.  The
+ * cache holds at most ANDFN_B200_POOL_MB MiB per device (environment,
+ * default 8192; 0 turns it off) and gives its memory back when an
+ * allocation fails.  release_cached_memory() frees every cached block of
+ * every device; cached_memory() reports the bytes held on `device` and the
+ * cache's hits and misses since the process started. */
+void andfn_b200_release_cached_memory(void);
+int andfn_b200_cached_memory(int32_t device, int64_t *bytes, int64_t *hits, int64_t *misses);
+
 /* Heads like andfn_b200_eval_heads, without allocating any memory (no
  * reference counterpart: the reference evaluates heads on the host).
  * For callers that cannot allocate device memory during a call -- a process

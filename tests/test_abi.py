@@ -75,6 +75,19 @@ def test_batch_inputs_rejected_before_device_use():
     assert L.andfn_b200_realizations(None) == 0
 
 
+def test_memory_cache_accessors_without_device_use():
+    """The device memory cache's accessors touch no device: an empty cache
+    reports zero bytes, a device index out of range is rejected."""
+    from andfn_b200 import _ffi
+    import andfn_b200
+    L = _ffi.lib()
+    b = ctypes.c_int64(-1)
+    assert L.andfn_b200_cached_memory(64, ctypes.byref(b), None, None) == 11
+    assert L.andfn_b200_cached_memory(-1, ctypes.byref(b), None, None) == 11
+    cm = andfn_b200.cached_memory(0)
+    assert cm["bytes"] >= 0 and cm["hits"] >= 0 and cm["misses"] >= 0
+
+
 def test_batch_records_must_share_dtypes():
     import andfn_b200
     from andfn_b200.records import element_dtype

@@ -176,3 +176,30 @@ def test_batch_with_a_singular_realization_raises():
     with pytest.raises(_ffi.AndfnError) as ei:
         andfn_b200.solve_batch([(F.copy(), E.copy()) for F, E in recs], 50, c)
     assert ei.value.code == 3 and "realization 1" in str(ei.value), str(ei.value)
+
+
+def test_cluster_solve_of_large_realizations_is_bitwise_the_single_cta_solve(monkeypatch):
+    """Realizations with at least ANDFN_B200_BINV_CLUSTER_SOLVE_N unknowns
+    solve on an 8-CTA cluster each (rows split over the CTAs, x0 and the
+    residual exchanged through distributed shared memory); every row's sums
+    run in the same order as in the one-CTA solve, so the results are the
+    same bit for bit."""
+    import andfn_b200
+    from andfn_b200 import network as nw
+    from andfn_b200.records import default_constants
+    recs = nw.to_records_batch([nw.batch_realization(2000 + i) for i in range(12)])
+    c = default_constants(MAX_ITERATIONS=120, MAX_ERROR=1e-8, MAX_NCOEF=15)
+    out = {}
+    for thr in ("1000000", "64"):
+        monkeypatch.setenv("ANDFN_B200_BINV_CLUSTER_SOLVE_N", thr)
+        batch = [(F.copy(), E.copy()) for F, E in recs]
+        st = andfn_b200.solve_batch(batch, 50, c)
+        out[thr] = (batch, st)
+    (b1, s1), (b2, s2) = out["1000000"], out["64"]
+    # the clustered run launches one more kernel per iteration
+    assert s2[0]["gpu_launches"] > s1[0]["gpu_launches"], (s1[0]["gpu_launches"], s2[0]["gpu_launches"])
+    for r in range(len(recs)):
+        assert s1[r]["iterations"] == s2[r]["iterations"] and s1[r]["status"] == s2[r]["status"], r
+        for name in ("coef", "q", "error", "error_coef", "dpsi_corr", "ncoef", "nint"):
+            assert np.array_equal(b1[r][1][name], b2[r][1][name], equal_nan=True), (r, name)
+        assert np.array_equal(b1[r][0]["constant"], b2[r][0]["constant"]), r
