@@ -138,6 +138,10 @@ struct Net {
   const struct TriDesc *tri; // [R]
   // known part of the head vector [N] (wells with a prescribed discharge), or null
   const double *bknown;
+  // DFT bases of the Cauchy-integral fits: element e's basis starts at
+  // dft_tab + dft_off[e], entry (k, j) at k * MC + j = exp(-i theta_k)^j
+  const cd *dft_tab;
+  const int *dft_off;
 };
 
 // ------------------------------------------------------------------------
@@ -561,6 +565,8 @@ __device__ __forceinline__ void sweep_table_item(const Net &net, const Item it, 
 
 // One CTA per item (the hardware block scheduler hands out the items, which
 // are sorted by estimated cost, largest first).
+// With an active list (batches), CTA i takes item alist[i] while i is below
+// the list's length *acount, and returns otherwise.
 __global__ void __launch_bounds__(EVAL_THREADS) sweep_table_kernel(Net net, const Item *__restrict__ items,
                                                                      const int2 *__restrict__ pts,
                                                                      const Group *__restrict__ groups,
@@ -569,8 +575,15 @@ __global__ void __launch_bounds__(EVAL_THREADS) sweep_table_kernel(Net net, cons
                                                                      const long long *__restrict__ tab_off,
                                                                      const cd *__restrict__ tw,
                                                                      const double *__restrict__ tl,
-                                                                     double *__restrict__ out, int chunk) {
-  sweep_table_item(net, items[blockIdx.x], pts, groups, fpt0, fnp, tab_off, tw, tl, out, chunk);
+                                                                     double *__restrict__ out, int chunk,
+                                                                     const int *__restrict__ alist,
+                                                                     const int *__restrict__ acount) {
+  int i = blockIdx.x;
+  if (alist) {
+    if (i >= *acount) return;
+    i = alist[i];
+  }
+  sweep_table_item(net, items[i], pts, groups, fpt0, fnp, tab_off, tw, tl, out, chunk);
 }
 
 // Persistent form: a grid of a few CTAs per SM takes the items (largest
@@ -583,15 +596,17 @@ __global__ void __launch_bounds__(EVAL_THREADS) sweep_table_queue_kernel(
     Net net, const Item *__restrict__ items, int n_items, const int2 *__restrict__ pts,
     const Group *__restrict__ groups, const int *__restrict__ fpt0, const int *__restrict__ fnp,
     const long long *__restrict__ tab_off, const cd *__restrict__ tw, const double *__restrict__ tl,
-    double *__restrict__ out, int chunk, WorkQueue *q) {
+    double *__restrict__ out, int chunk, WorkQueue *q, const int *__restrict__ alist,
+    const int *__restrict__ acount) {
   __shared__ int s_next;
+  if (alist) n_items = *acount;
   while (true) {
     if (threadIdx.x == 0) s_next = atomicAdd(&q->next, 1);
     __syncthreads();
     const int i = s_next;
     __syncthreads();  // every thread has read s_next before thread 0 fetches again
     if (i >= n_items) break;
-    sweep_table_item(net, items[i], pts, groups, fpt0, fnp, tab_off, tw, tl, out, chunk);
+    sweep_table_item(net, items[alist ? alist[i] : i], pts, groups, fpt0, fnp, tab_off, tw, tl, out, chunk);
   }
   if (threadIdx.x == 0) {
     __threadfence();
@@ -600,6 +615,118 @@ __global__ void __launch_bounds__(EVAL_THREADS) sweep_table_queue_kernel(
       q->done = 0;
       __threadfence();
     }
+  }
+}
+
+// ------------------------------------------------------------------------
+// Active work lists of a batch.  Once realizations finish, their rows, sweep
+// items and elements still occupy the grids of the per-iteration kernels
+// (each CTA or warp returning at entry); in a batch's last iterations, with
+// a few realizations left, those empty launches cost more than the work.
+// The lists below hold, in their original order, the entries of the
+// realizations still running; the kernels take entry alist[i] for i below
+// the list's length.  They are rebuilt at the end of an iteration in which
+// a realization finished (ndone changed), by two launches over chunks of
+// ACT_CHUNK entries: per-chunk counts, then each chunk's prefix (the sum of
+// the counts before it) and an order-preserving scatter.  Launches in which
+// nothing changed return at entry.
+// ------------------------------------------------------------------------
+static constexpr int ACT_CHUNK = 1024;
+static constexpr int ACT_LISTS = 3;  // head-vector rows, sweep items, updated elements
+
+struct ActState {
+  int seen;         // ndone when the lists were last built
+  unsigned arrive;  // CTAs of the scatter launch that have finished
+  int count[ACT_LISTS];
+};
+
+struct ActLists {
+  int n[ACT_LISTS];       // entries of the full lists
+  int chunk0[ACT_LISTS + 1];  // first compaction CTA of each list (chunk0[ACT_LISTS] = grid)
+  int *list[ACT_LISTS];   // active entries (indices into the full list)
+  int *ccnt;              // active entries per chunk, all lists
+  const Item *items;      // the sweep items (list 1's realization lookup)
+  ActState *st;
+};
+
+// the realization of entry i of list l
+__device__ __forceinline__ int act_real(const Net &net, const ActLists &A, int l, int i) {
+  if (l == 0) return net.real_row[i];
+  if (l == 1) return net.real_frac[A.items[i].frac];
+  return net.real_elem[i];
+}
+
+__device__ __forceinline__ void act_locate(const ActLists &A, int &l, int &c) {
+  l = 0;
+  while (l + 1 < ACT_LISTS && (int)blockIdx.x >= A.chunk0[l + 1]) l++;
+  c = (int)blockIdx.x - A.chunk0[l];
+}
+
+__global__ void __launch_bounds__(ACT_CHUNK) act_count_kernel(Net net, ActLists A) {
+  if (A.st->seen == *net.ndone) return;  // uniform: nothing finished since the last build
+  int l, c;
+  act_locate(A, l, c);
+  const int i = c * ACT_CHUNK + threadIdx.x;
+  const bool on = i < A.n[l] && !net.st[act_real(net, A, l, i)].done;
+  const int n = __syncthreads_count(on);
+  if (threadIdx.x == 0) A.ccnt[blockIdx.x] = n;
+}
+
+__global__ void __launch_bounds__(ACT_CHUNK) act_scatter_kernel(Net net, ActLists A) {
+  __shared__ int s_w[ACT_CHUNK / 32];
+  __shared__ int s_pre;
+  const int nd = *net.ndone;
+  if (A.st->seen == nd) return;
+  int l, c;
+  act_locate(A, l, c);
+  // prefix: active entries of this list's chunks before this one
+  int pre = 0;
+  for (int k = A.chunk0[l] + (int)threadIdx.x; k < A.chunk0[l] + c; k += ACT_CHUNK) pre += A.ccnt[k];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int o = 16; o > 0; o >>= 1) pre += __shfl_xor_sync(0xffffffffu, pre, o);
+  if (lane == 0) s_w[warp] = pre;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int w = 0; w < ACT_CHUNK / 32; w++) t += s_w[w];
+    s_pre = t;
+  }
+  __syncthreads();
+  const int base = s_pre;
+  // order-preserving scatter of the chunk's active entries
+  const int i = c * ACT_CHUNK + threadIdx.x;
+  const bool on = i < A.n[l] && !net.st[act_real(net, A, l, i)].done;
+  const unsigned m = __ballot_sync(0xffffffffu, on);
+  if (lane == 0) s_w[warp] = __popc(m);  // thread 0's reads of s_w ended at the barrier above
+  __syncthreads();
+  int wpre = 0;
+  for (int w = 0; w < warp; w++) wpre += s_w[w];
+  if (on) A.list[l][base + wpre + __popc(m & ((1u << lane) - 1u))] = i;
+  const int last_chunk = (A.n[l] + ACT_CHUNK - 1) / ACT_CHUNK - 1;
+  if (c == last_chunk && threadIdx.x == 0) {
+    int t = 0;
+    for (int w = 0; w < ACT_CHUNK / 32; w++) t += s_w[w];
+    A.st->count[l] = base + t;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(&A.st->arrive, 1u) == gridDim.x - 1) {  // the last CTA of the rebuild
+      A.st->arrive = 0;
+      A.st->seen = nd;
+      __threadfence();
+    }
+  }
+}
+
+// The full lists (identity) at the start of a run.
+__global__ void act_init_kernel(ActLists A, int ndone0) {
+  for (int l = 0; l < ACT_LISTS; l++)
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n[l]; i += gridDim.x * blockDim.x) A.list[l][i] = i;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    A.st->seen = ndone0;
+    A.st->arrive = 0;
+    for (int l = 0; l < ACT_LISTS; l++) A.st->count[l] = A.n[l];
   }
 }
 
@@ -636,16 +763,49 @@ __device__ __forceinline__ void dft_lane(const double *v, int n, int type, int j
   if (j == 0) out = mk(out.re / 2, out.im / 2);
 }
 
+// The Cauchy-integral DFT of one lane's coefficient j from the element's
+// basis B (entry (k, j) = exp(-i theta_k)^j, the powers the reference forms
+// by repeated multiplication, hpc_math_functions.py:244-297): the products
+// and sums in the reference's order (a product, then a sum, point by point).
+// Two value sets (the sides of an intersection) share the basis loads.
+template <int SETS>
+__device__ __forceinline__ void dft_basis(const double *v0, const double *v1, int n, const cd *__restrict__ B,
+                                          int MC, int j, bool imag_unit, cd &out0, cd &out1) {
+  double r0 = 0.0, i0 = 0.0, r1 = 0.0, i1 = 0.0;
+  for (int k = 0; k < n; k++) {
+    const cd b = B[(size_t)k * MC + j];
+    r0 = __dadd_rn(r0, __dmul_rn(v0[k], b.re));
+    i0 = __dadd_rn(i0, __dmul_rn(v0[k], b.im));
+    if (SETS == 2) {
+      r1 = __dadd_rn(r1, __dmul_rn(v1[k], b.re));
+      i1 = __dadd_rn(i1, __dmul_rn(v1[k], b.im));
+    }
+  }
+  // coef_j = 2 integral_j / n (real Cauchy integral), 2i integral_j / n
+  // (stream-function Cauchy integral); coef_0 halved
+  if (imag_unit)
+    out0 = mk(-2.0 * i0 / n, 2.0 * r0 / n);
+  else
+    out0 = mk(2.0 * r0 / n, 2.0 * i0 / n);
+  out1 = mk(2.0 * r1 / n, 2.0 * i1 / n);
+  if (j == 0) {
+    out0 = mk(out0.re / 2, out0.im / 2);
+    out1 = mk(out1.re / 2, out1.im / 2);
+  }
+}
+
 __global__ void __launch_bounds__(UPDATE_WARPS * 32) update_kernel(Net net, const int *__restrict__ elist, int nlist,
                                                                     const int *__restrict__ group_of,
                                                                     const Group *__restrict__ groups,
                                                                     const double *__restrict__ vals, int nvmax,
-                                                                    int blend_mode) {
+                                                                    int blend_mode,
+                                                                    const int *__restrict__ ncount = nullptr) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double *v0 = reinterpret_cast<double *>(smem_raw) + (size_t)warp * 2 * nvmax;
   double *v1 = v0 + nvmax;
   const int idx = blockIdx.x * UPDATE_WARPS + warp;
+  if (ncount) nlist = *ncount;  // a batch's active element list: its length on the device
   if (idx >= nlist) return;
   const int e = elist[idx];
   SolveState *st = net.st + net.real_elem[e];
@@ -724,23 +884,23 @@ __global__ void __launch_bounds__(UPDATE_WARPS * 32) update_kernel(Net net, cons
   const int i90 = (int)(m * 0.9);
   double s5 = 0.0, ecoef = 0.0;
   cd c1 = mk(0.0, 0.0), c10 = mk(0.0, 0.0);
+  const cd *B = net.dft_tab + net.dft_off[e];
   for (int j = lane; j < m; j += 32) {
     cd nj;
     if (type == 0) {
       cd a0, a1;
-      dft_lane(v0, n, type, j, false, a0);
-      dft_lane(v1, n, type, j, false, a1);
+      dft_basis<2>(v0, v1, n, B, MC, j, false, a0, a1);
       // Re((t0 c1 - t1 c0) / (t0 + t1)), coef_0 = 0 (hpc_intersection.py:95-102)
       nj = mk((t0 * a1.re - t1 * a0.re) / (t0 + t1), 0.0);
       if (j == 0) nj = mk(0.0, 0.0);
     } else if (type == 3) {
-      cd a;
-      dft_lane(v0, n, type, j, false, a);
+      cd a, unused;
+      dft_basis<1>(v0, v0, n, B, MC, j, false, a, unused);
       nj = mk(-a.re, 0.0);  // hpc_const_head_line.py:72-76
       if (j == 0) nj = mk(0.0, 0.0);
     } else {
-      cd a;
-      dft_lane(v0, n, type, j, true, a);
+      cd a, unused;
+      dft_basis<1>(v0, v0, n, B, MC, j, true, a, unused);
       if (type == 1) {
         nj = mk(-a.re, -a.im);  // hpc_bounding_circle.py:154
       } else if (type == 4) {
@@ -859,24 +1019,23 @@ __global__ void blend2_kernel(Net net) {
 // ------------------------------------------------------------------------
 // Max-reductions of the element errors and the convergence rule.
 // ------------------------------------------------------------------------
-__global__ void __launch_bounds__(1024) reduce_kernel(Net net) {
-  const int r = blockIdx.x;
-  SolveState *st = net.st + r;
-  if (st->done) return;
-  __shared__ double s_err[32], s_ec[32];
-  __shared__ int s_idx[32], s_nf[32];
+// The running maximum of the element errors with its (first) index, the
+// maximum of the coefficient errors and a non-finite flag, with np.max /
+// np.argmax semantics: a NaN wins, the first index among equal maxima or
+// NaNs.  merge() is associative and commutative, so any split of the
+// elements gives the same result.
+struct ErrAcc {
   double best = -INFINITY, bec = -INFINITY;
   int bidx = 0x7fffffff, nonfin = 0;
-  const int e0 = net.eoff[r], e1 = net.eoff[r + 1];
-#pragma unroll 4
-  for (int i = e0 + threadIdx.x; i < e1; i += blockDim.x) {  // loads of four elements in flight
-    double e = net.err[i], ec = net.err_coef[i];
-    if (!(e == e)) {  // NaN wins (np.max / np.argmax semantics)
-      if (best == best || i < bidx) {
+  // element i (visited in increasing order by one thread)
+  __device__ __forceinline__ void add(double e, double ec, int i) {
+    if (!(e == e)) {
+      if (best == best) {
         best = NAN;
-        bidx = (best == best) ? i : min(bidx, i);
+        bidx = i;
+      } else {
+        bidx = min(bidx, i);
       }
-      best = NAN;
       nonfin = 1;
     } else if (best == best && (e > best || (e == best && i < bidx))) {
       best = e;
@@ -889,13 +1048,8 @@ __global__ void __launch_bounds__(1024) reduce_kernel(Net net) {
       bec = ec;
     }
   }
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  for (int o = 16; o > 0; o >>= 1) {
-    double ob = __shfl_xor_sync(0xffffffffu, best, o);
-    int oi = __shfl_xor_sync(0xffffffffu, bidx, o);
-    double oec = __shfl_xor_sync(0xffffffffu, bec, o);
-    int onf = __shfl_xor_sync(0xffffffffu, nonfin, o);
-    bool onan = !(ob == ob), mnan = !(best == best);
+  __device__ __forceinline__ void merge(double ob, int oi, double oec, int onf) {
+    const bool onan = !(ob == ob), mnan = !(best == best);
     if (onan && (!mnan || oi < bidx)) {
       best = ob;
       bidx = oi;
@@ -906,43 +1060,103 @@ __global__ void __launch_bounds__(1024) reduce_kernel(Net net) {
     if (!(oec == oec) || (bec == bec && oec > bec)) bec = oec;
     nonfin |= onf;
   }
+  __device__ __forceinline__ void warp_merge() {
+    for (int o = 16; o > 0; o >>= 1)
+      merge(__shfl_xor_sync(0xffffffffu, best, o), __shfl_xor_sync(0xffffffffu, bidx, o),
+            __shfl_xor_sync(0xffffffffu, bec, o), __shfl_xor_sync(0xffffffffu, nonfin, o));
+  }
+};
+
+// The block's ErrAcc into thread 0 (every thread calls it).
+template <int THREADS>
+__device__ __forceinline__ void block_merge(ErrAcc &a) {
+  __shared__ double s_err[THREADS / 32], s_ec[THREADS / 32];
+  __shared__ int s_idx[THREADS / 32], s_nf[THREADS / 32];
+  a.warp_merge();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   if (lane == 0) {
-    s_err[w] = best;
-    s_idx[w] = bidx;
-    s_ec[w] = bec;
-    s_nf[w] = nonfin;
+    s_err[w] = a.best;
+    s_idx[w] = a.bidx;
+    s_ec[w] = a.bec;
+    s_nf[w] = a.nonfin;
   }
   __syncthreads();
+  if (threadIdx.x == 0)
+    for (int k = 1; k < THREADS / 32; k++) a.merge(s_err[k], s_idx[k], s_ec[k], s_nf[k]);
+}
+
+// The convergence rule of realization r from its errors (one thread).
+__device__ __forceinline__ void reduce_finish(Net &net, SolveState *st, const ErrAcc &a, int e0) {
+  int nf = a.nonfin;
+  st->error = a.best;
+  st->worst = a.bidx - e0;
+  st->error_coef = a.bec;
+  if (!(st->error_q == st->error_q)) nf = 1;
+  if (nf) st->nonfinite = 1;
+  // hpc_solve.py:237-239
+  if (a.bec < st->max_error && st->error_q < st->max_error) {
+    st->cnt_error += 1;
+    st->error_q = 1e30;
+  }
+  if (st->cnt_error >= 2 || st->nit >= st->max_it || st->nonfinite) {
+    st->done = 1;
+    atomicAdd(net.ndone, 1);
+  }
+  st->solve_q = (st->error_q > st->max_error / 1e30) ? 1 : 0;
+}
+
+// One CTA per realization.
+__global__ void __launch_bounds__(1024) reduce_kernel(Net net) {
+  const int r = blockIdx.x;
+  SolveState *st = net.st + r;
+  if (st->done) return;
+  ErrAcc a;
+  const int e0 = net.eoff[r], e1 = net.eoff[r + 1];
+#pragma unroll 4
+  for (int i = e0 + threadIdx.x; i < e1; i += blockDim.x) a.add(net.err[i], net.err_coef[i], i);
+  block_merge<1024>(a);
+  if (threadIdx.x == 0) reduce_finish(net, st, a, e0);
+}
+
+// A single network's reduction over several CTAs (REDUCE_SPLIT_ELEMS
+// elements each, one element per thread and round): every CTA writes its
+// partial result, the last to finish merges them in CTA order and applies
+// the convergence rule, then resets the ticket for the next launch.
+static constexpr int REDUCE_SPLIT_THREADS = 256;
+static constexpr int REDUCE_SPLIT_ELEMS = 4 * REDUCE_SPLIT_THREADS;
+struct ReducePart {
+  double best, bec;
+  int bidx, nonfin;
+};
+__global__ void __launch_bounds__(REDUCE_SPLIT_THREADS) reduce_split_kernel(Net net, ReducePart *parts,
+                                                                           unsigned *ticket) {
+  SolveState *st = net.st;
+  if (st->done) return;
+  ErrAcc a;
+  const int e1 = net.eoff[1];
+  const int c0 = blockIdx.x * REDUCE_SPLIT_ELEMS;
+#pragma unroll
+  for (int u = 0; u < REDUCE_SPLIT_ELEMS / REDUCE_SPLIT_THREADS; u++) {
+    const int i = c0 + u * REDUCE_SPLIT_THREADS + threadIdx.x;
+    if (i < e1) a.add(net.err[i], net.err_coef[i], i);
+  }
+  block_merge<REDUCE_SPLIT_THREADS>(a);
+  __shared__ int s_last;
   if (threadIdx.x == 0) {
-    double b = s_err[0], ec = s_ec[0];
-    int bi = s_idx[0], nf = s_nf[0];
-    for (int k = 1; k < (int)(blockDim.x + 31) / 32; k++) {
-      bool onan = !(s_err[k] == s_err[k]), mnan = !(b == b);
-      if (onan && (!mnan || s_idx[k] < bi)) {
-        b = s_err[k];
-        bi = s_idx[k];
-      } else if (!onan && !mnan && (s_err[k] > b || (s_err[k] == b && s_idx[k] < bi))) {
-        b = s_err[k];
-        bi = s_idx[k];
-      }
-      if (!(s_ec[k] == s_ec[k]) || (ec == ec && s_ec[k] > ec)) ec = s_ec[k];
-      nf |= s_nf[k];
-    }
-    st->error = b;
-    st->worst = bi - e0;
-    st->error_coef = ec;
-    if (!(st->error_q == st->error_q)) nf = 1;
-    if (nf) st->nonfinite = 1;
-    // hpc_solve.py:237-239
-    if (ec < st->max_error && st->error_q < st->max_error) {
-      st->cnt_error += 1;
-      st->error_q = 1e30;
-    }
-    if (st->cnt_error >= 2 || st->nit >= st->max_it || st->nonfinite) {
-      st->done = 1;
-      atomicAdd(net.ndone, 1);
-    }
-    st->solve_q = (st->error_q > st->max_error / 1e30) ? 1 : 0;
+    parts[blockIdx.x] = ReducePart{a.best, a.bec, a.bidx, a.nonfin};
+    __threadfence();
+    s_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  ErrAcc t;
+  for (int k = threadIdx.x; k < (int)gridDim.x; k += REDUCE_SPLIT_THREADS)
+    t.merge(__ldcg(&parts[k].best), __ldcg(&parts[k].bidx), __ldcg(&parts[k].bec), __ldcg(&parts[k].nonfin));
+  block_merge<REDUCE_SPLIT_THREADS>(t);
+  if (threadIdx.x == 0) {
+    reduce_finish(net, st, t, 0);
+    *ticket = 0;
   }
 }
 
@@ -3795,6 +4009,67 @@ struct DBuf {
   ~DBuf() { release(); }
 };
 
+// Page-locked host blocks (the Schur complement's staging buffer), kept
+// for later handles of the process like the device blocks above: a block is
+// handed out only after its owner's copies have finished (the owner
+// synchronises before it releases).  At most ANDFN_B200_PINNED_POOL_MB MiB
+// (default 1024) are kept; andfn_b200_release_cached_memory() frees them.
+struct PinnedPool {
+  std::mutex m;
+  std::multimap<size_t, void *> blocks;
+  size_t held = 0;
+};
+static PinnedPool &pinned_pool() {
+  static PinnedPool *pool = new PinnedPool();
+  return *pool;
+}
+static void *pinned_get(size_t bytes, size_t *cap) {
+  PinnedPool &P = pinned_pool();
+  {
+    std::lock_guard<std::mutex> lk(P.m);
+    auto it = P.blocks.lower_bound(bytes);
+    if (it != P.blocks.end() && it->first <= 2 * bytes) {
+      void *p = it->second;
+      *cap = it->first;
+      P.held -= it->first;
+      P.blocks.erase(it);
+      return p;
+    }
+  }
+  void *p = nullptr;
+  if (cudaMallocHost(&p, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  *cap = bytes;
+  return p;
+}
+static void pinned_put(void *p, size_t cap) {
+  if (!p) return;
+  static const size_t limit = [] {
+    long long mb = 1024;
+    if (const char *e = getenv("ANDFN_B200_PINNED_POOL_MB")) mb = std::max(0LL, atoll(e));
+    return (size_t)mb << 20;
+  }();
+  PinnedPool &P = pinned_pool();
+  {
+    std::lock_guard<std::mutex> lk(P.m);
+    if (P.held + cap <= limit) {
+      P.blocks.emplace(cap, p);
+      P.held += cap;
+      return;
+    }
+  }
+  cudaFreeHost(p);
+}
+static void pinned_flush() {
+  PinnedPool &P = pinned_pool();
+  std::lock_guard<std::mutex> lk(P.m);
+  for (auto &kv : P.blocks) cudaFreeHost(kv.second);
+  P.blocks.clear();
+  P.held = 0;
+}
+
 struct HostNet {
   // element SoA of all realizations (host copies of the geometry and of the initial state)
   std::vector<int> type, frac0, frac1, ncoef, nint;
@@ -3958,6 +4233,16 @@ struct AndfnHandle {
   int sweep_variant = -1;
   bool tune_sweep = true;  // false: the one-call solve uses a cached choice or the default
   DBuf<int> upd_list, psi_list;
+  DBuf<cd> dft_tab;  // DFT bases, one per (nint, theta layout) in use
+  DBuf<int> dft_off;
+  // a single network's split reduction: partial results and the ticket
+  DBuf<ReducePart> red_parts;
+  DBuf<unsigned> red_ticket;
+  // a batch's active work lists (rows, sweep items, elements) and their state
+  DBuf<int> act_l[3], act_ccnt;
+  DBuf<ActState> act_st;
+  ActLists act{};
+  bool act_on = false;
   int n_upd = 0, n_psi = 0;
   int nvmax = 0;
   // current ncoef / nint the tables were built for (they change with adaptive growth)
@@ -4058,12 +4343,14 @@ struct AndfnHandle {
     n.ndone = ndone.p;
     n.tri = tri.p;
     n.bknown = has_spec ? bknown.p : nullptr;
+    n.dft_tab = dft_tab.p;
+    n.dft_off = dft_off.p;
     return n;
   }
   ~AndfnHandle() {
     if (order_thread.joinable()) order_thread.join();
     if (dlu_ev) cudaEventDestroy(dlu_ev);
-    if (pin_schur) cudaFreeHost(pin_schur);
+    if (pin_schur) pinned_put(pin_schur, sizeof(double) * pin_schur_n);
     andfn::destroy_adj(adj);
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
     if (loop_exec) cudaGraphExecDestroy(loop_exec);
@@ -4235,6 +4522,26 @@ static thread_local int64_t g_h2d_bytes = 0, g_d2h_bytes = 0;
 static double ms_since(std::chrono::steady_clock::time_point t0) {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
+
+// Phase trace: with ANDFN_B200_TRACE set (to anything but 0), the host
+// phases of handle creation and of a run's set-up print their wall time to
+// stderr as they end (host time; a phase that waits for the stream includes
+// the device work queued before it).
+static bool trace_on() {
+  static const bool on = [] {
+    const char *e = getenv("ANDFN_B200_TRACE");
+    return e && atoi(e) != 0;
+  }();
+  return on;
+}
+
+struct PhaseTimer {
+  std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
+  void lap(const char *name) {
+    if (trace_on()) fprintf(stderr, "[andfn_b200] %-28s %8.3f ms\n", name, ms_since(t));
+    t = std::chrono::steady_clock::now();
+  }
+};
 
 template <class T>
 static cudaError_t upload(DBuf<T> &d, const std::vector<T> &v, cudaStream_t s) {
@@ -4420,10 +4727,55 @@ static void build_tables(AndfnHandle *H, bool rhs, std::vector<Group> &groups, s
 static int reset_impl(AndfnHandle *H);
 
 // Sweep / head-vector tables for the current ncoef and nint, uploaded.
+// DFT bases of the elements' Cauchy-integral fits, one per (nint, theta
+// layout) in use: entry (k, j) = exp_m[k]^j, exp_m[k] = exp(-i theta_k),
+// theta_k = start + k del (del = pi / n, start = del / 2; del = 2 pi / n,
+// start = 0 for bounding circles), the powers formed by repeated complex
+// multiplication from 1 as the reference forms them
+// (hpc_math_functions.py:244-297, 674-723).
+static int build_dft_tables(AndfnHandle *H) {
+  const HostNet &h = H->h;
+  const int ne = (int)H->ne, MC = H->MC;
+  std::map<std::pair<int, int>, int> where;
+  std::vector<cd> tab;
+  std::vector<int> off(std::max(1, ne), 0);
+  for (int e = 0; e < ne; e++) {
+    if (h.type[e] == 2) continue;
+    const int n = H->cur_nint[e], kind = (h.type[e] == 1) ? 1 : 0;
+    auto it = where.find({n, kind});
+    if (it == where.end()) {
+      const int o = (int)tab.size();
+      it = where.emplace(std::make_pair(n, kind), o).first;
+      tab.resize(tab.size() + (size_t)n * MC);
+      const double del = kind ? 2 * PI / n : PI / n, start = kind ? 0.0 : del / 2;
+      for (int k = 0; k < n; k++) {
+        const double th = start + k * del;
+        const double er = std::cos(-th), ei = std::sin(-th);
+        double pr = 1.0, pi = 0.0;
+        for (int j = 0; j < MC; j++) {
+          tab[(size_t)o + (size_t)k * MC + j] = mk(pr, pi);
+          const double nr = pr * er - pi * ei, ni = pr * ei + pi * er;
+          pr = nr;
+          pi = ni;
+        }
+      }
+    }
+    off[e] = it->second;
+  }
+  if (tab.empty()) tab.push_back(mk(0.0, 0.0));
+  CK(upload(H->dft_tab, tab, H->stream));
+  CK(upload(H->dft_off, off, H->stream));
+  return 0;
+}
+
 static int build_eval_tables(AndfnHandle *H) {
   HostNet &h = H->h;
   cudaStream_t s = H->stream;
   const int ne = (int)H->ne;
+  {
+    const int rcd = build_dft_tables(H);
+    if (rcd) return rcd;
+  }
   std::vector<Group> groups;
   std::vector<int> group_of, rhs_group;
   std::vector<Item> sitems, ritems;
@@ -4521,10 +4873,12 @@ static int create_impl(AndfnHandle *H, int R, const char *const *F, const int64_
   h.roff.assign(R + 1, 0);
   h.fptr.assign(1, 0);
   H->MC = 1;
+  PhaseTimer pt;
   for (int r = 0; r < R; r++) {
     int rc = parse_records(H, r, F[r], nf[r], E[r], ne[r]);
     if (rc) return rc;
   }
+  pt.lap("create: parse records");
   H->ne = h.eoff[R];
   H->nf = h.foff[R];
   H->N = h.roff[R];
@@ -4546,6 +4900,7 @@ static int create_impl(AndfnHandle *H, int R, const char *const *F, const int64_
     H->ent_kind.push_back(0);
   }
   for (char c : H->h.spec_q) H->has_spec |= (c != 0);
+  pt.lap("create: system patterns");
   // batches whose realizations the device inverts need no column order; it
   // is computed on first use if a run falls back to the sparse LU
   int maxn_sys = 0;
@@ -4572,6 +4927,7 @@ static int create_impl(AndfnHandle *H, int R, const char *const *F, const int64_
       }
     }
     H->ms_create_order = ms_since(tc2);
+    if (trace_on()) fprintf(stderr, "[andfn_b200] %-28s %8.3f ms\n", "create: column orders (thread)", H->ms_create_order);
   });
   h.coef.assign((size_t)H->ne * H->MC, mk(0.0, 0.0));
   for (int r = 0; r < R; r++) read_coefs(H, r, E[r]);
@@ -4641,17 +4997,24 @@ static int create_impl(AndfnHandle *H, int R, const char *const *F, const int64_
   CK(upload(H->d_ent_kind, H->ent_kind, s));
   CK(H->d_mvals.alloc(std::max<size_t>(1, H->ent_row.size())));
   H->ms_create_upload = ms_since(tc0);
+  pt.lap("create: uploads");
   auto tc1 = std::chrono::steady_clock::now();
   H->cur_ncoef = h.ncoef;
   H->cur_nint = h.nint;
   int rc = build_eval_tables(H);
   if (rc) return rc;
   H->ms_create_tables = ms_since(tc1);
+  pt.lap("create: evaluation tables");
   CK(H->disc.alloc(H->N));
   CK(H->work.alloc(H->N));
   CK(H->bvec.alloc(H->N));
   CK(H->ready.alloc(H->N));
   CK(H->st.alloc(R));
+  if (R == 1) {
+    CK(H->red_parts.alloc((H->ne + REDUCE_SPLIT_ELEMS - 1) / REDUCE_SPLIT_ELEMS));
+    CK(H->red_ticket.alloc(1));
+    CK(cudaMemsetAsync(H->red_ticket.p, 0, sizeof(unsigned), s));
+  }
   H->h_st.assign(R, SolveState());
   if (!H->h_ndone) CK(cudaMallocHost(&H->h_ndone, sizeof(int)));
   CK(cudaFuncSetAttribute(eval_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
@@ -5065,18 +5428,20 @@ static int factor_all(AndfnHandle *H, const std::vector<double> &mv) {
   // a large dense block is factorised on the device; several: one
   // realization per thread, dense blocks on the host
   const bool defer = R == 1 && H->sys[0].dense_k >= DLU_MIN_K && H->sys[0].dense_k <= DLU_MAX_K;
-  // a handle that factorises again (parameter sweeps, the adjoint's forward
-  // solves) forms the Schur complement straight into page-locked memory, so
-  // its upload is a DMA; a single solve does not pay for the allocation
+  // the Schur complement is formed straight into page-locked memory (from
+  // the process's cache of such blocks), so its upload is a DMA
   double *schur_buf = nullptr;
-  if (defer && H->factor_runs > 0) {
+  if (defer) {
     const size_t need = (size_t)H->sys[0].dense_k * H->sys[0].dense_k;
     if (H->pin_schur_n < need) {
-      if (H->pin_schur) cudaFreeHost(H->pin_schur);
+      if (H->pin_schur) pinned_put(H->pin_schur, sizeof(double) * H->pin_schur_n);
       H->pin_schur = nullptr;
       H->pin_schur_n = 0;
-      if (cudaMallocHost(reinterpret_cast<void **>(&H->pin_schur), sizeof(double) * need) == cudaSuccess)
-        H->pin_schur_n = need;
+      size_t cap = 0;
+      if (void *p = pinned_get(sizeof(double) * need, &cap)) {
+        H->pin_schur = static_cast<double *>(p);
+        H->pin_schur_n = cap / sizeof(double);
+      }
       else
         cudaGetLastError();
     }
@@ -5341,7 +5706,8 @@ static void launch_trisolve_kernel(AndfnHandle *H, const Net &net, cudaStream_t 
 static int build_head_sums(AndfnHandle *H);
 template <int T, int RPB>
 __global__ void head_vector_kernel(Net net, const int *__restrict__ gptr, const int *__restrict__ sidx,
-                                   const cd *__restrict__ S);
+                                   const cd *__restrict__ S, const int *__restrict__ alist,
+                                   const int *__restrict__ acount);
 
 // Kernels one discharge solve launches.
 static int tri_launches(const AndfnHandle *H) { return H->winv_ready ? 3 : 1; }  // batched inverses: 1
@@ -5505,16 +5871,18 @@ static int run_device_loop(AndfnHandle *H, const AndfnConstants *C, bool *ran, i
 enum SweepVariant { SWEEP_PER_ITEM = 0, SWEEP_QUEUE4 = 1, SWEEP_QUEUE6 = 2, SWEEP_VARIANTS = 3 };
 
 static void launch_sweep_variant(AndfnHandle *H, const Net &net, cudaStream_t s, int v) {
+  const int *alist = H->act_on ? H->act.list[1] : nullptr;
+  const int *acount = H->act_on ? &H->act.st->count[1] : nullptr;
   if (v == SWEEP_PER_ITEM) {
     sweep_table_kernel<<<H->n_sweep_items, EVAL_THREADS, H->tab_smem, s>>>(
         net, H->sweep_items.p, H->sweep_pts.p, H->d_groups.p, H->tab_fpt0.p, H->tab_fnp.p, H->tab_off.p, H->tab_w.p,
-        H->tab_l.p, H->sweep_vals.p, H->tab_chunk);
+        H->tab_l.p, H->sweep_vals.p, H->tab_chunk, alist, acount);
   } else {
     const int per_sm = (v == SWEEP_QUEUE4) ? 4 : 6;
     const int grid = std::min(H->n_sweep_items, per_sm * H->num_sms);
     sweep_table_queue_kernel<<<grid, EVAL_THREADS, H->tab_smem, s>>>(
         net, H->sweep_items.p, H->n_sweep_items, H->sweep_pts.p, H->d_groups.p, H->tab_fpt0.p, H->tab_fnp.p,
-        H->tab_off.p, H->tab_w.p, H->tab_l.p, H->sweep_vals.p, H->tab_chunk, H->sweep_q.p);
+        H->tab_off.p, H->tab_w.p, H->tab_l.p, H->sweep_vals.p, H->tab_chunk, H->sweep_q.p, alist, acount);
   }
 }
 
@@ -5610,11 +5978,15 @@ static int build_pair_table(AndfnHandle *H) {
 static int enqueue_iteration(AndfnHandle *H, cudaStream_t s, int blend_mode, int b) {
   Net net = H->net();
   mark(H, s, b, K_RHS, 0);
+  const int *arows = H->act_on ? H->act.list[0] : nullptr;
+  const int *arow_n = H->act_on ? &H->act.st->count[0] : nullptr;
   if (H->use_head_sums) {
     if (H->hs.long_rows)
-      head_vector_kernel<HV_THREADS, 1><<<H->N, HV_THREADS, 0, s>>>(net, H->hs.gptr.p, H->hs.sidx.p, H->hs.S.p);
+      head_vector_kernel<HV_THREADS, 1><<<H->N, HV_THREADS, 0, s>>>(net, H->hs.gptr.p, H->hs.sidx.p, H->hs.S.p,
+                                                                     arows, arow_n);
     else
-      head_vector_kernel<32, 4><<<(H->N + 3) / 4, 128, 0, s>>>(net, H->hs.gptr.p, H->hs.sidx.p, H->hs.S.p);
+      head_vector_kernel<32, 4><<<(H->N + 3) / 4, 128, 0, s>>>(net, H->hs.gptr.p, H->hs.sidx.p, H->hs.S.p, arows,
+                                                               arow_n);
   } else {
     if (H->n_rhs_items > 0)
       eval_kernel<true><<<H->n_rhs_items, EVAL_THREADS, H->eval_smem, s>>>(net, H->rhs_items.p, H->rhs_pts.p,
@@ -5633,13 +6005,52 @@ static int enqueue_iteration(AndfnHandle *H, cudaStream_t s, int blend_mode, int
   const size_t usmem = sizeof(double) * 2 * H->nvmax * UPDATE_WARPS;
   mark(H, s, b, K_UPDATE, 0);
   if (ub > 0)
-    update_kernel<<<ub, UPDATE_WARPS * 32, usmem, s>>>(net, H->upd_list.p, H->n_upd, H->group_of.p, H->d_groups.p,
-                                                        H->sweep_vals.p, H->nvmax, blend_mode);
+    update_kernel<<<ub, UPDATE_WARPS * 32, usmem, s>>>(
+        net, H->act_on ? H->act.list[2] : H->upd_list.p, H->n_upd, H->group_of.p, H->d_groups.p, H->sweep_vals.p,
+        H->nvmax, blend_mode, H->act_on ? &H->act.st->count[2] : nullptr);
   mark(H, s, b, K_UPDATE, 1);
   mark(H, s, b, K_REDUCE, 0);
-  reduce_kernel<<<H->R, 1024, 0, s>>>(net);
+  if (H->R == 1 && H->red_parts.p)
+    reduce_split_kernel<<<(int)((H->ne + REDUCE_SPLIT_ELEMS - 1) / REDUCE_SPLIT_ELEMS), REDUCE_SPLIT_THREADS, 0, s>>>(
+        net, H->red_parts.p, H->red_ticket.p);
+  else
+    reduce_kernel<<<H->R, 1024, 0, s>>>(net);
+  if (H->act_on) {  // the active lists of the next iteration (launches return at entry unless one finished)
+    act_count_kernel<<<H->act.chunk0[ACT_LISTS], ACT_CHUNK, 0, s>>>(net, H->act);
+    act_scatter_kernel<<<H->act.chunk0[ACT_LISTS], ACT_CHUNK, 0, s>>>(net, H->act);
+    H->launches += 2;
+  }
   mark(H, s, b, K_REDUCE, 1);
   H->launches += 4 + tri_launches(H);
+  return 0;
+}
+
+// A batch's active work lists for the iterations of this run: the full
+// lists, rebuilt after each iteration in which a realization finished.  The
+// element list relies on the update list being every element in order.
+static int act_setup(AndfnHandle *H, int ndone0) {
+  cudaStream_t s = H->stream;
+  const int n[ACT_LISTS] = {(int)H->N, H->n_sweep_items, H->n_upd};
+  ActLists &A = H->act;
+  int c0 = 0;
+  for (int l = 0; l < ACT_LISTS; l++) {
+    A.n[l] = n[l];
+    A.chunk0[l] = c0;
+    c0 += std::max(1, (n[l] + ACT_CHUNK - 1) / ACT_CHUNK);
+    if (H->act_l[l].cap < (size_t)std::max(1, n[l])) CK(H->act_l[l].alloc(std::max(1, n[l])));
+    A.list[l] = H->act_l[l].p;
+  }
+  A.chunk0[ACT_LISTS] = c0;
+  if (H->act_ccnt.cap < (size_t)c0) CK(H->act_ccnt.alloc(c0));
+  if (H->act_st.cap < 1) CK(H->act_st.alloc(1));
+  A.ccnt = H->act_ccnt.p;
+  A.items = H->sweep_items.p;
+  A.st = H->act_st.p;
+  const int mx = std::max({n[0], n[1], n[2], 1});
+  act_init_kernel<<<std::min(4 * H->num_sms, (mx + 255) / 256), 256, 0, s>>>(A, ndone0);
+  CK(cudaGetLastError());
+  H->launches += 1;
+  H->act_on = true;
   return 0;
 }
 
@@ -5804,6 +6215,7 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
   const int ndone0 = st0.done ? R : 0;
   CK(cudaMemcpyAsync(H->ndone.p, &ndone0, sizeof(int), cudaMemcpyHostToDevice, s));
   auto t_setup = std::chrono::steady_clock::now();
+  PhaseTimer pt;
   init_state_kernel<<<std::max<int64_t>(1, (H->ne + 255) / 256), 256, 0, s>>>(net);
   const int n_de = (int)H->h.de_ids.size();
   if (n_de > 0) zint_kernel<<<std::max(1, std::min(1184, (int)((n_de * H->D + 255) / 256))), 256, 0, s>>>(net);
@@ -5816,6 +6228,7 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
   if (!growth_possible) {
     int rch = build_head_sums(H);
     if (rch) return rch;
+    pt.lap("setup: head-vector sums");
     H->use_head_sums = true;
     if (const char *v = getenv("ANDFN_B200_PAIR_TABLES"); !v || atoi(v) != 0) {
       int rcp = build_pair_table(H);
@@ -5827,6 +6240,7 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
       }
       rcp = sweep_autotune(H);
       if (rcp) return rcp;
+      pt.lap("setup: pair tables");
     }
   }
   const long long nent = (long long)H->ent_row.size();
@@ -5846,6 +6260,7 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
   CK(cudaMemcpyAsync(H->disc.p, disc0.data(), sizeof(double) * H->N, cudaMemcpyHostToDevice, s));
   g_h2d_bytes += 8 * (int64_t)H->N;
   CK(cudaStreamSynchronize(s));
+  pt.lap("setup: matrix values (sync)");
   if (H->has_spec) {
     // the prescribed discharges' terms move to the right-hand side: minus
     // the entry times q in the rows, minus q in the continuity rows
@@ -5859,9 +6274,12 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
   base.ms_setup = ms_since(t_setup);
   // factorisation (host)
   auto t_fac = std::chrono::steady_clock::now();
+  pt.lap("setup: rest");
   if (H->order_thread.joinable()) H->order_thread.join();
+  pt.lap("factor: wait for column order");
   rc = factor_all(H, mv);
   if (rc) return rc;
+  pt.lap("factor");
   base.ms_factor = ms_since(t_fac);
   base.ms_factor_sparse = H->ms_fac[0];
   base.ms_factor_dense = H->ms_fac[1];
@@ -5874,6 +6292,17 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
     int rca = run_adaptive(H, C);
     if (rca) return rca;
   } else {
+    // a batch's kernels run over the work of its running realizations (the
+    // lists are off again when the loop ends, also on an error return)
+    struct ActOff {
+      AndfnHandle *h;
+      ~ActOff() { h->act_on = false; }
+    } act_off{H};
+    const char *al = getenv("ANDFN_B200_ACTIVE_LISTS");
+    if (R > 1 && !(al && atoi(al) == 0)) {
+      const int rca = act_setup(H, ndone0);
+      if (rca) return rca;
+    }
     // the whole loop in one launch (not with per-kernel event profiling,
     // whose event nodes a loop body cannot hold, nor with cluster-launched
     // triangular solves)
@@ -5886,6 +6315,7 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
       if (looped) loop_launches = 1;
     }
     if (!looped) {
+    int64_t launches_before = 0;
     if (H->graph_exec) {
       cudaGraphExecDestroy(H->graph_exec);
       H->graph_exec = nullptr;
@@ -5896,6 +6326,7 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
         for (auto &bb : H->ev)
           for (auto &c : bb)
             for (auto &e : c) CK(cudaEventCreate(&e));
+      launches_before = H->launches;
       CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
       for (int b = 0; b < ITER_BATCH; b++) enqueue_iteration(H, s, 0, b);
       {
@@ -5908,15 +6339,15 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
       CK(cudaGraphInstantiate(&H->graph_exec, g, 0));
       cudaGraphDestroy(g);
     }
-    const int per_it = (H->use_head_sums ? 4 : 5) + tri_launches(H);  // kernels of one captured iteration
-  H->launches -= ITER_BATCH * per_it;           // capture does not launch
+    const int64_t per_graph = H->launches - launches_before;  // kernels of the captured iterations
+    H->launches = launches_before;                          // capture does not launch
     int guard = 0;
     int nit_before = 0;
     while (true) {
       CK(cudaGraphLaunch(H->graph_exec, s));
       CK(cudaMemcpyAsync(H->h_ndone, H->ndone.p, sizeof(int), cudaMemcpyDeviceToHost, s));
       CK(cudaStreamSynchronize(s));
-      H->launches += ITER_BATCH * per_it;
+      H->launches += per_graph;
       if (H->profiling) {
         // only the iterations that did work (later ones return at entry)
         int rcs = read_states(H);
@@ -5940,6 +6371,7 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
     }
     }
   }
+  H->act_on = false;
   rc = read_states(H);
   if (rc) return rc;
   std::vector<SolveState> fin = H->h_st;
@@ -6407,10 +6839,12 @@ int andfn_b200_batch_create(AndfnHandle **out, int64_t R, void *const *frac_recs
     }
   }
   cudaGetDevice(&H->device);
-  cudaDeviceProp prop;
-  cudaGetDeviceProperties(&prop, H->device);
-  H->num_sms = prop.multiProcessorCount;
-  if (prop.major < 10) {
+  // two attributes, not cudaGetDeviceProperties (which queries them all and
+  // costs milliseconds a call)
+  int major = 0;
+  cudaDeviceGetAttribute(&H->num_sms, cudaDevAttrMultiProcessorCount, H->device);
+  cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, H->device);
+  if (major < 10) {
     delete H;
     set_error("an sm_100 (Blackwell) device is required");
     return ANDFN_NO_DEVICE;
@@ -6643,6 +7077,7 @@ int andfn_b200_fp64_peak(int32_t device, double *tflops) {
 }
 
 void andfn_b200_release_cached_memory(void) {
+  pinned_flush();
   DevicePool &P = device_pool();
   std::lock_guard<std::mutex> lk(P.m);
   int cur = 0;
@@ -7252,6 +7687,18 @@ __global__ void __launch_bounds__(EVAL_THREADS) adj_sweep_table_kernel(
 // for every (row side, source element of that side's fracture) pair (one warp
 // per pair), and each iteration gathers gc[s][j] += sum over the pairs of s of
 // weight * conj(S[pair][j]) (one thread per source coefficient).
+// The coefficient index (source * MC + power) of every power-sum entry: a
+// warp per (row side, source) pair, whose entries are consecutive from its
+// offset to the next pair's.
+__global__ void hs_index_kernel(const int *__restrict__ pair_src, const int *__restrict__ pair_off, int npairs,
+                                int total, int MC, int *__restrict__ sidx) {
+  const int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (p >= npairs) return;
+  const int o0 = pair_off[p], o1 = (p + 1 < npairs) ? pair_off[p + 1] : total;
+  const int base = pair_src[p] * MC;
+  for (int k = lane; k < o1 - o0; k += 32) sidx[o0 + k] = base + k;
+}
+
 __global__ void rhs_sums_kernel(Net net, const int *__restrict__ pair_g, const int *__restrict__ pair_src,
                                 const int *__restrict__ pair_off, int npairs, cd *S) {
   const int pr = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
@@ -7343,11 +7790,18 @@ __device__ __forceinline__ double hv_group_sum(double v, double *red) {
 template <int T, int RPB>
 __global__ void __launch_bounds__(T * RPB) head_vector_kernel(Net net, const int *__restrict__ gptr,
                                                                const int *__restrict__ sidx,
-                                                               const cd *__restrict__ S) {
+                                                               const cd *__restrict__ S,
+                                                               const int *__restrict__ alist,
+                                                               const int *__restrict__ acount) {
   __shared__ double red[T / 32 > 0 ? T / 32 : 1];
   const int t = (T == 32) ? (threadIdx.x & 31) : threadIdx.x;
-  const int g = blockIdx.x * RPB + ((T == 32) ? (threadIdx.x >> 5) : 0);
-  if (g >= net.N) return;  // uniform over the row's group
+  int g = blockIdx.x * RPB + ((T == 32) ? (threadIdx.x >> 5) : 0);
+  if (alist) {  // a batch's rows of running realizations
+    if (g >= *acount) return;  // uniform over the row's group
+    g = alist[g];
+  } else if (g >= net.N) {
+    return;
+  }
   const SolveState *st = net.st + net.real_row[g];
   if (st->done || !st->solve_q) return;
   const int r = net.row_de[g];
@@ -7780,8 +8234,11 @@ static int build_head_sums(AndfnHandle *H) {
   const HostNet &h = H->h;
   const int ne = (int)H->ne, n_de = (int)h.de_ids.size(), MC = H->MC;
   cudaStream_t s = H->stream;
-  std::vector<int> pg, ps, po, gptr(2 * (size_t)n_de + 1, 0), sidx;
-  std::vector<std::vector<int>> by_src(ne);
+  // pairs (row side, source element) in row order; the power-sum entries
+  // of a pair are consecutive (offset po, ncoef of the source entries), and
+  // the coefficient index of each entry is written on the device
+  std::vector<int> pg, ps, po, gptr(2 * (size_t)n_de + 1, 0);
+  std::vector<int> sp(ne + 1, 0);
   int off = 0;
   for (int j = 0; j < n_de; j++) {
     const int e = h.de_ids[j];
@@ -7794,21 +8251,19 @@ static int build_head_sums(AndfnHandle *H) {
         const int el = h.felem[k];
         const int m = H->cur_ncoef[el];
         if (h.type[el] == 2 || m <= 0) continue;
-        by_src[el].push_back((int)pg.size());
+        sp[el + 1]++;
         pg.push_back(2 * j + sd);
         ps.push_back(el);
         po.push_back(off);
-        for (int jj = 0; jj < m; jj++) sidx.push_back(el * MC + jj);
         off += m;
       }
     }
   }
   gptr[2 * (size_t)n_de] = off;
-  std::vector<int> sp(ne + 1, 0), spairs;
-  for (int el = 0; el < ne; el++) {
-    sp[el + 1] = sp[el] + (int)by_src[el].size();
-    spairs.insert(spairs.end(), by_src[el].begin(), by_src[el].end());
-  }
+  // the pairs of each source element, in pair order (counting sort)
+  for (int el = 0; el < ne; el++) sp[el + 1] += sp[el];
+  std::vector<int> spairs(pg.size()), fillp(sp.begin(), sp.end() - 1);
+  for (int p = 0; p < (int)ps.size(); p++) spairs[fillp[ps[p]]++] = p;
   hs.npairs = (int)pg.size();
   hs.long_rows = off > 256LL * std::max(1, H->N);
   CK(upload(hs.gptr, gptr, s));
@@ -7818,7 +8273,9 @@ static int build_head_sums(AndfnHandle *H) {
     CK(upload(hs.pair_off, po, s));
     CK(upload(hs.src_ptr, sp, s));
     CK(upload(hs.src_pairs, spairs, s));
-    CK(upload(hs.sidx, sidx, s));
+    CK(hs.sidx.alloc(std::max(1, off)));
+    hs_index_kernel<<<(hs.npairs * 32 + 127) / 128, 128, 0, s>>>(hs.pair_src.p, hs.pair_off.p, hs.npairs, off, MC,
+                                                                  hs.sidx.p);
     CK(hs.S.alloc(std::max(1, off)));
     rhs_sums_kernel<<<(hs.npairs * 32 + 127) / 128, 128, 0, s>>>(H->net(), hs.pair_g.p, hs.pair_src.p,
                                                                   hs.pair_off.p, hs.npairs, hs.S.p);

@@ -56,37 +56,52 @@ struct DegreeBuckets {
   }
 };
 
+// Variables are supervariables: columns found indistinguishable (the same
+// set of adjacent elements, hence the same neighbours) after an elimination
+// step are merged into one principal column of weight nv (the sum of their
+// weights), which is then updated and eliminated as one.  Degrees, element
+// sizes and |Lp| are weighted sums.  When a principal column is eliminated,
+// the order receives it and then the columns merged into it.
 std::vector<int> column_min_degree_order(const CscMatrix &A, int *dense_tail, double dense_frac, int max_dense) {
   const int n = A.n;
   if (dense_tail) *dense_tail = 0;
-  // Row-wise pattern: row r is the initial element r (a clique of its columns).
+  // Ei[j]: the distinct rows of column j (the initial elements of variable j);
+  // Le[r]: the columns of row r in increasing order (row r is the initial
+  // element r, a clique of its columns); elements n.. are created by pivots.
   std::vector<std::vector<int>> Le(2 * (size_t)n + 1);
   std::vector<std::vector<int>> Ei(n);
-  for (int j = 0; j < n; j++)
-    for (int p = A.colptr[j]; p < A.colptr[j + 1]; p++) {
-      int r = A.rowind[p];
-      Le[r].push_back(j);
-      Ei[j].push_back(r);
+  {
+    std::vector<int> mk(n, -1), cnt(n, 0);
+    for (int j = 0; j < n; j++) {
+      auto &E = Ei[j];
+      E.reserve(A.colptr[j + 1] - A.colptr[j]);
+      for (int p = A.colptr[j]; p < A.colptr[j + 1]; p++) {
+        const int r = A.rowind[p];
+        if (mk[r] == j) continue;
+        mk[r] = j;
+        E.push_back(r);
+        cnt[r]++;
+      }
     }
-  for (int r = 0; r < n; r++) {
-    std::sort(Le[r].begin(), Le[r].end());
-    Le[r].erase(std::unique(Le[r].begin(), Le[r].end()), Le[r].end());
+    for (int r = 0; r < n; r++) Le[r].reserve(cnt[r]);
+    for (int j = 0; j < n; j++)
+      for (int r : Ei[j]) Le[r].push_back(j);
   }
-  for (int j = 0; j < n; j++) {
-    std::sort(Ei[j].begin(), Ei[j].end());
-    Ei[j].erase(std::unique(Ei[j].begin(), Ei[j].end()), Ei[j].end());
-  }
-  // per element: the stamp and value of w (below), its list length and
+  // per element: the stamp and value of w (below), its weighted size and
   // whether it is active, side by side (one cache line per visit)
   struct ElemInfo {
     int stamp, w, len, active;
   };
   std::vector<ElemInfo> ei(2 * (size_t)n + 1, ElemInfo{-1, 0, 0, 0});
-  std::vector<char> alive(n, 1);
   for (int r = 0; r < n; r++) {
     ei[r].active = !Le[r].empty();
     ei[r].len = (int)Le[r].size();
   }
+  // nv: weight of a principal column (0 once merged or eliminated);
+  // svnext / svtail: the chain of columns merged into a principal
+  std::vector<int> nv(n, 1), svnext(n, -1), svtail(n);
+  for (int j = 0; j < n; j++) svtail[j] = j;
+  std::vector<char> alive(n, 1);  // a principal column not yet eliminated
   std::vector<int> mark(n, -1);
   DegreeBuckets queue(n);
   // Exact initial degree |union of row cliques containing j| - 1 (columns in
@@ -112,50 +127,59 @@ std::vector<int> column_min_degree_order(const CscMatrix &A, int *dense_tail, do
 
   std::vector<int> order;
   order.reserve(n);
-  int stamp = 0;
-  std::vector<int> Lp;
-  for (int k = 0; k < n; k++) {
-    const int remaining = n - k;
+  auto emit = [&](int p) {
+    for (int v = p; v >= 0; v = svnext[v]) order.push_back(v);
+  };
+  int stamp = 0, estamp = 0, eliminated = 0;
+  std::vector<int> emark(2 * (size_t)n + 1, -1);
+  std::vector<int> Lp, dnew(n, 0);
+  std::vector<unsigned> hsh(n, 0);
+  std::vector<int> byhash;
+  for (int step = 0; eliminated < n; step++) {
+    const int remaining = n - eliminated;
     while (queue.head[queue.mindeg] < 0) queue.mindeg++;
     if (dense_tail && remaining >= 64 && remaining <= max_dense && queue.mindeg >= dense_frac * (remaining - 1)) {
       // The remaining graph is nearly complete: it is factorised as a dense
       // block, where the column order does not change the fill.  Append the
-      // remaining columns by (degree, index).
+      // remaining principal columns by (degree, index), each followed by the
+      // columns merged into it.
       *dense_tail = remaining;
       std::vector<std::pair<int, int>> rest;
       for (int j = 0; j < n; j++)
         if (alive[j]) rest.push_back({queue.deg[j], j});
       std::sort(rest.begin(), rest.end());
-      for (auto &pr : rest) order.push_back(pr.second);
+      for (auto &pr : rest) emit(pr.second);
       return order;
     }
     const int p = queue.pop_min();
-    order.push_back(p);
+    emit(p);
+    eliminated += nv[p];
     alive[p] = 0;
     // New element: union of the active elements adjacent to p, minus p.
     stamp++;
     Lp.clear();
+    int lpw = 0;
     for (int e : Ei[p]) {
       if (!ei[e].active) continue;
       for (int v : Le[e])
-        if (v != p && alive[v] && mark[v] != stamp) {
+        if (alive[v] && mark[v] != stamp) {
           mark[v] = stamp;
           Lp.push_back(v);
+          lpw += nv[v];
         }
       ei[e].active = 0;  // absorbed into the new element
       std::vector<int>().swap(Le[e]);
     }
     std::vector<int>().swap(Ei[p]);
-    const int ne = n + k;
+    const int ne = n + step;
     if (Lp.empty()) continue;
     std::sort(Lp.begin(), Lp.end());
     Le[ne] = Lp;
     ei[ne].active = 1;
-    ei[ne].len = (int)Lp.size();
-    const int lp = (int)Lp.size();
+    ei[ne].len = lpw;
     // Prune absorbed elements from the neighbours' lists and add the new one;
-    // w(e) = |Le \ Lp| for every other element touching Lp (one pass).
-    const int wst = k;
+    // w(e) = weighted |Le \ Lp| for every other element touching Lp (one pass).
+    const int wst = step;
     for (int i : Lp) {
       auto &E = Ei[i];
       size_t o = 0;
@@ -168,17 +192,18 @@ std::vector<int> column_min_degree_order(const CscMatrix &A, int *dense_tail, do
           x.stamp = wst;
           x.w = x.len;
         }
-        x.w -= 1;
+        x.w -= nv[i];
       }
       E.resize(o);
       E.push_back(ne);
     }
-    // Aggressive absorption of elements contained in Lp, then degrees.
-    const int rem = n - k - 1;
+    // Aggressive absorption of elements contained in Lp, then approximate
+    // external degrees and a hash of each list for the supervariable test.
     for (int i : Lp) {
       auto &E = Ei[i];
       size_t o = 0;
-      long d = lp - 1;
+      long d = lpw - nv[i];
+      unsigned h = 0;
       for (size_t a = 0; a < E.size(); a++) {
         int e = E[a];
         ElemInfo &x = ei[e];
@@ -191,16 +216,60 @@ std::vector<int> column_min_degree_order(const CscMatrix &A, int *dense_tail, do
         }
         if (!x.active) continue;
         E[o++] = e;
+        h += (unsigned)e;
         if (e != ne) d += x.w;
       }
       E.resize(o);
-      long bound = (long)queue.deg[i] + lp - 1;
+      long bound = (long)queue.deg[i] + lpw - nv[i];
       if (d > bound) d = bound;
-      if (d > rem - 1) d = rem - 1;
+      if (d > remaining - nv[p] - nv[i]) d = remaining - nv[p] - nv[i];
       if (d < 0) d = 0;
+      dnew[i] = (int)d;
+      hsh[i] = h;
       queue.remove(i);
-      queue.insert(i, (int)d);
     }
+    // Supervariables: columns of Lp with the same element set are merged
+    // into the first of them (by index); the principal's external degree
+    // no longer counts the merged weight.
+    byhash.assign(Lp.begin(), Lp.end());
+    std::sort(byhash.begin(), byhash.end(), [&](int a, int b) {
+      if (hsh[a] != hsh[b]) return hsh[a] < hsh[b];
+      if (Ei[a].size() != Ei[b].size()) return Ei[a].size() < Ei[b].size();
+      return a < b;
+    });
+    for (size_t a = 0; a < byhash.size();) {
+      size_t b = a + 1;
+      while (b < byhash.size() && hsh[byhash[b]] == hsh[byhash[a]] &&
+             Ei[byhash[b]].size() == Ei[byhash[a]].size())
+        b++;
+      for (size_t u = a; u + 1 < b; u++) {
+        const int i = byhash[u];
+        if (!nv[i]) continue;
+        estamp++;
+        for (int e : Ei[i]) emark[e] = estamp;
+        for (size_t t = u + 1; t < b; t++) {
+          const int j = byhash[t];
+          if (!nv[j]) continue;
+          bool same = true;
+          for (int e : Ei[j])
+            if (emark[e] != estamp) {
+              same = false;
+              break;
+            }
+          if (!same) continue;
+          nv[i] += nv[j];
+          dnew[i] = std::max(0, dnew[i] - nv[j]);
+          nv[j] = 0;
+          alive[j] = 0;
+          svnext[svtail[i]] = j;
+          svtail[i] = svtail[j];
+          std::vector<int>().swap(Ei[j]);
+        }
+      }
+      a = b;
+    }
+    for (int i : Lp)
+      if (nv[i]) queue.insert(i, dnew[i]);
   }
   return order;
 }

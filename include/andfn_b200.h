@@ -242,7 +242,9 @@ int andfn_b200_fp64_peak(int32_t device, double *tflops);
  * default 8192; 0 turns it off) and gives its memory back when an
  * allocation fails.  release_cached_memory() frees every cached block of
  * every device; cached_memory() reports the bytes held on `device` and the
- * cache's hits and misses since the process started. */
+ * cache's hits and misses since the process started.  The page-locked host
+ * blocks that stage the Schur complement of a factorisation are cached the
+ * same way (ANDFN_B200_PINNED_POOL_MB, default 1024) and released with them. */
 void andfn_b200_release_cached_memory(void);
 int andfn_b200_cached_memory(int32_t device, int64_t *bytes, int64_t *hits, int64_t *misses);
 

@@ -203,3 +203,28 @@ def test_cluster_solve_of_large_realizations_is_bitwise_the_single_cta_solve(mon
         for name in ("coef", "q", "error", "error_coef", "dpsi_corr", "ncoef", "nint"):
             assert np.array_equal(b1[r][1][name], b2[r][1][name], equal_nan=True), (r, name)
         assert np.array_equal(b1[r][0]["constant"], b2[r][0]["constant"]), r
+
+
+def test_active_work_lists_are_bitwise_the_full_launches(monkeypatch):
+    """A batch's per-iteration kernels run over lists of the running
+    realizations' rows, sweep items and elements, rebuilt when one finishes;
+    every entry is computed as in the full launches (where finished
+    realizations return at entry), so the results are the same bit for bit,
+    with realizations that stop at different iterations."""
+    import andfn_b200
+    from andfn_b200 import network as nw
+    from andfn_b200.records import default_constants
+    recs = nw.to_records_batch([nw.batch_realization(3000 + i) for i in range(16)])
+    c = default_constants(MAX_ITERATIONS=120, MAX_ERROR=1e-8, MAX_NCOEF=15)
+    out = {}
+    for flag in ("0", "1"):
+        monkeypatch.setenv("ANDFN_B200_ACTIVE_LISTS", flag)
+        batch = [(F.copy(), E.copy()) for F, E in recs]
+        out[flag] = (batch, andfn_b200.solve_batch(batch, 50, c))
+    (b0, s0), (b1, s1) = out["0"], out["1"]
+    assert len({s["iterations"] for s in s1}) > 3  # realizations finish at different iterations
+    for r in range(len(recs)):
+        assert s0[r]["iterations"] == s1[r]["iterations"] and s0[r]["status"] == s1[r]["status"], r
+        for name in ("coef", "q", "error", "error_coef", "dpsi_corr", "ncoef", "nint"):
+            assert np.array_equal(b0[r][1][name], b1[r][1][name], equal_nan=True), (r, name)
+        assert np.array_equal(b0[r][0]["constant"], b1[r][0]["constant"]), r

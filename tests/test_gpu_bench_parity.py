@@ -144,3 +144,27 @@ def test_large_network_matches_reference_and_oracle():
     Fo, Eo = F0.copy(), E0.copy()
     orc.solve(Fo, Eo, 50, c)
     _compare_oracle(E, F, Eo, Fo, ("bench_c5 vs oracle", 3))
+
+
+@pytest.mark.parametrize("name", ["bench_c2", "bench_c5"])
+def test_one_launch_dense_lu_is_bitwise_the_three_kernel_lu(name, monkeypatch):
+    """The Schur complement's dense LU in one cooperative launch (look-ahead
+    panel on CTA 0, bounded grid barriers) computes every product and
+    quotient of the three-launch path in the same order: a solve through
+    either gives the same state bit for bit."""
+    from andfn_b200.records import default_constants
+    _, F0, E0 = golden_and_records(name)
+    mc = 20 if name == "bench_c2" else 30
+    c = default_constants(MAX_ITERATIONS=3, MAX_ERROR=1e-300, MAX_NCOEF=mc)
+    out = {}
+    for coop in ("0", "1"):
+        monkeypatch.setenv("ANDFN_B200_DLU_COOP", coop)
+        F, E = F0.copy(), E0.copy()
+        st = _gpu_solve(F, E, c)
+        assert st["dense_tail"] >= 64, st["dense_tail"]
+        out[coop] = (F, E, st)
+    (F1, E1, s1), (F2, E2, s2) = out["0"], out["1"]
+    assert s2["gpu_launches"] < s1["gpu_launches"]
+    for field in ("coef", "q", "error", "error_coef", "dpsi_corr"):
+        assert np.array_equal(E1[field], E2[field], equal_nan=True), field
+    assert np.array_equal(F1["constant"], F2["constant"])
