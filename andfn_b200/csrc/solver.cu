@@ -565,8 +565,8 @@ __device__ __forceinline__ void sweep_table_item(const Net &net, const Item it, 
 
 // One CTA per item (the hardware block scheduler hands out the items, which
 // are sorted by estimated cost, largest first).
-// With an active list (batches), CTA i takes item alist[i] while i is below
-// the list's length *acount, and returns otherwise.
+// With an active list (batches), the CTAs walk the list's items
+// (grid-stride, the list's length *acount on the device).
 __global__ void __launch_bounds__(EVAL_THREADS) sweep_table_kernel(Net net, const Item *__restrict__ items,
                                                                      const int2 *__restrict__ pts,
                                                                      const Group *__restrict__ groups,
@@ -578,12 +578,13 @@ __global__ void __launch_bounds__(EVAL_THREADS) sweep_table_kernel(Net net, cons
                                                                      double *__restrict__ out, int chunk,
                                                                      const int *__restrict__ alist,
                                                                      const int *__restrict__ acount) {
-  int i = blockIdx.x;
-  if (alist) {
-    if (i >= *acount) return;
-    i = alist[i];
+  if (alist) {  // grid-stride over the list (uniform over the CTA)
+    const int n = *acount;
+    for (int i = blockIdx.x; i < n; i += gridDim.x)
+      sweep_table_item(net, items[alist[i]], pts, groups, fpt0, fnp, tab_off, tw, tl, out, chunk);
+    return;
   }
-  sweep_table_item(net, items[i], pts, groups, fpt0, fnp, tab_off, tw, tl, out, chunk);
+  sweep_table_item(net, items[blockIdx.x], pts, groups, fpt0, fnp, tab_off, tw, tl, out, chunk);
 }
 
 // Persistent form: a grid of a few CTAs per SM takes the items (largest
@@ -632,7 +633,10 @@ __global__ void __launch_bounds__(EVAL_THREADS) sweep_table_queue_kernel(
 // nothing changed return at entry.
 // ------------------------------------------------------------------------
 static constexpr int ACT_CHUNK = 1024;
-static constexpr int ACT_LISTS = 3;  // head-vector rows, sweep items, updated elements
+// head-vector rows, sweep items, updated elements, realizations solved on a
+// cluster (a prefix of the size order), realizations solved by one CTA (the
+// rest of it), all realizations (the reduction)
+static constexpr int ACT_LISTS = 6;
 
 struct ActState {
   int seen;         // ndone when the lists were last built
@@ -646,14 +650,21 @@ struct ActLists {
   int *list[ACT_LISTS];   // active entries (indices into the full list)
   int *ccnt;              // active entries per chunk, all lists
   const Item *items;      // the sweep items (list 1's realization lookup)
+  const int *order;       // realizations by decreasing size (lists 3 and 4), or null
+  int nbig;               // realizations solved on a cluster (list 3's length)
   ActState *st;
 };
 
 // the realization of entry i of list l
 __device__ __forceinline__ int act_real(const Net &net, const ActLists &A, int l, int i) {
-  if (l == 0) return net.real_row[i];
-  if (l == 1) return net.real_frac[A.items[i].frac];
-  return net.real_elem[i];
+  switch (l) {
+    case 0: return net.real_row[i];
+    case 1: return net.real_frac[A.items[i].frac];
+    case 2: return net.real_elem[i];
+    case 3: return A.order[i];
+    case 4: return A.order[A.nbig + i];
+    default: return i;
+  }
 }
 
 __device__ __forceinline__ void act_locate(const ActLists &A, int &l, int &c) {
@@ -794,6 +805,12 @@ __device__ __forceinline__ void dft_basis(const double *v0, const double *v1, in
   }
 }
 
+__device__ __forceinline__ void update_element(Net &net, int e, const int *__restrict__ group_of,
+                                               const Group *__restrict__ groups, const double *__restrict__ vals,
+                                               double *v0, double *v1, int blend_mode);
+
+// One warp per element of the list; with an active list (batches: its
+// length *ncount on the device) the warps walk the list (grid-stride).
 __global__ void __launch_bounds__(UPDATE_WARPS * 32) update_kernel(Net net, const int *__restrict__ elist, int nlist,
                                                                     const int *__restrict__ group_of,
                                                                     const Group *__restrict__ groups,
@@ -801,13 +818,26 @@ __global__ void __launch_bounds__(UPDATE_WARPS * 32) update_kernel(Net net, cons
                                                                     int blend_mode,
                                                                     const int *__restrict__ ncount = nullptr) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
   double *v0 = reinterpret_cast<double *>(smem_raw) + (size_t)warp * 2 * nvmax;
   double *v1 = v0 + nvmax;
   const int idx = blockIdx.x * UPDATE_WARPS + warp;
-  if (ncount) nlist = *ncount;  // a batch's active element list: its length on the device
+  if (ncount) {
+    const int n = *ncount;
+    for (int i = idx; i < n; i += gridDim.x * UPDATE_WARPS) {
+      __syncwarp();  // the previous element's reads of v0 / v1 are done
+      update_element(net, elist[i], group_of, groups, vals, v0, v1, blend_mode);
+    }
+    return;
+  }
   if (idx >= nlist) return;
-  const int e = elist[idx];
+  update_element(net, elist[idx], group_of, groups, vals, v0, v1, blend_mode);
+}
+
+__device__ __forceinline__ void update_element(Net &net, int e, const int *__restrict__ group_of,
+                                               const Group *__restrict__ groups, const double *__restrict__ vals,
+                                               double *v0, double *v1, int blend_mode) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   SolveState *st = net.st + net.real_elem[e];
   if (st->done) return;
   const int type = net.type[e];
@@ -1105,17 +1135,30 @@ __device__ __forceinline__ void reduce_finish(Net &net, SolveState *st, const Er
   st->solve_q = (st->error_q > st->max_error / 1e30) ? 1 : 0;
 }
 
-// One CTA per realization.
-__global__ void __launch_bounds__(1024) reduce_kernel(Net net) {
-  const int r = blockIdx.x;
+__device__ __forceinline__ void reduce_one(Net &net, int r) {
   SolveState *st = net.st + r;
-  if (st->done) return;
+  if (st->done) return;  // uniform over the CTA
   ErrAcc a;
   const int e0 = net.eoff[r], e1 = net.eoff[r + 1];
 #pragma unroll 4
   for (int i = e0 + threadIdx.x; i < e1; i += blockDim.x) a.add(net.err[i], net.err_coef[i], i);
   block_merge<1024>(a);
   if (threadIdx.x == 0) reduce_finish(net, st, a, e0);
+}
+
+// One CTA per realization; with an active list (batches: its length
+// *acount on the device) the CTAs walk the running realizations.
+__global__ void __launch_bounds__(1024) reduce_kernel(Net net, const int *__restrict__ alist = nullptr,
+                                                      const int *__restrict__ acount = nullptr) {
+  if (alist) {
+    const int n = *acount;
+    for (int i = blockIdx.x; i < n; i += gridDim.x) {
+      __syncthreads();  // the previous realization's merge is read
+      reduce_one(net, alist[i]);
+    }
+    return;
+  }
+  reduce_one(net, blockIdx.x);
 }
 
 // A single network's reduction over several CTAs (REDUCE_SPLIT_ELEMS
@@ -2785,14 +2828,23 @@ __global__ void __launch_bounds__(WINV_THREADS) winv_upper_kernel(TriDesc TD, do
 // zeroes them for the next solve); the adjoint (ADJ: X holds the transposed
 // inverse, P and Q those of the transposed system, no refinement) writes
 // net.disc only.
+//
+// F32 (the refinement pass): X is read from a float copy (X32, the same
+// layout), each entry widened to double before its product.  The pass forms
+// the correction X r of a residual r that is about 1e-10 of b: single
+// precision entries (relative error 6e-8) leave an error near 1e-17 of x,
+// well below the double-precision pass's own (mixed-precision iterative
+// refinement: the residual in double, the correction in single).  Half the
+// bytes of that pass.
 static constexpr int WINV_RPC = 64;
 static_assert(WINV_THREADS == 512, "16 warps split each row of X");
 
-template <int STAGE, bool ADJ>
+template <int STAGE, bool ADJ, bool F32 = false>
 __global__ void __launch_bounds__(WINV_THREADS, 2) winv_gemv_kernel(Net net, const double *__restrict__ X, int ldw,
                                                                  const double *__restrict__ src,
                                                                  double *__restrict__ x0,
-                                                                 unsigned long long *__restrict__ acc) {
+                                                                 unsigned long long *__restrict__ acc,
+                                                                 const float *__restrict__ X32 = nullptr) {
   SolveState *st = net.st;
   if (st->done) return;
   // forward: without refinement (refine is set when the run starts) the
@@ -2823,25 +2875,49 @@ __global__ void __launch_bounds__(WINV_THREADS, 2) winv_gemv_kernel(Net net, con
   // row's segment in two halves of 32 double2), half the latency rounds of
   // two rows at a time; rows beyond r1 reread row k (results not stored)
   for (int k = r0; k < r1; k += 4) {
-    const double2 *ra = reinterpret_cast<const double2 *>(X + (size_t)k * ldw) + warp * seg;
-    const double2 *rb = (k + 1 < r1) ? ra + ldw / 2 : ra;
-    const double2 *rc = (k + 2 < r1) ? ra + ldw : ra;
-    const double2 *rd = (k + 3 < r1) ? ra + 3 * (size_t)(ldw / 2) : ra;
     double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0, c0 = 0.0, c1 = 0.0, d0 = 0.0, d1 = 0.0;
-    for (int j = lane; j < seg; j += 64) {
-      const bool h = j + 32 < seg;
-      const double2 wa0 = __ldcs(ra + j), wb0 = __ldcs(rb + j), wc0 = __ldcs(rc + j), wd0 = __ldcs(rd + j);
-      const double2 wa1 = h ? __ldcs(ra + j + 32) : zero2, wb1 = h ? __ldcs(rb + j + 32) : zero2;
-      const double2 wc1 = h ? __ldcs(rc + j + 32) : zero2, wd1 = h ? __ldcs(rd + j + 32) : zero2;
-      const double2 x0v = vs[j], x1v = h ? vs[j + 32] : zero2;
-      a0 = fma(wa0.y, x0v.y, fma(wa0.x, x0v.x, a0));
-      b0 = fma(wb0.y, x0v.y, fma(wb0.x, x0v.x, b0));
-      c0 = fma(wc0.y, x0v.y, fma(wc0.x, x0v.x, c0));
-      d0 = fma(wd0.y, x0v.y, fma(wd0.x, x0v.x, d0));
-      a1 = fma(wa1.y, x1v.y, fma(wa1.x, x1v.x, a1));
-      b1 = fma(wb1.y, x1v.y, fma(wb1.x, x1v.x, b1));
-      c1 = fma(wc1.y, x1v.y, fma(wc1.x, x1v.x, c1));
-      d1 = fma(wd1.y, x1v.y, fma(wd1.x, x1v.x, d1));
+    if (F32) {
+      // float4 loads (four entries, 16 B): this warp's segment of a row is
+      // seg / 2 of them (ldw is a multiple of 64 when the float copy exists)
+      const int seg4 = seg / 2;
+      const size_t rf = ldw / 4;
+      const float4 *fa = reinterpret_cast<const float4 *>(X32) + (size_t)k * rf + (size_t)warp * seg4;
+      const float4 *fb = (k + 1 < r1) ? fa + rf : fa, *fc = (k + 2 < r1) ? fa + 2 * rf : fa,
+                   *fd = (k + 3 < r1) ? fa + 3 * rf : fa;
+      // one float4 of each of the four rows in flight per lane (64 B: the
+      // same bytes in flight per lane as the double pass's first half, in
+      // the register budget of two CTAs an SM)
+      for (int j = lane; j < seg4; j += 32) {
+        const float4 wa = __ldcs(fa + j), wb = __ldcs(fb + j), wc = __ldcs(fc + j), wd = __ldcs(fd + j);
+        const double2 p = vs[2 * j], q = vs[2 * j + 1];
+#define WINV_F4(ACC, F) \
+  ACC = fma((double)F.w, q.y, fma((double)F.z, q.x, fma((double)F.y, p.y, fma((double)F.x, p.x, ACC))))
+        WINV_F4(a0, wa);
+        WINV_F4(b0, wb);
+        WINV_F4(c0, wc);
+        WINV_F4(d0, wd);
+#undef WINV_F4
+      }
+    } else {
+      const double2 *ra = reinterpret_cast<const double2 *>(X + (size_t)k * ldw) + warp * seg;
+      const double2 *rb = (k + 1 < r1) ? ra + ldw / 2 : ra;
+      const double2 *rc = (k + 2 < r1) ? ra + ldw : ra;
+      const double2 *rd = (k + 3 < r1) ? ra + 3 * (size_t)(ldw / 2) : ra;
+      for (int j = lane; j < seg; j += 64) {
+        const bool h = j + 32 < seg;
+        const double2 wa0 = __ldcs(ra + j), wb0 = __ldcs(rb + j), wc0 = __ldcs(rc + j), wd0 = __ldcs(rd + j);
+        const double2 wa1 = h ? __ldcs(ra + j + 32) : zero2, wb1 = h ? __ldcs(rb + j + 32) : zero2;
+        const double2 wc1 = h ? __ldcs(rc + j + 32) : zero2, wd1 = h ? __ldcs(rd + j + 32) : zero2;
+        const double2 x0v = vs[j], x1v = h ? vs[j + 32] : zero2;
+        a0 = fma(wa0.y, x0v.y, fma(wa0.x, x0v.x, a0));
+        b0 = fma(wb0.y, x0v.y, fma(wb0.x, x0v.x, b0));
+        c0 = fma(wc0.y, x0v.y, fma(wc0.x, x0v.x, c0));
+        d0 = fma(wd0.y, x0v.y, fma(wd0.x, x0v.x, d0));
+        a1 = fma(wa1.y, x1v.y, fma(wa1.x, x1v.x, a1));
+        b1 = fma(wb1.y, x1v.y, fma(wb1.x, x1v.x, b1));
+        c1 = fma(wc1.y, x1v.y, fma(wc1.x, x1v.x, c1));
+        d1 = fma(wd1.y, x1v.y, fma(wd1.x, x1v.x, d1));
+      }
     }
     const double sa = warp_sum(a0 + a1), sb = warp_sum(b0 + b1), sc = warp_sum(c0 + c1), sd = warp_sum(d0 + d1);
     if (lane == 0) {
@@ -3293,11 +3369,33 @@ __device__ __forceinline__ void binv_gemv(const double *__restrict__ X, int n, c
   binv_gemv_rows(X, n, n, v, out);
 }
 
+__device__ __forceinline__ void batch_winv_solve_one(Net &net, int r, const int *__restrict__ roff,
+                                                     const long long *__restrict__ xoff,
+                                                     const double *__restrict__ Xall, const int *__restrict__ ptr,
+                                                     const int *__restrict__ col, const double *__restrict__ vals);
+
+// One CTA per realization of order[]; with an active list (alist of
+// positions in order[], its length *acount on the device) the CTAs walk the
+// list (grid-stride).
 __global__ void __launch_bounds__(BINV_SOLVE_THREADS) batch_winv_solve_kernel(
     Net net, const int *__restrict__ order, const int *__restrict__ roff, const long long *__restrict__ xoff,
     const double *__restrict__ Xall, const int *__restrict__ ptr, const int *__restrict__ col,
-    const double *__restrict__ vals) {
-  const int r = order[blockIdx.x];
+    const double *__restrict__ vals, const int *__restrict__ alist = nullptr, const int *__restrict__ acount = nullptr) {
+  if (alist) {
+    const int n = *acount;
+    for (int i = blockIdx.x; i < n; i += gridDim.x) {
+      __syncthreads();  // the previous realization's shared memory reads are done
+      batch_winv_solve_one(net, order[alist[i]], roff, xoff, Xall, ptr, col, vals);
+    }
+    return;
+  }
+  batch_winv_solve_one(net, order[blockIdx.x], roff, xoff, Xall, ptr, col, vals);
+}
+
+__device__ __forceinline__ void batch_winv_solve_one(Net &net, int r, const int *__restrict__ roff,
+                                                     const long long *__restrict__ xoff,
+                                                     const double *__restrict__ Xall, const int *__restrict__ ptr,
+                                                     const int *__restrict__ col, const double *__restrict__ vals) {
   SolveState *st = net.st + r;
   if (st->done) return;
   if (threadIdx.x == 0) st->nit += 1;
@@ -3370,13 +3468,35 @@ __global__ void __launch_bounds__(BINV_SOLVE_THREADS) batch_winv_solve_kernel(
 //      (so xp may take the correction);
 //   3. every CTA's partial maxima are written;
 //   4. CTA 0 has read them (no CTA leaves while its shared memory is read).
+__device__ __forceinline__ void batch_winv_solve_cluster_one(Net &net, int r, const int *__restrict__ roff,
+                                                             const long long *__restrict__ xoff,
+                                                             const double *__restrict__ Xall,
+                                                             const int *__restrict__ ptr, const int *__restrict__ col,
+                                                             const double *__restrict__ vals);
+
+// One cluster per realization of big[]; with an active list (positions in
+// big[], its length *acount on the device) the clusters walk the list
+// (every CTA of a cluster takes the same realizations).
 __global__ void __launch_bounds__(BINV_SOLVE_THREADS) batch_winv_solve_cluster_kernel(
     Net net, const int *__restrict__ big, const int *__restrict__ roff, const long long *__restrict__ xoff,
     const double *__restrict__ Xall, const int *__restrict__ ptr, const int *__restrict__ col,
-    const double *__restrict__ vals) {
+    const double *__restrict__ vals, const int *__restrict__ alist, const int *__restrict__ acount) {
+  const int cid = blockIdx.x / BINV_CLUSTER, ncl = gridDim.x / BINV_CLUSTER;
+  if (alist) {
+    const int n = *acount;
+    for (int i = cid; i < n; i += ncl) batch_winv_solve_cluster_one(net, big[alist[i]], roff, xoff, Xall, ptr, col, vals);
+    return;
+  }
+  batch_winv_solve_cluster_one(net, big[cid], roff, xoff, Xall, ptr, col, vals);
+}
+
+__device__ __forceinline__ void batch_winv_solve_cluster_one(Net &net, int r, const int *__restrict__ roff,
+                                                             const long long *__restrict__ xoff,
+                                                             const double *__restrict__ Xall,
+                                                             const int *__restrict__ ptr, const int *__restrict__ col,
+                                                             const double *__restrict__ vals) {
   cg::cluster_group cluster = cg::this_cluster();
   const int crank = (int)cluster.block_rank();
-  const int r = big[blockIdx.x / BINV_CLUSTER];
   SolveState *st = net.st + r;
   if (st->done) return;
   if (crank == 0 && threadIdx.x == 0) st->nit += 1;
@@ -3979,6 +4099,9 @@ template <class T>
 struct DBuf {
   T *p = nullptr;
   size_t n = 0, cap = 0;
+  DBuf() = default;
+  DBuf(const DBuf &) = delete;  // one owner per block (the cache would hand out a doubly released block twice)
+  DBuf &operator=(const DBuf &) = delete;
   cudaError_t alloc(size_t count) {
     n = count;
     if (count <= cap && p) return cudaSuccess;
@@ -4181,6 +4304,8 @@ struct AndfnHandle {
   // explicit inverse of a single network's system (pivot order, rows padded
   // to winv_ldw), the system's CSR pattern and the solve's work arrays
   DBuf<double> winv, winv_t, wx0, wr;
+  DBuf<float> winv32;  // float copy of winv for the refinement pass
+  float *winv32_p = nullptr;
   DBuf<int> a_ptr, a_col;
   DBuf<unsigned long long> wacc;
   int winv_ldw = 0, num_sms = 148;
@@ -4239,7 +4364,7 @@ struct AndfnHandle {
   DBuf<ReducePart> red_parts;
   DBuf<unsigned> red_ticket;
   // a batch's active work lists (rows, sweep items, elements) and their state
-  DBuf<int> act_l[3], act_ccnt;
+  DBuf<int> act_l[ACT_LISTS], act_ccnt;
   DBuf<ActState> act_st;
   ActLists act{};
   bool act_on = false;
@@ -5032,6 +5157,10 @@ static int create_impl(AndfnHandle *H, int R, const char *const *F, const int64_
                           (int)(sizeof(double) * WINV_MAX_N)));
   CK(cudaFuncSetAttribute(winv_gemv_kernel<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)(sizeof(double) * WINV_MAX_N)));
+  CK(cudaFuncSetAttribute(winv_gemv_kernel<1, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)(sizeof(double) * WINV_MAX_N)));
+  CK(cudaFuncSetAttribute(winv_gemv_kernel<1, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)(sizeof(double) * WINV_MAX_N)));
   CK(cudaFuncSetAttribute(update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
   rc = reset_impl(H);
   if (rc) return rc;
@@ -5222,13 +5351,15 @@ static int gpu_dense_lu(AndfnHandle *H, LuFactors &F, bool want_w) {
   return sparse_lu_finish(F, piv, dg);
 }
 
+static float *make_winv_f32(AndfnHandle *H, DBuf<float> &Y, const double *X, size_t n);
+
 // Forms the explicit inverse of a single network's factorised system (its
 // TriDesc, dense-tail inverse in H->tail_w) when the device has room for it,
 // and the CSR pattern of the system for the refinement step.
 static int build_inverse(AndfnHandle *H, const TriDesc &td) {
   cudaStream_t s = H->stream;
   const int N = td.n, K = td.T.K, m0 = N - K;
-  const int ldw = (N + 31) / 32 * 32;
+  const int ldw = (N + 63) / 64 * 64;  // rows of 64-entry multiples: 512 B (double) / 256 B (float) aligned
   const size_t xbytes = sizeof(double) * (size_t)N * ldw, tbytes = sizeof(double) * (size_t)std::max(1, K) * ldw;
   // free device memory is queried only when the buffers have to grow (a
   // driver query per run would contend with monitoring tools)
@@ -5264,6 +5395,7 @@ static int build_inverse(AndfnHandle *H, const TriDesc &td) {
   CK(cudaMemsetAsync(H->wacc.p, 0, sizeof(unsigned long long) * 3, s));
   H->winv_ldw = ldw;
   H->winv_ready = true;
+  H->winv32_p = make_winv_f32(H, H->winv32, H->winv.p, (size_t)N * ldw);
   return 0;
 }
 
@@ -5717,7 +5849,7 @@ static int tri_launches(const AndfnHandle *H) { return H->winv_ready ? 3 : 1; } 
 // or A^T in CSR form (map: value index of each entry, null = entry order).
 template <bool ADJ>
 static void launch_winv_solve(AndfnHandle *H, const Net &net, cudaStream_t s, const double *X, const int *rp,
-                              const int *cols, const int *map) {
+                              const int *cols, const int *map, const float *X32 = nullptr) {
   const int N = H->N, ldw = H->winv_ldw;
   const size_t vsm = sizeof(double) * (size_t)ldw;
   // two CTAs of 512 threads per SM, at most WINV_RPC rows per CTA
@@ -5725,7 +5857,44 @@ static void launch_winv_solve(AndfnHandle *H, const Net &net, cudaStream_t s, co
   winv_gemv_kernel<0, ADJ><<<grid, WINV_THREADS, vsm, s>>>(net, X, ldw, net.bvec, H->wx0.p, H->wacc.p);
   winv_resid_kernel<ADJ><<<(N * 32 + 255) / 256, 256, 0, s>>>(net, rp, cols, map, H->d_mvals.p + H->sys[0].ent0,
                                                              H->wx0.p, H->wr.p, N);
-  winv_gemv_kernel<1, ADJ><<<grid, WINV_THREADS, vsm, s>>>(net, X, ldw, H->wr.p, H->wx0.p, H->wacc.p);
+  if (X32)
+    winv_gemv_kernel<1, ADJ, true><<<grid, WINV_THREADS, vsm, s>>>(net, X, ldw, H->wr.p, H->wx0.p, H->wacc.p, X32);
+  else
+    winv_gemv_kernel<1, ADJ><<<grid, WINV_THREADS, vsm, s>>>(net, X, ldw, H->wr.p, H->wx0.p, H->wacc.p);
+}
+
+// A float copy of an N x ldw inverse for the refinement pass.
+__global__ void winv_to_f32_kernel(const double *__restrict__ X, float *__restrict__ Y, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    Y[i] = (float)X[i];
+}
+
+// Whether the refinement passes read float copies of the inverses
+// (ANDFN_B200_WINV_F32=0 when the inverse is formed: the double inverse in
+// both passes).
+static bool winv_f32_enabled() {
+  const char *e = getenv("ANDFN_B200_WINV_F32");
+  return !(e && atoi(e) == 0);
+}
+
+// The float copy of X (N x ldw) when the device has room for it, else null.
+static float *make_winv_f32(AndfnHandle *H, DBuf<float> &Y, const double *X, size_t n) {
+  if (!winv_f32_enabled()) return nullptr;
+  if (Y.cap < n) {
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    if (sizeof(float) * n + ((size_t)1 << 30) > fr + sizeof(float) * Y.cap) return nullptr;
+  }
+  if (Y.alloc(n) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  winv_to_f32_kernel<<<4 * H->num_sms, 256, 0, H->stream>>>(X, Y.p, n);
+  H->launches += 1;
+  return Y.p;
 }
 
 static void launch_trisolve(AndfnHandle *H, cudaStream_t s) {
@@ -5733,7 +5902,10 @@ static void launch_trisolve(AndfnHandle *H, cudaStream_t s) {
   if (H->binv_ready) {
     // binv_order lists the realizations by decreasing size: the first
     // binv_ncsolve of them are solved by a cluster each, the rest by one CTA
+    // with active lists (every batch iteration loop) the CTAs take the
+    // running realizations from the lists
     const int nc = H->binv_ncsolve;
+    const bool act = H->act_on;
     if (nc > 0) {
       cudaLaunchConfig_t cfg = {};
       cudaLaunchAttribute attr[1];
@@ -5750,14 +5922,15 @@ static void launch_trisolve(AndfnHandle *H, cudaStream_t s) {
       const cudaError_t ce = cudaLaunchKernelEx(
           &cfg, batch_winv_solve_cluster_kernel, net, (const int *)H->binv_order.p, (const int *)H->binv_roff.p,
           (const long long *)H->binv_off.p, (const double *)H->binv.p, (const int *)H->bcsr_ptr.p,
-          (const int *)H->bcsr_col.p, (const double *)H->d_mvals.p);
+          (const int *)H->bcsr_col.p, (const double *)H->d_mvals.p, act ? (const int *)H->act.list[3] : nullptr,
+          act ? (const int *)&H->act.st->count[3] : nullptr);
       if (ce != cudaSuccess) set_error(std::string("batched cluster solve launch: ") + cudaGetErrorString(ce));
       H->launches += 1;
     }
     if (H->R > nc) {
       batch_winv_solve_kernel<<<H->R - nc, BINV_SOLVE_THREADS, 24 * (size_t)H->binv_maxn, s>>>(
           net, H->binv_order.p + nc, H->binv_roff.p, H->binv_off.p, H->binv.p, H->bcsr_ptr.p, H->bcsr_col.p,
-          H->d_mvals.p);
+          H->d_mvals.p, act ? H->act.list[4] : nullptr, act ? &H->act.st->count[4] : nullptr);
       H->launches += 1;
     }
     const cudaError_t le = cudaGetLastError();
@@ -5765,7 +5938,7 @@ static void launch_trisolve(AndfnHandle *H, cudaStream_t s) {
     return;
   }
   if (H->winv_ready) {
-    launch_winv_solve<false>(H, net, s, H->winv.p, H->a_ptr.p, H->a_col.p, nullptr);
+    launch_winv_solve<false>(H, net, s, H->winv.p, H->a_ptr.p, H->a_col.p, nullptr, H->winv32_p);
     const cudaError_t le = cudaGetLastError();
     if (le != cudaSuccess) set_error(std::string("explicit-inverse solve launch: ") + cudaGetErrorString(le));
     return;
@@ -6013,6 +6186,8 @@ static int enqueue_iteration(AndfnHandle *H, cudaStream_t s, int blend_mode, int
   if (H->R == 1 && H->red_parts.p)
     reduce_split_kernel<<<(int)((H->ne + REDUCE_SPLIT_ELEMS - 1) / REDUCE_SPLIT_ELEMS), REDUCE_SPLIT_THREADS, 0, s>>>(
         net, H->red_parts.p, H->red_ticket.p);
+  else if (H->act_on)
+    reduce_kernel<<<H->R, 1024, 0, s>>>(net, H->act.list[5], &H->act.st->count[5]);
   else
     reduce_kernel<<<H->R, 1024, 0, s>>>(net);
   if (H->act_on) {  // the active lists of the next iteration (launches return at entry unless one finished)
@@ -6030,8 +6205,12 @@ static int enqueue_iteration(AndfnHandle *H, cudaStream_t s, int blend_mode, int
 // element list relies on the update list being every element in order.
 static int act_setup(AndfnHandle *H, int ndone0) {
   cudaStream_t s = H->stream;
-  const int n[ACT_LISTS] = {(int)H->N, H->n_sweep_items, H->n_upd};
+  const int nbig = H->binv_ready ? H->binv_ncsolve : 0;
+  const int nsmall = H->binv_ready ? H->R - nbig : 0;
+  const int n[ACT_LISTS] = {(int)H->N, H->n_sweep_items, H->n_upd, nbig, nsmall, H->R};
   ActLists &A = H->act;
+  A.order = H->binv_ready ? H->binv_order.p : nullptr;
+  A.nbig = nbig;
   int c0 = 0;
   for (int l = 0; l < ACT_LISTS; l++) {
     A.n[l] = n[l];
@@ -6046,7 +6225,7 @@ static int act_setup(AndfnHandle *H, int ndone0) {
   A.ccnt = H->act_ccnt.p;
   A.items = H->sweep_items.p;
   A.st = H->act_st.p;
-  const int mx = std::max({n[0], n[1], n[2], 1});
+  const int mx = std::max({n[0], n[1], n[2], n[5], 1});
   act_init_kernel<<<std::min(4 * H->num_sms, (mx + 255) / 256), 256, 0, s>>>(A, ndone0);
   CK(cudaGetLastError());
   H->launches += 1;
@@ -6426,6 +6605,7 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
     st.sweep_variant = H->use_tab ? H->sweep_variant : -1;
     st.loop_launches = loop_launches;
     st.ms_alloc = g_alloc_ms;
+    st.refine_f32 = (H->winv_ready && H->winv32_p) ? 1 : 0;
     st.levels_l = H->sys[r].nlev_l;
     st.levels_u = H->sys[r].nlev_u;
     for (int i = 0; i < 8; i++) st.tri_cycles[i] = f.tri_cycles[i];
@@ -7298,6 +7478,8 @@ struct AdjBufs {
   // transposed explicit inverse (rows padded like the forward one) and A^T
   // in CSR form (value index of each entry in A's entry order)
   DBuf<double> xt;
+  DBuf<float> xt32;  // float copy of xt for the refinement pass
+  float *xt32_p = nullptr;
   DBuf<int> at_ptr, at_col, at_map;
   bool use_winv = false;
   DBuf<Item> items_sw;
@@ -7787,23 +7969,14 @@ __device__ __forceinline__ double hv_group_sum(double v, double *red) {
   for (int w = 0; w < T / 32; w++) t += red[w];
   return t;
 }
-template <int T, int RPB>
-__global__ void __launch_bounds__(T * RPB) head_vector_kernel(Net net, const int *__restrict__ gptr,
-                                                               const int *__restrict__ sidx,
-                                                               const cd *__restrict__ S,
-                                                               const int *__restrict__ alist,
-                                                               const int *__restrict__ acount) {
-  __shared__ double red[T / 32 > 0 ? T / 32 : 1];
-  const int t = (T == 32) ? (threadIdx.x & 31) : threadIdx.x;
-  int g = blockIdx.x * RPB + ((T == 32) ? (threadIdx.x >> 5) : 0);
-  if (alist) {  // a batch's rows of running realizations
-    if (g >= *acount) return;  // uniform over the row's group
-    g = alist[g];
-  } else if (g >= net.N) {
-    return;
-  }
+// One row group (a warp for T = 32, the CTA otherwise) per row; with an
+// active list (batches) the groups walk the list's rows (grid-stride; the
+// list's length on the device), else one row each.
+template <int T>
+__device__ __forceinline__ void head_row(const Net &net, int g, int t, const int *__restrict__ gptr,
+                                         const int *__restrict__ sidx, const cd *__restrict__ S, double *red) {
   const SolveState *st = net.st + net.real_row[g];
-  if (st->done || !st->solve_q) return;
+  if (st->done || !st->solve_q) return;  // uniform over the row's group
   const int r = net.row_de[g];
   if (r < 0) {
     if (t == 0) net.bvec[g] = net.bknown ? net.bknown[g] : 0.0;
@@ -7839,6 +8012,23 @@ __global__ void __launch_bounds__(T * RPB) head_vector_kernel(Net net, const int
     else
       b = net.phi[e] - sum[0] / D;
     net.bvec[g] = net.bknown ? b + net.bknown[g] : b;
+  }
+}
+
+template <int T, int RPB>
+__global__ void __launch_bounds__(T * RPB) head_vector_kernel(Net net, const int *__restrict__ gptr,
+                                                               const int *__restrict__ sidx,
+                                                               const cd *__restrict__ S,
+                                                               const int *__restrict__ alist,
+                                                               const int *__restrict__ acount) {
+  __shared__ double red[T / 32 > 0 ? T / 32 : 1];
+  const int t = (T == 32) ? (threadIdx.x & 31) : threadIdx.x;
+  const int g0 = blockIdx.x * RPB + ((T == 32) ? (threadIdx.x >> 5) : 0);
+  if (alist) {  // a batch's rows of running realizations
+    const int n = *acount;
+    for (int v = g0; v < n; v += gridDim.x * RPB) head_row<T>(net, alist[v], t, gptr, sidx, S, red);
+  } else if (g0 < net.N) {
+    head_row<T>(net, g0, t, gptr, sidx, S, red);
   }
 }
 
@@ -8376,6 +8566,7 @@ static int adj_build_factors(AndfnHandle *H) {
   td.T.lscale = H->tail_uinv.p;
   td.T.W = nullptr;
   A.use_winv = false;
+  A.xt32_p = nullptr;
   if (H->winv_ready) {  // A^-T = (Q X P)^T: X^T with the transposed system's P and Q
     const int ldw = H->winv_ldw;
     const size_t xbytes = sizeof(double) * (size_t)n * ldw;
@@ -8387,6 +8578,7 @@ static int adj_build_factors(AndfnHandle *H) {
       transpose_ld_kernel<<<dim3((n + 31) / 32, (n + 31) / 32), dim3(32, 8), 0, s>>>(H->winv.p, ldw, n, n, A.xt.p,
                                                                                      ldw);
       CK(cudaGetLastError());
+      A.xt32_p = make_winv_f32(H, A.xt32, A.xt.p, (size_t)n * ldw);
       const RealSys &S = H->sys[0];
       std::vector<int> cp(n + 1, 0), ri(S.mcol.size()), mp(S.mcol.size());
       for (int c : S.mcol) cp[c + 1]++;
@@ -8429,7 +8621,7 @@ static int adj_build_factors(AndfnHandle *H) {
 static void launch_trisolve_adj(AndfnHandle *H, const Net &net, cudaStream_t s) {
   if (H->adj->use_winv) {
     const AdjBufs &A = *H->adj;
-    launch_winv_solve<true>(H, net, s, A.xt.p, A.at_ptr.p, A.at_col.p, A.at_map.p);
+    launch_winv_solve<true>(H, net, s, A.xt.p, A.at_ptr.p, A.at_col.p, A.at_map.p, A.xt32_p);
     return;
   }
   const size_t ybytes = sizeof(double) * (size_t)H->max_n;

@@ -95,7 +95,8 @@ class AndfnSolveStats(ctypes.Structure):
                 ("explicit_inverse", ctypes.c_int64), ("ms_factor_sparse", ctypes.c_double),
                 ("ms_factor_dense", ctypes.c_double), ("ms_factor_levels", ctypes.c_double),
                 ("ms_inverse", ctypes.c_double), ("refined_solves", ctypes.c_int64),
-                ("sweep_variant", ctypes.c_int64), ("loop_launches", ctypes.c_int64), ("ms_alloc", ctypes.c_double)]
+                ("sweep_variant", ctypes.c_int64), ("loop_launches", ctypes.c_int64), ("ms_alloc", ctypes.c_double),
+                ("refine_f32", ctypes.c_int64)]
 
     def as_dict(self) -> dict:
         d = {name: getattr(self, name) for name, _ in self._fields_}

@@ -341,18 +341,27 @@ def run_gpu(args):
         # second pass for the solves that took the refinement step
         ldw = (N + 31) // 32 * 32
         frac_ref = stats.get("refined_solves", 0) / max(1, stats.get("iterations", 1))
-        tri_bytes = (1.0 + frac_ref) * (8.0 * N * ldw + 4.0 * 8 * N) + frac_ref * 12.0 * stats.get("nnz_matrix", 0)
-        tri_note = (f"explicit inverse: one streaming pass per solve, a residual SpMV and a second pass in "
-                    f"{100 * frac_ref:.0f}% of the solves (the refinement step)")
+        # the refinement pass reads the float copy of the inverse when there is one
+        ref_entry = 4.0 if int(stats.get("refine_f32", 0)) == 1 else 8.0
+        tri_bytes = (8.0 * N * ldw + frac_ref * ref_entry * N * ldw + (1.0 + frac_ref) * 4.0 * 8 * N
+                     + frac_ref * 12.0 * stats.get("nnz_matrix", 0))
+        tri_note = (f"explicit inverse: one streaming pass per solve (f64), a residual SpMV and a second pass "
+                    f"({'f32' if ref_entry == 4.0 else 'f64'} copy) in {100 * frac_ref:.0f}% of the solves "
+                    f"(the refinement step)")
     else:
         tri_bytes = 12.0 * (nnz - 2.0 * K * K - N) + 8.0 * K * K + 24.0 * N
         tri_note = "latency-bound dependency chain (levels of L and U)"
     roof = {}
     # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch
-    # on this workload, from one ncu capture of the plain-solve profile case
-    # (discharge solve: one winv_gemv pass, times the passes a solve makes)
-    measured_traffic = {"eval_sweep": 5274112.0 + 0.0,
-                        "trisolve": (1.0 + frac_ref) * (231307520.0 + 3308800.0) if inverse else None}
+    # on this workload, from ncu captures of the plain-solve profile case
+    # (discharge solve: the double pass, plus the refinement pass over the
+    # float copy, or a second double pass without one, in the solves that
+    # refine)
+    pass64 = 231318784.0 + 1533440.0
+    pass32 = 115842304.0 + 456704.0
+    ref_pass = pass32 if inverse and int(stats.get("refine_f32", 0)) == 1 else pass64
+    measured_traffic = {"eval_sweep": 111.6e6 + 3.6e6,
+                        "trisolve": pass64 + frac_ref * ref_pass if inverse else None}
     if dom in ("eval_sweep", "eval_rhs"):
         fl = work["eval_sweep_flops"] if dom == "eval_sweep" else work["eval_rhs_flops"]
         ach = fl / (per[dom] * 1e-3) / 1e12

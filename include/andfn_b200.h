@@ -112,6 +112,7 @@ typedef struct AndfnSolveStats {
   double ms_alloc;          /* host milliseconds in device allocation and release on the calling
                                thread (andfn_b200_solve: the whole call; a run: since the thread's
                                previous one-call solve) */
+  int64_t refine_f32;       /* 1: the refinement pass read a float copy of the explicit inverse */
 } AndfnSolveStats;
 
 /* ---- one-call drop-in (replaces andfn/hpc/hpc_solve.py:55 solve) --------

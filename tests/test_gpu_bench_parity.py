@@ -168,3 +168,31 @@ def test_one_launch_dense_lu_is_bitwise_the_three_kernel_lu(name, monkeypatch):
     for field in ("coef", "q", "error", "error_coef", "dpsi_corr"):
         assert np.array_equal(E1[field], E2[field], equal_nan=True), field
     assert np.array_equal(F1["constant"], F2["constant"])
+
+
+def test_single_precision_refinement_pass_matches_double(monkeypatch):
+    """The refinement pass of every discharge solve reads a float copy of the
+    explicit inverse (it forms the small correction X r); against both passes
+    in double, on the benchmark network after 3 iterations and at
+    convergence: the same iteration count and every coefficient, q and
+    constant within 1e-12 of the potential scale."""
+    from andfn_b200.records import default_constants
+    from conftest import potential_scale
+    _, F0, E0 = golden_and_records("bench_c2")
+    for c in (default_constants(MAX_ITERATIONS=3, MAX_ERROR=1e-300, MAX_NCOEF=20),
+              default_constants(MAX_ITERATIONS=200, MAX_ERROR=1e-8, MAX_NCOEF=20)):
+        out = {}
+        for flag in ("0", "1"):
+            monkeypatch.setenv("ANDFN_B200_WINV_F32", flag)
+            F, E = F0.copy(), E0.copy()
+            st = _gpu_solve(F, E, c)
+            assert st["explicit_inverse"] == 1 and st["refined_solves"] > 0, st
+            out[flag] = (F, E, st)
+        (F1, E1, s1), (F2, E2, s2) = out["0"], out["1"]
+        assert s1["iterations"] == s2["iterations"] and s1["status"] == s2["status"]
+        P = potential_scale(E1, F1)
+        for name, a, b in (("coef", E1["coef"], E2["coef"]), ("q", E1["q"], E2["q"]),
+                           ("constant", F1["constant"], F2["constant"])):
+            d = float(np.abs(a - b).max())
+            print(f"float refinement pass, {s1['iterations']} iterations: max |d {name}|/P {d / P:.2e}")
+            assert d <= 1e-12 * P, (name, d / P)
