@@ -578,13 +578,10 @@ __global__ void __launch_bounds__(EVAL_THREADS) sweep_table_kernel(Net net, cons
                                                                      double *__restrict__ out, int chunk,
                                                                      const int *__restrict__ alist,
                                                                      const int *__restrict__ acount) {
-  if (alist) {  // grid-stride over the list (uniform over the CTA)
-    const int n = *acount;
-    for (int i = blockIdx.x; i < n; i += gridDim.x)
-      sweep_table_item(net, items[alist[i]], pts, groups, fpt0, fnp, tab_off, tw, tl, out, chunk);
-    return;
-  }
-  sweep_table_item(net, items[blockIdx.x], pts, groups, fpt0, fnp, tab_off, tw, tl, out, chunk);
+  // one call site (a second inlined copy of the item body made the kernel slower)
+  const int n = alist ? *acount : (int)gridDim.x;
+  for (int i = blockIdx.x; i < n; i += gridDim.x)  // uniform over the CTA
+    sweep_table_item(net, items[alist ? alist[i] : i], pts, groups, fpt0, fnp, tab_off, tw, tl, out, chunk);
 }
 
 // Persistent form: a grid of a few CTAs per SM takes the items (largest
@@ -822,16 +819,11 @@ __global__ void __launch_bounds__(UPDATE_WARPS * 32) update_kernel(Net net, cons
   double *v0 = reinterpret_cast<double *>(smem_raw) + (size_t)warp * 2 * nvmax;
   double *v1 = v0 + nvmax;
   const int idx = blockIdx.x * UPDATE_WARPS + warp;
-  if (ncount) {
-    const int n = *ncount;
-    for (int i = idx; i < n; i += gridDim.x * UPDATE_WARPS) {
-      __syncwarp();  // the previous element's reads of v0 / v1 are done
-      update_element(net, elist[i], group_of, groups, vals, v0, v1, blend_mode);
-    }
-    return;
+  const int n = ncount ? *ncount : nlist;
+  for (int i = idx; i < n; i += gridDim.x * UPDATE_WARPS) {
+    __syncwarp();  // the previous element's reads of v0 / v1 are done
+    update_element(net, elist[i], group_of, groups, vals, v0, v1, blend_mode);
   }
-  if (idx >= nlist) return;
-  update_element(net, elist[idx], group_of, groups, vals, v0, v1, blend_mode);
 }
 
 __device__ __forceinline__ void update_element(Net &net, int e, const int *__restrict__ group_of,
@@ -1150,15 +1142,11 @@ __device__ __forceinline__ void reduce_one(Net &net, int r) {
 // *acount on the device) the CTAs walk the running realizations.
 __global__ void __launch_bounds__(1024) reduce_kernel(Net net, const int *__restrict__ alist = nullptr,
                                                       const int *__restrict__ acount = nullptr) {
-  if (alist) {
-    const int n = *acount;
-    for (int i = blockIdx.x; i < n; i += gridDim.x) {
-      __syncthreads();  // the previous realization's merge is read
-      reduce_one(net, alist[i]);
-    }
-    return;
+  const int n = alist ? *acount : (int)gridDim.x;
+  for (int i = blockIdx.x; i < n; i += gridDim.x) {
+    __syncthreads();  // the previous realization's merge is read
+    reduce_one(net, alist ? alist[i] : i);
   }
-  reduce_one(net, blockIdx.x);
 }
 
 // A single network's reduction over several CTAs (REDUCE_SPLIT_ELEMS
@@ -2839,95 +2827,16 @@ __global__ void __launch_bounds__(WINV_THREADS) winv_upper_kernel(TriDesc TD, do
 static constexpr int WINV_RPC = 64;
 static_assert(WINV_THREADS == 512, "16 warps split each row of X");
 
-template <int STAGE, bool ADJ, bool F32 = false>
-__global__ void __launch_bounds__(WINV_THREADS, 2) winv_gemv_kernel(Net net, const double *__restrict__ X, int ldw,
-                                                                 const double *__restrict__ src,
-                                                                 double *__restrict__ x0,
-                                                                 unsigned long long *__restrict__ acc,
-                                                                 const float *__restrict__ X32 = nullptr) {
+// The end of a pass over X: the rows' sums (warp partials in s_part, added
+// in warp order), x0 or the final discharges / constants, and for the final
+// forward pass the max-change error of the solve (the last CTA turns the
+// grid's maxima into error_q and zeroes them for the next solve).
+template <int STAGE, bool ADJ>
+__device__ __forceinline__ void winv_epilogue(Net &net, const TriDesc &TD, int r0, int r1,
+                                              double (*s_part)[16], double *__restrict__ x0,
+                                              unsigned long long *__restrict__ acc, bool fin) {
   SolveState *st = net.st;
-  if (st->done) return;
-  // forward: without refinement (refine is set when the run starts) the
-  // first pass writes the result itself and the second does not run; the
-  // adjoint's transposed solves always take the refinement step
-  const bool fin = (STAGE == 1) || (!ADJ && !st->refine);
-  if (!ADJ) {
-    if (STAGE == 0 && blockIdx.x == 0 && threadIdx.x == 0) st->nit += 1;
-    if (!st->solve_q) return;  // uniform: solve_q is written only by reduce_kernel
-    if (STAGE == 1 && !st->refine) return;
-    if (STAGE == 1 && blockIdx.x == 0 && threadIdx.x == 0) st->n_refined += 1;
-  }
-  const TriDesc &TD = net.tri[0];
-  const int N = TD.n;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ double s_part[WINV_RPC][16];
-  double *v = reinterpret_cast<double *>(smem_raw);
-  for (int i = threadIdx.x; i < N; i += blockDim.x) v[__ldg(TD.pinv + i)] = src[i];
-  for (int i = N + threadIdx.x; i < ldw; i += blockDim.x) v[i] = 0.0;
-  __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int rpc = (N + gridDim.x - 1) / gridDim.x;  // <= WINV_RPC (grid size chosen by the host)
-  const int r0 = min(N, (int)blockIdx.x * rpc), r1 = min(N, r0 + rpc);
-  const int seg = ldw / 32;  // double2 per warp and row
-  const double2 *vs = reinterpret_cast<const double2 *>(v) + warp * seg;
-  const double2 zero2 = make_double2(0.0, 0.0);
-  // four rows at a time: per lane 8 loads of 16 B in flight per round (each
-  // row's segment in two halves of 32 double2), half the latency rounds of
-  // two rows at a time; rows beyond r1 reread row k (results not stored)
-  for (int k = r0; k < r1; k += 4) {
-    double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0, c0 = 0.0, c1 = 0.0, d0 = 0.0, d1 = 0.0;
-    if (F32) {
-      // float4 loads (four entries, 16 B): this warp's segment of a row is
-      // seg / 2 of them (ldw is a multiple of 64 when the float copy exists)
-      const int seg4 = seg / 2;
-      const size_t rf = ldw / 4;
-      const float4 *fa = reinterpret_cast<const float4 *>(X32) + (size_t)k * rf + (size_t)warp * seg4;
-      const float4 *fb = (k + 1 < r1) ? fa + rf : fa, *fc = (k + 2 < r1) ? fa + 2 * rf : fa,
-                   *fd = (k + 3 < r1) ? fa + 3 * rf : fa;
-      // one float4 of each of the four rows in flight per lane (64 B: the
-      // same bytes in flight per lane as the double pass's first half, in
-      // the register budget of two CTAs an SM)
-      for (int j = lane; j < seg4; j += 32) {
-        const float4 wa = __ldcs(fa + j), wb = __ldcs(fb + j), wc = __ldcs(fc + j), wd = __ldcs(fd + j);
-        const double2 p = vs[2 * j], q = vs[2 * j + 1];
-#define WINV_F4(ACC, F) \
-  ACC = fma((double)F.w, q.y, fma((double)F.z, q.x, fma((double)F.y, p.y, fma((double)F.x, p.x, ACC))))
-        WINV_F4(a0, wa);
-        WINV_F4(b0, wb);
-        WINV_F4(c0, wc);
-        WINV_F4(d0, wd);
-#undef WINV_F4
-      }
-    } else {
-      const double2 *ra = reinterpret_cast<const double2 *>(X + (size_t)k * ldw) + warp * seg;
-      const double2 *rb = (k + 1 < r1) ? ra + ldw / 2 : ra;
-      const double2 *rc = (k + 2 < r1) ? ra + ldw : ra;
-      const double2 *rd = (k + 3 < r1) ? ra + 3 * (size_t)(ldw / 2) : ra;
-      for (int j = lane; j < seg; j += 64) {
-        const bool h = j + 32 < seg;
-        const double2 wa0 = __ldcs(ra + j), wb0 = __ldcs(rb + j), wc0 = __ldcs(rc + j), wd0 = __ldcs(rd + j);
-        const double2 wa1 = h ? __ldcs(ra + j + 32) : zero2, wb1 = h ? __ldcs(rb + j + 32) : zero2;
-        const double2 wc1 = h ? __ldcs(rc + j + 32) : zero2, wd1 = h ? __ldcs(rd + j + 32) : zero2;
-        const double2 x0v = vs[j], x1v = h ? vs[j + 32] : zero2;
-        a0 = fma(wa0.y, x0v.y, fma(wa0.x, x0v.x, a0));
-        b0 = fma(wb0.y, x0v.y, fma(wb0.x, x0v.x, b0));
-        c0 = fma(wc0.y, x0v.y, fma(wc0.x, x0v.x, c0));
-        d0 = fma(wd0.y, x0v.y, fma(wd0.x, x0v.x, d0));
-        a1 = fma(wa1.y, x1v.y, fma(wa1.x, x1v.x, a1));
-        b1 = fma(wb1.y, x1v.y, fma(wb1.x, x1v.x, b1));
-        c1 = fma(wc1.y, x1v.y, fma(wc1.x, x1v.x, c1));
-        d1 = fma(wd1.y, x1v.y, fma(wd1.x, x1v.x, d1));
-      }
-    }
-    const double sa = warp_sum(a0 + a1), sb = warp_sum(b0 + b1), sc = warp_sum(c0 + c1), sd = warp_sum(d0 + d1);
-    if (lane == 0) {
-      s_part[k - r0][warp] = sa;
-      if (k + 1 < r1) s_part[k + 1 - r0][warp] = sb;
-      if (k + 2 < r1) s_part[k + 2 - r0][warp] = sc;
-      if (k + 3 < r1) s_part[k + 3 - r0][warp] = sd;
-    }
-  }
-  __syncthreads();
   double md = 0.0, mo = 0.0;
   for (int t = threadIdx.x; t < r1 - r0; t += blockDim.x) {
     double y = 0.0;
@@ -2987,6 +2896,98 @@ __global__ void __launch_bounds__(WINV_THREADS, 2) winv_gemv_kernel(Net net, con
     acc[1] = 0ull;
     acc[2] = 0ull;
   }
+}
+
+template <int STAGE, bool ADJ, bool F32 = false>
+__global__ void __launch_bounds__(WINV_THREADS, 2) winv_gemv_kernel(Net net, const double *__restrict__ X, int ldw,
+                                                                 const double *__restrict__ src,
+                                                                 double *__restrict__ x0,
+                                                                 unsigned long long *__restrict__ acc,
+                                                                 const float *__restrict__ X32 = nullptr) {
+  SolveState *st = net.st;
+  if (st->done) return;
+  // forward: without refinement (refine is set when the run starts) the
+  // first pass writes the result itself and the second does not run; the
+  // adjoint's transposed solves always take the refinement step
+  const bool fin = (STAGE == 1) || (!ADJ && !st->refine);
+  if (!ADJ) {
+    if (STAGE == 0 && blockIdx.x == 0 && threadIdx.x == 0) st->nit += 1;
+    if (!st->solve_q) return;  // uniform: solve_q is written only by reduce_kernel
+    if (STAGE == 1 && !st->refine) return;
+    if (STAGE == 1 && blockIdx.x == 0 && threadIdx.x == 0) st->n_refined += 1;
+  }
+  const TriDesc &TD = net.tri[0];
+  const int N = TD.n;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ double s_part[WINV_RPC][16];
+  double *v = reinterpret_cast<double *>(smem_raw);
+  for (int i = threadIdx.x; i < N; i += blockDim.x) v[__ldg(TD.pinv + i)] = src[i];
+  for (int i = N + threadIdx.x; i < ldw; i += blockDim.x) v[i] = 0.0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int rpc = (N + gridDim.x - 1) / gridDim.x;  // <= WINV_RPC (grid size chosen by the host)
+  const int r0 = min(N, (int)blockIdx.x * rpc), r1 = min(N, r0 + rpc);
+  const int seg = ldw / 32;  // double2 per warp and row
+  const double2 *vs = reinterpret_cast<const double2 *>(v) + warp * seg;
+  const double2 zero2 = make_double2(0.0, 0.0);
+  // four rows at a time: per lane 8 loads of 16 B in flight per round (each
+  // row's segment in two halves of 32 double2), half the latency rounds of
+  // two rows at a time; rows beyond r1 reread row k (results not stored)
+  for (int k = r0; k < r1; k += 4) {
+    double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0, c0 = 0.0, c1 = 0.0, d0 = 0.0, d1 = 0.0;
+    if (F32) {
+      // float4 loads (four entries, 16 B): this warp's segment of a row is
+      // seg / 2 of them (ldw is a multiple of 64 when the float copy exists)
+      const int seg4 = seg / 2;
+      const size_t rf = ldw / 4;
+      const float4 *fa = reinterpret_cast<const float4 *>(X32) + (size_t)k * rf + (size_t)warp * seg4;
+      const float4 *fb = (k + 1 < r1) ? fa + rf : fa, *fc = (k + 2 < r1) ? fa + 2 * rf : fa,
+                   *fd = (k + 3 < r1) ? fa + 3 * rf : fa;
+      // one float4 of each of the four rows in flight per lane (64 B; two
+      // of each spilled registers in the budget of two CTAs an SM and ran
+      // slower)
+      for (int j = lane; j < seg4; j += 32) {
+        const float4 wa = __ldcs(fa + j), wb = __ldcs(fb + j), wc = __ldcs(fc + j), wd = __ldcs(fd + j);
+        const double2 p = vs[2 * j], q = vs[2 * j + 1];
+#define WINV_F4(ACC, F) \
+  ACC = fma((double)F.w, q.y, fma((double)F.z, q.x, fma((double)F.y, p.y, fma((double)F.x, p.x, ACC))))
+        WINV_F4(a0, wa);
+        WINV_F4(b0, wb);
+        WINV_F4(c0, wc);
+        WINV_F4(d0, wd);
+#undef WINV_F4
+      }
+    } else {
+      const double2 *ra = reinterpret_cast<const double2 *>(X + (size_t)k * ldw) + warp * seg;
+      const double2 *rb = (k + 1 < r1) ? ra + ldw / 2 : ra;
+      const double2 *rc = (k + 2 < r1) ? ra + ldw : ra;
+      const double2 *rd = (k + 3 < r1) ? ra + 3 * (size_t)(ldw / 2) : ra;
+      for (int j = lane; j < seg; j += 64) {
+        const bool h = j + 32 < seg;
+        const double2 wa0 = __ldcs(ra + j), wb0 = __ldcs(rb + j), wc0 = __ldcs(rc + j), wd0 = __ldcs(rd + j);
+        const double2 wa1 = h ? __ldcs(ra + j + 32) : zero2, wb1 = h ? __ldcs(rb + j + 32) : zero2;
+        const double2 wc1 = h ? __ldcs(rc + j + 32) : zero2, wd1 = h ? __ldcs(rd + j + 32) : zero2;
+        const double2 x0v = vs[j], x1v = h ? vs[j + 32] : zero2;
+        a0 = fma(wa0.y, x0v.y, fma(wa0.x, x0v.x, a0));
+        b0 = fma(wb0.y, x0v.y, fma(wb0.x, x0v.x, b0));
+        c0 = fma(wc0.y, x0v.y, fma(wc0.x, x0v.x, c0));
+        d0 = fma(wd0.y, x0v.y, fma(wd0.x, x0v.x, d0));
+        a1 = fma(wa1.y, x1v.y, fma(wa1.x, x1v.x, a1));
+        b1 = fma(wb1.y, x1v.y, fma(wb1.x, x1v.x, b1));
+        c1 = fma(wc1.y, x1v.y, fma(wc1.x, x1v.x, c1));
+        d1 = fma(wd1.y, x1v.y, fma(wd1.x, x1v.x, d1));
+      }
+    }
+    const double sa = warp_sum(a0 + a1), sb = warp_sum(b0 + b1), sc = warp_sum(c0 + c1), sd = warp_sum(d0 + d1);
+    if (lane == 0) {
+      s_part[k - r0][warp] = sa;
+      if (k + 1 < r1) s_part[k + 1 - r0][warp] = sb;
+      if (k + 2 < r1) s_part[k + 2 - r0][warp] = sc;
+      if (k + 3 < r1) s_part[k + 3 - r0][warp] = sd;
+    }
+  }
+  __syncthreads();
+  winv_epilogue<STAGE, ADJ>(net, TD, r0, r1, s_part, x0, acc, fin);
 }
 
 // r = b - M x0 with M's rows in CSR form (one warp per row): M = A (vals in
@@ -3381,15 +3382,11 @@ __global__ void __launch_bounds__(BINV_SOLVE_THREADS) batch_winv_solve_kernel(
     Net net, const int *__restrict__ order, const int *__restrict__ roff, const long long *__restrict__ xoff,
     const double *__restrict__ Xall, const int *__restrict__ ptr, const int *__restrict__ col,
     const double *__restrict__ vals, const int *__restrict__ alist = nullptr, const int *__restrict__ acount = nullptr) {
-  if (alist) {
-    const int n = *acount;
-    for (int i = blockIdx.x; i < n; i += gridDim.x) {
-      __syncthreads();  // the previous realization's shared memory reads are done
-      batch_winv_solve_one(net, order[alist[i]], roff, xoff, Xall, ptr, col, vals);
-    }
-    return;
+  const int n = alist ? *acount : (int)gridDim.x;
+  for (int i = blockIdx.x; i < n; i += gridDim.x) {
+    __syncthreads();  // the previous realization's shared memory reads are done
+    batch_winv_solve_one(net, order[alist ? alist[i] : i], roff, xoff, Xall, ptr, col, vals);
   }
-  batch_winv_solve_one(net, order[blockIdx.x], roff, xoff, Xall, ptr, col, vals);
 }
 
 __device__ __forceinline__ void batch_winv_solve_one(Net &net, int r, const int *__restrict__ roff,
@@ -3482,12 +3479,9 @@ __global__ void __launch_bounds__(BINV_SOLVE_THREADS) batch_winv_solve_cluster_k
     const double *__restrict__ Xall, const int *__restrict__ ptr, const int *__restrict__ col,
     const double *__restrict__ vals, const int *__restrict__ alist, const int *__restrict__ acount) {
   const int cid = blockIdx.x / BINV_CLUSTER, ncl = gridDim.x / BINV_CLUSTER;
-  if (alist) {
-    const int n = *acount;
-    for (int i = cid; i < n; i += ncl) batch_winv_solve_cluster_one(net, big[alist[i]], roff, xoff, Xall, ptr, col, vals);
-    return;
-  }
-  batch_winv_solve_cluster_one(net, big[cid], roff, xoff, Xall, ptr, col, vals);
+  const int n = alist ? *acount : ncl;
+  for (int i = cid; i < n; i += ncl)
+    batch_winv_solve_cluster_one(net, big[alist ? alist[i] : i], roff, xoff, Xall, ptr, col, vals);
 }
 
 __device__ __forceinline__ void batch_winv_solve_cluster_one(Net &net, int r, const int *__restrict__ roff,
@@ -5647,19 +5641,26 @@ static int factor_all(AndfnHandle *H, const std::vector<double> &mv) {
                  {true, true, m0, n, 0, m0, false},
                  {false, true, 0, m0, m0, n, false},
                  {false, false, 0, m0, 0, m0, true}};
+    // the four parts' level tables, then appended in part order (building
+    // them on four host threads measured slower on the box)
+    std::vector<int> levk[4], rowsk[4], eptrk[4], ecolk[4];
+    std::vector<double> evk[4], esck[4];
     for (int k = 0; k < 4; k++) {
-      std::vector<int> lev, rows, eptr, ecol;
-      std::vector<double> ev, esc;
       const auto &sp = spec[k];
       // without a dense tail the coupling parts are empty
       const int rlo = (K == 0 && (k == 1 || k == 2)) ? 0 : sp.rlo;
       const int rhi = (K == 0 && (k == 1 || k == 2)) ? 0 : sp.rhi;
       if (sp.lower)
-        build_levels(n, F.l_ptr, F.l_col, F.l_val, nullptr, true, rlo, rhi, sp.clo, sp.chi, sp.single, lev, rows,
-                     eptr, ecol, ev, esc);
+        build_levels(n, F.l_ptr, F.l_col, F.l_val, nullptr, true, rlo, rhi, sp.clo, sp.chi, sp.single, levk[k],
+                     rowsk[k], eptrk[k], ecolk[k], evk[k], esck[k]);
       else
         build_levels(n, F.u_ptr, F.u_col, F.u_val, sp.scaled ? &F.u_inv_diag : nullptr, false, rlo, rhi, sp.clo,
-                     sp.chi, sp.single, lev, rows, eptr, ecol, ev, esc);
+                     sp.chi, sp.single, levk[k], rowsk[k], eptrk[k], ecolk[k], evk[k], esck[k]);
+    }
+    for (int k = 0; k < 4; k++) {
+      const auto &sp = spec[k];
+      const std::vector<int> &lev = levk[k], &rows = rowsk[k], &eptr = eptrk[k], &ecol = ecolk[k];
+      const std::vector<double> &ev = evk[k], &esc = esck[k];
       LevelParts &P = parts[k];
       off[r][k] = {(int)P.lev.size(), (int)P.rows.size(), (int)P.col.size()};
       nlev[r][k] = (int)lev.size() - 1;
@@ -8024,12 +8025,9 @@ __global__ void __launch_bounds__(T * RPB) head_vector_kernel(Net net, const int
   __shared__ double red[T / 32 > 0 ? T / 32 : 1];
   const int t = (T == 32) ? (threadIdx.x & 31) : threadIdx.x;
   const int g0 = blockIdx.x * RPB + ((T == 32) ? (threadIdx.x >> 5) : 0);
-  if (alist) {  // a batch's rows of running realizations
-    const int n = *acount;
-    for (int v = g0; v < n; v += gridDim.x * RPB) head_row<T>(net, alist[v], t, gptr, sidx, S, red);
-  } else if (g0 < net.N) {
-    head_row<T>(net, g0, t, gptr, sidx, S, red);
-  }
+  // a batch's rows of running realizations, or every row
+  const int n = alist ? *acount : net.N;
+  for (int v = g0; v < n; v += gridDim.x * RPB) head_row<T>(net, alist ? alist[v] : v, t, gptr, sidx, S, red);
 }
 
 __global__ void adj_rhs_gather_kernel(Net net, const int *__restrict__ src_ptr, const int *__restrict__ src_pairs,

@@ -196,3 +196,4 @@ def test_single_precision_refinement_pass_matches_double(monkeypatch):
             d = float(np.abs(a - b).max())
             print(f"float refinement pass, {s1['iterations']} iterations: max |d {name}|/P {d / P:.2e}")
             assert d <= 1e-12 * P, (name, d / P)
+
