@@ -802,12 +802,110 @@ __device__ __forceinline__ void dft_basis(const double *v0, const double *v1, in
   }
 }
 
-__device__ __forceinline__ void update_element(Net &net, int e, const int *__restrict__ group_of,
+// The running maximum of the element errors with its (first) index, the
+// maximum of the coefficient errors and a non-finite flag, with np.max /
+// np.argmax semantics: a NaN wins, the first index among equal maxima or
+// NaNs.  merge() is associative and commutative, so any split of the
+// elements gives the same result.
+struct ErrAcc {
+  double best = -INFINITY, bec = -INFINITY;
+  int bidx = 0x7fffffff, nonfin = 0;
+  // element i (visited in increasing order by one thread)
+  __device__ __forceinline__ void add(double e, double ec, int i) {
+    if (!(e == e)) {
+      if (best == best) {
+        best = NAN;
+        bidx = i;
+      } else {
+        bidx = min(bidx, i);
+      }
+      nonfin = 1;
+    } else if (best == best && (e > best || (e == best && i < bidx))) {
+      best = e;
+      bidx = i;
+    }
+    if (!(ec == ec)) {
+      bec = NAN;
+      nonfin = 1;
+    } else if (bec == bec && ec > bec) {
+      bec = ec;
+    }
+  }
+  __device__ __forceinline__ void merge(double ob, int oi, double oec, int onf) {
+    const bool onan = !(ob == ob), mnan = !(best == best);
+    if (onan && (!mnan || oi < bidx)) {
+      best = ob;
+      bidx = oi;
+    } else if (!onan && !mnan && (ob > best || (ob == best && oi < bidx))) {
+      best = ob;
+      bidx = oi;
+    }
+    if (!(oec == oec) || (bec == bec && oec > bec)) bec = oec;
+    nonfin |= onf;
+  }
+  __device__ __forceinline__ void warp_merge() {
+    for (int o = 16; o > 0; o >>= 1)
+      merge(__shfl_xor_sync(0xffffffffu, best, o), __shfl_xor_sync(0xffffffffu, bidx, o),
+            __shfl_xor_sync(0xffffffffu, bec, o), __shfl_xor_sync(0xffffffffu, nonfin, o));
+  }
+};
+
+// The block's ErrAcc into thread 0 (every thread calls it).
+template <int THREADS>
+__device__ __forceinline__ void block_merge(ErrAcc &a) {
+  __shared__ double s_err[THREADS / 32], s_ec[THREADS / 32];
+  __shared__ int s_idx[THREADS / 32], s_nf[THREADS / 32];
+  a.warp_merge();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) {
+    s_err[w] = a.best;
+    s_idx[w] = a.bidx;
+    s_ec[w] = a.bec;
+    s_nf[w] = a.nonfin;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int k = 1; k < THREADS / 32; k++) a.merge(s_err[k], s_idx[k], s_ec[k], s_nf[k]);
+}
+
+// The convergence rule of realization r from its errors (one thread).
+__device__ __forceinline__ void reduce_finish(Net &net, SolveState *st, const ErrAcc &a, int e0) {
+  int nf = a.nonfin;
+  st->error = a.best;
+  st->worst = a.bidx - e0;
+  st->error_coef = a.bec;
+  if (!(st->error_q == st->error_q)) nf = 1;
+  if (nf) st->nonfinite = 1;
+  // hpc_solve.py:237-239
+  if (a.bec < st->max_error && st->error_q < st->max_error) {
+    st->cnt_error += 1;
+    st->error_q = 1e30;
+  }
+  if (st->cnt_error >= 2 || st->nit >= st->max_it || st->nonfinite) {
+    st->done = 1;
+    atomicAdd(net.ndone, 1);
+  }
+  st->solve_q = (st->error_q > st->max_error / 1e30) ? 1 : 0;
+}
+
+static constexpr int REDUCE_SPLIT_THREADS = 256;
+static constexpr int REDUCE_SPLIT_ELEMS = 4 * REDUCE_SPLIT_THREADS;
+struct ReducePart {
+  double best, bec;
+  int bidx, nonfin;
+};
+
+// Returns false when the element's realization is done (nothing updated);
+// otherwise lane 0's er / erc are the element's new errors.
+__device__ __forceinline__ bool update_element(Net &net, int e, const int *__restrict__ group_of,
                                                const Group *__restrict__ groups, const double *__restrict__ vals,
-                                               double *v0, double *v1, int blend_mode);
+                                               double *v0, double *v1, int blend_mode, double &er, double &erc);
 
 // One warp per element of the list; with an active list (batches: its
 // length *ncount on the device) the warps walk the list (grid-stride).
+// (Reducing a single network's errors at the end of this kernel, the last
+// CTA merging the CTAs' partial maxima, measured 5 us slower an iteration
+// than the separate launch: 1,344 CTAs' fences and atomics on one ticket.)
 __global__ void __launch_bounds__(UPDATE_WARPS * 32) update_kernel(Net net, const int *__restrict__ elist, int nlist,
                                                                     const int *__restrict__ group_of,
                                                                     const Group *__restrict__ groups,
@@ -822,21 +920,25 @@ __global__ void __launch_bounds__(UPDATE_WARPS * 32) update_kernel(Net net, cons
   const int n = ncount ? *ncount : nlist;
   for (int i = idx; i < n; i += gridDim.x * UPDATE_WARPS) {
     __syncwarp();  // the previous element's reads of v0 / v1 are done
-    update_element(net, elist[i], group_of, groups, vals, v0, v1, blend_mode);
+    double er, erc;
+    update_element(net, elist[i], group_of, groups, vals, v0, v1, blend_mode, er, erc);
   }
 }
 
-__device__ __forceinline__ void update_element(Net &net, int e, const int *__restrict__ group_of,
+__device__ __forceinline__ bool update_element(Net &net, int e, const int *__restrict__ group_of,
                                                const Group *__restrict__ groups, const double *__restrict__ vals,
-                                               double *v0, double *v1, int blend_mode) {
+                                               double *v0, double *v1, int blend_mode, double &er_out,
+                                               double &erc_out) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   SolveState *st = net.st + net.real_elem[e];
-  if (st->done) return;
+  if (st->done) return false;
   const int type = net.type[e];
   const int MC = net.MC;
   if (type == 2) {  // hpc_solve.py:366-368
     if (lane == 0) net.err[e] = 0.0;
-    return;
+    er_out = 0.0;
+    erc_out = net.err_coef[e];
+    return true;
   }
   const int n = net.nint[e], m = net.ncoef[e];
   const Group g0 = groups[group_of[2 * e]];
@@ -955,6 +1057,8 @@ __device__ __forceinline__ void update_element(Net &net, int e, const int *__res
     net.err_old[e] = net.err[e];
     net.err[e] = er;
     net.err_coef[e] = erc;
+    er_out = er;
+    erc_out = erc;
   }
   // damped blends (hpc_solve.py:383-388 and, for nit >= 2, 561-575)
   const double d = st->damping;
@@ -967,6 +1071,7 @@ __device__ __forceinline__ void update_element(Net &net, int e, const int *__res
     // a non-finite leading coefficient ends the realization's loop (read by reduce_kernel)
     if (j == 0 && !isfinite(c.re)) st->nonfinite = 1;
   }
+  return true;
 }
 
 // ------------------------------------------------------------------------
@@ -1041,91 +1146,6 @@ __global__ void blend2_kernel(Net net) {
 // ------------------------------------------------------------------------
 // Max-reductions of the element errors and the convergence rule.
 // ------------------------------------------------------------------------
-// The running maximum of the element errors with its (first) index, the
-// maximum of the coefficient errors and a non-finite flag, with np.max /
-// np.argmax semantics: a NaN wins, the first index among equal maxima or
-// NaNs.  merge() is associative and commutative, so any split of the
-// elements gives the same result.
-struct ErrAcc {
-  double best = -INFINITY, bec = -INFINITY;
-  int bidx = 0x7fffffff, nonfin = 0;
-  // element i (visited in increasing order by one thread)
-  __device__ __forceinline__ void add(double e, double ec, int i) {
-    if (!(e == e)) {
-      if (best == best) {
-        best = NAN;
-        bidx = i;
-      } else {
-        bidx = min(bidx, i);
-      }
-      nonfin = 1;
-    } else if (best == best && (e > best || (e == best && i < bidx))) {
-      best = e;
-      bidx = i;
-    }
-    if (!(ec == ec)) {
-      bec = NAN;
-      nonfin = 1;
-    } else if (bec == bec && ec > bec) {
-      bec = ec;
-    }
-  }
-  __device__ __forceinline__ void merge(double ob, int oi, double oec, int onf) {
-    const bool onan = !(ob == ob), mnan = !(best == best);
-    if (onan && (!mnan || oi < bidx)) {
-      best = ob;
-      bidx = oi;
-    } else if (!onan && !mnan && (ob > best || (ob == best && oi < bidx))) {
-      best = ob;
-      bidx = oi;
-    }
-    if (!(oec == oec) || (bec == bec && oec > bec)) bec = oec;
-    nonfin |= onf;
-  }
-  __device__ __forceinline__ void warp_merge() {
-    for (int o = 16; o > 0; o >>= 1)
-      merge(__shfl_xor_sync(0xffffffffu, best, o), __shfl_xor_sync(0xffffffffu, bidx, o),
-            __shfl_xor_sync(0xffffffffu, bec, o), __shfl_xor_sync(0xffffffffu, nonfin, o));
-  }
-};
-
-// The block's ErrAcc into thread 0 (every thread calls it).
-template <int THREADS>
-__device__ __forceinline__ void block_merge(ErrAcc &a) {
-  __shared__ double s_err[THREADS / 32], s_ec[THREADS / 32];
-  __shared__ int s_idx[THREADS / 32], s_nf[THREADS / 32];
-  a.warp_merge();
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  if (lane == 0) {
-    s_err[w] = a.best;
-    s_idx[w] = a.bidx;
-    s_ec[w] = a.bec;
-    s_nf[w] = a.nonfin;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0)
-    for (int k = 1; k < THREADS / 32; k++) a.merge(s_err[k], s_idx[k], s_ec[k], s_nf[k]);
-}
-
-// The convergence rule of realization r from its errors (one thread).
-__device__ __forceinline__ void reduce_finish(Net &net, SolveState *st, const ErrAcc &a, int e0) {
-  int nf = a.nonfin;
-  st->error = a.best;
-  st->worst = a.bidx - e0;
-  st->error_coef = a.bec;
-  if (!(st->error_q == st->error_q)) nf = 1;
-  if (nf) st->nonfinite = 1;
-  // hpc_solve.py:237-239
-  if (a.bec < st->max_error && st->error_q < st->max_error) {
-    st->cnt_error += 1;
-    st->error_q = 1e30;
-  }
-  if (st->cnt_error >= 2 || st->nit >= st->max_it || st->nonfinite) {
-    st->done = 1;
-    atomicAdd(net.ndone, 1);
-  }
-  st->solve_q = (st->error_q > st->max_error / 1e30) ? 1 : 0;
-}
 
 __device__ __forceinline__ void reduce_one(Net &net, int r) {
   SolveState *st = net.st + r;
@@ -1153,12 +1173,6 @@ __global__ void __launch_bounds__(1024) reduce_kernel(Net net, const int *__rest
 // elements each, one element per thread and round): every CTA writes its
 // partial result, the last to finish merges them in CTA order and applies
 // the convergence rule, then resets the ticket for the next launch.
-static constexpr int REDUCE_SPLIT_THREADS = 256;
-static constexpr int REDUCE_SPLIT_ELEMS = 4 * REDUCE_SPLIT_THREADS;
-struct ReducePart {
-  double best, bec;
-  int bidx, nonfin;
-};
 __global__ void __launch_bounds__(REDUCE_SPLIT_THREADS) reduce_split_kernel(Net net, ReducePart *parts,
                                                                            unsigned *ticket) {
   SolveState *st = net.st;
@@ -1762,6 +1776,125 @@ __global__ void __launch_bounds__(256) dense_inverse_kernel(const double *__rest
   for (int idx = threadIdx.x; idx < K * ncl; idx += blockDim.x) {
     const int c = idx / K, i = idx - c * K;
     W[(size_t)(c0 + c) * K + i] = X[i * nc + c];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// The same W = U^-1 L^-1 by blocks of DINVB = 64 rows, GEMM-rich: the
+// per-column kernel above streams all of L and U through every CTA (2.9 GB
+// of L2 reads for K = 1,535, 2.6 TFLOP/s).  W (column-major, ld K) starts as
+// the identity; then
+//   forward, block i = 0, 1, ...: Y_i := L_ii^-1 Y_i on the columns up to
+//     the block's end (Y = L^-1 is lower triangular), then
+//     Y_below -= L_below,i Y_i (a GEMM with inner dimension 64);
+//   backward, block i = last, ..., 0: W_i := U_ii^-1 W_i on every column,
+//     then W_above -= U_above,i W_i.
+static constexpr int DINVB = 64;
+
+// Y[r0 .. r0+nb, c] := T^-1 Y[r0 .. r0+nb, c] for the columns c < ncols, T
+// the diagonal block of LU (unit lower, or upper scaled by uinv): a warp per
+// column, lane l holding rows l and l + 32, the solved value of each row
+// broadcast by a shuffle (a thread per column ran each column as one chain
+// of 2,016 dependent products, 29-86 us a block); the block is staged in
+// shared memory, zero outside nb (rows past nb stay zero).
+template <bool LOWER>
+__global__ void __launch_bounds__(256) dinvb_diag_kernel(const double *__restrict__ LU,
+                                                         const double *__restrict__ uinv, int K, int r0, int nb,
+                                                         int ncols, double *__restrict__ W) {
+  __shared__ double T[DINVB][DINVB + 1];  // T[row][col] of the diagonal block
+  __shared__ double di[DINVB];
+  for (int idx = threadIdx.x; idx < DINVB * DINVB; idx += blockDim.x) {
+    const int c = idx / DINVB, r = idx - c * DINVB;
+    T[r][c] = (r < nb && c < nb) ? LU[(size_t)(r0 + c) * K + r0 + r] : 0.0;
+  }
+  for (int r = threadIdx.x; r < DINVB; r += blockDim.x) di[r] = (LOWER || r >= nb) ? 1.0 : uinv[r0 + r];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (c >= ncols) return;  // uniform over the warp
+  double *w = W + (size_t)c * K + r0;
+  double x0 = (lane < nb) ? w[lane] : 0.0, x1 = (lane + 32 < nb) ? w[lane + 32] : 0.0;
+  if (LOWER) {
+    for (int j = 0; j < 32; j++) {
+      const double xj = __shfl_sync(0xffffffffu, x0, j);
+      if (lane > j) x0 = fma(-T[lane][j], xj, x0);
+      x1 = fma(-T[lane + 32][j], xj, x1);
+    }
+    for (int j = 0; j < 32; j++) {
+      const double xj = __shfl_sync(0xffffffffu, x1, j);
+      if (lane > j) x1 = fma(-T[lane + 32][j + 32], xj, x1);
+    }
+  } else {
+    for (int j = 31; j >= 0; j--) {
+      if (lane == j) x1 *= di[j + 32];
+      const double xj = __shfl_sync(0xffffffffu, x1, j);
+      if (lane < j) x1 = fma(-T[lane + 32][j + 32], xj, x1);
+      x0 = fma(-T[lane][j + 32], xj, x0);
+    }
+    for (int j = 31; j >= 0; j--) {
+      if (lane == j) x0 *= di[j];
+      const double xj = __shfl_sync(0xffffffffu, x0, j);
+      if (lane < j) x0 = fma(-T[lane][j], xj, x0);
+    }
+  }
+  if (lane < nb) w[lane] = x0;
+  if (lane + 32 < nb) w[lane + 32] = x1;
+}
+
+// C[m0 .. m0+M, 0 .. N) -= A[m0 .. m0+M, k0 .. k0+kb) B[k0 .. k0+kb, 0 .. N),
+// all column-major with leading dimension K (A a block column of L or U,
+// B and C rows of W): 64 x 64 tiles, 16 x 16 threads with 4 x 4 outputs.
+__global__ void __launch_bounds__(256) dinvb_gemm_kernel(const double *__restrict__ A, double *__restrict__ W, int K,
+                                                         int m0, int M, int k0, int kb, int N) {
+  __shared__ double As[16][64], Bs[16][65];
+  const int rb = blockIdx.x * 64, cb = blockIdx.y * 64;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  double acc[4][4];
+#pragma unroll
+  for (int r = 0; r < 4; r++)
+#pragma unroll
+    for (int q = 0; q < 4; q++) acc[r][q] = 0.0;
+  for (int kk0 = 0; kk0 < kb; kk0 += 16) {
+    for (int idx = threadIdx.x; idx < 16 * 64; idx += blockDim.x) {
+      const int kk = idx >> 6, i = idx & 63;  // A: rows contiguous in a column
+      const bool kv = kk0 + kk < kb;
+      As[kk][i] = (kv && rb + i < M) ? A[(size_t)(k0 + kk0 + kk) * K + m0 + rb + i] : 0.0;
+      const int c = idx >> 4, k2 = idx & 15;  // B: the 16 k of a column together
+      Bs[k2][c] = (kk0 + k2 < kb && cb + c < N) ? W[(size_t)(cb + c) * K + k0 + kk0 + k2] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < 16; kk++) {
+      double a[4], b[4];
+#pragma unroll
+      for (int r = 0; r < 4; r++) a[r] = As[kk][tx + 16 * r];
+#pragma unroll
+      for (int q = 0; q < 4; q++) b[q] = Bs[kk][ty + 16 * q];
+#pragma unroll
+      for (int r = 0; r < 4; r++)
+#pragma unroll
+        for (int q = 0; q < 4; q++) acc[r][q] = fma(a[r], b[q], acc[r][q]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int c = cb + ty + 16 * q;
+    if (c >= N) continue;
+    double *col = W + (size_t)c * K + m0;
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+      const int i = rb + tx + 16 * r;
+      if (i < M) col[i] -= acc[r][q];
+    }
+  }
+}
+
+__global__ void identity_kernel(double *__restrict__ W, int K) {
+  const size_t n = (size_t)K * K;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const size_t c = i / K, r = i - c * K;
+    W[i] = (r == c) ? 1.0 : 0.0;
   }
 }
 
@@ -2944,8 +3077,8 @@ __global__ void __launch_bounds__(WINV_THREADS, 2) winv_gemv_kernel(Net net, con
       const float4 *fb = (k + 1 < r1) ? fa + rf : fa, *fc = (k + 2 < r1) ? fa + 2 * rf : fa,
                    *fd = (k + 3 < r1) ? fa + 3 * rf : fa;
       // one float4 of each of the four rows in flight per lane (64 B; two
-      // of each spilled registers in the budget of two CTAs an SM and ran
-      // slower)
+      // of each spilled in the budget of two CTAs an SM and ran at 43 us,
+      // three at one CTA an SM ran at 37 us against 34 us)
       for (int j = lane; j < seg4; j += 32) {
         const float4 wa = __ldcs(fa + j), wb = __ldcs(fb + j), wc = __ldcs(fc + j), wd = __ldcs(fd + j);
         const double2 p = vs[2 * j], q = vs[2 * j + 1];
@@ -5129,7 +5262,7 @@ static int create_impl(AndfnHandle *H, int R, const char *const *F, const int64_
   CK(H->bvec.alloc(H->N));
   CK(H->ready.alloc(H->N));
   CK(H->st.alloc(R));
-  if (R == 1) {
+  if (R == 1) {  // partial results of the split reduction, one per CTA
     CK(H->red_parts.alloc((H->ne + REDUCE_SPLIT_ELEMS - 1) / REDUCE_SPLIT_ELEMS));
     CK(H->red_ticket.alloc(1));
     CK(cudaMemsetAsync(H->red_ticket.p, 0, sizeof(unsigned), s));
@@ -5262,6 +5395,28 @@ __global__ void recip_kernel(const double *__restrict__ d, double *__restrict__ 
 static int launch_tail_inverse(AndfnHandle *H, int K) {
   cudaStream_t s = H->stream;
   CK(H->tail_w.alloc((size_t)K * K));
+  // by blocks (ANDFN_B200_DINV_BLOCKED=0: a CTA per group of columns)
+  const char *eb = getenv("ANDFN_B200_DINV_BLOCKED");
+  if (!(eb && atoi(eb) == 0)) {
+    double *W = H->tail_w.p;
+    const double *LU = H->tail_l.p;
+    identity_kernel<<<4 * H->num_sms, 256, 0, s>>>(W, K);
+    const int nbk = (K + DINVB - 1) / DINVB;
+    for (int i = 0; i < nbk; i++) {  // forward: Y = L^-1, lower triangular
+      const int r0 = i * DINVB, nb = std::min(DINVB, K - r0), e = r0 + nb;
+      dinvb_diag_kernel<true><<<(e + 7) / 8, 256, 0, s>>>(LU, nullptr, K, r0, nb, e, W);
+      if (e < K)
+        dinvb_gemm_kernel<<<dim3((K - e + 63) / 64, (e + 63) / 64), 256, 0, s>>>(LU, W, K, e, K - e, r0, nb, e);
+    }
+    for (int i = nbk - 1; i >= 0; i--) {  // backward: W = U^-1 Y
+      const int r0 = i * DINVB, nb = std::min(DINVB, K - r0);
+      dinvb_diag_kernel<false><<<(K + 7) / 8, 256, 0, s>>>(LU, H->tail_uinv.p, K, r0, nb, K, W);
+      if (r0 > 0) dinvb_gemm_kernel<<<dim3((r0 + 63) / 64, (K + 63) / 64), 256, 0, s>>>(LU, W, K, 0, r0, r0, nb, K);
+    }
+    H->launches += 1 + 4 * nbk;
+    CK(cudaGetLastError());
+    return 0;
+  }
   // about one CTA per SM (nc columns of the inverse each)
   const int nc = std::max(1, std::min({DINV_NC, (int)(200 * 1024 / (sizeof(double) * (size_t)K)), K / H->num_sms}));
   dense_inverse_kernel<<<(K + nc - 1) / nc, 256, sizeof(double) * (size_t)K * nc, s>>>(H->tail_l.p, H->tail_l.p,

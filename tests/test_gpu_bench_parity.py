@@ -197,3 +197,31 @@ def test_single_precision_refinement_pass_matches_double(monkeypatch):
             print(f"float refinement pass, {s1['iterations']} iterations: max |d {name}|/P {d / P:.2e}")
             assert d <= 1e-12 * P, (name, d / P)
 
+
+
+def test_blocked_tail_inverse_matches_per_column_inverse(monkeypatch):
+    """The dense tail's inverse W22 = U22^-1 L22^-1 formed by 64-row blocks
+    (diagonal-block solves and GEMM updates) against the per-column solve:
+    a different summation order, so the states after 5 and 90 iterations
+    agree to round-off (1e-12 of the potential scale) with equal iteration
+    counts."""
+    from andfn_b200.records import default_constants
+    from conftest import potential_scale
+    _, F0, E0 = golden_and_records("bench_c2")
+    for c in (default_constants(MAX_ITERATIONS=5, MAX_ERROR=1e-300, MAX_NCOEF=20),
+              default_constants(MAX_ITERATIONS=200, MAX_ERROR=1e-8, MAX_NCOEF=20)):
+        out = {}
+        for flag in ("0", "1"):
+            monkeypatch.setenv("ANDFN_B200_DINV_BLOCKED", flag)
+            F, E = F0.copy(), E0.copy()
+            st = _gpu_solve(F, E, c)
+            assert st["dense_tail"] >= 64 and st["explicit_inverse"] == 1, st
+            out[flag] = (F, E, st)
+        (F1, E1, s1), (F2, E2, s2) = out["0"], out["1"]
+        assert s1["iterations"] == s2["iterations"] and s1["status"] == s2["status"]
+        P = potential_scale(E1, F1)
+        for name, a, b in (("coef", E1["coef"], E2["coef"]), ("q", E1["q"], E2["q"]),
+                           ("constant", F1["constant"], F2["constant"])):
+            d = float(np.abs(a - b).max())
+            print(f"blocked tail inverse, {s1['iterations']} iterations: max |d {name}|/P {d / P:.2e}")
+            assert d <= 1e-12 * P, (name, d / P)
