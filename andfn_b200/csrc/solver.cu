@@ -2239,9 +2239,12 @@ __device__ __forceinline__ bool dluc_barrier(DluSync *sy, unsigned nblocks) {
 // loads (other CTAs wrote it), stores it back and writes the pivots, U's
 // diagonal, the composite interchange and the bad-pivot flag.
 __device__ void dluc_panel(double *__restrict__ S, int K, int j0, int nb, const DluScratch &D, double *P) {
-  __shared__ double s_wv[DLUC_THREADS / 32];
-  __shared__ int s_wi[DLUC_THREADS / 32];
-  __shared__ int s_bad[DLUC_THREADS / 32];
+  // the warps' candidates, double-buffered by column parity: the next
+  // column's candidates are written before the barrier that ends the
+  // current column's reads, so the update needs no barrier of its own
+  __shared__ double s_wv[2][DLUC_THREADS / 32];
+  __shared__ int s_wi[2][DLUC_THREADS / 32];
+  __shared__ int s_bad[2][DLUC_THREADS / 32];
   __shared__ int s_piv[DLU_NB];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   constexpr int NW = DLUC_THREADS / 32;
@@ -2280,15 +2283,16 @@ __device__ void dluc_panel(double *__restrict__ S, int K, int j0, int nb, const 
       }
     }
     bad = __any_sync(0xffffffffu, bad);
+    const int pb = jj & 1;
     if (lane == 0) {
-      s_wv[warp] = best;
-      s_wi[warp] = bi;
-      s_bad[warp] = bad;
+      s_wv[pb][warp] = best;
+      s_wi[pb][warp] = bi;
+      s_bad[pb][warp] = bad;
     }
-    __syncthreads();
-    best = (lane < NW) ? s_wv[lane] : -1.0;
-    bi = (lane < NW) ? s_wi[lane] : m;
-    bad = (lane < NW) ? s_bad[lane] : 0;
+    __syncthreads();  // also: every thread's update by column jj - 1 is done
+    best = (lane < NW) ? s_wv[pb][lane] : -1.0;
+    bi = (lane < NW) ? s_wi[pb][lane] : m;
+    bad = (lane < NW) ? s_bad[pb][lane] : 0;
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
       const double ov = __shfl_down_sync(0xffffffffu, best, off);
@@ -2335,8 +2339,8 @@ __device__ void dluc_panel(double *__restrict__ S, int K, int j0, int nb, const 
         }
       }
     }
-    __syncthreads();
   }
+  __syncthreads();  // the last column's updates are done
   for (int c = 0; c < nb; c++)
     for (int i = tid; i < m; i += DLUC_THREADS) Sp[i + (size_t)c * K] = P[i * (DLU_NB + 1) + c];
   if (warp == 0) {
@@ -2373,7 +2377,7 @@ __device__ void dluc_panel(double *__restrict__ S, int K, int j0, int nb, const 
 }
 
 __global__ void __launch_bounds__(DLUC_THREADS, 1) dlu_coop_kernel(double *__restrict__ S, int K, DluScratch D,
-                                                                   DluSync *sy) {
+                                                                   DluSync *sy, unsigned *__restrict__ colcnt) {
   // one dynamic buffer, used by one phase at a time: the panel (CTA 0), or
   // L11 (phase S), or an item's L21 rows and U12 block (phase G)
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -2400,8 +2404,12 @@ __global__ void __launch_bounds__(DLUC_THREADS, 1) dlu_coop_kernel(double *__res
     const int cnt = __ldcg(D.swap_cnt);
     const int sw_src = (lane < cnt) ? __ldcg(D.swap_src + lane) : 0;
     const int sw_dst = (lane < cnt) ? __ldcg(D.swap_dst + lane) : 0;
+    // the trailing columns first (from c0: panel k+1's columns on CTA 0's
+    // warps), then the columns left of the panel (interchanges only); each
+    // trailing column done bumps its 16-column block's counter, which the G
+    // items of that block wait for (no grid barrier between S and G)
     for (int cidx = cta * NW + warp; cidx < K - nb; cidx += G * NW) {
-      const int c = (cidx < j0) ? cidx : cidx + nb;
+      const int c = (cidx < mt) ? c0 + cidx : cidx - mt;
       double *col = S + (size_t)c * K;
       double v = 0.0;
       if (lane < cnt) v = __ldcg(col + sw_src);
@@ -2416,8 +2424,10 @@ __global__ void __launch_bounds__(DLUC_THREADS, 1) dlu_coop_kernel(double *__res
         if (lane > j && lane < nb) x = fma(-L11[lane][j], xj, x);
       }
       if (lane < nb) col[j0 + lane] = x;
+      __threadfence();
+      __syncwarp();
+      if (lane == 0) atomicAdd(&colcnt[c / DLU_NB], 1u);
     }
-    if (!dluc_barrier(sy, G)) return;
     if (mt <= 0) break;
     // G(k): items (row tile, column block); column block 0 = panel k+1
     const int nrt = (mt + DLUC_TR - 1) / DLUC_TR, ncb = (mt + DLU_NB - 1) / DLU_NB;
@@ -2429,7 +2439,27 @@ __global__ void __launch_bounds__(DLUC_THREADS, 1) dlu_coop_kernel(double *__res
         const int cb = it / nrt, rt = it - cb * nrt;
         const int r0 = rt * DLUC_TR, cc0 = cb * DLU_NB;
         const int ncols = min(DLU_NB, mt - cc0);
-        __syncthreads();  // the previous item's reads of s_l / s_u are done
+        // the block's columns have had S(0 .. k): ncols bumps a panel
+        __shared__ int s_ok;
+        if (threadIdx.x == 0) {
+          volatile unsigned *cc = colcnt + (c0 + cc0) / DLU_NB;
+          volatile int *err = &sy->err;
+          const unsigned target = (unsigned)ncols * (unsigned)(k + 1);
+          unsigned spin = 0;
+          int ok = 1;
+          while (*cc < target) {
+            if (*err || ++spin > DLUC_SPIN_LIMIT) {
+              atomicExch(&sy->err, 1);
+              ok = 0;
+              break;
+            }
+            __nanosleep(32);
+          }
+          __threadfence();
+          s_ok = ok;
+        }
+        __syncthreads();  // also: the previous item's reads of s_l / s_u are done
+        if (!s_ok) break;
         for (int idx = threadIdx.x; idx < DLUC_TR * DLU_NB; idx += DLUC_THREADS) {
           const int kk = idx / DLUC_TR, i = idx - kk * DLUC_TR;
           s_l[i][kk] = (kk < nb && r0 + i < mt) ? __ldcg(S + (size_t)(j0 + kk) * K + c0 + r0 + i) : 0.0;
@@ -2459,11 +2489,9 @@ __global__ void __launch_bounds__(DLUC_THREADS, 1) dlu_coop_kernel(double *__res
           }
         }
         if (cb == 0) {
+          __threadfence();
           __syncthreads();
-          if (threadIdx.x == 0) {
-            __threadfence();
-            atomicAdd(&sy->cb0, 1u);
-          }
+          if (threadIdx.x == 0) atomicAdd(&sy->cb0, 1u);
         }
       }
     }
@@ -4427,7 +4455,9 @@ struct AndfnHandle {
   DBuf<double> tail_l, tail_uinv, tail_w;
   DBuf<int> dlu_i;  // device dense-LU scratch
   DBuf<double> dlu_d;
+  cudaEvent_t mv_ev = nullptr;  // the matrix values' copy to the host has landed
   DBuf<DluSync> dlu_sync;  // barrier state of the one-launch dense LU
+  DBuf<unsigned> dlu_colcnt;  // its per-16-column-block counters of finished S steps
   // explicit inverse of a single network's system (pivot order, rows padded
   // to winv_ldw), the system's CSR pattern and the solve's work arrays
   DBuf<double> winv, winv_t, wx0, wr;
@@ -4602,6 +4632,7 @@ struct AndfnHandle {
   ~AndfnHandle() {
     if (order_thread.joinable()) order_thread.join();
     if (dlu_ev) cudaEventDestroy(dlu_ev);
+    if (mv_ev) cudaEventDestroy(mv_ev);
     if (pin_schur) pinned_put(pin_schur, sizeof(double) * pin_schur_n);
     andfn::destroy_adj(adj);
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
@@ -5455,9 +5486,13 @@ static int gpu_dense_lu(AndfnHandle *H, LuFactors &F, bool want_w) {
     if (coop) {
       if (H->dlu_sync.cap < 1) CK(H->dlu_sync.alloc(1));
       CK(cudaMemsetAsync(H->dlu_sync.p, 0, sizeof(DluSync), s));
+      const int nblk = (K + DLU_NB - 1) / DLU_NB;
+      if (H->dlu_colcnt.cap < (size_t)nblk) CK(H->dlu_colcnt.alloc(nblk));
+      CK(cudaMemsetAsync(H->dlu_colcnt.p, 0, sizeof(unsigned) * nblk, s));
       DluSync *sy = H->dlu_sync.p;
+      unsigned *colcnt = H->dlu_colcnt.p;
       int Kv = K;
-      void *args[] = {(void *)&S, (void *)&Kv, (void *)&D, (void *)&sy};
+      void *args[] = {(void *)&S, (void *)&Kv, (void *)&D, (void *)&sy, (void *)&colcnt};
       CK(cudaLaunchCooperativeKernel((void *)dlu_coop_kernel, dim3(H->num_sms), dim3(DLUC_THREADS), args, sm, s));
       H->launches += 1;
     }
@@ -6551,9 +6586,31 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
   CK(cudaMemcpyAsync(H->ndone.p, &ndone0, sizeof(int), cudaMemcpyHostToDevice, s));
   auto t_setup = std::chrono::steady_clock::now();
   PhaseTimer pt;
+  // initial discharges (get_old_discharges, hpc_solve.py:765-775), uploaded
+  // before the set-up kernels (a pageable upload waits for the stream)
+  {
+    std::vector<double> disc0(H->N, 0.0);
+    for (int g = 0; g < H->N; g++) {
+      const int d = H->h.row_de[g];
+      disc0[g] = d >= 0 ? H->h.q[H->h.de_ids[d]] : H->h.constant[H->h.row_frac[g]];
+    }
+    CK(cudaMemcpyAsync(H->disc.p, disc0.data(), sizeof(double) * H->N, cudaMemcpyHostToDevice, s));
+    g_h2d_bytes += 8 * (int64_t)H->N;
+  }
   init_state_kernel<<<std::max<int64_t>(1, (H->ne + 255) / 256), 256, 0, s>>>(net);
   const int n_de = (int)H->h.de_ids.size();
   if (n_de > 0) zint_kernel<<<std::max(1, std::min(1184, (int)((n_de * H->D + 255) / 256))), 256, 0, s>>>(net);
+  // the matrix values first: the host factorisation waits for them only,
+  // while the device goes on with the rest of the set-up
+  const long long nent = (long long)H->ent_row.size();
+  if (nent > 0)
+    matrix_values_kernel<<<(unsigned)((nent * 32 + 255) / 256), 256, 0, s>>>(
+        net, H->d_ent_row.p, H->d_ent_src.p, H->d_ent_side.p, H->d_ent_kind.p, H->d_mvals.p, nent);
+  std::vector<double> mv(std::max<long long>(1, nent));
+  if (nent > 0) CK(cudaMemcpyAsync(mv.data(), H->d_mvals.p, sizeof(double) * nent, cudaMemcpyDeviceToHost, s));
+  g_d2h_bytes += 8 * nent;
+  if (!H->mv_ev) CK(cudaEventCreateWithFlags(&H->mv_ev, cudaEventDisableTiming));
+  CK(cudaEventRecord(H->mv_ev, s));
   if (H->n_psi > 0) cuts_kernel<<<(H->n_psi * 32 + 127) / 128, 128, 0, s>>>(net, H->psi_list.p, H->n_psi);
   // head vector from power sums and the sweep from pair tables, unless
   // coefficients may grow (then the points and series lengths change)
@@ -6578,24 +6635,9 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
       pt.lap("setup: pair tables");
     }
   }
-  const long long nent = (long long)H->ent_row.size();
-  if (nent > 0)
-    matrix_values_kernel<<<(unsigned)((nent * 32 + 255) / 256), 256, 0, s>>>(
-        net, H->d_ent_row.p, H->d_ent_src.p, H->d_ent_side.p, H->d_ent_kind.p, H->d_mvals.p, nent);
   H->launches += 4;
-  std::vector<double> mv(std::max<long long>(1, nent));
-  if (nent > 0) CK(cudaMemcpyAsync(mv.data(), H->d_mvals.p, sizeof(double) * nent, cudaMemcpyDeviceToHost, s));
-  g_d2h_bytes += 8 * nent;
-  // initial discharges (get_old_discharges, hpc_solve.py:765-775)
-  std::vector<double> disc0(H->N, 0.0);
-  for (int g = 0; g < H->N; g++) {
-    const int d = H->h.row_de[g];
-    disc0[g] = d >= 0 ? H->h.q[H->h.de_ids[d]] : H->h.constant[H->h.row_frac[g]];
-  }
-  CK(cudaMemcpyAsync(H->disc.p, disc0.data(), sizeof(double) * H->N, cudaMemcpyHostToDevice, s));
-  g_h2d_bytes += 8 * (int64_t)H->N;
-  CK(cudaStreamSynchronize(s));
-  pt.lap("setup: matrix values (sync)");
+  CK(cudaEventSynchronize(H->mv_ev));
+  pt.lap("setup: wait for matrix values");
   if (H->has_spec) {
     // the prescribed discharges' terms move to the right-hand side: minus
     // the entry times q in the rows, minus q in the continuity rows
