@@ -1953,9 +1953,9 @@ static constexpr size_t DLU_SMEM_MAX = 220 * 1024;
 struct DluScratch {
   int *piv;       // [K] block row swapped with row j at step j
   double *diag;   // [K] U(j, j)
-  int *swap_src;  // [2 DLU_NB] composite interchange of the last panel:
-  int *swap_dst;  //   row swap_dst[k] receives the old row swap_src[k]
-  int *swap_cnt;  // [1]
+  int *swap_src;  // [2][2 DLU_NB] composite interchange of a panel (slot = panel
+  int *swap_dst;  //   parity in the one-launch LU, slot 0 otherwise): row
+  int *swap_cnt;  // [2]  swap_dst[k] receives the old row swap_src[k]
   int *flag;      // [1] first zero / non-finite pivot column + 1 (0 = none)
 };
 
@@ -1964,6 +1964,42 @@ struct DluScratch {
 template <bool SMEM>
 __device__ __forceinline__ int dlu_at(int i, int c, int K) {
   return SMEM ? i * (DLU_NB + 1) + c : i + c * K;
+}
+
+// The interchanges of a panel (position j0 + jj swapped with j0 + s_piv[jj],
+// jj in order) as one permutation of at most 2 nb rows, by one warp: lane k
+// holds slot k (its row, and the row whose old content it gets).
+__device__ void dlu_compose_swaps(const int *s_piv, int j0, int nb, int *dst, int *src, int *cnt_out) {
+  const int lane = threadIdx.x & 31;
+  __syncwarp();
+  int row = -1, org = -1, cnt = 0;
+  for (int jj = 0; jj < nb; jj++) {
+    const int a = j0 + jj, b = j0 + s_piv[jj];
+    if (a == b) continue;
+    int ka, kb;
+    const unsigned ma = __ballot_sync(0xffffffffu, row == a);
+    if (ma) {
+      ka = __ffs(ma) - 1;
+    } else {
+      ka = cnt++;
+      if (lane == ka) row = org = a;
+    }
+    const unsigned mb = __ballot_sync(0xffffffffu, row == b);
+    if (mb) {
+      kb = __ffs(mb) - 1;
+    } else {
+      kb = cnt++;
+      if (lane == kb) row = org = b;
+    }
+    const int oa = __shfl_sync(0xffffffffu, org, ka), ob = __shfl_sync(0xffffffffu, org, kb);
+    if (lane == ka) org = ob;
+    if (lane == kb) org = oa;
+  }
+  if (lane < cnt) {
+    dst[lane] = row;
+    src[lane] = org;
+  }
+  if (lane == 0) *cnt_out = cnt;
 }
 
 template <bool SMEM>
@@ -2058,39 +2094,7 @@ __global__ void __launch_bounds__(DLU_THREADS) dlu_panel_kernel(double *__restri
     for (int c = 0; c < nb; c++)
       for (int i = tid; i < m; i += bd) Sp[i + c * K] = P[dlu_at<true>(i, c, K)];
   }
-  if (warp == 0) {
-    // the panel's interchanges as one permutation of at most 2 nb rows:
-    // lane k holds slot k (its row, and the row whose old content it gets)
-    __syncwarp();
-    int row = -1, org = -1, cnt = 0;
-    for (int jj = 0; jj < nb; jj++) {
-      const int a = j0 + jj, b = j0 + s_piv[jj];
-      if (a == b) continue;
-      int ka, kb;
-      const unsigned ma = __ballot_sync(0xffffffffu, row == a);
-      if (ma) {
-        ka = __ffs(ma) - 1;
-      } else {
-        ka = cnt++;
-        if (lane == ka) row = org = a;
-      }
-      const unsigned mb = __ballot_sync(0xffffffffu, row == b);
-      if (mb) {
-        kb = __ffs(mb) - 1;
-      } else {
-        kb = cnt++;
-        if (lane == kb) row = org = b;
-      }
-      const int oa = __shfl_sync(0xffffffffu, org, ka), ob = __shfl_sync(0xffffffffu, org, kb);
-      if (lane == ka) org = ob;
-      if (lane == kb) org = oa;
-    }
-    if (lane < cnt) {
-      D.swap_dst[lane] = row;
-      D.swap_src[lane] = org;
-    }
-    if (lane == 0) *D.swap_cnt = cnt;
-  }
+  if (warp == 0) dlu_compose_swaps(s_piv, j0, nb, D.swap_dst, D.swap_src, D.swap_cnt);
 }
 
 // One warp per column outside the panel: the panel's interchanges, then for
@@ -2169,19 +2173,21 @@ __global__ void __launch_bounds__(256) dlu_gemm_kernel(double *__restrict__ S, i
 
 // ---------------------------------------------------------------------------
 // The same dense LU in one cooperative launch with a look-ahead of one panel:
-// every panel step costs two grid barriers instead of three kernel launches,
-// and CTA 0 factorises panel k+1 while the other CTAs are still applying
-// panel k to the rest of the trailing block.
+// one grid barrier a panel step instead of three kernel launches, and CTA 0
+// factorises panel k+1 while the other CTAs are still applying panel k to
+// the rest of the trailing block.
 //   phase S(k)  all CTAs, a warp per column outside panel k: the panel's row
 //               interchanges, then U12 = L11^-1 A12 (as dlu_update_kernel);
-//   barrier;
-//   phase G(k)  A22 -= L21 U12 in items of DLUC_TR rows x DLU_NB columns (as
-//               dlu_gemm_kernel); the items of panel k+1's columns come
-//               first and each bumps a counter;
-//   phase P(k+1) CTA 0, once that counter shows panel k+1's columns are
-//               updated: the panel factorisation (as dlu_panel_kernel, the
-//               pivot search of a column fused with the update by the
-//               column before);
+//               panel k+1's columns are CTA 0's; every trailing column done
+//               bumps the counter of its 16-column block;
+//   phase P(k+1) CTA 0 at once: the update A22 -= L21 U12 of panel k+1's
+//               columns (as dlu_gemm_kernel) straight into shared memory,
+//               then the panel factorisation (as dlu_panel_kernel, the pivot
+//               search of a column fused with the update by the column
+//               before, the rows left in place);
+//   phase G(k)  the other CTAs: A22 -= L21 U12 for the other columns in
+//               items of DLUC_TR rows x DLU_NB columns, each item once its
+//               column block's counter shows S(k) done there;
 //   barrier.
 // Every product, quotient and fused multiply-add is the one the three-kernel
 // path computes, in the same order, so the factors are the same bit for bit.
@@ -2199,7 +2205,6 @@ static size_t dluc_smem(int K) {
 struct DluSync {
   unsigned count;  // CTAs arrived at the current barrier
   unsigned gen;    // barrier generation
-  unsigned cb0;    // G items of the next panel's columns finished (all panels)
   int err;         // a wait ran out
 };
 
@@ -2234,23 +2239,18 @@ __device__ __forceinline__ bool dluc_barrier(DluSync *sy, unsigned nblocks) {
   return s_ok != 0;
 }
 
-// Panel factorisation of columns j0 .. j0+nb-1 (rows j0 .. K-1) by one CTA in
-// shared memory P (m x (DLU_NB + 1), row-major); loads the panel with L2
-// loads (other CTAs wrote it), stores it back and writes the pivots, U's
-// diagonal, the composite interchange and the bad-pivot flag.
-__device__ void dluc_panel(double *__restrict__ S, int K, int j0, int nb, const DluScratch &D, double *P) {
-  // the warps' candidates, double-buffered by column parity: the next
-  // column's candidates are written before the barrier that ends the
-  // current column's reads, so the update needs no barrier of its own
-  __shared__ double s_wv[2][DLUC_THREADS / 32];
-  __shared__ int s_wi[2][DLUC_THREADS / 32];
-  __shared__ int s_bad[2][DLUC_THREADS / 32];
-  __shared__ int s_piv[DLU_NB];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  constexpr int NW = DLUC_THREADS / 32;
+// Rows of the panel a thread of dlu_coop_kernel holds: i = tid + r DLUC_THREADS.
+static constexpr int DLUC_ROWS = 4;
+static_assert(DLU_SMEM_MAX / (sizeof(double) * (DLU_NB + 1)) <= (size_t)DLUC_ROWS * DLUC_THREADS,
+              "a panel of the one-launch LU has at most DLUC_ROWS rows a thread");
+static_assert(DLUC_THREADS / 32 >= DLU_NB, "CTA 0's warps take the next panel's columns in phase S");
+
+// Loads the panel (columns j0 .. j0+nb-1, rows j0 .. K-1) into shared memory
+// P (row-major, padded rows) with L2 loads (other CTAs wrote it).
+__device__ void dluc_panel_load(const double *__restrict__ S, int K, int j0, int nb, double *P) {
   const int m = K - j0;
-  double *const Sp = S + (size_t)j0 * K + j0;
-  for (int i = tid; i < m; i += DLUC_THREADS) {
+  const double *const Sp = S + (size_t)j0 * K + j0;
+  for (int i = threadIdx.x; i < m; i += DLUC_THREADS) {
     double v[DLU_NB];
 #pragma unroll
     for (int c = 0; c < DLU_NB; c++) v[c] = (c < nb) ? __ldcg(Sp + i + (size_t)c * K) : 0.0;
@@ -2259,121 +2259,249 @@ __device__ void dluc_panel(double *__restrict__ S, int K, int j0, int nb, const 
       if (c < nb) P[i * (DLU_NB + 1) + c] = v[c];
   }
   __syncthreads();
-  // candidate of column 0
-  double best = -1.0;
-  int bi = m, bad = 0;
-  for (int i = tid; i < m; i += DLUC_THREADS) {
-    const double v = fabs(P[i * (DLU_NB + 1)]);
-    if (!(v <= DBL_MAX)) bad = 1;
-    if (v > best) {
-      best = v;
-      bi = i;
+}
+
+// Warp argmax of (key, position): the largest key, the smallest position on
+// a tie (key 0: no candidate); returns the winning lane.  Three redux
+// instructions and a ballot instead of a shuffle tree.
+__device__ __forceinline__ int dluc_warp_argmax(unsigned long long key, int pos) {
+  const unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
+  const unsigned mhi = __reduce_max_sync(0xffffffffu, hi);
+  const unsigned mlo = __reduce_max_sync(0xffffffffu, hi == mhi ? lo : 0u);
+  const bool top = hi == mhi && lo == mlo;
+  const unsigned mpos = __reduce_min_sync(0xffffffffu, top ? (unsigned)pos : 0xffffffffu);
+  return __ffs(__ballot_sync(0xffffffffu, top && (unsigned)pos == mpos)) - 1;
+}
+
+// Argmax key of a candidate magnitude v >= 0 (the bits of a non-negative
+// double order as the values do); none (v < 0) is 0.
+__device__ __forceinline__ unsigned long long dluc_key(double v) {
+  return (v >= 0.0) ? (unsigned long long)__double_as_longlong(v) + 1ull : 0ull;
+}
+
+// Columns c0+1 .. nb-1 of a row update by the pivot row (distinct rows of
+// P); column c0 < nb is updated first and returned (the next candidate).
+__device__ __forceinline__ double dluc_row_update(double *__restrict__ Pi, const double *__restrict__ Pq, double l,
+                                                  int c0, int nb) {
+  double x0 = 0.0;
+  if (c0 < nb) {
+    x0 = fma(-l, Pq[c0], Pi[c0]);
+    Pi[c0] = x0;
+  }
+#pragma unroll 4
+  for (int c = c0 + 1; c < nb; c++) Pi[c] = fma(-l, Pq[c], Pi[c]);
+  return x0;
+}
+
+// Panel factorisation of the panel in P (m = K - j0 rows) by one CTA.  The
+// rows do not move: a thread keeps the positions of its rows in registers
+// (position = the row's index after the interchanges so far), the pivot row
+// of column jj takes position jj and the row that held position jj takes the
+// pivot's old position, exactly the interchange of the row-swapping form.
+// The pivot is the largest magnitude, the smallest position on a tie, and
+// every quotient and fused multiply-add is the row-swapping form's, so the
+// factors are the same bit for bit.  A column: each warp's argmax, a block
+// barrier, warp 0's argmax over the warps and the one division, a block
+// barrier (the warps' candidates are double-buffered by column parity).
+// Stores the panel back in position order and writes the pivots, U's
+// diagonal, the bad-pivot flag and the composite interchange (slot par).
+__device__ void dluc_panel_factor(double *__restrict__ S, int K, int j0, int nb, const DluScratch &D, double *P,
+                                  int par) {
+  __shared__ unsigned long long s_wk[2][DLUC_THREADS / 32];
+  __shared__ double s_wv[2][DLUC_THREADS / 32];
+  __shared__ int s_wp[2][DLUC_THREADS / 32];
+  __shared__ int s_wq[2][DLUC_THREADS / 32];
+  __shared__ int s_bad[2][DLUC_THREADS / 32];
+  __shared__ int s_piv[DLU_NB];
+  __shared__ int s_p, s_q, s_found;
+  __shared__ double s_inv;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  constexpr int NW = DLUC_THREADS / 32;
+  const int m = K - j0;
+  int pos[DLUC_ROWS];
+  unsigned done = 0;  // bit r: the thread's row r is a pivot row
+#pragma unroll
+  for (int r = 0; r < DLUC_ROWS; r++) pos[r] = tid + r * DLUC_THREADS;
+  // candidate of column 0 (rows in position order): magnitude, position,
+  // row, signed value
+  double best = -1.0, bval = 0.0;
+  int bp = m, bq = m, bad = 0;
+#pragma unroll
+  for (int r = 0; r < DLUC_ROWS; r++) {
+    const int i = tid + r * DLUC_THREADS;
+    if (i < m) {
+      const double x = P[i * (DLU_NB + 1)], v = fabs(x);
+      if (!(v <= DBL_MAX)) bad = 1;
+      if (v > best) {
+        best = v;
+        bp = i;
+        bq = i;
+        bval = x;
+      }
     }
   }
   for (int jj = 0; jj < nb; jj++) {
-    // block argmax of column jj (largest magnitude, first row on a tie);
-    // every warp reduces the warps' candidates itself
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-      const double ov = __shfl_down_sync(0xffffffffu, best, off);
-      const int oi = __shfl_down_sync(0xffffffffu, bi, off);
-      if (ov > best || (ov == best && oi < bi)) {
-        best = ov;
-        bi = oi;
-      }
-    }
-    bad = __any_sync(0xffffffffu, bad);
+    // block argmax of column jj: each warp's, then warp 0's over the warps
     const int pb = jj & 1;
-    if (lane == 0) {
-      s_wv[pb][warp] = best;
-      s_wi[pb][warp] = bi;
-      s_bad[pb][warp] = bad;
+    {
+      const unsigned long long key = dluc_key(best);
+      const int wl = dluc_warp_argmax(key, bp);
+      bad = __any_sync(0xffffffffu, bad);
+      if (lane == wl) {
+        s_wk[pb][warp] = key;
+        s_wp[pb][warp] = bp;
+        s_wq[pb][warp] = bq;
+        s_wv[pb][warp] = bval;
+      }
+      if (lane == 0) s_bad[pb][warp] = bad;
     }
     __syncthreads();  // also: every thread's update by column jj - 1 is done
-    best = (lane < NW) ? s_wv[pb][lane] : -1.0;
-    bi = (lane < NW) ? s_wi[pb][lane] : m;
-    bad = (lane < NW) ? s_bad[pb][lane] : 0;
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-      const double ov = __shfl_down_sync(0xffffffffu, best, off);
-      const int oi = __shfl_down_sync(0xffffffffu, bi, off);
-      if (ov > best || (ov == best && oi < bi)) {
-        best = ov;
-        bi = oi;
+    if (warp == 0) {
+      const unsigned long long k2 = (lane < NW) ? s_wk[pb][lane] : 0ull;
+      const int p2 = (lane < NW) ? s_wp[pb][lane] : m;
+      const int bad2 = __any_sync(0xffffffffu, (lane < NW) ? s_bad[pb][lane] : 0);
+      const int wl2 = dluc_warp_argmax(k2, p2);
+      if (lane == wl2) {
+        const bool found = k2 != 0ull;
+        const double piv = s_wv[pb][lane];
+        s_found = found;
+        if (found) {
+          s_p = p2;
+          s_q = s_wq[pb][lane];
+          s_inv = (piv != 0.0) ? 1.0 / piv : 0.0;
+          s_piv[jj] = p2;
+          D.piv[j0 + jj] = j0 + p2;
+          D.diag[j0 + jj] = piv;
+        }
+        if ((bad2 || !found || !(fabs(piv) > 0.0)) && *D.flag == 0) *D.flag = j0 + jj + 1;
       }
     }
-    bad = __any_sync(0xffffffffu, bad);
-    int p = __shfl_sync(0xffffffffu, bi, 0);
-    const double bv = __shfl_sync(0xffffffffu, best, 0);
-    if (p >= m) p = jj;  // every entry NaN: keep the diagonal, flagged below
-    if (tid == 0) {
-      s_piv[jj] = p;
-      D.piv[j0 + jj] = j0 + p;
-      if ((bad || !(bv > 0.0)) && *D.flag == 0) *D.flag = j0 + jj + 1;
-    }
-    if (p != jj && tid < nb) {
-      const double a = P[jj * (DLU_NB + 1) + tid], b = P[p * (DLU_NB + 1) + tid];
-      P[jj * (DLU_NB + 1) + tid] = b;
-      P[p * (DLU_NB + 1) + tid] = a;
-    }
     __syncthreads();
-    const double piv = P[jj * (DLU_NB + 1) + jj];
-    if (tid == 0) D.diag[j0 + jj] = piv;
-    const double inv = (piv != 0.0) ? 1.0 / piv : 0.0;
+    int p, q;
+    double inv;
+    if (s_found) {
+      p = s_p;
+      q = s_q;
+      inv = s_inv;
+    } else {
+      // every entry NaN: the row at position jj stays (flagged above); its
+      // holder names it (the same branch in every thread)
+      p = jj;
+#pragma unroll
+      for (int r = 0; r < DLUC_ROWS; r++) {
+        const int i = tid + r * DLUC_THREADS;
+        if (i < m && !((done >> r) & 1u) && pos[r] == jj) s_q = i;
+      }
+      __syncthreads();
+      q = s_q;
+      const double piv = P[q * (DLU_NB + 1) + jj];
+      inv = (piv != 0.0) ? 1.0 / piv : 0.0;
+      if (tid == 0) {
+        s_piv[jj] = p;
+        D.piv[j0 + jj] = j0 + p;
+        D.diag[j0 + jj] = piv;
+      }
+    }
+    const double *const Pq = P + q * (DLU_NB + 1);
+    // the interchange, in positions
+#pragma unroll
+    for (int r = 0; r < DLUC_ROWS; r++) {
+      const int i = tid + r * DLUC_THREADS;
+      if (i == q) {
+        done |= 1u << r;
+        pos[r] = jj;
+      } else if (!((done >> r) & 1u) && pos[r] == jj) {
+        pos[r] = p;
+      }
+    }
     // update by column jj, and the candidate of column jj + 1
     best = -1.0;
-    bi = m;
+    bval = 0.0;
+    bp = m;
+    bq = m;
     bad = 0;
     const int nx = jj + 1;
-    for (int i = jj + 1 + tid; i < m; i += DLUC_THREADS) {
+#pragma unroll
+    for (int r = 0; r < DLUC_ROWS; r++) {
+      const int i = tid + r * DLUC_THREADS;
+      if (i >= m || ((done >> r) & 1u)) continue;
       double *Pi = P + i * (DLU_NB + 1);
       const double l = Pi[jj] * inv;
       Pi[jj] = l;
-      for (int c = jj + 1; c < nb; c++) Pi[c] = fma(-l, P[jj * (DLU_NB + 1) + c], Pi[c]);
+      const double x = dluc_row_update(Pi, Pq, l, nx, nb);
       if (nx < nb) {
-        const double v = fabs(Pi[nx]);
+        const double v = fabs(x);
         if (!(v <= DBL_MAX)) bad = 1;
-        if (v > best) {
+        if (v > best || (v == best && pos[r] < bp)) {
           best = v;
-          bi = i;
+          bp = pos[r];
+          bq = i;
+          bval = x;
         }
       }
     }
   }
   __syncthreads();  // the last column's updates are done
-  for (int c = 0; c < nb; c++)
-    for (int i = tid; i < m; i += DLUC_THREADS) Sp[i + (size_t)c * K] = P[i * (DLU_NB + 1) + c];
-  if (warp == 0) {
-    // the panel's interchanges as one permutation of at most 2 nb rows
-    int row = -1, org = -1, cnt = 0;
-    for (int jj = 0; jj < nb; jj++) {
-      const int a = j0 + jj, b = j0 + s_piv[jj];
-      if (a == b) continue;
-      int ka, kb;
-      const unsigned ma = __ballot_sync(0xffffffffu, row == a);
-      if (ma) {
-        ka = __ffs(ma) - 1;
-      } else {
-        ka = cnt++;
-        if (lane == ka) row = org = a;
-      }
-      const unsigned mb = __ballot_sync(0xffffffffu, row == b);
-      if (mb) {
-        kb = __ffs(mb) - 1;
-      } else {
-        kb = cnt++;
-        if (lane == kb) row = org = b;
-      }
-      const int oa = __shfl_sync(0xffffffffu, org, ka), ob = __shfl_sync(0xffffffffu, org, kb);
-      if (lane == ka) org = ob;
-      if (lane == kb) org = oa;
-    }
-    if (lane < cnt) {
-      D.swap_dst[lane] = row;
-      D.swap_src[lane] = org;
-    }
-    if (lane == 0) *D.swap_cnt = cnt;
+  double *const Sp = S + (size_t)j0 * K + j0;
+#pragma unroll
+  for (int r = 0; r < DLUC_ROWS; r++) {
+    const int i = tid + r * DLUC_THREADS;
+    if (i < m)
+      for (int c = 0; c < nb; c++) Sp[pos[r] + (size_t)c * K] = P[i * (DLU_NB + 1) + c];
   }
+  if (warp == 0)
+    dlu_compose_swaps(s_piv, j0, nb, D.swap_dst + par * 2 * DLU_NB, D.swap_src + par * 2 * DLU_NB,
+                      D.swap_cnt + par);
+}
+
+// CTA 0's part of G(k) for panel k+1's columns c0 .. c0+ncols-1 (their
+// interchanges and U12 rows are done by its own warps in S(k)): the update
+// A22 -= L21 U12 of their rows c0 .. K-1, each entry the fused multiply-add
+// chain of a G item, written straight into the panel buffer P of P(k+1).
+__device__ void dluc_next_panel(const double *__restrict__ S, int K, int j0, int c0, int ncols, double *P) {
+  __shared__ __align__(16) double s_u12[DLU_NB][DLU_NB];
+  const int mt = K - c0;
+  for (int idx = threadIdx.x; idx < DLU_NB * DLU_NB; idx += DLUC_THREADS) {
+    const int c = idx / DLU_NB, kk = idx - c * DLU_NB;
+    s_u12[kk][c] = (c < ncols) ? __ldcg(S + (size_t)(c0 + c) * K + j0 + kk) : 0.0;
+  }
+  __syncthreads();
+  for (int r = threadIdx.x; r < mt; r += DLUC_THREADS) {
+    // the row's L21 entries issued together; kk outer over the accumulators
+    // of a quarter of the columns (each still summed in kk order), U12 rows
+    // read 16 bytes at a time; a quarter's old values are loaded before its
+    // products
+    double a[DLU_NB];
+#pragma unroll
+    for (int kk = 0; kk < DLU_NB; kk++) a[kk] = __ldcg(S + (size_t)(j0 + kk) * K + c0 + r);
+#pragma unroll 1
+    for (int h = 0; h < 4; h++) {
+      constexpr int HC = DLU_NB / 4;
+      double acc[HC], o[HC];
+#pragma unroll
+      for (int c = 0; c < HC; c++) {
+        const int cc = h * HC + c;
+        o[c] = (cc < ncols) ? __ldcg(S + (size_t)(c0 + cc) * K + c0 + r) : 0.0;
+        acc[c] = 0.0;
+      }
+#pragma unroll
+      for (int kk = 0; kk < DLU_NB; kk++) {
+        const double2 *u2 = reinterpret_cast<const double2 *>(&s_u12[kk][h * HC]);
+#pragma unroll
+        for (int c2 = 0; c2 < HC / 2; c2++) {
+          const double2 u = u2[c2];
+          acc[2 * c2] = fma(a[kk], u.x, acc[2 * c2]);
+          acc[2 * c2 + 1] = fma(a[kk], u.y, acc[2 * c2 + 1]);
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < HC; c++) {
+        const int cc = h * HC + c;
+        if (cc < ncols) P[r * (DLU_NB + 1) + cc] = o[c] - acc[c];
+      }
+    }
+  }
+  __syncthreads();
 }
 
 __global__ void __launch_bounds__(DLUC_THREADS, 1) dlu_coop_kernel(double *__restrict__ S, int K, DluScratch D,
@@ -2390,24 +2518,27 @@ __global__ void __launch_bounds__(DLUC_THREADS, 1) dlu_coop_kernel(double *__res
   const int cta = blockIdx.x, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   constexpr int NW = DLUC_THREADS / 32;
   const int np = (K + DLU_NB - 1) / DLU_NB;
-  if (cta == 0) dluc_panel(S, K, 0, min(DLU_NB, K), D, P);
+  if (cta == 0) {
+    dluc_panel_load(S, K, 0, min(DLU_NB, K), P);
+    dluc_panel_factor(S, K, 0, min(DLU_NB, K), D, P, 0);
+  }
   if (!dluc_barrier(sy, G)) return;
-  unsigned cb0_target = 0;
   for (int k = 0; k < np; k++) {
     const int j0 = k * DLU_NB, nb = min(DLU_NB, K - j0), c0 = j0 + nb, mt = K - c0;
+    const int par = k & 1;
     // S(k): interchanges for every column outside the panel, U12 for the trailing ones
     for (int idx = threadIdx.x; idx < nb * nb; idx += DLUC_THREADS) {
       const int c = idx / nb, r = idx - c * nb;
       L11[r][c] = (r > c) ? __ldcg(S + (size_t)(j0 + c) * K + j0 + r) : 0.0;
     }
     __syncthreads();
-    const int cnt = __ldcg(D.swap_cnt);
-    const int sw_src = (lane < cnt) ? __ldcg(D.swap_src + lane) : 0;
-    const int sw_dst = (lane < cnt) ? __ldcg(D.swap_dst + lane) : 0;
-    // the trailing columns first (from c0: panel k+1's columns on CTA 0's
-    // warps), then the columns left of the panel (interchanges only); each
-    // trailing column done bumps its 16-column block's counter, which the G
-    // items of that block wait for (no grid barrier between S and G)
+    const int cnt = __ldcg(D.swap_cnt + par);
+    const int sw_src = (lane < cnt) ? __ldcg(D.swap_src + par * 2 * DLU_NB + lane) : 0;
+    const int sw_dst = (lane < cnt) ? __ldcg(D.swap_dst + par * 2 * DLU_NB + lane) : 0;
+    // the trailing columns first (from c0: panel k+1's columns are CTA 0's
+    // warps 0 .. DLU_NB-1), then the columns left of the panel (interchanges
+    // only); each trailing column done bumps its 16-column block's counter,
+    // which the G items of that block wait for (no grid barrier between S and G)
     for (int cidx = cta * NW + warp; cidx < K - nb; cidx += G * NW) {
       const int c = (cidx < mt) ? c0 + cidx : cidx - mt;
       double *col = S + (size_t)c * K;
@@ -2424,19 +2555,28 @@ __global__ void __launch_bounds__(DLUC_THREADS, 1) dlu_coop_kernel(double *__res
         if (lane > j && lane < nb) x = fma(-L11[lane][j], xj, x);
       }
       if (lane < nb) col[j0 + lane] = x;
+      if (c < c0 + DLU_NB) continue;  // panel k+1's columns: CTA 0's own, no counter
       __threadfence();
       __syncwarp();
       if (lane == 0) atomicAdd(&colcnt[c / DLU_NB], 1u);
     }
     if (mt <= 0) break;
-    // G(k): items (row tile, column block); column block 0 = panel k+1
+    // P(k+1) on CTA 0 right away: it updates panel k+1's columns itself (G's
+    // column block 0) and factorises them, while the other CTAs run G(k)'s
+    // other column blocks
+    const int ncols0 = min(DLU_NB, mt);
+    if (cta == 0) {
+      __syncthreads();  // S(k) of panel k+1's columns (this CTA's warps) is done; L11 reads too
+      dluc_next_panel(S, K, j0, c0, ncols0, P);
+      dluc_panel_factor(S, K, c0, ncols0, D, P, par ^ 1);
+    }
+    // G(k): items (row tile, column block >= 1)
     const int nrt = (mt + DLUC_TR - 1) / DLUC_TR, ncb = (mt + DLU_NB - 1) / DLU_NB;
-    const int nitems = nrt * ncb;
-    cb0_target += (unsigned)nrt;
+    const int nitems = nrt * (ncb - 1);
     const int first = (G > 1) ? cta - 1 : 0, stride = (G > 1) ? (int)G - 1 : 1;
     if (G == 1 || cta > 0) {
       for (int it = first; it < nitems; it += stride) {
-        const int cb = it / nrt, rt = it - cb * nrt;
+        const int cb = 1 + it / nrt, rt = it - (cb - 1) * nrt;
         const int r0 = rt * DLUC_TR, cc0 = cb * DLU_NB;
         const int ncols = min(DLU_NB, mt - cc0);
         // the block's columns have had S(0 .. k): ncols bumps a panel
@@ -2488,34 +2628,7 @@ __global__ void __launch_bounds__(DLUC_THREADS, 1) dlu_coop_kernel(double *__res
             }
           }
         }
-        if (cb == 0) {
-          __threadfence();
-          __syncthreads();
-          if (threadIdx.x == 0) atomicAdd(&sy->cb0, 1u);
-        }
       }
-    }
-    // P(k+1) on CTA 0 once panel k+1's columns are updated
-    if (cta == 0) {
-      __shared__ int s_go;
-      if (threadIdx.x == 0) {
-        volatile unsigned *cb0 = &sy->cb0;
-        volatile int *err = &sy->err;
-        unsigned it = 0;
-        int go = 1;
-        while (*cb0 < cb0_target) {
-          if (*err || ++it > DLUC_SPIN_LIMIT) {
-            atomicExch(&sy->err, 1);
-            go = 0;
-            break;
-          }
-          __nanosleep(64);
-        }
-        __threadfence();
-        s_go = go;
-      }
-      __syncthreads();
-      if (s_go) dluc_panel(S, K, c0, min(DLU_NB, mt), D, P);
     }
     if (!dluc_barrier(sy, G)) return;
   }
@@ -5467,10 +5580,10 @@ static int gpu_dense_lu(AndfnHandle *H, LuFactors &F, bool want_w) {
   CK(H->tail_l.alloc((size_t)K * K));
   CK(cudaMemcpyAsync(H->tail_l.p, F.schur, sizeof(double) * (size_t)K * K, cudaMemcpyHostToDevice, s));
   g_h2d_bytes += (int64_t)(sizeof(double) * (size_t)K * K);
-  CK(H->dlu_i.alloc((size_t)K + 4 * DLU_NB + 2));
+  CK(H->dlu_i.alloc((size_t)K + 8 * DLU_NB + 3));
   CK(H->dlu_d.alloc((size_t)K));
   int *ib = H->dlu_i.p;
-  DluScratch D{ib, H->dlu_d.p, ib + K, ib + K + 2 * DLU_NB, ib + K + 4 * DLU_NB, ib + K + 4 * DLU_NB + 1};
+  DluScratch D{ib, H->dlu_d.p, ib + K, ib + K + 4 * DLU_NB, ib + K + 8 * DLU_NB, ib + K + 8 * DLU_NB + 2};
   CK(cudaMemsetAsync(D.flag, 0, sizeof(int), s));
   double *S = H->tail_l.p;
   // one cooperative launch when the panel fits one CTA's shared memory and
