@@ -4554,8 +4554,12 @@ struct AndfnHandle {
   double ms_create_upload = 0, ms_create_tables = 0, ms_create_order = 0;
   // the column orders are computed on this host thread while the evaluation
   // tables are built and the first run's device set-up goes on; joined
-  // before the first factorisation (and on destruction)
+  // before the first factorisation (and on destruction).  A single network's
+  // order is also published column by column (order_prog), and the first
+  // factorisation takes its leading pivot steps as the columns arrive.
   std::thread order_thread;
+  OrderProgress order_prog;
+  bool order_follow = false;
   DBuf<double> disc, work, bvec;
   DBuf<int> ready;
   // factors of all realizations (level-ordered parts, dense tails, permutations)
@@ -5313,13 +5317,16 @@ static int create_impl(AndfnHandle *H, int R, const char *const *F, const int64_
     if (x > 0.0 && x <= 1.0) dense_frac = x;
   }
   H->dense_frac = dense_frac;
+  H->order_follow = R == 1 && !skip_order;
+  if (H->order_follow) H->order_prog.reset(H->sys[0].n);
   H->order_thread = std::thread([H, R, skip_order, dense_frac]() {
     auto tc2 = std::chrono::steady_clock::now();
     if (!skip_order) {
 #pragma omp parallel for schedule(dynamic, 1) if (R > 1)
       for (int r = 0; r < R; r++) {
         CscMatrix P = system_csc(H->sys[r], nullptr);
-        H->sys[r].colorder = column_min_degree_order(P, &H->sys[r].dense_k, dense_frac);
+        H->sys[r].colorder = column_min_degree_order(P, &H->sys[r].dense_k, dense_frac, 3072,
+                                                     H->order_follow ? &H->order_prog : nullptr);
       }
     }
     H->ms_create_order = ms_since(tc2);
@@ -5853,6 +5860,23 @@ static int factor_all(AndfnHandle *H, const std::vector<double> &mv) {
   }
   std::vector<LuFactors> LU(R);
   std::vector<int> rcs(R, 0);
+  auto tf0 = std::chrono::steady_clock::now();
+  // a single network whose column order is still being computed: its
+  // leading pivot steps follow the published order (the same steps in the
+  // same order as after it), then the thread is joined
+  LuLeading lead_st;
+  CscMatrix A0;
+  bool followed = false;
+  int lead_rc = 0;
+  if (H->order_thread.joinable()) {
+    if (R == 1 && H->order_follow) {
+      A0 = system_csc(H->sys[0], mv.data());
+      lu_leading_init(lead_st, A0.n);
+      lead_rc = lu_leading_follow(A0, H->order_prog, lead_st);
+      followed = true;
+    }
+    H->order_thread.join();
+  }
   // one realization: the Schur complement's columns use the host threads and
   // a large dense block is factorised on the device; several: one
   // realization per thread, dense blocks on the host
@@ -5882,10 +5906,15 @@ static int factor_all(AndfnHandle *H, const std::vector<double> &mv) {
       CscMatrix P = system_csc(H->sys[r], nullptr);
       H->sys[r].colorder = column_min_degree_order(P, &H->sys[r].dense_k, H->dense_frac);
     }
+    if (followed && r == 0) {
+      rcs[0] = lead_rc ? lead_rc
+                       : sparse_lu_factor_rest(A0, H->sys[0].colorder, lead_st, LU[0], H->sys[0].dense_k, defer,
+                                               schur_buf);
+      return;
+    }
     CscMatrix A = system_csc(H->sys[r], mv.data());
     rcs[r] = sparse_lu_factor(A, H->sys[r].colorder, 1.0, LU[r], H->sys[r].dense_k, defer, schur_buf);
   };
-  auto tf0 = std::chrono::steady_clock::now();
   if (R == 1) {
     factor_one(0);
   } else {
@@ -6765,7 +6794,7 @@ static int run_impl(AndfnHandle *H, const AndfnConstants *C, AndfnSolveStats *S)
   // factorisation (host)
   auto t_fac = std::chrono::steady_clock::now();
   pt.lap("setup: rest");
-  if (H->order_thread.joinable()) H->order_thread.join();
+  if (H->order_thread.joinable() && !H->order_follow) H->order_thread.join();
   pt.lap("factor: wait for column order");
   rc = factor_all(H, mv);
   if (rc) return rc;

@@ -20,6 +20,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <thread>
 #include <utility>
 
 namespace andfn {
@@ -62,9 +63,11 @@ struct DegreeBuckets {
 // weights), which is then updated and eliminated as one.  Degrees, element
 // sizes and |Lp| are weighted sums.  When a principal column is eliminated,
 // the order receives it and then the columns merged into it.
-std::vector<int> column_min_degree_order(const CscMatrix &A, int *dense_tail, double dense_frac, int max_dense) {
+std::vector<int> column_min_degree_order(const CscMatrix &A, int *dense_tail, double dense_frac, int max_dense,
+                                         OrderProgress *prog) {
   const int n = A.n;
   if (dense_tail) *dense_tail = 0;
+  if (prog && (int)prog->order.size() != n) prog->reset(n);
   // Ei[j]: the distinct rows of column j (the initial elements of variable j);
   // Le[r]: the columns of row r in increasing order (row r is the initial
   // element r, a clique of its columns); elements n.. are created by pivots.
@@ -128,7 +131,17 @@ std::vector<int> column_min_degree_order(const CscMatrix &A, int *dense_tail, do
   std::vector<int> order;
   order.reserve(n);
   auto emit = [&](int p) {
-    for (int v = p; v >= 0; v = svnext[v]) order.push_back(v);
+    for (int v = p; v >= 0; v = svnext[v]) {
+      if (prog) prog->order[order.size()] = v;
+      order.push_back(v);
+    }
+  };
+  // the leading columns are published after every pivot step, the tail at once
+  auto publish_done = [&](int lead) {
+    if (!prog) return;
+    prog->lead.store(lead, std::memory_order_release);
+    prog->count.store((int)order.size(), std::memory_order_release);
+    prog->done.store(1, std::memory_order_release);
   };
   int stamp = 0, estamp = 0, eliminated = 0;
   std::vector<int> emark(2 * (size_t)n + 1, -1);
@@ -144,15 +157,19 @@ std::vector<int> column_min_degree_order(const CscMatrix &A, int *dense_tail, do
       // remaining principal columns by (degree, index), each followed by the
       // columns merged into it.
       *dense_tail = remaining;
+      const int lead = (int)order.size();
+      if (prog) prog->lead.store(lead, std::memory_order_release);
       std::vector<std::pair<int, int>> rest;
       for (int j = 0; j < n; j++)
         if (alive[j]) rest.push_back({queue.deg[j], j});
       std::sort(rest.begin(), rest.end());
       for (auto &pr : rest) emit(pr.second);
+      publish_done(lead);
       return order;
     }
     const int p = queue.pop_min();
     emit(p);
+    if (prog) prog->count.store((int)order.size(), std::memory_order_release);
     eliminated += nv[p];
     alive[p] = 0;
     // New element: union of the active elements adjacent to p, minus p.
@@ -271,6 +288,7 @@ std::vector<int> column_min_degree_order(const CscMatrix &A, int *dense_tail, do
     for (int i : Lp)
       if (nv[i]) queue.insert(i, dnew[i]);
   }
+  publish_done((int)order.size());
   return order;
 }
 
@@ -331,130 +349,180 @@ static int dense_lu(double *S, int n, std::vector<int> &piv, double &min_piv) {
 static int finish_factors(LuFactors &F, LuPending &W, const std::vector<int> &dpiv, const double *S,
                           const double *tail_diag);
 
+void lu_leading_init(LuLeading &st, int n) {
+  st.n = n;
+  st.k = 0;
+  st.pinv.assign(n, -1);
+  st.prow.assign(n, -1);
+  st.Lcp.assign(1, 0);
+  st.Lri.clear();
+  st.Lv.clear();
+  st.Ucp.assign(1, 0);
+  st.Uri.clear();
+  st.Uv.clear();
+  st.diag.assign(n, 0.0);
+  st.x.assign(n, 0.0);
+  st.touched.assign(n, -1);
+  st.visited.assign(n, -1);
+  st.pattern.clear();
+  st.pattern.reserve(n);
+  st.topo.clear();
+  st.topo.reserve(n);
+  st.stack.clear();
+  st.childpos.clear();
+  st.min_piv = INFINITY;
+}
+
+int lu_leading_step(const CscMatrix &A, LuLeading &st, int col) {
+  const int k = st.k;
+  std::vector<int> &pinv = st.pinv, &prow = st.prow, &Lcp = st.Lcp, &Lri = st.Lri, &Ucp = st.Ucp, &Uri = st.Uri;
+  std::vector<double> &Lv = st.Lv, &Uv = st.Uv, &diag = st.diag, &x = st.x;
+  std::vector<int> &touched = st.touched, &visited = st.visited, &pattern = st.pattern, &topo = st.topo,
+                   &stack = st.stack, &childpos = st.childpos;
+  double &min_piv = st.min_piv;
+  pattern.clear();
+  topo.clear();
+  // Scatter A(:, col) and find the reach of its pivoted rows in L's graph.
+  for (int p = A.colptr[col]; p < A.colptr[col + 1]; p++) {
+    int r = A.rowind[p];
+    if (touched[r] != k) {
+      touched[r] = k;
+      pattern.push_back(r);
+      x[r] = 0.0;
+    }
+    x[r] += A.val[p];
+    int j = pinv[r];
+    if (j >= 0 && visited[j] != k) {
+      // iterative DFS from pivot step j over L's column structure
+      stack.clear();
+      childpos.clear();
+      stack.push_back(j);
+      childpos.push_back(Lcp[j]);
+      visited[j] = k;
+      while (!stack.empty()) {
+        int jj = stack.back();
+        int &cp = childpos.back();
+        bool pushed = false;
+        while (cp < Lcp[jj + 1]) {
+          int rr = Lri[cp++];
+          int j2 = pinv[rr];
+          if (j2 >= 0 && visited[j2] != k) {
+            visited[j2] = k;
+            stack.push_back(j2);
+            childpos.push_back(Lcp[j2]);
+            pushed = true;
+            break;
+          }
+        }
+        if (!pushed) {
+          topo.push_back(jj);
+          stack.pop_back();
+          childpos.pop_back();
+        }
+      }
+    }
+  }
+  // Numeric: apply the reached columns of L in topological order.
+  for (int t = (int)topo.size() - 1; t >= 0; t--) {
+    int j = topo[t];
+    const int rj = prow[j];
+    double xj = (touched[rj] == k) ? x[rj] : 0.0;
+    if (xj == 0.0) continue;
+    for (int p = Lcp[j]; p < Lcp[j + 1]; p++) {
+      int r = Lri[p];
+      if (touched[r] != k) {
+        touched[r] = k;
+        pattern.push_back(r);
+        x[r] = 0.0;
+      }
+      x[r] -= Lv[p] * xj;
+    }
+  }
+  // U(:, k): the pivoted rows, in topological order (dependency order).
+  for (int t = (int)topo.size() - 1; t >= 0; t--) {
+    int j = topo[t];
+    const int rj = prow[j];
+    double v = (touched[rj] == k) ? x[rj] : 0.0;
+    if (v != 0.0) {
+      Uri.push_back(j);
+      Uv.push_back(v);
+    }
+  }
+  Ucp.push_back((int)Uri.size());
+  // Partial pivoting over the not-yet-pivoted rows.
+  int piv = -1;
+  double amax = 0.0;
+  for (int r : pattern)
+    if (pinv[r] < 0) {
+      double a = std::fabs(x[r]);
+      if (a > amax || (a == amax && piv >= 0 && r < piv && a > 0)) {
+        amax = a;
+        piv = r;
+      }
+    }
+  if (piv < 0 || amax == 0.0 || !std::isfinite(amax)) return 3;
+  double pv = x[piv];
+  pinv[piv] = k;
+  prow[k] = piv;
+  diag[k] = pv;
+  if (amax < min_piv) min_piv = amax;
+  for (int r : pattern)
+    if (pinv[r] < 0 && x[r] != 0.0) {
+      Lri.push_back(r);
+      Lv.push_back(x[r] / pv);
+    }
+  Lcp.push_back((int)Lri.size());
+  st.k = k + 1;
+  return 0;
+}
+
+int lu_leading_follow(const CscMatrix &A, const OrderProgress &prog, LuLeading &st) {
+  for (;;) {
+    const int done = prog.done.load(std::memory_order_acquire);
+    const int count = prog.count.load(std::memory_order_acquire);
+    const int lead = prog.lead.load(std::memory_order_acquire);
+    const int lim = (lead >= 0) ? std::min(count, lead) : count;
+    if (st.k < lim) {
+      while (st.k < lim)
+        if (lu_leading_step(A, st, prog.order[st.k])) return 3;
+      continue;
+    }
+    if (done) return 0;
+    std::this_thread::yield();
+  }
+}
+
 int sparse_lu_factor(const CscMatrix &A, const std::vector<int> &q, double pivot_threshold, LuFactors &F,
                      int dense, bool defer_dense, double *schur_buf) {
+  (void)pivot_threshold;
+  const int n = A.n;
+  if (dense < 0 || dense > n) dense = 0;
+  LuLeading st;
+  lu_leading_init(st, n);
+  for (int k = 0; k < n - dense; k++)
+    if (lu_leading_step(A, st, q[k])) return 3;
+  return sparse_lu_factor_rest(A, q, st, F, dense, defer_dense, schur_buf);
+}
+
+int sparse_lu_factor_rest(const CscMatrix &A, const std::vector<int> &q, LuLeading &st, LuFactors &F, int dense,
+                          bool defer_dense, double *schur_buf) {
   const int n = A.n;
   if (dense < 0 || dense > n) dense = 0;
   const int m0 = n - dense;
+  if (st.n != n || st.k != m0) return 3;
   F.n = n;
   F.q = q;
   F.dense = dense;
-  F.pinv.assign(n, -1);
-  std::vector<int> prow(n, -1);
-  // Column-wise L (original row indices) and U (pivot-step indices).
-  std::vector<int> Lcp(1, 0), Lri;
-  std::vector<double> Lv;
-  std::vector<int> Ucp(1, 0), Uri;
-  std::vector<double> Uv;
-  std::vector<double> diag(n, 0.0);
-  std::vector<double> x(n, 0.0);
-  std::vector<int> touched(n, -1), pattern;
-  std::vector<int> visited(n, -1), topo, stack, childpos;
-  pattern.reserve(n);
-  topo.reserve(n);
-  double min_piv = INFINITY;
+  F.pinv = std::move(st.pinv);
+  std::vector<int> &prow = st.prow, &Lcp = st.Lcp, &Lri = st.Lri, &Ucp = st.Ucp, &Uri = st.Uri;
+  std::vector<double> &Lv = st.Lv, &Uv = st.Uv, &diag = st.diag;
+  double min_piv = st.min_piv;
   std::vector<int> tail_row;           // dense-block row of each original row (or -1)
   // Schur complement, column-major dense x dense (columns zeroed by the
   // thread that forms them)
   std::unique_ptr<double[]> S_own;
   double *S = nullptr;
   std::vector<int> tail_rows;          // original rows of the dense block, in block order
-  for (int k = 0; k < m0; k++) {
-    const int col = q[k];
-    pattern.clear();
-    topo.clear();
-    // Scatter A(:, col) and find the reach of its pivoted rows in L's graph.
-    for (int p = A.colptr[col]; p < A.colptr[col + 1]; p++) {
-      int r = A.rowind[p];
-      if (touched[r] != k) {
-        touched[r] = k;
-        pattern.push_back(r);
-        x[r] = 0.0;
-      }
-      x[r] += A.val[p];
-      int j = F.pinv[r];
-      if (j >= 0 && visited[j] != k) {
-        // iterative DFS from pivot step j over L's column structure
-        stack.clear();
-        childpos.clear();
-        stack.push_back(j);
-        childpos.push_back(Lcp[j]);
-        visited[j] = k;
-        while (!stack.empty()) {
-          int jj = stack.back();
-          int &cp = childpos.back();
-          bool pushed = false;
-          while (cp < Lcp[jj + 1]) {
-            int rr = Lri[cp++];
-            int j2 = F.pinv[rr];
-            if (j2 >= 0 && visited[j2] != k) {
-              visited[j2] = k;
-              stack.push_back(j2);
-              childpos.push_back(Lcp[j2]);
-              pushed = true;
-              break;
-            }
-          }
-          if (!pushed) {
-            topo.push_back(jj);
-            stack.pop_back();
-            childpos.pop_back();
-          }
-        }
-      }
-    }
-    // Numeric: apply the reached columns of L in topological order.
-    for (int t = (int)topo.size() - 1; t >= 0; t--) {
-      int j = topo[t];
-      const int rj = prow[j];
-      double xj = (touched[rj] == k) ? x[rj] : 0.0;
-      if (xj == 0.0) continue;
-      for (int p = Lcp[j]; p < Lcp[j + 1]; p++) {
-        int r = Lri[p];
-        if (touched[r] != k) {
-          touched[r] = k;
-          pattern.push_back(r);
-          x[r] = 0.0;
-        }
-        x[r] -= Lv[p] * xj;
-      }
-    }
-    // U(:, k): the pivoted rows, in topological order (dependency order).
-    for (int t = (int)topo.size() - 1; t >= 0; t--) {
-      int j = topo[t];
-      const int rj = prow[j];
-      double v = (touched[rj] == k) ? x[rj] : 0.0;
-      if (v != 0.0) {
-        Uri.push_back(j);
-        Uv.push_back(v);
-      }
-    }
-    Ucp.push_back((int)Uri.size());
-    // Partial pivoting over the not-yet-pivoted rows.
-    int piv = -1;
-    double amax = 0.0;
-    for (int r : pattern)
-      if (F.pinv[r] < 0) {
-        double a = std::fabs(x[r]);
-        if (a > amax || (a == amax && piv >= 0 && r < piv && a > 0)) {
-          amax = a;
-          piv = r;
-        }
-      }
-    (void)pivot_threshold;
-    if (piv < 0 || amax == 0.0 || !std::isfinite(amax)) return 3;
-    double pv = x[piv];
-    F.pinv[piv] = k;
-    prow[k] = piv;
-    diag[k] = pv;
-    if (amax < min_piv) min_piv = amax;
-    for (int r : pattern)
-      if (F.pinv[r] < 0 && x[r] != 0.0) {
-        Lri.push_back(r);
-        Lv.push_back(x[r] / pv);
-      }
-    Lcp.push_back((int)Lri.size());
-  }
   if (dense > 0) {
     // The dense block: the rows not pivoted yet.  Its columns (the Schur
     // complement) depend only on the finished leading columns of L, so they

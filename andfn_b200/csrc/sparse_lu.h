@@ -8,6 +8,8 @@
 // and the device solves x = Q U^-1 L^-1 P b every iteration with a
 // dependency-driven kernel (see solver.cu).
 #pragma once
+#include <atomic>
+#include <cmath>
 #include <cstdint>
 #include <memory>
 #include <vector>
@@ -60,8 +62,47 @@ struct LuFactors {
 // *dense_tail (optional) receives the number of trailing columns that remain
 // once the minimum degree reaches dense_frac of the remaining columns (the
 // graph is then nearly complete; 0 if that never happens with >= 64 left).
+//
+// With prog, the order is also published while it is computed, for a
+// factorisation that runs beside it (see OrderProgress).
+struct OrderProgress;
 std::vector<int> column_min_degree_order(const CscMatrix &A, int *dense_tail = nullptr, double dense_frac = 0.15,
-                                         int max_dense = 3072);
+                                         int max_dense = 3072, OrderProgress *prog = nullptr);
+
+// A column order published while it is computed: order[0 .. count) are
+// final; lead >= 0 once the number of leading (sparse) columns is known,
+// and then no entry below lead changes; done once all n entries are there.
+// Stores are release, loads acquire.
+struct OrderProgress {
+  std::vector<int> order;  // n entries
+  std::atomic<int> count{0};
+  std::atomic<int> lead{-1};
+  std::atomic<int> done{0};
+  void reset(int n) {
+    order.assign(n, -1);
+    count.store(0);
+    lead.store(-1);
+    done.store(0);
+  }
+};
+
+// The left-looking sparse pivot steps of sparse_lu_factor, kept between
+// calls so that they can be taken while the column order is still being
+// computed (lu_leading_follow) and finished by sparse_lu_factor_rest.
+struct LuLeading {
+  int n = 0, k = 0;  // pivot steps taken
+  std::vector<int> pinv, prow, Lcp, Lri, Ucp, Uri;
+  std::vector<double> Lv, Uv, diag, x;
+  std::vector<int> touched, visited, pattern, topo, stack, childpos;
+  double min_piv = INFINITY;
+};
+void lu_leading_init(LuLeading &st, int n);
+// One pivot step on column col; 0, or 3 if it has no nonzero pivot.
+int lu_leading_step(const CscMatrix &A, LuLeading &st, int col);
+// Takes the pivot steps of the leading columns as the ordering publishes
+// them; returns once the ordering is done and every leading column is
+// factorised (0), or 3 on a zero pivot (the ordering is still waited for).
+int lu_leading_follow(const CscMatrix &A, const OrderProgress &prog, LuLeading &st);
 
 // LU with partial pivoting: left-looking sparse (Gilbert-Peierls) for the
 // first n - dense pivot steps, then the Schur complement of the last `dense`
@@ -70,6 +111,10 @@ std::vector<int> column_min_degree_order(const CscMatrix &A, int *dense_tail = n
 // column has no nonzero pivot.
 int sparse_lu_factor(const CscMatrix &A, const std::vector<int> &q, double pivot_threshold, LuFactors &out,
                      int dense = 0, bool defer_dense = false, double *schur_buf = nullptr);
+// sparse_lu_factor after its leading pivot steps (st.k == n - dense) were
+// taken by lu_leading_step / lu_leading_follow; the same factors.
+int sparse_lu_factor_rest(const CscMatrix &A, const std::vector<int> &q, LuLeading &st, LuFactors &out, int dense,
+                          bool defer_dense, double *schur_buf);
 
 // With defer_dense, sparse_lu_factor stops after forming the Schur complement
 // (out.schur: schur_buf when given, dense x dense doubles, e.g. page-locked

@@ -539,6 +539,7 @@ def run_batched(args, device, flush, sample=32):
     return {"workload": BATCH_WORKLOAD, "realizations": R, "realizations_this_rank": len(recs),
             "fractures": int(sum(len(F) for F, _ in recs_all)), "elements": int(sum(len(E) for _, E in recs_all)),
             "value": value, "unit": "realizations/s", "ms_per_step": total_ms / args.steps,
+            "step_ms": [round(x, 3) for x in ms],
             "gpu_launches_per_step": launches / args.steps,
             "sharding": f"{ws} rank(s), longest processing time first by sweep pairs",
             "e2e": {"value": R / (e2e_s / 1e3), "unit": "realizations/s", "statistic": "median, slowest rank",
