@@ -356,9 +356,11 @@ def run_gpu(args):
     # on this workload, from ncu captures of the plain-solve profile case
     # (discharge solve: the double pass, plus the refinement pass over the
     # float copy, or a second double pass without one, in the solves that
-    # refine)
-    pass64 = 231318784.0 + 1533440.0
-    pass32 = 115842304.0 + 456704.0
+    # refine); mean of two launches each of the capture
+    # `ncu --metrics gpu__time_duration.sum,dram__bytes_read.sum,dram__bytes_write.sum
+    #  -k regex:winv_gemv -s 8 -c 4 python bench.py --profile-case plain --profile-iterations 30`
+    pass64 = 231325056.0 + 2604416.0
+    pass32 = 115852928.0 + 663040.0
     ref_pass = pass32 if inverse and int(stats.get("refine_f32", 0)) == 1 else pass64
     measured_traffic = {"eval_sweep": 111.6e6 + 3.6e6,
                         "trisolve": pass64 + frac_ref * ref_pass if inverse else None}
