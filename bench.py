@@ -435,15 +435,15 @@ def run_gpu(args):
                                 "note": "series truncation residual at the collocation points (ncoef 20); "
                                         "convergence uses the reference's MAX_ERROR rule"},
                 "adjoint": adjoint, "large": large, "tracking": tracking}
-        # the north-star ratios, last so that a truncated copy of the line keeps them
-        line["north_star"] = north_star_summary(value, e2e_val, cpu, roof, batched, adjoint, large)
+        # the headline ratios, last so that a truncated copy of the line keeps them
+        line["headline"] = headline_summary(value, e2e_val, cpu, roof, batched, adjoint, large)
         print(json.dumps(line), flush=True)
     solver.close()
     if ws > 1:
         torch.distributed.destroy_process_group()
 
 
-def north_star_summary(value, e2e, cpu, roof, batched, adjoint, large):
+def headline_summary(value, e2e, cpu, roof, batched, adjoint, large):
     """Plain GPU vs CPU solves/s (device-resident and end to end), batched
     per-realization rate vs the plain single-network rate, gradient time vs
     forward time, the finite-difference check and the dominant kernel's
