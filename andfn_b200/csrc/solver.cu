@@ -2997,41 +2997,47 @@ __global__ void __launch_bounds__(WINV_THREADS) winv_lower_kernel(TriDesc TD, do
 // C (K x ldw, row-major) = W (K x K, column-major) T (K x ldw, row-major):
 // 64 x 64 tiles, 16-deep slices of W and T in shared memory, 4 x 4 outputs a
 // thread (rows and columns 16 apart, so loads and stores coalesce).
-__global__ void __launch_bounds__(256) winv_gemm_kernel(const double *__restrict__ W, int K,
-                                                        const double *__restrict__ T, int ldw,
-                                                        double *__restrict__ C) {
-  __shared__ double As[16][64], Bs[16][64];
-  const int rb = blockIdx.x * 64, cb = blockIdx.y * 64;
+__global__ void __launch_bounds__(256, 2) winv_gemm_kernel(const double *__restrict__ W, int K,
+                                                           const double *__restrict__ T, int ldw,
+                                                           double *__restrict__ C) {
+  // 128 x 64 tile of C a CTA, 8 x 4 a thread (rows ty + 16 r, columns
+  // tx + 16 q: the A reads broadcast in half-warps, the B reads consecutive),
+  // a 16-deep k step: 12 shared loads per 32 fused multiply-adds; every
+  // entry is one chain over k in order, whatever the tile
+  __shared__ double As[16][128], Bs[16][64];
+  const int rb = blockIdx.x * 128, cb = blockIdx.y * 64;
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  double acc[4][4];
+  double acc[8][4];
 #pragma unroll
-  for (int r = 0; r < 4; r++)
+  for (int r = 0; r < 8; r++)
 #pragma unroll
     for (int q = 0; q < 4; q++) acc[r][q] = 0.0;
   for (int k0 = 0; k0 < K; k0 += 16) {
+    for (int idx = threadIdx.x; idx < 16 * 128; idx += blockDim.x) {
+      const int kk = idx >> 7, i = idx & 127;
+      As[kk][i] = (k0 + kk < K && rb + i < K) ? __ldg(W + (size_t)(k0 + kk) * K + rb + i) : 0.0;
+    }
     for (int idx = threadIdx.x; idx < 16 * 64; idx += blockDim.x) {
       const int kk = idx >> 6, i = idx & 63;
-      const bool kv = k0 + kk < K;
-      As[kk][i] = (kv && rb + i < K) ? __ldg(W + (size_t)(k0 + kk) * K + rb + i) : 0.0;
-      Bs[kk][i] = (kv && cb + i < ldw) ? __ldg(T + (size_t)(k0 + kk) * ldw + cb + i) : 0.0;
+      Bs[kk][i] = (k0 + kk < K && cb + i < ldw) ? __ldg(T + (size_t)(k0 + kk) * ldw + cb + i) : 0.0;
     }
     __syncthreads();
 #pragma unroll
     for (int kk = 0; kk < 16; kk++) {
-      double a[4], b[4];
+      double a[8], b[4];
 #pragma unroll
-      for (int r = 0; r < 4; r++) a[r] = As[kk][ty + 16 * r];
+      for (int r = 0; r < 8; r++) a[r] = As[kk][ty + 16 * r];
 #pragma unroll
       for (int q = 0; q < 4; q++) b[q] = Bs[kk][tx + 16 * q];
 #pragma unroll
-      for (int r = 0; r < 4; r++)
+      for (int r = 0; r < 8; r++)
 #pragma unroll
         for (int q = 0; q < 4; q++) acc[r][q] = fma(a[r], b[q], acc[r][q]);
     }
     __syncthreads();
   }
 #pragma unroll
-  for (int r = 0; r < 4; r++) {
+  for (int r = 0; r < 8; r++) {
     const int i = rb + ty + 16 * r;
     if (i >= K) continue;
 #pragma unroll
@@ -5679,8 +5685,8 @@ static int build_inverse(AndfnHandle *H, const TriDesc &td) {
   const int nchunk = ldw / WINV_CW;
   winv_lower_kernel<<<nchunk, WINV_THREADS, 0, s>>>(td, H->winv.p, ldw, H->winv_t.p);
   if (K > 0) {
-    winv_gemm_kernel<<<dim3((K + 63) / 64, (ldw + 63) / 64), 256, 0, s>>>(H->tail_w.p, K, H->winv_t.p, ldw,
-                                                                         H->winv.p + (size_t)m0 * ldw);
+    winv_gemm_kernel<<<dim3((K + 127) / 128, (ldw + 63) / 64), 256, 0, s>>>(H->tail_w.p, K, H->winv_t.p, ldw,
+                                                                          H->winv.p + (size_t)m0 * ldw);
     if (td.Ux.nslots > 0)
       winv_coupling_kernel<<<dim3((td.Ux.nslots + WINV_COUPLE_ROWS - 1) / WINV_COUPLE_ROWS, (ldw + 255) / 256), 256,
                              0, s>>>(td.Ux, H->winv.p, ldw);
