@@ -1844,7 +1844,7 @@ __global__ void __launch_bounds__(256) dinvb_diag_kernel(const double *__restric
 // C[m0 .. m0+M, 0 .. N) -= A[m0 .. m0+M, k0 .. k0+kb) B[k0 .. k0+kb, 0 .. N),
 // all column-major with leading dimension K (A a block column of L or U,
 // B and C rows of W): 64 x 64 tiles, 16 x 16 threads with 4 x 4 outputs.
-__global__ void __launch_bounds__(256) dinvb_gemm_kernel(const double *__restrict__ A, double *__restrict__ W, int K,
+__global__ void __launch_bounds__(256, 3) dinvb_gemm_kernel(const double *__restrict__ A, double *__restrict__ W, int K,
                                                          int m0, int M, int k0, int kb, int N) {
   __shared__ double As[16][64], Bs[16][65];
   const int rb = blockIdx.x * 64, cb = blockIdx.y * 64;
@@ -1854,15 +1854,30 @@ __global__ void __launch_bounds__(256) dinvb_gemm_kernel(const double *__restric
   for (int r = 0; r < 4; r++)
 #pragma unroll
     for (int q = 0; q < 4; q++) acc[r][q] = 0.0;
+  // a k step's tiles are loaded into registers while the step before it
+  // computes (4 entries of A and 4 of B a thread), then stored to shared
+  // memory: A's rows contiguous in a column, B's 16 k of a column together
+  double la[4], lb[4];
+  auto load_step = [&](int kk0) {
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const int idx = threadIdx.x + 256 * u;
+      const int kk = idx >> 6, i = idx & 63;
+      la[u] = (kk0 + kk < kb && rb + i < M) ? A[(size_t)(k0 + kk0 + kk) * K + m0 + rb + i] : 0.0;
+      const int c = idx >> 4, k2 = idx & 15;
+      lb[u] = (kk0 + k2 < kb && cb + c < N) ? W[(size_t)(cb + c) * K + k0 + kk0 + k2] : 0.0;
+    }
+  };
+  load_step(0);
   for (int kk0 = 0; kk0 < kb; kk0 += 16) {
-    for (int idx = threadIdx.x; idx < 16 * 64; idx += blockDim.x) {
-      const int kk = idx >> 6, i = idx & 63;  // A: rows contiguous in a column
-      const bool kv = kk0 + kk < kb;
-      As[kk][i] = (kv && rb + i < M) ? A[(size_t)(k0 + kk0 + kk) * K + m0 + rb + i] : 0.0;
-      const int c = idx >> 4, k2 = idx & 15;  // B: the 16 k of a column together
-      Bs[k2][c] = (kk0 + k2 < kb && cb + c < N) ? W[(size_t)(cb + c) * K + k0 + kk0 + k2] : 0.0;
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const int idx = threadIdx.x + 256 * u;
+      As[idx >> 6][idx & 63] = la[u];
+      Bs[idx & 15][idx >> 4] = lb[u];
     }
     __syncthreads();
+    if (kk0 + 16 < kb) load_step(kk0 + 16);
 #pragma unroll
     for (int kk = 0; kk < 16; kk++) {
       double a[4], b[4];
