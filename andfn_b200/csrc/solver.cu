@@ -1392,6 +1392,11 @@ __device__ __forceinline__ void cp_async8(void *dst, const void *src) {
   const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
 }
+// 8 bytes from src, or zeros when !valid (source size 0: nothing is read)
+__device__ __forceinline__ void cp_async8_zfill(void *dst, const void *src, bool valid) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(valid ? 8 : 0) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
@@ -3018,8 +3023,10 @@ __global__ void __launch_bounds__(256, 2) winv_gemm_kernel(const double *__restr
   // 128 x 64 tile of C a CTA, 8 x 4 a thread (rows ty + 16 r, columns
   // tx + 16 q: the A reads broadcast in half-warps, the B reads consecutive),
   // a 16-deep k step: 12 shared loads per 32 fused multiply-adds; every
-  // entry is one chain over k in order, whatever the tile
-  __shared__ double As[16][128], Bs[16][64];
+  // entry is one chain over k in order, whatever the tile.  The next k
+  // step's tiles arrive by asynchronous copies (zero-filled outside the
+  // matrices) into the other half of a double buffer while this one computes.
+  __shared__ __align__(16) double As[2][16][128], Bs[2][16][64];
   const int rb = blockIdx.x * 128, cb = blockIdx.y * 64;
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   double acc[8][4];
@@ -3027,23 +3034,36 @@ __global__ void __launch_bounds__(256, 2) winv_gemm_kernel(const double *__restr
   for (int r = 0; r < 8; r++)
 #pragma unroll
     for (int q = 0; q < 4; q++) acc[r][q] = 0.0;
-  for (int k0 = 0; k0 < K; k0 += 16) {
+  auto issue = [&](int k0, int buf) {
     for (int idx = threadIdx.x; idx < 16 * 128; idx += blockDim.x) {
       const int kk = idx >> 7, i = idx & 127;
-      As[kk][i] = (k0 + kk < K && rb + i < K) ? __ldg(W + (size_t)(k0 + kk) * K + rb + i) : 0.0;
+      const bool v = k0 + kk < K && rb + i < K;
+      cp_async8_zfill(&As[buf][kk][i], v ? W + (size_t)(k0 + kk) * K + rb + i : W, v);
     }
     for (int idx = threadIdx.x; idx < 16 * 64; idx += blockDim.x) {
       const int kk = idx >> 6, i = idx & 63;
-      Bs[kk][i] = (k0 + kk < K && cb + i < ldw) ? __ldg(T + (size_t)(k0 + kk) * ldw + cb + i) : 0.0;
+      const bool v = k0 + kk < K && cb + i < ldw;
+      cp_async8_zfill(&Bs[buf][kk][i], v ? T + (size_t)(k0 + kk) * ldw + cb + i : T, v);
+    }
+    cp_async_commit();
+  };
+  issue(0, 0);
+  int buf = 0;
+  for (int k0 = 0; k0 < K; k0 += 16, buf ^= 1) {
+    if (k0 + 16 < K) {
+      issue(k0 + 16, buf ^ 1);  // that half was last read before the barrier ending the step before
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
     }
     __syncthreads();
 #pragma unroll
     for (int kk = 0; kk < 16; kk++) {
       double a[8], b[4];
 #pragma unroll
-      for (int r = 0; r < 8; r++) a[r] = As[kk][ty + 16 * r];
+      for (int r = 0; r < 8; r++) a[r] = As[buf][kk][ty + 16 * r];
 #pragma unroll
-      for (int q = 0; q < 4; q++) b[q] = Bs[kk][tx + 16 * q];
+      for (int q = 0; q < 4; q++) b[q] = Bs[buf][kk][tx + 16 * q];
 #pragma unroll
       for (int r = 0; r < 8; r++)
 #pragma unroll
